@@ -1,0 +1,235 @@
+/*
+ * raygen_b200.h - C ABI of the B200 wavefront path tracer.
+ *
+ * This is the drop-in boundary for RayGen's shader-5 (BSDF) render path.
+ * Every entry point takes plain pointers and sizes, returns an rg_status
+ * (0 = OK, negative = error), never throws across the boundary, and is
+ * thread-safe per handle (one render in flight per handle).
+ *
+ * Reference interfaces replaced (paths relative to the RayGen project):
+ *   rg_settings            <- RendererSettings            src/raygen/rayrenderer.h:98-153
+ *   rg_create              <- RayRenderer::RayRenderer    src/raygen/rayrenderer.cpp:53-86
+ *   rg_set_scene           <- Renderer::setScene          src/raygen/renderer.h:48-50
+ *                             + RayRenderer::transformScene src/raygen/rayrenderer.cpp:157-363
+ *                             + TriangleBVH::build        src/raygen/bvh.cpp:76-98
+ *   rg_render              <- RayRenderer::render         src/raygen/rayrenderer.cpp:478-596
+ *   rg_set_progress_cb     <- RayRenderer::progressCallback src/raygen/rayrenderer.h:317
+ *   rg_cancel              <- RayRenderer::cancelRequested  src/raygen/rayrenderer.h:427
+ *   rg_get_hdr             <- RayRenderer::getHdrResult   src/raygen/rayrenderer.h:411
+ *   rg_get_ldr             <- RayRenderer::getRenderResult src/raygen/rayrenderer.h:404
+ *   rg_trace_closest       <- TriangleBVH::intersectClosest src/raygen/bvh.cpp:233-285
+ *   rg_trace_any           <- TriangleBVH::intersectAny   src/raygen/bvh.h:63-101
+ *   rg_denoise_atrous      <- RayRenderer::denoiseImage   src/raygen/rayrenderer.cpp:2649-2772
+ *   rg_tonemap             <- RayRenderer::applyTonemapGamma src/raygen/rayrenderer.cpp:2610-2647
+ *   rg_scene_builtin       <- (procedural stand-ins for the sample scenes; no reference symbol)
+ *   rg_load_scene_json     <- RendererSceneLoader::load   src/raygen/sceneloader.cpp:1113-1137
+ */
+#ifndef RAYGEN_B200_H
+#define RAYGEN_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef int rg_status;
+#define RG_OK 0
+#define RG_ERR_INVALID_ARGUMENT (-1)
+#define RG_ERR_NO_SCENE (-2)
+#define RG_ERR_UNSUPPORTED (-3)      /* shader id 4 (reserved in the reference) */
+#define RG_ERR_CUDA (-4)
+#define RG_ERR_OUT_OF_MEMORY (-5)
+#define RG_ERR_CANCELLED (-6)
+#define RG_ERR_DEVICE_STATUS (-7)    /* a kernel raised its error flag */
+#define RG_ERR_IO (-8)
+#define RG_ERR_PARSE (-9)
+#define RG_ERR_BUSY (-10)
+#define RG_ERR_NO_DEVICE (-11)
+
+/* Mix-shader evaluation: the reference sums every lobe (tree); the GPU picks
+ * one lobe per vertex with probability proportional to its weight (select). */
+#define RG_MIX_SELECT 0
+
+/* Adaptive sampling granularity. */
+#define RG_ADAPTIVE_PIXEL 0   /* per-pixel relative SEM (16 -> 256 spp)      */
+#define RG_ADAPTIVE_TILE 1    /* reference: per 32x32 tile mean relative SEM */
+
+/* Mirrors RendererSettings (rayrenderer.h:98-153) plus the tracer's own knobs. */
+typedef struct rg_settings {
+  int32_t resolution_width, resolution_height;
+  int32_t threads;            /* host threads (loader / CPU helpers)          */
+  int32_t samples;            /* samples per pixel (adaptive: maximum)        */
+  int32_t shader_provider;    /* 0,1,2,3,5 ; 4 -> RG_ERR_UNSUPPORTED          */
+  int32_t enable_antialias;
+  int32_t enable_point_light_antialias;
+  int32_t enable_color_sampling;
+  int32_t enable_rendering_postprocess; /* bloom                              */
+  int32_t enable_denoise;     /* A-Trous                                      */
+  int32_t cull_back_face;
+  int32_t denoise_levels;
+  float denoise_sigma_color, denoise_sigma_normal, denoise_sigma_depth;
+  float denoise_intensity;
+  float firefly_clamp;
+  int32_t enable_adaptive_sampling;
+  int32_t adaptive_base_samples;
+  float adaptive_threshold;
+  int32_t adaptive_mode;      /* RG_ADAPTIVE_PIXEL / RG_ADAPTIVE_TILE         */
+  float bloom_threshold, bloom_strength, bloom_radius, bloom_size_aspect, bloom_curve;
+  float world_color[3];
+  float back_color[4];
+  /* tracer knobs (no reference counterpart; reference values in brackets) */
+  uint32_t seed;              /* counter-based RNG seed [1]                   */
+  int32_t max_depth;          /* MAX_TRACE_DEPTH [32]                         */
+  int32_t rr_depth;           /* MIN_RR_DEPTH [3]                             */
+  int32_t light_pick_fix;     /* 1: weight NEE by the light count [0]         */
+  int32_t paths_per_wave;     /* wavefront size; 0 = automatic                */
+  int32_t bvh_bins;           /* SAH bins for the device build [32]           */
+} rg_settings;
+
+typedef struct rg_material {
+  float color[3];
+  float diffuse, glossy, roughness, transparency, refraction, refraction_ratio;
+  float chroma_dispersion, metallic, anisotropy, aniso_rotation, emission, spot_range;
+  int32_t texture;            /* index into rg_scene_desc.textures, -1 none   */
+  float tex_tiling[2];
+} rg_material;
+
+/* Homogeneous participating medium (medium.h:37-334, constant emission). */
+typedef struct rg_medium {
+  float sigma_a[3], sigma_s[3], sigma_e[3];
+  float g, density;
+} rg_medium;
+
+typedef struct rg_object {
+  int32_t material;
+  int32_t interior_medium;    /* -1 none */
+} rg_object;
+
+/* A mesh-less emissive object of the reference (a point or spot light). */
+typedef struct rg_point_light {
+  float position[3];          /* world space */
+  float normal[3];            /* world space */
+  int32_t material;
+} rg_point_light;
+
+typedef struct rg_camera {
+  float location[3];
+  float angle[3];             /* degrees; see DESIGN.md for the order       */
+  float field_of_view;        /* vertical, degrees                           */
+  float view_near, view_far;
+  float depth_of_field, aperture;
+  int32_t aperture_blades;
+  float aperture_rotation;    /* degrees */
+  float exposure;
+} rg_camera;
+
+typedef struct rg_texture {
+  int32_t width, height;
+  int32_t is_hdr;             /* 0: sRGB-decoded on sample                   */
+  const float* rgba;          /* width*height*4                              */
+} rg_texture;
+
+/* Flattened scene: world-space triangle soup grouped into meshes and objects.
+ * Triangle order is the reference's DFS order (objects -> meshes -> triangles)
+ * and is the triangle id used by rg_trace_closest. */
+typedef struct rg_scene_desc {
+  int32_t num_triangles;
+  const float* positions;     /* [num_triangles][3][3]                       */
+  const float* normals;       /* [num_triangles][3][3]                       */
+  const float* uvs;           /* [num_triangles][3][2] or NULL               */
+  const int32_t* tri_mesh;    /* [num_triangles]                             */
+  int32_t num_meshes;
+  const int32_t* mesh_object; /* [num_meshes]                                */
+  int32_t num_objects;
+  const rg_object* objects;
+  int32_t num_materials;
+  const rg_material* materials;
+  int32_t num_media;
+  const rg_medium* media;
+  int32_t global_medium;      /* -1 none */
+  int32_t num_point_lights;
+  const rg_point_light* point_lights;
+  int32_t num_textures;
+  const rg_texture* textures;
+  rg_camera camera;
+} rg_scene_desc;
+
+typedef struct rg_stats {
+  double trace_ms;            /* device time of the last render's trace     */
+  double post_ms;             /* device time of denoise / tonemap            */
+  double build_ms;            /* device time of the last BVH build           */
+  uint64_t samples;           /* primary samples traced                      */
+  uint64_t closest_rays, shadow_rays;
+  uint64_t nodes_visited, tris_tested;          /* closest-hit kernels        */
+  uint64_t shadow_nodes_visited, shadow_tris_tested;
+  double extend_ms, shade_ms, connect_ms;       /* per-kernel device time     */
+  int32_t bvh_nodes;
+  int32_t waves;
+  int32_t kernel_launches;
+  int32_t device_error;       /* first device error code, 0 = none           */
+} rg_stats;
+
+typedef struct rg_handle rg_handle;
+typedef void (*rg_progress_fn)(float progress, void* user);
+
+void rg_settings_default(rg_settings* s);
+rg_status rg_create(const rg_settings* s, rg_handle** out);
+rg_status rg_destroy(rg_handle* h);
+rg_status rg_update_settings(rg_handle* h, const rg_settings* s);
+rg_status rg_set_scene(rg_handle* h, const rg_scene_desc* scene);
+rg_status rg_render(rg_handle* h);
+rg_status rg_set_progress_cb(rg_handle* h, rg_progress_fn fn, void* user);
+rg_status rg_cancel(rg_handle* h);
+/* Linear HDR result (width*height*4 floats, alpha = 1). */
+rg_status rg_get_hdr(rg_handle* h, float* rgba, size_t count);
+/* Tonemapped result in [0,1] (width*height*4 floats). */
+rg_status rg_get_ldr(rg_handle* h, float* rgba, size_t count);
+/* Guide buffers of the last render (normal*0.5+0.5, albedo, depth), 3 floats
+ * per pixel each, as the denoiser saw them; NULL pointers are skipped. */
+rg_status rg_get_aovs(rg_handle* h, float* normal, float* albedo, float* depth, size_t count);
+/* Per-pixel sample counts of the last render (int32 per pixel). */
+rg_status rg_get_sample_counts(rg_handle* h, int32_t* counts, size_t count);
+rg_status rg_get_stats(rg_handle* h, rg_stats* out);
+const char* rg_last_error(void);
+const char* rg_version(void);
+
+/* Ray-batch queries against the scene's view-space BVH.
+ * rays: n x 6 floats (origin xyz, dir xyz) in view space.
+ * closest: out_tuv n x 3 (t, u, v), out_prim n (DFS triangle id, -1 = miss).
+ * any: tmax n floats; predicate 0 = area-light occluder, 1 = point/env
+ *      occluder, 2 = AO occluder, 3 = every triangle; out_hit n bytes. */
+rg_status rg_trace_closest(rg_handle* h, const float* rays, int32_t n, float* out_tuv, int32_t* out_prim);
+rg_status rg_trace_any(rg_handle* h, const float* rays, const float* tmax, int32_t n, int32_t predicate, uint8_t* out_hit);
+/* View-space camera transform the scene was flattened with (4x4 row-major,
+ * row-vector convention: p_view = [p 1] * M). */
+rg_status rg_get_view_matrix(rg_handle* h, float* m16);
+
+/* Stand-alone post passes on caller buffers (device work, host pointers).
+ * color/out: w*h*3 floats; normal/albedo: w*h*3 (encoded as the AOVs);
+ * albedo_alpha: w*h floats (1 = geometry hit); depth: w*h floats. */
+rg_status rg_denoise_atrous(int32_t w, int32_t h, const float* color, const float* normal,
+                            const float* depth, const float* albedo, const float* albedo_alpha,
+                            int32_t levels, float sigma_color, float sigma_normal,
+                            float sigma_depth, float intensity, float* out);
+rg_status rg_tonemap(int32_t w, int32_t h, const float* hdr_rgba, float* ldr_rgba);
+
+/* Procedural scenes (host C++, no device work).
+ * kind 1: cube room (10 walls, two boxes, one 2.5x2.5 ceiling light).
+ * kind 2: displaced icosphere x4 in a 20x20 room with 16 ceiling lights;
+ *         iparams[0] = triangles per sphere (default 1,003,520).
+ * kind 3: kind 2 + a global homogeneous medium (sigma_t 0.05, albedo 0.8, g 0.3).
+ * kind 4: one job of the heterogeneous batch: iparams[0] = triangles,
+ *         iparams[1] = emitters.
+ * The returned description is owned by the library: free with rg_scene_free. */
+rg_status rg_scene_builtin(int32_t kind, uint32_t seed, const int32_t* iparams, int32_t n_iparams,
+                           rg_scene_desc** out);
+rg_status rg_scene_free(rg_scene_desc* scene);
+/* Reference scene JSON (sceneloader.cpp schema) -> flattened description. */
+rg_status rg_load_scene_json(const char* path, rg_scene_desc** out);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* RAYGEN_B200_H */

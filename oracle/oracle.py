@@ -1,0 +1,185 @@
+"""TEST INFRASTRUCTURE ONLY: ctypes front end of the CPU oracle (rg_oracle.cpp).
+
+Loaded by tests/, __graft_entry__.smoke() and bench.py's CPU-baseline /
+reference arm; never by the product path.  The oracle restates RayGen's
+shader-5 renderer on the CPU (see the header of rg_oracle.cpp for the
+reference files it follows and the documented deviations).
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+
+
+class orc_settings(C.Structure):
+    _fields_ = [
+        ("width", C.c_int32), ("height", C.c_int32), ("spp", C.c_int32), ("shader", C.c_int32),
+        ("antialias", C.c_int32), ("color_sampling", C.c_int32), ("denoise", C.c_int32),
+        ("denoise_levels", C.c_int32),
+        ("sigma_color", C.c_float), ("sigma_normal", C.c_float), ("sigma_depth", C.c_float),
+        ("denoise_intensity", C.c_float), ("firefly_clamp", C.c_float),
+        ("adaptive", C.c_int32), ("adaptive_base", C.c_int32), ("adaptive_mode", C.c_int32),
+        ("adaptive_threshold", C.c_float),
+        ("world_color", C.c_float * 3), ("back_color", C.c_float * 4),
+        ("seed", C.c_uint32), ("max_depth", C.c_int32), ("rr_depth", C.c_int32),
+        ("light_pick_fix", C.c_int32), ("threads", C.c_int32), ("mix_tree", C.c_int32),
+    ]
+
+
+_libs = {}
+
+
+def build() -> None:
+    subprocess.run(["make", "-s", "-C", HERE], check=True)
+
+
+def load(fast: bool = False) -> C.CDLL:
+    name = "liboracle_fast.so" if fast else "liboracle.so"
+    if name in _libs:
+        return _libs[name]
+    path = os.path.join(HERE, name)
+    if not os.path.exists(path):
+        build()
+    lib = C.CDLL(path)
+    P = C.POINTER
+    f = P(C.c_float)
+    lib.orc_scene_create.restype = C.c_void_p
+    lib.orc_scene_create.argtypes = [C.c_void_p, C.c_int32]
+    lib.orc_scene_destroy.argtypes = [C.c_void_p]
+    lib.orc_bvh_nodes.restype = C.c_int32
+    lib.orc_bvh_nodes.argtypes = [C.c_void_p]
+    for nm in ("orc_closest", "orc_closest_brute"):
+        getattr(lib, nm).argtypes = [C.c_void_p, f, C.c_int32, f, P(C.c_int32)]
+    lib.orc_any.argtypes = [C.c_void_p, f, f, C.c_int32, C.c_int32, P(C.c_uint8)]
+    lib.orc_render.restype = C.c_int32
+    lib.orc_render.argtypes = [C.c_void_p, P(orc_settings), P(C.c_double), P(C.c_double), P(C.c_int32), f, f, f, f, f]
+    lib.orc_denoise.argtypes = [C.c_int32, C.c_int32, f, f, f, f, f, C.c_int32, C.c_float, C.c_float, C.c_float,
+                                C.c_float, f]
+    lib.orc_tonemap.argtypes = [C.c_int32, C.c_int32, f, f]
+    lib.orc_lds.restype = C.c_float
+    lib.orc_lds.argtypes = [C.c_uint32] * 5 + [C.c_int32]
+    lib.orc_prng.restype = C.c_float
+    lib.orc_prng.argtypes = [C.c_uint32] * 5 + [C.c_int32, C.c_int32]
+    lib.orc_phase_pdf.restype = C.c_float
+    lib.orc_phase_pdf.argtypes = [C.c_float, C.c_float]
+    lib.orc_sample_phase.argtypes = [C.c_float, C.c_float, C.c_float, f]
+    _libs[name] = lib
+    return lib
+
+
+def _fp(a):
+    return a.ctypes.data_as(C.POINTER(C.c_float))
+
+
+class OracleScene:
+    """CPU restatement of the flattened scene + reference BVH (16 bins by default)."""
+
+    def __init__(self, desc_ptr, bins: int = 16, fast: bool = False):
+        self.lib = load(fast)
+        self.h = self.lib.orc_scene_create(C.cast(desc_ptr, C.c_void_p), bins)
+
+    def close(self):
+        if self.h:
+            self.lib.orc_scene_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def bvh_nodes(self) -> int:
+        return self.lib.orc_bvh_nodes(self.h)
+
+    def closest(self, rays, brute: bool = False):
+        rays = np.ascontiguousarray(rays, np.float32).reshape(-1, 6)
+        n = rays.shape[0]
+        tuv = np.empty((n, 3), np.float32)
+        prim = np.empty(n, np.int32)
+        fn = self.lib.orc_closest_brute if brute else self.lib.orc_closest
+        fn(self.h, _fp(rays), n, _fp(tuv), prim.ctypes.data_as(C.POINTER(C.c_int32)))
+        return tuv, prim
+
+    def any(self, rays, tmax, predicate: int = 0):
+        rays = np.ascontiguousarray(rays, np.float32).reshape(-1, 6)
+        tmax = np.ascontiguousarray(tmax, np.float32).reshape(-1)
+        n = rays.shape[0]
+        out = np.empty(n, np.uint8)
+        self.lib.orc_any(self.h, _fp(rays), _fp(tmax), n, predicate, out.ctypes.data_as(C.POINTER(C.c_uint8)))
+        return out.astype(bool)
+
+    def render(self, width, height, spp, shader=5, seed=1, max_depth=32, rr_depth=3, threads=None,
+               mix_tree=False, antialias=True, color_sampling=True, denoise=False, denoise_levels=5,
+               sigma_color=0.4, sigma_normal=128.0, sigma_depth=0.1, denoise_intensity=1.0,
+               firefly_clamp=10.0, adaptive=False, adaptive_base=4, adaptive_mode=1,
+               adaptive_threshold=0.02, light_pick_fix=False, world_color=(0.1, 0.095, 0.09),
+               back_color=(0.2, 0.19, 0.18, 0.0)):
+        """Returns dict with sum/sumsq (H,W,3 float64), n (H,W), hdr/ldr (H,W,4) and guides."""
+        s = orc_settings()
+        s.width, s.height, s.spp, s.shader = width, height, spp, shader
+        s.antialias, s.color_sampling, s.denoise, s.denoise_levels = int(antialias), int(color_sampling), int(denoise), denoise_levels
+        s.sigma_color, s.sigma_normal, s.sigma_depth = sigma_color, sigma_normal, sigma_depth
+        s.denoise_intensity, s.firefly_clamp = denoise_intensity, firefly_clamp
+        s.adaptive, s.adaptive_base, s.adaptive_mode, s.adaptive_threshold = int(adaptive), adaptive_base, adaptive_mode, adaptive_threshold
+        for i in range(3):
+            s.world_color[i] = world_color[i]
+        for i in range(4):
+            s.back_color[i] = back_color[i]
+        s.seed, s.max_depth, s.rr_depth = seed, max_depth, rr_depth
+        s.light_pick_fix = int(light_pick_fix)
+        s.threads = threads if threads else (os.cpu_count() or 1)
+        s.mix_tree = int(mix_tree)
+        n = width * height
+        out = {
+            "sum": np.zeros((height, width, 3), np.float64),
+            "sumsq": np.zeros((height, width, 3), np.float64),
+            "n": np.zeros((height, width), np.int32),
+            "hdr": np.zeros((height, width, 4), np.float32),
+            "ldr": np.zeros((height, width, 4), np.float32),
+            "normal": np.zeros((height, width, 3), np.float32),
+            "albedo": np.zeros((height, width, 3), np.float32),
+            "depth": np.zeros((height, width), np.float32),
+        }
+        dp = C.POINTER(C.c_double)
+        rc = self.lib.orc_render(self.h, C.byref(s), out["sum"].ctypes.data_as(dp), out["sumsq"].ctypes.data_as(dp),
+                                 out["n"].ctypes.data_as(C.POINTER(C.c_int32)), _fp(out["hdr"]), _fp(out["ldr"]),
+                                 _fp(out["normal"]), _fp(out["albedo"]), _fp(out["depth"]))
+        if rc != 0:
+            raise RuntimeError(f"oracle render failed: {rc}")
+        del n
+        return out
+
+
+def denoise(color, normal, depth, albedo, albedo_alpha, levels=5, sigma_color=0.4, sigma_normal=128.0,
+            sigma_depth=0.1, intensity=1.0):
+    lib = load()
+    color = np.ascontiguousarray(color, np.float32)
+    h, w = color.shape[:2]
+    a = [np.ascontiguousarray(x, np.float32) for x in (normal, depth, albedo, albedo_alpha)]
+    out = np.empty((h, w, 3), np.float32)
+    lib.orc_denoise(w, h, _fp(color), _fp(a[0]), _fp(a[1]), _fp(a[2]), _fp(a[3]), levels, sigma_color,
+                    sigma_normal, sigma_depth, intensity, _fp(out))
+    return out
+
+
+def tonemap(hdr):
+    lib = load()
+    hdr = np.ascontiguousarray(hdr, np.float32)
+    h, w = hdr.shape[:2]
+    out = np.empty_like(hdr)
+    lib.orc_tonemap(w, h, _fp(hdr), _fp(out))
+    return out
+
+
+def lds(x, y, width, sample, seed, dim):
+    return load().orc_lds(x, y, width, sample, seed, dim)
+
+
+def prng(x, y, width, sample, seed, vertex, slot):
+    return load().orc_prng(x, y, width, sample, seed, vertex, slot)

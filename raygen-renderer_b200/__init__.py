@@ -1,0 +1,496 @@
+"""raygen-renderer_b200: B200 wavefront path tracer behind RayGen's renderer interface.
+
+Python host mirror of the reference's C++ surface (src/raygen/rayrenderer.h):
+
+* ``RendererSettings``   <- RendererSettings (rayrenderer.h:98-153), same field names
+* ``RayRenderer``        <- RayRenderer: ``set_scene`` / ``render`` /
+  ``get_render_result`` / ``get_hdr_result`` / ``progress_callback`` / ``cancel``
+* ``Scene``              <- a flattened scene description (procedural workloads,
+  the reference JSON schema, or caller arrays)
+
+Every call goes through the C ABI of ``librg_b200.so`` (include/raygen_b200.h);
+there is no CPU fallback: without the library or a CUDA device the calls fail
+with ``RayGenError``.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from dataclasses import dataclass, field, fields
+from typing import Callable, Optional
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "librg_b200.so")
+
+RG_OK = 0
+RG_ERR_INVALID_ARGUMENT = -1
+RG_ERR_NO_SCENE = -2
+RG_ERR_UNSUPPORTED = -3
+RG_ERR_CUDA = -4
+RG_ERR_OUT_OF_MEMORY = -5
+RG_ERR_CANCELLED = -6
+RG_ERR_DEVICE_STATUS = -7
+RG_ERR_IO = -8
+RG_ERR_PARSE = -9
+RG_ERR_BUSY = -10
+RG_ERR_NO_DEVICE = -11
+
+RG_ADAPTIVE_PIXEL = 0
+RG_ADAPTIVE_TILE = 1
+
+# occluder predicates of rg_trace_any
+PRED_AREA, PRED_POINT, PRED_AO, PRED_ALL = 0, 1, 2, 3
+
+
+class RayGenError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"rg status {code}: {msg}")
+        self.code = code
+
+
+# ------------------------------------------------------------------ ABI types
+class rg_settings(C.Structure):
+    _fields_ = [
+        ("resolution_width", C.c_int32), ("resolution_height", C.c_int32),
+        ("threads", C.c_int32), ("samples", C.c_int32), ("shader_provider", C.c_int32),
+        ("enable_antialias", C.c_int32), ("enable_point_light_antialias", C.c_int32),
+        ("enable_color_sampling", C.c_int32), ("enable_rendering_postprocess", C.c_int32),
+        ("enable_denoise", C.c_int32), ("cull_back_face", C.c_int32),
+        ("denoise_levels", C.c_int32),
+        ("denoise_sigma_color", C.c_float), ("denoise_sigma_normal", C.c_float),
+        ("denoise_sigma_depth", C.c_float), ("denoise_intensity", C.c_float),
+        ("firefly_clamp", C.c_float),
+        ("enable_adaptive_sampling", C.c_int32), ("adaptive_base_samples", C.c_int32),
+        ("adaptive_threshold", C.c_float), ("adaptive_mode", C.c_int32),
+        ("bloom_threshold", C.c_float), ("bloom_strength", C.c_float), ("bloom_radius", C.c_float),
+        ("bloom_size_aspect", C.c_float), ("bloom_curve", C.c_float),
+        ("world_color", C.c_float * 3), ("back_color", C.c_float * 4),
+        ("seed", C.c_uint32), ("max_depth", C.c_int32), ("rr_depth", C.c_int32),
+        ("light_pick_fix", C.c_int32), ("paths_per_wave", C.c_int32), ("bvh_bins", C.c_int32),
+    ]
+
+
+class rg_material(C.Structure):
+    _fields_ = [
+        ("color", C.c_float * 3),
+        ("diffuse", C.c_float), ("glossy", C.c_float), ("roughness", C.c_float),
+        ("transparency", C.c_float), ("refraction", C.c_float), ("refraction_ratio", C.c_float),
+        ("chroma_dispersion", C.c_float), ("metallic", C.c_float), ("anisotropy", C.c_float),
+        ("aniso_rotation", C.c_float), ("emission", C.c_float), ("spot_range", C.c_float),
+        ("texture", C.c_int32), ("tex_tiling", C.c_float * 2),
+    ]
+
+
+class rg_medium(C.Structure):
+    _fields_ = [("sigma_a", C.c_float * 3), ("sigma_s", C.c_float * 3), ("sigma_e", C.c_float * 3),
+                ("g", C.c_float), ("density", C.c_float)]
+
+
+class rg_object(C.Structure):
+    _fields_ = [("material", C.c_int32), ("interior_medium", C.c_int32)]
+
+
+class rg_point_light(C.Structure):
+    _fields_ = [("position", C.c_float * 3), ("normal", C.c_float * 3), ("material", C.c_int32)]
+
+
+class rg_camera(C.Structure):
+    _fields_ = [
+        ("location", C.c_float * 3), ("angle", C.c_float * 3), ("field_of_view", C.c_float),
+        ("view_near", C.c_float), ("view_far", C.c_float), ("depth_of_field", C.c_float),
+        ("aperture", C.c_float), ("aperture_blades", C.c_int32), ("aperture_rotation", C.c_float),
+        ("exposure", C.c_float),
+    ]
+
+
+class rg_texture(C.Structure):
+    _fields_ = [("width", C.c_int32), ("height", C.c_int32), ("is_hdr", C.c_int32),
+                ("rgba", C.POINTER(C.c_float))]
+
+
+class rg_scene_desc(C.Structure):
+    _fields_ = [
+        ("num_triangles", C.c_int32), ("positions", C.POINTER(C.c_float)),
+        ("normals", C.POINTER(C.c_float)), ("uvs", C.POINTER(C.c_float)),
+        ("tri_mesh", C.POINTER(C.c_int32)), ("num_meshes", C.c_int32),
+        ("mesh_object", C.POINTER(C.c_int32)), ("num_objects", C.c_int32),
+        ("objects", C.POINTER(rg_object)), ("num_materials", C.c_int32),
+        ("materials", C.POINTER(rg_material)), ("num_media", C.c_int32),
+        ("media", C.POINTER(rg_medium)), ("global_medium", C.c_int32),
+        ("num_point_lights", C.c_int32), ("point_lights", C.POINTER(rg_point_light)),
+        ("num_textures", C.c_int32), ("textures", C.POINTER(rg_texture)),
+        ("camera", rg_camera),
+    ]
+
+
+class rg_stats(C.Structure):
+    _fields_ = [
+        ("trace_ms", C.c_double), ("post_ms", C.c_double), ("build_ms", C.c_double),
+        ("samples", C.c_uint64), ("closest_rays", C.c_uint64), ("shadow_rays", C.c_uint64),
+        ("nodes_visited", C.c_uint64), ("tris_tested", C.c_uint64),
+        ("shadow_nodes_visited", C.c_uint64), ("shadow_tris_tested", C.c_uint64),
+        ("extend_ms", C.c_double), ("shade_ms", C.c_double), ("connect_ms", C.c_double),
+        ("bvh_nodes", C.c_int32), ("waves", C.c_int32), ("kernel_launches", C.c_int32),
+        ("device_error", C.c_int32),
+    ]
+
+
+PROGRESS_FN = C.CFUNCTYPE(None, C.c_float, C.c_void_p)
+
+_lib = None
+
+
+def load_library(path: str = LIB_PATH) -> C.CDLL:
+    """Load librg_b200.so (raises if it has not been built)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(path):
+        raise RayGenError(RG_ERR_IO, f"{path} is missing: run __graft_entry__.build()")
+    lib = C.CDLL(path)
+    P = C.POINTER
+    sig = {
+        "rg_settings_default": (None, [P(rg_settings)]),
+        "rg_create": (C.c_int, [P(rg_settings), P(C.c_void_p)]),
+        "rg_destroy": (C.c_int, [C.c_void_p]),
+        "rg_update_settings": (C.c_int, [C.c_void_p, P(rg_settings)]),
+        "rg_set_scene": (C.c_int, [C.c_void_p, P(rg_scene_desc)]),
+        "rg_render": (C.c_int, [C.c_void_p]),
+        "rg_set_progress_cb": (C.c_int, [C.c_void_p, PROGRESS_FN, C.c_void_p]),
+        "rg_cancel": (C.c_int, [C.c_void_p]),
+        "rg_get_hdr": (C.c_int, [C.c_void_p, P(C.c_float), C.c_size_t]),
+        "rg_get_ldr": (C.c_int, [C.c_void_p, P(C.c_float), C.c_size_t]),
+        "rg_get_aovs": (C.c_int, [C.c_void_p, P(C.c_float), P(C.c_float), P(C.c_float), C.c_size_t]),
+        "rg_get_sample_counts": (C.c_int, [C.c_void_p, P(C.c_int32), C.c_size_t]),
+        "rg_get_stats": (C.c_int, [C.c_void_p, P(rg_stats)]),
+        "rg_last_error": (C.c_char_p, []),
+        "rg_version": (C.c_char_p, []),
+        "rg_trace_closest": (C.c_int, [C.c_void_p, P(C.c_float), C.c_int32, P(C.c_float), P(C.c_int32)]),
+        "rg_trace_any": (C.c_int, [C.c_void_p, P(C.c_float), P(C.c_float), C.c_int32, C.c_int32, P(C.c_uint8)]),
+        "rg_get_view_matrix": (C.c_int, [C.c_void_p, P(C.c_float)]),
+        "rg_denoise_atrous": (C.c_int, [C.c_int32, C.c_int32, P(C.c_float), P(C.c_float), P(C.c_float),
+                                        P(C.c_float), P(C.c_float), C.c_int32, C.c_float, C.c_float,
+                                        C.c_float, C.c_float, P(C.c_float)]),
+        "rg_tonemap": (C.c_int, [C.c_int32, C.c_int32, P(C.c_float), P(C.c_float)]),
+        "rg_scene_builtin": (C.c_int, [C.c_int32, C.c_uint32, P(C.c_int32), C.c_int32, P(P(rg_scene_desc))]),
+        "rg_scene_free": (C.c_int, [P(rg_scene_desc)]),
+        "rg_load_scene_json": (C.c_int, [C.c_char_p, P(P(rg_scene_desc))]),
+    }
+    for name, (res, args) in sig.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    _lib = lib
+    return lib
+
+
+def _check(code: int) -> None:
+    if code != RG_OK:
+        msg = load_library().rg_last_error()
+        raise RayGenError(code, msg.decode() if msg else "")
+
+
+def _fptr(a: np.ndarray):
+    return a.ctypes.data_as(C.POINTER(C.c_float))
+
+
+def version() -> str:
+    return load_library().rg_version().decode()
+
+
+# --------------------------------------------------------------- settings
+@dataclass
+class RendererSettings:
+    """Field-for-field mirror of the reference RendererSettings (rayrenderer.h:98-153)."""
+    resolutionWidth: int = 800
+    resolutionHeight: int = 600
+    threads: int = 1
+    samples: int = 100
+    shaderProvider: int = 5
+    enableAntialias: bool = True
+    enablePointLightAntialias: bool = True
+    enableColorSampling: bool = True
+    enableRenderingPostProcess: bool = False
+    enableDenoise: bool = False
+    cullBackFace: bool = False
+    denoiseLevels: int = 5
+    denoiseSigmaColor: float = 0.4
+    denoiseSigmaNormal: float = 128.0
+    denoiseSigmaDepth: float = 0.1
+    denoiseIntensity: float = 1.0
+    fireflyClamp: float = 10.0
+    enableAdaptiveSampling: bool = False
+    adaptiveBaseSamples: int = 4
+    adaptiveThreshold: float = 0.02
+    adaptiveMode: int = RG_ADAPTIVE_TILE
+    bloomThreshold: float = 1.0
+    bloomStrength: float = 1.0
+    bloomRadius: float = 0.03
+    bloomSizeAspect: float = 0.15
+    bloomCurve: float = 1.0
+    worldColor: tuple = (0.1, 0.095, 0.09)
+    backColor: tuple = (0.2, 0.19, 0.18, 0.0)
+    # tracer knobs
+    seed: int = 1
+    maxDepth: int = 32
+    rrDepth: int = 3
+    lightPickFix: bool = False
+    pathsPerWave: int = 0
+    bvhBins: int = 32
+
+    _MAP = {
+        "resolutionWidth": "resolution_width", "resolutionHeight": "resolution_height",
+        "threads": "threads", "samples": "samples", "shaderProvider": "shader_provider",
+        "enableAntialias": "enable_antialias", "enablePointLightAntialias": "enable_point_light_antialias",
+        "enableColorSampling": "enable_color_sampling",
+        "enableRenderingPostProcess": "enable_rendering_postprocess", "enableDenoise": "enable_denoise",
+        "cullBackFace": "cull_back_face", "denoiseLevels": "denoise_levels",
+        "denoiseSigmaColor": "denoise_sigma_color", "denoiseSigmaNormal": "denoise_sigma_normal",
+        "denoiseSigmaDepth": "denoise_sigma_depth", "denoiseIntensity": "denoise_intensity",
+        "fireflyClamp": "firefly_clamp", "enableAdaptiveSampling": "enable_adaptive_sampling",
+        "adaptiveBaseSamples": "adaptive_base_samples", "adaptiveThreshold": "adaptive_threshold",
+        "adaptiveMode": "adaptive_mode", "bloomThreshold": "bloom_threshold",
+        "bloomStrength": "bloom_strength", "bloomRadius": "bloom_radius",
+        "bloomSizeAspect": "bloom_size_aspect", "bloomCurve": "bloom_curve",
+        "seed": "seed", "maxDepth": "max_depth", "rrDepth": "rr_depth",
+        "lightPickFix": "light_pick_fix", "pathsPerWave": "paths_per_wave", "bvhBins": "bvh_bins",
+    }
+
+    def to_c(self) -> rg_settings:
+        s = rg_settings()
+        for k, v in self._MAP.items():
+            val = getattr(self, k)
+            setattr(s, v, int(val) if isinstance(val, bool) else val)
+        for i in range(3):
+            s.world_color[i] = self.worldColor[i]
+        for i in range(4):
+            s.back_color[i] = self.backColor[i]
+        return s
+
+
+def default_settings_c() -> rg_settings:
+    s = rg_settings()
+    load_library().rg_settings_default(C.byref(s))
+    return s
+
+
+# ------------------------------------------------------------------ scenes
+class Scene:
+    """A flattened scene description (rg_scene_desc) owned by the library or by Python arrays."""
+
+    def __init__(self, desc_ptr, owned_by_lib: bool, keepalive=None):
+        self._ptr = desc_ptr
+        self._owned = owned_by_lib
+        self._keep = keepalive
+
+    @property
+    def desc(self) -> rg_scene_desc:
+        return self._ptr.contents
+
+    @property
+    def ptr(self):
+        return self._ptr
+
+    @classmethod
+    def builtin(cls, kind: int, seed: int = 1, iparams=None) -> "Scene":
+        lib = load_library()
+        out = C.POINTER(rg_scene_desc)()
+        ip = (C.c_int32 * len(iparams))(*iparams) if iparams else None
+        _check(lib.rg_scene_builtin(kind, seed, ip, len(iparams) if iparams else 0, C.byref(out)))
+        return cls(out, True)
+
+    @classmethod
+    def from_json(cls, path: str) -> "Scene":
+        lib = load_library()
+        out = C.POINTER(rg_scene_desc)()
+        _check(lib.rg_load_scene_json(path.encode(), C.byref(out)))
+        return cls(out, True)
+
+    @classmethod
+    def from_arrays(cls, positions, normals, tri_mesh, mesh_object, objects, materials, camera,
+                    media=(), global_medium=-1, point_lights=(), uvs=None) -> "Scene":
+        pos = np.ascontiguousarray(positions, dtype=np.float32).reshape(-1, 9)
+        nrm = np.ascontiguousarray(normals, dtype=np.float32).reshape(-1, 9)
+        tm = np.ascontiguousarray(tri_mesh, dtype=np.int32)
+        mo = np.ascontiguousarray(mesh_object, dtype=np.int32)
+        objs = (rg_object * max(1, len(objects)))(*objects)
+        mats = (rg_material * max(1, len(materials)))(*materials)
+        meds = (rg_medium * max(1, len(media)))(*media)
+        pls = (rg_point_light * max(1, len(point_lights)))(*point_lights)
+        d = rg_scene_desc()
+        d.num_triangles = pos.shape[0]
+        d.positions = _fptr(pos)
+        d.normals = _fptr(nrm)
+        uv = None
+        if uvs is not None:
+            uv = np.ascontiguousarray(uvs, dtype=np.float32).reshape(-1, 6)
+            d.uvs = _fptr(uv)
+        d.tri_mesh = tm.ctypes.data_as(C.POINTER(C.c_int32))
+        d.num_meshes = len(mo)
+        d.mesh_object = mo.ctypes.data_as(C.POINTER(C.c_int32))
+        d.num_objects = len(objects)
+        d.objects = objs
+        d.num_materials = len(materials)
+        d.materials = mats
+        d.num_media = len(media)
+        d.media = meds
+        d.global_medium = global_medium
+        d.num_point_lights = len(point_lights)
+        d.point_lights = pls
+        d.camera = camera
+        keep = (pos, nrm, tm, mo, objs, mats, meds, pls, uv, d)
+        return cls(C.pointer(d), False, keep)
+
+    def arrays(self):
+        """numpy views of the triangle arrays (positions n x 9, normals n x 9, tri_mesh n)."""
+        d = self.desc
+        n = d.num_triangles
+        pos = np.ctypeslib.as_array(d.positions, shape=(n, 9)) if n else np.zeros((0, 9), np.float32)
+        nrm = np.ctypeslib.as_array(d.normals, shape=(n, 9)) if n else np.zeros((0, 9), np.float32)
+        tm = np.ctypeslib.as_array(d.tri_mesh, shape=(n,)) if n else np.zeros((0,), np.int32)
+        return pos, nrm, tm
+
+    def close(self):
+        if self._owned and self._ptr:
+            load_library().rg_scene_free(self._ptr)
+        self._ptr = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+# ---------------------------------------------------------------- renderer
+class RayRenderer:
+    """Mirror of the reference RayRenderer (rayrenderer.h:199-434) over the device tracer."""
+
+    def __init__(self, settings: Optional[RendererSettings] = None):
+        self.settings = settings or RendererSettings()
+        self._lib = load_library()
+        self._h = C.c_void_p()
+        s = self.settings.to_c()
+        _check(self._lib.rg_create(C.byref(s), C.byref(self._h)))
+        self.progressCallback: Optional[Callable[[float], None]] = None
+        self._cb = None
+        self._scene: Optional[Scene] = None
+
+    def _sync_settings(self):
+        s = self.settings.to_c()
+        _check(self._lib.rg_update_settings(self._h, C.byref(s)))
+
+    def set_scene(self, scene: Scene) -> None:
+        self._sync_settings()
+        _check(self._lib.rg_set_scene(self._h, scene.ptr))
+        self._scene = scene
+
+    setScene = set_scene
+
+    def render(self) -> None:
+        self._sync_settings()
+        if self.progressCallback is not None:
+            user = self.progressCallback
+            self._cb = PROGRESS_FN(lambda p, _u: user(float(p)))
+            _check(self._lib.rg_set_progress_cb(self._h, self._cb, None))
+        _check(self._lib.rg_render(self._h))
+
+    def cancel(self) -> None:
+        _check(self._lib.rg_cancel(self._h))
+
+    def _size(self):
+        return self.settings.resolutionHeight, self.settings.resolutionWidth
+
+    def get_hdr_result(self) -> np.ndarray:
+        h, w = self._size()
+        out = np.empty((h, w, 4), np.float32)
+        _check(self._lib.rg_get_hdr(self._h, _fptr(out), out.size))
+        return out
+
+    def get_render_result(self) -> np.ndarray:
+        h, w = self._size()
+        out = np.empty((h, w, 4), np.float32)
+        _check(self._lib.rg_get_ldr(self._h, _fptr(out), out.size))
+        return out
+
+    getHdrResult = get_hdr_result
+    getRenderResult = get_render_result
+
+    def get_aovs(self):
+        h, w = self._size()
+        n = np.empty((h, w, 3), np.float32)
+        a = np.empty((h, w, 3), np.float32)
+        d = np.empty((h, w), np.float32)
+        _check(self._lib.rg_get_aovs(self._h, _fptr(n), _fptr(a), _fptr(d), n.size))
+        return n, a, d
+
+    def get_sample_counts(self) -> np.ndarray:
+        h, w = self._size()
+        out = np.empty((h, w), np.int32)
+        _check(self._lib.rg_get_sample_counts(self._h, out.ctypes.data_as(C.POINTER(C.c_int32)), out.size))
+        return out
+
+    def stats(self) -> dict:
+        s = rg_stats()
+        _check(self._lib.rg_get_stats(self._h, C.byref(s)))
+        return {f[0]: getattr(s, f[0]) for f in rg_stats._fields_}
+
+    def view_matrix(self) -> np.ndarray:
+        m = np.empty(16, np.float32)
+        _check(self._lib.rg_get_view_matrix(self._h, _fptr(m)))
+        return m.reshape(4, 4)
+
+    def trace_closest(self, rays: np.ndarray):
+        rays = np.ascontiguousarray(rays, dtype=np.float32).reshape(-1, 6)
+        n = rays.shape[0]
+        tuv = np.empty((n, 3), np.float32)
+        prim = np.empty(n, np.int32)
+        _check(self._lib.rg_trace_closest(self._h, _fptr(rays), n, _fptr(tuv),
+                                          prim.ctypes.data_as(C.POINTER(C.c_int32))))
+        return tuv, prim
+
+    def trace_any(self, rays: np.ndarray, tmax: np.ndarray, predicate: int = PRED_AREA):
+        rays = np.ascontiguousarray(rays, dtype=np.float32).reshape(-1, 6)
+        tmax = np.ascontiguousarray(tmax, dtype=np.float32).reshape(-1)
+        n = rays.shape[0]
+        out = np.empty(n, np.uint8)
+        _check(self._lib.rg_trace_any(self._h, _fptr(rays), _fptr(tmax), n, predicate,
+                                      out.ctypes.data_as(C.POINTER(C.c_uint8))))
+        return out.astype(bool)
+
+    def close(self):
+        if self._h:
+            self._lib.rg_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def denoise_atrous(color, normal, depth, albedo, albedo_alpha, levels=5, sigma_color=0.4,
+                   sigma_normal=128.0, sigma_depth=0.1, intensity=1.0) -> np.ndarray:
+    """Device A-Trous on host arrays (RayRenderer::denoiseImage, rayrenderer.cpp:2649-2772)."""
+    lib = load_library()
+    color = np.ascontiguousarray(color, np.float32)
+    h, w = color.shape[:2]
+    args = [np.ascontiguousarray(a, np.float32) for a in (normal, depth, albedo, albedo_alpha)]
+    out = np.empty((h, w, 3), np.float32)
+    _check(lib.rg_denoise_atrous(w, h, _fptr(color), _fptr(args[0]), _fptr(args[1]), _fptr(args[2]),
+                                 _fptr(args[3]), levels, sigma_color, sigma_normal, sigma_depth,
+                                 intensity, _fptr(out)))
+    return out
+
+
+def tonemap(hdr_rgba: np.ndarray) -> np.ndarray:
+    """Device Reinhard + gamma (RayRenderer::applyTonemapGamma, rayrenderer.cpp:2610-2647)."""
+    lib = load_library()
+    hdr = np.ascontiguousarray(hdr_rgba, np.float32)
+    h, w = hdr.shape[:2]
+    out = np.empty_like(hdr)
+    _check(lib.rg_tonemap(w, h, _fptr(hdr), _fptr(out)))
+    return out

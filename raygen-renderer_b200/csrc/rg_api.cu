@@ -1,0 +1,1014 @@
+// rg_api.cu - host runtime behind the C ABI (include/raygen_b200.h).
+//
+// Mirrors the RayRenderer lifecycle (rayrenderer.cpp:53-596): settings are
+// copied at creation, the scene is flattened to view space and its BVH built
+// on the device when it is set, and render() runs the wavefront tracer
+// (optionally in adaptive passes), the A-Trous denoiser and the tonemap, all
+// on the device.  Waves of paths are replayed through one captured CUDA
+// graph; the wave descriptors live on the device and a one-thread kernel at
+// the end of the graph advances to the next one.
+#include <cuda_fp16.h>
+
+#include <algorithm>
+#include <chrono>
+#include <cstdlib>
+#include <unordered_map>
+#include <cmath>
+#include <cstring>
+#include <memory>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "rg_device.cuh"
+#include "rg_host.h"
+#include "rg_trace.cuh"
+
+namespace rg {
+
+static thread_local std::string g_lastError;
+void setLastError(const std::string& msg) { g_lastError = msg; }
+
+#define RG_CUDA_CHECK(call)                                                     \
+  do {                                                                          \
+    cudaError_t e__ = (call);                                                   \
+    if (e__ != cudaSuccess) {                                                   \
+      setLastError(std::string(#call) + ": " + cudaGetErrorString(e__));        \
+      return RG_ERR_CUDA;                                                       \
+    }                                                                           \
+  } while (0)
+
+namespace {
+
+__global__ void k_nextWave(int* cur) { *cur += 1; }
+
+struct Mat4 {
+  float m[16];
+};
+
+// Camera view matrix, row-vector convention p_view = [p 1] * M.
+// Camera orientation R = Ry(angle.y) * Rx(angle.x) * Rz(angle.z) (degrees);
+// p_view = R^T (p - location).  With zero angles this is exactly p - location.
+Mat4 viewMatrix(const rg_camera& c) {
+  const float d2r = 3.14159265358979323846f / 180.0f;
+  const float ax = c.angle[0] * d2r, ay = c.angle[1] * d2r, az = c.angle[2] * d2r;
+  const double cx = std::cos(ax), sx = std::sin(ax), cy = std::cos(ay), sy = std::sin(ay), cz = std::cos(az), sz = std::sin(az);
+  double Rx[3][3] = {{1, 0, 0}, {0, cx, -sx}, {0, sx, cx}};
+  double Ry[3][3] = {{cy, 0, sy}, {0, 1, 0}, {-sy, 0, cy}};
+  double Rz[3][3] = {{cz, -sz, 0}, {sz, cz, 0}, {0, 0, 1}};
+  double T[3][3], R[3][3];
+  for (int i = 0; i < 3; i++)
+    for (int j = 0; j < 3; j++) {
+      T[i][j] = 0;
+      for (int k = 0; k < 3; k++) T[i][j] += Ry[i][k] * Rx[k][j];
+    }
+  for (int i = 0; i < 3; i++)
+    for (int j = 0; j < 3; j++) {
+      R[i][j] = 0;
+      for (int k = 0; k < 3; k++) R[i][j] += T[i][k] * Rz[k][j];
+    }
+  Mat4 M;
+  std::memset(M.m, 0, sizeof(M.m));
+  // p_view_j = sum_i (p_i - loc_i) R[i][j]
+  for (int i = 0; i < 3; i++)
+    for (int j = 0; j < 3; j++) M.m[i * 4 + j] = (float)R[i][j];
+  for (int j = 0; j < 3; j++) {
+    const float t = c.location[0] * M.m[0 * 4 + j] + c.location[1] * M.m[1 * 4 + j] + c.location[2] * M.m[2 * 4 + j];
+    M.m[12 + j] = -t;
+  }
+  M.m[15] = 1.0f;
+  return M;
+}
+
+inline void xformPoint(const Mat4& M, const float* p, float* o) {
+  for (int j = 0; j < 3; j++) o[j] = ((p[0] * M.m[j] + p[1] * M.m[4 + j]) + p[2] * M.m[8 + j]) + M.m[12 + j];
+}
+inline void xformDir(const Mat4& M, const float* p, float* o) {
+  for (int j = 0; j < 3; j++) o[j] = (p[0] * M.m[j] + p[1] * M.m[4 + j]) + p[2] * M.m[8 + j];
+  const float l = std::sqrt((o[0] * o[0] + o[1] * o[1]) + o[2] * o[2]);
+  if (l > 0) { o[0] /= l; o[1] /= l; o[2] /= l; }
+}
+
+struct F3h {
+  float x, y, z;
+};
+inline F3h sub(F3h a, F3h b) { return {a.x - b.x, a.y - b.y, a.z - b.z}; }
+inline F3h crs(F3h a, F3h b) { return {a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x}; }
+inline float len(F3h a) { return std::sqrt((a.x * a.x + a.y * a.y) + a.z * a.z); }
+
+DevMaterial toDev(const rg_material& m) {
+  DevMaterial d;
+  d.cr = m.color[0]; d.cg = m.color[1]; d.cb = m.color[2];
+  d.glossy = m.glossy; d.roughness = m.roughness; d.transparency = m.transparency; d.refraction = m.refraction;
+  d.ior = m.refraction_ratio; d.chroma = m.chroma_dispersion; d.metallic = m.metallic; d.aniso = m.anisotropy;
+  d.anisoRot = m.aniso_rotation; d.emission = m.emission; d.spotRange = m.spot_range; d.texture = m.texture;
+  d.tileU = m.tex_tiling[0]; d.tileV = m.tex_tiling[1]; d.pad = 0;
+  return d;
+}
+
+// HomogeneousMedium::prepare (medium.cpp:18-57), constant mode.
+DevMedium toDev(const rg_medium& m) {
+  DevMedium d;
+  const float dn = std::fmax(0.0f, m.density);
+  d.ssr = m.sigma_s[0] * dn; d.ssg = m.sigma_s[1] * dn; d.ssb = m.sigma_s[2] * dn;
+  d.ser = m.sigma_e[0] * dn; d.seg = m.sigma_e[1] * dn; d.seb = m.sigma_e[2] * dn;
+  d.str = m.sigma_a[0] * dn + d.ssr; d.stg = m.sigma_a[1] * dn + d.ssg; d.stb = m.sigma_a[2] * dn + d.ssb;
+  d.hero = (d.str + d.stg + d.stb) * (1.0f / 3.0f);
+  d.g = m.g;
+  d.pad = 0;
+  return d;
+}
+
+
+}  // namespace
+
+}  // namespace rg
+
+using namespace rg;
+
+struct rg_handle {
+  rg_settings st;
+  std::mutex mu;
+  cudaStream_t stream = nullptr;
+  int device = 0;
+  int numSMs = 148;
+  std::unique_ptr<DeviceScene> scene;
+  DevScene dscene{};
+  rg_camera camera{};
+  Mat4 view{};
+  bool hasScene = false;
+  // render buffers
+  DevBuf<float4> sum, sumSq, hdr, ldr, bufA, bufB;
+  DevBuf<int> cnt, pixelList, listCount;
+  DevBuf<__half> aovNormal, aovAlbedo, aovAlbedoA, aovDepth;
+  int W = 0, H = 0;
+  bool haveResult = false;
+  // wavefront
+  DevBuf<float4> rayO0, rayO1, rayD0, rayD1, hits, pathT, pathR, pathL, shO0, shO1, shD0, shD1, shC0, shC1;
+  DevBuf<int> counters, error, curWave;
+  DevBuf<unsigned long long> stats;
+  DevBuf<DevWave> waves, waveSlot;
+  int capacity = 0;
+  int maxIter = 0;
+  // graph
+  cudaGraphExec_t graph = nullptr;
+  std::string graphKey;
+  // progress / cancel
+  rg_progress_fn progress = nullptr;
+  void* progressUser = nullptr;
+  std::atomic<bool> cancel{false};
+  rg_stats lastStats{};
+  ~rg_handle() {
+    if (graph) cudaGraphExecDestroy(graph);
+    scene.reset();
+    if (stream) cudaStreamDestroy(stream);
+  }
+};
+
+namespace rg {
+namespace {
+
+rg_status ensureQueues(rg_handle* h, int capacity, int maxIter) {
+  if (capacity <= h->capacity && maxIter <= h->maxIter) return RG_OK;
+  const size_t c = (size_t)std::max(capacity, h->capacity);
+  const int mi = std::max(maxIter, h->maxIter);
+  bool ok = h->rayO0.alloc(c) && h->rayO1.alloc(c) && h->rayD0.alloc(c) && h->rayD1.alloc(c) && h->hits.alloc(c) &&
+            h->pathT.alloc(c) && h->pathR.alloc(c) && h->pathL.alloc(c) && h->shO0.alloc(c) && h->shO1.alloc(c) &&
+            h->shD0.alloc(c) && h->shD1.alloc(c) && h->shC0.alloc(c) && h->shC1.alloc(c) &&
+            h->counters.alloc((size_t)(mi + 1) * kCountersPerIter) && h->error.alloc(1) && h->stats.alloc(8) &&
+            h->curWave.alloc(1);
+  if (!ok) {
+    setLastError("out of device memory (wavefront queues)");
+    return RG_ERR_OUT_OF_MEMORY;
+  }
+  h->capacity = (int)c;
+  h->maxIter = mi;
+  if (h->graph) {
+    cudaGraphExecDestroy(h->graph);
+    h->graph = nullptr;
+    h->graphKey.clear();
+  }
+  return RG_OK;
+}
+
+DevQueues makeQueues(rg_handle* h, int maxIter) {
+  DevQueues Q;
+  Q.rayO[0] = h->rayO0.p; Q.rayO[1] = h->rayO1.p;
+  Q.rayD[0] = h->rayD0.p; Q.rayD[1] = h->rayD1.p;
+  Q.hits = h->hits.p;
+  Q.pathT = h->pathT.p; Q.pathR = h->pathR.p; Q.pathL = h->pathL.p;
+  Q.shO[0] = h->shO0.p; Q.shO[1] = h->shO1.p;
+  Q.shD[0] = h->shD0.p; Q.shD[1] = h->shD1.p;
+  Q.shC[0] = h->shC0.p; Q.shC[1] = h->shC1.p;
+  Q.counters = h->counters.p;
+  Q.stats = h->stats.p;
+  Q.error = h->error.p;
+  Q.capacity = h->capacity;
+  Q.maxIter = maxIter;
+  return Q;
+}
+
+DevRender makeRender(const rg_handle* h) {
+  const rg_settings& s = h->st;
+  const rg_camera& c = h->camera;
+  DevRender R;
+  R.width = s.resolution_width;
+  R.height = s.resolution_height;
+  const float fov = std::fmin(std::fmax(c.field_of_view, 1.0f), 179.0f);
+  R.viewScale = (2.0f * std::tan(fov * (3.14159265358979323846f / 180.0f) * 0.5f)) / (float)R.height;
+  R.halfW = (float)R.width * 0.5f;
+  R.halfH = (float)R.height * 0.5f;
+  R.dof = c.depth_of_field;
+  R.aperture = c.aperture > 0.0f ? 1.0f / c.aperture : 0.0f;
+  R.blades = c.aperture_blades;
+  R.apertureRot = c.aperture_rotation * (3.14159265358979323846f / 180.0f);
+  R.exposure = c.exposure;
+  R.viewFar = c.view_far;
+  R.aa = s.enable_antialias;
+  R.colorSampling = s.enable_color_sampling;
+  R.shader = s.shader_provider;
+  R.maxDepth = s.max_depth;
+  R.rrDepth = s.rr_depth;
+  R.lightFix = s.light_pick_fix;
+  R.seed = s.seed;
+  R.clampMax = s.firefly_clamp;
+  R.backR = s.back_color[0]; R.backG = s.back_color[1]; R.backB = s.back_color[2];
+  R.worldR = s.world_color[0]; R.worldG = s.world_color[1]; R.worldB = s.world_color[2];
+  R.aoSamples = std::max(1, s.samples);
+  return R;
+}
+
+struct Grids {
+  int gen, ext, shade, conn, acc, simple;
+};
+
+Grids grids(rg_handle* h) {
+  Grids g;
+  g.gen = h->numSMs * 8;
+  g.ext = h->numSMs * 8;
+  g.shade = h->numSMs * 4;
+  g.conn = h->numSMs * 8;
+  g.acc = h->numSMs * 4;
+  g.simple = h->numSMs * 8;
+  return g;
+}
+
+// Launch one wave's kernel sequence on the stream (captured or direct).
+void enqueueWave(rg_handle* h, const DevRender& R, const DevQueues& Q, const DevWave* W, const int* cur, bool profile,
+                 std::vector<cudaEvent_t>* ev) {
+  (void)cur;
+  const Grids g = grids(h);
+  const cudaStream_t st = h->stream;
+  if (R.shader != 5) {
+    launchSimple(h->dscene, R, W, Q, g.simple, st);
+  } else {
+    launchGenerate(R, W, Q, h->dscene.globalMedium, g.gen, st);
+    for (int it = 0; it < Q.maxIter; it++) {
+      if (profile) cudaEventRecord((*ev)[it * 4 + 0], st);
+      launchExtend(h->dscene, Q, it, g.ext, st);
+      if (profile) cudaEventRecord((*ev)[it * 4 + 1], st);
+      launchShade(h->dscene, R, W, Q, it, g.shade, st);
+      if (profile) cudaEventRecord((*ev)[it * 4 + 2], st);
+      launchConnect(h->dscene, Q, it, 0, g.conn, st);
+      if (h->dscene.numPointLights > 0) launchConnect(h->dscene, Q, it, 1, g.conn, st);
+      if (profile) cudaEventRecord((*ev)[it * 4 + 3], st);
+    }
+  }
+  launchAccumulate(R, W, Q, h->sum.p, h->sumSq.p, h->cnt.p, g.acc, st);
+  k_nextWave<<<1, 1, 0, st>>>(h->curWave.p);
+}
+
+}  // namespace
+}  // namespace rg
+
+// The wave descriptor array is indexed through *curWave by every kernel; the
+// kernels take a pointer to the current element computed on the device.
+namespace rg {
+namespace {
+__global__ void k_selectWave(const DevWave* waves, const int* cur, DevWave* slot) {
+  if (threadIdx.x == 0 && blockIdx.x == 0) *slot = waves[*cur];
+}
+}  // namespace
+}  // namespace rg
+
+extern "C" {
+
+void rg_settings_default(rg_settings* s) {
+  if (!s) return;
+  std::memset(s, 0, sizeof(*s));
+  s->resolution_width = 800;  // DEFAULT_RENDER_WIDTH / HEIGHT, rayrenderer.h:25-26
+  s->resolution_height = 600;
+  s->threads = 1;             // RENDER_THREADS (linux), rayrenderer.h:42-44
+  s->samples = 100;           // TRACE_PATH_SAMPLES (linux)
+  s->shader_provider = 5;
+  s->enable_antialias = 1;
+  s->enable_point_light_antialias = 1;
+  s->enable_color_sampling = 1;
+  s->enable_rendering_postprocess = 0;
+  s->enable_denoise = 0;
+  s->cull_back_face = 0;
+  s->denoise_levels = 5;
+  s->denoise_sigma_color = 0.4f;
+  s->denoise_sigma_normal = 128.0f;
+  s->denoise_sigma_depth = 0.1f;
+  s->denoise_intensity = 1.0f;
+  s->firefly_clamp = 10.0f;
+  s->enable_adaptive_sampling = 0;
+  s->adaptive_base_samples = 4;
+  s->adaptive_threshold = 0.02f;
+  s->adaptive_mode = RG_ADAPTIVE_TILE;
+  s->bloom_threshold = 1.0f;
+  s->bloom_strength = 1.0f;
+  s->bloom_radius = 0.03f;
+  s->bloom_size_aspect = 0.15f;
+  s->bloom_curve = 1.0f;
+  s->world_color[0] = 0.1f; s->world_color[1] = 0.095f; s->world_color[2] = 0.09f;
+  s->back_color[0] = 0.2f; s->back_color[1] = 0.19f; s->back_color[2] = 0.18f; s->back_color[3] = 0.0f;
+  s->seed = 1;
+  s->max_depth = 32;          // MAX_TRACE_DEPTH, rayrenderer.cpp:38
+  s->rr_depth = 3;            // MIN_RR_DEPTH, rayrenderer.cpp:41
+  s->light_pick_fix = 0;
+  s->paths_per_wave = 0;
+  s->bvh_bins = 32;
+}
+
+const char* rg_last_error(void) { return g_lastError.c_str(); }
+const char* rg_version(void) { return "raygen-b200 0.1 (sm_100a wavefront tracer)"; }
+
+rg_status rg_create(const rg_settings* s, rg_handle** out) {
+  if (!out) return RG_ERR_INVALID_ARGUMENT;
+  *out = nullptr;
+  int n = 0;
+  if (cudaGetDeviceCount(&n) != cudaSuccess || n == 0) {
+    cudaGetLastError();
+    setLastError("no CUDA device");
+    return RG_ERR_NO_DEVICE;
+  }
+  rg_handle* h = new (std::nothrow) rg_handle();
+  if (!h) return RG_ERR_OUT_OF_MEMORY;
+  if (s) h->st = *s;
+  else rg_settings_default(&h->st);
+  cudaGetDevice(&h->device);
+  cudaDeviceGetAttribute(&h->numSMs, cudaDevAttrMultiProcessorCount, h->device);
+  if (cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking) != cudaSuccess) {
+    setLastError("cudaStreamCreate failed");
+    delete h;
+    return RG_ERR_CUDA;
+  }
+  *out = h;
+  return RG_OK;
+}
+
+rg_status rg_destroy(rg_handle* h) {
+  if (!h) return RG_ERR_INVALID_ARGUMENT;
+  {
+    std::lock_guard<std::mutex> lk(h->mu);
+    if (h->stream) cudaStreamSynchronize(h->stream);
+  }
+  delete h;
+  return RG_OK;
+}
+
+rg_status rg_update_settings(rg_handle* h, const rg_settings* s) {
+  if (!h || !s) return RG_ERR_INVALID_ARGUMENT;
+  std::lock_guard<std::mutex> lk(h->mu);
+  h->st = *s;
+  return RG_OK;
+}
+
+rg_status rg_set_progress_cb(rg_handle* h, rg_progress_fn fn, void* user) {
+  if (!h) return RG_ERR_INVALID_ARGUMENT;
+  h->progress = fn;
+  h->progressUser = user;
+  return RG_OK;
+}
+
+rg_status rg_cancel(rg_handle* h) {
+  if (!h) return RG_ERR_INVALID_ARGUMENT;
+  h->cancel.store(true);
+  return RG_OK;
+}
+
+rg_status rg_set_scene(rg_handle* h, const rg_scene_desc* d) {
+  if (!h || !d) return RG_ERR_INVALID_ARGUMENT;
+  std::lock_guard<std::mutex> lk(h->mu);
+  const int nt = d->num_triangles;
+  if (nt < 0 || d->num_meshes < 0 || d->num_objects < 0 || d->num_materials < 0 || d->num_media < 0 ||
+      d->num_point_lights < 0 || d->num_textures < 0) {
+    setLastError("negative count in scene description");
+    return RG_ERR_INVALID_ARGUMENT;
+  }
+  if (nt > 0 && (!d->positions || !d->normals || !d->tri_mesh)) {
+    setLastError("scene description without triangle arrays");
+    return RG_ERR_INVALID_ARGUMENT;
+  }
+  if (nt >= (1 << 28)) {
+    setLastError("more than 2^28 triangles");
+    return RG_ERR_INVALID_ARGUMENT;
+  }
+  for (int i = 0; i < d->num_meshes; i++)
+    if (d->mesh_object[i] < 0 || d->mesh_object[i] >= d->num_objects) {
+      setLastError("mesh_object index out of range");
+      return RG_ERR_INVALID_ARGUMENT;
+    }
+  for (int i = 0; i < d->num_objects; i++)
+    if (d->objects[i].material < 0 || d->objects[i].material >= d->num_materials ||
+        d->objects[i].interior_medium >= d->num_media) {
+      setLastError("object material / medium index out of range");
+      return RG_ERR_INVALID_ARGUMENT;
+    }
+  for (int i = 0; i < nt; i++)
+    if (d->tri_mesh[i] < 0 || d->tri_mesh[i] >= d->num_meshes) {
+      setLastError("tri_mesh index out of range");
+      return RG_ERR_INVALID_ARGUMENT;
+    }
+  for (int i = 0; i < d->num_materials; i++)
+    if (d->materials[i].texture >= d->num_textures) {
+      setLastError("material texture index out of range");
+      return RG_ERR_INVALID_ARGUMENT;
+    }
+  if (d->global_medium >= d->num_media || d->num_media > 1000) {
+    setLastError("global medium index out of range");
+    return RG_ERR_INVALID_ARGUMENT;
+  }
+  cudaStream_t st = h->stream;
+  h->hasScene = false;
+  h->haveResult = false;
+  h->scene.reset(new DeviceScene());
+  DeviceScene& ds = *h->scene;
+  ds.numTris = nt;
+  h->camera = d->camera;
+  h->view = viewMatrix(d->camera);
+  ds.hasUV = d->uvs != nullptr && d->num_textures > 0;
+  // tables
+  std::vector<int> meshTriCount(d->num_meshes, 0);
+  for (int i = 0; i < nt; i++) meshTriCount[d->tri_mesh[i]]++;
+  std::vector<int> objMat(d->num_objects), objMed(d->num_objects);
+  for (int i = 0; i < d->num_objects; i++) { objMat[i] = d->objects[i].material; objMed[i] = d->objects[i].interior_medium; }
+  std::vector<DevMaterial> mats(d->num_materials);
+  for (int i = 0; i < d->num_materials; i++) mats[i] = toDev(d->materials[i]);
+  std::vector<DevMedium> media(d->num_media);
+  for (int i = 0; i < d->num_media; i++) media[i] = toDev(d->media[i]);
+  ds.globalMedium = d->global_medium;
+  // area lights (rayrenderer.cpp:333-353): emissive objects with meshes, object order
+  std::vector<std::vector<int>> objMeshes(d->num_objects);
+  for (int i = 0; i < d->num_meshes; i++) objMeshes[d->mesh_object[i]].push_back(i);
+  std::vector<std::vector<int>> meshTris(d->num_meshes);
+  std::vector<int> areaLightObj, lightMeshList;
+  std::vector<int2> lightObjMeshes(std::max(1, d->num_objects), make_int2(0, 0));
+  std::vector<int2> lightMeshTris(std::max(1, d->num_meshes), make_int2(0, 0));
+  std::vector<float4> lightTris;
+  {
+    std::vector<char> isLightMesh(d->num_meshes, 0);
+    for (int o = 0; o < d->num_objects; o++) {
+      if (!(d->materials[objMat[o]].emission > 0.0f) || objMeshes[o].empty()) continue;
+      areaLightObj.push_back(o);
+      lightObjMeshes[o] = make_int2((int)lightMeshList.size(), (int)objMeshes[o].size());
+      for (int m : objMeshes[o]) { lightMeshList.push_back(m); isLightMesh[m] = 1; }
+    }
+    for (int i = 0; i < nt; i++)
+      if (isLightMesh[d->tri_mesh[i]]) meshTris[d->tri_mesh[i]].push_back(i);
+    for (int m = 0; m < d->num_meshes; m++) {
+      if (!isLightMesh[m]) continue;
+      lightMeshTris[m] = make_int2((int)(lightTris.size() / 6), (int)meshTris[m].size());
+      for (int i : meshTris[m]) {
+        float v[3][3], n[3][3];
+        for (int k = 0; k < 3; k++) {
+          xformPoint(h->view, &d->positions[(size_t)i * 9 + k * 3], v[k]);
+          xformDir(h->view, &d->normals[(size_t)i * 9 + k * 3], n[k]);
+        }
+        const F3h v1{v[0][0], v[0][1], v[0][2]}, v2{v[1][0], v[1][1], v[1][2]}, v3_{v[2][0], v[2][1], v[2][2]};
+        const float tia = 1.0f / len(crs(sub(v1, v2), sub(v1, v3_)));
+        const float area = 0.5f * len(crs(sub(v2, v1), sub(v3_, v1)));
+        lightTris.push_back(make_float4(v1.x, v1.y, v1.z, tia));
+        lightTris.push_back(make_float4(v2.x, v2.y, v2.z, area));
+        lightTris.push_back(make_float4(v3_.x, v3_.y, v3_.z, 0.0f));
+        for (int k = 0; k < 3; k++) lightTris.push_back(make_float4(n[k][0], n[k][1], n[k][2], 0.0f));
+      }
+    }
+  }
+  std::vector<DevPointLight> pts(d->num_point_lights);
+  for (int i = 0; i < d->num_point_lights; i++) {
+    float p[3], n[3];
+    xformPoint(h->view, d->point_lights[i].position, p);
+    xformDir(h->view, d->point_lights[i].normal, n);
+    pts[i] = DevPointLight{p[0], p[1], p[2], n[0], n[1], n[2], d->point_lights[i].material, 0};
+  }
+  bool ok = ds.meshTriCount.upload(meshTriCount.data(), meshTriCount.size(), st) &&
+            ds.meshObj.upload(d->mesh_object, d->num_meshes, st) && ds.objMat.upload(objMat.data(), objMat.size(), st) &&
+            ds.objMedium.upload(objMed.data(), objMed.size(), st) && ds.mats.upload(mats.data(), mats.size(), st) &&
+            ds.media.upload(media.data(), media.size(), st) &&
+            ds.areaLightObj.upload(areaLightObj.data(), areaLightObj.size(), st) &&
+            ds.lightMeshList.upload(lightMeshList.data(), lightMeshList.size(), st) &&
+            ds.lightObjMeshes.upload(lightObjMeshes.data(), lightObjMeshes.size(), st) &&
+            ds.lightMeshTris.upload(lightMeshTris.data(), lightMeshTris.size(), st) &&
+            ds.lightTris.upload(lightTris.data(), lightTris.size(), st) && ds.points.upload(pts.data(), pts.size(), st) &&
+            ds.view.upload(h->view.m, 16, st) && ds.inPos.upload(d->positions, (size_t)nt * 9, st) &&
+            ds.inNrm.upload(d->normals, (size_t)nt * 9, st) && ds.inTriMesh.upload(d->tri_mesh, nt, st);
+  if (ok && ds.hasUV) ok = ds.inUV.upload(d->uvs, (size_t)nt * 6, st);
+  // textures
+  std::vector<DevTexture> texs(d->num_textures);
+  for (int i = 0; ok && i < d->num_textures; i++) {
+    const rg_texture& t = d->textures[i];
+    auto* buf = new DevBuf<float4>();
+    ds.texels.push_back(buf);
+    const size_t cnt = (size_t)std::max(0, t.width) * std::max(0, t.height);
+    ok = buf->upload(reinterpret_cast<const float4*>(t.rgba), cnt, st);
+    texs[i] = DevTexture{buf->p, t.width, t.height, t.is_hdr, 0};
+  }
+  if (ok) ok = ds.textures.upload(texs.data(), texs.size(), st);
+  if (!ok) {
+    setLastError("scene upload failed (device memory)");
+    h->scene.reset();
+    return RG_ERR_OUT_OF_MEMORY;
+  }
+  ds.numAreaLights = (int)areaLightObj.size();
+  ds.numPointLights = (int)pts.size();
+  ds.numTextures = d->num_textures;
+  cudaEvent_t e0, e1;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  cudaEventRecord(e0, st);
+  std::string err;
+  const rg_status rs = buildDeviceBvh(ds, h->st.bvh_bins > 1 ? h->st.bvh_bins : 32, st, err);
+  cudaEventRecord(e1, st);
+  cudaStreamSynchronize(st);
+  float ms = 0.0f;
+  cudaEventElapsedTime(&ms, e0, e1);
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  if (rs != RG_OK) {
+    setLastError(err);
+    h->scene.reset();
+    return rs;
+  }
+  h->lastStats.build_ms = ms;
+  h->lastStats.bvh_nodes = ds.numNodes;
+  ds.inPos.release();
+  ds.inNrm.release();
+  ds.inUV.release();
+  ds.inTriMesh.release();
+  DevScene& S = h->dscene;
+  S.nodes = ds.nodes.p;
+  S.numNodes = ds.numNodes;
+  S.rootIsLeaf = ds.rootIsLeaf;
+  S.rootLeafRef = ds.rootLeafRef;
+  S.triVerts = ds.triVerts.p;
+  S.triShade = ds.triShade.p;
+  S.triUV = ds.hasUV ? ds.triUV.p : nullptr;
+  S.triOrig = ds.triOrig.p;
+  S.numTris = nt;
+  S.meshObj = ds.meshObj.p;
+  S.meshTriCount = ds.meshTriCount.p;
+  S.objMat = ds.objMat.p;
+  S.objMedium = ds.objMedium.p;
+  S.mats = ds.mats.p;
+  S.media = ds.media.p;
+  S.globalMedium = ds.globalMedium;
+  S.numAreaLights = ds.numAreaLights;
+  S.areaLightObj = ds.areaLightObj.p;
+  S.lightObjMeshes = ds.lightObjMeshes.p;
+  S.lightMeshList = ds.lightMeshList.p;
+  S.lightMeshTris = ds.lightMeshTris.p;
+  S.lightTris = ds.lightTris.p;
+  S.numPointLights = ds.numPointLights;
+  S.points = ds.points.p;
+  S.textures = ds.textures.p;
+  S.numTextures = ds.numTextures;
+  h->hasScene = true;
+  if (h->graph) {
+    cudaGraphExecDestroy(h->graph);
+    h->graph = nullptr;
+    h->graphKey.clear();
+  }
+  return RG_OK;
+}
+
+static rg_status runPass(rg_handle* h, const DevRender& R, int numPixels, const int* pixelList, int spp,
+                         int& wavesDone, int totalWavesHint, bool profile, double* kernelMs) {
+  if (numPixels <= 0 || spp <= 0) return RG_OK;
+  const long long cap = h->st.paths_per_wave > 0 ? h->st.paths_per_wave : (8ll << 20);
+  std::vector<DevWave> ws;
+  const int spw = numPixels >= cap ? 1 : (int)std::min<long long>(spp, std::max<long long>(1, cap / numPixels));
+  const int pixChunk = (int)std::min<long long>(numPixels, cap);
+  for (int s = 0; s < spp; s += spw)
+    for (int p = 0; p < numPixels; p += pixChunk) {
+      DevWave w;
+      w.numPixels = std::min(pixChunk, numPixels - p);
+      w.samplesInWave = std::min(spw, spp - s);
+      w.sampleBase = 0;
+      w.pixelOffset = p;
+      w.pixelList = pixelList;
+      w.pixelSampleBase = h->cnt.p;
+      ws.push_back(w);
+    }
+  const int capacity = std::min<long long>(cap, (long long)pixChunk * spw);
+  const int maxIter = R.maxDepth + 2;
+  rg_status rs = ensureQueues(h, capacity, maxIter);
+  if (rs != RG_OK) return rs;
+  if (!h->waves.alloc(ws.size() + 1)) {
+    setLastError("out of device memory (waves)");
+    return RG_ERR_OUT_OF_MEMORY;
+  }
+  RG_CUDA_CHECK(cudaMemcpyAsync(h->waves.p, ws.data(), ws.size() * sizeof(DevWave), cudaMemcpyHostToDevice, h->stream));
+  RG_CUDA_CHECK(cudaMemsetAsync(h->curWave.p, 0, sizeof(int), h->stream));
+  const DevQueues Q = makeQueues(h, maxIter);
+  // the kernels read the current wave from a fixed one-element slot
+  if (!h->waveSlot.alloc(1)) return RG_ERR_OUT_OF_MEMORY;
+  DevWave* slot = h->waveSlot.p;
+  std::vector<cudaEvent_t> ev;
+  if (profile) {
+    ev.resize((size_t)maxIter * 4);
+    for (auto& e : ev) cudaEventCreate(&e);
+  }
+  // graph of one wave: select the wave descriptor, then the kernel sequence
+  const std::string key = std::to_string((uintptr_t)h->waves.p) + ":" + std::to_string((uintptr_t)slot) + ":" +
+                          std::to_string(maxIter) + ":" + std::to_string(R.shader) + ":" + std::to_string(h->capacity) +
+                          ":" + std::to_string((uintptr_t)pixelList) + ":" +
+                          std::string((const char*)&R, sizeof(R));
+  if (!profile && (h->graph == nullptr || h->graphKey != key)) {
+    if (h->graph) {
+      cudaGraphExecDestroy(h->graph);
+      h->graph = nullptr;
+    }
+    cudaGraph_t g;
+    RG_CUDA_CHECK(cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
+    k_selectWave<<<1, 1, 0, h->stream>>>(h->waves.p, h->curWave.p, slot);
+    enqueueWave(h, R, Q, slot, h->curWave.p, false, nullptr);
+    RG_CUDA_CHECK(cudaStreamEndCapture(h->stream, &g));
+    const cudaError_t ie = cudaGraphInstantiate(&h->graph, g, 0);
+    cudaGraphDestroy(g);
+    if (ie != cudaSuccess) {
+      setLastError(std::string("cudaGraphInstantiate: ") + cudaGetErrorString(ie));
+      h->graph = nullptr;
+      return RG_ERR_CUDA;
+    }
+    h->graphKey = key;
+  }
+  for (size_t k = 0; k < ws.size(); k++) {
+    if (h->cancel.load()) return RG_ERR_CANCELLED;
+    if (profile) {
+      k_selectWave<<<1, 1, 0, h->stream>>>(h->waves.p, h->curWave.p, slot);
+      enqueueWave(h, R, Q, slot, h->curWave.p, true, &ev);
+      RG_CUDA_CHECK(cudaStreamSynchronize(h->stream));
+      if (R.shader == 5) {
+        for (int it = 0; it < maxIter; it++) {
+          float a = 0, b = 0, c = 0;
+          cudaEventElapsedTime(&a, ev[it * 4 + 0], ev[it * 4 + 1]);
+          cudaEventElapsedTime(&b, ev[it * 4 + 1], ev[it * 4 + 2]);
+          cudaEventElapsedTime(&c, ev[it * 4 + 2], ev[it * 4 + 3]);
+          kernelMs[0] += a;
+          kernelMs[1] += b;
+          kernelMs[2] += c;
+        }
+      }
+    } else {
+      RG_CUDA_CHECK(cudaGraphLaunch(h->graph, h->stream));
+    }
+    wavesDone++;
+    if (h->progress) {
+      // progress is reported from the calling thread once the wave is queued
+      const float pr = totalWavesHint > 0 ? std::min(1.0f, (float)wavesDone / (float)totalWavesHint) : 0.0f;
+      h->progress(pr, h->progressUser);
+    }
+  }
+  for (auto& e : ev) cudaEventDestroy(e);
+  return RG_OK;
+}
+
+rg_status rg_render(rg_handle* h) {
+  if (!h) return RG_ERR_INVALID_ARGUMENT;
+  std::lock_guard<std::mutex> lk(h->mu);
+  const rg_settings& s = h->st;
+  if (s.shader_provider == 4) {
+    setLastError("shader 4 is reserved (no provider in the reference)");
+    return RG_ERR_UNSUPPORTED;
+  }
+  if (s.shader_provider < 0 || s.shader_provider > 5) {
+    setLastError("unknown shader id");
+    return RG_ERR_INVALID_ARGUMENT;
+  }
+  if (!h->hasScene) {
+    setLastError("no scene set");
+    return RG_ERR_NO_SCENE;
+  }
+  if (s.resolution_width <= 0 || s.resolution_height <= 0 ||
+      (long long)s.resolution_width * s.resolution_height > (1ll << 28) || s.max_depth < 1 || s.max_depth > 250 ||
+      s.samples < 0) {
+    setLastError("invalid resolution / depth / samples");
+    return RG_ERR_INVALID_ARGUMENT;
+  }
+  h->cancel.store(false);
+  h->haveResult = false;
+  const int W = s.resolution_width, H = s.resolution_height, N = W * H;
+  const bool profile = std::getenv("RG_PROFILE_KERNELS") != nullptr;
+  if (!h->sum.alloc(N) || !h->sumSq.alloc(N) || !h->cnt.alloc(N) || !h->hdr.alloc(N) || !h->ldr.alloc(N) ||
+      !h->pixelList.alloc(N) || !h->listCount.alloc(1)) {
+    setLastError("out of device memory (image buffers)");
+    return RG_ERR_OUT_OF_MEMORY;
+  }
+  h->W = W;
+  h->H = H;
+  cudaStream_t st = h->stream;
+  RG_CUDA_CHECK(cudaMemsetAsync(h->sum.p, 0, sizeof(float4) * N, st));
+  RG_CUDA_CHECK(cudaMemsetAsync(h->sumSq.p, 0, sizeof(float4) * N, st));
+  RG_CUDA_CHECK(cudaMemsetAsync(h->cnt.p, 0, sizeof(int) * N, st));
+  DevRender R = makeRender(h);
+  // stats reset
+  if (!h->stats.alloc(8) || !h->error.alloc(1)) return RG_ERR_OUT_OF_MEMORY;
+  RG_CUDA_CHECK(cudaMemsetAsync(h->stats.p, 0, sizeof(unsigned long long) * 8, st));
+  RG_CUDA_CHECK(cudaMemsetAsync(h->error.p, 0, sizeof(int), st));
+  if (s.enable_denoise) {
+    if (!h->aovNormal.alloc((size_t)N * 3) || !h->aovAlbedo.alloc((size_t)N * 3) || !h->aovAlbedoA.alloc(N) ||
+        !h->aovDepth.alloc(N) || !h->bufA.alloc(N) || !h->bufB.alloc(N)) {
+      setLastError("out of device memory (denoise buffers)");
+      return RG_ERR_OUT_OF_MEMORY;
+    }
+    launchAov(h->dscene, R, h->aovNormal.p, h->aovAlbedo.p, h->aovAlbedoA.p, h->aovDepth.p, st);
+  }
+  cudaEvent_t t0, t1, t2;
+  cudaEventCreate(&t0);
+  cudaEventCreate(&t1);
+  cudaEventCreate(&t2);
+  cudaEventRecord(t0, st);
+  int wavesDone = 0;
+  double kms[3] = {0, 0, 0};
+  rg_status rs = RG_OK;
+  const int target = std::max(0, s.samples);
+  if (!s.enable_adaptive_sampling) {
+    const long long cap = s.paths_per_wave > 0 ? s.paths_per_wave : (8ll << 20);
+    const int spw = N >= cap ? 1 : (int)std::min<long long>(std::max(1, target), std::max<long long>(1, cap / N));
+    const int hint = (int)(((target + spw - 1) / std::max(1, spw)) * ((N + cap - 1) / cap));
+    rs = runPass(h, R, N, nullptr, target, wavesDone, hint, profile, kms);
+  } else {
+    // renderAdaptive (rayrenderer.cpp:1162-1252): base pass, then refinement passes
+    const int base = std::max(1, s.adaptive_base_samples);
+    int spent = std::min(base, target);
+    rs = runPass(h, R, N, nullptr, spent, wavesDone, 0, profile, kms);
+    while (rs == RG_OK && spent < target) {
+      RG_CUDA_CHECK(cudaMemsetAsync(h->listCount.p, 0, sizeof(int), st));
+      if (s.adaptive_mode == RG_ADAPTIVE_TILE)
+        launchAdaptiveTiles(W, H, h->sum.p, h->sumSq.p, h->cnt.p, target, s.adaptive_threshold, h->pixelList.p,
+                            h->listCount.p, st);
+      else
+        launchAdaptivePixels(N, h->sum.p, h->sumSq.p, h->cnt.p, target, s.adaptive_threshold, h->pixelList.p,
+                             h->listCount.p, st);
+      int active = 0;
+      RG_CUDA_CHECK(cudaMemcpyAsync(&active, h->listCount.p, sizeof(int), cudaMemcpyDeviceToHost, st));
+      RG_CUDA_CHECK(cudaStreamSynchronize(st));
+      if (active == 0) break;
+      const int passCount = std::min(base, target - spent);
+      rs = runPass(h, R, active, h->pixelList.p, passCount, wavesDone, 0, profile, kms);
+      spent += passCount;
+    }
+  }
+  cudaEventRecord(t1, st);
+  if (rs != RG_OK) {
+    cudaStreamSynchronize(st);
+    cudaEventDestroy(t0);
+    cudaEventDestroy(t1);
+    cudaEventDestroy(t2);
+    return rs;
+  }
+  launchResolve(N, h->sum.p, h->cnt.p, h->camera.exposure, h->hdr.p, st);
+  if (s.enable_denoise) {
+    launchDenoise(W, H, h->hdr.p, h->aovNormal.p, h->aovDepth.p, h->aovAlbedo.p, h->aovAlbedoA.p, s.denoise_levels,
+                  s.denoise_sigma_color, s.denoise_sigma_normal, s.denoise_sigma_depth, s.denoise_intensity, h->bufA.p,
+                  h->bufB.p, h->ldr.p, st);
+    RG_CUDA_CHECK(cudaMemcpyAsync(h->hdr.p, h->ldr.p, sizeof(float4) * N, cudaMemcpyDeviceToDevice, st));
+  }
+  launchTonemap(N, h->hdr.p, h->ldr.p, st);
+  cudaEventRecord(t2, st);
+  const cudaError_t se = cudaStreamSynchronize(st);
+  float traceMs = 0, postMs = 0;
+  cudaEventElapsedTime(&traceMs, t0, t1);
+  cudaEventElapsedTime(&postMs, t1, t2);
+  cudaEventDestroy(t0);
+  cudaEventDestroy(t1);
+  cudaEventDestroy(t2);
+  if (se != cudaSuccess) {
+    setLastError(std::string("render failed: ") + cudaGetErrorString(se));
+    return RG_ERR_CUDA;
+  }
+  unsigned long long stv[8] = {0};
+  int derr = 0;
+  cudaMemcpy(stv, h->stats.p, sizeof(stv), cudaMemcpyDeviceToHost);
+  cudaMemcpy(&derr, h->error.p, sizeof(int), cudaMemcpyDeviceToHost);
+  rg_stats& S = h->lastStats;
+  S.trace_ms = traceMs;
+  S.post_ms = postMs;
+  S.nodes_visited = stv[0];
+  S.tris_tested = stv[1];
+  S.shadow_nodes_visited = stv[2];
+  S.shadow_tris_tested = stv[3];
+  S.closest_rays = stv[4];
+  S.shadow_rays = stv[5];
+  S.extend_ms = kms[0];
+  S.shade_ms = kms[1];
+  S.connect_ms = kms[2];
+  S.waves = wavesDone;
+  S.device_error = derr;
+  {
+    std::vector<int> c(N);
+    cudaMemcpy(c.data(), h->cnt.p, sizeof(int) * N, cudaMemcpyDeviceToHost);
+    uint64_t tot = 0;
+    for (int v : c) tot += (uint64_t)v;
+    S.samples = tot;
+  }
+  const int perWave = s.shader_provider == 5 ? (3 + (h->maxIter) * (3 + (h->dscene.numPointLights > 0))) : 4;
+  S.kernel_launches = wavesDone * perWave;
+  if (derr != 0) {
+    setLastError("device error flag raised: " + std::to_string(derr));
+    return RG_ERR_DEVICE_STATUS;
+  }
+  h->haveResult = true;
+  return RG_OK;
+}
+
+rg_status rg_get_hdr(rg_handle* h, float* rgba, size_t count) {
+  if (!h || !rgba) return RG_ERR_INVALID_ARGUMENT;
+  std::lock_guard<std::mutex> lk(h->mu);
+  if (!h->haveResult) return RG_ERR_NO_SCENE;
+  if (count < (size_t)h->W * h->H * 4) return RG_ERR_INVALID_ARGUMENT;
+  RG_CUDA_CHECK(cudaMemcpy(rgba, h->hdr.p, sizeof(float4) * h->W * h->H, cudaMemcpyDeviceToHost));
+  return RG_OK;
+}
+
+rg_status rg_get_ldr(rg_handle* h, float* rgba, size_t count) {
+  if (!h || !rgba) return RG_ERR_INVALID_ARGUMENT;
+  std::lock_guard<std::mutex> lk(h->mu);
+  if (!h->haveResult) return RG_ERR_NO_SCENE;
+  if (count < (size_t)h->W * h->H * 4) return RG_ERR_INVALID_ARGUMENT;
+  RG_CUDA_CHECK(cudaMemcpy(rgba, h->ldr.p, sizeof(float4) * h->W * h->H, cudaMemcpyDeviceToHost));
+  return RG_OK;
+}
+
+rg_status rg_get_aovs(rg_handle* h, float* normal, float* albedo, float* depth, size_t count) {
+  if (!h) return RG_ERR_INVALID_ARGUMENT;
+  std::lock_guard<std::mutex> lk(h->mu);
+  if (!h->haveResult || !h->st.enable_denoise) return RG_ERR_NO_SCENE;
+  const int N = h->W * h->H;
+  if (count < (size_t)N * 3) return RG_ERR_INVALID_ARGUMENT;
+  DevBuf<float> tmp;
+  if (!tmp.alloc((size_t)N * 3)) return RG_ERR_OUT_OF_MEMORY;
+  if (normal) {
+    launchHalfToFloat(N * 3, h->aovNormal.p, tmp.p, h->stream);
+    RG_CUDA_CHECK(cudaMemcpyAsync(normal, tmp.p, sizeof(float) * N * 3, cudaMemcpyDeviceToHost, h->stream));
+    RG_CUDA_CHECK(cudaStreamSynchronize(h->stream));
+  }
+  if (albedo) {
+    launchHalfToFloat(N * 3, h->aovAlbedo.p, tmp.p, h->stream);
+    RG_CUDA_CHECK(cudaMemcpyAsync(albedo, tmp.p, sizeof(float) * N * 3, cudaMemcpyDeviceToHost, h->stream));
+    RG_CUDA_CHECK(cudaStreamSynchronize(h->stream));
+  }
+  if (depth) {
+    launchHalfToFloat(N, h->aovDepth.p, tmp.p, h->stream);
+    RG_CUDA_CHECK(cudaMemcpyAsync(depth, tmp.p, sizeof(float) * N, cudaMemcpyDeviceToHost, h->stream));
+    RG_CUDA_CHECK(cudaStreamSynchronize(h->stream));
+  }
+  return RG_OK;
+}
+
+rg_status rg_get_sample_counts(rg_handle* h, int32_t* counts, size_t count) {
+  if (!h || !counts) return RG_ERR_INVALID_ARGUMENT;
+  std::lock_guard<std::mutex> lk(h->mu);
+  if (!h->haveResult) return RG_ERR_NO_SCENE;
+  if (count < (size_t)h->W * h->H) return RG_ERR_INVALID_ARGUMENT;
+  RG_CUDA_CHECK(cudaMemcpy(counts, h->cnt.p, sizeof(int) * h->W * h->H, cudaMemcpyDeviceToHost));
+  return RG_OK;
+}
+
+rg_status rg_get_stats(rg_handle* h, rg_stats* out) {
+  if (!h || !out) return RG_ERR_INVALID_ARGUMENT;
+  *out = h->lastStats;
+  return RG_OK;
+}
+
+rg_status rg_get_view_matrix(rg_handle* h, float* m16) {
+  if (!h || !m16) return RG_ERR_INVALID_ARGUMENT;
+  std::memcpy(m16, h->view.m, sizeof(float) * 16);
+  return RG_OK;
+}
+
+rg_status rg_trace_closest(rg_handle* h, const float* rays, int32_t n, float* out_tuv, int32_t* out_prim) {
+  if (!h || n < 0 || (n > 0 && (!rays || !out_tuv || !out_prim))) return RG_ERR_INVALID_ARGUMENT;
+  std::lock_guard<std::mutex> lk(h->mu);
+  if (!h->hasScene) return RG_ERR_NO_SCENE;
+  if (n == 0) return RG_OK;
+  DevBuf<float> r, t;
+  DevBuf<int> p;
+  if (!r.upload(rays, (size_t)n * 6, h->stream) || !t.alloc((size_t)n * 3) || !p.alloc(n)) return RG_ERR_OUT_OF_MEMORY;
+  launchQueryClosest(h->dscene, r.p, n, t.p, p.p, h->stream);
+  RG_CUDA_CHECK(cudaMemcpyAsync(out_tuv, t.p, sizeof(float) * n * 3, cudaMemcpyDeviceToHost, h->stream));
+  RG_CUDA_CHECK(cudaMemcpyAsync(out_prim, p.p, sizeof(int) * n, cudaMemcpyDeviceToHost, h->stream));
+  RG_CUDA_CHECK(cudaStreamSynchronize(h->stream));
+  return RG_OK;
+}
+
+rg_status rg_trace_any(rg_handle* h, const float* rays, const float* tmax, int32_t n, int32_t predicate, uint8_t* out) {
+  if (!h || n < 0 || predicate < 0 || predicate > 3 || (n > 0 && (!rays || !tmax || !out))) return RG_ERR_INVALID_ARGUMENT;
+  std::lock_guard<std::mutex> lk(h->mu);
+  if (!h->hasScene) return RG_ERR_NO_SCENE;
+  if (n == 0) return RG_OK;
+  DevBuf<float> r, tm;
+  DevBuf<uint8_t> o;
+  if (!r.upload(rays, (size_t)n * 6, h->stream) || !tm.upload(tmax, n, h->stream) || !o.alloc(n)) return RG_ERR_OUT_OF_MEMORY;
+  const uint32_t occ = predicate == 0 ? kOccArea : (predicate == 1 ? kOccPoint : (predicate == 2 ? kOccAO : kOccAll));
+  launchQueryAny(h->dscene, r.p, tm.p, n, occ, o.p, h->stream);
+  RG_CUDA_CHECK(cudaMemcpyAsync(out, o.p, n, cudaMemcpyDeviceToHost, h->stream));
+  RG_CUDA_CHECK(cudaStreamSynchronize(h->stream));
+  return RG_OK;
+}
+
+rg_status rg_denoise_atrous(int32_t w, int32_t h, const float* color, const float* normal, const float* depth,
+                            const float* albedo, const float* albedo_alpha, int32_t levels, float sigma_color,
+                            float sigma_normal, float sigma_depth, float intensity, float* out) {
+  if (w <= 0 || h <= 0 || !color || !normal || !depth || !albedo || !albedo_alpha || !out) return RG_ERR_INVALID_ARGUMENT;
+  int dc = 0;
+  if (cudaGetDeviceCount(&dc) != cudaSuccess || dc == 0) {
+    cudaGetLastError();
+    return RG_ERR_NO_DEVICE;
+  }
+  const int N = w * h;
+  std::vector<float4> c4(N);
+  for (int i = 0; i < N; i++) c4[i] = make_float4(color[i * 3], color[i * 3 + 1], color[i * 3 + 2], 1.0f);
+  DevBuf<float4> c, a, b, o;
+  DevBuf<float> fn, fa, fd, faa;
+  DevBuf<__half> hn, ha, hd, haa;
+  cudaStream_t st = 0;
+  if (!c.upload(c4.data(), N, st) || !a.alloc(N) || !b.alloc(N) || !o.alloc(N) || !fn.upload(normal, (size_t)N * 3, st) ||
+      !fa.upload(albedo, (size_t)N * 3, st) || !fd.upload(depth, N, st) || !faa.upload(albedo_alpha, N, st) ||
+      !hn.alloc((size_t)N * 3) || !ha.alloc((size_t)N * 3) || !hd.alloc(N) || !haa.alloc(N))
+    return RG_ERR_OUT_OF_MEMORY;
+  launchFloatToHalf(N * 3, fn.p, hn.p, st);
+  launchFloatToHalf(N * 3, fa.p, ha.p, st);
+  launchFloatToHalf(N, fd.p, hd.p, st);
+  launchFloatToHalf(N, faa.p, haa.p, st);
+  launchDenoise(w, h, c.p, hn.p, hd.p, ha.p, haa.p, levels, sigma_color, sigma_normal, sigma_depth, intensity, a.p, b.p,
+                o.p, st);
+  RG_CUDA_CHECK(cudaMemcpy(c4.data(), o.p, sizeof(float4) * N, cudaMemcpyDeviceToHost));
+  for (int i = 0; i < N; i++) { out[i * 3] = c4[i].x; out[i * 3 + 1] = c4[i].y; out[i * 3 + 2] = c4[i].z; }
+  return RG_OK;
+}
+
+rg_status rg_tonemap(int32_t w, int32_t h, const float* hdr_rgba, float* ldr_rgba) {
+  if (w <= 0 || h <= 0 || !hdr_rgba || !ldr_rgba) return RG_ERR_INVALID_ARGUMENT;
+  int dc = 0;
+  if (cudaGetDeviceCount(&dc) != cudaSuccess || dc == 0) {
+    cudaGetLastError();
+    return RG_ERR_NO_DEVICE;
+  }
+  const int N = w * h;
+  DevBuf<float4> a, b;
+  if (!a.upload(reinterpret_cast<const float4*>(hdr_rgba), N, 0) || !b.alloc(N)) return RG_ERR_OUT_OF_MEMORY;
+  launchTonemap(N, a.p, b.p, 0);
+  RG_CUDA_CHECK(cudaMemcpy(ldr_rgba, b.p, sizeof(float4) * N, cudaMemcpyDeviceToHost));
+  return RG_OK;
+}
+
+static std::mutex g_storeMu;
+static std::unordered_map<const rg_scene_desc*, SceneStore*> g_stores;
+
+static rg_scene_desc* registerStore(SceneStore* st) {
+  std::lock_guard<std::mutex> lk(g_storeMu);
+  g_stores[&st->desc] = st;
+  return &st->desc;
+}
+
+rg_status rg_scene_builtin(int32_t kind, uint32_t seed, const int32_t* iparams, int32_t n_iparams, rg_scene_desc** out) {
+  if (!out) return RG_ERR_INVALID_ARGUMENT;
+  SceneStore* st = nullptr;
+  const rg_status rs = buildBuiltinScene(kind, seed, iparams, n_iparams, &st);
+  if (rs != RG_OK) return rs;
+  *out = registerStore(st);
+  return RG_OK;
+}
+
+rg_status rg_scene_free(rg_scene_desc* scene) {
+  if (!scene) return RG_ERR_INVALID_ARGUMENT;
+  SceneStore* st = nullptr;
+  {
+    std::lock_guard<std::mutex> lk(g_storeMu);
+    auto it = g_stores.find(scene);
+    if (it == g_stores.end()) return RG_ERR_INVALID_ARGUMENT;
+    st = it->second;
+    g_stores.erase(it);
+  }
+  delete st;
+  return RG_OK;
+}
+
+rg_status rg_load_scene_json(const char* path, rg_scene_desc** out) {
+  if (!path || !out) return RG_ERR_INVALID_ARGUMENT;
+  SceneStore* st = nullptr;
+  std::string err;
+  const rg_status rs = loadSceneJson(path, &st, err);
+  if (rs != RG_OK) {
+    setLastError(err);
+    return rs;
+  }
+  *out = registerStore(st);
+  return RG_OK;
+}
+
+}  // extern "C"

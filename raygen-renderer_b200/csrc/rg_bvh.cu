@@ -1,0 +1,590 @@
+// rg_bvh.cu - scene preparation and binned-SAH BVH build on the device.
+//
+// Reference: RayRenderer::transformScene / transformObject
+// (rayrenderer.cpp:157-363), RenderMeshTriangle::precalc (raycommon.cpp:128-149)
+// and TriangleBVH::build / buildRecursive (bvh.cpp:76-231).
+//
+// The reference builds top-down and recursively on one CPU thread: widest
+// centroid axis, 16 bins, leaf <= 4, cost 1 + 1.5 (A_L N_L + A_R N_R)/A_P
+// against 1.5 N.  Here the same split rule (bin count a parameter, 32 by
+// default) runs breadth-first: every level bins all open nodes at once
+// (shared-memory bins for blocks inside one node, global atomics across
+// nodes), picks splits one thread per node, and scatters primitives with
+// warp-aggregated atomics.  Leaves hold at most kMaxLeaf (8) triangles:
+// where the reference would keep a larger leaf, the best SAH bin (or, for
+// coincident centroids, an index median) splits it further.
+#include <cub/device/device_scan.cuh>
+
+#include <cfloat>
+#include <vector>
+
+#include "rg_device.cuh"
+#include "rg_host.h"
+
+namespace rg {
+
+namespace {
+
+__device__ __forceinline__ uint32_t fenc(float f) {
+  const uint32_t u = __float_as_uint(f);
+  return (u & 0x80000000u) ? ~u : (u | 0x80000000u);
+}
+__device__ __forceinline__ float fdec(uint32_t u) {
+  return __uint_as_float((u & 0x80000000u) ? (u & 0x7FFFFFFFu) : ~u);
+}
+
+struct BNode {
+  float bmin[3], bmax[3];
+  float cmin[3], cmax[3];
+  int start, count;
+  int left;      // first child (right = left + 1), -1 for leaves
+  int axis;
+  int binSlot;   // slot in the level's bin array while open
+  int splitBin;  // bins <= splitBin go left; -2 = index median split
+  int fill[2];   // scatter cursors for the children
+};
+
+struct BinData {  // ordered-uint encoded bounds, 16 words
+  uint32_t bmin[3], bmax[3], cmin[3], cmax[3];
+  uint32_t count;
+  uint32_t pad[3];
+};
+
+// ---- triangle preparation -------------------------------------------------
+// World -> view (camera translation; angles handled on the host by rotating
+// the input), edges, geometric normal, bounds, occluder bits.
+__global__ void k_prepTriangles(int n, const float* __restrict__ pos, const float* __restrict__ nrm,
+                                const float* __restrict__ uv, const int* __restrict__ triMesh,
+                                const int* __restrict__ meshObj, const int* __restrict__ objMat,
+                                const DevMaterial* __restrict__ mats, const float* __restrict__ view,
+                                float4* __restrict__ verts, float4* __restrict__ shade, float2* __restrict__ uvOut,
+                                float4* __restrict__ bmin, float4* __restrict__ bmax) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const float* p = pos + (size_t)i * 9;
+  const float* q = nrm + (size_t)i * 9;
+  V3 v[3], nn[3];
+  for (int k = 0; k < 3; k++) {
+    const V3 w = v3(p[k * 3], p[k * 3 + 1], p[k * 3 + 2]);
+    // p_view = [p 1] * M (row vector, M row-major 4x4), non-contracted
+    v[k].x = __fadd_rn(__fadd_rn(__fadd_rn(__fmul_rn(w.x, view[0]), __fmul_rn(w.y, view[4])), __fmul_rn(w.z, view[8])), view[12]);
+    v[k].y = __fadd_rn(__fadd_rn(__fadd_rn(__fmul_rn(w.x, view[1]), __fmul_rn(w.y, view[5])), __fmul_rn(w.z, view[9])), view[13]);
+    v[k].z = __fadd_rn(__fadd_rn(__fadd_rn(__fmul_rn(w.x, view[2]), __fmul_rn(w.y, view[6])), __fmul_rn(w.z, view[10])), view[14]);
+    const V3 m = v3(q[k * 3], q[k * 3 + 1], q[k * 3 + 2]);
+    // normals: [n 0] * inverse-transpose(M); M is rigid here, so its 3x3 block
+    V3 r;
+    r.x = __fadd_rn(__fadd_rn(__fmul_rn(m.x, view[0]), __fmul_rn(m.y, view[4])), __fmul_rn(m.z, view[8]));
+    r.y = __fadd_rn(__fadd_rn(__fmul_rn(m.x, view[1]), __fmul_rn(m.y, view[5])), __fmul_rn(m.z, view[9]));
+    r.z = __fadd_rn(__fadd_rn(__fmul_rn(m.x, view[2]), __fmul_rn(m.y, view[6])), __fmul_rn(m.z, view[10]));
+    const float l = __fsqrt_rn(dot_rn(r, r));
+    nn[k] = l > 0.0f ? v3(__fdiv_rn(r.x, l), __fdiv_rn(r.y, l), __fdiv_rn(r.z, l)) : r;
+  }
+  const V3 e1 = sub_rn(v[1], v[0]), e2 = sub_rn(v[2], v[0]);
+  const V3 pd = cross_rn(sub_rn(v[1], v[0]), sub_rn(v[2], v[1]));
+  const float pl = __fsqrt_rn(dot_rn(pd, pd));
+  const V3 gn = pl > 0.0f ? v3(__fdiv_rn(pd.x, pl), __fdiv_rn(pd.y, pl), __fdiv_rn(pd.z, pl)) : pd;
+  const int mesh = triMesh[i];
+  const DevMaterial mt = mats[objMat[meshObj[mesh]]];
+  uint32_t occ = kOccAll;
+  if (mt.transparency < 0.01f && mt.emission <= 0.0f) occ |= kOccArea;
+  if (mt.emission <= 0.0f && (mt.transparency < 0.01f || mt.refraction > 0.1f)) occ |= kOccPoint;
+  if (mt.transparency < 0.01f) occ |= kOccAO;
+  verts[(size_t)i * 3 + 0] = make_float4(v[0].x, v[0].y, v[0].z, __int_as_float(mesh));
+  verts[(size_t)i * 3 + 1] = make_float4(e1.x, e1.y, e1.z, __uint_as_float(occ));
+  verts[(size_t)i * 3 + 2] = make_float4(e2.x, e2.y, e2.z, 0.0f);
+  shade[(size_t)i * 3 + 0] = make_float4(nn[0].x, nn[0].y, nn[0].z, nn[1].x);
+  shade[(size_t)i * 3 + 1] = make_float4(nn[1].y, nn[1].z, nn[2].x, nn[2].y);
+  shade[(size_t)i * 3 + 2] = make_float4(nn[2].z, gn.x, gn.y, gn.z);
+  if (uvOut) {
+    for (int k = 0; k < 3; k++) uvOut[(size_t)i * 3 + k] = uv ? make_float2(uv[(size_t)i * 6 + k * 2], uv[(size_t)i * 6 + k * 2 + 1]) : make_float2(0, 0);
+  }
+  const V3 lo = v3(fminf(v[0].x, fminf(v[1].x, v[2].x)), fminf(v[0].y, fminf(v[1].y, v[2].y)), fminf(v[0].z, fminf(v[1].z, v[2].z)));
+  const V3 hi = v3(fmaxf(v[0].x, fmaxf(v[1].x, v[2].x)), fmaxf(v[0].y, fmaxf(v[1].y, v[2].y)), fmaxf(v[0].z, fmaxf(v[1].z, v[2].z)));
+  bmin[i] = make_float4(lo.x, lo.y, lo.z, 0.0f);
+  bmax[i] = make_float4(hi.x, hi.y, hi.z, 0.0f);
+}
+
+// ---- root bounds -------------------------------------------------------------
+__global__ void k_rootBounds(int n, const float4* __restrict__ bmin, const float4* __restrict__ bmax, uint32_t* out) {
+  // out: bmin[3] bmax[3] cmin[3] cmax[3] (encoded)
+  float lo[3] = {FLT_MAX, FLT_MAX, FLT_MAX}, hi[3] = {-FLT_MAX, -FLT_MAX, -FLT_MAX};
+  float clo[3] = {FLT_MAX, FLT_MAX, FLT_MAX}, chi[3] = {-FLT_MAX, -FLT_MAX, -FLT_MAX};
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const float4 a = bmin[i], b = bmax[i];
+    const float av[3] = {a.x, a.y, a.z}, bv[3] = {b.x, b.y, b.z};
+    for (int k = 0; k < 3; k++) {
+      lo[k] = fminf(lo[k], av[k]);
+      hi[k] = fmaxf(hi[k], bv[k]);
+      const float c = (av[k] + bv[k]) * 0.5f;
+      clo[k] = fminf(clo[k], c);
+      chi[k] = fmaxf(chi[k], c);
+    }
+  }
+  for (int k = 0; k < 3; k++) {
+    for (int o = 16; o > 0; o >>= 1) {
+      lo[k] = fminf(lo[k], __shfl_xor_sync(0xffffffffu, lo[k], o));
+      hi[k] = fmaxf(hi[k], __shfl_xor_sync(0xffffffffu, hi[k], o));
+      clo[k] = fminf(clo[k], __shfl_xor_sync(0xffffffffu, clo[k], o));
+      chi[k] = fmaxf(chi[k], __shfl_xor_sync(0xffffffffu, chi[k], o));
+    }
+  }
+  if ((threadIdx.x & 31) == 0) {
+    for (int k = 0; k < 3; k++) {
+      atomicMin(&out[k], fenc(lo[k]));
+      atomicMax(&out[3 + k], fenc(hi[k]));
+      atomicMin(&out[6 + k], fenc(clo[k]));
+      atomicMax(&out[9 + k], fenc(chi[k]));
+    }
+  }
+}
+
+__global__ void k_initRoot(int n, const uint32_t* rb, BNode* nodes, int* primIdx, int* primNode, int rootOpen) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i == 0) {
+    BNode r;
+    for (int k = 0; k < 3; k++) {
+      r.bmin[k] = fdec(rb[k]); r.bmax[k] = fdec(rb[3 + k]);
+      r.cmin[k] = fdec(rb[6 + k]); r.cmax[k] = fdec(rb[9 + k]);
+    }
+    r.start = 0; r.count = n; r.left = -1; r.axis = 0; r.binSlot = 0; r.splitBin = -1;
+    r.fill[0] = r.fill[1] = 0;
+    nodes[0] = r;
+  }
+  if (i < n) {
+    primIdx[i] = i;
+    primNode[i] = rootOpen ? 0 : -1;
+  }
+}
+
+// Prepare open nodes of a level: pick the widest centroid axis (bvh.cpp:125-131).
+__global__ void k_prepareLevel(int numTasks, const int* tasks, BNode* nodes, BinData* bins, int nbins) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t < numTasks) {
+    BNode& nd = nodes[tasks[t]];
+    const float ex = nd.cmax[0] - nd.cmin[0], ey = nd.cmax[1] - nd.cmin[1], ez = nd.cmax[2] - nd.cmin[2];
+    int axis = 0;
+    if (ey > ex) axis = 1;
+    if (ez > ((axis == 0) ? ex : ey)) axis = 2;
+    nd.axis = axis;
+    nd.binSlot = t;
+  }
+  // reset bins (one thread per bin)
+  const int b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b < numTasks * nbins) {
+    BinData z;
+    for (int k = 0; k < 3; k++) {
+      z.bmin[k] = 0xFFFFFFFFu; z.bmax[k] = 0u; z.cmin[k] = 0xFFFFFFFFu; z.cmax[k] = 0u;
+    }
+    z.count = 0; z.pad[0] = z.pad[1] = z.pad[2] = 0;
+    bins[b] = z;
+  }
+}
+
+__device__ __forceinline__ int binOf(const BNode& nd, float c, int nbins) {
+  const float cmin = nd.cmin[nd.axis];
+  const float ext = nd.cmax[nd.axis] - cmin;
+  const float scale = (float)nbins / ext;
+  int b = (int)((c - cmin) * scale);
+  if (b < 0) b = 0;
+  if (b >= nbins) b = nbins - 1;
+  return b;
+}
+
+__device__ __forceinline__ float axisOf(const float4& v, int a) { return a == 0 ? v.x : (a == 1 ? v.y : v.z); }
+
+constexpr int kBinChunk = 4096;
+constexpr int kMaxBins = 64;
+
+__global__ void __launch_bounds__(256) k_bin(int n, const int* __restrict__ primIdx, const int* __restrict__ primNode,
+                                             const BNode* __restrict__ nodes, const float4* __restrict__ bmin,
+                                             const float4* __restrict__ bmax, BinData* bins, int nbins) {
+  __shared__ uint32_t sb[kMaxBins][13];
+  const int first = blockIdx.x * kBinChunk;
+  if (first >= n) return;
+  const int last = min(n, first + kBinChunk) - 1;
+  const int nodeA = primNode[first], nodeB = primNode[last];
+  const bool uniform = (nodeA == nodeB) && nodeA >= 0;
+  if (uniform) {
+    for (int b = threadIdx.x; b < nbins; b += blockDim.x) {
+      for (int k = 0; k < 3; k++) {
+        sb[b][k] = 0xFFFFFFFFu; sb[b][3 + k] = 0u; sb[b][6 + k] = 0xFFFFFFFFu; sb[b][9 + k] = 0u;
+      }
+      sb[b][12] = 0;
+    }
+    __syncthreads();
+    const BNode nd = nodes[nodeA];
+    if (nd.binSlot < 0) return;
+    const float ext = nd.cmax[nd.axis] - nd.cmin[nd.axis];
+    if (ext >= 1e-12f) {
+      for (int i = first + threadIdx.x; i <= last; i += blockDim.x) {
+        const int p = primIdx[i];
+        const float4 lo = bmin[p], hi = bmax[p];
+        const float4 c = make_float4((lo.x + hi.x) * 0.5f, (lo.y + hi.y) * 0.5f, (lo.z + hi.z) * 0.5f, 0.0f);
+        const int b = binOf(nd, axisOf(c, nd.axis), nbins);
+        atomicMin(&sb[b][0], fenc(lo.x)); atomicMin(&sb[b][1], fenc(lo.y)); atomicMin(&sb[b][2], fenc(lo.z));
+        atomicMax(&sb[b][3], fenc(hi.x)); atomicMax(&sb[b][4], fenc(hi.y)); atomicMax(&sb[b][5], fenc(hi.z));
+        atomicMin(&sb[b][6], fenc(c.x)); atomicMin(&sb[b][7], fenc(c.y)); atomicMin(&sb[b][8], fenc(c.z));
+        atomicMax(&sb[b][9], fenc(c.x)); atomicMax(&sb[b][10], fenc(c.y)); atomicMax(&sb[b][11], fenc(c.z));
+        atomicAdd(&sb[b][12], 1u);
+      }
+    }
+    __syncthreads();
+    BinData* nb = bins + (size_t)nd.binSlot * nbins;
+    for (int b = threadIdx.x; b < nbins; b += blockDim.x) {
+      if (sb[b][12] == 0) continue;
+      for (int k = 0; k < 3; k++) {
+        atomicMin(&nb[b].bmin[k], sb[b][k]);
+        atomicMax(&nb[b].bmax[k], sb[b][3 + k]);
+        atomicMin(&nb[b].cmin[k], sb[b][6 + k]);
+        atomicMax(&nb[b].cmax[k], sb[b][9 + k]);
+      }
+      atomicAdd(&nb[b].count, sb[b][12]);
+    }
+    return;
+  }
+  for (int i = first + threadIdx.x; i <= last; i += blockDim.x) {
+    const int node = primNode[i];
+    if (node < 0) continue;
+    const BNode& nd = nodes[node];
+    if (nd.binSlot < 0) continue;
+    const float ext = nd.cmax[nd.axis] - nd.cmin[nd.axis];
+    if (ext < 1e-12f) continue;
+    const int p = primIdx[i];
+    const float4 lo = bmin[p], hi = bmax[p];
+    const float4 c = make_float4((lo.x + hi.x) * 0.5f, (lo.y + hi.y) * 0.5f, (lo.z + hi.z) * 0.5f, 0.0f);
+    const int b = binOf(nd, axisOf(c, nd.axis), nbins);
+    BinData& bd = bins[(size_t)nd.binSlot * nbins + b];
+    atomicMin(&bd.bmin[0], fenc(lo.x)); atomicMin(&bd.bmin[1], fenc(lo.y)); atomicMin(&bd.bmin[2], fenc(lo.z));
+    atomicMax(&bd.bmax[0], fenc(hi.x)); atomicMax(&bd.bmax[1], fenc(hi.y)); atomicMax(&bd.bmax[2], fenc(hi.z));
+    atomicMin(&bd.cmin[0], fenc(c.x)); atomicMin(&bd.cmin[1], fenc(c.y)); atomicMin(&bd.cmin[2], fenc(c.z));
+    atomicMax(&bd.cmax[0], fenc(c.x)); atomicMax(&bd.cmax[1], fenc(c.y)); atomicMax(&bd.cmax[2], fenc(c.z));
+    atomicAdd(&bd.count, 1u);
+  }
+}
+
+__device__ __forceinline__ float areaOf(const float lo[3], const float hi[3]) {
+  const float dx = hi[0] - lo[0], dy = hi[1] - lo[1], dz = hi[2] - lo[2];
+  return 2.0f * (dx * dy + dy * dz + dz * dx);
+}
+
+// Split decision per open node (bvh.cpp:133-211 cost model).
+__global__ void k_split(int numTasks, const int* __restrict__ tasks, BNode* nodes, const BinData* __restrict__ bins,
+                        int nbins, int* nodeCounter, int* nextTasks, int* nextCount) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= numTasks) return;
+  const int id = tasks[t];
+  BNode nd = nodes[id];
+  const BinData* nb = bins + (size_t)nd.binSlot * nbins;
+  const float ext = nd.cmax[nd.axis] - nd.cmin[nd.axis];
+  int best = -1;
+  float bestCost = (float)nd.count * 1.5f;
+  float forcedCost = FLT_MAX;
+  int forced = -1;
+  // sweeps
+  float la[kMaxBins];
+  int lc[kMaxBins];
+  if (ext >= 1e-12f) {
+    float lo[3] = {FLT_MAX, FLT_MAX, FLT_MAX}, hi[3] = {-FLT_MAX, -FLT_MAX, -FLT_MAX};
+    int c = 0;
+    for (int i = 0; i < nbins - 1; i++) {
+      if (nb[i].count > 0) {
+        for (int k = 0; k < 3; k++) { lo[k] = fminf(lo[k], fdec(nb[i].bmin[k])); hi[k] = fmaxf(hi[k], fdec(nb[i].bmax[k])); }
+      }
+      c += nb[i].count;
+      la[i] = c > 0 ? areaOf(lo, hi) : 0.0f;
+      lc[i] = c;
+    }
+    const float pa = areaOf(nd.bmin, nd.bmax);
+    const float invPa = pa > 0.0f ? 1.0f / pa : 0.0f;
+    float rlo[3] = {FLT_MAX, FLT_MAX, FLT_MAX}, rhi[3] = {-FLT_MAX, -FLT_MAX, -FLT_MAX};
+    int rc = 0;
+    for (int i = nbins - 1; i > 0; i--) {
+      if (nb[i].count > 0) {
+        for (int k = 0; k < 3; k++) { rlo[k] = fminf(rlo[k], fdec(nb[i].bmin[k])); rhi[k] = fmaxf(rhi[k], fdec(nb[i].bmax[k])); }
+      }
+      rc += nb[i].count;
+      const float ra = rc > 0 ? areaOf(rlo, rhi) : 0.0f;
+      const int s = i - 1;
+      if (lc[s] == 0 || rc == 0) continue;
+      const float cost = 1.0f + 1.5f * invPa * (la[s] * (float)lc[s] + ra * (float)rc);
+      if (cost < bestCost || (cost == bestCost && best >= 0 && s < best)) { bestCost = cost; best = s; }
+      if (cost < forcedCost || (cost == forcedCost && s < forced)) { forcedCost = cost; forced = s; }
+    }
+  }
+  int split = best;
+  if (split < 0 && nd.count > kMaxLeaf) split = forced >= 0 ? forced : -2;  // -2: index median
+  nd.binSlot = -1;
+  if (split == -1) {
+    nd.left = -1;
+    nodes[id] = nd;
+    return;
+  }
+  const int left = atomicAdd(nodeCounter, 2);
+  BNode ch[2];
+  int cnt[2];
+  if (split == -2) {
+    cnt[0] = nd.count / 2;
+    cnt[1] = nd.count - cnt[0];
+    for (int s = 0; s < 2; s++) {
+      for (int k = 0; k < 3; k++) {
+        ch[s].bmin[k] = nd.bmin[k]; ch[s].bmax[k] = nd.bmax[k];
+        ch[s].cmin[k] = nd.cmin[k]; ch[s].cmax[k] = nd.cmax[k];
+      }
+    }
+  } else {
+    for (int s = 0; s < 2; s++) {
+      float lo[3] = {FLT_MAX, FLT_MAX, FLT_MAX}, hi[3] = {-FLT_MAX, -FLT_MAX, -FLT_MAX};
+      float clo[3] = {FLT_MAX, FLT_MAX, FLT_MAX}, chi[3] = {-FLT_MAX, -FLT_MAX, -FLT_MAX};
+      int c = 0;
+      const int b0 = s == 0 ? 0 : split + 1, b1 = s == 0 ? split + 1 : nbins;
+      for (int b = b0; b < b1; b++) {
+        if (nb[b].count == 0) continue;
+        c += nb[b].count;
+        for (int k = 0; k < 3; k++) {
+          lo[k] = fminf(lo[k], fdec(nb[b].bmin[k])); hi[k] = fmaxf(hi[k], fdec(nb[b].bmax[k]));
+          clo[k] = fminf(clo[k], fdec(nb[b].cmin[k])); chi[k] = fmaxf(chi[k], fdec(nb[b].cmax[k]));
+        }
+      }
+      cnt[s] = c;
+      for (int k = 0; k < 3; k++) { ch[s].bmin[k] = lo[k]; ch[s].bmax[k] = hi[k]; ch[s].cmin[k] = clo[k]; ch[s].cmax[k] = chi[k]; }
+    }
+  }
+  for (int s = 0; s < 2; s++) {
+    ch[s].start = nd.start + (s == 0 ? 0 : cnt[0]);
+    ch[s].count = cnt[s];
+    ch[s].left = -1;
+    ch[s].axis = 0;
+    ch[s].binSlot = -1;
+    ch[s].splitBin = -1;
+    ch[s].fill[0] = ch[s].fill[1] = 0;
+    nodes[left + s] = ch[s];
+    if (cnt[s] > 4) {  // BVH_LEAF_SIZE (bvh.cpp:23): larger children stay open
+      const int slot = atomicAdd(nextCount, 1);
+      nextTasks[slot] = left + s;
+    }
+  }
+  nd.left = left;
+  nd.splitBin = split;
+  nd.fill[0] = nd.fill[1] = 0;
+  nodes[id] = nd;
+}
+
+// Scatter the primitives of split nodes to their children (warp-aggregated).
+__global__ void k_partition(int n, const int* __restrict__ primIdx, const int* __restrict__ primNode,
+                            BNode* nodes, const float4* __restrict__ bmin, const float4* __restrict__ bmax,
+                            int* __restrict__ outIdx, int* __restrict__ outNode, int nbins) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const bool inRange = i < n;
+  const int node = inRange ? primNode[i] : -1;
+  const int p = inRange ? primIdx[i] : 0;
+  int side = -1, child = -1;
+  if (node >= 0) {
+    const BNode& nd = nodes[node];
+    if (nd.left >= 0) {
+      if (nd.splitBin == -2) {
+        side = (i - nd.start) < nd.count / 2 ? 0 : 1;
+      } else {
+        const float4 lo = bmin[p], hi = bmax[p];
+        const float c = nd.axis == 0 ? (lo.x + hi.x) * 0.5f : (nd.axis == 1 ? (lo.y + hi.y) * 0.5f : (lo.z + hi.z) * 0.5f);
+        side = binOf(nd, c, nbins) <= nd.splitBin ? 0 : 1;
+      }
+      child = nd.left + side;
+    }
+  }
+  // warp-aggregated cursor bump per (child) group
+  const unsigned active = __activemask();
+  const int key = child;
+  const unsigned grp = __match_any_sync(active, key);
+  int pos = -1;
+  if (child >= 0) {
+    const int leader = __ffs(grp) - 1;
+    const int rank = __popc(grp & ((1u << (threadIdx.x & 31)) - 1));
+    int base = 0;
+    if ((int)(threadIdx.x & 31) == leader) base = atomicAdd(&nodes[node].fill[side], __popc(grp));
+    base = __shfl_sync(grp, base, leader);
+    pos = nodes[child].start + base + rank;
+  }
+  if (!inRange) return;
+  if (child >= 0) {
+    outIdx[pos] = p;
+    outNode[pos] = nodes[child].count > 4 ? child : -1;
+  } else {
+    outIdx[i] = p;
+    outNode[i] = -1;
+  }
+}
+
+__global__ void k_innerFlags(int numNodes, const BNode* __restrict__ nodes, int* flags) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < numNodes) flags[i] = nodes[i].left >= 0 ? 1 : 0;
+}
+
+__device__ __forceinline__ float inflateLo(float x) { return x - fmaxf(fabsf(x), 1.0f) * 2e-6f; }
+__device__ __forceinline__ float inflateHi(float x) { return x + fmaxf(fabsf(x), 1.0f) * 2e-6f; }
+
+__global__ void k_emitNodes(int numNodes, const BNode* __restrict__ nodes, const int* __restrict__ travIdx,
+                            float4* __restrict__ out) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= numNodes) return;
+  const BNode nd = nodes[i];
+  if (nd.left < 0) return;
+  const BNode a = nodes[nd.left], b = nodes[nd.left + 1];
+  int refs[2];
+  const BNode* cs[2] = {&a, &b};
+  for (int s = 0; s < 2; s++) {
+    const BNode& c = *cs[s];
+    if (c.left >= 0) refs[s] = travIdx[nd.left + s];
+    else refs[s] = ~((c.start << 3) | (c.count - 1));
+  }
+  float4* o = out + (size_t)travIdx[i] * 4;
+  o[0] = make_float4(inflateLo(a.bmin[0]), inflateHi(a.bmax[0]), inflateLo(a.bmin[1]), inflateHi(a.bmax[1]));
+  o[1] = make_float4(inflateLo(b.bmin[0]), inflateHi(b.bmax[0]), inflateLo(b.bmin[1]), inflateHi(b.bmax[1]));
+  o[2] = make_float4(inflateLo(a.bmin[2]), inflateHi(a.bmax[2]), inflateLo(b.bmin[2]), inflateHi(b.bmax[2]));
+  o[3] = make_float4(__int_as_float(refs[0]), __int_as_float(refs[1]), 0.0f, 0.0f);
+}
+
+__global__ void k_gather(int n, const int* __restrict__ primIdx, const float4* __restrict__ vIn,
+                         const float4* __restrict__ sIn, const float2* __restrict__ uvIn, float4* __restrict__ vOut,
+                         float4* __restrict__ sOut, float2* __restrict__ uvOut, int* __restrict__ orig) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const int p = primIdx[i];
+  for (int k = 0; k < 3; k++) {
+    vOut[(size_t)i * 3 + k] = vIn[(size_t)p * 3 + k];
+    sOut[(size_t)i * 3 + k] = sIn[(size_t)p * 3 + k];
+    if (uvOut) uvOut[(size_t)i * 3 + k] = uvIn[(size_t)p * 3 + k];
+  }
+  orig[i] = p;
+}
+
+inline int gridFor(long long n, int block) { return (int)((n + block - 1) / block); }
+
+}  // namespace
+
+// Builds the view-space triangle arrays and the BVH for `n` triangles whose
+// world-space inputs are already on the device (DeviceSceneBuild fields).
+rg_status buildDeviceBvh(DeviceScene& ds, int nbins, cudaStream_t st, std::string& err) {
+  const int n = ds.numTris;
+  nbins = nbins < 2 ? 2 : (nbins > kMaxBins ? kMaxBins : nbins);
+  ds.rootIsLeaf = 0;
+  ds.rootLeafRef = 0;
+  ds.numNodes = 0;
+  if (n == 0) return RG_OK;
+  DevBuf<float4> vTmp, sTmp, lo, hi;
+  DevBuf<float2> uvTmp;
+  if (!vTmp.alloc((size_t)n * 3) || !sTmp.alloc((size_t)n * 3) || !lo.alloc(n) || !hi.alloc(n)) {
+    err = "out of device memory (triangle staging)";
+    return RG_ERR_OUT_OF_MEMORY;
+  }
+  if (ds.hasUV && !uvTmp.alloc((size_t)n * 3)) return RG_ERR_OUT_OF_MEMORY;
+  k_prepTriangles<<<gridFor(n, 256), 256, 0, st>>>(n, ds.inPos.p, ds.inNrm.p, ds.hasUV ? ds.inUV.p : nullptr,
+                                                   ds.inTriMesh.p, ds.meshObj.p, ds.objMat.p, ds.mats.p, ds.view.p,
+                                                   vTmp.p, sTmp.p, ds.hasUV ? uvTmp.p : nullptr, lo.p, hi.p);
+  // root bounds
+  DevBuf<uint32_t> rb;
+  rb.alloc(12);
+  {
+    std::vector<uint32_t> init(12);
+    for (int k = 0; k < 3; k++) { init[k] = 0xFFFFFFFFu; init[3 + k] = 0u; init[6 + k] = 0xFFFFFFFFu; init[9 + k] = 0u; }
+    cudaMemcpyAsync(rb.p, init.data(), 12 * sizeof(uint32_t), cudaMemcpyHostToDevice, st);
+  }
+  k_rootBounds<<<std::min(gridFor(n, 256), 1184), 256, 0, st>>>(n, lo.p, hi.p, rb.p);
+  const size_t maxNodes = 2 * (size_t)n + 1;
+  // bins for at most chunkTasks open nodes at a time (<= 256 MB)
+  const int chunkTasks = (int)std::min<size_t>((size_t)n / 4 + 2, ((size_t)256 << 20) / (sizeof(BinData) * nbins));
+  DevBuf<BNode> nodes;
+  DevBuf<int> idxA, idxB, nodeA, nodeB, tasksA, tasksB, counters;
+  DevBuf<BinData> bins;
+  if (!nodes.alloc(maxNodes) || !idxA.alloc(n) || !idxB.alloc(n) || !nodeA.alloc(n) || !nodeB.alloc(n) ||
+      !tasksA.alloc((size_t)n / 4 + 2) || !tasksB.alloc((size_t)n / 4 + 2) || !counters.alloc(4) ||
+      !bins.alloc((size_t)chunkTasks * nbins)) {
+    err = "out of device memory (BVH build)";
+    return RG_ERR_OUT_OF_MEMORY;
+  }
+  const int rootOpen = n > 4 ? 1 : 0;
+  k_initRoot<<<gridFor(n, 256), 256, 0, st>>>(n, rb.p, nodes.p, idxA.p, nodeA.p, rootOpen);
+  int h_counters[4] = {1, 0, 0, 0};  // [0] node count, [1] next task count
+  cudaMemcpyAsync(counters.p, h_counters, sizeof(h_counters), cudaMemcpyHostToDevice, st);
+  int numTasks = rootOpen;
+  {
+    const int zero = 0;
+    cudaMemcpyAsync(tasksA.p, &zero, sizeof(int), cudaMemcpyHostToDevice, st);
+  }
+  int* curIdx = idxA.p;
+  int* curNode = nodeA.p;
+  int* altIdx = idxB.p;
+  int* altNode = nodeB.p;
+  int* curTasks = tasksA.p;
+  int* nxtTasks = tasksB.p;
+  int levels = 0;
+  while (numTasks > 0) {
+    levels++;
+    cudaMemsetAsync(counters.p + 1, 0, sizeof(int), st);
+    for (int c0 = 0; c0 < numTasks; c0 += chunkTasks) {
+      const int nt = std::min(chunkTasks, numTasks - c0);
+      const int prepN = std::max(nt, nt * nbins);
+      k_prepareLevel<<<gridFor(prepN, 256), 256, 0, st>>>(nt, curTasks + c0, nodes.p, bins.p, nbins);
+      k_bin<<<gridFor(n, kBinChunk), 256, 0, st>>>(n, curIdx, curNode, nodes.p, lo.p, hi.p, bins.p, nbins);
+      k_split<<<gridFor(nt, 128), 128, 0, st>>>(nt, curTasks + c0, nodes.p, bins.p, nbins, counters.p, nxtTasks,
+                                                 counters.p + 1);
+    }
+    k_partition<<<gridFor(n, 256), 256, 0, st>>>(n, curIdx, curNode, nodes.p, lo.p, hi.p, altIdx, altNode, nbins);
+    std::swap(curIdx, altIdx);
+    std::swap(curNode, altNode);
+    std::swap(curTasks, nxtTasks);
+    cudaMemcpyAsync(&numTasks, counters.p + 1, sizeof(int), cudaMemcpyDeviceToHost, st);
+    if (cudaStreamSynchronize(st) != cudaSuccess) {
+      err = "BVH build level failed";
+      return RG_ERR_CUDA;
+    }
+    if (levels > 200) {
+      err = "BVH build did not converge";
+      return RG_ERR_DEVICE_STATUS;
+    }
+  }
+  int numNodes = 0;
+  cudaMemcpyAsync(&numNodes, counters.p, sizeof(int), cudaMemcpyDeviceToHost, st);
+  cudaStreamSynchronize(st);
+  ds.buildLevels = levels;
+  // traversal layout
+  DevBuf<int> flags, trav;
+  flags.alloc(numNodes);
+  trav.alloc(numNodes);
+  k_innerFlags<<<gridFor(numNodes, 256), 256, 0, st>>>(numNodes, nodes.p, flags.p);
+  size_t tmpBytes = 0;
+  cub::DeviceScan::ExclusiveSum(nullptr, tmpBytes, flags.p, trav.p, numNodes, st);
+  DevBuf<unsigned char> tmp;
+  tmp.alloc(tmpBytes + 16);
+  cub::DeviceScan::ExclusiveSum(tmp.p, tmpBytes, flags.p, trav.p, numNodes, st);
+  int lastFlag = 0, lastTrav = 0;
+  cudaMemcpyAsync(&lastFlag, flags.p + numNodes - 1, sizeof(int), cudaMemcpyDeviceToHost, st);
+  cudaMemcpyAsync(&lastTrav, trav.p + numNodes - 1, sizeof(int), cudaMemcpyDeviceToHost, st);
+  cudaStreamSynchronize(st);
+  const int numInner = lastFlag + lastTrav;
+  ds.numNodes = numInner;
+  if (numInner == 0) {
+    ds.rootIsLeaf = 1;
+    ds.rootLeafRef = ~((0 << 3) | (n - 1));
+    ds.nodes.alloc(4);
+  } else {
+    if (!ds.nodes.alloc((size_t)numInner * 4)) {
+      err = "out of device memory (BVH nodes)";
+      return RG_ERR_OUT_OF_MEMORY;
+    }
+    k_emitNodes<<<gridFor(numNodes, 256), 256, 0, st>>>(numNodes, nodes.p, trav.p, ds.nodes.p);
+  }
+  if (!ds.triVerts.alloc((size_t)n * 3) || !ds.triShade.alloc((size_t)n * 3) || !ds.triOrig.alloc(n)) {
+    err = "out of device memory (triangles)";
+    return RG_ERR_OUT_OF_MEMORY;
+  }
+  if (ds.hasUV) ds.triUV.alloc((size_t)n * 3);
+  k_gather<<<gridFor(n, 256), 256, 0, st>>>(n, curIdx, vTmp.p, sTmp.p, ds.hasUV ? uvTmp.p : nullptr, ds.triVerts.p,
+                                            ds.triShade.p, ds.hasUV ? ds.triUV.p : nullptr, ds.triOrig.p);
+  if (cudaStreamSynchronize(st) != cudaSuccess) {
+    err = std::string("BVH build failed: ") + cudaGetErrorString(cudaGetLastError());
+    return RG_ERR_CUDA;
+  }
+  return RG_OK;
+}
+
+}  // namespace rg

@@ -1,0 +1,282 @@
+// rg_device.cuh - device data layout, vector math and the counter-based RNG
+// of the B200 wavefront tracer.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace rg {
+
+// ------------------------------------------------------------ constants ----
+constexpr float kPi = 3.14159265358979323846f;
+constexpr float kSurfaceThickness = 0.0001f;  // SURFACE_THICKNESS, raycommon.h:21
+constexpr float kMaxRayDistance = 1.0e6f;     // MAX_RAY_DISTANCE, raycommon.h:34
+constexpr float kRayMaxDistance = 100.0f;     // RAY_MAX_DISTANCE, rayrenderer.h:48
+constexpr float kRRMin = 0.05f, kRRMax = 0.95f;  // rayrenderer.cpp:44-45
+constexpr int kMaxLeaf = 8;                   // triangles per leaf in the device BVH
+constexpr int kStackSize = 64;
+
+// occluder classes (bit per shadow-ray predicate)
+constexpr uint32_t kOccArea = 1u;   // transparency < 0.01 && emission <= 0   (rayrenderer.cpp:1956-1959)
+constexpr uint32_t kOccPoint = 2u;  // emission <= 0 && (transparency < 0.01 || refraction > 0.1) (:2211-2215)
+constexpr uint32_t kOccAO = 4u;     // transparency < 0.01                    (:2388-2390)
+constexpr uint32_t kOccAll = 8u;
+
+// -------------------------------------------------------------- structs ----
+struct DevMaterial {
+  float cr, cg, cb;
+  float glossy, roughness, transparency, refraction, ior;
+  float chroma, metallic, aniso, anisoRot;
+  float emission, spotRange;
+  int texture;
+  float tileU, tileV;
+  float pad;
+};
+
+struct DevMedium {
+  float ssr, ssg, ssb;   // sigma_s * density
+  float ser, seg, seb;   // sigma_e * density
+  float str, stg, stb;   // sigma_t
+  float hero, g, pad;
+};
+
+struct DevPointLight {
+  float px, py, pz;      // view space
+  float nx, ny, nz;
+  int material;
+  int pad;
+};
+
+struct DevTexture {
+  const float4* texels;
+  int width, height, isHdr, pad;
+};
+
+// Everything the kernels read about the scene.  Triangle arrays are in BVH
+// leaf order; `triOrig` maps back to the DFS triangle id.
+struct DevScene {
+  const float4* nodes;        // 4 float4 per BVH2 node (two child boxes + refs)
+  int numNodes;
+  int rootIsLeaf;             // whole scene in one leaf: rootLeafRef holds it
+  int rootLeafRef;
+  const float4* triVerts;     // 3 float4 per triangle: (v1, mesh bits) (e1, occluder bits) (e2, 0)
+  const float4* triShade;     // 3 float4: (n1.xyz, n2.x) (n2.yz, n3.xy) (n3.z, gn.xyz)
+  const float2* triUV;        // 3 float2 per triangle (NULL when the scene has no textures)
+  const int* triOrig;
+  int numTris;
+  const int* meshObj;         // mesh -> object
+  const int* meshTriCount;    // mesh -> triangle count (areaLightSampledArea)
+  const int* objMat;          // object -> material
+  const int* objMedium;       // object -> interior medium (-1 none)
+  const DevMaterial* mats;
+  const DevMedium* media;
+  int globalMedium;
+  int numAreaLights;
+  const int* areaLightObj;    // area light -> object
+  const int2* lightObjMeshes; // object -> (first, count) in lightMeshList (light objects only)
+  const int* lightMeshList;   // flattened mesh ids
+  const int2* lightMeshTris;  // mesh -> (first, count) in lightTris (light meshes only)
+  const float4* lightTris;    // 6 float4 per emitter triangle: (v1,ti.a) (v2,area) (v3,0) (n1,0) (n2,0) (n3,0)
+  int numPointLights;
+  const DevPointLight* points;
+  const DevTexture* textures;
+  int numTextures;
+};
+
+// Render-wide constants for the trace kernels.
+struct DevRender {
+  int width, height;
+  float viewScale;            // 2 tan(fov/2) / H
+  float halfW, halfH;
+  float dof, aperture;        // aperture = 1/camera.aperture (0 when disabled)
+  int blades;
+  float apertureRot;          // radians
+  float exposure;
+  float viewFar;
+  int aa;
+  int colorSampling;
+  int shader;
+  int maxDepth, rrDepth;
+  int lightFix;
+  uint32_t seed;
+  float clampMax;
+  float backR, backG, backB;
+  float worldR, worldG, worldB;
+  int aoSamples;              // settings.samples (calcAO loop count)
+};
+
+// One wave: paths p = s_local * numPixels + i, pixel = pixelList ? pixelList[i] : i.
+struct DevWave {
+  int numPixels;
+  int samplesInWave;
+  int sampleBase;
+  int pixelOffset;            // first entry of this wave in pixelList (or first pixel)
+  const int* pixelList;       // NULL: identity
+  const int* pixelSampleBase; // per pixel: first sample index (NULL: sampleBase)
+};
+
+// Wavefront buffers.
+struct DevQueues {
+  float4* rayO[2];            // (origin, path id bits)
+  float4* rayD[2];            // (dir, 0)
+  float4* hits;               // (t, u, v, prim bits) per queue slot
+  float4* pathT;              // (beta rgb, bsdfPdf)
+  float4* pathR;              // (rrT rgb, flags bits)
+  float4* pathL;              // (L rgb, vertex bits)
+  float4* shO[2];             // shadow queues A (area) / B (point): (origin, path id bits)
+  float4* shD[2];             // (dir, tmax)
+  float4* shC[2];             // (contribution rgb, predicate bits)
+  int* counters;              // per-iteration counters, zeroed by the generate kernel
+  unsigned long long* stats;  // [0] nodes closest [1] tris closest [2] nodes shadow [3] tris shadow [4] closest rays [5] shadow rays
+  int* error;                 // first device error code
+  int capacity;
+  int maxIter;
+};
+
+// counters layout: [k*8 + c] for iteration k
+enum CounterSlot { C_RAYS = 0, C_FETCH_EXT = 1, C_SHA = 2, C_SHB = 3, C_FETCH_SHA = 4, C_FETCH_SHB = 5, C_FETCH_SHADE = 6 };
+constexpr int kCountersPerIter = 8;
+
+// path flags (pathR.w)
+constexpr uint32_t F_PASSES_MASK = 0xFFu;
+constexpr uint32_t F_CHROMA_SHIFT = 8;       // 0 = none, 1..3 = channel+1
+constexpr uint32_t F_CHROMA_MASK = 0x300u;
+constexpr uint32_t F_MED_SHIFT = 12;         // medium + 1 (0 = none), 10 bits
+constexpr uint32_t F_MED_MASK = 0x3FF000u;
+constexpr uint32_t F_EYE = 1u << 24;         // next event is the eye vertex
+constexpr uint32_t F_EYE_NOHIT = 1u << 25;   // eye ray hit no triangle
+
+// ------------------------------------------------------------------ math ----
+struct V3 {
+  float x, y, z;
+};
+__host__ __device__ __forceinline__ V3 v3(float x, float y, float z) { return V3{x, y, z}; }
+__host__ __device__ __forceinline__ V3 operator+(V3 a, V3 b) { return v3(a.x + b.x, a.y + b.y, a.z + b.z); }
+__host__ __device__ __forceinline__ V3 operator-(V3 a, V3 b) { return v3(a.x - b.x, a.y - b.y, a.z - b.z); }
+__host__ __device__ __forceinline__ V3 operator-(V3 a) { return v3(-a.x, -a.y, -a.z); }
+__host__ __device__ __forceinline__ V3 operator*(V3 a, float s) { return v3(a.x * s, a.y * s, a.z * s); }
+__host__ __device__ __forceinline__ V3 operator*(V3 a, V3 b) { return v3(a.x * b.x, a.y * b.y, a.z * b.z); }
+__host__ __device__ __forceinline__ float dot(V3 a, V3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+__host__ __device__ __forceinline__ V3 cross(V3 a, V3 b) {
+  return v3(a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x);
+}
+__host__ __device__ __forceinline__ float maxc(V3 a) { return fmaxf(a.x, fmaxf(a.y, a.z)); }
+__device__ __forceinline__ V3 normalize(V3 a) {
+  const float l = sqrtf(dot(a, a));
+  return l > 0.0f ? v3(a.x / l, a.y / l, a.z / l) : a;
+}
+__device__ __forceinline__ V3 reflect(V3 d, V3 n) { return d - n * (dot(d, n) * 2.0f); }
+__device__ __forceinline__ V3 xyz(float4 f) { return v3(f.x, f.y, f.z); }
+
+// Non-contracted (round-to-nearest, no FMA) forms used where device results
+// must match the CPU oracle bit for bit (triangle tests, scene transform).
+__device__ __forceinline__ V3 sub_rn(V3 a, V3 b) { return v3(__fsub_rn(a.x, b.x), __fsub_rn(a.y, b.y), __fsub_rn(a.z, b.z)); }
+__device__ __forceinline__ float dot_rn(V3 a, V3 b) {
+  return __fadd_rn(__fadd_rn(__fmul_rn(a.x, b.x), __fmul_rn(a.y, b.y)), __fmul_rn(a.z, b.z));
+}
+__device__ __forceinline__ V3 cross_rn(V3 a, V3 b) {
+  return v3(__fsub_rn(__fmul_rn(a.y, b.z), __fmul_rn(a.z, b.y)), __fsub_rn(__fmul_rn(a.z, b.x), __fmul_rn(a.x, b.z)),
+            __fsub_rn(__fmul_rn(a.x, b.y), __fmul_rn(a.y, b.x)));
+}
+
+// ------------------------------------------------------------------- RNG ----
+// Shared specification with the CPU oracle:
+//   lds(dim)        dims < 16: Halton (radicalInverse(sample+1, prime[dim]),
+//                   raycommon.cpp:48-61) + Cranley-Patterson offset
+//                   hashPixel(dim, 0, hashPixel(x, y, seed-1)) (raycommon.cpp:71-87);
+//                   dims >= 16: prng(vertex = dim, slot 63)
+//   prng(v, slot)   pcg4d(pixel, sample, v<<6 | slot, seed).x >> 8, * 2^-24
+__host__ __device__ __forceinline__ uint32_t hashPixel(uint32_t x, uint32_t y, uint32_t salt) {
+  uint32_t v = x * 73856093u ^ y * 19349663u ^ salt * 83492791u;
+  v ^= v >> 16; v *= 0x7feb352du;
+  v ^= v >> 15; v *= 0x846ca68bu;
+  v ^= v >> 16;
+  return v;
+}
+__host__ __device__ __forceinline__ uint32_t pcg4d_x(uint32_t a, uint32_t b, uint32_t c, uint32_t d) {
+  uint32_t v0 = a * 1664525u + 1013904223u, v1 = b * 1664525u + 1013904223u;
+  uint32_t v2 = c * 1664525u + 1013904223u, v3_ = d * 1664525u + 1013904223u;
+  v0 += v1 * v3_; v1 += v2 * v0; v2 += v0 * v1; v3_ += v1 * v2;
+  v0 ^= v0 >> 16; v1 ^= v1 >> 16; v2 ^= v2 >> 16; v3_ ^= v3_ >> 16;
+  v0 += v1 * v3_; v1 += v2 * v0; v2 += v0 * v1; v3_ += v1 * v2;
+  return v0;
+}
+
+template <int BASE>
+__device__ __forceinline__ float radicalInverseT(uint32_t i) {
+  const float invBase = 1.0f / (float)BASE;
+  float invBaseN = 1.0f;
+  uint64_t rev = 0;
+  while (i > 0) {
+    const uint32_t next = i / BASE;
+    const uint32_t digit = i - next * BASE;
+    rev = rev * BASE + digit;
+    invBaseN = __fmul_rn(invBaseN, invBase);
+    i = next;
+  }
+  const float v = __fmul_rn((float)rev, invBaseN);
+  return v < 1.0f ? v : 0.9999999f;
+}
+
+__device__ __forceinline__ float radicalInverseDim(uint32_t i, int dim) {
+  switch (dim) {
+    case 0: return radicalInverseT<2>(i);
+    case 1: return radicalInverseT<3>(i);
+    case 2: return radicalInverseT<5>(i);
+    case 3: return radicalInverseT<7>(i);
+    case 4: return radicalInverseT<11>(i);
+    case 5: return radicalInverseT<13>(i);
+    case 6: return radicalInverseT<17>(i);
+    case 7: return radicalInverseT<19>(i);
+    case 8: return radicalInverseT<23>(i);
+    case 9: return radicalInverseT<29>(i);
+    case 10: return radicalInverseT<31>(i);
+    case 11: return radicalInverseT<37>(i);
+    case 12: return radicalInverseT<41>(i);
+    case 13: return radicalInverseT<43>(i);
+    case 14: return radicalInverseT<47>(i);
+    default: return radicalInverseT<53>(i);
+  }
+}
+
+enum Slot {
+  S_LOBE = 0, S_LIGHT = 1, S_MESH = 2, S_TRI = 3, S_VNDF0 = 4, S_VNDF1 = 5, S_RR = 6,
+  S_FRESNEL = 7, S_CHROMA = 8, S_HEMI0 = 9, S_HEMI1 = 10, S_POINT = 11, S_ENV0 = 12,
+  S_ENV1 = 13, S_FLIGHT = 14, S_PHASE0 = 15, S_PHASE1 = 16, S_MEDRR = 17, S_EYETR = 18,
+  S_LDS = 63
+};
+
+struct Rng {
+  uint32_t pixel, sample, seed, scramble;
+  int dimBase;
+  __device__ __forceinline__ void init(uint32_t x, uint32_t y, uint32_t width, uint32_t s, uint32_t sd, int base) {
+    pixel = y * width + x;
+    sample = s;
+    seed = sd;
+    scramble = hashPixel(x, y, sd - 1u);
+    dimBase = base;
+  }
+  __device__ __forceinline__ float prng(int v, int slot) const {
+    const uint32_t h = pcg4d_x(pixel, sample, ((uint32_t)v << 6) | (uint32_t)slot, seed);
+    return (float)(h >> 8) * (1.0f / 16777216.0f);
+  }
+  __device__ __forceinline__ float lds(int dim) const {
+    if (dim >= 16) return prng(dim, S_LDS);
+    const float v = radicalInverseDim(sample + 1u, dim);
+    const uint32_t h = hashPixel((uint32_t)dim, 0u, scramble);
+    const float off = (float)(h >> 8) * (1.0f / 16777216.0f);
+    float w = __fadd_rn(v, off);
+    if (w >= 1.0f) w = __fsub_rn(w, 1.0f);
+    return w;
+  }
+  __device__ __forceinline__ int dirDim(int v) const { return dimBase + 4 * v; }
+  __device__ __forceinline__ int neeDim(int v) const { return dimBase + 4 * v + 2; }
+};
+
+__device__ __forceinline__ int pickIndex(float u, int n) {
+  const int i = (int)(u * (float)n);
+  return i < n - 1 ? i : n - 1;
+}
+
+__device__ __forceinline__ void setError(int* err, int code) { atomicCAS(err, 0, code); }
+
+}  // namespace rg

@@ -1,0 +1,116 @@
+// rg_host.h - host-side internals of the B200 tracer (not part of the C ABI).
+#pragma once
+#include <cuda_runtime.h>
+
+#include <atomic>
+#include <cstdint>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "../../include/raygen_b200.h"
+
+namespace rg {
+
+struct DevMaterial;
+struct DevMedium;
+struct DevPointLight;
+struct DevTexture;
+
+// Owning device allocation.
+template <class T>
+struct DevBuf {
+  T* p = nullptr;
+  size_t n = 0;
+  DevBuf() = default;
+  DevBuf(const DevBuf&) = delete;
+  DevBuf& operator=(const DevBuf&) = delete;
+  ~DevBuf() { release(); }
+  bool alloc(size_t count) {
+    if (count <= n && p) return true;
+    release();
+    if (count == 0) count = 1;
+    if (cudaMalloc((void**)&p, count * sizeof(T)) != cudaSuccess) {
+      p = nullptr;
+      n = 0;
+      cudaGetLastError();
+      return false;
+    }
+    n = count;
+    return true;
+  }
+  void release() {
+    if (p) cudaFree(p);
+    p = nullptr;
+    n = 0;
+  }
+  bool upload(const T* src, size_t count, cudaStream_t st) {
+    if (!alloc(count)) return false;
+    if (count && src) return cudaMemcpyAsync(p, src, count * sizeof(T), cudaMemcpyHostToDevice, st) == cudaSuccess;
+    return true;
+  }
+};
+
+// Procedural / loaded scene description owned by the library.
+struct TextureStore {
+  int width = 0, height = 0, isHdr = 0;
+  std::vector<float> rgba;
+};
+
+struct SceneStore {
+  std::vector<float> positions, normals, uvs;
+  std::vector<int32_t> triMesh, meshObject;
+  std::vector<rg_object> objects;
+  std::vector<rg_material> materials;
+  std::vector<rg_medium> media;
+  int32_t globalMedium = -1;
+  std::vector<rg_point_light> pointLights;
+  std::vector<TextureStore> textures;
+  std::vector<rg_texture> textureDescs;
+  rg_camera camera{};
+  rg_scene_desc desc{};
+  void finalize();
+};
+
+rg_status buildBuiltinScene(int kind, uint32_t seed, const int32_t* ip, int nip, SceneStore** out);
+rg_status loadSceneJson(const char* path, SceneStore** out, std::string& err);
+
+// Device-resident scene (BVH + triangle and light tables).
+struct DeviceScene {
+  int numTris = 0;
+  bool hasUV = false;
+  // world-space inputs (freed after the build)
+  DevBuf<float> inPos, inNrm, inUV;
+  DevBuf<int> inTriMesh;
+  DevBuf<float> view;
+  // tables
+  DevBuf<int> meshObj, meshTriCount, objMat, objMedium;
+  DevBuf<DevMaterial> mats;
+  DevBuf<DevMedium> media;
+  int globalMedium = -1;
+  DevBuf<int> areaLightObj, lightMeshList;
+  DevBuf<int2> lightObjMeshes, lightMeshTris;
+  DevBuf<float4> lightTris;
+  int numAreaLights = 0;
+  DevBuf<DevPointLight> points;
+  int numPointLights = 0;
+  DevBuf<DevTexture> textures;
+  std::vector<DevBuf<float4>*> texels;
+  int numTextures = 0;
+  // BVH + leaf-order triangles
+  DevBuf<float4> nodes, triVerts, triShade;
+  DevBuf<float2> triUV;
+  DevBuf<int> triOrig;
+  int numNodes = 0;
+  int rootIsLeaf = 0, rootLeafRef = 0;
+  int buildLevels = 0;
+  ~DeviceScene() {
+    for (auto* t : texels) delete t;
+  }
+};
+
+rg_status buildDeviceBvh(DeviceScene& ds, int nbins, cudaStream_t st, std::string& err);
+
+void setLastError(const std::string& msg);
+
+}  // namespace rg

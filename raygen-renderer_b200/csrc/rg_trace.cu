@@ -1,0 +1,1046 @@
+// rg_trace.cu - wavefront kernels of the shader-5 path tracer.
+//
+// The reference traces one sample at a time with a recursive
+// tracePath -> shade -> {Diffuse,Glossy,Refraction,Transparency}Shader ->
+// tracePath loop (rayrenderer.cpp:1596-1864, :2776-2896, bsdf.cpp:54-610).
+// Here every bounce of a whole wave of paths is one kernel sequence:
+//   generate -> [extend -> shade -> connect(A) -> connect(B)] x depth -> accumulate
+// Rays live in SoA float4 queues (128-bit loads), the shade kernel compacts
+// the surviving paths into the next queue with warp ballots plus one atomic
+// per warp, and NEE shadow rays go to two shadow queues (area lights /
+// point lights) whose visibility kernels add the contribution to the path.
+// The mix shader picks one lobe per vertex with probability proportional to
+// its weight (the reference evaluates every lobe); all other estimator rules
+// (MIS weights, back-face rules, Russian roulette on the reference's
+// throughput, depth cap, media) follow the reference line by line.
+#include <cuda_fp16.h>
+
+#include "rg_device.cuh"
+#include "rg_trace.cuh"
+#include "rg_traverse.cuh"
+
+namespace rg {
+
+// ------------------------------------------------------------ helpers ----
+__device__ __forceinline__ int warpPush(int* counter, bool want) {
+  const unsigned act = __activemask();
+  const unsigned m = __ballot_sync(act, want);
+  const int lane = threadIdx.x & 31;
+  int base = 0;
+  if (m) {
+    const int leader = __ffs(m) - 1;
+    if (lane == leader) base = atomicAdd(counter, __popc(m));
+    base = __shfl_sync(act, base, leader);
+  }
+  return want ? base + __popc(m & ((1u << lane) - 1u)) : -1;
+}
+
+__device__ __forceinline__ void warpAddStat(unsigned long long* dst, uint32_t v) {
+  const unsigned act = __activemask();
+  unsigned long long s = v;
+  for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(act, s, o);
+  const int leader = __ffs(act) - 1;
+  if ((int)(threadIdx.x & 31) == leader && s) atomicAdd(dst, s);
+}
+
+// raycommon.h:82-85
+__device__ __forceinline__ V3 surfaceOrigin(V3 hit, V3 dir, V3 n) {
+  const float side = dot(dir, n) >= 0.0f ? 1.0f : -1.0f;
+  return hit + n * (side * kSurfaceThickness);
+}
+
+// raycommon.cpp:94-115
+__device__ __forceinline__ V3 cosineWeightedDirection(V3 n, float r1, float r2) {
+  const float theta = acosf(sqrtf(1.0f - r1));
+  const float phi = 2.0f * kPi * r2;
+  float st, ct, sp, cp;
+  sincosf(theta, &st, &ct);
+  sincosf(phi, &sp, &cp);
+  V3 tangent = fabsf(n.x) > fabsf(n.y) ? normalize(cross(v3(0, 1, 0), n)) : normalize(cross(v3(1, 0, 0), n));
+  const V3 bit = cross(n, tangent);
+  return normalize(tangent * (st * cp) + bit * (st * sp) + n * ct);
+}
+
+// Uniform direction on the sphere flipped into n's hemisphere (stand-in for
+// ugm randomRayInHemisphere, which is not vendored).
+__device__ __forceinline__ V3 randomRayInHemisphere(V3 n, float u1, float u2) {
+  const float z = 1.0f - 2.0f * u1;
+  const float r = sqrtf(fmaxf(0.0f, 1.0f - z * z));
+  float s, c;
+  sincosf(2.0f * kPi * u2, &s, &c);
+  V3 d = v3(r * c, r * s, z);
+  if (dot(d, n) < 0.0f) d = -d;
+  return d;
+}
+
+__device__ __forceinline__ float srgbToLinear(float c) {  // texture.cpp:204-207
+  if (c <= 0.04045f) return c * (1.0f / 12.92f);
+  return powf((c + 0.055f) * (1.0f / 1.055f), 2.4f);
+}
+
+// Texture::sample: texture.cpp:210-241
+__device__ V3 texSample(const DevScene& S, int tex, float u, float v) {
+  const DevTexture T = S.textures[tex];
+  if (T.width <= 0 || T.height <= 0) return v3(0, 0, 0);
+  if (!(u == u) || !(v == v)) return v3(0, 0, 0);
+  float fu = u - floorf(u), fv = v - floorf(v);
+  if (fu < 0.0f || fu >= 1.0f) fu = 0.0f;
+  if (fv < 0.0f || fv >= 1.0f) fv = 0.0f;
+  const int x = min(max((int)(fu * T.width), 0), T.width - 1);
+  const int y = min(max((int)(fv * T.height), 0), T.height - 1);
+  const float4 p = __ldg(T.texels + (size_t)y * T.width + x);
+  V3 c = v3(p.x, p.y, p.z);
+  if (!T.isHdr) c = v3(srgbToLinear(c.x), srgbToLinear(c.y), srgbToLinear(c.z));
+  return c;
+}
+
+struct Hit {
+  V3 p;        // hit point
+  V3 n;        // interpolated shading normal
+  V3 gn;       // ti.normalizedpd
+  float uvx, uvy;
+  int mesh;
+  int prim;
+};
+
+__device__ __forceinline__ Hit loadHit(const DevScene& S, int prim, V3 o, V3 d, float t, float u, float v) {
+  Hit h;
+  const float4* ts = S.triShade + (size_t)prim * 3;
+  const float4 a = __ldg(ts), b = __ldg(ts + 1), c = __ldg(ts + 2);
+  const V3 n1 = v3(a.x, a.y, a.z), n2 = v3(a.w, b.x, b.y), n3 = v3(b.z, b.w, c.x);
+  const float w = 1.0f - u - v;
+  h.n = normalize(n1 * w + n2 * u + n3 * v);
+  h.gn = v3(c.y, c.z, c.w);
+  h.p = o + d * t;
+  h.mesh = __float_as_int(__ldg(&S.triVerts[(size_t)prim * 3].w));
+  h.prim = prim;
+  h.uvx = h.uvy = 0.0f;
+  if (S.triUV) {
+    const float2 t1 = S.triUV[(size_t)prim * 3], t2 = S.triUV[(size_t)prim * 3 + 1], t3 = S.triUV[(size_t)prim * 3 + 2];
+    h.uvx = t1.x * w + t2.x * u + t3.x * v;
+    h.uvy = t1.y * w + t2.y * u + t3.y * v;
+  }
+  return h;
+}
+
+__device__ __forceinline__ V3 matColor(const DevMaterial& m) { return v3(m.cr, m.cg, m.cb); }
+__device__ __forceinline__ V3 albedoOf(const DevScene& S, const DevMaterial& m, const Hit& h) {
+  V3 a = matColor(m);
+  if (m.texture >= 0) a = a * texSample(S, m.texture, h.uvx * m.tileU, h.uvy * m.tileV);
+  return a;
+}
+
+// An area-light sample (the pick in traceAreaLight / sampleAreaLightForNEE,
+// rayrenderer.cpp:1916-2036).
+struct LightSample {
+  V3 p;        // point on the emitter
+  V3 ln;       // interpolated (unnormalised) emitter normal
+  float area;  // triangles in the mesh * triangle area
+  V3 Le;
+};
+
+__device__ bool pickAreaLight(const DevScene& S, const Rng& rng, int v, int lightObj, LightSample& ls) {
+  const int2 om = S.lightObjMeshes[lightObj];
+  if (om.y <= 0) return false;
+  const int mesh = S.lightMeshList[om.x + pickIndex(rng.prng(v, S_MESH), om.y)];
+  const int2 mt = S.lightMeshTris[mesh];
+  if (mt.y <= 0) return false;
+  const int k = mt.x + pickIndex(rng.prng(v, S_TRI), mt.y);
+  const float4* lt = S.lightTris + (size_t)k * 6;
+  const float4 a = __ldg(lt), b = __ldg(lt + 1), c = __ldg(lt + 2);
+  const float4 na = __ldg(lt + 3), nb = __ldg(lt + 4), nc = __ldg(lt + 5);
+  const V3 v1 = xyz(a), v2 = xyz(b), v3_ = xyz(c);
+  float u = rng.lds(rng.neeDim(v)), w = rng.lds(rng.neeDim(v) + 1);  // ldsPointInTriangle
+  if (u + w > 1.0f) { u = 1.0f - u; w = 1.0f - w; }
+  ls.p = v1 + (v2 - v1) * u + (v3_ - v1) * w;
+  // calcVertexInterpolation(tri, p): rayrenderer.cpp:2337-2352
+  const V3 f1 = v1 - ls.p, f2 = v2 - ls.p, f3 = v3_ - ls.p;
+  const V3 c1 = cross(f2, f3), c2 = cross(f3, f1), c3 = cross(f1, f2);
+  const float a1 = sqrtf(dot(c1, c1)) * a.w, a2 = sqrtf(dot(c2, c2)) * a.w, a3 = sqrtf(dot(c3, c3)) * a.w;
+  ls.ln = xyz(na) * a1 + xyz(nb) * a2 + xyz(nc) * a3;
+  ls.area = (float)mt.y * b.w;
+  const DevMaterial& m = S.mats[S.objMat[lightObj]];
+  ls.Le = matColor(m) * m.emission;
+  return true;
+}
+
+struct Shadow {
+  bool on;
+  V3 o, d;
+  float tmax;
+  V3 c;
+};
+
+// traceAreaLight (rayrenderer.cpp:1916-1984) up to the shadow test; the
+// contribution is deferred to the shadow ray.  `w` multiplies the result.
+__device__ void traceAreaLight(const DevScene& S, const DevRender& R, const Rng& rng, int v, V3 hit, V3 n, V3 w,
+                               Shadow& sh) {
+  const int N = S.numAreaLights;
+  if (N <= 0) return;
+  const int lo = S.areaLightObj[pickIndex(rng.prng(v, S_LIGHT), N)];
+  LightSample ls;
+  if (!pickAreaLight(S, rng, v, lo, ls)) return;
+  const V3 lr = ls.p - hit;
+  const V3 ld = normalize(lr);
+  const float dObj = dot(ld, n);
+  if (dObj <= 0.0f) return;
+  const float dLight = dot(-ld, ls.ln);
+  if (dLight <= 0.0f) return;
+  const float lf = R.lightFix ? (float)N : 1.0f;
+  const float r2 = dot(lr, lr);
+  const float pl = r2 / (dLight * ls.area) / lf;
+  const float pb = dObj / kPi;
+  const float wl = pl * pl / (pl * pl + pb * pb);
+  sh.on = true;
+  sh.o = surfaceOrigin(hit, lr, n);
+  sh.d = lr;
+  sh.tmax = 0.99999f;
+  sh.c = w * ls.Le * (dObj * dLight * ls.area / (kPi * r2) * wl * lf);
+}
+
+// tracePointLight (rayrenderer.cpp:2205-2269) up to the shadow test.
+__device__ void tracePointLight(const DevScene& S, int idx, V3 hit, V3 n, V3 w, Shadow& sh) {
+  const DevPointLight P = S.points[idx];
+  const V3 lr = v3(P.px, P.py, P.pz) - hit;
+  const V3 ldir = normalize(lr);
+  const float dObj = dot(ldir, n);
+  float dLight = dot(ldir, v3(P.nx, P.ny, P.nz));
+  if (!(dObj > 0.0f)) return;
+  const DevMaterial& m = S.mats[P.material];
+  if (m.spotRange > 0.0f) {
+    const float spotDot = cosf(m.spotRange * 0.5f * (180.0f / kPi));
+    const float e0 = fmaxf(spotDot - 0.1f, 0.0f), e1 = fminf(spotDot + 0.1f, 1.0f);
+    float x = (dLight - e0) / (e1 - e0);
+    x = fminf(fmaxf(x, 0.0f), 1.0f);
+    dLight = dLight * (x * x * (3.0f - 2.0f * x));
+  } else {
+    dLight = fabsf(dObj);
+  }
+  if (!(dLight > 0.0f)) return;
+  const float da = 1.0f / dot(lr, lr);
+  const float lum = m.emission * dLight * da;
+  V3 col = matColor(m) * lum;
+  col = v3(fminf(fmaxf(col.x, 0.0f), 1.0f), fminf(fmaxf(col.y, 0.0f), 1.0f), fminf(fmaxf(col.z, 0.0f), 1.0f));
+  sh.on = true;
+  sh.o = surfaceOrigin(hit, lr, n);
+  sh.d = lr;
+  sh.tmax = 0.99999f;
+  sh.c = w * col;
+}
+
+// traceLight (rayrenderer.cpp:2271-2293): one area light + one point light.
+__device__ void traceLight(const DevScene& S, const DevRender& R, const Rng& rng, int v, V3 hit, V3 n, V3 w,
+                           Shadow& a, Shadow& b) {
+  traceAreaLight(S, R, rng, v, hit, n, w, a);
+  const int np = S.numPointLights;
+  if (np > 0) tracePointLight(S, np == 1 ? 0 : pickIndex(rng.prng(v, S_POINT), np), hit, n, w, b);
+}
+
+// sampleAreaLightForNEE (rayrenderer.cpp:1986-2036) up to the shadow test.
+__device__ bool sampleAreaLightForNEE(const DevScene& S, const DevRender& R, const Rng& rng, int v, V3 hit, V3 n,
+                                      V3& dir, float& pdf, V3& Le, Shadow& sh) {
+  const int N = S.numAreaLights;
+  if (N <= 0) return false;
+  const int lo = S.areaLightObj[pickIndex(rng.prng(v, S_LIGHT), N)];
+  LightSample ls;
+  if (!pickAreaLight(S, rng, v, lo, ls)) return false;
+  const V3 lr = ls.p - hit;
+  dir = normalize(lr);
+  const float cObj = dot(dir, n);
+  if (cObj <= 0.0f) return false;
+  const float cLight = dot(-dir, ls.ln);
+  if (cLight <= 0.0f) return false;
+  const float lf = R.lightFix ? (float)N : 1.0f;
+  pdf = dot(lr, lr) / (cLight * ls.area) / lf;
+  Le = ls.Le;
+  sh.o = surfaceOrigin(hit, lr, n);
+  sh.d = lr;
+  sh.tmax = 0.99999f;
+  return true;
+}
+
+// ------------------------------------------------------------ kernels ----
+__device__ __forceinline__ void waveCoords(const DevRender& R, const DevWave& W, int pid, int& px, int& py,
+                                           uint32_t& sample) {
+  const int i = pid % W.numPixels;
+  const int sl = pid / W.numPixels;
+  const int pixel = W.pixelList ? W.pixelList[W.pixelOffset + i] : W.pixelOffset + i;
+  px = pixel % R.width;
+  py = pixel / R.width;
+  sample = (uint32_t)((W.pixelSampleBase ? W.pixelSampleBase[pixel] : W.sampleBase) + sl);
+}
+
+__device__ __forceinline__ int dimBaseOf(const DevRender& R) { return (R.dof >= 0.001f && R.aperture > 0.0f) ? 4 : 2; }
+
+// accumulatePixelSamples ray generation (rayrenderer.cpp:847-934).
+__device__ void primaryRay(const DevRender& R, const Rng& rng, int x, int y, V3& o, V3& d) {
+  const float vs = R.viewScale;
+  const float dx = ((float)x + 0.5f - R.halfW) * vs;
+  const float dy = -((float)y + 0.5f - R.halfH) * vs;
+  const float jx = rng.lds(0), jy = rng.lds(1);
+  const float jxo = R.aa ? (jx - 0.5f) : 0.0f, jyo = R.aa ? (jy - 0.5f) : 0.0f;
+  if (R.dof >= 0.001f && R.aperture > 0.0f) {
+    const float pxDx = dx + jxo * vs, pxDy = dy - jyo * vs;
+    const V3 fp = v3(pxDx * R.dof, pxDy * R.dof, -R.dof);
+    const float du = rng.lds(2), dv = rng.lds(3);
+    float ox, oy;
+    if (R.blades >= 3) {
+      const int N = R.blades;
+      const float u0 = du * (float)N;
+      const int wedge = (int)fminf((float)(N - 1), floorf(u0));
+      float s = u0 - (float)wedge, t = dv;
+      if (s + t > 1.0f) { s = 1.0f - s; t = 1.0f - t; }
+      const float step = 2.0f * kPi / (float)N;
+      const float a0 = R.apertureRot + step * (float)wedge, a1 = a0 + step;
+      ox = (cosf(a0) * s + cosf(a1) * t) * R.aperture;
+      oy = (sinf(a0) * s + sinf(a1) * t) * R.aperture;
+    } else {
+      const float a = 2.0f * du - 1.0f, b = 2.0f * dv - 1.0f;
+      float r, phi;
+      if (a == 0.0f && b == 0.0f) { r = 0.0f; phi = 0.0f; }
+      else if (a * a > b * b) { r = a; phi = (kPi / 4.0f) * (b / a); }
+      else { r = b; phi = (kPi / 2.0f) - (kPi / 4.0f) * (a / b); }
+      ox = r * cosf(phi) * R.aperture;
+      oy = r * sinf(phi) * R.aperture;
+    }
+    o = v3(ox, oy, 0.0f);
+    d = normalize(fp - o);
+  } else {
+    o = v3(0, 0, 0);
+    d = normalize(v3(dx + jxo * vs, dy - jyo * vs, -1.0f));
+  }
+}
+
+__global__ void __launch_bounds__(256) k_generate(DevRender R, const DevWave* __restrict__ Wp, DevQueues Q,
+                                                  int globalMedium) {
+  const DevWave W = *Wp;
+  const int numPaths = W.numPixels * W.samplesInWave;
+  if (blockIdx.x == 0) {
+    for (int i = threadIdx.x; i < Q.maxIter * kCountersPerIter; i += blockDim.x) Q.counters[i] = 0;
+    __syncthreads();
+    if (threadIdx.x == 0) Q.counters[C_RAYS] = numPaths;
+  }
+  const int dimBase = dimBaseOf(R);
+  const uint32_t medFlag = (uint32_t)(globalMedium + 1) << F_MED_SHIFT;
+  for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < numPaths; p += gridDim.x * blockDim.x) {
+    int x, y;
+    uint32_t sample;
+    waveCoords(R, W, p, x, y, sample);
+    Rng rng;
+    rng.init(x, y, R.width, sample, R.seed, dimBase);
+    V3 o, d;
+    primaryRay(R, rng, x, y, o, d);
+    Q.rayO[0][p] = make_float4(o.x, o.y, o.z, __int_as_float(p));
+    Q.rayD[0][p] = make_float4(d.x, d.y, d.z, 0.0f);
+    Q.pathT[p] = make_float4(1.0f, 1.0f, 1.0f, 0.0f);
+    Q.pathR[p] = make_float4(1.0f, 1.0f, 1.0f, __uint_as_float(F_EYE | medFlag));
+    Q.pathL[p] = make_float4(0.0f, 0.0f, 0.0f, __int_as_float(0));
+  }
+}
+
+// Closest hit for the iteration's queue; persistent warps fetch 32 rays at a time.
+__global__ void __launch_bounds__(128) k_extend(DevScene S, DevQueues Q, int iter) {
+  const int count = Q.counters[iter * kCountersPerIter + C_RAYS];
+  int* fetch = &Q.counters[iter * kCountersPerIter + C_FETCH_EXT];
+  const float4* __restrict__ rO = Q.rayO[iter & 1];
+  const float4* __restrict__ rD = Q.rayD[iter & 1];
+  const int lane = threadIdx.x & 31;
+  uint32_t nodes = 0, tris = 0, rays = 0;
+  for (;;) {
+    int base = 0;
+    if (lane == 0) base = atomicAdd(fetch, 32);
+    base = __shfl_sync(0xffffffffu, base, 0);
+    if (base >= count) break;
+    const int q = base + lane;
+    if (q < count) {
+      const float4 a = rO[q], b = rD[q];
+      const ClosestHit h = traceClosest(S, xyz(a), xyz(b), nodes, tris);
+      Q.hits[q] = make_float4(h.t, h.u, h.v, __int_as_float(h.prim));
+      rays++;
+    }
+  }
+  warpAddStat(&Q.stats[0], nodes);
+  warpAddStat(&Q.stats[1], tris);
+  warpAddStat(&Q.stats[4], rays);
+}
+
+// Shadow-ray visibility; unoccluded contributions are added to the path.
+__global__ void __launch_bounds__(128) k_connect(DevScene S, DevQueues Q, int iter, int which) {
+  const int count = Q.counters[iter * kCountersPerIter + (which ? C_SHB : C_SHA)];
+  int* fetch = &Q.counters[iter * kCountersPerIter + (which ? C_FETCH_SHB : C_FETCH_SHA)];
+  const float4* __restrict__ sO = Q.shO[which];
+  const float4* __restrict__ sD = Q.shD[which];
+  const float4* __restrict__ sC = Q.shC[which];
+  const uint32_t occ = which ? kOccPoint : kOccArea;
+  const int lane = threadIdx.x & 31;
+  uint32_t nodes = 0, tris = 0, rays = 0;
+  for (;;) {
+    int base = 0;
+    if (lane == 0) base = atomicAdd(fetch, 32);
+    base = __shfl_sync(0xffffffffu, base, 0);
+    if (base >= count) break;
+    const int q = base + lane;
+    if (q < count) {
+      const float4 a = sO[q], b = sD[q];
+      rays++;
+      if (!traceAny(S, xyz(a), xyz(b), b.w, occ, nodes, tris)) {
+        const float4 c = sC[q];
+        const int pid = __float_as_int(a.w);
+        float4 l = Q.pathL[pid];
+        l.x += c.x; l.y += c.y; l.z += c.z;
+        Q.pathL[pid] = l;
+      }
+    }
+  }
+  warpAddStat(&Q.stats[2], nodes);
+  warpAddStat(&Q.stats[3], tris);
+  warpAddStat(&Q.stats[5], rays);
+}
+
+// One path vertex (RayBSDFShaderProvider::shade + lobes + tracePath's medium branch).
+__global__ void __launch_bounds__(256) k_shade(DevScene S, DevRender R, const DevWave* __restrict__ Wp, DevQueues Q,
+                                               int iter) {
+  const DevWave W = *Wp;
+  const int count = Q.counters[iter * kCountersPerIter + C_RAYS];
+  const int inB = iter & 1, outB = (iter + 1) & 1;
+  const int dimBase = dimBaseOf(R);
+  const int stride = gridDim.x * blockDim.x;
+  const int rounded = ((count + 31) / 32) * 32;
+  for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < rounded; q += stride) {
+    const bool valid = q < count;
+    Shadow shA, shB;
+    shA.on = false;
+    shB.on = false;
+    bool cont = false;
+    V3 no = v3(0, 0, 0), nd = v3(0, 0, 0);
+    int pid = 0;
+    if (valid) {
+      const float4 ro = Q.rayO[inB][q], rd = Q.rayD[inB][q];
+      pid = __float_as_int(ro.w);
+      const V3 o = xyz(ro), d = xyz(rd);
+      const float4 hq = Q.hits[q];
+      const int prim = __float_as_int(hq.w);
+      const float4 PT = Q.pathT[pid], PR = Q.pathR[pid], PL = Q.pathL[pid];
+      V3 beta = xyz(PT);
+      float bsdfPdf = PT.w;
+      V3 rrT = xyz(PR);
+      uint32_t flags = __float_as_uint(PR.w);
+      V3 L = xyz(PL);
+      const int v = __float_as_int(PL.w);
+      bool eye = (flags & F_EYE) != 0;
+      int passes = (int)(flags & F_PASSES_MASK);
+      int chroma = (int)((flags & F_CHROMA_MASK) >> F_CHROMA_SHIFT) - 1;
+      int med = (int)((flags & F_MED_MASK) >> F_MED_SHIFT) - 1;
+      if (eye && prim < 0) flags |= F_EYE_NOHIT;
+      int x, y;
+      uint32_t sample;
+      waveCoords(R, W, pid, x, y, sample);
+      Rng rng;
+      rng.init(x, y, R.width, sample, R.seed, dimBase);
+      bool done = false;
+      bool silhouette = false;
+      // ---- participating medium on the segment (tracePath, rayrenderer.cpp:1665-1831)
+      const bool medActive = med >= 0 && S.media[med].hero > 0.0f;
+      if (medActive) {
+        const DevMedium M = S.media[med];
+        const float maxT = prim >= 0 ? hq.x : kRayMaxDistance;
+        const float xi = fminf(0.9999999f, fmaxf(0.0f, rng.prng(v, S_FLIGHT)));
+        const float tF = -logf(1.0f - xi) / M.hero;
+        const bool scat = tF < maxT;
+        const float el = scat ? tF : maxT;
+        if (el > 0.0f) {
+          auto ew = [](float st, float dd) { return st < 1e-6f ? dd : (1.0f - expf(-st * dd)) / st; };
+          L = L + beta * v3(M.ser * ew(M.str, el), M.seg * ew(M.stg, el), M.seb * ew(M.stb, el));
+        }
+        if (scat) {
+          const float pHero = M.hero * expf(-M.hero * tF);
+          V3 sw = v3(0, 0, 0);
+          if (pHero > 0.0f)
+            sw = v3(M.ssr * expf(-M.str * tF) / pHero, M.ssg * expf(-M.stg * tF) / pHero, M.ssb * expf(-M.stb * tF) / pHero);
+          const int passesS = eye ? 1 : passes + 1;
+          if ((sw.x == 0.0f && sw.y == 0.0f && sw.z == 0.0f) || passesS > R.maxDepth) {
+            done = true;
+          } else {
+            const V3 pos = o + d * tF;
+            const V3 proxy = -d;
+            V3 lDir, Le;
+            float pl;
+            if (sampleAreaLightForNEE(S, R, rng, v, pos, proxy, lDir, pl, Le, shA) && pl > 0.0f) {
+              const float g = M.g;
+              const float cosT = dot(-d, lDir);
+              const float den = 1.0f + g * g - 2.0f * g * cosT;
+              const float phase = (1.0f - g * g) * (1.0f / (4.0f * kPi)) / (den * sqrtf(fmaxf(1e-8f, den)));
+              shA.on = true;
+              shA.c = beta * sw * Le * (phase / pl);
+            }
+            // samplePhase: medium.cpp:496-517
+            const float u1 = rng.prng(v, S_PHASE0), u2 = rng.prng(v, S_PHASE1);
+            float cosTheta;
+            if (fabsf(M.g) < 1e-3f) cosTheta = 1.0f - 2.0f * u1;
+            else {
+              const float sq = (1.0f - M.g * M.g) / (1.0f - M.g + 2.0f * M.g * u1);
+              cosTheta = (1.0f + M.g * M.g - sq * sq) / (2.0f * M.g);
+            }
+            const float sinTheta = sqrtf(fmaxf(0.0f, 1.0f - cosTheta * cosTheta));
+            float sp, cp;
+            sincosf(2.0f * kPi * u2, &sp, &cp);
+            V3 t1;
+            if (fabsf(d.x) > fabsf(d.y)) { const float inv = 1.0f / sqrtf(d.x * d.x + d.z * d.z); t1 = v3(-d.z * inv, 0.0f, d.x * inv); }
+            else { const float inv = 1.0f / sqrtf(d.y * d.y + d.z * d.z); t1 = v3(0.0f, d.z * inv, -d.y * inv); }
+            const V3 t2 = cross(d, t1);
+            const V3 ndir = normalize(t1 * (sinTheta * cp) + t2 * (sinTheta * sp) + d * cosTheta);
+            const V3 rrBase = eye ? v3(1, 1, 1) : rrT;
+            float rrW = 1.0f;
+            bool killed = false;
+            if (passesS >= R.rrDepth) {
+              float qq = maxc(rrBase * sw);
+              qq = fminf(kRRMax, fmaxf(kRRMin, qq));
+              if (rng.prng(v, S_MEDRR) >= qq) killed = true;
+              else rrW = 1.0f / qq;
+            }
+            if (killed) {
+              done = true;
+            } else {
+              beta = beta * sw * rrW;
+              rrT = rrBase;
+              if (eye) chroma = -1;
+              bsdfPdf = 0.0f;
+              passes = passesS;
+              eye = false;
+              cont = true;
+              no = pos + normalize(ndir) * kSurfaceThickness;  // ThicknessRay
+              nd = ndir;
+            }
+          }
+        } else {
+          const float surv = expf(-M.hero * maxT);
+          if (surv > 0.0f)
+            beta = beta * v3(expf(-M.str * maxT) / surv, expf(-M.stg * maxT) / surv, expf(-M.stb * maxT) / surv);
+          if (prim < 0) done = true;
+          silhouette = true;
+        }
+      } else if (prim < 0) {
+        done = true;  // environment miss: no environment map
+      }
+      // ---- surface vertex (RayBSDFShaderProvider::shade, rayrenderer.cpp:2776-2896)
+      if (!done && !cont) {
+        Hit h = loadHit(S, prim, o, d, hq.x, hq.y, hq.z);
+        if (silhouette) {  // rayrenderer.cpp:1842-1846
+          const V3 geomN = dot(h.gn, d) <= 0.0f ? h.gn : -h.gn;
+          if (dot(d, h.n) > 0.0f && dot(d, geomN) < 0.0f) h.n = geomN;
+        }
+        const int obj = S.meshObj[h.mesh];
+        const DevMaterial m = S.mats[S.objMat[obj]];
+        const V3 gN = dot(h.gn, h.n) >= 0.0f ? h.gn : -h.gn;  // geomNormal, bsdf.cpp:27-30
+        const float lf = R.lightFix ? (float)S.numAreaLights : 1.0f;
+        int lobe = -1;  // 0 diffuse 1 glossy 2 refraction 3 transparency
+        if (m.emission > 0.0f) {
+          V3 e = matColor(m) * m.emission;
+          if (!eye && bsdfPdf > 0.0f) {
+            const float cosL = -dot(d, h.n);
+            if (cosL <= 0.0f) e = v3(0, 0, 0);
+            else {
+              const V3 dv = h.p - o;
+              const float r2 = dot(dv, dv);
+              const float4 e1 = __ldg(&S.triVerts[(size_t)prim * 3 + 1]), e2 = __ldg(&S.triVerts[(size_t)prim * 3 + 2]);
+              const V3 cr = cross(xyz(e1), xyz(e2));
+              const float area = 0.5f * sqrtf(dot(cr, cr)) * (float)S.meshTriCount[h.mesh];
+              const float pl = r2 / (cosL * area) / lf;
+              e = e * (bsdfPdf * bsdfPdf / (bsdfPdf * bsdfPdf + pl * pl));
+            }
+          }
+          L = L + beta * e;
+          done = true;
+        } else {
+          bool backTransparency = false;
+          if (dot(d, h.n) > 0.0f) {
+            if (m.transparency > 0.001f) {
+              if (!eye && passes + 1 <= R.maxDepth) {
+                backTransparency = true;
+                passes = passes + 1;
+                chroma = -1;
+                bsdfPdf = 0.0f;
+                lobe = 3;
+              } else {
+                done = true;
+              }
+            } else if (m.refraction < 0.001f && m.glossy > 0.001f) {
+              done = true;
+            }
+          }
+          if (!done && !backTransparency) {
+            if (!eye) {
+              if (passes + 1 >= R.maxDepth) {  // depth cap: direct light only
+                if (1.0f - m.glossy - m.refraction > 0.00001f) {
+                  const V3 col = R.colorSampling ? albedoOf(S, m, h) : v3(0, 0, 0);
+                  traceLight(S, R, rng, v, h.p, h.n, beta * col, shA, shB);
+                }
+                done = true;
+              } else {
+                passes = passes + 1;
+                if (passes >= R.rrDepth) {
+                  float qq = maxc(rrT);
+                  qq = fminf(kRRMax, fmaxf(kRRMin, qq));
+                  if (rng.prng(v, S_RR) >= qq) done = true;
+                  else beta = beta * (1.0f / qq);
+                }
+                if (!done) lobe = m.transparency > 0.001f ? 3 : 4;
+              }
+            } else {
+              passes = 0;
+              rrT = v3(1, 1, 1);
+              chroma = -1;
+              bsdfPdf = 0.0f;
+              if (m.transparency > 0.01f) {
+                // mix * (1 - t) + transparency: pick transparency with probability t
+                lobe = rng.prng(v, S_EYETR) < m.transparency ? 3 : 4;
+                if (lobe == 3) beta = beta * (1.0f / m.transparency);
+              } else {
+                lobe = 4;
+              }
+            }
+          }
+          if (!done && lobe == 4) {  // MixShader (bsdf.cpp:579-610), one lobe selected
+            const float wv[3] = {1.0f - m.glossy - m.refraction, m.glossy, m.refraction};
+            float sum = 0.0f;
+            for (int k = 0; k < 3; k++) if (wv[k] > 0.00001f) sum += wv[k];
+            if (sum > 0.0f) {
+              const float u = rng.prng(v, S_LOBE) * sum;
+              float acc = 0.0f;
+              for (int k = 0; k < 3; k++) {
+                if (!(wv[k] > 0.00001f)) continue;
+                lobe = k;
+                acc += wv[k];
+                if (u < acc) break;
+              }
+              beta = beta * sum;
+              rrT = rrT * wv[lobe];
+            } else {
+              done = true;
+            }
+          }
+          if (!done && lobe == 0) {  // DiffuseShader (bsdf.cpp:54-108)
+            const V3 albedo = R.colorSampling ? albedoOf(S, m, h) : v3(1, 1, 1);
+            const int d0 = rng.dirDim(v);
+            const V3 dir = cosineWeightedDirection(h.n, rng.lds(d0), rng.lds(d0 + 1));
+            traceLight(S, R, rng, v, h.p, h.n, beta * albedo, shA, shB);
+            bsdfPdf = fmaxf(0.0f, dot(dir, h.n)) * (1.0f / kPi);
+            beta = beta * albedo;
+            rrT = rrT * albedo;
+            cont = true;
+            no = surfaceOrigin(h.p, dir, gN);
+            nd = dir;
+          } else if (!done && lobe == 1) {  // GlossyShader (bsdf.cpp:173-374)
+            V3 albedo = matColor(m);
+            if (R.colorSampling && m.texture >= 0) albedo = albedoOf(S, m, h);
+            const V3 F0 = m.metallic >= 1.0f ? albedo : (albedo * m.metallic + v3(0.04f, 0.04f, 0.04f) * (1.0f - m.metallic));
+            auto schlick = [&](float VdotH) {
+              const float a1 = fmaxf(0.0f, 1.0f - VdotH);
+              const float a5 = a1 * a1 * a1 * a1 * a1;
+              return F0 + (v3(1, 1, 1) - F0) * a5;
+            };
+            if (m.roughness < 1e-3f) {
+              V3 r = reflect(d, h.n);
+              if (dot(r, gN) <= 0.0f) r = reflect(d, gN);
+              const V3 F = schlick(fmaxf(0.0f, -dot(d, h.n)));
+              beta = beta * F;
+              rrT = rrT * F;
+              bsdfPdf = 0.0f;
+              cont = true;
+              no = surfaceOrigin(h.p, r, gN);
+              nd = r;
+            } else {
+              const V3 up = fabsf(h.n.y) > 0.99f ? v3(1, 0, 0) : v3(0, 1, 0);
+              V3 t = normalize(cross(up, h.n));
+              V3 b = cross(h.n, t);
+              if (fabsf(m.anisoRot) > 0.0f) {
+                float sa, ca;
+                sincosf(m.anisoRot * (kPi / 180.0f), &sa, &ca);
+                const V3 t2 = t * ca + b * sa, b2 = b * ca - t * sa;
+                t = t2;
+                b = b2;
+              }
+              const float aniso = fmaxf(-0.99f, fminf(0.99f, m.aniso));
+              const float r2 = m.roughness * m.roughness;
+              const float ax = fmaxf(1e-3f, r2 * (1.0f - aniso));
+              const float ay = fmaxf(1e-3f, r2 * (1.0f + aniso));
+              const V3 Vw = -d;
+              const V3 Vl = v3(dot(Vw, t), dot(Vw, b), dot(Vw, h.n));
+              if (Vl.z <= 0.0f) {
+                done = true;
+              } else {
+                auto smithG1 = [&](V3 w) {
+                  if (w.z <= 0.0f) return 0.0f;
+                  const float ax2 = (ax * w.x) * (ax * w.x), ay2 = (ay * w.y) * (ay * w.y);
+                  const float lambda = 0.5f * (sqrtf(1.0f + (ax2 + ay2) / (w.z * w.z)) - 1.0f);
+                  return 1.0f / (1.0f + lambda);
+                };
+                const float G1v = smithG1(Vl);
+                // area-light NEE with MIS (bsdf.cpp:271-284)
+                V3 lDir, Le;
+                float pl;
+                if (sampleAreaLightForNEE(S, R, rng, v, h.p, h.n, lDir, pl, Le, shA)) {
+                  const V3 Ll = v3(dot(lDir, t), dot(lDir, b), dot(lDir, h.n));
+                  if (Ll.z > 0.0f) {
+                    V3 Hl = Vl + Ll;
+                    const float hl2 = dot(Hl, Hl);
+                    if (hl2 > 0.0f) {
+                      Hl = Hl * (1.0f / sqrtf(hl2));
+                      const float VdotH = fmaxf(0.0f, dot(Vl, Hl));
+                      if (Hl.z > 0.0f && VdotH > 0.0f) {
+                        const float hx = Hl.x / ax, hy = Hl.y / ay;
+                        const float den = hx * hx + hy * hy + Hl.z * Hl.z;
+                        const float D = 1.0f / (kPi * ax * ay * den * den);
+                        const V3 fCos = schlick(VdotH) * (D * G1v * smithG1(Ll) / (4.0f * Vl.z));
+                        const float pb = G1v * D / (4.0f * Vl.z);
+                        const float wl = pl * pl / (pl * pl + pb * pb);
+                        shA.on = true;
+                        shA.c = beta * Le * fCos * (wl / pl);
+                      }
+                    }
+                  }
+                }
+                // VNDF sample (bsdf.cpp:139-161, 319-373)
+                const float u1 = rng.prng(v, S_VNDF0), u2 = rng.prng(v, S_VNDF1);
+                const V3 Vh = normalize(v3(ax * Vl.x, ay * Vl.y, Vl.z));
+                const float lensq = Vh.x * Vh.x + Vh.y * Vh.y;
+                const V3 T1 = lensq > 0.0f ? v3(-Vh.y, Vh.x, 0.0f) * (1.0f / sqrtf(lensq)) : v3(1, 0, 0);
+                const V3 T2 = cross(Vh, T1);
+                const float rr = sqrtf(u1);
+                float sphi, cphi;
+                sincosf(2.0f * kPi * u2, &sphi, &cphi);
+                const float t1 = rr * cphi;
+                float t2 = rr * sphi;
+                const float sw = 0.5f * (1.0f + Vh.z);
+                t2 = (1.0f - sw) * sqrtf(fmaxf(0.0f, 1.0f - t1 * t1)) + sw * t2;
+                const V3 Nh = T1 * t1 + T2 * t2 + Vh * sqrtf(fmaxf(0.0f, 1.0f - t1 * t1 - t2 * t2));
+                const V3 H = normalize(v3(ax * Nh.x, ay * Nh.y, fmaxf(0.0f, Nh.z)));
+                const V3 Ll = H * (2.0f * dot(Vl, H)) - Vl;
+                if (Ll.z <= 0.0f) {
+                  done = true;
+                } else {
+                  const V3 Lw = t * Ll.x + b * Ll.y + h.n * Ll.z;
+                  if (dot(Lw, gN) <= 0.0f) {
+                    done = true;
+                  } else {
+                    const V3 F = schlick(fmaxf(0.0f, dot(Vl, H)));
+                    const V3 wgt = F * smithG1(Ll);
+                    const float hx = H.x / ax, hy = H.y / ay;
+                    const float den = hx * hx + hy * hy + H.z * H.z;
+                    const float D = 1.0f / (kPi * ax * ay * den * den);
+                    bsdfPdf = G1v * D / (4.0f * Vl.z);
+                    beta = beta * wgt;
+                    rrT = rrT * wgt;
+                    cont = true;
+                    no = surfaceOrigin(h.p, Lw, gN);
+                    nd = Lw;
+                  }
+                }
+              }
+            }
+          } else if (!done && lobe == 2) {  // RefractionShader (bsdf.cpp:376-483)
+            const float cosTheta = fabsf(dot(d, h.n));
+            float ior = m.ior;
+            V3 mask = v3(1, 1, 1);
+            if (m.chroma > 0.0f) {
+              bool first = false;
+              if (chroma < 0) {
+                chroma = (int)fminf(2.0f, floorf(rng.prng(v, S_CHROMA) * 3.0f));
+                first = true;
+              }
+              if (chroma == 0) ior = m.ior * (1.0f - m.chroma);
+              else if (chroma == 2) ior = m.ior * (1.0f + m.chroma);
+              if (first) mask = chroma == 0 ? v3(3, 0, 0) : (chroma == 1 ? v3(0, 3, 0) : v3(0, 0, 3));
+            }
+            float r0 = (1.0f - ior) / (1.0f + ior);
+            r0 = r0 * r0;
+            const float mm = 1.0f - cosTheta;
+            const float F = r0 + (1.0f - r0) * (mm * mm) * (mm * mm) * mm;
+            const bool pickReflect = rng.prng(v, S_FRESNEL) < F;
+            V3 dir;
+            if (pickReflect) {
+              dir = reflect(d, h.n);
+            } else {  // refract (bsdf.cpp:39-52)
+              const V3 nl = dot(d, h.n) < 0.0f ? h.n : -h.n;
+              const bool into = dot(nl, h.n) > 0.0f;
+              const float rr = into ? 1.0f / ior : ior;
+              const float c = dot(d, nl);
+              const float tt = 1.0f - rr * rr * (1.0f - c * c);
+              if (tt < 0.0f) dir = reflect(d, h.n);
+              else dir = normalize(d * rr - h.n * ((into ? 1.0f : -1.0f) * (c * rr + sqrtf(tt))));
+            }
+            if (m.roughness > 0.0f)
+              dir = normalize(dir + randomRayInHemisphere(h.n, rng.prng(v, S_HEMI0), rng.prng(v, S_HEMI1)) * m.roughness);
+            if (pickReflect && dot(dir, gN) <= 0.0f) dir = reflect(d, gN);
+            const float dIn = dot(d, h.n), dOut = dot(dir, h.n);
+            if (dIn * dOut > 0.0f) {
+              if (dIn < 0.0f) { const int im = S.objMedium[obj]; if (im >= 0) med = im; }
+              else med = S.globalMedium;
+            }
+            const V3 col = matColor(m);
+            beta = beta * col * mask;
+            rrT = rrT * col;
+            bsdfPdf = 0.0f;
+            cont = true;
+            no = surfaceOrigin(h.p, dir, gN);
+            nd = dir;
+          } else if (!done && lobe == 3) {  // TransparencyShader (bsdf.cpp:513-546)
+            const float tr = m.transparency;
+            beta = beta * tr;
+            rrT = rrT * tr;
+            if (dot(d, h.n) < 0.0f) { const int im = S.objMedium[obj]; if (im >= 0) med = im; }
+            else med = S.globalMedium;
+            cont = true;
+            no = surfaceOrigin(h.p, d, gN);
+            nd = d;
+          }
+          if (!done && cont) eye = false;
+        }
+      }
+      // write back the path state
+      flags = (flags & ~(F_PASSES_MASK | F_CHROMA_MASK | F_MED_MASK | F_EYE)) | ((uint32_t)passes & F_PASSES_MASK) |
+              ((uint32_t)(chroma + 1) << F_CHROMA_SHIFT) | ((uint32_t)(med + 1) << F_MED_SHIFT) | (eye ? F_EYE : 0u);
+      Q.pathT[pid] = make_float4(beta.x, beta.y, beta.z, bsdfPdf);
+      Q.pathR[pid] = make_float4(rrT.x, rrT.y, rrT.z, __uint_as_float(flags));
+      Q.pathL[pid] = make_float4(L.x, L.y, L.z, __int_as_float(v + 1));
+      if (!cont) {
+        no = v3(0, 0, 0);
+      }
+    }
+    // queue pushes (warp-aggregated)
+    const int slot = warpPush(&Q.counters[(iter + 1) * kCountersPerIter + C_RAYS], cont && (iter + 1) < Q.maxIter);
+    if (slot >= 0) {
+      Q.rayO[outB][slot] = make_float4(no.x, no.y, no.z, __int_as_float(pid));
+      Q.rayD[outB][slot] = make_float4(nd.x, nd.y, nd.z, 0.0f);
+    }
+    const int sa = warpPush(&Q.counters[iter * kCountersPerIter + C_SHA], shA.on);
+    if (sa >= 0) {
+      Q.shO[0][sa] = make_float4(shA.o.x, shA.o.y, shA.o.z, __int_as_float(pid));
+      Q.shD[0][sa] = make_float4(shA.d.x, shA.d.y, shA.d.z, shA.tmax);
+      Q.shC[0][sa] = make_float4(shA.c.x, shA.c.y, shA.c.z, 0.0f);
+    }
+    const int sb = warpPush(&Q.counters[iter * kCountersPerIter + C_SHB], shB.on);
+    if (sb >= 0) {
+      Q.shO[1][sb] = make_float4(shB.o.x, shB.o.y, shB.o.z, __int_as_float(pid));
+      Q.shD[1][sb] = make_float4(shB.d.x, shB.d.y, shB.d.z, shB.tmax);
+      Q.shC[1][sb] = make_float4(shB.c.x, shB.c.y, shB.c.z, 0.0f);
+    }
+  }
+}
+
+// ---- shader ids 0-3 (one thread per path; rayrenderer.h:456-474, lambert.cpp:14-65)
+__device__ float calcAO(const DevScene& S, const DevRender& R, const Rng& rng, int v, V3 hit, V3 n, float dist,
+                        uint32_t& nodes, uint32_t& tris) {
+  float sum = 0.0f;
+  const int N = R.aoSamples;
+  for (int i = 0; i < N; i++) {
+    const int d0 = rng.dimBase + 4 * v + 4 + 2 * i;
+    const V3 dir = cosineWeightedDirection(n, rng.lds(d0), rng.lds(d0 + 1));
+    const V3 o = hit + normalize(dir) * kSurfaceThickness;
+    if (!traceAny(S, o, dir, dist, kOccAO, nodes, tris)) sum += fmaxf(dot(dir, n), 0.0f);
+  }
+  return sum / (float)N;
+}
+
+__device__ V3 lambertLights(const DevScene& S, const DevRender& R, const Rng& rng, int v, V3 hit, V3 n,
+                            uint32_t& nodes, uint32_t& tris) {
+  V3 acc = v3(0, 0, 0);
+  Shadow a;
+  a.on = false;
+  traceAreaLight(S, R, rng, v, hit, n, v3(1, 1, 1), a);
+  if (a.on && !traceAny(S, a.o, a.d, a.tmax, kOccArea, nodes, tris)) acc = acc + a.c;
+  for (int i = 0; i < S.numPointLights; i++) {
+    Shadow b;
+    b.on = false;
+    tracePointLight(S, i, hit, n, v3(1, 1, 1), b);
+    if (b.on && !traceAny(S, b.o, b.d, b.tmax, kOccPoint, nodes, tris)) acc = acc + b.c;
+  }
+  return acc + v3(R.worldR, R.worldG, R.worldB);
+}
+
+__global__ void __launch_bounds__(128) k_simple(DevScene S, DevRender R, const DevWave* __restrict__ Wp, DevQueues Q) {
+  const DevWave W = *Wp;
+  const int numPaths = W.numPixels * W.samplesInWave;
+  const int dimBase = dimBaseOf(R);
+  uint32_t nodes = 0, tris = 0;
+  for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < numPaths; p += gridDim.x * blockDim.x) {
+    int x, y;
+    uint32_t sample;
+    waveCoords(R, W, p, x, y, sample);
+    Rng rng;
+    rng.init(x, y, R.width, sample, R.seed, dimBase);
+    V3 o, d;
+    primaryRay(R, rng, x, y, o, d);
+    // tracePath through transparent surfaces, accumulating (color, weight)
+    V3 total = v3(0, 0, 0), w = v3(1, 1, 1);
+    bool eyeHit = false;
+    for (int depth = 0, v = 0; depth < R.maxDepth; depth++, v++) {
+      const ClosestHit ch = traceClosest(S, o, d, nodes, tris);
+      if (ch.prim < 0) break;
+      if (depth == 0) eyeHit = true;
+      const Hit h = loadHit(S, ch.prim, o, d, ch.t, ch.u, ch.v);
+      const DevMaterial m = S.mats[S.objMat[S.meshObj[h.mesh]]];
+      if (R.shader == 0) {
+        const V3 Ld = normalize(v3(1, 1, 1));
+        const float c = 0.1f + fmaxf(dot(Ld, h.n), 0.0f);
+        total = total + w * c;
+        break;
+      }
+      if (R.shader == 1) {
+        const float a = fminf(fmaxf(calcAO(S, R, rng, v, h.p, h.n, kRayMaxDistance, nodes, tris), 0.0f), 1.0f);
+        total = total + w * a;
+        break;
+      }
+      if (m.emission > 0.0f) {
+        total = total + w * matColor(m) * m.emission;
+        break;
+      }
+      const V3 light = lambertLights(S, R, rng, v, h.p, h.n, nodes, tris) * 0.3f;
+      V3 col;
+      float through = 0.0f;
+      if (R.shader == 2) {
+        col = light;
+        if (R.colorSampling) col = col * albedoOf(S, m, h);
+        if (m.transparency > 0.0f) {
+          col = matColor(m) * (light + v3(0.5f, 0.5f, 0.5f)) * (1.0f - m.transparency);
+          through = m.transparency;
+        }
+      } else {
+        col = light * 0.2f + light * 0.8f * calcAO(S, R, rng, v, h.p, h.n, 2.0f, nodes, tris);
+        if (R.colorSampling) col = col * albedoOf(S, m, h);
+        if (m.transparency > 0.0f) through = m.transparency;
+      }
+      total = total + w * col;
+      if (through <= 0.0f || depth + 1 >= R.maxDepth) break;
+      w = w * through;
+      o = h.p + normalize(d) * kSurfaceThickness;  // ThicknessRay(hit, inray.dir)
+    }
+    const uint32_t flags = eyeHit ? 0u : F_EYE_NOHIT;
+    Q.pathR[p] = make_float4(1, 1, 1, __uint_as_float(flags));
+    Q.pathL[p] = make_float4(total.x, total.y, total.z, 0.0f);
+  }
+  warpAddStat(&Q.stats[0], nodes);
+  warpAddStat(&Q.stats[1], tris);
+}
+
+// Per-sample clamp and accumulation into the pixel sums (rayrenderer.cpp:936-951).
+__global__ void __launch_bounds__(256) k_accumulate(DevRender R, const DevWave* __restrict__ Wp, DevQueues Q,
+                                                    float4* __restrict__ sum, float4* __restrict__ sumSq,
+                                                    int* __restrict__ cnt) {
+  const DevWave W = *Wp;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < W.numPixels; i += gridDim.x * blockDim.x) {
+    const int pixel = W.pixelList ? W.pixelList[W.pixelOffset + i] : W.pixelOffset + i;
+    float sr = 0, sg = 0, sb = 0, qr = 0, qg = 0, qb = 0;
+    for (int s = 0; s < W.samplesInWave; s++) {
+      const int p = s * W.numPixels + i;
+      const float4 l = Q.pathL[p];
+      const uint32_t flags = __float_as_uint(Q.pathR[p].w);
+      float r = l.x, g = l.y, b = l.z;
+      if ((flags & F_EYE_NOHIT) && r == 0.0f && g == 0.0f && b == 0.0f) { r = R.backR; g = R.backG; b = R.backB; }
+      r = fmaxf(r, 0.0f); g = fmaxf(g, 0.0f); b = fmaxf(b, 0.0f);
+      if (R.clampMax > 0.0f) { r = fminf(r, R.clampMax); g = fminf(g, R.clampMax); b = fminf(b, R.clampMax); }
+      sr += r; sg += g; sb += b;
+      qr += r * r; qg += g * g; qb += b * b;
+    }
+    float4 a = sum[pixel], c = sumSq[pixel];
+    a.x += sr; a.y += sg; a.z += sb;
+    c.x += qr; c.y += qg; c.z += qb;
+    sum[pixel] = a;
+    sumSq[pixel] = c;
+    cnt[pixel] += W.samplesInWave;
+  }
+}
+
+// AOV guides from the pixel-centre primary ray (rayrenderer.cpp:819-844).
+__global__ void k_aov(DevScene S, DevRender R, __half* __restrict__ normal, __half* __restrict__ albedo,
+                      __half* __restrict__ albedoA, __half* __restrict__ depth) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= R.width * R.height) return;
+  const int x = i % R.width, y = i / R.width;
+  const float dx = ((float)x + 0.5f - R.halfW) * R.viewScale;
+  const float dy = -((float)y + 0.5f - R.halfH) * R.viewScale;
+  const V3 d = normalize(v3(dx, dy, -1.0f));
+  uint32_t nodes = 0, tris = 0;
+  const ClosestHit ch = traceClosest(S, v3(0, 0, 0), d, nodes, tris);
+  if (ch.prim >= 0) {
+    const Hit h = loadHit(S, ch.prim, v3(0, 0, 0), d, ch.t, ch.u, ch.v);
+    const DevMaterial m = S.mats[S.objMat[S.meshObj[h.mesh]]];
+    normal[i * 3] = __float2half(h.n.x * 0.5f + 0.5f);
+    normal[i * 3 + 1] = __float2half(h.n.y * 0.5f + 0.5f);
+    normal[i * 3 + 2] = __float2half(h.n.z * 0.5f + 0.5f);
+    albedo[i * 3] = __float2half(m.cr);
+    albedo[i * 3 + 1] = __float2half(m.cg);
+    albedo[i * 3 + 2] = __float2half(m.cb);
+    albedoA[i] = __float2half(1.0f);
+    float dd = sqrtf(sqrtf(dot(h.p, h.p)) / R.viewFar);
+    depth[i] = __float2half(1.0f - fminf(fmaxf(dd, 0.0f), 1.0f));
+  } else {
+    normal[i * 3] = normal[i * 3 + 1] = normal[i * 3 + 2] = __float2half(0.5f);
+    albedo[i * 3] = __float2half(R.backR);
+    albedo[i * 3 + 1] = __float2half(R.backG);
+    albedo[i * 3 + 2] = __float2half(R.backB);
+    albedoA[i] = __float2half(0.0f);
+    depth[i] = __float2half(0.0f);
+  }
+}
+
+// Ray-batch queries (parity API).
+__global__ void k_queryClosest(DevScene S, const float* __restrict__ rays, int n, float* __restrict__ tuv,
+                               int* __restrict__ prim) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  uint32_t nodes = 0, tris = 0;
+  const V3 o = v3(rays[i * 6], rays[i * 6 + 1], rays[i * 6 + 2]);
+  const V3 d = v3(rays[i * 6 + 3], rays[i * 6 + 4], rays[i * 6 + 5]);
+  const ClosestHit h = traceClosest(S, o, d, nodes, tris);
+  tuv[i * 3] = h.t;
+  tuv[i * 3 + 1] = h.u;
+  tuv[i * 3 + 2] = h.v;
+  prim[i] = h.prim >= 0 ? S.triOrig[h.prim] : -1;
+}
+
+__global__ void k_queryAny(DevScene S, const float* __restrict__ rays, const float* __restrict__ tmax, int n,
+                           uint32_t occ, uint8_t* __restrict__ out) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  uint32_t nodes = 0, tris = 0;
+  const V3 o = v3(rays[i * 6], rays[i * 6 + 1], rays[i * 6 + 2]);
+  const V3 d = v3(rays[i * 6 + 3], rays[i * 6 + 4], rays[i * 6 + 5]);
+  out[i] = traceAny(S, o, d, tmax[i], occ, nodes, tris) ? 1 : 0;
+}
+
+// ------------------------------------------------------------ launchers ----
+void launchGenerate(const DevRender& R, const DevWave* W, const DevQueues& Q, int globalMedium, int grid, cudaStream_t st) {
+  k_generate<<<grid, 256, 0, st>>>(R, W, Q, globalMedium);
+}
+void launchExtend(const DevScene& S, const DevQueues& Q, int iter, int grid, cudaStream_t st) {
+  k_extend<<<grid, 128, 0, st>>>(S, Q, iter);
+}
+void launchShade(const DevScene& S, const DevRender& R, const DevWave* W, const DevQueues& Q, int iter, int grid,
+                 cudaStream_t st) {
+  k_shade<<<grid, 256, 0, st>>>(S, R, W, Q, iter);
+}
+void launchConnect(const DevScene& S, const DevQueues& Q, int iter, int which, int grid, cudaStream_t st) {
+  k_connect<<<grid, 128, 0, st>>>(S, Q, iter, which);
+}
+void launchSimple(const DevScene& S, const DevRender& R, const DevWave* W, const DevQueues& Q, int grid, cudaStream_t st) {
+  k_simple<<<grid, 128, 0, st>>>(S, R, W, Q);
+}
+void launchAccumulate(const DevRender& R, const DevWave* W, const DevQueues& Q, float4* sum, float4* sumSq, int* cnt,
+                      int grid, cudaStream_t st) {
+  k_accumulate<<<grid, 256, 0, st>>>(R, W, Q, sum, sumSq, cnt);
+}
+void launchAov(const DevScene& S, const DevRender& R, __half* normal, __half* albedo, __half* albedoA, __half* depth,
+               cudaStream_t st) {
+  const int n = R.width * R.height;
+  k_aov<<<(n + 127) / 128, 128, 0, st>>>(S, R, normal, albedo, albedoA, depth);
+}
+void launchQueryClosest(const DevScene& S, const float* rays, int n, float* tuv, int* prim, cudaStream_t st) {
+  if (n > 0) k_queryClosest<<<(n + 127) / 128, 128, 0, st>>>(S, rays, n, tuv, prim);
+}
+void launchQueryAny(const DevScene& S, const float* rays, const float* tmax, int n, uint32_t occ, uint8_t* out,
+                    cudaStream_t st) {
+  if (n > 0) k_queryAny<<<(n + 127) / 128, 128, 0, st>>>(S, rays, tmax, n, occ, out);
+}
+
+}  // namespace rg

@@ -1,0 +1,38 @@
+// rg_trace.cuh - launchers of the trace and post kernels (host-callable).
+#pragma once
+#include <cuda_fp16.h>
+#include <cuda_runtime.h>
+
+#include "rg_device.cuh"
+
+namespace rg {
+
+void launchGenerate(const DevRender& R, const DevWave* W, const DevQueues& Q, int globalMedium, int grid, cudaStream_t st);
+void launchExtend(const DevScene& S, const DevQueues& Q, int iter, int grid, cudaStream_t st);
+void launchShade(const DevScene& S, const DevRender& R, const DevWave* W, const DevQueues& Q, int iter, int grid,
+                 cudaStream_t st);
+void launchConnect(const DevScene& S, const DevQueues& Q, int iter, int which, int grid, cudaStream_t st);
+void launchSimple(const DevScene& S, const DevRender& R, const DevWave* W, const DevQueues& Q, int grid, cudaStream_t st);
+void launchAccumulate(const DevRender& R, const DevWave* W, const DevQueues& Q, float4* sum, float4* sumSq, int* cnt,
+                      int grid, cudaStream_t st);
+void launchAov(const DevScene& S, const DevRender& R, __half* normal, __half* albedo, __half* albedoA, __half* depth,
+               cudaStream_t st);
+void launchQueryClosest(const DevScene& S, const float* rays, int n, float* tuv, int* prim, cudaStream_t st);
+void launchQueryAny(const DevScene& S, const float* rays, const float* tmax, int n, uint32_t occ, uint8_t* out,
+                    cudaStream_t st);
+
+// post (rg_post.cu)
+void launchResolve(int n, const float4* sum, const int* cnt, float exposure, float4* hdr, cudaStream_t st);
+void launchDenoise(int w, int h, const float4* noisy, const __half* normal, const __half* depth, const __half* albedo,
+                   const __half* albedoA, int levels, float sigC, float sigN, float sigD, float intensity,
+                   float4* bufA, float4* bufB, float4* out, cudaStream_t st);
+void launchTonemap(int n, const float4* hdr, float4* ldr, cudaStream_t st);
+// adaptive: per-pixel relative SEM -> compacted active pixel list; returns count via *outCount (device)
+void launchAdaptivePixels(int n, const float4* sum, const float4* sumSq, const int* cnt, int target, float threshold,
+                          int* list, int* outCount, cudaStream_t st);
+void launchAdaptiveTiles(int w, int h, const float4* sum, const float4* sumSq, const int* cnt, int target,
+                         float threshold, int* list, int* outCount, cudaStream_t st);
+void launchHalfToFloat(int n, const __half* in, float* out, cudaStream_t st);
+void launchFloatToHalf(int n, const float* in, __half* out, cudaStream_t st);
+
+}  // namespace rg

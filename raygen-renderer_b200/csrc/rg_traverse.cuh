@@ -1,0 +1,183 @@
+// rg_traverse.cuh - closest-hit and any-hit traversal of the device BVH.
+//
+// Node layout (64 B, one node holds the boxes of both children so a single
+// fetch tests two boxes):
+//   n0 = (c0.lo.x, c0.hi.x, c0.lo.y, c0.hi.y)
+//   n1 = (c1.lo.x, c1.hi.x, c1.lo.y, c1.hi.y)
+//   n2 = (c0.lo.z, c0.hi.z, c1.lo.z, c1.hi.z)
+//   n3 = (ref0, ref1, -, -)  ref >= 0: inner node, ref < 0: ~((first << 3) | (count - 1))
+// Triangles (48 B, leaf order): (v1, mesh) (e1 = v2 - v1, occluder bits) (e2 = v3 - v1, -).
+//
+// The box test is the reference slab test (bvh.cpp:250-265) including its
+// reciprocal guard; the triangle tests are Moller-Trumbore exactly as
+// raycommon.cpp:151-235, evaluated without FMA contraction so hit ids, t,
+// u and v are bit-identical to the CPU restatement when both find the same
+// candidate.
+#pragma once
+#include "rg_device.cuh"
+
+namespace rg {
+
+__device__ __forceinline__ float4 ldg4(const float4* p) { return __ldg(p); }
+
+__device__ __forceinline__ V3 safeInv(V3 d) {
+  return v3(fabsf(d.x) > 1e-20f ? 1.0f / d.x : 1e30f, fabsf(d.y) > 1e-20f ? 1.0f / d.y : 1e30f,
+            fabsf(d.z) > 1e-20f ? 1.0f / d.z : 1e30f);
+}
+
+// Slab test of both children. Returns a 2-bit mask and the entry distances.
+__device__ __forceinline__ int boxPair(const float4 n0, const float4 n1, const float4 n2, V3 inv, V3 oi, float tcap,
+                                       float& t0, float& t1) {
+  const float a0 = fmaf(n0.x, inv.x, -oi.x), a1 = fmaf(n0.y, inv.x, -oi.x);
+  const float b0 = fmaf(n0.z, inv.y, -oi.y), b1 = fmaf(n0.w, inv.y, -oi.y);
+  const float c0 = fmaf(n2.x, inv.z, -oi.z), c1 = fmaf(n2.y, inv.z, -oi.z);
+  const float tmin0 = fmaxf(fmaxf(fminf(a0, a1), fminf(b0, b1)), fminf(c0, c1));
+  const float tmax0 = fminf(fminf(fmaxf(a0, a1), fmaxf(b0, b1)), fmaxf(c0, c1));
+  const float d0 = fmaf(n1.x, inv.x, -oi.x), d1 = fmaf(n1.y, inv.x, -oi.x);
+  const float e0 = fmaf(n1.z, inv.y, -oi.y), e1 = fmaf(n1.w, inv.y, -oi.y);
+  const float f0 = fmaf(n2.z, inv.z, -oi.z), f1 = fmaf(n2.w, inv.z, -oi.z);
+  const float tmin1 = fmaxf(fmaxf(fminf(d0, d1), fminf(e0, e1)), fminf(f0, f1));
+  const float tmax1 = fminf(fminf(fmaxf(d0, d1), fmaxf(e0, e1)), fmaxf(f0, f1));
+  t0 = tmin0;
+  t1 = tmin1;
+  const bool h0 = !(tmax0 < 0.0f || tmin0 > tmax0 || tmin0 > tcap);
+  const bool h1 = !(tmax1 < 0.0f || tmin1 > tmax1 || tmin1 > tcap);
+  return (h0 ? 1 : 0) | (h1 ? 2 : 0);
+}
+
+struct ClosestHit {
+  float t, u, v;
+  int prim;
+};
+
+// RenderMeshTriangle::intersectsRay(ray, info): raycommon.cpp:200-235
+__device__ __forceinline__ bool mtClosest(V3 o, V3 d, V3 p1, V3 e1, V3 e2, ClosestHit& h) {
+  const V3 pvec = cross_rn(d, e2);
+  const float det = dot_rn(e1, pvec);
+  if (fabsf(det) < 1e-8f) return false;
+  const float invDet = __fdiv_rn(1.0f, det);
+  const V3 tvec = sub_rn(o, p1);
+  const float u = __fmul_rn(dot_rn(tvec, pvec), invDet);
+  if (u < 0.0f || u > 1.0f) return false;
+  const V3 qvec = cross_rn(tvec, e1);
+  const float v = __fmul_rn(dot_rn(d, qvec), invDet);
+  if (v < 0.0f || __fadd_rn(u, v) > 1.0f) return false;
+  const float t = __fmul_rn(dot_rn(e2, qvec), invDet);
+  if (t < 0.0f) return false;
+  if (t >= h.t) return false;
+  h.t = t;
+  h.u = u;
+  h.v = v;
+  return true;
+}
+
+// RenderMeshTriangle::intersectsRay(ray, maxt, t, hit): raycommon.cpp:151-198
+__device__ __forceinline__ bool mtAny(V3 o, V3 d, V3 p1, V3 e1, V3 e2, float maxt) {
+  const V3 h = cross_rn(d, e2);
+  const float a = dot_rn(e1, h);
+  if (fabsf(a) < 1e-6f) return false;
+  const float f = __fdiv_rn(1.0f, a);
+  const V3 s = sub_rn(o, p1);
+  const float u = __fmul_rn(f, dot_rn(s, h));
+  if (u < 0.0f || u > 1.0f) return false;
+  const V3 q = cross_rn(s, e1);
+  const float v = __fmul_rn(f, dot_rn(d, q));
+  if (v < 0.0f || __fadd_rn(u, v) > 1.0f) return false;
+  const float t = __fmul_rn(f, dot_rn(e2, q));
+  return t > 1e-6f && t < maxt;
+}
+
+// Closest hit (TriangleBVH::intersectClosest, bvh.cpp:233-285). Near child
+// first by entry distance. Returns the leaf-order primitive or -1.
+__device__ __forceinline__ ClosestHit traceClosest(const DevScene& S, V3 o, V3 d, uint32_t& nodeCount,
+                                                   uint32_t& triCount) {
+  ClosestHit h;
+  h.t = kMaxRayDistance;
+  h.u = h.v = 0.0f;
+  h.prim = -1;
+  const V3 inv = safeInv(d);
+  const V3 oi = v3(o.x * inv.x, o.y * inv.y, o.z * inv.z);
+  int stack[kStackSize];
+  int sp = 0;
+  int ref = S.rootIsLeaf ? S.rootLeafRef : 0;
+  if (S.numTris == 0) return h;
+  for (;;) {
+    while (ref >= 0) {
+      const float4* np = S.nodes + (size_t)ref * 4;
+      const float4 n0 = ldg4(np), n1 = ldg4(np + 1), n2 = ldg4(np + 2), n3 = ldg4(np + 3);
+      nodeCount++;
+      float t0, t1;
+      const int m = boxPair(n0, n1, n2, inv, oi, h.t, t0, t1);
+      const int r0 = __float_as_int(n3.x), r1 = __float_as_int(n3.y);
+      if (m == 0) {
+        ref = sp > 0 ? stack[--sp] : INT_MAX;
+        if (ref == INT_MAX) break;
+      } else if (m == 3) {
+        const bool near0 = t0 <= t1;
+        if (sp < kStackSize) stack[sp++] = near0 ? r1 : r0;
+        ref = near0 ? r0 : r1;
+      } else {
+        ref = (m == 1) ? r0 : r1;
+      }
+    }
+    if (ref == INT_MAX) break;
+    // leaf
+    const int enc = ~ref;
+    const int first = enc >> 3, cnt = (enc & 7) + 1;
+    for (int i = first; i < first + cnt; i++) {
+      const float4* tp = S.triVerts + (size_t)i * 3;
+      const float4 a = ldg4(tp), b = ldg4(tp + 1), c = ldg4(tp + 2);
+      triCount++;
+      if (mtClosest(o, d, xyz(a), xyz(b), xyz(c), h)) h.prim = i;
+    }
+    if (sp == 0) break;
+    ref = stack[--sp];
+  }
+  return h;
+}
+
+// Any hit with an occluder-class predicate (TriangleBVH::intersectAny, bvh.h:63-101).
+__device__ __forceinline__ bool traceAny(const DevScene& S, V3 o, V3 d, float maxT, uint32_t occMask,
+                                         uint32_t& nodeCount, uint32_t& triCount) {
+  if (S.numTris == 0) return false;
+  const V3 inv = safeInv(d);
+  const V3 oi = v3(o.x * inv.x, o.y * inv.y, o.z * inv.z);
+  int stack[kStackSize];
+  int sp = 0;
+  int ref = S.rootIsLeaf ? S.rootLeafRef : 0;
+  for (;;) {
+    while (ref >= 0) {
+      const float4* np = S.nodes + (size_t)ref * 4;
+      const float4 n0 = ldg4(np), n1 = ldg4(np + 1), n2 = ldg4(np + 2), n3 = ldg4(np + 3);
+      nodeCount++;
+      float t0, t1;
+      const int m = boxPair(n0, n1, n2, inv, oi, maxT, t0, t1);
+      const int r0 = __float_as_int(n3.x), r1 = __float_as_int(n3.y);
+      if (m == 0) {
+        ref = sp > 0 ? stack[--sp] : INT_MAX;
+        if (ref == INT_MAX) break;
+      } else if (m == 3) {
+        if (sp < kStackSize) stack[sp++] = r1;
+        ref = r0;
+      } else {
+        ref = (m == 1) ? r0 : r1;
+      }
+    }
+    if (ref == INT_MAX) break;
+    const int enc = ~ref;
+    const int first = enc >> 3, cnt = (enc & 7) + 1;
+    for (int i = first; i < first + cnt; i++) {
+      const float4* tp = S.triVerts + (size_t)i * 3;
+      const float4 b = ldg4(tp + 1);
+      if (!(__float_as_uint(b.w) & occMask)) continue;
+      const float4 a = ldg4(tp), c = ldg4(tp + 2);
+      triCount++;
+      if (mtAny(o, d, xyz(a), xyz(b), xyz(c), maxT)) return true;
+    }
+    if (sp == 0) break;
+    ref = stack[--sp];
+  }
+  return false;
+}
+
+}  // namespace rg

@@ -1,0 +1,117 @@
+"""Small analytic scenes for known-answer and parity tests (built from arrays)."""
+import math
+
+import numpy as np
+
+
+def material(rg, color=(0.8, 0.8, 0.8), emission=0.0, glossy=0.0, roughness=0.5, metallic=0.0,
+             refraction=0.0, ior=1.45, transparency=0.0):
+    m = rg.rg_material()
+    for i in range(3):
+        m.color[i] = color[i]
+    m.diffuse = 0.8
+    m.glossy = glossy
+    m.roughness = roughness
+    m.metallic = metallic
+    m.refraction = refraction
+    m.refraction_ratio = ior
+    m.transparency = transparency
+    m.emission = emission
+    m.texture = -1
+    m.tex_tiling[0] = m.tex_tiling[1] = 1.0
+    return m
+
+
+def camera(rg, loc=(0, 0, 0), fov=40.0):
+    c = rg.rg_camera()
+    for i in range(3):
+        c.location[i] = loc[i]
+        c.angle[i] = 0.0
+    c.field_of_view = fov
+    c.view_near = 0.1
+    c.view_far = 50.0
+    c.depth_of_field = 0.0
+    c.aperture = 1.8
+    c.aperture_blades = 0
+    c.exposure = 1.0
+    return c
+
+
+def quad_z(z, half, facing):
+    """Axis-aligned square in the plane z, normal +z (facing=+1) or -z (facing=-1)."""
+    a, b, c, d = (-half, -half, z), (half, -half, z), (half, half, z), (-half, half, z)
+    if facing < 0:
+        b, d = d, b
+    n = (0.0, 0.0, float(facing))
+    tris = [a + b + c, a + c + d]
+    return np.array(tris, np.float32), np.array([n * 3, n * 3], np.float32)
+
+
+def build(rg, parts, cam, media=(), global_medium=-1):
+    """parts: list of (positions n x 9, normals n x 9, rg_material, interior_medium)."""
+    pos, nrm, tri_mesh, mesh_obj, objs, mats = [], [], [], [], [], []
+    for k, (p, n, m, med) in enumerate(parts):
+        pos.append(p)
+        nrm.append(n)
+        tri_mesh += [k] * len(p)
+        mesh_obj.append(k)
+        o = rg.rg_object()
+        o.material = k
+        o.interior_medium = med
+        objs.append(o)
+        mats.append(m)
+    return rg.Scene.from_arrays(np.concatenate(pos), np.concatenate(nrm), tri_mesh, mesh_obj, objs, mats, cam,
+                                media=media, global_medium=global_medium)
+
+
+def form_factor_centered_square(half, h):
+    """Point-to-parallel-square form factor, point below the centre (four corner rectangles)."""
+    X = Y = half / h
+    f = (X / math.sqrt(1 + X * X) * math.atan(Y / math.sqrt(1 + X * X))
+         + Y / math.sqrt(1 + Y * Y) * math.atan(X / math.sqrt(1 + Y * Y))) / (2 * math.pi)
+    return 4.0 * f
+
+
+def lit_floor_scene(rg, albedo=0.5, le=2.0, half=3.0, h=3.0):
+    """Diffuse floor at z=-2 facing +z under an emitter at z=-2+h facing -z; camera at z=0 looking -z."""
+    fp, fn = quad_z(-2.0, 50.0, +1)
+    lp, ln = quad_z(-2.0 + h, half, -1)
+    parts = [(fp, fn, material(rg, (albedo,) * 3), -1), (lp, ln, material(rg, (1, 1, 1), emission=le), -1)]
+    return build(rg, parts, camera(rg, fov=1.0)), albedo * le * form_factor_centered_square(half, h)
+
+
+def mirror_scene(rg, le=3.0):
+    """Smooth metal mirror (F0 = 1) at z=-2 reflecting an emitter at z=+3 facing -z."""
+    mp, mn = quad_z(-2.0, 10.0, +1)
+    lp, ln = quad_z(3.0, 10.0, -1)
+    parts = [(mp, mn, material(rg, (1, 1, 1), glossy=1.0, metallic=1.0, roughness=0.0), -1),
+             (lp, ln, material(rg, (1, 1, 1), emission=le), -1)]
+    return build(rg, parts, camera(rg, fov=10.0)), le
+
+
+def absorber_scene(rg, sigma_a=0.1, d=5.0, le=2.0):
+    """Emitter at z=-d facing +z seen through a purely absorbing global medium."""
+    lp, ln = quad_z(-d, 50.0, +1)
+    med = rg.rg_medium()
+    for i in range(3):
+        med.sigma_a[i] = sigma_a
+        med.sigma_s[i] = 0.0
+        med.sigma_e[i] = 0.0
+    med.g = 0.0
+    med.density = 1.0
+    parts = [(lp, ln, material(rg, (1, 1, 1), emission=le), -1)]
+    return build(rg, parts, camera(rg, fov=1.0), media=[med], global_medium=0), le * math.exp(-sigma_a * d)
+
+
+def random_rays(scene_bounds, n, seed, camera_fraction=0.5, camera=(0, 0, 0)):
+    """Rays in view space: a mix of camera rays and rays from random interior points."""
+    rng = np.random.default_rng(seed)
+    lo, hi = np.asarray(scene_bounds[0], np.float32), np.asarray(scene_bounds[1], np.float32)
+    nc = int(n * camera_fraction)
+    o = np.empty((n, 3), np.float32)
+    o[:nc] = camera
+    o[nc:] = lo + (hi - lo) * rng.random((n - nc, 3), dtype=np.float32)
+    d = rng.normal(size=(n, 3)).astype(np.float32)
+    d[:nc, 2] = -np.abs(d[:nc, 2]) - 1.0
+    d /= np.linalg.norm(d, axis=1, keepdims=True)
+    return np.concatenate([o, d], axis=1).astype(np.float32)

@@ -1,0 +1,193 @@
+"""Device tracer vs CPU oracle, through the C ABI (needs a B200).
+
+Tolerances (from the tracer's specification):
+* ray batches: hit triangle ids bit-identical except exact ties / edge grazes
+  (< 0.1% of rays), t, u, v within 1e-5 relative;
+* images: per-pixel mean within the Monte-Carlo error -- |z| = |gpu - oracle| /
+  sqrt(sem_gpu^2 + sem_oracle^2); mean |z| ~ 0.8 and < 0.5% of channels above 4;
+* deterministic passes (A-Trous, tonemap): 1e-4 relative + 1e-6 absolute.
+"""
+import numpy as np
+import pytest
+
+import scenes
+
+pytestmark = pytest.mark.gpu
+
+
+def render_gpu(rg, scene, W, H, spp, **kw):
+    st = rg.RendererSettings(resolutionWidth=W, resolutionHeight=H, samples=spp, **kw)
+    r = rg.RayRenderer(st)
+    r.set_scene(scene)
+    r.render()
+    return r
+
+
+def image_parity(rg, orc, scene, W, H, spp, **kw):
+    oracle_kw = dict(max_depth=kw.get("maxDepth", 32), rr_depth=kw.get("rrDepth", 3), seed=kw.get("seed", 1),
+                     firefly_clamp=kw.get("fireflyClamp", 10.0), shader=kw.get("shaderProvider", 5))
+    ref = orc.OracleScene(scene.ptr).render(W, H, spp, **oracle_kw)
+    r = render_gpu(rg, scene, W, H, spp, **kw)
+    g = r.get_hdr_result()[..., :3].astype(np.float64)
+    n = ref["n"][..., None].astype(np.float64)
+    m2 = ref["sum"] / n
+    v2 = np.maximum(ref["sumsq"] / n - m2 * m2, 0.0)
+    # same sample sequence on both sides -> compare against the oracle's own SEM (x sqrt2 for two estimates)
+    se = np.sqrt(2.0 * v2 / n)
+    z = np.abs(g - m2) / np.maximum(se, 1e-6)
+    z[(se < 1e-6) & (np.abs(g - m2) < 1e-4)] = 0.0
+    stats = r.stats()
+    r.close()
+    return z, g, m2, stats
+
+
+def check_z(z, g, m, label, tail=0.005):
+    frac = float((z > 4.0).mean())
+    rel = abs(g.mean() - m.mean()) / max(m.mean(), 1e-9)
+    assert frac < tail, f"{label}: {frac:.4f} of channels beyond 4 sigma"
+    assert rel < 0.01, f"{label}: image mean differs by {rel:.4f}"
+
+
+# ----------------------------------------------------------------- ray batches
+@pytest.mark.parametrize("kind,params", [(1, None), (2, [20000]), (4, [100000, 8])])
+def test_closest_hit_parity(rg, orc, kind, params):
+    sc = rg.Scene.builtin(kind, 3, params)
+    r = rg.RayRenderer(rg.RendererSettings(resolutionWidth=8, resolutionHeight=8, samples=1))
+    r.set_scene(sc)
+    o = orc.OracleScene(sc.ptr)
+    bounds = ((-5, -5, -20), (5, 5, -1)) if kind == 1 else ((-9, -4.9, -19), (9, 4.9, -1))
+    rays = scenes.random_rays(bounds, 50000, kind)
+    tg, pg = r.trace_closest(rays)
+    to, po = o.closest(rays)
+    same = pg == po
+    assert same.mean() > 0.999, same.mean()
+    hit = same & (po >= 0)
+    assert hit.mean() > 0.5
+    np.testing.assert_allclose(tg[hit], to[hit], rtol=1e-5, atol=1e-7)
+    # non-matching ids must be genuine ties: same t within 1e-5
+    diff = ~same
+    if diff.any():
+        np.testing.assert_allclose(tg[diff, 0], to[diff, 0], rtol=1e-5)
+    r.close()
+
+
+def test_any_hit_parity(rg, orc):
+    sc = rg.Scene.builtin(2, 4, [20000])
+    r = rg.RayRenderer(rg.RendererSettings(resolutionWidth=8, resolutionHeight=8, samples=1))
+    r.set_scene(sc)
+    o = orc.OracleScene(sc.ptr)
+    rays = scenes.random_rays(((-9, -4.9, -19), (9, 4.9, -1)), 40000, 9)
+    rng = np.random.default_rng(2)
+    tmax = rng.uniform(0.1, 20.0, len(rays)).astype(np.float32)
+    for pred in (0, 1, 2, 3):
+        a = r.trace_any(rays, tmax, pred)
+        b = o.any(rays, tmax, pred)
+        assert (a == b).mean() > 0.999, pred
+    r.close()
+
+
+# ----------------------------------------------------------------- images
+def test_cube_room_image_parity(rg, orc):
+    sc = rg.Scene.builtin(1, 1)
+    z, g, m, stats = image_parity(rg, orc, sc, 64, 64, 64, maxDepth=5, rrDepth=3, seed=1)
+    check_z(z, g, m, "cube room")
+    assert stats["kernel_launches"] > 0 and stats["closest_rays"] > 64 * 64 * 64
+
+
+def test_glossy_dielectric_image_parity(rg, orc):
+    sc = rg.Scene.builtin(2, 5, [20000])
+    z, g, m, _ = image_parity(rg, orc, sc, 48, 27, 128, maxDepth=8, rrDepth=3, seed=2)
+    check_z(z, g, m, "metal/dielectric spheres", tail=0.01)
+
+
+def test_medium_image_parity(rg, orc):
+    sc = rg.Scene.builtin(3, 5, [5000])
+    z, g, m, _ = image_parity(rg, orc, sc, 32, 18, 256, maxDepth=8, rrDepth=3, seed=4)
+    check_z(z, g, m, "homogeneous medium", tail=0.01)
+
+
+@pytest.mark.parametrize("shader", [0, 1, 2, 3])
+def test_simple_shaders_parity(rg, orc, shader):
+    sc = rg.Scene.builtin(1, 1)
+    spp = 8 if shader in (1, 3) else 32
+    z, g, m, _ = image_parity(rg, orc, sc, 32, 32, spp, shaderProvider=shader, maxDepth=5)
+    check_z(z, g, m, f"shader {shader}")
+
+
+def test_known_answers_on_device(rg):
+    sc, expected = scenes.lit_floor_scene(rg)
+    r = render_gpu(rg, sc, 32, 32, 64, maxDepth=4, fireflyClamp=0.0)
+    assert np.allclose(r.get_hdr_result()[..., :3].mean(axis=(0, 1)), expected, rtol=0.01)
+    sc, expected = scenes.mirror_scene(rg)
+    r = render_gpu(rg, sc, 16, 16, 4, maxDepth=4, fireflyClamp=0.0)
+    assert np.allclose(r.get_hdr_result()[..., :3], expected, rtol=1e-5)
+    sc, expected = scenes.absorber_scene(rg)
+    r = render_gpu(rg, sc, 32, 32, 64, maxDepth=4, fireflyClamp=0.0)
+    assert np.allclose(r.get_hdr_result()[..., :3].mean(axis=(0, 1)), expected, rtol=0.01)
+
+
+def test_adaptive_sampling_parity(rg, orc):
+    sc = rg.Scene.builtin(1, 1)
+    for mode in (0, 1):
+        ref = orc.OracleScene(sc.ptr).render(64, 64, 64, max_depth=5, adaptive=True, adaptive_base=8,
+                                             adaptive_mode=mode, adaptive_threshold=0.05)
+        r = render_gpu(rg, sc, 64, 64, 64, maxDepth=5, enableAdaptiveSampling=True, adaptiveBaseSamples=8,
+                       adaptiveMode=mode, adaptiveThreshold=0.05)
+        cg = r.get_sample_counts()
+        assert (cg == ref["n"]).mean() > 0.97, mode
+        assert abs(cg.sum() - ref["n"].sum()) / ref["n"].sum() < 0.03
+        g = r.get_hdr_result()[..., :3]
+        m = ref["sum"] / ref["n"][..., None]
+        assert abs(g.mean() - m.mean()) / m.mean() < 0.01
+        r.close()
+
+
+def test_determinism_and_errors(rg):
+    sc = rg.Scene.builtin(1, 1)
+    a = render_gpu(rg, sc, 32, 32, 8, maxDepth=5)
+    b = render_gpu(rg, sc, 32, 32, 8, maxDepth=5)
+    assert np.array_equal(a.get_hdr_result(), b.get_hdr_result())
+    st = rg.RendererSettings(resolutionWidth=16, resolutionHeight=16, samples=1, shaderProvider=4)
+    r = rg.RayRenderer(st)
+    r.set_scene(sc)
+    with pytest.raises(rg.RayGenError) as e:
+        r.render()
+    assert e.value.code == rg.RG_ERR_UNSUPPORTED
+    r2 = rg.RayRenderer(rg.RendererSettings(resolutionWidth=16, resolutionHeight=16, samples=1))
+    with pytest.raises(rg.RayGenError) as e:
+        r2.render()
+    assert e.value.code == rg.RG_ERR_NO_SCENE
+
+
+# ----------------------------------------------------------------- post
+def test_atrous_parity(rg, orc):
+    rng = np.random.default_rng(5)
+    h, w = 64, 80
+    color = (rng.random((h, w, 3)) * 2).astype(np.float32)
+    color[10, 10] = 50.0  # firefly
+    q = lambda a: a.astype(np.float16).astype(np.float32)  # guides are stored in FP16 on the device
+    normal = q(rng.random((h, w, 3)).astype(np.float32) * 0.2 + 0.4)
+    depth = q(rng.random((h, w)).astype(np.float32))
+    albedo = q(rng.random((h, w, 3)).astype(np.float32))
+    alpha = (rng.random((h, w)) > 0.1).astype(np.float32)
+    a = rg.denoise_atrous(color, normal, depth, albedo, alpha)
+    b = orc.denoise(color, normal, depth, albedo, alpha)
+    np.testing.assert_allclose(a, b, rtol=1e-4, atol=1e-6)
+
+
+def test_tonemap_parity(rg, orc):
+    rng = np.random.default_rng(6)
+    hdr = np.concatenate([rng.random((32, 32, 3)) * 20, np.ones((32, 32, 1))], axis=2).astype(np.float32)
+    np.testing.assert_allclose(rg.tonemap(hdr), orc.tonemap(hdr), rtol=1e-5, atol=1e-6)
+
+
+def test_denoised_render_matches_oracle(rg, orc):
+    sc = rg.Scene.builtin(1, 1)
+    W = H = 48
+    ref = orc.OracleScene(sc.ptr).render(W, H, 16, max_depth=5, denoise=True)
+    r = render_gpu(rg, sc, W, H, 16, maxDepth=5, enableDenoise=True)
+    n, a, d = r.get_aovs()
+    assert np.allclose(n, ref["normal"], atol=2e-3)
+    assert np.allclose(a, ref["albedo"], atol=2e-3)
+    g = r.get_hdr_result()[..., :3]
+    assert abs(g.mean() - ref["hdr"][..., :3].mean()) / ref["hdr"][..., :3].mean() < 0.02

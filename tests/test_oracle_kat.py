@@ -1,0 +1,149 @@
+"""Known-answer tests that pin the CPU oracle (no GPU).
+
+The reference ships no tests or golden outputs, so the oracle is pinned by
+analytic answers: the LDS stratification, a Lambertian floor under a square
+emitter (form factor), a smooth mirror, Beer-Lambert absorption, the
+Henyey-Greenstein normalisation, BVH-vs-brute-force closest hits, and the
+tonemap / A-Trous identities.
+"""
+import math
+
+import numpy as np
+import pytest
+
+import scenes
+
+
+def test_lds_dimension0_is_stratified(orc):
+    # Halton base 2 (indices 1..1023 sit on the k/1024 lattice) with a constant
+    # per-(pixel, dim) rotation: every sample lands in its own 1/1024 cell
+    v = np.array([orc.lds(5, 7, 64, s, 1, 0) for s in range(1023)])
+    assert ((v >= 0) & (v < 1)).all()
+    cells = np.floor(v * 1024).astype(int)
+    assert len(set(cells.tolist())) == 1023
+
+
+def test_lds_seed1_matches_unsalted_reference_scramble(orc):
+    # dim 0, sample 0: radicalInverse(1, 2) = 0.5 plus the Cranley-Patterson offset of
+    # hashPixel(0, 0, hashPixel(x, y, 0)) (raycommon.cpp:35-87)
+    def hp(x, y, salt):
+        m = 0xFFFFFFFF
+        v = ((x * 73856093) & m) ^ ((y * 19349663) & m) ^ ((salt * 83492791) & m)
+        v ^= v >> 16; v = (v * 0x7feb352d) & m
+        v ^= v >> 15; v = (v * 0x846ca68b) & m
+        v ^= v >> 16
+        return v
+    scr = hp(3, 4, 0)
+    off = (hp(0, 0, scr) >> 8) / float(1 << 24)
+    w = 0.5 + off
+    if w >= 1.0:
+        w -= 1.0
+    assert abs(orc.lds(3, 4, 16, 0, 1, 0) - w) < 1e-7
+
+
+def test_prng_uniform(orc):
+    u = np.array([orc.prng(x, 0, 64, s, 1, 2, 6) for x in range(32) for s in range(128)])
+    hist, _ = np.histogram(u, bins=16, range=(0, 1))
+    chi2 = ((hist - len(u) / 16) ** 2 / (len(u) / 16)).sum()
+    assert chi2 < 40.0  # 15 dof, p ~ 5e-4
+
+
+@pytest.mark.parametrize("g", [0.0, 0.3, -0.5, 0.8])
+def test_hg_phase_normalised(orc, g):
+    lib = orc.load()
+    c = np.linspace(-1, 1, 20001)
+    p = np.array([lib.orc_phase_pdf(g, float(x)) for x in c])
+    integral = 2 * math.pi * np.trapezoid(p, c)
+    assert abs(integral - 1.0) < 2e-3
+
+
+def test_hg_sampling_matches_pdf(orc):
+    import ctypes as C
+    lib = orc.load()
+    g = 0.3
+    rng = np.random.default_rng(0)
+    out = (C.c_float * 3)()
+    cos = []
+    for u1, u2 in rng.random((20000, 2)):
+        lib.orc_sample_phase(g, float(u1), float(u2), out)
+        cos.append(out[2])
+    mean = np.mean(cos)
+    assert abs(mean - g) < 0.015  # E[cos theta] of HG = g
+
+
+def test_lambert_floor_form_factor(rg, orc):
+    sc, expected = scenes.lit_floor_scene(rg)
+    o = orc.OracleScene(sc.ptr)
+    out = o.render(32, 32, 64, max_depth=4, firefly_clamp=0.0)
+    mean = out["sum"].sum(axis=(0, 1)) / out["n"].sum()
+    assert np.allclose(mean, expected, rtol=0.01), (mean, expected)
+
+
+def test_smooth_mirror_returns_emitter_radiance(rg, orc):
+    sc, expected = scenes.mirror_scene(rg)
+    o = orc.OracleScene(sc.ptr)
+    out = o.render(16, 16, 4, max_depth=4, firefly_clamp=0.0)
+    m = out["sum"] / out["n"][..., None]
+    assert np.allclose(m, expected, rtol=1e-5)
+
+
+def test_beer_lambert_absorption(rg, orc):
+    sc, expected = scenes.absorber_scene(rg)
+    o = orc.OracleScene(sc.ptr)
+    out = o.render(32, 32, 64, max_depth=4, firefly_clamp=0.0)
+    mean = out["sum"].sum(axis=(0, 1)) / out["n"].sum()
+    assert np.allclose(mean, expected, rtol=0.01), (mean, expected)
+
+
+def test_bvh_closest_equals_brute_force(rg, orc):
+    for kind, params in ((1, None), (4, [3000, 3])):
+        sc = rg.Scene.builtin(kind, 5, params)
+        o = orc.OracleScene(sc.ptr)
+        rays = scenes.random_rays(((-5, -5, -20), (5, 5, -1)), 4000, 1)
+        t1, p1 = o.closest(rays)
+        t2, p2 = o.closest(rays, brute=True)
+        same = p1 == p2
+        assert same.mean() > 0.999
+        assert np.allclose(t1[same], t2[same], rtol=1e-6)
+        o.close()
+        sc.close()
+
+
+def test_tree_and_select_mix_agree(rg, orc):
+    """Stochastic lobe selection has the mean of the reference's lobe sum (bsdf.cpp:579-610)."""
+    sc = rg.Scene.builtin(4, 11, [800, 2])
+    d = sc.desc
+    # make the sphere a 3-lobe mix
+    m = d.materials[d.num_materials - 1]
+    m.glossy, m.refraction, m.roughness, m.metallic = 0.3, 0.2, 0.3, 0.0
+    o = orc.OracleScene(sc.ptr)
+    a = o.render(24, 16, 256, max_depth=5, mix_tree=False, seed=3)
+    b = o.render(24, 16, 64, max_depth=5, mix_tree=True, seed=4)
+    ma = a["sum"].sum() / a["n"].sum()
+    mb = b["sum"].sum() / b["n"].sum()
+    assert abs(ma - mb) / mb < 0.05, (ma, mb)
+
+
+def test_tonemap_known_values(orc):
+    hdr = np.array([[[0, 0, 0, 1], [1, 1, 1, 1], [10, 0, 0, 1], [0.5, 0.25, 0.1, 1]]], np.float32)
+    ldr = orc.tonemap(hdr)
+    L = 1.0
+    assert np.allclose(ldr[0, 0], [0, 0, 0, 1])
+    assert np.allclose(ldr[0, 1, :3], (L / (L + 1)) ** (1 / 2.2), rtol=1e-6)
+    assert np.allclose(ldr[0, 2, :3], [1, 0, 0], atol=1e-6)  # hue-preserving peak clip
+
+
+def test_atrous_identities(orc):
+    rng = np.random.default_rng(0)
+    h, w = 24, 32
+    normal = np.full((h, w, 3), 0.5, np.float32)
+    normal[..., 2] = 1.0
+    depth = np.full((h, w), 0.5, np.float32)
+    albedo = np.full((h, w, 3), 0.7, np.float32)
+    alpha = np.ones((h, w), np.float32)
+    const = np.full((h, w, 3), 0.4, np.float32)
+    out = orc.denoise(const, normal, depth, albedo, alpha)
+    assert np.allclose(out, const, rtol=1e-5)
+    noisy = rng.random((h, w, 3)).astype(np.float32)
+    passthrough = orc.denoise(noisy, normal, depth, albedo, alpha, intensity=0.0)
+    assert np.allclose(passthrough, noisy)
