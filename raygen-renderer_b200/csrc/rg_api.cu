@@ -575,6 +575,9 @@ rg_status rg_set_scene(rg_handle* h, const rg_scene_desc* d) {
   S.points = ds.points.p;
   S.textures = ds.textures.p;
   S.numTextures = ds.numTextures;
+  if (!h->error.alloc(1)) return RG_ERR_OUT_OF_MEMORY;
+  cudaMemsetAsync(h->error.p, 0, sizeof(int), st);
+  S.error = h->error.p;
   h->hasScene = true;
   if (h->graph) {
     cudaGraphExecDestroy(h->graph);
@@ -901,7 +904,13 @@ rg_status rg_trace_closest(rg_handle* h, const float* rays, int32_t n, float* ou
   launchQueryClosest(h->dscene, r.p, n, t.p, p.p, h->stream);
   RG_CUDA_CHECK(cudaMemcpyAsync(out_tuv, t.p, sizeof(float) * n * 3, cudaMemcpyDeviceToHost, h->stream));
   RG_CUDA_CHECK(cudaMemcpyAsync(out_prim, p.p, sizeof(int) * n, cudaMemcpyDeviceToHost, h->stream));
+  int derr = 0;
+  RG_CUDA_CHECK(cudaMemcpyAsync(&derr, h->error.p, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
   RG_CUDA_CHECK(cudaStreamSynchronize(h->stream));
+  if (derr) {
+    setLastError("device error flag raised: " + std::to_string(derr));
+    return RG_ERR_DEVICE_STATUS;
+  }
   return RG_OK;
 }
 
@@ -916,7 +925,13 @@ rg_status rg_trace_any(rg_handle* h, const float* rays, const float* tmax, int32
   const uint32_t occ = predicate == 0 ? kOccArea : (predicate == 1 ? kOccPoint : (predicate == 2 ? kOccAO : kOccAll));
   launchQueryAny(h->dscene, r.p, tm.p, n, occ, o.p, h->stream);
   RG_CUDA_CHECK(cudaMemcpyAsync(out, o.p, n, cudaMemcpyDeviceToHost, h->stream));
+  int derr = 0;
+  RG_CUDA_CHECK(cudaMemcpyAsync(&derr, h->error.p, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
   RG_CUDA_CHECK(cudaStreamSynchronize(h->stream));
+  if (derr) {
+    setLastError("device error flag raised: " + std::to_string(derr));
+    return RG_ERR_DEVICE_STATUS;
+  }
   return RG_OK;
 }
 

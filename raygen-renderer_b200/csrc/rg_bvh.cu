@@ -372,7 +372,7 @@ __global__ void k_split(int numTasks, const int* __restrict__ tasks, BNode* node
 // Scatter the primitives of split nodes to their children (warp-aggregated).
 __global__ void k_partition(int n, const int* __restrict__ primIdx, const int* __restrict__ primNode,
                             BNode* nodes, const float4* __restrict__ bmin, const float4* __restrict__ bmax,
-                            int* __restrict__ outIdx, int* __restrict__ outNode, int nbins) {
+                            int* __restrict__ outIdx, int* __restrict__ outNode, int nbins, int* err) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   const bool inRange = i < n;
   const int node = inRange ? primNode[i] : -1;
@@ -402,10 +402,12 @@ __global__ void k_partition(int n, const int* __restrict__ primIdx, const int* _
     int base = 0;
     if ((int)(threadIdx.x & 31) == leader) base = atomicAdd(&nodes[node].fill[side], __popc(grp));
     base = __shfl_sync(grp, base, leader);
-    pos = nodes[child].start + base + rank;
+    if (base + rank < nodes[child].count) pos = nodes[child].start + base + rank;
+    else atomicCAS(err, 0, kErrPartition);
   }
   if (!inRange) return;
   if (child >= 0) {
+    if (pos < 0) return;
     outIdx[pos] = p;
     outNode[pos] = nodes[child].count > 4 ? child : -1;
   } else {
@@ -503,7 +505,7 @@ rg_status buildDeviceBvh(DeviceScene& ds, int nbins, cudaStream_t st, std::strin
   }
   const int rootOpen = n > 4 ? 1 : 0;
   k_initRoot<<<gridFor(n, 256), 256, 0, st>>>(n, rb.p, nodes.p, idxA.p, nodeA.p, rootOpen);
-  int h_counters[4] = {1, 0, 0, 0};  // [0] node count, [1] next task count
+  int h_counters[4] = {1, 0, 0, 0};  // [0] node count, [1] next task count, [2] error
   cudaMemcpyAsync(counters.p, h_counters, sizeof(h_counters), cudaMemcpyHostToDevice, st);
   int numTasks = rootOpen;
   {
@@ -528,7 +530,8 @@ rg_status buildDeviceBvh(DeviceScene& ds, int nbins, cudaStream_t st, std::strin
       k_split<<<gridFor(nt, 128), 128, 0, st>>>(nt, curTasks + c0, nodes.p, bins.p, nbins, counters.p, nxtTasks,
                                                  counters.p + 1);
     }
-    k_partition<<<gridFor(n, 256), 256, 0, st>>>(n, curIdx, curNode, nodes.p, lo.p, hi.p, altIdx, altNode, nbins);
+    k_partition<<<gridFor(n, 256), 256, 0, st>>>(n, curIdx, curNode, nodes.p, lo.p, hi.p, altIdx, altNode, nbins,
+                                                 counters.p + 2);
     std::swap(curIdx, altIdx);
     std::swap(curNode, altNode);
     std::swap(curTasks, nxtTasks);
@@ -542,9 +545,14 @@ rg_status buildDeviceBvh(DeviceScene& ds, int nbins, cudaStream_t st, std::strin
       return RG_ERR_DEVICE_STATUS;
     }
   }
-  int numNodes = 0;
+  int numNodes = 0, buildErr = 0;
   cudaMemcpyAsync(&numNodes, counters.p, sizeof(int), cudaMemcpyDeviceToHost, st);
+  cudaMemcpyAsync(&buildErr, counters.p + 2, sizeof(int), cudaMemcpyDeviceToHost, st);
   cudaStreamSynchronize(st);
+  if (buildErr != 0) {
+    err = "BVH build scatter error " + std::to_string(buildErr);
+    return RG_ERR_DEVICE_STATUS;
+  }
   ds.buildLevels = levels;
   // traversal layout
   DevBuf<int> flags, trav;

@@ -80,7 +80,15 @@ struct DevScene {
   const DevPointLight* points;
   const DevTexture* textures;
   int numTextures;
+  int* error;                 // device error word (first error code wins)
 };
+
+// device error codes
+constexpr int kErrTraversalSteps = 1;   // traversal exceeded its step bound
+constexpr int kErrStackOverflow = 2;    // traversal stack full
+constexpr int kErrLeafRange = 3;        // leaf outside the triangle array
+constexpr int kErrPartition = 4;        // BVH build scatter outside a child range
+constexpr int kMaxTraversalSteps = 1 << 22;
 
 // Render-wide constants for the trace kernels.
 struct DevRender {

@@ -101,8 +101,13 @@ __device__ __forceinline__ ClosestHit traceClosest(const DevScene& S, V3 o, V3 d
   int sp = 0;
   int ref = S.rootIsLeaf ? S.rootLeafRef : 0;
   if (S.numTris == 0) return h;
+  int steps = 0;
   for (;;) {
     while (ref >= 0) {
+      if (++steps > kMaxTraversalSteps || ref >= S.numNodes) {
+        atomicCAS(S.error, 0, kErrTraversalSteps);
+        return h;
+      }
       const float4* np = S.nodes + (size_t)ref * 4;
       const float4 n0 = ldg4(np), n1 = ldg4(np + 1), n2 = ldg4(np + 2), n3 = ldg4(np + 3);
       nodeCount++;
@@ -115,6 +120,7 @@ __device__ __forceinline__ ClosestHit traceClosest(const DevScene& S, V3 o, V3 d
       } else if (m == 3) {
         const bool near0 = t0 <= t1;
         if (sp < kStackSize) stack[sp++] = near0 ? r1 : r0;
+        else atomicCAS(S.error, 0, kErrStackOverflow);
         ref = near0 ? r0 : r1;
       } else {
         ref = (m == 1) ? r0 : r1;
@@ -124,6 +130,10 @@ __device__ __forceinline__ ClosestHit traceClosest(const DevScene& S, V3 o, V3 d
     // leaf
     const int enc = ~ref;
     const int first = enc >> 3, cnt = (enc & 7) + 1;
+    if (first + cnt > S.numTris) {
+      atomicCAS(S.error, 0, kErrLeafRange);
+      return h;
+    }
     for (int i = first; i < first + cnt; i++) {
       const float4* tp = S.triVerts + (size_t)i * 3;
       const float4 a = ldg4(tp), b = ldg4(tp + 1), c = ldg4(tp + 2);
@@ -145,8 +155,13 @@ __device__ __forceinline__ bool traceAny(const DevScene& S, V3 o, V3 d, float ma
   int stack[kStackSize];
   int sp = 0;
   int ref = S.rootIsLeaf ? S.rootLeafRef : 0;
+  int steps = 0;
   for (;;) {
     while (ref >= 0) {
+      if (++steps > kMaxTraversalSteps || ref >= S.numNodes) {
+        atomicCAS(S.error, 0, kErrTraversalSteps);
+        return false;
+      }
       const float4* np = S.nodes + (size_t)ref * 4;
       const float4 n0 = ldg4(np), n1 = ldg4(np + 1), n2 = ldg4(np + 2), n3 = ldg4(np + 3);
       nodeCount++;
@@ -158,6 +173,7 @@ __device__ __forceinline__ bool traceAny(const DevScene& S, V3 o, V3 d, float ma
         if (ref == INT_MAX) break;
       } else if (m == 3) {
         if (sp < kStackSize) stack[sp++] = r1;
+        else atomicCAS(S.error, 0, kErrStackOverflow);
         ref = r0;
       } else {
         ref = (m == 1) ? r0 : r1;
@@ -166,6 +182,10 @@ __device__ __forceinline__ bool traceAny(const DevScene& S, V3 o, V3 d, float ma
     if (ref == INT_MAX) break;
     const int enc = ~ref;
     const int first = enc >> 3, cnt = (enc & 7) + 1;
+    if (first + cnt > S.numTris) {
+      atomicCAS(S.error, 0, kErrLeafRange);
+      return false;
+    }
     for (int i = first; i < first + cnt; i++) {
       const float4* tp = S.triVerts + (size_t)i * 3;
       const float4 b = ldg4(tp + 1);

