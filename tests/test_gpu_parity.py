@@ -194,3 +194,16 @@ def test_denoised_render_matches_oracle(rg, orc):
     assert (np.abs(d - ref["depth"]) < 2e-3).mean() > 0.99
     g = r.get_hdr_result()[..., :3]
     assert abs(g.mean() - ref["hdr"][..., :3].mean()) / ref["hdr"][..., :3].mean() < 0.02
+
+
+def test_device_matches_golden_ray_batch(rg):
+    import os
+    g = np.load(os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "oracle_golden.npz"))
+    sc = rg.Scene.builtin(1, 1)
+    r = rg.RayRenderer(rg.RendererSettings(resolutionWidth=8, resolutionHeight=8, samples=1))
+    r.set_scene(sc)
+    tuv, prim = r.trace_closest(g["rays"])
+    same = prim == g["prim"]
+    assert same.mean() > 0.999
+    np.testing.assert_allclose(tuv[same], g["tuv"][same], rtol=1e-5, atol=1e-7)
+    r.close()
