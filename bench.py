@@ -52,6 +52,7 @@ def parse():
     p.add_argument("--spp", type=int, default=SPP)
     p.add_argument("--res", default=f"{W}x{H}", help="resolution WxH (profiling runs only)")
     p.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline (profiling runs only)")
+    p.add_argument("--bvh-width", type=int, default=8, choices=[2, 8])
     a = p.parse_args()
     a.w, a.h = (int(x) for x in a.res.lower().split("x"))
     return a
@@ -212,7 +213,7 @@ def main():
     ntris = desc.num_triangles
     Wr, Hr = args.w, args.h
     st = rg.RendererSettings(resolutionWidth=Wr, resolutionHeight=Hr, samples=args.spp, maxDepth=DEPTH, rrDepth=RR,
-                             seed=SEED, bvhBins=32)
+                             seed=SEED, bvhBins=32, bvhWidth=args.bvh_width)
     r = rg.RayRenderer(st)
     r.set_scene(scene)
     build_ms = r.stats()["build_ms"]
@@ -269,7 +270,8 @@ def main():
     s = r.stats()
     os.environ.pop("RG_PROFILE_KERNELS", None)
     ext_ms = s["extend_ms"]
-    alg_bytes = s["closest_rays"] * 48 + s["nodes_visited"] * 64 + s["tris_tested"] * 48
+    node_bytes = 80 if st.bvhWidth == 8 else 64
+    alg_bytes = s["closest_rays"] * 48 + s["nodes_visited"] * node_bytes + s["tris_tested"] * 48
     launches_ext = s["waves"] * (DEPTH + 2)
     achieved = alg_bytes / (ext_ms * 1e-3) / 1e9 if ext_ms > 0 else None
     peak, peak_kind = measured_peak_hbm()
@@ -286,6 +288,10 @@ def main():
                 "shade_ms": round(s["shade_ms"], 2), "connect_ms": round(s["connect_ms"], 2),
                 "extend_ms": round(ext_ms, 2),
                 "rays_per_sample": round((s["closest_rays"] + s["shadow_rays"]) / max(1, s["samples"]), 3),
+                "nodes_per_ray": round(s["nodes_visited"] / max(1, s["closest_rays"]), 2),
+                "tris_per_ray": round(s["tris_tested"] / max(1, s["closest_rays"]), 2),
+                "shadow_nodes_per_ray": round(s["shadow_nodes_visited"] / max(1, s["shadow_rays"]), 2),
+                "shadow_tris_per_ray": round(s["shadow_tris_tested"] / max(1, s["shadow_rays"]), 2),
                 "mrays_per_s": round((s["closest_rays"] + s["shadow_rays"]) / ((s["trace_ms"]) * 1e3), 1)}
 
     # ---- CPU baseline (rank 0, N = 1 only)
@@ -307,7 +313,8 @@ def main():
             "config": {"workload": "heavy geometry single job: 4 x 1,003,520-triangle displaced icospheres "
                                    "in a 20x20 room, 16 emissive quads, metal/dielectric",
                        "triangles": ntris, "resolution": f"{Wr}x{Hr}", "spp": args.spp, "max_depth": DEPTH,
-                       "bvh": "device binned SAH, 32 bins", "bvh_build_ms": round(build_ms, 2),
+                       "bvh": f"device binned SAH (32 bins), {st.bvhWidth}-wide" + (" compressed" if st.bvhWidth == 8 else ""),
+                       "bvh_build_ms": round(build_ms, 2),
                        "l2": "inputs larger than L2 (BVH + triangles ~400 MB)",
                        "parallelism": f"replicas x{world}" if world > 1 else "single GPU"},
             "e2e": {"value": round(e2e_value, 3), "unit": "Msamples/s", "h2d_bytes_per_step": int(h2d),

@@ -86,6 +86,7 @@ typedef struct rg_settings {
   int32_t light_pick_fix;     /* 1: weight NEE by the light count [0]         */
   int32_t paths_per_wave;     /* wavefront size; 0 = automatic                */
   int32_t bvh_bins;           /* SAH bins for the device build [32]           */
+  int32_t bvh_width;          /* 8: compressed 8-wide BVH (default), 2: binary */
 } rg_settings;
 
 typedef struct rg_material {

@@ -421,21 +421,29 @@ struct HitInfo {  // RayTriangleIntersectionInfo, raycommon.h:168-180
   float u = 0, v = 0, w = 0;
 };
 
+// Triangle-test products in a fixed FMA form (the device evaluates the same
+// operations in the same order, so hits agree bit for bit):
+//   dotF(a, b) = fma(a.z, b.z, fma(a.y, b.y, a.x * b.x)); crossF likewise per component.
+static inline float dotF(V3 a, V3 b) { return fmaf(a.z, b.z, fmaf(a.y, b.y, a.x * b.x)); }
+static inline V3 crossF(V3 a, V3 b) {
+  return V3(fmaf(a.y, b.z, -(a.z * b.y)), fmaf(a.z, b.x, -(a.x * b.z)), fmaf(a.x, b.y, -(a.y * b.x)));
+}
+
 // RenderMeshTriangle::intersectsRay(closest): raycommon.cpp:200-235
 static inline bool intersectClosestTri(const Tri& tr, int id, const Ray& ray, HitInfo& info) {
   const V3 edge1 = tr.v2 - tr.v1;
   const V3 edge2 = tr.v3 - tr.v1;
-  const V3 pvec = cross(ray.d, edge2);
-  const float det = dot(edge1, pvec);
+  const V3 pvec = crossF(ray.d, edge2);
+  const float det = dotF(edge1, pvec);
   if (fabsf(det) < 1e-8f) return false;
   const float invDet = 1.0f / det;
   const V3 tvec = ray.o - tr.v1;
-  const float u = dot(tvec, pvec) * invDet;
+  const float u = dotF(tvec, pvec) * invDet;
   if (u < 0.0f || u > 1.0f) return false;
-  const V3 qvec = cross(tvec, edge1);
-  const float v = dot(ray.d, qvec) * invDet;
+  const V3 qvec = crossF(tvec, edge1);
+  const float v = dotF(ray.d, qvec) * invDet;
   if (v < 0.0f || u + v > 1.0f) return false;
-  const float t = dot(edge2, qvec) * invDet;
+  const float t = dotF(edge2, qvec) * invDet;
   if (t < 0.0f) return false;
   if (t >= info.t) return false;
   info.t = t;
@@ -450,17 +458,17 @@ static inline bool intersectAnyTri(const Tri& tr, const Ray& ray, float maxt) {
   const float EPS = 1e-6f;
   const V3 edge1 = tr.v2 - tr.v1;
   const V3 edge2 = tr.v3 - tr.v1;
-  const V3 h = cross(ray.d, edge2);
-  const float a = dot(edge1, h);
+  const V3 h = crossF(ray.d, edge2);
+  const float a = dotF(edge1, h);
   if (fabsf(a) < EPS) return false;
   const float f = 1.0f / a;
   const V3 s = ray.o - tr.v1;
-  const float u = f * dot(s, h);
+  const float u = f * dotF(s, h);
   if (u < 0.0f || u > 1.0f) return false;
-  const V3 q = cross(s, edge1);
-  const float v = f * dot(ray.d, q);
+  const V3 q = crossF(s, edge1);
+  const float v = f * dotF(ray.d, q);
   if (v < 0.0f || u + v > 1.0f) return false;
-  const float t = f * dot(edge2, q);
+  const float t = f * dotF(edge2, q);
   return t > EPS && t < maxt;
 }
 

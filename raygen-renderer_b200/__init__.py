@@ -69,6 +69,7 @@ class rg_settings(C.Structure):
         ("world_color", C.c_float * 3), ("back_color", C.c_float * 4),
         ("seed", C.c_uint32), ("max_depth", C.c_int32), ("rr_depth", C.c_int32),
         ("light_pick_fix", C.c_int32), ("paths_per_wave", C.c_int32), ("bvh_bins", C.c_int32),
+        ("bvh_width", C.c_int32),
     ]
 
 
@@ -239,6 +240,7 @@ class RendererSettings:
     lightPickFix: bool = False
     pathsPerWave: int = 0
     bvhBins: int = 32
+    bvhWidth: int = 8
 
     _MAP = {
         "resolutionWidth": "resolution_width", "resolutionHeight": "resolution_height",
@@ -256,6 +258,7 @@ class RendererSettings:
         "bloomSizeAspect": "bloom_size_aspect", "bloomCurve": "bloom_curve",
         "seed": "seed", "maxDepth": "max_depth", "rrDepth": "rr_depth",
         "lightPickFix": "light_pick_fix", "pathsPerWave": "paths_per_wave", "bvhBins": "bvh_bins",
+        "bvhWidth": "bvh_width",
     }
 
     def to_c(self) -> rg_settings:

@@ -245,9 +245,9 @@ struct Grids {
 Grids grids(rg_handle* h) {
   Grids g;
   g.gen = h->numSMs * 8;
-  g.ext = h->numSMs * 8;
+  g.ext = h->numSMs * residentBlocks(0, h->dscene.bvhWidth);
   g.shade = h->numSMs * 4;
-  g.conn = h->numSMs * 8;
+  g.conn = h->numSMs * residentBlocks(1, h->dscene.bvhWidth);
   g.acc = h->numSMs * 4;
   g.simple = h->numSMs * 8;
   return g;
@@ -330,6 +330,7 @@ void rg_settings_default(rg_settings* s) {
   s->light_pick_fix = 0;
   s->paths_per_wave = 0;
   s->bvh_bins = 32;
+  s->bvh_width = 8;
 }
 
 const char* rg_last_error(void) { return g_lastError.c_str(); }
@@ -530,7 +531,7 @@ rg_status rg_set_scene(rg_handle* h, const rg_scene_desc* d) {
   cudaEventCreate(&e1);
   cudaEventRecord(e0, st);
   std::string err;
-  const rg_status rs = buildDeviceBvh(ds, h->st.bvh_bins > 1 ? h->st.bvh_bins : 32, st, err);
+  const rg_status rs = buildDeviceBvh(ds, h->st.bvh_bins > 1 ? h->st.bvh_bins : 32, h->st.bvh_width != 2, st, err);
   cudaEventRecord(e1, st);
   cudaStreamSynchronize(st);
   float ms = 0.0f;
@@ -543,7 +544,7 @@ rg_status rg_set_scene(rg_handle* h, const rg_scene_desc* d) {
     return rs;
   }
   h->lastStats.build_ms = ms;
-  h->lastStats.bvh_nodes = ds.numNodes;
+  h->lastStats.bvh_nodes = ds.bvhWidth == 8 ? ds.numNodes8 : ds.numNodes;
   ds.inPos.release();
   ds.inNrm.release();
   ds.inUV.release();
@@ -578,6 +579,9 @@ rg_status rg_set_scene(rg_handle* h, const rg_scene_desc* d) {
   if (!h->error.alloc(1)) return RG_ERR_OUT_OF_MEMORY;
   cudaMemsetAsync(h->error.p, 0, sizeof(int), st);
   S.error = h->error.p;
+  S.nodes8 = ds.nodes8.p;
+  S.numNodes8 = ds.numNodes8;
+  S.bvhWidth = ds.bvhWidth;
   h->hasScene = true;
   if (h->graph) {
     cudaGraphExecDestroy(h->graph);

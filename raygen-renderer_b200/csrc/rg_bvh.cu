@@ -269,7 +269,7 @@ __device__ __forceinline__ float areaOf(const float lo[3], const float hi[3]) {
 
 // Split decision per open node (bvh.cpp:133-211 cost model).
 __global__ void k_split(int numTasks, const int* __restrict__ tasks, BNode* nodes, const BinData* __restrict__ bins,
-                        int nbins, int* nodeCounter, int* nextTasks, int* nextCount) {
+                        int nbins, int* nodeCounter, int* nextTasks, int* nextCount, int maxLeaf) {
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= numTasks) return;
   const int id = tasks[t];
@@ -312,7 +312,7 @@ __global__ void k_split(int numTasks, const int* __restrict__ tasks, BNode* node
     }
   }
   int split = best;
-  if (split < 0 && nd.count > kMaxLeaf) split = forced >= 0 ? forced : -2;  // -2: index median
+  if (split < 0 && nd.count > maxLeaf) split = forced >= 0 ? forced : -2;  // -2: index median
   nd.binSlot = -1;
   if (split == -1) {
     nd.left = -1;
@@ -459,13 +459,165 @@ __global__ void k_gather(int n, const int* __restrict__ primIdx, const float4* _
   orig[i] = p;
 }
 
+
+// ---- 8-wide compressed BVH (collapse of the binary build) ---------------------
+// Node (80 B = 5 float4): (lo.xyz, e.x | e.y << 8 | e.z << 16 | imask << 24)
+// (childBase, triBase, meta[0..3], meta[4..7]) (qlo.x[8], qlo.y[8]) (qlo.z[8], qhi.x[8])
+// (qhi.y[8], qhi.z[8]).  Child box = lo + 2^e * q.  imask bit s: slot s is an inner
+// child, stored at childBase + popc(imask below s).  meta[s] = (count << 5) | offset
+// for a leaf of `count` (1..4) triangles at triBase + offset; 0 = empty slot.
+// Slots are assigned per octant: a child whose centre lies on the negative side
+// of the node centre along axis k prefers slots with bit k set, so visiting hit
+// slots in descending order of (slot XOR ray octant) is roughly front to back.
+__global__ void k_collapse(int numTasks, const int2* __restrict__ tasks, const BNode* __restrict__ nodes,
+                           const int* __restrict__ primIdx, float4* __restrict__ nodes8, int* counters,
+                           int2* __restrict__ nextTasks, int* __restrict__ triOrder, int maxNodes8) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= numTasks) return;
+  const int2 task = tasks[t];
+  const BNode& nd = nodes[task.x];
+  int ch[8];
+  int nc;
+  if (nd.left < 0) {
+    ch[0] = task.x;
+    nc = 1;
+  } else {
+    ch[0] = nd.left;
+    ch[1] = nd.left + 1;
+    nc = 2;
+    while (nc < 8) {
+      int best = -1;
+      float bestA = -1.0f;
+      for (int i = 0; i < nc; i++) {
+        const BNode& c = nodes[ch[i]];
+        if (c.left < 0) continue;
+        const float a = areaOf(c.bmin, c.bmax);
+        if (a > bestA) { bestA = a; best = i; }
+      }
+      if (best < 0) break;
+      const int l = nodes[ch[best]].left;
+      ch[best] = l;
+      ch[nc++] = l + 1;
+    }
+  }
+  float lo[3] = {FLT_MAX, FLT_MAX, FLT_MAX}, hi[3] = {-FLT_MAX, -FLT_MAX, -FLT_MAX};
+  float cc[8][3];
+  for (int i = 0; i < nc; i++) {
+    const BNode& c = nodes[ch[i]];
+    for (int k = 0; k < 3; k++) {
+      const float a = inflateLo(c.bmin[k]), b = inflateHi(c.bmax[k]);
+      lo[k] = fminf(lo[k], a);
+      hi[k] = fmaxf(hi[k], b);
+      cc[i][k] = 0.5f * (c.bmin[k] + c.bmax[k]);
+    }
+  }
+  // greedy octant slot assignment
+  int slotOf[8];
+  bool slotUsed[8] = {false, false, false, false, false, false, false, false};
+  bool childDone[8] = {false, false, false, false, false, false, false, false};
+  const float ctr[3] = {0.5f * (lo[0] + hi[0]), 0.5f * (lo[1] + hi[1]), 0.5f * (lo[2] + hi[2])};
+  for (int it = 0; it < nc; it++) {
+    float bestS = -FLT_MAX;
+    int bj = -1, bs = -1;
+    for (int j = 0; j < nc; j++) {
+      if (childDone[j]) continue;
+      for (int sl = 0; sl < 8; sl++) {
+        if (slotUsed[sl]) continue;
+        const float sc = (cc[j][0] - ctr[0]) * ((sl & 1) ? -1.0f : 1.0f) + (cc[j][1] - ctr[1]) * ((sl & 2) ? -1.0f : 1.0f) +
+                         (cc[j][2] - ctr[2]) * ((sl & 4) ? -1.0f : 1.0f);
+        if (sc > bestS) { bestS = sc; bj = j; bs = sl; }
+      }
+    }
+    childDone[bj] = true;
+    slotUsed[bs] = true;
+    slotOf[bj] = bs;
+  }
+  int childAt[8];
+  for (int sl = 0; sl < 8; sl++) childAt[sl] = -1;
+  for (int j = 0; j < nc; j++) childAt[slotOf[j]] = ch[j];
+  // quantisation frame
+  // The quantum 2^e covers the extent in at most 250 steps and is at least four
+  // ulps of the node's coordinates; the origin sits one quantum below the
+  // box so every child keeps a full quantum of margin after rounding.
+  int e[3];
+  float inv[3], org[3];
+  for (int k = 0; k < 3; k++) {
+    const float ext = __fsub_ru(hi[k], lo[k]);
+    int em;
+    frexpf(fmaxf(fmaxf(fabsf(lo[k]), fabsf(hi[k])), 1e-30f), &em);
+    int ex = em - 22;
+    if (ext > 0.0f) {
+      int e2;
+      frexpf(ext / 250.0f, &e2);
+      ex = max(ex, e2);
+    }
+    ex = max(-100, min(100, ex));
+    e[k] = ex;
+    inv[k] = ldexpf(1.0f, -ex);
+    org[k] = __fsub_rd(lo[k], ldexpf(1.0f, ex));
+  }
+  uint32_t qlo[3][2] = {{0, 0}, {0, 0}, {0, 0}}, qhi[3][2] = {{0, 0}, {0, 0}, {0, 0}};
+  uint32_t meta[2] = {0, 0};
+  uint32_t imask = 0;
+  int ni = 0, ntri = 0;
+  for (int sl = 0; sl < 8; sl++) {
+    const int c = childAt[sl];
+    if (c < 0) continue;
+    const BNode& cn = nodes[c];
+    for (int k = 0; k < 3; k++) {
+      // one quantum of margin on each side (covers the traversal's folded 2^23 offset)
+      int a = (int)floorf(__fsub_rd(inflateLo(cn.bmin[k]), org[k]) * inv[k]) - 1;
+      int b = (int)ceilf(__fsub_ru(inflateHi(cn.bmax[k]), org[k]) * inv[k]) + 1;
+      a = max(0, min(255, a));
+      b = max(0, min(255, b));
+      qlo[k][sl >> 2] |= (uint32_t)a << (8 * (sl & 3));
+      qhi[k][sl >> 2] |= (uint32_t)b << (8 * (sl & 3));
+    }
+    if (cn.left >= 0) {
+      imask |= 1u << sl;
+      meta[sl >> 2] |= 0x20u << (8 * (sl & 3));
+      ni++;
+    } else {
+      meta[sl >> 2] |= (uint32_t)((cn.count << 5) | ntri) << (8 * (sl & 3));
+      ntri += cn.count;
+    }
+  }
+  const int childBase = ni ? atomicAdd(&counters[0], ni) : 0;
+  const int triBase = atomicAdd(&counters[1], ntri);
+  if (childBase + ni > maxNodes8) {
+    atomicCAS(&counters[3], 0, kErrPartition);
+    return;
+  }
+  float4* o = nodes8 + (size_t)task.y * 5;
+  const uint32_t eb = ((uint32_t)(e[0] & 0xff)) | ((uint32_t)(e[1] & 0xff) << 8) | ((uint32_t)(e[2] & 0xff) << 16) | (imask << 24);
+  o[0] = make_float4(org[0], org[1], org[2], __uint_as_float(eb));
+  o[1] = make_float4(__int_as_float(childBase), __int_as_float(triBase), __uint_as_float(meta[0]), __uint_as_float(meta[1]));
+  o[2] = make_float4(__uint_as_float(qlo[0][0]), __uint_as_float(qlo[0][1]), __uint_as_float(qlo[1][0]), __uint_as_float(qlo[1][1]));
+  o[3] = make_float4(__uint_as_float(qlo[2][0]), __uint_as_float(qlo[2][1]), __uint_as_float(qhi[0][0]), __uint_as_float(qhi[0][1]));
+  o[4] = make_float4(__uint_as_float(qhi[1][0]), __uint_as_float(qhi[1][1]), __uint_as_float(qhi[2][0]), __uint_as_float(qhi[2][1]));
+  int k = 0, off = 0;
+  for (int sl = 0; sl < 8; sl++) {
+    const int c = childAt[sl];
+    if (c < 0) continue;
+    const BNode& cn = nodes[c];
+    if (cn.left >= 0) {
+      const int slot = atomicAdd(&counters[2], 1);
+      nextTasks[slot] = make_int2(c, childBase + k);
+      k++;
+    } else {
+      for (int q = 0; q < cn.count; q++) triOrder[triBase + off + q] = primIdx[cn.start + q];
+      off += cn.count;
+    }
+  }
+}
+
 inline int gridFor(long long n, int block) { return (int)((n + block - 1) / block); }
 
 }  // namespace
 
 // Builds the view-space triangle arrays and the BVH for `n` triangles whose
 // world-space inputs are already on the device (DeviceSceneBuild fields).
-rg_status buildDeviceBvh(DeviceScene& ds, int nbins, cudaStream_t st, std::string& err) {
+rg_status buildDeviceBvh(DeviceScene& ds, int nbins, bool wide, cudaStream_t st, std::string& err) {
   const int n = ds.numTris;
   nbins = nbins < 2 ? 2 : (nbins > kMaxBins ? kMaxBins : nbins);
   ds.rootIsLeaf = 0;
@@ -528,7 +680,7 @@ rg_status buildDeviceBvh(DeviceScene& ds, int nbins, cudaStream_t st, std::strin
       k_prepareLevel<<<gridFor(prepN, 256), 256, 0, st>>>(nt, curTasks + c0, nodes.p, bins.p, nbins);
       k_bin<<<gridFor(n, kBinChunk), 256, 0, st>>>(n, curIdx, curNode, nodes.p, lo.p, hi.p, bins.p, nbins);
       k_split<<<gridFor(nt, 128), 128, 0, st>>>(nt, curTasks + c0, nodes.p, bins.p, nbins, counters.p, nxtTasks,
-                                                 counters.p + 1);
+                                                 counters.p + 1, wide ? 4 : kMaxLeaf);
     }
     k_partition<<<gridFor(n, 256), 256, 0, st>>>(n, curIdx, curNode, nodes.p, lo.p, hi.p, altIdx, altNode, nbins,
                                                  counters.p + 2);
@@ -554,7 +706,62 @@ rg_status buildDeviceBvh(DeviceScene& ds, int nbins, cudaStream_t st, std::strin
     return RG_ERR_DEVICE_STATUS;
   }
   ds.buildLevels = levels;
-  // traversal layout
+  if (!ds.triVerts.alloc((size_t)n * 3) || !ds.triShade.alloc((size_t)n * 3) || !ds.triOrig.alloc(n)) {
+    err = "out of device memory (triangles)";
+    return RG_ERR_OUT_OF_MEMORY;
+  }
+  if (ds.hasUV) ds.triUV.alloc((size_t)n * 3);
+  if (wide) {
+    // collapse to the 8-wide compressed layout, level by level
+    ds.bvhWidth = 8;
+    const int maxNodes8 = numNodes + 1;
+    DevBuf<int2> ta, tb;
+    DevBuf<int> order, c8;
+    if (!ds.nodes8.alloc((size_t)maxNodes8 * 5) || !ta.alloc(maxNodes8) || !tb.alloc(maxNodes8) || !order.alloc(n) ||
+        !c8.alloc(4)) {
+      err = "out of device memory (wide BVH)";
+      return RG_ERR_OUT_OF_MEMORY;
+    }
+    const int init[4] = {1, 0, 0, 0};  // [0] nodes (root preallocated) [1] triangles [2] next tasks [3] error
+    cudaMemcpyAsync(c8.p, init, sizeof(init), cudaMemcpyHostToDevice, st);
+    const int2 root = make_int2(0, 0);
+    cudaMemcpyAsync(ta.p, &root, sizeof(int2), cudaMemcpyHostToDevice, st);
+    int nt = 1;
+    int2* cur = ta.p;
+    int2* nxt = tb.p;
+    int lv = 0;
+    while (nt > 0) {
+      cudaMemsetAsync(c8.p + 2, 0, sizeof(int), st);
+      k_collapse<<<gridFor(nt, 64), 64, 0, st>>>(nt, cur, nodes.p, curIdx, ds.nodes8.p, c8.p, nxt, order.p, maxNodes8);
+      cudaMemcpyAsync(&nt, c8.p + 2, sizeof(int), cudaMemcpyDeviceToHost, st);
+      if (cudaStreamSynchronize(st) != cudaSuccess) {
+        err = "wide BVH collapse failed";
+        return RG_ERR_CUDA;
+      }
+      std::swap(cur, nxt);
+      if (++lv > 200) {
+        err = "wide BVH collapse did not converge";
+        return RG_ERR_DEVICE_STATUS;
+      }
+    }
+    int h8[4];
+    cudaMemcpy(h8, c8.p, sizeof(h8), cudaMemcpyDeviceToHost);
+    if (h8[3] != 0 || h8[1] != n) {
+      err = "wide BVH collapse error (nodes " + std::to_string(h8[0]) + ", triangles " + std::to_string(h8[1]) + ")";
+      return RG_ERR_DEVICE_STATUS;
+    }
+    ds.numNodes8 = h8[0];
+    ds.numNodes = 0;
+    k_gather<<<gridFor(n, 256), 256, 0, st>>>(n, order.p, vTmp.p, sTmp.p, ds.hasUV ? uvTmp.p : nullptr, ds.triVerts.p,
+                                              ds.triShade.p, ds.hasUV ? ds.triUV.p : nullptr, ds.triOrig.p);
+    if (cudaStreamSynchronize(st) != cudaSuccess) {
+      err = std::string("BVH gather failed: ") + cudaGetErrorString(cudaGetLastError());
+      return RG_ERR_CUDA;
+    }
+    return RG_OK;
+  }
+  // binary traversal layout
+  ds.bvhWidth = 2;
   DevBuf<int> flags, trav;
   flags.alloc(numNodes);
   trav.alloc(numNodes);
@@ -581,11 +788,6 @@ rg_status buildDeviceBvh(DeviceScene& ds, int nbins, cudaStream_t st, std::strin
     }
     k_emitNodes<<<gridFor(numNodes, 256), 256, 0, st>>>(numNodes, nodes.p, trav.p, ds.nodes.p);
   }
-  if (!ds.triVerts.alloc((size_t)n * 3) || !ds.triShade.alloc((size_t)n * 3) || !ds.triOrig.alloc(n)) {
-    err = "out of device memory (triangles)";
-    return RG_ERR_OUT_OF_MEMORY;
-  }
-  if (ds.hasUV) ds.triUV.alloc((size_t)n * 3);
   k_gather<<<gridFor(n, 256), 256, 0, st>>>(n, curIdx, vTmp.p, sTmp.p, ds.hasUV ? uvTmp.p : nullptr, ds.triVerts.p,
                                             ds.triShade.p, ds.hasUV ? ds.triUV.p : nullptr, ds.triOrig.p);
   if (cudaStreamSynchronize(st) != cudaSuccess) {

@@ -81,6 +81,9 @@ struct DevScene {
   const DevTexture* textures;
   int numTextures;
   int* error;                 // device error word (first error code wins)
+  const float4* nodes8;       // 5 float4 per 8-wide compressed node (when bvhWidth == 8)
+  int numNodes8;
+  int bvhWidth;               // 2 or 8
 };
 
 // device error codes
@@ -180,6 +183,16 @@ __device__ __forceinline__ V3 xyz(float4 f) { return v3(f.x, f.y, f.z); }
 __device__ __forceinline__ V3 sub_rn(V3 a, V3 b) { return v3(__fsub_rn(a.x, b.x), __fsub_rn(a.y, b.y), __fsub_rn(a.z, b.z)); }
 __device__ __forceinline__ float dot_rn(V3 a, V3 b) {
   return __fadd_rn(__fadd_rn(__fmul_rn(a.x, b.x), __fmul_rn(a.y, b.y)), __fmul_rn(a.z, b.z));
+}
+// FMA forms with a fixed evaluation order, mirrored exactly by the CPU oracle:
+//   dot(a, b)   = fma(a.z, b.z, fma(a.y, b.y, a.x * b.x))
+//   cross(a, b) = (fma(a.y, b.z, -(a.z * b.y)), fma(a.z, b.x, -(a.x * b.z)), fma(a.x, b.y, -(a.y * b.x)))
+__device__ __forceinline__ float dot_f(V3 a, V3 b) {
+  return __fmaf_rn(a.z, b.z, __fmaf_rn(a.y, b.y, __fmul_rn(a.x, b.x)));
+}
+__device__ __forceinline__ V3 cross_f(V3 a, V3 b) {
+  return v3(__fmaf_rn(a.y, b.z, -__fmul_rn(a.z, b.y)), __fmaf_rn(a.z, b.x, -__fmul_rn(a.x, b.z)),
+            __fmaf_rn(a.x, b.y, -__fmul_rn(a.y, b.x)));
 }
 __device__ __forceinline__ V3 cross_rn(V3 a, V3 b) {
   return v3(__fsub_rn(__fmul_rn(a.y, b.z), __fmul_rn(a.z, b.y)), __fsub_rn(__fmul_rn(a.z, b.x), __fmul_rn(a.x, b.z)),

@@ -98,7 +98,9 @@ struct DeviceScene {
   std::vector<DevBuf<float4>*> texels;
   int numTextures = 0;
   // BVH + leaf-order triangles
-  DevBuf<float4> nodes, triVerts, triShade;
+  DevBuf<float4> nodes, nodes8, triVerts, triShade;
+  int numNodes8 = 0;
+  int bvhWidth = 2;
   DevBuf<float2> triUV;
   DevBuf<int> triOrig;
   int numNodes = 0;
@@ -109,7 +111,7 @@ struct DeviceScene {
   }
 };
 
-rg_status buildDeviceBvh(DeviceScene& ds, int nbins, cudaStream_t st, std::string& err);
+rg_status buildDeviceBvh(DeviceScene& ds, int nbins, bool wide, cudaStream_t st, std::string& err);
 
 void setLastError(const std::string& msg);
 

@@ -354,7 +354,7 @@ __global__ void __launch_bounds__(128) k_extend(DevScene S, DevQueues Q, int ite
     const int q = base + lane;
     if (q < count) {
       const float4 a = rO[q], b = rD[q];
-      const ClosestHit h = traceClosest(S, xyz(a), xyz(b), nodes, tris);
+      const ClosestHit h = traceClosest2(S, xyz(a), xyz(b), nodes, tris);
       Q.hits[q] = make_float4(h.t, h.u, h.v, __int_as_float(h.prim));
       rays++;
     }
@@ -383,7 +383,7 @@ __global__ void __launch_bounds__(128) k_connect(DevScene S, DevQueues Q, int it
     if (q < count) {
       const float4 a = sO[q], b = sD[q];
       rays++;
-      if (!traceAny(S, xyz(a), xyz(b), b.w, occ, nodes, tris)) {
+      if (!traceAny2(S, xyz(a), xyz(b), b.w, occ, nodes, tris)) {
         const float4 c = sC[q];
         const int pid = __float_as_int(a.w);
         float4 l = Q.pathL[pid];
@@ -392,6 +392,193 @@ __global__ void __launch_bounds__(128) k_connect(DevScene S, DevQueues Q, int it
       }
     }
   }
+  warpAddStat(&Q.stats[2], nodes);
+  warpAddStat(&Q.stats[3], tris);
+  warpAddStat(&Q.stats[5], rays);
+}
+
+// ---- 8-wide traversal kernels with per-lane ray refill ----------------------
+// Persistent warps (Aila & Laine's persistent threads with ray refill, with
+// the triangle postponing of Ylitie et al.'s compressed wide BVH traversal):
+// * a lane whose ray finished is refilled once enough lanes of its warp are
+//   idle (warp ballot + one atomic per warp);
+// * every step a lane either intersects one node or tests one triangle; a
+//   lane with pending triangles pushes them as a triangle group and keeps
+//   descending unless enough lanes of the warp have triangles to test, so the
+//   warp runs mostly one kind of step at a time.
+// Stack entries: node group (childBase, hits | imask << 8) or triangle group
+// (triBase | 0x80000000, triangle mask).
+constexpr int kRefillIdle = 8;     // refill once this many lanes are idle
+constexpr int kTriVotes = 10;      // lanes with triangles needed to run a triangle step
+
+template <bool ANY>
+__device__ __forceinline__ void traverseWave8(const DevScene& S, int count, int* fetch, const float4* __restrict__ rO,
+                                              const float4* __restrict__ rD, uint32_t occ, float4* __restrict__ hitsOut,
+                                              const float4* __restrict__ contrib, float4* __restrict__ pathL,
+                                              uint32_t& nodes, uint32_t& tris, uint32_t& rays) {
+  const int lane = threadIdx.x & 31;
+  const unsigned ltMask = (1u << lane) - 1u;
+  int q = -1;  // -1: needs a ray, -2: none left
+  V3 o = v3(0, 0, 0), d = v3(0, 0, 1), inv = v3(0, 0, 0);
+  uint32_t oct = 0;
+  float tmax = 0.0f, hu = 0.0f, hv = 0.0f;
+  int prim = -1, pid = 0;
+  uint32_t gInner = 0, gImask = 0, tMask = 0;
+  int gBase = 0, tBase = 0, sp = 0, steps = 0;
+  uint2 stack[kStack8];
+  for (;;) {
+    // ---- refill idle lanes
+    const bool need = q == -1;
+    const unsigned needMask = __ballot_sync(0xffffffffu, need);
+    if (needMask) {
+      const int leader = __ffs(needMask) - 1;
+      int base = 0;
+      if (lane == leader) base = atomicAdd(fetch, __popc(needMask));
+      base = __shfl_sync(0xffffffffu, base, leader);
+      if (need) {
+        const int idx = base + __popc(needMask & ltMask);
+        if (idx < count) {
+          q = idx;
+          const float4 a = rO[q], b = rD[q];
+          o = xyz(a);
+          d = xyz(b);
+          if (ANY) {
+            tmax = b.w;
+            pid = __float_as_int(a.w);
+          } else {
+            tmax = kMaxRayDistance;
+          }
+          prim = -1;
+          hu = hv = 0.0f;
+          inv = safeInv(d);
+          oct = rayOctant(inv);
+          gBase = 0;
+          gImask = 1u;          // the root as a one-child group
+          gInner = 1u << oct;   // slot 0 at priority position 0 ^ oct
+          tMask = 0;
+          sp = 0;
+          steps = 0;
+          rays++;
+        } else {
+          q = -2;
+        }
+      }
+    }
+    if (__ballot_sync(0xffffffffu, q >= 0) == 0) break;
+    // ---- traversal steps until enough lanes are idle
+    for (;;) {
+      const bool alive = q >= 0;
+      int result = 0;  // 1: finished (closest: hit record, any: unoccluded), 2: occluded
+      if (alive && tMask == 0 && gInner == 0) {
+        if (sp == 0) {
+          result = 1;
+        } else {
+          const uint2 e = stack[--sp];
+          if (e.x & 0x80000000u) {
+            tBase = (int)(e.x & 0x7fffffffu);
+            tMask = e.y;
+          } else {
+            gBase = (int)e.x;
+            gInner = e.y & 0xffu;
+            gImask = e.y >> 8;
+          }
+        }
+      }
+      const bool hasTri = alive && result == 0 && tMask != 0;
+      const int triVotes = __popc(__ballot_sync(0xffffffffu, hasTri));
+      if (alive && result == 0) {
+        const bool doTri = hasTri && (gInner == 0 || triVotes >= kTriVotes);
+        if (doTri) {
+          const int i = __ffs(tMask) - 1;
+          tMask &= tMask - 1u;
+          const int tk = tBase + i;
+          const float4* tp = S.triVerts + (size_t)tk * 3;
+          const float4 b = ldg4(tp + 1);
+          if (!ANY || (__float_as_uint(b.w) & occ)) {
+            const float4 a = ldg4(tp), c = ldg4(tp + 2);
+            tris++;
+            if (ANY) {
+              if (mtAny(o, d, xyz(a), xyz(b), xyz(c), tmax)) result = 2;
+            } else {
+              ClosestHit h;
+              h.t = tmax;
+              h.u = hu;
+              h.v = hv;
+              if (mtClosest(o, d, xyz(a), xyz(b), xyz(c), h)) {
+                tmax = h.t;
+                hu = h.u;
+                hv = h.v;
+                prim = tk;
+              }
+            }
+          }
+        } else {
+          // node step (pending triangles are postponed onto the stack)
+          if (hasTri) {
+            if (sp < kStack8) stack[sp++] = make_uint2((uint32_t)tBase | 0x80000000u, tMask);
+            else atomicCAS(S.error, 0, kErrStackOverflow);
+            tMask = 0;
+          }
+          const int pos = 31 - __clz(gInner);
+          gInner &= ~(1u << pos);
+          const int slot = pos ^ (int)oct;
+          const int node = gBase + __popc(gImask & ((1u << slot) - 1u));
+          if (gInner) {
+            if (sp < kStack8) stack[sp++] = make_uint2((uint32_t)gBase, gInner | (gImask << 8));
+            else atomicCAS(S.error, 0, kErrStackOverflow);
+          }
+          if (node >= S.numNodes8 || ++steps > kMaxTraversalSteps) {
+            atomicCAS(S.error, 0, kErrTraversalSteps);
+            result = ANY ? 2 : 1;
+          } else {
+            const Node8Hit g = intersectNode8(S.nodes8 + (size_t)node * 5, o, inv, tmax, oct);
+            nodes++;
+            gInner = g.inner;
+            gImask = g.imask;
+            gBase = g.childBase;
+            tMask = g.tris;
+            tBase = g.triBase;
+          }
+        }
+      }
+      if (result != 0) {
+        if (ANY) {
+          if (result == 1) {
+            const float4 c = contrib[q];
+            float4 l = pathL[pid];
+            l.x += c.x;
+            l.y += c.y;
+            l.z += c.z;
+            pathL[pid] = l;
+          }
+        } else {
+          hitsOut[q] = make_float4(tmax, hu, hv, __int_as_float(prim));
+        }
+        q = -1;
+      }
+      const unsigned idle = __ballot_sync(0xffffffffu, q == -1);
+      const unsigned live = __ballot_sync(0xffffffffu, q >= 0);
+      if (live == 0 || __popc(idle) >= kRefillIdle) break;
+    }
+  }
+}
+
+__global__ void __launch_bounds__(128) k_extend8(DevScene S, DevQueues Q, int iter) {
+  const int count = Q.counters[iter * kCountersPerIter + C_RAYS];
+  uint32_t nodes = 0, tris = 0, rays = 0;
+  traverseWave8<false>(S, count, &Q.counters[iter * kCountersPerIter + C_FETCH_EXT], Q.rayO[iter & 1],
+                       Q.rayD[iter & 1], 0u, Q.hits, nullptr, nullptr, nodes, tris, rays);
+  warpAddStat(&Q.stats[0], nodes);
+  warpAddStat(&Q.stats[1], tris);
+  warpAddStat(&Q.stats[4], rays);
+}
+
+__global__ void __launch_bounds__(128) k_connect8(DevScene S, DevQueues Q, int iter, int which) {
+  const int count = Q.counters[iter * kCountersPerIter + (which ? C_SHB : C_SHA)];
+  uint32_t nodes = 0, tris = 0, rays = 0;
+  traverseWave8<true>(S, count, &Q.counters[iter * kCountersPerIter + (which ? C_FETCH_SHB : C_FETCH_SHA)],
+                      Q.shO[which], Q.shD[which], which ? kOccPoint : kOccArea, nullptr, Q.shC[which], Q.pathL, nodes,
+                      tris, rays);
   warpAddStat(&Q.stats[2], nodes);
   warpAddStat(&Q.stats[3], tris);
   warpAddStat(&Q.stats[5], rays);
@@ -1010,18 +1197,28 @@ __global__ void k_queryAny(DevScene S, const float* __restrict__ rays, const flo
 }
 
 // ------------------------------------------------------------ launchers ----
+// Resident blocks per SM for the persistent traversal kernels.
+int residentBlocks(int kernel, int width) {
+  int perSM = 0;
+  if (kernel == 0) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSM, width == 8 ? (const void*)k_extend8 : (const void*)k_extend, 128, 0);
+  else cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSM, width == 8 ? (const void*)k_connect8 : (const void*)k_connect, 128, 0);
+  return perSM < 1 ? 1 : perSM;
+}
+
 void launchGenerate(const DevRender& R, const DevWave* W, const DevQueues& Q, int globalMedium, int grid, cudaStream_t st) {
   k_generate<<<grid, 256, 0, st>>>(R, W, Q, globalMedium);
 }
 void launchExtend(const DevScene& S, const DevQueues& Q, int iter, int grid, cudaStream_t st) {
-  k_extend<<<grid, 128, 0, st>>>(S, Q, iter);
+  if (S.bvhWidth == 8) k_extend8<<<grid, 128, 0, st>>>(S, Q, iter);
+  else k_extend<<<grid, 128, 0, st>>>(S, Q, iter);
 }
 void launchShade(const DevScene& S, const DevRender& R, const DevWave* W, const DevQueues& Q, int iter, int grid,
                  cudaStream_t st) {
   k_shade<<<grid, 256, 0, st>>>(S, R, W, Q, iter);
 }
 void launchConnect(const DevScene& S, const DevQueues& Q, int iter, int which, int grid, cudaStream_t st) {
-  k_connect<<<grid, 128, 0, st>>>(S, Q, iter, which);
+  if (S.bvhWidth == 8) k_connect8<<<grid, 128, 0, st>>>(S, Q, iter, which);
+  else k_connect<<<grid, 128, 0, st>>>(S, Q, iter, which);
 }
 void launchSimple(const DevScene& S, const DevRender& R, const DevWave* W, const DevQueues& Q, int grid, cudaStream_t st) {
   k_simple<<<grid, 128, 0, st>>>(S, R, W, Q);

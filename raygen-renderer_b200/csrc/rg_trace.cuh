@@ -7,6 +7,7 @@
 
 namespace rg {
 
+int residentBlocks(int kernel, int width);
 void launchGenerate(const DevRender& R, const DevWave* W, const DevQueues& Q, int globalMedium, int grid, cudaStream_t st);
 void launchExtend(const DevScene& S, const DevQueues& Q, int iter, int grid, cudaStream_t st);
 void launchShade(const DevScene& S, const DevRender& R, const DevWave* W, const DevQueues& Q, int iter, int grid,

@@ -51,18 +51,19 @@ struct ClosestHit {
 };
 
 // RenderMeshTriangle::intersectsRay(ray, info): raycommon.cpp:200-235
+// (dot / cross in the fixed FMA form of dot_f / cross_f, as in the oracle)
 __device__ __forceinline__ bool mtClosest(V3 o, V3 d, V3 p1, V3 e1, V3 e2, ClosestHit& h) {
-  const V3 pvec = cross_rn(d, e2);
-  const float det = dot_rn(e1, pvec);
+  const V3 pvec = cross_f(d, e2);
+  const float det = dot_f(e1, pvec);
   if (fabsf(det) < 1e-8f) return false;
   const float invDet = __fdiv_rn(1.0f, det);
   const V3 tvec = sub_rn(o, p1);
-  const float u = __fmul_rn(dot_rn(tvec, pvec), invDet);
+  const float u = __fmul_rn(dot_f(tvec, pvec), invDet);
   if (u < 0.0f || u > 1.0f) return false;
-  const V3 qvec = cross_rn(tvec, e1);
-  const float v = __fmul_rn(dot_rn(d, qvec), invDet);
+  const V3 qvec = cross_f(tvec, e1);
+  const float v = __fmul_rn(dot_f(d, qvec), invDet);
   if (v < 0.0f || __fadd_rn(u, v) > 1.0f) return false;
-  const float t = __fmul_rn(dot_rn(e2, qvec), invDet);
+  const float t = __fmul_rn(dot_f(e2, qvec), invDet);
   if (t < 0.0f) return false;
   if (t >= h.t) return false;
   h.t = t;
@@ -73,24 +74,24 @@ __device__ __forceinline__ bool mtClosest(V3 o, V3 d, V3 p1, V3 e1, V3 e2, Close
 
 // RenderMeshTriangle::intersectsRay(ray, maxt, t, hit): raycommon.cpp:151-198
 __device__ __forceinline__ bool mtAny(V3 o, V3 d, V3 p1, V3 e1, V3 e2, float maxt) {
-  const V3 h = cross_rn(d, e2);
-  const float a = dot_rn(e1, h);
+  const V3 h = cross_f(d, e2);
+  const float a = dot_f(e1, h);
   if (fabsf(a) < 1e-6f) return false;
   const float f = __fdiv_rn(1.0f, a);
   const V3 s = sub_rn(o, p1);
-  const float u = __fmul_rn(f, dot_rn(s, h));
+  const float u = __fmul_rn(f, dot_f(s, h));
   if (u < 0.0f || u > 1.0f) return false;
-  const V3 q = cross_rn(s, e1);
-  const float v = __fmul_rn(f, dot_rn(d, q));
+  const V3 q = cross_f(s, e1);
+  const float v = __fmul_rn(f, dot_f(d, q));
   if (v < 0.0f || __fadd_rn(u, v) > 1.0f) return false;
-  const float t = __fmul_rn(f, dot_rn(e2, q));
+  const float t = __fmul_rn(f, dot_f(e2, q));
   return t > 1e-6f && t < maxt;
 }
 
 // Closest hit (TriangleBVH::intersectClosest, bvh.cpp:233-285). Near child
 // first by entry distance. Returns the leaf-order primitive or -1.
-__device__ __forceinline__ ClosestHit traceClosest(const DevScene& S, V3 o, V3 d, uint32_t& nodeCount,
-                                                   uint32_t& triCount) {
+__device__ __forceinline__ ClosestHit traceClosest2(const DevScene& S, V3 o, V3 d, uint32_t& nodeCount,
+                                                    uint32_t& triCount) {
   ClosestHit h;
   h.t = kMaxRayDistance;
   h.u = h.v = 0.0f;
@@ -147,8 +148,8 @@ __device__ __forceinline__ ClosestHit traceClosest(const DevScene& S, V3 o, V3 d
 }
 
 // Any hit with an occluder-class predicate (TriangleBVH::intersectAny, bvh.h:63-101).
-__device__ __forceinline__ bool traceAny(const DevScene& S, V3 o, V3 d, float maxT, uint32_t occMask,
-                                         uint32_t& nodeCount, uint32_t& triCount) {
+__device__ __forceinline__ bool traceAny2(const DevScene& S, V3 o, V3 d, float maxT, uint32_t occMask,
+                                          uint32_t& nodeCount, uint32_t& triCount) {
   if (S.numTris == 0) return false;
   const V3 inv = safeInv(d);
   const V3 oi = v3(o.x * inv.x, o.y * inv.y, o.z * inv.z);
@@ -198,6 +199,214 @@ __device__ __forceinline__ bool traceAny(const DevScene& S, V3 o, V3 d, float ma
     ref = stack[--sp];
   }
   return false;
+}
+
+// ---- 8-wide compressed BVH ----------------------------------------------------
+// Node layout: see k_collapse (rg_bvh.cu).  Traversal keeps a "node group"
+// (child base, hit bits, inner-slot mask) and a "triangle group" (triangle base,
+// 32-bit mask); hit inner children are visited in descending order of
+// (slot XOR ray octant), an approximate front-to-back order.
+
+__device__ __forceinline__ float byteAsFloat(uint32_t w, int sh) {
+  return __uint_as_float(0x4B000000u | ((w >> sh) & 0xffu)) - 8388608.0f;
+}
+
+struct Node8Hit {
+  uint32_t inner;    // hit inner children, bit (slot ^ octant)
+  uint32_t tris;     // triangle mask relative to triBase
+  uint32_t imask;
+  int childBase, triBase;
+};
+
+// Quantised plane -> float: one PRMT puts byte k of w under the exponent of
+// 2^23, giving 2^23 + q exactly; the 2^23 offset is folded into the per-node
+// origin term.  The folded offset costs at most half a quantum of precision,
+// covered by the one-quantum margin the build adds on every side.
+__device__ __forceinline__ float biasedByte(uint32_t w, uint32_t k) {
+  return __uint_as_float(__byte_perm(w, 0x4B000000u, 0x7540u | k));
+}
+
+__device__ __forceinline__ Node8Hit intersectNode8(const float4* np, V3 o, V3 inv, float tcap, uint32_t oct) {
+  const float4 n0 = ldg4(np), n1 = ldg4(np + 1), n2 = ldg4(np + 2), n3 = ldg4(np + 3), n4 = ldg4(np + 4);
+  const uint32_t eb = __float_as_uint(n0.w);
+  const int ex = (int)(int8_t)(eb & 0xffu), ey = (int)(int8_t)((eb >> 8) & 0xffu), ez = (int)(int8_t)((eb >> 16) & 0xffu);
+  const float sx = __int_as_float((ex + 127) << 23), sy = __int_as_float((ey + 127) << 23),
+              sz = __int_as_float((ez + 127) << 23);
+  const V3 adj = v3(sx * inv.x, sy * inv.y, sz * inv.z);
+  const V3 org = v3(fmaf(-8388608.0f, adj.x, (n0.x - o.x) * inv.x), fmaf(-8388608.0f, adj.y, (n0.y - o.y) * inv.y),
+                    fmaf(-8388608.0f, adj.z, (n0.z - o.z) * inv.z));
+  Node8Hit r;
+  r.imask = eb >> 24;
+  r.childBase = __float_as_int(n1.x);
+  r.triBase = __float_as_int(n1.y);
+  r.inner = 0;
+  r.tris = 0;
+  const uint32_t meta[2] = {__float_as_uint(n1.z), __float_as_uint(n1.w)};
+  // near / far planes per axis from the ray direction signs (inv < 0 swaps lo and hi)
+  const bool fx = (oct & 1u) != 0, fy = (oct & 2u) != 0, fz = (oct & 4u) != 0;
+  const uint32_t nx[2] = {__float_as_uint(fx ? n3.z : n2.x), __float_as_uint(fx ? n3.w : n2.y)};
+  const uint32_t ny[2] = {__float_as_uint(fy ? n4.x : n2.z), __float_as_uint(fy ? n4.y : n2.w)};
+  const uint32_t nz[2] = {__float_as_uint(fz ? n4.z : n3.x), __float_as_uint(fz ? n4.w : n3.y)};
+  const uint32_t fxw[2] = {__float_as_uint(fx ? n2.x : n3.z), __float_as_uint(fx ? n2.y : n3.w)};
+  const uint32_t fyw[2] = {__float_as_uint(fy ? n2.z : n4.x), __float_as_uint(fy ? n2.w : n4.y)};
+  const uint32_t fzw[2] = {__float_as_uint(fz ? n3.x : n4.z), __float_as_uint(fz ? n3.y : n4.w)};
+#pragma unroll
+  for (int i = 0; i < 8; i++) {
+    const int w = i >> 2;
+    const uint32_t k = (uint32_t)(i & 3);
+    const uint32_t m = (meta[w] >> (8 * k)) & 0xffu;
+    const float tnx = fmaf(biasedByte(nx[w], k), adj.x, org.x), tfx = fmaf(biasedByte(fxw[w], k), adj.x, org.x);
+    const float tny = fmaf(biasedByte(ny[w], k), adj.y, org.y), tfy = fmaf(biasedByte(fyw[w], k), adj.y, org.y);
+    const float tnz = fmaf(biasedByte(nz[w], k), adj.z, org.z), tfz = fmaf(biasedByte(fzw[w], k), adj.z, org.z);
+    const float tmin = fmaxf(fmaxf(tnx, tny), tnz);
+    const float tmax = fminf(fminf(tfx, tfy), tfz);
+    const bool hit = m != 0u && !(tmax < 0.0f || tmin > tmax || tmin > tcap);
+    if (hit) {
+      if ((r.imask >> i) & 1u) r.inner |= 1u << (i ^ oct);
+      else r.tris |= ((1u << (m >> 5)) - 1u) << (m & 31u);
+    }
+  }
+  return r;
+}
+
+// Octant from the guarded reciprocal (not from d): a tiny negative component
+// has a positive reciprocal (1e30), and the near/far plane choice must follow it.
+__device__ __forceinline__ uint32_t rayOctant(V3 inv) {
+  return (inv.x < 0.0f ? 1u : 0u) | (inv.y < 0.0f ? 2u : 0u) | (inv.z < 0.0f ? 4u : 0u);
+}
+
+constexpr int kStack8 = 32;
+
+__device__ __forceinline__ ClosestHit traceClosest8(const DevScene& S, V3 o, V3 d, uint32_t& nodeCount,
+                                                    uint32_t& triCount) {
+  ClosestHit h;
+  h.t = kMaxRayDistance;
+  h.u = h.v = 0.0f;
+  h.prim = -1;
+  if (S.numTris == 0) return h;
+  const V3 inv = safeInv(d);
+  const uint32_t oct = rayOctant(inv);
+  uint2 stack[kStack8];
+  int sp = 0;
+  Node8Hit g = intersectNode8(S.nodes8, o, inv, h.t, oct);
+  nodeCount++;
+  uint32_t gInner = g.inner, gImask = g.imask, tMask = g.tris;
+  int gBase = g.childBase, tBase = g.triBase;
+  int steps = 0;
+  for (;;) {
+    while (tMask) {
+      const int i = __ffs(tMask) - 1;
+      tMask &= tMask - 1u;
+      const int k = tBase + i;
+      const float4* tp = S.triVerts + (size_t)k * 3;
+      const float4 a = ldg4(tp), b = ldg4(tp + 1), c = ldg4(tp + 2);
+      triCount++;
+      if (mtClosest(o, d, xyz(a), xyz(b), xyz(c), h)) h.prim = k;
+    }
+    if (gInner == 0) {
+      if (sp == 0) break;
+      const uint2 e = stack[--sp];
+      gBase = (int)e.x;
+      gInner = e.y & 0xffu;
+      gImask = e.y >> 8;
+      continue;
+    }
+    if (++steps > kMaxTraversalSteps) {
+      atomicCAS(S.error, 0, kErrTraversalSteps);
+      break;
+    }
+    const int pos = 31 - __clz(gInner);
+    gInner &= ~(1u << pos);
+    const int slot = pos ^ (int)oct;
+    const int node = gBase + __popc(gImask & ((1u << slot) - 1u));
+    if (gInner) {
+      if (sp < kStack8) stack[sp++] = make_uint2((uint32_t)gBase, gInner | (gImask << 8));
+      else atomicCAS(S.error, 0, kErrStackOverflow);
+    }
+    if (node >= S.numNodes8) {
+      atomicCAS(S.error, 0, kErrTraversalSteps);
+      break;
+    }
+    g = intersectNode8(S.nodes8 + (size_t)node * 5, o, inv, h.t, oct);
+    nodeCount++;
+    gInner = g.inner;
+    gImask = g.imask;
+    gBase = g.childBase;
+    tMask = g.tris;
+    tBase = g.triBase;
+  }
+  return h;
+}
+
+__device__ __forceinline__ bool traceAny8(const DevScene& S, V3 o, V3 d, float maxT, uint32_t occMask,
+                                          uint32_t& nodeCount, uint32_t& triCount) {
+  if (S.numTris == 0) return false;
+  const V3 inv = safeInv(d);
+  const uint32_t oct = rayOctant(inv);
+  uint2 stack[kStack8];
+  int sp = 0;
+  Node8Hit g = intersectNode8(S.nodes8, o, inv, maxT, oct);
+  nodeCount++;
+  uint32_t gInner = g.inner, gImask = g.imask, tMask = g.tris;
+  int gBase = g.childBase, tBase = g.triBase;
+  int steps = 0;
+  for (;;) {
+    while (tMask) {
+      const int i = __ffs(tMask) - 1;
+      tMask &= tMask - 1u;
+      const int k = tBase + i;
+      const float4* tp = S.triVerts + (size_t)k * 3;
+      const float4 b = ldg4(tp + 1);
+      if (!(__float_as_uint(b.w) & occMask)) continue;
+      const float4 a = ldg4(tp), c = ldg4(tp + 2);
+      triCount++;
+      if (mtAny(o, d, xyz(a), xyz(b), xyz(c), maxT)) return true;
+    }
+    if (gInner == 0) {
+      if (sp == 0) break;
+      const uint2 e = stack[--sp];
+      gBase = (int)e.x;
+      gInner = e.y & 0xffu;
+      gImask = e.y >> 8;
+      continue;
+    }
+    if (++steps > kMaxTraversalSteps) {
+      atomicCAS(S.error, 0, kErrTraversalSteps);
+      break;
+    }
+    const int pos = 31 - __clz(gInner);
+    gInner &= ~(1u << pos);
+    const int slot = pos ^ (int)oct;
+    const int node = gBase + __popc(gImask & ((1u << slot) - 1u));
+    if (gInner) {
+      if (sp < kStack8) stack[sp++] = make_uint2((uint32_t)gBase, gInner | (gImask << 8));
+      else atomicCAS(S.error, 0, kErrStackOverflow);
+    }
+    if (node >= S.numNodes8) {
+      atomicCAS(S.error, 0, kErrTraversalSteps);
+      break;
+    }
+    g = intersectNode8(S.nodes8 + (size_t)node * 5, o, inv, maxT, oct);
+    nodeCount++;
+    gInner = g.inner;
+    gImask = g.imask;
+    gBase = g.childBase;
+    tMask = g.tris;
+    tBase = g.triBase;
+  }
+  return false;
+}
+
+__device__ __forceinline__ ClosestHit traceClosest(const DevScene& S, V3 o, V3 d, uint32_t& nodeCount,
+                                                   uint32_t& triCount) {
+  if (S.bvhWidth == 8) return traceClosest8(S, o, d, nodeCount, triCount);
+  return traceClosest2(S, o, d, nodeCount, triCount);
+}
+
+__device__ __forceinline__ bool traceAny(const DevScene& S, V3 o, V3 d, float maxT, uint32_t occMask,
+                                         uint32_t& nodeCount, uint32_t& triCount) {
+  if (S.bvhWidth == 8) return traceAny8(S, o, d, maxT, occMask, nodeCount, triCount);
+  return traceAny2(S, o, d, maxT, occMask, nodeCount, triCount);
 }
 
 }  // namespace rg

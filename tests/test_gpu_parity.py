@@ -49,10 +49,11 @@ def check_z(z, g, m, label, tail=0.005):
 
 
 # ----------------------------------------------------------------- ray batches
-@pytest.mark.parametrize("kind,params", [(1, None), (2, [20000]), (4, [100000, 8])])
-def test_closest_hit_parity(rg, orc, kind, params):
+@pytest.mark.parametrize("width", [8, 2])
+@pytest.mark.parametrize("kind,params", [(1, None), (2, [20000]), (4, [100000, 8]), (4, [10, 1])])
+def test_closest_hit_parity(rg, orc, kind, params, width):
     sc = rg.Scene.builtin(kind, 3, params)
-    r = rg.RayRenderer(rg.RendererSettings(resolutionWidth=8, resolutionHeight=8, samples=1))
+    r = rg.RayRenderer(rg.RendererSettings(resolutionWidth=8, resolutionHeight=8, samples=1, bvhWidth=width))
     r.set_scene(sc)
     o = orc.OracleScene(sc.ptr)
     bounds = ((-5, -5, -20), (5, 5, -1)) if kind == 1 else ((-9, -4.9, -19), (9, 4.9, -1))
@@ -71,9 +72,10 @@ def test_closest_hit_parity(rg, orc, kind, params):
     r.close()
 
 
-def test_any_hit_parity(rg, orc):
+@pytest.mark.parametrize("width", [8, 2])
+def test_any_hit_parity(rg, orc, width):
     sc = rg.Scene.builtin(2, 4, [20000])
-    r = rg.RayRenderer(rg.RendererSettings(resolutionWidth=8, resolutionHeight=8, samples=1))
+    r = rg.RayRenderer(rg.RendererSettings(resolutionWidth=8, resolutionHeight=8, samples=1, bvhWidth=width))
     r.set_scene(sc)
     o = orc.OracleScene(sc.ptr)
     rays = scenes.random_rays(((-9, -4.9, -19), (9, 4.9, -1)), 40000, 9)
