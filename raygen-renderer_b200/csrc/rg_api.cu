@@ -145,6 +145,9 @@ struct rg_handle {
   bool haveResult = false;
   // wavefront
   DevBuf<float4> rayO0, rayO1, rayD0, rayD1, hits, pathT, pathR, pathL, shO0, shO1, shD0, shD1, shC0, shC1;
+  DevBuf<int2> pathPS;
+  DevBuf<DevJob> jobsDev;
+  DevBuf<DevSegment> segs;
   DevBuf<int> counters, error, curWave;
   DevBuf<unsigned long long> stats;
   DevBuf<DevWave> waves, waveSlot;
@@ -174,7 +177,7 @@ rg_status ensureQueues(rg_handle* h, int capacity, int maxIter) {
   const int mi = std::max(maxIter, h->maxIter);
   bool ok = h->rayO0.alloc(c) && h->rayO1.alloc(c) && h->rayD0.alloc(c) && h->rayD1.alloc(c) && h->hits.alloc(c) &&
             h->pathT.alloc(c) && h->pathR.alloc(c) && h->pathL.alloc(c) && h->shO0.alloc(c) && h->shO1.alloc(c) &&
-            h->shD0.alloc(c) && h->shD1.alloc(c) && h->shC0.alloc(c) && h->shC1.alloc(c) &&
+            h->shD0.alloc(c) && h->shD1.alloc(c) && h->shC0.alloc(c) && h->shC1.alloc(c) && h->pathPS.alloc(c) &&
             h->counters.alloc((size_t)(mi + 1) * kCountersPerIter) && h->error.alloc(1) && h->stats.alloc(8) &&
             h->curWave.alloc(1);
   if (!ok) {
@@ -197,6 +200,7 @@ DevQueues makeQueues(rg_handle* h, int maxIter) {
   Q.rayD[0] = h->rayD0.p; Q.rayD[1] = h->rayD1.p;
   Q.hits = h->hits.p;
   Q.pathT = h->pathT.p; Q.pathR = h->pathR.p; Q.pathL = h->pathL.p;
+  Q.pathPS = h->pathPS.p;
   Q.shO[0] = h->shO0.p; Q.shO[1] = h->shO1.p;
   Q.shD[0] = h->shD0.p; Q.shD[1] = h->shD1.p;
   Q.shC[0] = h->shC0.p; Q.shC[1] = h->shC1.p;
@@ -254,27 +258,28 @@ Grids grids(rg_handle* h) {
 }
 
 // Launch one wave's kernel sequence on the stream (captured or direct).
-void enqueueWave(rg_handle* h, const DevRender& R, const DevQueues& Q, const DevWave* W, const int* cur, bool profile,
+void enqueueWave(rg_handle* h, const DevRender& R, const DevQueues& Q, const DevJob* jobs, const DevWave* W, bool profile,
                  std::vector<cudaEvent_t>* ev) {
-  (void)cur;
+  const int shader = R.shader;
   const Grids g = grids(h);
   const cudaStream_t st = h->stream;
-  if (R.shader != 5) {
-    launchSimple(h->dscene, R, W, Q, g.simple, st);
+  const int width = h->dscene.bvhWidth;
+  if (shader != 5) {
+    launchSimple(jobs, W, Q, g.simple, st);
   } else {
-    launchGenerate(R, W, Q, h->dscene.globalMedium, g.gen, st);
+    launchGenerate(jobs, W, Q, g.gen, st);
     for (int it = 0; it < Q.maxIter; it++) {
       if (profile) cudaEventRecord((*ev)[it * 4 + 0], st);
-      launchExtend(h->dscene, Q, it, g.ext, st);
+      launchExtend(&h->dscene, jobs, width, Q, it, g.ext, st);
       if (profile) cudaEventRecord((*ev)[it * 4 + 1], st);
-      launchShade(h->dscene, R, W, Q, it, g.shade, st);
+      launchShade(&h->dscene, &R, jobs, Q, it, g.shade, st);
       if (profile) cudaEventRecord((*ev)[it * 4 + 2], st);
-      launchConnect(h->dscene, Q, it, 0, g.conn, st);
-      if (h->dscene.numPointLights > 0) launchConnect(h->dscene, Q, it, 1, g.conn, st);
+      launchConnect(&h->dscene, jobs, width, Q, it, 0, g.conn, st);
+      if (h->dscene.numPointLights > 0) launchConnect(&h->dscene, jobs, width, Q, it, 1, g.conn, st);
       if (profile) cudaEventRecord((*ev)[it * 4 + 3], st);
     }
   }
-  launchAccumulate(R, W, Q, h->sum.p, h->sumSq.p, h->cnt.p, g.acc, st);
+  launchAccumulate(jobs, W, Q, g.acc, st);
   k_nextWave<<<1, 1, 0, st>>>(h->curWave.p);
 }
 
@@ -595,20 +600,34 @@ static rg_status runPass(rg_handle* h, const DevRender& R, int numPixels, const 
                          int& wavesDone, int totalWavesHint, bool profile, double* kernelMs) {
   if (numPixels <= 0 || spp <= 0) return RG_OK;
   const long long cap = h->st.paths_per_wave > 0 ? h->st.paths_per_wave : (8ll << 20);
-  std::vector<DevWave> ws;
+  std::vector<DevSegment> sg;
   const int spw = numPixels >= cap ? 1 : (int)std::min<long long>(spp, std::max<long long>(1, cap / numPixels));
   const int pixChunk = (int)std::min<long long>(numPixels, cap);
   for (int s = 0; s < spp; s += spw)
     for (int p = 0; p < numPixels; p += pixChunk) {
-      DevWave w;
-      w.numPixels = std::min(pixChunk, numPixels - p);
-      w.samplesInWave = std::min(spw, spp - s);
-      w.sampleBase = 0;
-      w.pixelOffset = p;
-      w.pixelList = pixelList;
-      w.pixelSampleBase = h->cnt.p;
-      ws.push_back(w);
+      DevSegment e;
+      e.slot = 0;
+      e.numPixels = std::min(pixChunk, numPixels - p);
+      e.samples = std::min(spw, spp - s);
+      e.pathBase = 0;
+      e.pixelOffset = p;
+      e.pixBase = 0;
+      e.pixelList = pixelList;
+      sg.push_back(e);
     }
+  if (!h->segs.alloc(sg.size())) {
+    setLastError("out of device memory (segments)");
+    return RG_ERR_OUT_OF_MEMORY;
+  }
+  std::vector<DevWave> ws(sg.size());
+  for (size_t k = 0; k < sg.size(); k++) {
+    ws[k].numSegments = 1;
+    ws[k].numPaths = sg[k].numPixels * sg[k].samples;
+    ws[k].numPixelsTotal = sg[k].numPixels;
+    ws[k].pad = 0;
+    ws[k].segs = h->segs.p + k;
+  }
+  RG_CUDA_CHECK(cudaMemcpyAsync(h->segs.p, sg.data(), sg.size() * sizeof(DevSegment), cudaMemcpyHostToDevice, h->stream));
   const int capacity = std::min<long long>(cap, (long long)pixChunk * spw);
   const int maxIter = R.maxDepth + 2;
   rg_status rs = ensureQueues(h, capacity, maxIter);
@@ -620,6 +639,19 @@ static rg_status runPass(rg_handle* h, const DevRender& R, int numPixels, const 
   RG_CUDA_CHECK(cudaMemcpyAsync(h->waves.p, ws.data(), ws.size() * sizeof(DevWave), cudaMemcpyHostToDevice, h->stream));
   RG_CUDA_CHECK(cudaMemsetAsync(h->curWave.p, 0, sizeof(int), h->stream));
   const DevQueues Q = makeQueues(h, maxIter);
+  // the single job of this handle
+  if (!h->jobsDev.alloc(1)) return RG_ERR_OUT_OF_MEMORY;
+  {
+    DevJob J;
+    std::memset(&J, 0, sizeof(J));
+    J.S = h->dscene;
+    J.R = R;
+    J.sum = h->sum.p;
+    J.sumSq = h->sumSq.p;
+    J.cnt = h->cnt.p;
+    RG_CUDA_CHECK(cudaMemcpyAsync(h->jobsDev.p, &J, sizeof(J), cudaMemcpyHostToDevice, h->stream));
+    RG_CUDA_CHECK(cudaStreamSynchronize(h->stream));
+  }
   // the kernels read the current wave from a fixed one-element slot
   if (!h->waveSlot.alloc(1)) return RG_ERR_OUT_OF_MEMORY;
   DevWave* slot = h->waveSlot.p;
@@ -631,7 +663,7 @@ static rg_status runPass(rg_handle* h, const DevRender& R, int numPixels, const 
   // graph of one wave: select the wave descriptor, then the kernel sequence
   const std::string key = std::to_string((uintptr_t)h->waves.p) + ":" + std::to_string((uintptr_t)slot) + ":" +
                           std::to_string(maxIter) + ":" + std::to_string(R.shader) + ":" + std::to_string(h->capacity) +
-                          ":" + std::to_string((uintptr_t)pixelList) + ":" +
+                          ":" + std::to_string((uintptr_t)pixelList) + ":" + std::to_string((uintptr_t)h->jobsDev.p) + ":" +
                           std::string((const char*)&R, sizeof(R));
   if (!profile && (h->graph == nullptr || h->graphKey != key)) {
     if (h->graph) {
@@ -641,7 +673,7 @@ static rg_status runPass(rg_handle* h, const DevRender& R, int numPixels, const 
     cudaGraph_t g;
     RG_CUDA_CHECK(cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
     k_selectWave<<<1, 1, 0, h->stream>>>(h->waves.p, h->curWave.p, slot);
-    enqueueWave(h, R, Q, slot, h->curWave.p, false, nullptr);
+    enqueueWave(h, R, Q, h->jobsDev.p, slot, false, nullptr);
     RG_CUDA_CHECK(cudaStreamEndCapture(h->stream, &g));
     const cudaError_t ie = cudaGraphInstantiate(&h->graph, g, 0);
     cudaGraphDestroy(g);
@@ -656,7 +688,7 @@ static rg_status runPass(rg_handle* h, const DevRender& R, int numPixels, const 
     if (h->cancel.load()) return RG_ERR_CANCELLED;
     if (profile) {
       k_selectWave<<<1, 1, 0, h->stream>>>(h->waves.p, h->curWave.p, slot);
-      enqueueWave(h, R, Q, slot, h->curWave.p, true, &ev);
+      enqueueWave(h, R, Q, h->jobsDev.p, slot, true, &ev);
       RG_CUDA_CHECK(cudaStreamSynchronize(h->stream));
       if (R.shader == 5) {
         for (int it = 0; it < maxIter; it++) {

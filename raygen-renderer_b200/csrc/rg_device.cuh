@@ -115,27 +115,52 @@ struct DevRender {
   int aoSamples;              // settings.samples (calcAO loop count)
 };
 
-// One wave: paths p = s_local * numPixels + i, pixel = pixelList ? pixelList[i] : i.
-struct DevWave {
+// One render job resident on the device: its scene, render constants and
+// accumulation buffers.  Kernels index a table of jobs by slot; the ray and
+// shadow queues carry the slot of every ray.
+struct DevJob {
+  DevScene S;
+  DevRender R;
+  float4* sum;
+  float4* sumSq;
+  int* cnt;                   // samples per pixel so far (= next sample index)
+  int pad[2];
+};
+
+// A wave is a list of segments; segment k holds paths
+// [pathBase, pathBase + numPixels * samples) of job `slot`:
+//   path = pathBase + s * numPixels + i, pixel = pixelList ? pixelList[pixelOffset + i] : pixelOffset + i,
+//   sample = cnt[pixel] + s.
+struct DevSegment {
+  int slot;
   int numPixels;
-  int samplesInWave;
-  int sampleBase;
-  int pixelOffset;            // first entry of this wave in pixelList (or first pixel)
-  const int* pixelList;       // NULL: identity
-  const int* pixelSampleBase; // per pixel: first sample index (NULL: sampleBase)
+  int samples;
+  int pathBase;
+  int pixelOffset;
+  int pixBase;                // prefix sum of numPixels over the wave's segments
+  const int* pixelList;
+};
+
+struct DevWave {
+  int numSegments;
+  int numPaths;
+  int numPixelsTotal;
+  int pad;
+  const DevSegment* segs;
 };
 
 // Wavefront buffers.
 struct DevQueues {
   float4* rayO[2];            // (origin, path id bits)
-  float4* rayD[2];            // (dir, 0)
+  float4* rayD[2];            // (dir, job slot bits)
   float4* hits;               // (t, u, v, prim bits) per queue slot
   float4* pathT;              // (beta rgb, bsdfPdf)
   float4* pathR;              // (rrT rgb, flags bits)
   float4* pathL;              // (L rgb, vertex bits)
+  int2* pathPS;               // (pixel, sample) of every path
   float4* shO[2];             // shadow queues A (area) / B (point): (origin, path id bits)
   float4* shD[2];             // (dir, tmax)
-  float4* shC[2];             // (contribution rgb, predicate bits)
+  float4* shC[2];             // (contribution rgb, job slot bits)
   int* counters;              // per-iteration counters, zeroed by the generate kernel
   unsigned long long* stats;  // [0] nodes closest [1] tris closest [2] nodes shadow [3] tris shadow [4] closest rays [5] shadow rays
   int* error;                 // first device error code

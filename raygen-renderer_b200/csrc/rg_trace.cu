@@ -260,14 +260,25 @@ __device__ bool sampleAreaLightForNEE(const DevScene& S, const DevRender& R, con
 }
 
 // ------------------------------------------------------------ kernels ----
-__device__ __forceinline__ void waveCoords(const DevRender& R, const DevWave& W, int pid, int& px, int& py,
-                                           uint32_t& sample) {
-  const int i = pid % W.numPixels;
-  const int sl = pid / W.numPixels;
-  const int pixel = W.pixelList ? W.pixelList[W.pixelOffset + i] : W.pixelOffset + i;
-  px = pixel % R.width;
-  py = pixel / R.width;
-  sample = (uint32_t)((W.pixelSampleBase ? W.pixelSampleBase[pixel] : W.sampleBase) + sl);
+// Segment of the wave holding path p (segments are few; linear scan after a
+// binary search on the path prefix).
+__device__ __forceinline__ int segmentOfPath(const DevWave& W, int p) {
+  int lo = 0, hi = W.numSegments - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (W.segs[mid].pathBase <= p) lo = mid;
+    else hi = mid - 1;
+  }
+  return lo;
+}
+__device__ __forceinline__ int segmentOfPixel(const DevWave& W, int t) {
+  int lo = 0, hi = W.numSegments - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (W.segs[mid].pixBase <= t) lo = mid;
+    else hi = mid - 1;
+  }
+  return lo;
 }
 
 __device__ __forceinline__ int dimBaseOf(const DevRender& R) { return (R.dof >= 0.001f && R.aperture > 0.0f) ? 4 : 2; }
@@ -311,35 +322,40 @@ __device__ void primaryRay(const DevRender& R, const Rng& rng, int x, int y, V3&
   }
 }
 
-__global__ void __launch_bounds__(256) k_generate(DevRender R, const DevWave* __restrict__ Wp, DevQueues Q,
-                                                  int globalMedium) {
+__global__ void __launch_bounds__(256) k_generate(const DevJob* __restrict__ jobs, const DevWave* __restrict__ Wp,
+                                                  DevQueues Q) {
   const DevWave W = *Wp;
-  const int numPaths = W.numPixels * W.samplesInWave;
+  const int numPaths = W.numPaths;
   if (blockIdx.x == 0) {
     for (int i = threadIdx.x; i < Q.maxIter * kCountersPerIter; i += blockDim.x) Q.counters[i] = 0;
     __syncthreads();
     if (threadIdx.x == 0) Q.counters[C_RAYS] = numPaths;
   }
-  const int dimBase = dimBaseOf(R);
-  const uint32_t medFlag = (uint32_t)(globalMedium + 1) << F_MED_SHIFT;
   for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < numPaths; p += gridDim.x * blockDim.x) {
-    int x, y;
-    uint32_t sample;
-    waveCoords(R, W, p, x, y, sample);
+    const DevSegment seg = W.segs[segmentOfPath(W, p)];
+    const int local = p - seg.pathBase;
+    const int i = local % seg.numPixels, sl = local / seg.numPixels;
+    const int pixel = seg.pixelList ? seg.pixelList[seg.pixelOffset + i] : seg.pixelOffset + i;
+    const DevJob& J = jobs[seg.slot];
+    const DevRender& R = J.R;
+    const int x = pixel % R.width, y = pixel / R.width;
+    const uint32_t sample = (uint32_t)(J.cnt[pixel] + sl);
     Rng rng;
-    rng.init(x, y, R.width, sample, R.seed, dimBase);
+    rng.init(x, y, R.width, sample, R.seed, dimBaseOf(R));
     V3 o, d;
     primaryRay(R, rng, x, y, o, d);
+    const uint32_t medFlag = (uint32_t)(J.S.globalMedium + 1) << F_MED_SHIFT;
     Q.rayO[0][p] = make_float4(o.x, o.y, o.z, __int_as_float(p));
-    Q.rayD[0][p] = make_float4(d.x, d.y, d.z, 0.0f);
+    Q.rayD[0][p] = make_float4(d.x, d.y, d.z, __int_as_float(seg.slot));
     Q.pathT[p] = make_float4(1.0f, 1.0f, 1.0f, 0.0f);
     Q.pathR[p] = make_float4(1.0f, 1.0f, 1.0f, __uint_as_float(F_EYE | medFlag));
     Q.pathL[p] = make_float4(0.0f, 0.0f, 0.0f, __int_as_float(0));
+    Q.pathPS[p] = make_int2(pixel, (int)sample);
   }
 }
 
 // Closest hit for the iteration's queue; persistent warps fetch 32 rays at a time.
-__global__ void __launch_bounds__(128) k_extend(DevScene S, DevQueues Q, int iter) {
+__global__ void __launch_bounds__(128) k_extend(const DevJob* __restrict__ jobs, DevQueues Q, int iter) {
   const int count = Q.counters[iter * kCountersPerIter + C_RAYS];
   int* fetch = &Q.counters[iter * kCountersPerIter + C_FETCH_EXT];
   const float4* __restrict__ rO = Q.rayO[iter & 1];
@@ -354,6 +370,7 @@ __global__ void __launch_bounds__(128) k_extend(DevScene S, DevQueues Q, int ite
     const int q = base + lane;
     if (q < count) {
       const float4 a = rO[q], b = rD[q];
+      const DevScene& S = jobs[__float_as_int(b.w)].S;
       const ClosestHit h = traceClosest2(S, xyz(a), xyz(b), nodes, tris);
       Q.hits[q] = make_float4(h.t, h.u, h.v, __int_as_float(h.prim));
       rays++;
@@ -365,7 +382,7 @@ __global__ void __launch_bounds__(128) k_extend(DevScene S, DevQueues Q, int ite
 }
 
 // Shadow-ray visibility; unoccluded contributions are added to the path.
-__global__ void __launch_bounds__(128) k_connect(DevScene S, DevQueues Q, int iter, int which) {
+__global__ void __launch_bounds__(128) k_connect(const DevJob* __restrict__ jobs, DevQueues Q, int iter, int which) {
   const int count = Q.counters[iter * kCountersPerIter + (which ? C_SHB : C_SHA)];
   int* fetch = &Q.counters[iter * kCountersPerIter + (which ? C_FETCH_SHB : C_FETCH_SHA)];
   const float4* __restrict__ sO = Q.shO[which];
@@ -382,9 +399,10 @@ __global__ void __launch_bounds__(128) k_connect(DevScene S, DevQueues Q, int it
     const int q = base + lane;
     if (q < count) {
       const float4 a = sO[q], b = sD[q];
+      const float4 c = sC[q];
+      const DevScene& S = jobs[__float_as_int(c.w)].S;
       rays++;
       if (!traceAny2(S, xyz(a), xyz(b), b.w, occ, nodes, tris)) {
-        const float4 c = sC[q];
         const int pid = __float_as_int(a.w);
         float4 l = Q.pathL[pid];
         l.x += c.x; l.y += c.y; l.z += c.z;
@@ -411,8 +429,8 @@ __global__ void __launch_bounds__(128) k_connect(DevScene S, DevQueues Q, int it
 constexpr int kRefillIdle = 8;     // refill once this many lanes are idle
 constexpr int kTriVotes = 10;      // lanes with triangles needed to run a triangle step
 
-template <bool ANY>
-__device__ __forceinline__ void traverseWave8(const DevScene& S, int count, int* fetch, const float4* __restrict__ rO,
+template <bool ANY, bool MULTI>
+__device__ __forceinline__ void traverseWave8(const DevScene& S0, const DevJob* __restrict__ jobs, int count, int* fetch, const float4* __restrict__ rO,
                                               const float4* __restrict__ rD, uint32_t occ, float4* __restrict__ hitsOut,
                                               const float4* __restrict__ contrib, float4* __restrict__ pathL,
                                               uint32_t& nodes, uint32_t& tris, uint32_t& rays) {
@@ -426,6 +444,10 @@ __device__ __forceinline__ void traverseWave8(const DevScene& S, int count, int*
   uint32_t gInner = 0, gImask = 0, tMask = 0;
   int gBase = 0, tBase = 0, sp = 0, steps = 0;
   uint2 stack[kStack8];
+  const float4* nodesP = nullptr;
+  const float4* trisP = nullptr;
+  int numNodes = 0;
+  int* errP = nullptr;
   for (;;) {
     // ---- refill idle lanes
     const bool need = q == -1;
@@ -442,11 +464,26 @@ __device__ __forceinline__ void traverseWave8(const DevScene& S, int count, int*
           const float4 a = rO[q], b = rD[q];
           o = xyz(a);
           d = xyz(b);
+          int slot;
           if (ANY) {
             tmax = b.w;
             pid = __float_as_int(a.w);
+            slot = __float_as_int(contrib[q].w);
           } else {
             tmax = kMaxRayDistance;
+            slot = __float_as_int(b.w);
+          }
+          if (MULTI) {
+            const DevScene& S = jobs[slot].S;
+            nodesP = S.nodes8;
+            trisP = S.triVerts;
+            numNodes = S.numNodes8;
+            errP = S.error;
+          } else {
+            nodesP = S0.nodes8;
+            trisP = S0.triVerts;
+            numNodes = S0.numNodes8;
+            errP = S0.error;
           }
           prim = -1;
           hu = hv = 0.0f;
@@ -492,7 +529,7 @@ __device__ __forceinline__ void traverseWave8(const DevScene& S, int count, int*
           const int i = __ffs(tMask) - 1;
           tMask &= tMask - 1u;
           const int tk = tBase + i;
-          const float4* tp = S.triVerts + (size_t)tk * 3;
+          const float4* tp = trisP + (size_t)tk * 3;
           const float4 b = ldg4(tp + 1);
           if (!ANY || (__float_as_uint(b.w) & occ)) {
             const float4 a = ldg4(tp), c = ldg4(tp + 2);
@@ -516,7 +553,7 @@ __device__ __forceinline__ void traverseWave8(const DevScene& S, int count, int*
           // node step (pending triangles are postponed onto the stack)
           if (hasTri) {
             if (sp < kStack8) stack[sp++] = make_uint2((uint32_t)tBase | 0x80000000u, tMask);
-            else atomicCAS(S.error, 0, kErrStackOverflow);
+            else atomicCAS(errP, 0, kErrStackOverflow);
             tMask = 0;
           }
           const int pos = 31 - __clz(gInner);
@@ -525,13 +562,13 @@ __device__ __forceinline__ void traverseWave8(const DevScene& S, int count, int*
           const int node = gBase + __popc(gImask & ((1u << slot) - 1u));
           if (gInner) {
             if (sp < kStack8) stack[sp++] = make_uint2((uint32_t)gBase, gInner | (gImask << 8));
-            else atomicCAS(S.error, 0, kErrStackOverflow);
+            else atomicCAS(errP, 0, kErrStackOverflow);
           }
-          if (node >= S.numNodes8 || ++steps > kMaxTraversalSteps) {
-            atomicCAS(S.error, 0, kErrTraversalSteps);
+          if (node >= numNodes || ++steps > kMaxTraversalSteps) {
+            atomicCAS(errP, 0, kErrTraversalSteps);
             result = ANY ? 2 : 1;
           } else {
-            const Node8Hit g = intersectNode8(S.nodes8 + (size_t)node * 5, o, inv, tmax, oct);
+            const Node8Hit g = intersectNode8(nodesP + (size_t)node * 5, o, inv, tmax, oct);
             nodes++;
             gInner = g.inner;
             gImask = g.imask;
@@ -563,20 +600,23 @@ __device__ __forceinline__ void traverseWave8(const DevScene& S, int count, int*
   }
 }
 
-__global__ void __launch_bounds__(128) k_extend8(DevScene S, DevQueues Q, int iter) {
+template <bool MULTI>
+__global__ void __launch_bounds__(128) k_extend8(DevScene S0, const DevJob* __restrict__ jobs, DevQueues Q, int iter) {
   const int count = Q.counters[iter * kCountersPerIter + C_RAYS];
   uint32_t nodes = 0, tris = 0, rays = 0;
-  traverseWave8<false>(S, count, &Q.counters[iter * kCountersPerIter + C_FETCH_EXT], Q.rayO[iter & 1],
+  traverseWave8<false, MULTI>(S0, jobs, count, &Q.counters[iter * kCountersPerIter + C_FETCH_EXT], Q.rayO[iter & 1],
                        Q.rayD[iter & 1], 0u, Q.hits, nullptr, nullptr, nodes, tris, rays);
   warpAddStat(&Q.stats[0], nodes);
   warpAddStat(&Q.stats[1], tris);
   warpAddStat(&Q.stats[4], rays);
 }
 
-__global__ void __launch_bounds__(128) k_connect8(DevScene S, DevQueues Q, int iter, int which) {
+template <bool MULTI>
+__global__ void __launch_bounds__(128) k_connect8(DevScene S0, const DevJob* __restrict__ jobs, DevQueues Q, int iter,
+                                                  int which) {
   const int count = Q.counters[iter * kCountersPerIter + (which ? C_SHB : C_SHA)];
   uint32_t nodes = 0, tris = 0, rays = 0;
-  traverseWave8<true>(S, count, &Q.counters[iter * kCountersPerIter + (which ? C_FETCH_SHB : C_FETCH_SHA)],
+  traverseWave8<true, MULTI>(S0, jobs, count, &Q.counters[iter * kCountersPerIter + (which ? C_FETCH_SHB : C_FETCH_SHA)],
                       Q.shO[which], Q.shD[which], which ? kOccPoint : kOccArea, nullptr, Q.shC[which], Q.pathL, nodes,
                       tris, rays);
   warpAddStat(&Q.stats[2], nodes);
@@ -585,12 +625,13 @@ __global__ void __launch_bounds__(128) k_connect8(DevScene S, DevQueues Q, int i
 }
 
 // One path vertex (RayBSDFShaderProvider::shade + lobes + tracePath's medium branch).
-__global__ void __launch_bounds__(256) k_shade(DevScene S, DevRender R, const DevWave* __restrict__ Wp, DevQueues Q,
+// MULTI = false: one job whose scene and render constants come in as kernel
+// parameters (constant bank); MULTI = true: per-ray job slot into the table.
+template <bool MULTI>
+__global__ void __launch_bounds__(256) k_shade(DevScene S0, DevRender R0, const DevJob* __restrict__ jobs, DevQueues Q,
                                                int iter) {
-  const DevWave W = *Wp;
   const int count = Q.counters[iter * kCountersPerIter + C_RAYS];
   const int inB = iter & 1, outB = (iter + 1) & 1;
-  const int dimBase = dimBaseOf(R);
   const int stride = gridDim.x * blockDim.x;
   const int rounded = ((count + 31) / 32) * 32;
   for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < rounded; q += stride) {
@@ -600,10 +641,13 @@ __global__ void __launch_bounds__(256) k_shade(DevScene S, DevRender R, const De
     shB.on = false;
     bool cont = false;
     V3 no = v3(0, 0, 0), nd = v3(0, 0, 0);
-    int pid = 0;
+    int pid = 0, slot = 0;
     if (valid) {
       const float4 ro = Q.rayO[inB][q], rd = Q.rayD[inB][q];
       pid = __float_as_int(ro.w);
+      slot = __float_as_int(rd.w);
+      const DevScene S = MULTI ? jobs[slot].S : S0;
+      const DevRender R = MULTI ? jobs[slot].R : R0;
       const V3 o = xyz(ro), d = xyz(rd);
       const float4 hq = Q.hits[q];
       const int prim = __float_as_int(hq.w);
@@ -619,11 +663,10 @@ __global__ void __launch_bounds__(256) k_shade(DevScene S, DevRender R, const De
       int chroma = (int)((flags & F_CHROMA_MASK) >> F_CHROMA_SHIFT) - 1;
       int med = (int)((flags & F_MED_MASK) >> F_MED_SHIFT) - 1;
       if (eye && prim < 0) flags |= F_EYE_NOHIT;
-      int x, y;
-      uint32_t sample;
-      waveCoords(R, W, pid, x, y, sample);
+      const int2 ps = Q.pathPS[pid];
+      const int x = ps.x % R.width, y = ps.x / R.width;
       Rng rng;
-      rng.init(x, y, R.width, sample, R.seed, dimBase);
+      rng.init(x, y, R.width, (uint32_t)ps.y, R.seed, dimBaseOf(R));
       bool done = false;
       bool silhouette = false;
       // ---- participating medium on the segment (tracePath, rayrenderer.cpp:1665-1831)
@@ -995,22 +1038,22 @@ __global__ void __launch_bounds__(256) k_shade(DevScene S, DevRender R, const De
       }
     }
     // queue pushes (warp-aggregated)
-    const int slot = warpPush(&Q.counters[(iter + 1) * kCountersPerIter + C_RAYS], cont && (iter + 1) < Q.maxIter);
-    if (slot >= 0) {
-      Q.rayO[outB][slot] = make_float4(no.x, no.y, no.z, __int_as_float(pid));
-      Q.rayD[outB][slot] = make_float4(nd.x, nd.y, nd.z, 0.0f);
+    const int qslot = warpPush(&Q.counters[(iter + 1) * kCountersPerIter + C_RAYS], cont && (iter + 1) < Q.maxIter);
+    if (qslot >= 0) {
+      Q.rayO[outB][qslot] = make_float4(no.x, no.y, no.z, __int_as_float(pid));
+      Q.rayD[outB][qslot] = make_float4(nd.x, nd.y, nd.z, __int_as_float(slot));
     }
     const int sa = warpPush(&Q.counters[iter * kCountersPerIter + C_SHA], shA.on);
     if (sa >= 0) {
       Q.shO[0][sa] = make_float4(shA.o.x, shA.o.y, shA.o.z, __int_as_float(pid));
       Q.shD[0][sa] = make_float4(shA.d.x, shA.d.y, shA.d.z, shA.tmax);
-      Q.shC[0][sa] = make_float4(shA.c.x, shA.c.y, shA.c.z, 0.0f);
+      Q.shC[0][sa] = make_float4(shA.c.x, shA.c.y, shA.c.z, __int_as_float(slot));
     }
     const int sb = warpPush(&Q.counters[iter * kCountersPerIter + C_SHB], shB.on);
     if (sb >= 0) {
       Q.shO[1][sb] = make_float4(shB.o.x, shB.o.y, shB.o.z, __int_as_float(pid));
       Q.shD[1][sb] = make_float4(shB.d.x, shB.d.y, shB.d.z, shB.tmax);
-      Q.shC[1][sb] = make_float4(shB.c.x, shB.c.y, shB.c.z, 0.0f);
+      Q.shC[1][sb] = make_float4(shB.c.x, shB.c.y, shB.c.z, __int_as_float(slot));
     }
   }
 }
@@ -1045,17 +1088,22 @@ __device__ V3 lambertLights(const DevScene& S, const DevRender& R, const Rng& rn
   return acc + v3(R.worldR, R.worldG, R.worldB);
 }
 
-__global__ void __launch_bounds__(128) k_simple(DevScene S, DevRender R, const DevWave* __restrict__ Wp, DevQueues Q) {
+__global__ void __launch_bounds__(128) k_simple(const DevJob* __restrict__ jobs, const DevWave* __restrict__ Wp,
+                                                DevQueues Q) {
   const DevWave W = *Wp;
-  const int numPaths = W.numPixels * W.samplesInWave;
-  const int dimBase = dimBaseOf(R);
+  const int numPaths = W.numPaths;
   uint32_t nodes = 0, tris = 0;
   for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < numPaths; p += gridDim.x * blockDim.x) {
-    int x, y;
-    uint32_t sample;
-    waveCoords(R, W, p, x, y, sample);
+    const DevSegment seg = W.segs[segmentOfPath(W, p)];
+    const int local = p - seg.pathBase;
+    const int li = local % seg.numPixels, sl = local / seg.numPixels;
+    const int pixel = seg.pixelList ? seg.pixelList[seg.pixelOffset + li] : seg.pixelOffset + li;
+    const DevScene& S = jobs[seg.slot].S;
+    const DevRender& R = jobs[seg.slot].R;
+    const int x = pixel % R.width, y = pixel / R.width;
+    const uint32_t sample = (uint32_t)(jobs[seg.slot].cnt[pixel] + sl);
     Rng rng;
-    rng.init(x, y, R.width, sample, R.seed, dimBase);
+    rng.init(x, y, R.width, sample, R.seed, dimBaseOf(R));
     V3 o, d;
     primaryRay(R, rng, x, y, o, d);
     // tracePath through transparent surfaces, accumulating (color, weight)
@@ -1111,15 +1159,18 @@ __global__ void __launch_bounds__(128) k_simple(DevScene S, DevRender R, const D
 }
 
 // Per-sample clamp and accumulation into the pixel sums (rayrenderer.cpp:936-951).
-__global__ void __launch_bounds__(256) k_accumulate(DevRender R, const DevWave* __restrict__ Wp, DevQueues Q,
-                                                    float4* __restrict__ sum, float4* __restrict__ sumSq,
-                                                    int* __restrict__ cnt) {
+__global__ void __launch_bounds__(256) k_accumulate(const DevJob* __restrict__ jobs, const DevWave* __restrict__ Wp,
+                                                    DevQueues Q) {
   const DevWave W = *Wp;
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < W.numPixels; i += gridDim.x * blockDim.x) {
-    const int pixel = W.pixelList ? W.pixelList[W.pixelOffset + i] : W.pixelOffset + i;
+  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < W.numPixelsTotal; t += gridDim.x * blockDim.x) {
+    const DevSegment seg = W.segs[segmentOfPixel(W, t)];
+    const int i = t - seg.pixBase;
+    const int pixel = seg.pixelList ? seg.pixelList[seg.pixelOffset + i] : seg.pixelOffset + i;
+    const DevJob& J = jobs[seg.slot];
+    const DevRender& R = J.R;
     float sr = 0, sg = 0, sb = 0, qr = 0, qg = 0, qb = 0;
-    for (int s = 0; s < W.samplesInWave; s++) {
-      const int p = s * W.numPixels + i;
+    for (int s = 0; s < seg.samples; s++) {
+      const int p = seg.pathBase + s * seg.numPixels + i;
       const float4 l = Q.pathL[p];
       const uint32_t flags = __float_as_uint(Q.pathR[p].w);
       float r = l.x, g = l.y, b = l.z;
@@ -1129,12 +1180,12 @@ __global__ void __launch_bounds__(256) k_accumulate(DevRender R, const DevWave* 
       sr += r; sg += g; sb += b;
       qr += r * r; qg += g * g; qb += b * b;
     }
-    float4 a = sum[pixel], c = sumSq[pixel];
+    float4 a = J.sum[pixel], c = J.sumSq[pixel];
     a.x += sr; a.y += sg; a.z += sb;
     c.x += qr; c.y += qg; c.z += qb;
-    sum[pixel] = a;
-    sumSq[pixel] = c;
-    cnt[pixel] += W.samplesInWave;
+    J.sum[pixel] = a;
+    J.sumSq[pixel] = c;
+    J.cnt[pixel] += seg.samples;
   }
 }
 
@@ -1200,32 +1251,42 @@ __global__ void k_queryAny(DevScene S, const float* __restrict__ rays, const flo
 // Resident blocks per SM for the persistent traversal kernels.
 int residentBlocks(int kernel, int width) {
   int perSM = 0;
-  if (kernel == 0) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSM, width == 8 ? (const void*)k_extend8 : (const void*)k_extend, 128, 0);
-  else cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSM, width == 8 ? (const void*)k_connect8 : (const void*)k_connect, 128, 0);
+  if (kernel == 0) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSM, width == 8 ? (const void*)k_extend8<true> : (const void*)k_extend, 128, 0);
+  else cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSM, width == 8 ? (const void*)k_connect8<true> : (const void*)k_connect, 128, 0);
   return perSM < 1 ? 1 : perSM;
 }
 
-void launchGenerate(const DevRender& R, const DevWave* W, const DevQueues& Q, int globalMedium, int grid, cudaStream_t st) {
-  k_generate<<<grid, 256, 0, st>>>(R, W, Q, globalMedium);
+void launchGenerate(const DevJob* jobs, const DevWave* W, const DevQueues& Q, int grid, cudaStream_t st) {
+  k_generate<<<grid, 256, 0, st>>>(jobs, W, Q);
 }
-void launchExtend(const DevScene& S, const DevQueues& Q, int iter, int grid, cudaStream_t st) {
-  if (S.bvhWidth == 8) k_extend8<<<grid, 128, 0, st>>>(S, Q, iter);
-  else k_extend<<<grid, 128, 0, st>>>(S, Q, iter);
+void launchExtend(const DevScene* single, const DevJob* jobs, int width, const DevQueues& Q, int iter, int grid,
+                  cudaStream_t st) {
+  if (width == 8) {
+    if (single) k_extend8<false><<<grid, 128, 0, st>>>(*single, jobs, Q, iter);
+    else k_extend8<true><<<grid, 128, 0, st>>>(DevScene{}, jobs, Q, iter);
+  } else {
+    k_extend<<<grid, 128, 0, st>>>(jobs, Q, iter);
+  }
 }
-void launchShade(const DevScene& S, const DevRender& R, const DevWave* W, const DevQueues& Q, int iter, int grid,
-                 cudaStream_t st) {
-  k_shade<<<grid, 256, 0, st>>>(S, R, W, Q, iter);
+void launchShade(const DevScene* single, const DevRender* singleR, const DevJob* jobs, const DevQueues& Q, int iter,
+                 int grid, cudaStream_t st) {
+  if (single) k_shade<false><<<grid, 256, 0, st>>>(*single, *singleR, jobs, Q, iter);
+  else k_shade<true><<<grid, 256, 0, st>>>(DevScene{}, DevRender{}, jobs, Q, iter);
 }
-void launchConnect(const DevScene& S, const DevQueues& Q, int iter, int which, int grid, cudaStream_t st) {
-  if (S.bvhWidth == 8) k_connect8<<<grid, 128, 0, st>>>(S, Q, iter, which);
-  else k_connect<<<grid, 128, 0, st>>>(S, Q, iter, which);
+void launchConnect(const DevScene* single, const DevJob* jobs, int width, const DevQueues& Q, int iter, int which,
+                   int grid, cudaStream_t st) {
+  if (width == 8) {
+    if (single) k_connect8<false><<<grid, 128, 0, st>>>(*single, jobs, Q, iter, which);
+    else k_connect8<true><<<grid, 128, 0, st>>>(DevScene{}, jobs, Q, iter, which);
+  } else {
+    k_connect<<<grid, 128, 0, st>>>(jobs, Q, iter, which);
+  }
 }
-void launchSimple(const DevScene& S, const DevRender& R, const DevWave* W, const DevQueues& Q, int grid, cudaStream_t st) {
-  k_simple<<<grid, 128, 0, st>>>(S, R, W, Q);
+void launchSimple(const DevJob* jobs, const DevWave* W, const DevQueues& Q, int grid, cudaStream_t st) {
+  k_simple<<<grid, 128, 0, st>>>(jobs, W, Q);
 }
-void launchAccumulate(const DevRender& R, const DevWave* W, const DevQueues& Q, float4* sum, float4* sumSq, int* cnt,
-                      int grid, cudaStream_t st) {
-  k_accumulate<<<grid, 256, 0, st>>>(R, W, Q, sum, sumSq, cnt);
+void launchAccumulate(const DevJob* jobs, const DevWave* W, const DevQueues& Q, int grid, cudaStream_t st) {
+  k_accumulate<<<grid, 256, 0, st>>>(jobs, W, Q);
 }
 void launchAov(const DevScene& S, const DevRender& R, __half* normal, __half* albedo, __half* albedoA, __half* depth,
                cudaStream_t st) {

@@ -8,14 +8,17 @@
 namespace rg {
 
 int residentBlocks(int kernel, int width);
-void launchGenerate(const DevRender& R, const DevWave* W, const DevQueues& Q, int globalMedium, int grid, cudaStream_t st);
-void launchExtend(const DevScene& S, const DevQueues& Q, int iter, int grid, cudaStream_t st);
-void launchShade(const DevScene& S, const DevRender& R, const DevWave* W, const DevQueues& Q, int iter, int grid,
-                 cudaStream_t st);
-void launchConnect(const DevScene& S, const DevQueues& Q, int iter, int which, int grid, cudaStream_t st);
-void launchSimple(const DevScene& S, const DevRender& R, const DevWave* W, const DevQueues& Q, int grid, cudaStream_t st);
-void launchAccumulate(const DevRender& R, const DevWave* W, const DevQueues& Q, float4* sum, float4* sumSq, int* cnt,
-                      int grid, cudaStream_t st);
+void launchGenerate(const DevJob* jobs, const DevWave* W, const DevQueues& Q, int grid, cudaStream_t st);
+// `single` (and `singleR`) non-null: one job with its constants as kernel parameters;
+// null: per-ray job slots into `jobs`.
+void launchExtend(const DevScene* single, const DevJob* jobs, int width, const DevQueues& Q, int iter, int grid,
+                  cudaStream_t st);
+void launchShade(const DevScene* single, const DevRender* singleR, const DevJob* jobs, const DevQueues& Q, int iter,
+                 int grid, cudaStream_t st);
+void launchConnect(const DevScene* single, const DevJob* jobs, int width, const DevQueues& Q, int iter, int which,
+                   int grid, cudaStream_t st);
+void launchSimple(const DevJob* jobs, const DevWave* W, const DevQueues& Q, int grid, cudaStream_t st);
+void launchAccumulate(const DevJob* jobs, const DevWave* W, const DevQueues& Q, int grid, cudaStream_t st);
 void launchAov(const DevScene& S, const DevRender& R, __half* normal, __half* albedo, __half* albedoA, __half* depth,
                cudaStream_t st);
 void launchQueryClosest(const DevScene& S, const float* rays, int n, float* tuv, int* prim, cudaStream_t st);
