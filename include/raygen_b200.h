@@ -23,6 +23,8 @@
  *   rg_tonemap             <- RayRenderer::applyTonemapGamma src/raygen/rayrenderer.cpp:2610-2647
  *   rg_scene_builtin       <- (procedural stand-ins for the sample scenes; no reference symbol)
  *   rg_load_scene_json     <- RendererSceneLoader::load   src/raygen/sceneloader.cpp:1113-1137
+ *   rg_server_*            <- the viewer's render-job worker (src/viewer/main.cpp:775-850),
+ *                             generalised to many resident jobs (batching / serving)
  */
 #ifndef RAYGEN_B200_H
 #define RAYGEN_B200_H
@@ -229,6 +231,63 @@ rg_status rg_scene_builtin(int32_t kind, uint32_t seed, const int32_t* iparams, 
 rg_status rg_scene_free(rg_scene_desc* scene);
 /* Reference scene JSON (sceneloader.cpp schema) -> flattened description. */
 rg_status rg_load_scene_json(const char* path, rg_scene_desc** out);
+
+/* ---- resident multi-job server (batched and served rendering) ----------- */
+#define RG_JOB_QUEUED 0
+#define RG_JOB_RESIDENT 1
+#define RG_JOB_DONE 2
+#define RG_JOB_FAILED 3
+
+typedef struct rg_server rg_server;
+
+typedef struct rg_server_config {
+  uint64_t hbm_budget_bytes;  /* admission budget for resident jobs [120 GiB]  */
+  int32_t max_resident_jobs;  /* job slots [256]                               */
+  int32_t paths_per_wave;     /* wavefront size shared by all jobs [8 Mi]      */
+  int32_t max_depth_cap;      /* largest max_depth a job may use [10]          */
+} rg_server_config;
+
+/* One render request.  The scene description is borrowed: it must stay valid
+ * until the job reaches RG_JOB_DONE or RG_JOB_FAILED. */
+typedef struct rg_job_desc {
+  const rg_scene_desc* scene;
+  int32_t width, height, samples;
+  int32_t max_depth, rr_depth;  /* <= 0: the server's base settings */
+  uint32_t seed;                /* RNG key: results do not depend on the mix */
+  int32_t denoise;              /* 1: A-Trous on the finished image */
+} rg_job_desc;
+
+typedef struct rg_job_status {
+  int32_t state;                /* RG_JOB_* */
+  rg_status error;
+  double submit_ms, start_ms, done_ms, latency_ms;
+  int64_t samples_issued, samples_total;
+} rg_job_status;
+
+typedef struct rg_server_stats {
+  int64_t jobs_done;
+  double p50_ms, p99_ms, mean_ms, max_ms;  /* submit -> result latency */
+  double images_per_s;                     /* done jobs / (last done - first submit) */
+  uint64_t samples_done;
+  double device_ms;                        /* device time of all waves */
+  int64_t waves;
+  int32_t resident_peak;
+  int32_t pending;
+  uint64_t bytes_peak;                     /* peak admitted footprint estimate */
+} rg_server_stats;
+
+void rg_server_config_default(rg_server_config* c);
+rg_status rg_server_create(const rg_settings* base, const rg_server_config* cfg, rg_server** out);
+rg_status rg_server_submit(rg_server* s, const rg_job_desc* job, int64_t* job_id);
+rg_status rg_server_poll(rg_server* s, int64_t job_id, rg_job_status* out);
+/* RG_ERR_BUSY on timeout. */
+rg_status rg_server_wait(rg_server* s, int64_t job_id, double timeout_ms);
+/* Linear HDR result (width*height*4 floats); release != 0 forgets the job. */
+rg_status rg_server_get_result(rg_server* s, int64_t job_id, float* hdr_rgba, size_t count, int32_t release);
+/* Progressive result of a resident job (current sample mean), taken between waves. */
+rg_status rg_server_snapshot(rg_server* s, int64_t job_id, float* hdr_rgba, size_t count, double timeout_ms);
+rg_status rg_server_get_stats(rg_server* s, rg_server_stats* out);
+rg_status rg_server_destroy(rg_server* s);
 
 #ifdef __cplusplus
 }

@@ -138,6 +138,32 @@ class rg_stats(C.Structure):
     ]
 
 
+class rg_server_config(C.Structure):
+    _fields_ = [("hbm_budget_bytes", C.c_uint64), ("max_resident_jobs", C.c_int32),
+                ("paths_per_wave", C.c_int32), ("max_depth_cap", C.c_int32)]
+
+
+class rg_job_desc(C.Structure):
+    _fields_ = [("scene", C.POINTER(rg_scene_desc)), ("width", C.c_int32), ("height", C.c_int32),
+                ("samples", C.c_int32), ("max_depth", C.c_int32), ("rr_depth", C.c_int32),
+                ("seed", C.c_uint32), ("denoise", C.c_int32)]
+
+
+class rg_job_status(C.Structure):
+    _fields_ = [("state", C.c_int32), ("error", C.c_int32), ("submit_ms", C.c_double), ("start_ms", C.c_double),
+                ("done_ms", C.c_double), ("latency_ms", C.c_double), ("samples_issued", C.c_int64),
+                ("samples_total", C.c_int64)]
+
+
+class rg_server_stats(C.Structure):
+    _fields_ = [("jobs_done", C.c_int64), ("p50_ms", C.c_double), ("p99_ms", C.c_double), ("mean_ms", C.c_double),
+                ("max_ms", C.c_double), ("images_per_s", C.c_double), ("samples_done", C.c_uint64),
+                ("device_ms", C.c_double), ("waves", C.c_int64), ("resident_peak", C.c_int32),
+                ("pending", C.c_int32), ("bytes_peak", C.c_uint64)]
+
+
+RG_JOB_QUEUED, RG_JOB_RESIDENT, RG_JOB_DONE, RG_JOB_FAILED = 0, 1, 2, 3
+
 PROGRESS_FN = C.CFUNCTYPE(None, C.c_float, C.c_void_p)
 
 _lib = None
@@ -178,6 +204,15 @@ def load_library(path: str = LIB_PATH) -> C.CDLL:
         "rg_scene_builtin": (C.c_int, [C.c_int32, C.c_uint32, P(C.c_int32), C.c_int32, P(P(rg_scene_desc))]),
         "rg_scene_free": (C.c_int, [P(rg_scene_desc)]),
         "rg_load_scene_json": (C.c_int, [C.c_char_p, P(P(rg_scene_desc))]),
+        "rg_server_config_default": (None, [P(rg_server_config)]),
+        "rg_server_create": (C.c_int, [P(rg_settings), P(rg_server_config), P(C.c_void_p)]),
+        "rg_server_submit": (C.c_int, [C.c_void_p, P(rg_job_desc), P(C.c_int64)]),
+        "rg_server_poll": (C.c_int, [C.c_void_p, C.c_int64, P(rg_job_status)]),
+        "rg_server_wait": (C.c_int, [C.c_void_p, C.c_int64, C.c_double]),
+        "rg_server_get_result": (C.c_int, [C.c_void_p, C.c_int64, P(C.c_float), C.c_size_t, C.c_int32]),
+        "rg_server_snapshot": (C.c_int, [C.c_void_p, C.c_int64, P(C.c_float), C.c_size_t, C.c_double]),
+        "rg_server_get_stats": (C.c_int, [C.c_void_p, P(rg_server_stats)]),
+        "rg_server_destroy": (C.c_int, [C.c_void_p]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)
@@ -497,3 +532,74 @@ def tonemap(hdr_rgba: np.ndarray) -> np.ndarray:
     out = np.empty_like(hdr)
     _check(lib.rg_tonemap(w, h, _fptr(hdr), _fptr(out)))
     return out
+
+
+class RenderServer:
+    """Resident multi-job server: continuous batching of many render jobs on one GPU.
+
+    Jobs are admitted under an HBM budget; every wave mixes paths of all resident
+    jobs; finished jobs are resolved (optionally A-Trous denoised) on the device.
+    """
+
+    def __init__(self, settings: Optional[RendererSettings] = None, hbm_budget_gb: float = 120.0,
+                 max_resident_jobs: int = 256, paths_per_wave: int = 8 << 20, max_depth_cap: int = 10):
+        self._lib = load_library()
+        cfg = rg_server_config()
+        self._lib.rg_server_config_default(C.byref(cfg))
+        cfg.hbm_budget_bytes = int(hbm_budget_gb * (1 << 30))
+        cfg.max_resident_jobs = max_resident_jobs
+        cfg.paths_per_wave = paths_per_wave
+        cfg.max_depth_cap = max_depth_cap
+        base = (settings or RendererSettings()).to_c()
+        self._h = C.c_void_p()
+        _check(self._lib.rg_server_create(C.byref(base), C.byref(cfg), C.byref(self._h)))
+        self._jobs = {}
+
+    def submit(self, scene: Scene, width: int, height: int, samples: int, max_depth: int = 8, rr_depth: int = 3,
+               seed: int = 1, denoise: bool = False) -> int:
+        d = rg_job_desc()
+        d.scene = scene.ptr
+        d.width, d.height, d.samples = width, height, samples
+        d.max_depth, d.rr_depth, d.seed, d.denoise = max_depth, rr_depth, seed, int(denoise)
+        jid = C.c_int64()
+        _check(self._lib.rg_server_submit(self._h, C.byref(d), C.byref(jid)))
+        self._jobs[jid.value] = (scene, width, height)  # keep the scene alive until done
+        return jid.value
+
+    def status(self, job: int) -> dict:
+        st = rg_job_status()
+        _check(self._lib.rg_server_poll(self._h, job, C.byref(st)))
+        return {f[0]: getattr(st, f[0]) for f in rg_job_status._fields_}
+
+    def wait(self, job: int, timeout_ms: float = 600000.0) -> None:
+        _check(self._lib.rg_server_wait(self._h, job, timeout_ms))
+
+    def result(self, job: int, release: bool = True) -> np.ndarray:
+        _, w, h = self._jobs[job]
+        out = np.empty((h, w, 4), np.float32)
+        _check(self._lib.rg_server_get_result(self._h, job, _fptr(out), out.size, int(release)))
+        if release:
+            self._jobs.pop(job, None)
+        return out
+
+    def snapshot(self, job: int, timeout_ms: float = 10000.0) -> np.ndarray:
+        _, w, h = self._jobs[job]
+        out = np.empty((h, w, 4), np.float32)
+        _check(self._lib.rg_server_snapshot(self._h, job, _fptr(out), out.size, timeout_ms))
+        return out
+
+    def stats(self) -> dict:
+        st = rg_server_stats()
+        _check(self._lib.rg_server_get_stats(self._h, C.byref(st)))
+        return {f[0]: getattr(st, f[0]) for f in rg_server_stats._fields_}
+
+    def close(self):
+        if self._h:
+            self._lib.rg_server_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

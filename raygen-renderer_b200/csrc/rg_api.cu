@@ -38,13 +38,7 @@ void setLastError(const std::string& msg) { g_lastError = msg; }
     }                                                                           \
   } while (0)
 
-namespace {
-
 __global__ void k_nextWave(int* cur) { *cur += 1; }
-
-struct Mat4 {
-  float m[16];
-};
 
 // Camera view matrix, row-vector convention p_view = [p 1] * M.
 // Camera orientation R = Ry(angle.y) * Rx(angle.x) * Rz(angle.z) (degrees);
@@ -79,6 +73,8 @@ Mat4 viewMatrix(const rg_camera& c) {
   M.m[15] = 1.0f;
   return M;
 }
+
+namespace {
 
 inline void xformPoint(const Mat4& M, const float* p, float* o) {
   for (int j = 0; j < 3; j++) o[j] = ((p[0] * M.m[j] + p[1] * M.m[4 + j]) + p[2] * M.m[8 + j]) + M.m[12 + j];
@@ -212,9 +208,9 @@ DevQueues makeQueues(rg_handle* h, int maxIter) {
   return Q;
 }
 
-DevRender makeRender(const rg_handle* h) {
-  const rg_settings& s = h->st;
-  const rg_camera& c = h->camera;
+}  // namespace
+
+DevRender makeRenderParams(const rg_settings& s, const rg_camera& c) {
   DevRender R;
   R.width = s.resolution_width;
   R.height = s.resolution_height;
@@ -241,6 +237,10 @@ DevRender makeRender(const rg_handle* h) {
   R.aoSamples = std::max(1, s.samples);
   return R;
 }
+
+namespace {
+
+DevRender makeRender(const rg_handle* h) { return makeRenderParams(h->st, h->camera); }
 
 struct Grids {
   int gen, ext, shade, conn, acc, simple;
@@ -395,9 +395,14 @@ rg_status rg_cancel(rg_handle* h) {
   return RG_OK;
 }
 
-rg_status rg_set_scene(rg_handle* h, const rg_scene_desc* d) {
-  if (!h || !d) return RG_ERR_INVALID_ARGUMENT;
-  std::lock_guard<std::mutex> lk(h->mu);
+}  // extern "C"
+
+namespace rg {
+
+// Validates a scene description, uploads it, builds its BVH and fills the
+// device-side table of pointers.  Used by rg_set_scene and the job server.
+rg_status prepareScene(const rg_scene_desc* d, int bins, bool wide, cudaStream_t st, int* errWord,
+                       std::unique_ptr<DeviceScene>& out, DevScene& S, Mat4& view, float* buildMs) {
   const int nt = d->num_triangles;
   if (nt < 0 || d->num_meshes < 0 || d->num_objects < 0 || d->num_materials < 0 || d->num_media < 0 ||
       d->num_point_lights < 0 || d->num_textures < 0) {
@@ -437,14 +442,10 @@ rg_status rg_set_scene(rg_handle* h, const rg_scene_desc* d) {
     setLastError("global medium index out of range");
     return RG_ERR_INVALID_ARGUMENT;
   }
-  cudaStream_t st = h->stream;
-  h->hasScene = false;
-  h->haveResult = false;
-  h->scene.reset(new DeviceScene());
-  DeviceScene& ds = *h->scene;
+  out.reset(new DeviceScene());
+  DeviceScene& ds = *out;
   ds.numTris = nt;
-  h->camera = d->camera;
-  h->view = viewMatrix(d->camera);
+  view = viewMatrix(d->camera);
   ds.hasUV = d->uvs != nullptr && d->num_textures > 0;
   // tables
   std::vector<int> meshTriCount(d->num_meshes, 0);
@@ -480,8 +481,8 @@ rg_status rg_set_scene(rg_handle* h, const rg_scene_desc* d) {
       for (int i : meshTris[m]) {
         float v[3][3], n[3][3];
         for (int k = 0; k < 3; k++) {
-          xformPoint(h->view, &d->positions[(size_t)i * 9 + k * 3], v[k]);
-          xformDir(h->view, &d->normals[(size_t)i * 9 + k * 3], n[k]);
+          xformPoint(view, &d->positions[(size_t)i * 9 + k * 3], v[k]);
+          xformDir(view, &d->normals[(size_t)i * 9 + k * 3], n[k]);
         }
         const F3h v1{v[0][0], v[0][1], v[0][2]}, v2{v[1][0], v[1][1], v[1][2]}, v3_{v[2][0], v[2][1], v[2][2]};
         const float tia = 1.0f / len(crs(sub(v1, v2), sub(v1, v3_)));
@@ -496,8 +497,8 @@ rg_status rg_set_scene(rg_handle* h, const rg_scene_desc* d) {
   std::vector<DevPointLight> pts(d->num_point_lights);
   for (int i = 0; i < d->num_point_lights; i++) {
     float p[3], n[3];
-    xformPoint(h->view, d->point_lights[i].position, p);
-    xformDir(h->view, d->point_lights[i].normal, n);
+    xformPoint(view, d->point_lights[i].position, p);
+    xformDir(view, d->point_lights[i].normal, n);
     pts[i] = DevPointLight{p[0], p[1], p[2], n[0], n[1], n[2], d->point_lights[i].material, 0};
   }
   bool ok = ds.meshTriCount.upload(meshTriCount.data(), meshTriCount.size(), st) &&
@@ -509,7 +510,7 @@ rg_status rg_set_scene(rg_handle* h, const rg_scene_desc* d) {
             ds.lightObjMeshes.upload(lightObjMeshes.data(), lightObjMeshes.size(), st) &&
             ds.lightMeshTris.upload(lightMeshTris.data(), lightMeshTris.size(), st) &&
             ds.lightTris.upload(lightTris.data(), lightTris.size(), st) && ds.points.upload(pts.data(), pts.size(), st) &&
-            ds.view.upload(h->view.m, 16, st) && ds.inPos.upload(d->positions, (size_t)nt * 9, st) &&
+            ds.view.upload(view.m, 16, st) && ds.inPos.upload(d->positions, (size_t)nt * 9, st) &&
             ds.inNrm.upload(d->normals, (size_t)nt * 9, st) && ds.inTriMesh.upload(d->tri_mesh, nt, st);
   if (ok && ds.hasUV) ok = ds.inUV.upload(d->uvs, (size_t)nt * 6, st);
   // textures
@@ -525,7 +526,7 @@ rg_status rg_set_scene(rg_handle* h, const rg_scene_desc* d) {
   if (ok) ok = ds.textures.upload(texs.data(), texs.size(), st);
   if (!ok) {
     setLastError("scene upload failed (device memory)");
-    h->scene.reset();
+    out.reset();
     return RG_ERR_OUT_OF_MEMORY;
   }
   ds.numAreaLights = (int)areaLightObj.size();
@@ -536,7 +537,7 @@ rg_status rg_set_scene(rg_handle* h, const rg_scene_desc* d) {
   cudaEventCreate(&e1);
   cudaEventRecord(e0, st);
   std::string err;
-  const rg_status rs = buildDeviceBvh(ds, h->st.bvh_bins > 1 ? h->st.bvh_bins : 32, h->st.bvh_width != 2, st, err);
+  const rg_status rs = buildDeviceBvh(ds, bins > 1 ? bins : 32, wide, st, err);
   cudaEventRecord(e1, st);
   cudaStreamSynchronize(st);
   float ms = 0.0f;
@@ -545,16 +546,15 @@ rg_status rg_set_scene(rg_handle* h, const rg_scene_desc* d) {
   cudaEventDestroy(e1);
   if (rs != RG_OK) {
     setLastError(err);
-    h->scene.reset();
+    out.reset();
     return rs;
   }
-  h->lastStats.build_ms = ms;
-  h->lastStats.bvh_nodes = ds.bvhWidth == 8 ? ds.numNodes8 : ds.numNodes;
+  if (buildMs) *buildMs = ms;
   ds.inPos.release();
   ds.inNrm.release();
   ds.inUV.release();
   ds.inTriMesh.release();
-  DevScene& S = h->dscene;
+  std::memset(&S, 0, sizeof(S));
   S.nodes = ds.nodes.p;
   S.numNodes = ds.numNodes;
   S.rootIsLeaf = ds.rootIsLeaf;
@@ -581,12 +581,31 @@ rg_status rg_set_scene(rg_handle* h, const rg_scene_desc* d) {
   S.points = ds.points.p;
   S.textures = ds.textures.p;
   S.numTextures = ds.numTextures;
-  if (!h->error.alloc(1)) return RG_ERR_OUT_OF_MEMORY;
-  cudaMemsetAsync(h->error.p, 0, sizeof(int), st);
-  S.error = h->error.p;
+  S.error = errWord;
   S.nodes8 = ds.nodes8.p;
   S.numNodes8 = ds.numNodes8;
   S.bvhWidth = ds.bvhWidth;
+  return RG_OK;
+}
+
+}  // namespace rg
+
+extern "C" {
+
+rg_status rg_set_scene(rg_handle* h, const rg_scene_desc* d) {
+  if (!h || !d) return RG_ERR_INVALID_ARGUMENT;
+  std::lock_guard<std::mutex> lk(h->mu);
+  h->hasScene = false;
+  h->haveResult = false;
+  if (!h->error.alloc(1)) return RG_ERR_OUT_OF_MEMORY;
+  cudaMemsetAsync(h->error.p, 0, sizeof(int), h->stream);
+  float ms = 0.0f;
+  const rg_status rs = prepareScene(d, h->st.bvh_bins, h->st.bvh_width != 2, h->stream, h->error.p, h->scene,
+                                    h->dscene, h->view, &ms);
+  if (rs != RG_OK) return rs;
+  h->camera = d->camera;
+  h->lastStats.build_ms = ms;
+  h->lastStats.bvh_nodes = h->scene->bvhWidth == 8 ? h->scene->numNodes8 : h->scene->numNodes;
   h->hasScene = true;
   if (h->graph) {
     cudaGraphExecDestroy(h->graph);

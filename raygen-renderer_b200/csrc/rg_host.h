@@ -3,6 +3,7 @@
 #include <cuda_runtime.h>
 
 #include <atomic>
+#include <memory>
 #include <cstdint>
 #include <mutex>
 #include <string>
@@ -14,6 +15,15 @@ namespace rg {
 
 struct DevMaterial;
 struct DevMedium;
+struct DevScene;
+struct DevRender;
+
+// 4x4 row-major matrix, row-vector convention p' = [p 1] * M.
+struct Mat4 {
+  float m[16];
+};
+Mat4 viewMatrix(const rg_camera& c);
+DevRender makeRenderParams(const rg_settings& s, const rg_camera& c);
 struct DevPointLight;
 struct DevTexture;
 
@@ -112,6 +122,8 @@ struct DeviceScene {
 };
 
 rg_status buildDeviceBvh(DeviceScene& ds, int nbins, bool wide, cudaStream_t st, std::string& err);
+rg_status prepareScene(const rg_scene_desc* d, int bins, bool wide, cudaStream_t st, int* errWord,
+                       std::unique_ptr<DeviceScene>& out, DevScene& S, Mat4& view, float* buildMs);
 
 void setLastError(const std::string& msg);
 

@@ -1,0 +1,609 @@
+// rg_serve.cu - resident multi-job render server (batched and served rendering).
+//
+// The reference renders one scene per process run (src/main.cpp:162-489) and
+// its viewer runs one render job at a time on a worker thread
+// (src/viewer/main.cpp:775-850).  Here one worker thread owns a CUDA stream
+// and keeps many jobs resident at once:
+//  * admission: queued jobs are admitted while a job slot is free and the
+//    estimated device footprint fits the HBM budget; admission uploads the
+//    scene, builds its BVH and allocates the accumulation buffers;
+//  * continuous batching: every wave takes a share of paths from every
+//    resident job (one segment per job in the wave table), so jobs that
+//    arrive while others are in flight join the next wave;
+//  * completion: a job whose samples are all traced is resolved (optionally
+//    A-Trous denoised) and tonemapped on the device, read back, and its
+//    memory and slot are released.
+// The per-path RNG is keyed by (job seed, pixel, sample), never by slot or
+// wave, so a job's image does not depend on the mix it was rendered in.
+#include <cuda_fp16.h>
+
+#include <algorithm>
+#include <chrono>
+#include <condition_variable>
+#include <cstring>
+#include <deque>
+#include <map>
+#include <memory>
+#include <mutex>
+#include <thread>
+#include <vector>
+
+#include "rg_device.cuh"
+#include "rg_host.h"
+#include "rg_trace.cuh"
+
+namespace rg {
+
+namespace {
+
+double nowMs() {
+  using namespace std::chrono;
+  return duration<double, std::milli>(steady_clock::now().time_since_epoch()).count();
+}
+
+struct ServerJob {
+  int64_t id = 0;
+  rg_job_desc desc{};
+  int state = RG_JOB_QUEUED;
+  rg_status error = RG_OK;
+  double tSubmit = 0, tStart = 0, tDone = 0;
+  int slot = -1;
+  size_t bytes = 0;
+  std::unique_ptr<DeviceScene> ds;
+  DevScene S{};
+  DevRender R{};
+  Mat4 view{};
+  DevBuf<int> errWord;
+  DevBuf<float4> sum, sumSq, hdr, ldr, bufA, bufB;
+  DevBuf<int> cnt;
+  DevBuf<__half> aovN, aovA, aovAA, aovD;
+  int pixels = 0;
+  int issuedSamples = 0;
+  int pixelCursor = 0;
+  std::vector<float> result;
+  std::vector<float> snapshot;
+  bool snapshotRequested = false;
+  bool snapshotReady = false;
+};
+
+size_t estimateBytes(const rg_job_desc& d) {
+  const size_t tris = d.scene ? (size_t)std::max(0, d.scene->num_triangles) : 0;
+  const size_t px = (size_t)std::max(0, d.width) * (size_t)std::max(0, d.height);
+  return tris * 520 + px * 176 + ((size_t)64 << 20);
+}
+
+}  // namespace
+}  // namespace rg
+
+using namespace rg;
+
+struct rg_server {
+  rg_settings base{};
+  rg_server_config cfg{};
+  std::mutex mu;
+  std::condition_variable cv;
+  std::deque<ServerJob*> pending;
+  std::map<int64_t, std::unique_ptr<ServerJob>> jobs;
+  std::vector<ServerJob*> slotJob;
+  std::vector<int> freeSlots;
+  int64_t nextId = 1;
+  size_t bytesUsed = 0, bytesPeak = 0;
+  int residentPeak = 0;
+  bool stop = false;
+  std::thread worker;
+  cudaStream_t stream = nullptr;
+  int numSMs = 148;
+  // device tables and wavefront buffers
+  DevBuf<DevJob> jobTable;
+  DevBuf<DevSegment> segs;
+  DevBuf<DevWave> waveSlot;
+  DevBuf<float4> rayO0, rayO1, rayD0, rayD1, hits, pathT, pathR, pathL, shO0, shO1, shD0, shD1, shC0, shC1;
+  DevBuf<int2> pathPS;
+  DevBuf<int> counters;
+  DevBuf<unsigned long long> stats;
+  DevBuf<int> errWord;
+  DevSegment* hostSegs = nullptr;
+  DevWave* hostWave = nullptr;
+  cudaGraphExec_t graph = nullptr;
+  int maxIter = 12;
+  // statistics
+  std::vector<double> latencies;
+  double firstSubmit = -1, lastDone = 0;
+  uint64_t samplesDone = 0;
+  int64_t waves = 0;
+  double deviceMs = 0;
+  ~rg_server() {
+    if (graph) cudaGraphExecDestroy(graph);
+    if (hostSegs) cudaFreeHost(hostSegs);
+    if (hostWave) cudaFreeHost(hostWave);
+    if (stream) cudaStreamDestroy(stream);
+  }
+};
+
+namespace rg {
+namespace {
+
+DevQueues serverQueues(rg_server* s) {
+  DevQueues Q;
+  Q.rayO[0] = s->rayO0.p; Q.rayO[1] = s->rayO1.p;
+  Q.rayD[0] = s->rayD0.p; Q.rayD[1] = s->rayD1.p;
+  Q.hits = s->hits.p;
+  Q.pathT = s->pathT.p; Q.pathR = s->pathR.p; Q.pathL = s->pathL.p;
+  Q.pathPS = s->pathPS.p;
+  Q.shO[0] = s->shO0.p; Q.shO[1] = s->shO1.p;
+  Q.shD[0] = s->shD0.p; Q.shD[1] = s->shD1.p;
+  Q.shC[0] = s->shC0.p; Q.shC[1] = s->shC1.p;
+  Q.counters = s->counters.p;
+  Q.stats = s->stats.p;
+  Q.error = s->errWord.p;
+  Q.capacity = s->cfg.paths_per_wave;
+  Q.maxIter = s->maxIter;
+  return Q;
+}
+
+bool allocServer(rg_server* s) {
+  const size_t c = (size_t)s->cfg.paths_per_wave;
+  const int slots = s->cfg.max_resident_jobs;
+  bool ok = s->rayO0.alloc(c) && s->rayO1.alloc(c) && s->rayD0.alloc(c) && s->rayD1.alloc(c) && s->hits.alloc(c) &&
+            s->pathT.alloc(c) && s->pathR.alloc(c) && s->pathL.alloc(c) && s->shO0.alloc(c) && s->shO1.alloc(c) &&
+            s->shD0.alloc(c) && s->shD1.alloc(c) && s->shC0.alloc(c) && s->shC1.alloc(c) && s->pathPS.alloc(c) &&
+            s->counters.alloc((size_t)(s->maxIter + 1) * kCountersPerIter) && s->stats.alloc(8) &&
+            s->errWord.alloc(1) && s->jobTable.alloc(slots) && s->segs.alloc((size_t)slots * 2) && s->waveSlot.alloc(1);
+  if (!ok) return false;
+  if (cudaMallocHost((void**)&s->hostSegs, sizeof(DevSegment) * (size_t)slots * 2) != cudaSuccess) return false;
+  if (cudaMallocHost((void**)&s->hostWave, sizeof(DevWave)) != cudaSuccess) return false;
+  cudaMemsetAsync(s->stats.p, 0, sizeof(unsigned long long) * 8, s->stream);
+  cudaMemsetAsync(s->errWord.p, 0, sizeof(int), s->stream);
+  return cudaStreamSynchronize(s->stream) == cudaSuccess;
+}
+
+// Capture the multi-job wave (generate, bounce loop, accumulate) once.
+bool captureGraph(rg_server* s) {
+  const DevQueues Q = serverQueues(s);
+  const int ext = s->numSMs * residentBlocks(0, 8), conn = s->numSMs * residentBlocks(1, 8);
+  cudaGraph_t g;
+  if (cudaStreamBeginCapture(s->stream, cudaStreamCaptureModeThreadLocal) != cudaSuccess) return false;
+  launchGenerate(s->jobTable.p, s->waveSlot.p, Q, s->numSMs * 8, s->stream);
+  for (int it = 0; it < Q.maxIter; it++) {
+    launchExtend(nullptr, s->jobTable.p, 8, Q, it, ext, s->stream);
+    launchShade(nullptr, nullptr, s->jobTable.p, Q, it, s->numSMs * 4, s->stream);
+    launchConnect(nullptr, s->jobTable.p, 8, Q, it, 0, conn, s->stream);
+    launchConnect(nullptr, s->jobTable.p, 8, Q, it, 1, conn, s->stream);
+  }
+  launchAccumulate(s->jobTable.p, s->waveSlot.p, Q, s->numSMs * 4, s->stream);
+  if (cudaStreamEndCapture(s->stream, &g) != cudaSuccess) return false;
+  const bool ok = cudaGraphInstantiate(&s->graph, g, 0) == cudaSuccess;
+  cudaGraphDestroy(g);
+  return ok;
+}
+
+void releaseJob(rg_server* s, ServerJob* j) {
+  j->ds.reset();
+  j->sum.release(); j->sumSq.release(); j->hdr.release(); j->ldr.release(); j->bufA.release(); j->bufB.release();
+  j->cnt.release(); j->aovN.release(); j->aovA.release(); j->aovAA.release(); j->aovD.release(); j->errWord.release();
+  if (j->slot >= 0) {
+    s->slotJob[j->slot] = nullptr;
+    s->freeSlots.push_back(j->slot);
+    j->slot = -1;
+  }
+  s->bytesUsed -= std::min(s->bytesUsed, j->bytes);
+}
+
+// Upload scene, build BVH, allocate buffers, publish the job-table slot.
+rg_status admit(rg_server* s, ServerJob* j) {
+  const rg_job_desc& d = j->desc;
+  cudaStream_t st = s->stream;
+  if (!j->errWord.alloc(1)) return RG_ERR_OUT_OF_MEMORY;
+  cudaMemsetAsync(j->errWord.p, 0, sizeof(int), st);
+  rg_status rs = prepareScene(d.scene, s->base.bvh_bins, true, st, j->errWord.p, j->ds, j->S, j->view, nullptr);
+  if (rs != RG_OK) return rs;
+  rg_settings js = s->base;
+  js.resolution_width = d.width;
+  js.resolution_height = d.height;
+  js.samples = d.samples;
+  js.max_depth = std::min(d.max_depth > 0 ? d.max_depth : s->base.max_depth, s->maxIter - 2);
+  js.rr_depth = d.rr_depth > 0 ? d.rr_depth : s->base.rr_depth;
+  js.seed = d.seed;
+  js.shader_provider = 5;
+  j->R = makeRenderParams(js, d.scene->camera);
+  j->pixels = d.width * d.height;
+  const int N = j->pixels;
+  if (!j->sum.alloc(N) || !j->sumSq.alloc(N) || !j->cnt.alloc(N) || !j->hdr.alloc(N) || !j->ldr.alloc(N))
+    return RG_ERR_OUT_OF_MEMORY;
+  cudaMemsetAsync(j->sum.p, 0, sizeof(float4) * N, st);
+  cudaMemsetAsync(j->sumSq.p, 0, sizeof(float4) * N, st);
+  cudaMemsetAsync(j->cnt.p, 0, sizeof(int) * N, st);
+  if (d.denoise) {
+    if (!j->aovN.alloc((size_t)N * 3) || !j->aovA.alloc((size_t)N * 3) || !j->aovAA.alloc(N) || !j->aovD.alloc(N) ||
+        !j->bufA.alloc(N) || !j->bufB.alloc(N))
+      return RG_ERR_OUT_OF_MEMORY;
+    launchAov(j->S, j->R, j->aovN.p, j->aovA.p, j->aovAA.p, j->aovD.p, st);
+  }
+  DevJob J;
+  std::memset(&J, 0, sizeof(J));
+  J.S = j->S;
+  J.R = j->R;
+  J.sum = j->sum.p;
+  J.sumSq = j->sumSq.p;
+  J.cnt = j->cnt.p;
+  if (cudaMemcpyAsync(s->jobTable.p + j->slot, &J, sizeof(J), cudaMemcpyHostToDevice, st) != cudaSuccess)
+    return RG_ERR_CUDA;
+  if (cudaStreamSynchronize(st) != cudaSuccess) return RG_ERR_CUDA;
+  return RG_OK;
+}
+
+void finishJob(rg_server* s, ServerJob* j) {
+  cudaStream_t st = s->stream;
+  const int N = j->pixels;
+  launchResolve(N, j->sum.p, j->cnt.p, j->R.exposure, j->hdr.p, st);
+  if (j->desc.denoise) {
+    launchDenoise(j->desc.width, j->desc.height, j->hdr.p, j->aovN.p, j->aovD.p, j->aovA.p, j->aovAA.p,
+                  s->base.denoise_levels, s->base.denoise_sigma_color, s->base.denoise_sigma_normal,
+                  s->base.denoise_sigma_depth, s->base.denoise_intensity, j->bufA.p, j->bufB.p, j->ldr.p, st);
+    cudaMemcpyAsync(j->hdr.p, j->ldr.p, sizeof(float4) * N, cudaMemcpyDeviceToDevice, st);
+  }
+  j->result.resize((size_t)N * 4);
+  cudaMemcpyAsync(j->result.data(), j->hdr.p, sizeof(float4) * N, cudaMemcpyDeviceToHost, st);
+  int derr = 0;
+  cudaMemcpyAsync(&derr, j->errWord.p, sizeof(int), cudaMemcpyDeviceToHost, st);
+  const cudaError_t ce = cudaStreamSynchronize(st);
+  j->error = ce != cudaSuccess ? RG_ERR_CUDA : (derr ? RG_ERR_DEVICE_STATUS : RG_OK);
+}
+
+void serverLoop(rg_server* s) {
+  cudaStream_t st = s->stream;
+  int rr = 0;
+  for (;;) {
+    // ---- admission
+    std::vector<ServerJob*> toAdmit;
+    {
+      std::unique_lock<std::mutex> lk(s->mu);
+      if (s->stop) return;
+      bool anyResident = false;
+      for (auto* j : s->slotJob)
+        if (j) anyResident = true;
+      if (!anyResident && s->pending.empty()) {
+        s->cv.wait_for(lk, std::chrono::milliseconds(50));
+        continue;
+      }
+      while (!s->pending.empty() && !s->freeSlots.empty()) {
+        ServerJob* j = s->pending.front();
+        const size_t need = estimateBytes(j->desc);
+        if (anyResident && s->bytesUsed + need > s->cfg.hbm_budget_bytes) break;
+        s->pending.pop_front();
+        j->slot = s->freeSlots.back();
+        s->freeSlots.pop_back();
+        s->slotJob[j->slot] = j;
+        j->bytes = need;
+        s->bytesUsed += need;
+        s->bytesPeak = std::max(s->bytesPeak, s->bytesUsed);
+        toAdmit.push_back(j);
+        anyResident = true;
+      }
+    }
+    for (auto* j : toAdmit) {
+      const rg_status rs = admit(s, j);
+      std::lock_guard<std::mutex> lk(s->mu);
+      if (rs != RG_OK) {
+        j->error = rs;
+        j->state = RG_JOB_FAILED;
+        j->tDone = nowMs();
+        releaseJob(s, j);
+        s->cv.notify_all();
+      } else {
+        j->state = RG_JOB_RESIDENT;
+        j->tStart = nowMs();
+      }
+      s->cv.notify_all();
+    }
+    // ---- one wave over the resident jobs
+    std::vector<ServerJob*> active;
+    {
+      std::lock_guard<std::mutex> lk(s->mu);
+      const int n = (int)s->slotJob.size();
+      for (int k = 0; k < n; k++) {
+        ServerJob* j = s->slotJob[(rr + k) % n];
+        if (j && j->state == RG_JOB_RESIDENT && j->issuedSamples < j->desc.samples) active.push_back(j);
+      }
+      int residents = 0;
+      for (auto* j : s->slotJob)
+        if (j) residents++;
+      s->residentPeak = std::max(s->residentPeak, residents);
+      rr++;
+    }
+    if (!active.empty()) {
+      const long long cap = s->cfg.paths_per_wave;
+      const long long quota = std::max<long long>(1, cap / (long long)active.size());
+      long long paths = 0, pixTotal = 0;
+      int nseg = 0;
+      std::vector<std::pair<ServerJob*, DevSegment>> plan;
+      for (auto* j : active) {
+        if (paths >= cap) break;
+        DevSegment e;
+        e.slot = j->slot;
+        e.pixelList = nullptr;
+        const long long room = std::min(quota, cap - paths);
+        if (j->pixelCursor == 0 && j->pixels <= room) {
+          e.numPixels = j->pixels;
+          e.pixelOffset = 0;
+          e.samples = (int)std::min<long long>(j->desc.samples - j->issuedSamples, std::max<long long>(1, room / j->pixels));
+        } else {
+          e.numPixels = (int)std::min<long long>(j->pixels - j->pixelCursor, room);
+          e.pixelOffset = j->pixelCursor;
+          e.samples = 1;
+        }
+        e.pathBase = (int)paths;
+        e.pixBase = (int)pixTotal;
+        paths += (long long)e.numPixels * e.samples;
+        pixTotal += e.numPixels;
+        s->hostSegs[nseg++] = e;
+        plan.push_back({j, e});
+      }
+      DevWave* w = s->hostWave;
+      w->numSegments = nseg;
+      w->numPaths = (int)paths;
+      w->numPixelsTotal = (int)pixTotal;
+      w->pad = 0;
+      w->segs = s->segs.p;
+      cudaEvent_t e0, e1;
+      cudaEventCreate(&e0);
+      cudaEventCreate(&e1);
+      cudaMemcpyAsync(s->segs.p, s->hostSegs, sizeof(DevSegment) * nseg, cudaMemcpyHostToDevice, st);
+      cudaMemcpyAsync(s->waveSlot.p, w, sizeof(DevWave), cudaMemcpyHostToDevice, st);
+      cudaEventRecord(e0, st);
+      cudaGraphLaunch(s->graph, st);
+      cudaEventRecord(e1, st);
+      const cudaError_t ce = cudaStreamSynchronize(st);
+      float ms = 0;
+      cudaEventElapsedTime(&ms, e0, e1);
+      cudaEventDestroy(e0);
+      cudaEventDestroy(e1);
+      std::vector<ServerJob*> finished;
+      {
+        std::lock_guard<std::mutex> lk(s->mu);
+        s->waves++;
+        s->deviceMs += ms;
+        s->samplesDone += (uint64_t)paths;
+        for (auto& pe : plan) {
+          ServerJob* j = pe.first;
+          const DevSegment& e = pe.second;
+          if (ce != cudaSuccess) {
+            j->error = RG_ERR_CUDA;
+            finished.push_back(j);
+            continue;
+          }
+          if (e.pixelOffset == 0 && e.numPixels == j->pixels) {
+            j->issuedSamples += e.samples;
+          } else {
+            j->pixelCursor += e.numPixels;
+            if (j->pixelCursor >= j->pixels) {
+              j->pixelCursor = 0;
+              j->issuedSamples += 1;
+            }
+          }
+          if (j->issuedSamples >= j->desc.samples) finished.push_back(j);
+        }
+      }
+      for (auto* j : finished) {
+        if (j->error == RG_OK) finishJob(s, j);
+        std::lock_guard<std::mutex> lk(s->mu);
+        j->state = j->error == RG_OK ? RG_JOB_DONE : RG_JOB_FAILED;
+        j->tDone = nowMs();
+        s->latencies.push_back(j->tDone - j->tSubmit);
+        s->lastDone = j->tDone;
+        releaseJob(s, j);
+        s->cv.notify_all();
+      }
+    }
+    // ---- progressive snapshots (between waves)
+    std::vector<ServerJob*> snaps;
+    {
+      std::lock_guard<std::mutex> lk(s->mu);
+      for (auto* j : s->slotJob)
+        if (j && j->snapshotRequested && j->state == RG_JOB_RESIDENT) snaps.push_back(j);
+    }
+    for (auto* j : snaps) {
+      launchResolve(j->pixels, j->sum.p, j->cnt.p, j->R.exposure, j->hdr.p, st);
+      std::vector<float> tmp((size_t)j->pixels * 4);
+      cudaMemcpyAsync(tmp.data(), j->hdr.p, sizeof(float4) * j->pixels, cudaMemcpyDeviceToHost, st);
+      cudaStreamSynchronize(st);
+      std::lock_guard<std::mutex> lk(s->mu);
+      j->snapshot.swap(tmp);
+      j->snapshotRequested = false;
+      j->snapshotReady = true;
+      s->cv.notify_all();
+    }
+  }
+}
+
+}  // namespace
+}  // namespace rg
+
+extern "C" {
+
+void rg_server_config_default(rg_server_config* c) {
+  if (!c) return;
+  std::memset(c, 0, sizeof(*c));
+  c->hbm_budget_bytes = (uint64_t)120 << 30;
+  c->max_resident_jobs = 256;
+  c->paths_per_wave = 8 << 20;
+  c->max_depth_cap = 10;
+}
+
+rg_status rg_server_create(const rg_settings* base, const rg_server_config* cfg, rg_server** out) {
+  if (!out) return RG_ERR_INVALID_ARGUMENT;
+  *out = nullptr;
+  int n = 0;
+  if (cudaGetDeviceCount(&n) != cudaSuccess || n == 0) {
+    cudaGetLastError();
+    setLastError("no CUDA device");
+    return RG_ERR_NO_DEVICE;
+  }
+  rg_server* s = new (std::nothrow) rg_server();
+  if (!s) return RG_ERR_OUT_OF_MEMORY;
+  if (base) s->base = *base;
+  else rg_settings_default(&s->base);
+  if (cfg) s->cfg = *cfg;
+  else rg_server_config_default(&s->cfg);
+  if (s->cfg.max_resident_jobs <= 0 || s->cfg.max_resident_jobs > 4096 || s->cfg.paths_per_wave <= 0) {
+    delete s;
+    return RG_ERR_INVALID_ARGUMENT;
+  }
+  s->maxIter = std::max(3, std::min(s->cfg.max_depth_cap > 0 ? s->cfg.max_depth_cap : 10, 250)) + 2;
+  int dev = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&s->numSMs, cudaDevAttrMultiProcessorCount, dev);
+  if (cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking) != cudaSuccess || !allocServer(s) ||
+      !captureGraph(s)) {
+    setLastError("server initialisation failed (device memory or graph capture)");
+    delete s;
+    return RG_ERR_OUT_OF_MEMORY;
+  }
+  s->slotJob.assign(s->cfg.max_resident_jobs, nullptr);
+  for (int i = s->cfg.max_resident_jobs - 1; i >= 0; i--) s->freeSlots.push_back(i);
+  s->worker = std::thread(serverLoop, s);
+  *out = s;
+  return RG_OK;
+}
+
+rg_status rg_server_submit(rg_server* s, const rg_job_desc* d, int64_t* job) {
+  if (!s || !d || !d->scene || d->width <= 0 || d->height <= 0 || d->samples <= 0 ||
+      (long long)d->width * d->height > (1ll << 26))
+    return RG_ERR_INVALID_ARGUMENT;
+  auto j = std::make_unique<ServerJob>();
+  j->desc = *d;
+  j->tSubmit = nowMs();
+  std::lock_guard<std::mutex> lk(s->mu);
+  if (s->stop) return RG_ERR_BUSY;
+  j->id = s->nextId++;
+  if (s->firstSubmit < 0) s->firstSubmit = j->tSubmit;
+  if (job) *job = j->id;
+  s->pending.push_back(j.get());
+  s->jobs[j->id] = std::move(j);
+  s->cv.notify_all();
+  return RG_OK;
+}
+
+rg_status rg_server_poll(rg_server* s, int64_t job, rg_job_status* out) {
+  if (!s || !out) return RG_ERR_INVALID_ARGUMENT;
+  std::lock_guard<std::mutex> lk(s->mu);
+  auto it = s->jobs.find(job);
+  if (it == s->jobs.end()) return RG_ERR_INVALID_ARGUMENT;
+  const ServerJob* j = it->second.get();
+  out->state = j->state;
+  out->error = j->error;
+  out->submit_ms = j->tSubmit;
+  out->start_ms = j->tStart;
+  out->done_ms = j->tDone;
+  out->latency_ms = j->state >= RG_JOB_DONE ? j->tDone - j->tSubmit : -1.0;
+  out->samples_issued = (int64_t)j->issuedSamples * j->pixels + j->pixelCursor;
+  out->samples_total = (int64_t)j->desc.samples * j->desc.width * j->desc.height;
+  return RG_OK;
+}
+
+rg_status rg_server_wait(rg_server* s, int64_t job, double timeout_ms) {
+  if (!s) return RG_ERR_INVALID_ARGUMENT;
+  std::unique_lock<std::mutex> lk(s->mu);
+  auto it = s->jobs.find(job);
+  if (it == s->jobs.end()) return RG_ERR_INVALID_ARGUMENT;
+  ServerJob* j = it->second.get();
+  const auto deadline = std::chrono::steady_clock::now() + std::chrono::duration<double, std::milli>(timeout_ms);
+  while (j->state < RG_JOB_DONE) {
+    if (s->cv.wait_until(lk, deadline) == std::cv_status::timeout && j->state < RG_JOB_DONE) return RG_ERR_BUSY;
+  }
+  return j->state == RG_JOB_DONE ? RG_OK : j->error;
+}
+
+rg_status rg_server_get_result(rg_server* s, int64_t job, float* hdr_rgba, size_t count, int32_t release) {
+  if (!s) return RG_ERR_INVALID_ARGUMENT;
+  std::lock_guard<std::mutex> lk(s->mu);
+  auto it = s->jobs.find(job);
+  if (it == s->jobs.end()) return RG_ERR_INVALID_ARGUMENT;
+  ServerJob* j = it->second.get();
+  if (j->state == RG_JOB_FAILED) return j->error;
+  if (j->state != RG_JOB_DONE) return RG_ERR_BUSY;
+  if (hdr_rgba) {
+    if (count < j->result.size()) return RG_ERR_INVALID_ARGUMENT;
+    std::memcpy(hdr_rgba, j->result.data(), j->result.size() * sizeof(float));
+  }
+  if (release) s->jobs.erase(it);
+  return RG_OK;
+}
+
+rg_status rg_server_snapshot(rg_server* s, int64_t job, float* hdr_rgba, size_t count, double timeout_ms) {
+  if (!s || !hdr_rgba) return RG_ERR_INVALID_ARGUMENT;
+  std::unique_lock<std::mutex> lk(s->mu);
+  auto it = s->jobs.find(job);
+  if (it == s->jobs.end()) return RG_ERR_INVALID_ARGUMENT;
+  ServerJob* j = it->second.get();
+  const auto deadline = std::chrono::steady_clock::now() + std::chrono::duration<double, std::milli>(timeout_ms);
+  while (j->state == RG_JOB_QUEUED) {  // wait for admission
+    if (s->cv.wait_until(lk, deadline) == std::cv_status::timeout && j->state == RG_JOB_QUEUED) return RG_ERR_BUSY;
+  }
+  if (j->state == RG_JOB_DONE) {
+    if (count < j->result.size()) return RG_ERR_INVALID_ARGUMENT;
+    std::memcpy(hdr_rgba, j->result.data(), j->result.size() * sizeof(float));
+    return RG_OK;
+  }
+  if (j->state != RG_JOB_RESIDENT) return j->error;
+  j->snapshotReady = false;
+  j->snapshotRequested = true;
+  while (!j->snapshotReady && j->state == RG_JOB_RESIDENT) {
+    if (s->cv.wait_until(lk, deadline) == std::cv_status::timeout) return RG_ERR_BUSY;
+  }
+  const std::vector<float>& src = j->snapshotReady ? j->snapshot : j->result;
+  if (count < src.size() || src.empty()) return RG_ERR_BUSY;
+  std::memcpy(hdr_rgba, src.data(), src.size() * sizeof(float));
+  return RG_OK;
+}
+
+rg_status rg_server_get_stats(rg_server* s, rg_server_stats* out) {
+  if (!s || !out) return RG_ERR_INVALID_ARGUMENT;
+  std::lock_guard<std::mutex> lk(s->mu);
+  std::memset(out, 0, sizeof(*out));
+  std::vector<double> l = s->latencies;
+  std::sort(l.begin(), l.end());
+  auto pct = [&](double p) {
+    if (l.empty()) return 0.0;
+    const size_t k = (size_t)std::min<double>((double)l.size() - 1, std::ceil(p * (double)l.size()) - 1);
+    return l[k];
+  };
+  out->jobs_done = (int64_t)l.size();
+  out->p50_ms = pct(0.50);
+  out->p99_ms = pct(0.99);
+  double mean = 0;
+  for (double v : l) mean += v;
+  out->mean_ms = l.empty() ? 0 : mean / (double)l.size();
+  out->max_ms = l.empty() ? 0 : l.back();
+  const double span = s->lastDone - s->firstSubmit;
+  out->images_per_s = span > 0 ? (double)l.size() / (span * 1e-3) : 0;
+  out->samples_done = s->samplesDone;
+  out->device_ms = s->deviceMs;
+  out->waves = s->waves;
+  out->resident_peak = s->residentPeak;
+  out->bytes_peak = s->bytesPeak;
+  out->pending = (int32_t)s->pending.size();
+  return RG_OK;
+}
+
+rg_status rg_server_destroy(rg_server* s) {
+  if (!s) return RG_ERR_INVALID_ARGUMENT;
+  {
+    std::lock_guard<std::mutex> lk(s->mu);
+    s->stop = true;
+    // drop jobs that never started
+    for (auto* j : s->pending) {
+      j->state = RG_JOB_FAILED;
+      j->error = RG_ERR_CANCELLED;
+    }
+    s->pending.clear();
+    s->cv.notify_all();
+  }
+  if (s->worker.joinable()) s->worker.join();
+  for (auto* j : s->slotJob)
+    if (j) releaseJob(s, j);
+  delete s;
+  return RG_OK;
+}
+
+}  // extern "C"
