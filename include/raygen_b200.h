@@ -237,6 +237,7 @@ rg_status rg_load_scene_json(const char* path, rg_scene_desc** out);
 #define RG_JOB_RESIDENT 1
 #define RG_JOB_DONE 2
 #define RG_JOB_FAILED 3
+#define RG_JOB_ADMITTING 4  /* slot reserved; scene upload / BVH build in progress */
 
 typedef struct rg_server rg_server;
 

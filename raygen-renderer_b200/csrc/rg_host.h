@@ -27,7 +27,10 @@ DevRender makeRenderParams(const rg_settings& s, const rg_camera& c);
 struct DevPointLight;
 struct DevTexture;
 
-// Owning device allocation.
+// Owning device allocation from the stream-ordered pool.  Allocation and free
+// are ordered on the calling thread's per-thread stream, so releasing a buffer
+// does not synchronise the device; callers release a buffer only after the
+// streams that used it have been synchronised.
 template <class T>
 struct DevBuf {
   T* p = nullptr;
@@ -40,7 +43,8 @@ struct DevBuf {
     if (count <= n && p) return true;
     release();
     if (count == 0) count = 1;
-    if (cudaMalloc((void**)&p, count * sizeof(T)) != cudaSuccess) {
+    if (cudaMallocAsync((void**)&p, count * sizeof(T), cudaStreamPerThread) != cudaSuccess ||
+        cudaStreamSynchronize(cudaStreamPerThread) != cudaSuccess) {
       p = nullptr;
       n = 0;
       cudaGetLastError();
@@ -50,7 +54,7 @@ struct DevBuf {
     return true;
   }
   void release() {
-    if (p) cudaFree(p);
+    if (p) cudaFreeAsync(p, cudaStreamPerThread);
     p = nullptr;
     n = 0;
   }

@@ -66,6 +66,8 @@ struct ServerJob {
   bool snapshotReady = false;
 };
 
+constexpr int kAdmitThreads = 4;
+
 size_t estimateBytes(const rg_job_desc& d) {
   const size_t tris = d.scene ? (size_t)std::max(0, d.scene->num_triangles) : 0;
   const size_t px = (size_t)std::max(0, d.width) * (size_t)std::max(0, d.height);
@@ -91,7 +93,9 @@ struct rg_server {
   int residentPeak = 0;
   bool stop = false;
   std::thread worker;
+  std::vector<std::thread> admitters;
   cudaStream_t stream = nullptr;
+  std::vector<cudaStream_t> admitStreams;
   int numSMs = 148;
   // device tables and wavefront buffers
   DevBuf<DevJob> jobTable;
@@ -117,6 +121,7 @@ struct rg_server {
     if (hostSegs) cudaFreeHost(hostSegs);
     if (hostWave) cudaFreeHost(hostWave);
     if (stream) cudaStreamDestroy(stream);
+    for (auto a : admitStreams) cudaStreamDestroy(a);
   }
 };
 
@@ -190,9 +195,8 @@ void releaseJob(rg_server* s, ServerJob* j) {
 }
 
 // Upload scene, build BVH, allocate buffers, publish the job-table slot.
-rg_status admit(rg_server* s, ServerJob* j) {
+rg_status admit(rg_server* s, ServerJob* j, cudaStream_t st) {
   const rg_job_desc& d = j->desc;
-  cudaStream_t st = s->stream;
   if (!j->errWord.alloc(1)) return RG_ERR_OUT_OF_MEMORY;
   cudaMemsetAsync(j->errWord.p, 0, sizeof(int), st);
   rg_status rs = prepareScene(d.scene, s->base.bvh_bins, true, st, j->errWord.p, j->ds, j->S, j->view, nullptr);
@@ -250,51 +254,68 @@ void finishJob(rg_server* s, ServerJob* j) {
   j->error = ce != cudaSuccess ? RG_ERR_CUDA : (derr ? RG_ERR_DEVICE_STATUS : RG_OK);
 }
 
+// Admission thread: reserves a slot and budget for queued jobs and prepares
+// them (upload, BVH build, buffers) on its own stream, overlapping the waves.
+void admitLoop(rg_server* s, int idx) {
+  cudaStream_t st = s->admitStreams[idx];
+  for (;;) {
+    ServerJob* j = nullptr;
+    {
+      std::unique_lock<std::mutex> lk(s->mu);
+      for (;;) {
+        if (s->stop) return;
+        bool anyResident = false;
+        for (auto* x : s->slotJob)
+          if (x) anyResident = true;
+        if (!s->pending.empty() && !s->freeSlots.empty()) {
+          ServerJob* c = s->pending.front();
+          const size_t need = estimateBytes(c->desc);
+          if (!anyResident || s->bytesUsed + need <= s->cfg.hbm_budget_bytes) {
+            s->pending.pop_front();
+            c->slot = s->freeSlots.back();
+            s->freeSlots.pop_back();
+            s->slotJob[c->slot] = c;
+            c->state = RG_JOB_ADMITTING;
+            c->bytes = need;
+            s->bytesUsed += need;
+            s->bytesPeak = std::max(s->bytesPeak, s->bytesUsed);
+            j = c;
+            break;
+          }
+        }
+        s->cv.wait_for(lk, std::chrono::milliseconds(20));
+      }
+    }
+    const rg_status rs = admit(s, j, st);
+    std::lock_guard<std::mutex> lk(s->mu);
+    if (rs != RG_OK) {
+      j->error = rs;
+      j->state = RG_JOB_FAILED;
+      j->tDone = nowMs();
+      cudaStreamSynchronize(st);
+      releaseJob(s, j);
+    } else {
+      j->state = RG_JOB_RESIDENT;
+      j->tStart = nowMs();
+    }
+    s->cv.notify_all();
+  }
+}
+
 void serverLoop(rg_server* s) {
   cudaStream_t st = s->stream;
   int rr = 0;
   for (;;) {
-    // ---- admission
-    std::vector<ServerJob*> toAdmit;
     {
       std::unique_lock<std::mutex> lk(s->mu);
       if (s->stop) return;
-      bool anyResident = false;
+      bool work = false;
       for (auto* j : s->slotJob)
-        if (j) anyResident = true;
-      if (!anyResident && s->pending.empty()) {
-        s->cv.wait_for(lk, std::chrono::milliseconds(50));
+        if (j && j->state == RG_JOB_RESIDENT) work = true;
+      if (!work) {
+        s->cv.wait_for(lk, std::chrono::milliseconds(20));
         continue;
       }
-      while (!s->pending.empty() && !s->freeSlots.empty()) {
-        ServerJob* j = s->pending.front();
-        const size_t need = estimateBytes(j->desc);
-        if (anyResident && s->bytesUsed + need > s->cfg.hbm_budget_bytes) break;
-        s->pending.pop_front();
-        j->slot = s->freeSlots.back();
-        s->freeSlots.pop_back();
-        s->slotJob[j->slot] = j;
-        j->bytes = need;
-        s->bytesUsed += need;
-        s->bytesPeak = std::max(s->bytesPeak, s->bytesUsed);
-        toAdmit.push_back(j);
-        anyResident = true;
-      }
-    }
-    for (auto* j : toAdmit) {
-      const rg_status rs = admit(s, j);
-      std::lock_guard<std::mutex> lk(s->mu);
-      if (rs != RG_OK) {
-        j->error = rs;
-        j->state = RG_JOB_FAILED;
-        j->tDone = nowMs();
-        releaseJob(s, j);
-        s->cv.notify_all();
-      } else {
-        j->state = RG_JOB_RESIDENT;
-        j->tStart = nowMs();
-      }
-      s->cv.notify_all();
     }
     // ---- one wave over the resident jobs
     std::vector<ServerJob*> active;
@@ -453,7 +474,13 @@ rg_status rg_server_create(const rg_settings* base, const rg_server_config* cfg,
   int dev = 0;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&s->numSMs, cudaDevAttrMultiProcessorCount, dev);
-  if (cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking) != cudaSuccess || !allocServer(s) ||
+  bool streamsOk = cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking) == cudaSuccess;
+  for (int i = 0; i < kAdmitThreads && streamsOk; i++) {
+    cudaStream_t a = nullptr;
+    streamsOk = cudaStreamCreateWithFlags(&a, cudaStreamNonBlocking) == cudaSuccess;
+    if (streamsOk) s->admitStreams.push_back(a);
+  }
+  if (!streamsOk || !allocServer(s) ||
       !captureGraph(s)) {
     setLastError("server initialisation failed (device memory or graph capture)");
     delete s;
@@ -462,6 +489,7 @@ rg_status rg_server_create(const rg_settings* base, const rg_server_config* cfg,
   s->slotJob.assign(s->cfg.max_resident_jobs, nullptr);
   for (int i = s->cfg.max_resident_jobs - 1; i >= 0; i--) s->freeSlots.push_back(i);
   s->worker = std::thread(serverLoop, s);
+  for (int i = 0; i < (int)s->admitStreams.size(); i++) s->admitters.emplace_back(admitLoop, s, i);
   *out = s;
   return RG_OK;
 }
@@ -495,7 +523,7 @@ rg_status rg_server_poll(rg_server* s, int64_t job, rg_job_status* out) {
   out->submit_ms = j->tSubmit;
   out->start_ms = j->tStart;
   out->done_ms = j->tDone;
-  out->latency_ms = j->state >= RG_JOB_DONE ? j->tDone - j->tSubmit : -1.0;
+  out->latency_ms = (j->state == RG_JOB_DONE || j->state == RG_JOB_FAILED) ? j->tDone - j->tSubmit : -1.0;
   out->samples_issued = (int64_t)j->issuedSamples * j->pixels + j->pixelCursor;
   out->samples_total = (int64_t)j->desc.samples * j->desc.width * j->desc.height;
   return RG_OK;
@@ -508,8 +536,9 @@ rg_status rg_server_wait(rg_server* s, int64_t job, double timeout_ms) {
   if (it == s->jobs.end()) return RG_ERR_INVALID_ARGUMENT;
   ServerJob* j = it->second.get();
   const auto deadline = std::chrono::steady_clock::now() + std::chrono::duration<double, std::milli>(timeout_ms);
-  while (j->state < RG_JOB_DONE) {
-    if (s->cv.wait_until(lk, deadline) == std::cv_status::timeout && j->state < RG_JOB_DONE) return RG_ERR_BUSY;
+  auto finished = [&]() { return j->state == RG_JOB_DONE || j->state == RG_JOB_FAILED; };
+  while (!finished()) {
+    if (s->cv.wait_until(lk, deadline) == std::cv_status::timeout && !finished()) return RG_ERR_BUSY;
   }
   return j->state == RG_JOB_DONE ? RG_OK : j->error;
 }
@@ -537,8 +566,9 @@ rg_status rg_server_snapshot(rg_server* s, int64_t job, float* hdr_rgba, size_t 
   if (it == s->jobs.end()) return RG_ERR_INVALID_ARGUMENT;
   ServerJob* j = it->second.get();
   const auto deadline = std::chrono::steady_clock::now() + std::chrono::duration<double, std::milli>(timeout_ms);
-  while (j->state == RG_JOB_QUEUED) {  // wait for admission
-    if (s->cv.wait_until(lk, deadline) == std::cv_status::timeout && j->state == RG_JOB_QUEUED) return RG_ERR_BUSY;
+  auto waiting = [&]() { return j->state == RG_JOB_QUEUED || j->state == RG_JOB_ADMITTING; };
+  while (waiting()) {  // wait for admission
+    if (s->cv.wait_until(lk, deadline) == std::cv_status::timeout && waiting()) return RG_ERR_BUSY;
   }
   if (j->state == RG_JOB_DONE) {
     if (count < j->result.size()) return RG_ERR_INVALID_ARGUMENT;
@@ -600,6 +630,9 @@ rg_status rg_server_destroy(rg_server* s) {
     s->cv.notify_all();
   }
   if (s->worker.joinable()) s->worker.join();
+  for (auto& t : s->admitters)
+    if (t.joinable()) t.join();
+  cudaDeviceSynchronize();
   for (auto* j : s->slotJob)
     if (j) releaseJob(s, j);
   delete s;
