@@ -115,3 +115,27 @@ def random_rays(scene_bounds, n, seed, camera_fraction=0.5, camera=(0, 0, 0)):
     d[:nc, 2] = -np.abs(d[:nc, 2]) - 1.0
     d /= np.linalg.norm(d, axis=1, keepdims=True)
     return np.concatenate([o, d], axis=1).astype(np.float32)
+
+
+# A small room in the reference scene-JSON schema (comments, trailing commas and
+# a bare key included): 6 planes, an emissive quad and a rotated box.
+JSON_ROOM = """
+// a small room in the reference schema (comments, trailing commas and a bare key)
+{
+  "mainCamera": { "location": [0, 0.5, 6], "angle": [-5, 0, 0], "fieldOfView": 60, exposure: 1.5, },
+  "_materials": { "wall": { "color": "#ccbbaa", "diffuse": 0.9 } },
+  "room": {
+    "lamp": { "location": [0, 2.9, 0], "angle": [180, 0, 0], "scale": [1, 1, 1],
+              "mesh": { "type": "plane" }, "mat": { "color": "#fffff0", "emission": 8 } },
+    "floor": { "location": [0, -3, 0], "scale": [6, 1, 6], "mesh": { "type": "plane" }, "mat": "wall" },
+    "ceiling": { "location": [0, 3, 0], "angle": [180, 0, 0], "scale": [6, 1, 6], "mesh": { "type": "plane" }, "mat": "wall" },
+    "left": { "location": [-3, 0, 0], "angle": [0, 0, -90], "scale": [6, 1, 6], "mesh": { "type": "plane" },
+              "mat": { "color": "#ff5555" } },
+    "right": { "location": [3, 0, 0], "angle": [0, 0, 90], "scale": [6, 1, 6], "mesh": { "type": "plane" },
+               "mat": { "color": [0.3, 1.0, 0.3] } },
+    "back": { "location": [0, 0, -3], "angle": [90, 0, 0], "scale": [6, 1, 6], "mesh": { "type": "plane" }, "mat": "wall" },
+    "box": { "location": [1.2, -2, -0.5], "angle": [0, -30, 0], "scale": [1.6, 2, 1.6], "mesh": { "type": "cube" },
+             "mat": { "color": "#ffffff", "glossy": 0.3, "roughness": 0.2 } },
+  },
+}
+"""
