@@ -216,6 +216,29 @@ rg_status rg_denoise_atrous(int32_t w, int32_t h, const float* color, const floa
                             const float* depth, const float* albedo, const float* albedo_alpha,
                             int32_t levels, float sigma_color, float sigma_normal,
                             float sigma_depth, float intensity, float* out);
+/* The same A-Trous filter on DEVICE buffers, without allocating.  No
+ * counterpart in the reference: it exists for callers that cannot let the
+ * library allocate device memory (a preview loop that must not take the
+ * device-wide synchronisation of cudaFree, an application whose device memory
+ * all comes from its own pool).  The library makes no cudaMalloc/cudaFree or
+ * other allocating call here; the filter's working buffers are one static
+ * device array per device.
+ *   color_rgba, out_rgba: w*h float4 (RGBA, alpha ignored / written as 1),
+ *                         16-byte aligned device memory of the current device;
+ *   normal, albedo: w*h*3 floats; depth, albedo_alpha: w*h floats (device).
+ *   stream: a cudaStream_t, NULL for the default stream.  The work is
+ *   enqueued on it and the call returns; out_rgba is ready when it completes.
+ * Limit: w*h <= 1,048,576 pixels, else RG_ERR_INVALID_ARGUMENT.  Host or
+ * foreign-device pointers give RG_ERR_INVALID_ARGUMENT.  Buffer sizes cannot
+ * be checked: each must hold w*h elements of the layout above.
+ * Calls whose device work overlaps (other streams, unsynchronised threads)
+ * share the working buffers and race; serialise them.  The first call on a
+ * device resolves the working array's address; make it before any stream
+ * capture begins.  Results equal rg_denoise_atrous on the same inputs. */
+rg_status rg_denoise_atrous_noalloc(int32_t w, int32_t h, const float* color_rgba, const float* normal,
+                                    const float* depth, const float* albedo, const float* albedo_alpha,
+                                    int32_t levels, float sigma_color, float sigma_normal,
+                                    float sigma_depth, float intensity, float* out_rgba, void* stream);
 rg_status rg_tonemap(int32_t w, int32_t h, const float* hdr_rgba, float* ldr_rgba);
 
 /* Procedural scenes (host C++, no device work).

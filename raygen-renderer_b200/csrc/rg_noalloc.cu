@@ -1,0 +1,166 @@
+// rg_noalloc.cu - A-Trous denoise on caller device buffers, without allocating.
+//
+// rg_denoise_atrous takes host buffers and allocates its own device copies
+// and working buffers on every call.  Some callers cannot have the library
+// allocate: an interactive preview loop that denoises every progressive
+// snapshot cannot absorb the device-wide synchronisation that cudaFree
+// implies, and a host application that owns all device memory through its
+// own pool (a framework's caching allocator, a fixed memory budget per
+// process) does not want a second allocator touching the device at all.
+// rg_denoise_atrous_noalloc serves them: inputs and output stay in the
+// caller's device memory and the filter's working buffers live in one
+// statically sized __device__ array of this module, so a call makes no
+// cudaMalloc / cudaFree / allocating-library call of any kind.
+//
+// It runs exactly the kernels of rg_denoise_atrous (float -> half guide
+// conversion, firefly pre-clamp + albedo demodulation, the A-Trous levels,
+// remodulation), so the two agree bit for bit on the same inputs.
+//
+// Limits and rules (also stated in the C header):
+//  * w * h <= kMaxPixels (1,048,576, e.g. 1024 x 1024); larger images are
+//    rejected with RG_ERR_INVALID_ARGUMENT before any device work.
+//  * The working buffers are shared by all calls on a device: calls whose
+//    device work overlaps (different streams, or different host threads
+//    without ordering) race on them and corrupt each other's results.
+//    Serialise them on one stream, or wait for one call's stream work before
+//    the next call is issued.
+//  * Nothing in the working buffers has to start at zero: every pass writes
+//    each pixel of its destination before any later pass reads it, so no
+//    clearing is done between calls.
+//  * The first call on a device resolves the array's device address
+//    (cudaGetSymbolAddress, which may load this module); make that first
+//    call before any stream capture begins.
+#include <cuda_fp16.h>
+#include <cuda_runtime.h>
+
+#include <mutex>
+#include <string>
+
+#include "rg_host.h"
+#include "rg_trace.cuh"
+
+namespace rg {
+
+namespace {
+
+constexpr size_t kMaxPixels = size_t(1) << 20;
+// Layout of the working array, each part 256-byte aligned:
+//   two float4 ping-pong colour buffers, then the half guides
+//   (normal x3, albedo x3, depth, albedo alpha).
+constexpr size_t kColourBytes = kMaxPixels * sizeof(float4);
+constexpr size_t kOffA = 0;
+constexpr size_t kOffB = kOffA + kColourBytes;
+constexpr size_t kOffNormal = kOffB + kColourBytes;
+constexpr size_t kOffAlbedo = kOffNormal + kMaxPixels * 3 * sizeof(__half);
+constexpr size_t kOffDepth = kOffAlbedo + kMaxPixels * 3 * sizeof(__half);
+constexpr size_t kOffAlbedoA = kOffDepth + kMaxPixels * sizeof(__half);
+constexpr size_t kScratchBytes = kOffAlbedoA + kMaxPixels * sizeof(__half);  // 48 MiB
+static_assert(kOffB % 256 == 0 && kOffNormal % 256 == 0 && kOffAlbedo % 256 == 0 && kOffDepth % 256 == 0 &&
+                  kOffAlbedoA % 256 == 0,
+              "working buffer parts must stay 256-byte aligned");
+
+static __device__ __align__(256) unsigned char g_atrousScratch[kScratchBytes];
+
+constexpr int kMaxDevices = 64;
+std::mutex g_setupMu;
+unsigned char* g_scratchOnDevice[kMaxDevices] = {};
+
+// Device address of the working array on the current device, resolved once
+// per device (with that device current).
+rg_status scratchForCurrentDevice(unsigned char** out) {
+  int dev = -1;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    setLastError(std::string("rg_denoise_atrous_noalloc: no current CUDA device: ") + cudaGetErrorString(e));
+    return RG_ERR_NO_DEVICE;
+  }
+  if (dev < 0 || dev >= kMaxDevices) {
+    setLastError("rg_denoise_atrous_noalloc: device ordinal out of range");
+    return RG_ERR_NO_DEVICE;
+  }
+  std::lock_guard<std::mutex> lk(g_setupMu);
+  if (!g_scratchOnDevice[dev]) {
+    void* p = nullptr;
+    e = cudaGetSymbolAddress(&p, g_atrousScratch);
+    if (e != cudaSuccess || !p) {
+      cudaGetLastError();
+      setLastError(std::string("rg_denoise_atrous_noalloc: cudaGetSymbolAddress failed: ") + cudaGetErrorString(e));
+      return RG_ERR_CUDA;
+    }
+    g_scratchOnDevice[dev] = static_cast<unsigned char*>(p);
+  }
+  *out = g_scratchOnDevice[dev];
+  return RG_OK;
+}
+
+// A caller pointer must be device (or managed) memory visible on the current
+// device and aligned for its element type; host pointers are refused here
+// rather than faulting in a kernel.
+bool deviceBuffer(const void* p, size_t align, int dev, const char* name) {
+  if (!p || (reinterpret_cast<uintptr_t>(p) % align) != 0) {
+    setLastError(std::string("rg_denoise_atrous_noalloc: ") + name + " is null or misaligned");
+    return false;
+  }
+  cudaPointerAttributes a;
+  const cudaError_t e = cudaPointerGetAttributes(&a, p);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    setLastError(std::string("rg_denoise_atrous_noalloc: ") + name + ": " + cudaGetErrorString(e));
+    return false;
+  }
+  const bool ok = a.type == cudaMemoryTypeManaged || (a.type == cudaMemoryTypeDevice && a.device == dev);
+  if (!ok) setLastError(std::string("rg_denoise_atrous_noalloc: ") + name + " is not device memory of the current device");
+  return ok;
+}
+
+}  // namespace
+
+}  // namespace rg
+
+extern "C" rg_status rg_denoise_atrous_noalloc(int32_t w, int32_t h, const float* color_rgba, const float* normal,
+                                               const float* depth, const float* albedo, const float* albedo_alpha,
+                                               int32_t levels, float sigma_color, float sigma_normal,
+                                               float sigma_depth, float intensity, float* out_rgba, void* stream) {
+  using namespace rg;
+  if (w <= 0 || h <= 0) {
+    setLastError("rg_denoise_atrous_noalloc: width and height must be positive");
+    return RG_ERR_INVALID_ARGUMENT;
+  }
+  const size_t n = (size_t)w * (size_t)h;
+  if (n > kMaxPixels) {
+    setLastError("rg_denoise_atrous_noalloc: " + std::to_string(w) + " x " + std::to_string(h) + " = " +
+                 std::to_string(n) + " pixels exceeds the working-buffer limit of " + std::to_string(kMaxPixels) +
+                 " pixels; use rg_denoise_atrous");
+    return RG_ERR_INVALID_ARGUMENT;
+  }
+  unsigned char* s = nullptr;
+  const rg_status rs = scratchForCurrentDevice(&s);
+  if (rs != RG_OK) return rs;
+  int dev = 0;
+  cudaGetDevice(&dev);
+  if (!deviceBuffer(color_rgba, 16, dev, "color_rgba") || !deviceBuffer(out_rgba, 16, dev, "out_rgba") ||
+      !deviceBuffer(normal, 4, dev, "normal") || !deviceBuffer(depth, 4, dev, "depth") ||
+      !deviceBuffer(albedo, 4, dev, "albedo") || !deviceBuffer(albedo_alpha, 4, dev, "albedo_alpha"))
+    return RG_ERR_INVALID_ARGUMENT;
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  float4* bufA = reinterpret_cast<float4*>(s + kOffA);
+  float4* bufB = reinterpret_cast<float4*>(s + kOffB);
+  __half* hn = reinterpret_cast<__half*>(s + kOffNormal);
+  __half* ha = reinterpret_cast<__half*>(s + kOffAlbedo);
+  __half* hd = reinterpret_cast<__half*>(s + kOffDepth);
+  __half* haa = reinterpret_cast<__half*>(s + kOffAlbedoA);
+  const int N = (int)n;
+  launchFloatToHalf(N * 3, normal, hn, st);
+  launchFloatToHalf(N * 3, albedo, ha, st);
+  launchFloatToHalf(N, depth, hd, st);
+  launchFloatToHalf(N, albedo_alpha, haa, st);
+  launchDenoise(w, h, reinterpret_cast<const float4*>(color_rgba), hn, hd, ha, haa, levels, sigma_color, sigma_normal,
+                sigma_depth, intensity, bufA, bufB, reinterpret_cast<float4*>(out_rgba), st);
+  const cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) {
+    setLastError(std::string("rg_denoise_atrous_noalloc: launch failed: ") + cudaGetErrorString(e));
+    return RG_ERR_CUDA;
+  }
+  return RG_OK;
+}
