@@ -1521,12 +1521,71 @@ static void tonemap(int w, int h, const float* src, float* dst) {
   }
 }
 
+// Camera view transform, Renderer::applyCameraTransform (renderer.cpp:24-28):
+// rotate by -angle, then translate by -location.  Row-vector convention
+// p_view = [p 1] * M, whose 3x3 block is R = Ry(ay) Rx(ax) Rz(az) (degrees,
+// active right-handed rotations) and whose last row is -(location * R); that
+// is, p_view = R^T (p - location).  The order of the three axis rotations
+// lives in the graphics-module submodule, which the reference tree does not
+// vendor; single-axis angles (the sample scenes') do not depend on it.  The
+// products run in a fixed order without contraction (this file is built with
+// -ffp-contract=off), so view-space vertices are bit-identical to the
+// device's, and angle 0 reduces to p - location exactly.
+struct ViewM {
+  float m[16];
+};
+
+static ViewM cameraView(const rg_camera& c) {
+  const float d2r = 3.14159265358979323846f / 180.0f;
+  const float ax = c.angle[0] * d2r, ay = c.angle[1] * d2r, az = c.angle[2] * d2r;
+  const double cx = std::cos(ax), sx = std::sin(ax), cy = std::cos(ay), sy = std::sin(ay), cz = std::cos(az),
+               sz = std::sin(az);
+  const double Rx[3][3] = {{1, 0, 0}, {0, cx, -sx}, {0, sx, cx}};
+  const double Ry[3][3] = {{cy, 0, sy}, {0, 1, 0}, {-sy, 0, cy}};
+  const double Rz[3][3] = {{cz, -sz, 0}, {sz, cz, 0}, {0, 0, 1}};
+  double T[3][3], R[3][3];
+  for (int i = 0; i < 3; i++)
+    for (int j = 0; j < 3; j++) {
+      T[i][j] = 0;
+      for (int k = 0; k < 3; k++) T[i][j] += Ry[i][k] * Rx[k][j];
+    }
+  for (int i = 0; i < 3; i++)
+    for (int j = 0; j < 3; j++) {
+      R[i][j] = 0;
+      for (int k = 0; k < 3; k++) R[i][j] += T[i][k] * Rz[k][j];
+    }
+  ViewM M;
+  memset(M.m, 0, sizeof(M.m));
+  for (int i = 0; i < 3; i++)
+    for (int j = 0; j < 3; j++) M.m[i * 4 + j] = (float)R[i][j];
+  for (int j = 0; j < 3; j++) {
+    const float t = c.location[0] * M.m[j] + c.location[1] * M.m[4 + j] + c.location[2] * M.m[8 + j];
+    M.m[12 + j] = -t;
+  }
+  M.m[15] = 1.0f;
+  return M;
+}
+
+static V3 viewPoint(const ViewM& M, const float* p) {
+  float o[3];
+  for (int j = 0; j < 3; j++) o[j] = ((p[0] * M.m[j] + p[1] * M.m[4 + j]) + p[2] * M.m[8 + j]) + M.m[12 + j];
+  return V3(o[0], o[1], o[2]);
+}
+
+// Directions by the rotation block, renormalised (R is orthonormal, so it is
+// its own inverse transpose).
+static V3 viewDir(const ViewM& M, const float* p) {
+  float o[3];
+  for (int j = 0; j < 3; j++) o[j] = (p[0] * M.m[j] + p[1] * M.m[4 + j]) + p[2] * M.m[8 + j];
+  const float l = sqrtf((o[0] * o[0] + o[1] * o[1]) + o[2] * o[2]);
+  return l > 0.0f ? V3(o[0] / l, o[1] / l, o[2] / l) : V3(o[0], o[1], o[2]);
+}
+
 static Scene* buildScene(const rg_scene_desc* d, int bins) {
   Scene* s = new Scene();
   const int nt = d->num_triangles;
-  // Camera: view = translate(-location) for angle == 0 (renderer.cpp:24-28).
-  const V3 loc(d->camera.location[0], d->camera.location[1], d->camera.location[2]);
-  s->camLoc = loc;
+  const ViewM view = cameraView(d->camera);
+  s->camLoc = V3(d->camera.location[0], d->camera.location[1], d->camera.location[2]);
   s->fov = d->camera.field_of_view;
   s->viewNear = d->camera.view_near;
   s->viewFar = d->camera.view_far;
@@ -1574,9 +1633,8 @@ static Scene* buildScene(const rg_scene_desc* d, int bins) {
     Tri& t = s->tris[i];
     const float* p = &d->positions[(size_t)i * 9];
     const float* n = &d->normals[(size_t)i * 9];
-    t.v1 = V3(p[0], p[1], p[2]) - loc; t.v2 = V3(p[3], p[4], p[5]) - loc; t.v3 = V3(p[6], p[7], p[8]) - loc;
-    t.n1 = normalize(V3(n[0], n[1], n[2])); t.n2 = normalize(V3(n[3], n[4], n[5]));
-    t.n3 = normalize(V3(n[6], n[7], n[8]));
+    t.v1 = viewPoint(view, p); t.v2 = viewPoint(view, p + 3); t.v3 = viewPoint(view, p + 6);
+    t.n1 = viewDir(view, n); t.n2 = viewDir(view, n + 3); t.n3 = viewDir(view, n + 6);
     for (int k = 0; k < 6; k++) t.uv[k] = d->uvs ? d->uvs[(size_t)i * 6 + k] : 0.0f;
     // precalc: raycommon.cpp:128-149
     const V3 pd = cross(t.v2 - t.v1, t.v3 - t.v2);
@@ -1597,8 +1655,8 @@ static Scene* buildScene(const rg_scene_desc* d, int bins) {
   for (int i = 0; i < d->num_point_lights; i++) {
     const rg_point_light& pl = d->point_lights[i];
     PointLight o;
-    o.pos = V3(pl.position[0], pl.position[1], pl.position[2]) - loc;
-    o.normal = V3(pl.normal[0], pl.normal[1], pl.normal[2]);
+    o.pos = viewPoint(view, pl.position);
+    o.normal = viewDir(view, pl.normal);
     o.mat = pl.material;
     s->points.push_back(o);
   }

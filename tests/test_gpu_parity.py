@@ -34,6 +34,9 @@ def image_parity(rg, orc, scene, W, H, spp, **kw):
     v2 = np.maximum(ref["sumsq"] / n - m2 * m2, 0.0)
     # same sample sequence on both sides -> compare against the oracle's own SEM (x sqrt2 for two estimates)
     se = np.sqrt(2.0 * v2 / n)
+    # the HDR result is the sample mean times the camera exposure (rayrenderer.cpp:997-999)
+    exposure = float(scene.desc.camera.exposure)
+    m2, se = m2 * exposure, se * exposure
     z = np.abs(g - m2) / np.maximum(se, 1e-6)
     z[(se < 1e-6) & (np.abs(g - m2) < 1e-4)] = 0.0
     stats = r.stats()
