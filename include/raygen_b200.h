@@ -157,6 +157,17 @@ typedef struct rg_scene_desc {
   int32_t num_textures;
   const rg_texture* textures;
   rg_camera camera;
+  /* Environment map (Scene::envmap / envmapIntensity / envmapRotation,
+   * scene.h:187-190; sampleEnvironment, rayrenderer.cpp:1299-1348): an
+   * equirectangular texture looked up by the VIEW-space ray direction (as in
+   * the reference), rotated by envmap_rotation degrees about +Y, times
+   * envmap_intensity; importance-sampled by luminance x sin(theta)
+   * (Scene::buildEnvmapCDF, scene.cpp:330-463).  A zero-initialised
+   * description has no environment map. */
+  int32_t has_envmap;         /* 0 none */
+  int32_t envmap_texture;     /* index into textures                          */
+  float envmap_intensity;
+  float envmap_rotation;      /* degrees */
 } rg_scene_desc;
 
 typedef struct rg_stats {

@@ -68,6 +68,8 @@ def load(fast: bool = False) -> C.CDLL:
     lib.orc_phase_pdf.restype = C.c_float
     lib.orc_phase_pdf.argtypes = [C.c_float, C.c_float]
     lib.orc_sample_phase.argtypes = [C.c_float, C.c_float, C.c_float, f]
+    lib.orc_env_eval.argtypes = [C.c_void_p, f, C.c_int32, f, f]
+    lib.orc_env_sample.argtypes = [C.c_void_p, f, C.c_int32, f, f]
     _libs[name] = lib
     return lib
 
@@ -113,6 +115,22 @@ class OracleScene:
         out = np.empty(n, np.uint8)
         self.lib.orc_any(self.h, _fp(rays), _fp(tmax), n, predicate, out.ctypes.data_as(C.POINTER(C.c_uint8)))
         return out.astype(bool)
+
+    def env_eval(self, dirs):
+        """(radiance n x 3, pdf n) of the environment map for view-space directions n x 3."""
+        d = np.ascontiguousarray(dirs, np.float32).reshape(-1, 3)
+        rgb = np.zeros((d.shape[0], 3), np.float32)
+        pdf = np.zeros(d.shape[0], np.float32)
+        self.lib.orc_env_eval(self.h, _fp(d), d.shape[0], _fp(rgb), _fp(pdf))
+        return rgb, pdf
+
+    def env_sample(self, u):
+        """Luminance-importance samples: u n x 2 in [0,1) -> (directions n x 3, pdf n)."""
+        uu = np.ascontiguousarray(u, np.float32).reshape(-1, 2)
+        d = np.zeros((uu.shape[0], 3), np.float32)
+        pdf = np.zeros(uu.shape[0], np.float32)
+        self.lib.orc_env_sample(self.h, _fp(uu), uu.shape[0], _fp(d), _fp(pdf))
+        return d, pdf
 
     def render(self, width, height, spp, shader=5, seed=1, max_depth=32, rr_depth=3, threads=None,
                mix_tree=False, antialias=True, color_sampling=True, denoise=False, denoise_levels=5,

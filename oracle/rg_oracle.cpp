@@ -289,6 +289,11 @@ struct Scene {
   std::vector<int> areaLights;   // object ids
   std::vector<PointLight> points;
   std::vector<Texture> textures;
+  // equirectangular environment (Scene::envmap*, scene.h:187-190)
+  int envTex = -1;
+  int envW = 0, envH = 0;
+  float envIntensity = 1.0f, envCosY = 1.0f, envSinY = 0.0f, envTotal = 0.0f;
+  std::vector<float> envMarg, envCond;  // H+1 ; H x (W+1)
   // camera (RenderThreadContext, rayrenderer.cpp:97-132)
   V3 camLoc;
   float fov, viewNear, viewFar, dof, aperture, apertureRot, exposure;
@@ -724,6 +729,124 @@ struct Tracer {
     return a + p;
   }
 
+  // ---- equirectangular environment map ----------------------------------
+  bool envSampling() const { return s.envTex >= 0 && s.envW > 0 && s.envTotal > 0.0f; }
+  const float* envTexel(int x, int y) const {
+    return &s.textures[s.envTex].rgba[((size_t)y * s.envW + x) * 4];
+  }
+  static float texelLum(const float* c) { return fmaxf(0.0f, 0.2126f * c[0] + 0.7152f * c[1] + 0.0722f * c[2]); }
+
+  // sampleEnvironment, equirectangular branch (rayrenderer.cpp:1299-1348):
+  // view-space direction, yaw about +Y, lat-long lookup through Texture::sample.
+  C3 sampleEnvironment(V3 dir) const {
+    if (s.envTex < 0) return C3();
+    const V3 d = normalize(dir);
+    const float rx = d.x * s.envCosY - d.z * s.envSinY;
+    const float rz = d.x * s.envSinY + d.z * s.envCosY;
+    const float u = 0.5f + atan2f(rz, rx) * (float)(0.5 / M_PI);
+    const float v = 0.5f - asinf(fminf(fmaxf(d.y, -1.0f), 1.0f)) * (float)(1.0 / M_PI);
+    return texSample(s, s.envTex, u, v) * s.envIntensity;
+  }
+
+  // envmapDirectionPdf, equirectangular branch (rayrenderer.cpp:1521-1573)
+  float envmapDirectionPdf(V3 dir) const {
+    if (!envSampling()) return 0.0f;
+    const V3 d = normalize(dir);
+    const float rx = d.x * s.envCosY - d.z * s.envSinY;
+    const float rz = d.x * s.envSinY + d.z * s.envCosY;
+    const int W = s.envW, H = s.envH;
+    const float u = 0.5f + atan2f(rz, rx) * (float)(0.5 / M_PI);
+    const float v = 0.5f - asinf(fminf(fmaxf(d.y, -1.0f), 1.0f)) * (float)(1.0 / M_PI);
+    int x = (int)(u * W); if (x < 0) x = 0; if (x >= W) x = W - 1;
+    int y = (int)(v * H); if (y < 0) y = 0; if (y >= H) y = H - 1;
+    const float lum = texelLum(envTexel(x, y));
+    const float sinTheta = sinf((float)M_PI * v);
+    if (sinTheta <= 0.0f) return 0.0f;
+    const float pdfUV = (lum * sinTheta) / s.envTotal;
+    return pdfUV * (float)(W * H) / (2.0f * (float)(M_PI * M_PI) * sinTheta);
+  }
+
+  // searchCDF (rayrenderer.cpp:1353-1362): largest i with cdf[i] <= u in [0, n-1]
+  static int searchCDF(const float* cdf, int n, float u) {
+    int lo = 0, hi = n;
+    while (lo < hi) {
+      const int mid = (lo + hi) >> 1;
+      if (cdf[mid + 1] <= u) lo = mid + 1;
+      else hi = mid;
+    }
+    return lo < n ? lo : n - 1;
+  }
+
+  // sampleEnvmapDirection, equirectangular branch (rayrenderer.cpp:1426-1482)
+  void sampleEnvmapDirection(float u0, float u1, V3& outDir, float& outPdf) const {
+    outDir = V3(0, 1, 0);
+    outPdf = 0.0f;
+    if (!envSampling()) return;
+    const int W = s.envW, H = s.envH;
+    const int y = searchCDF(s.envMarg.data(), H, u0);
+    const float* row = &s.envCond[(size_t)y * (W + 1)];
+    const int x = searchCDF(row, W, u1);
+    const float yPrev = s.envMarg[y], ySpan = s.envMarg[y + 1] - yPrev;
+    const float xPrev = row[x], xSpan = row[x + 1] - xPrev;
+    const float yFrac = ySpan > 0.0f ? (u0 - yPrev) / ySpan : 0.5f;
+    const float xFrac = xSpan > 0.0f ? (u1 - xPrev) / xSpan : 0.5f;
+    const float u = (x + xFrac) / (float)W;
+    const float v = (y + yFrac) / (float)H;
+    const float phi = (u - 0.5f) * 2.0f * (float)M_PI;
+    const float theta = (0.5f - v) * (float)M_PI;
+    const float cosT = cosf(theta);
+    const float dx = cosT * cosf(phi), dy = sinf(theta), dz = cosT * sinf(phi);
+    const float wx = dx * s.envCosY + dz * s.envSinY;
+    const float wz = -dx * s.envSinY + dz * s.envCosY;
+    outDir = normalize(V3(wx, dy, wz));
+    const float lum = texelLum(envTexel(x, y));
+    const float sinTheta = sinf((float)M_PI * v);
+    if (sinTheta <= 0.0f) return;
+    const float pdfUV = (lum * sinTheta) / s.envTotal;
+    outPdf = pdfUV * (float)(W * H) / (2.0f * (float)(M_PI * M_PI) * sinTheta);
+  }
+
+  // sampleEnvmapForNEE (rayrenderer.cpp:2038-2065): luminance-IS direction,
+  // front-facing test, unbounded shadow ray with the point/env occluders.
+  bool sampleEnvmapForNEE(V3 hit, V3 n, int v, V3& outDir, float& outPdf, C3& outLi) const {
+    if (!envSampling()) return false;
+    V3 dir;
+    float pdf = 0.0f;
+    sampleEnvmapDirection(c.prng(v, S_ENV0), c.prng(v, S_ENV1), dir, pdf);
+    if (pdf <= 0.0f) return false;
+    if (dot(dir, n) <= 0.0f) return false;
+    if (intersectAny(s, SurfaceRay(hit, dir, n), 1e30f, P_POINT)) return false;
+    outDir = dir;
+    outPdf = pdf;
+    outLi = sampleEnvironment(dir);
+    return true;
+  }
+
+  // traceEnvmapLight (rayrenderer.cpp:1484-1519): Lambertian env NEE; the MIS
+  // partner is the caller's bsdfPdf argument.
+  C3 traceEnvmapLight(V3 hit, V3 n, float bsdfPdf, int v) const {
+    V3 dir;
+    float pdf = 0.0f;
+    C3 Li;
+    if (!sampleEnvmapForNEE(hit, n, v, dir, pdf, Li)) return C3();
+    const float cosObj = dot(dir, n);
+    float w = 1.0f;
+    if (bsdfPdf > 0.0f) w = (pdf * pdf) / (pdf * pdf + bsdfPdf * bsdfPdf);
+    return Li * (cosObj * w / ((float)M_PI * pdf));
+  }
+
+  // Miss radiance with the BSDF-side MIS weight (rayrenderer.cpp:1619-1630).
+  C3 missRadiance(const Ray& ray, const Param* sp) const {
+    C3 env = sampleEnvironment(ray.d);
+    if (sp && sp->bsdfPdf > 0.0f) {
+      const float envPdf = envmapDirectionPdf(ray.d);
+      const float b2 = sp->bsdfPdf * sp->bsdfPdf, e2 = envPdf * envPdf;
+      const float w = (b2 + e2 > 0.0f) ? b2 / (b2 + e2) : 1.0f;
+      env = env * w;
+    }
+    return env;
+  }
+
   // lambertTraceLights: rayrenderer.cpp:2319-2335
   C3 lambertTraceLights(V3 hit, V3 n, int v) const {
     C3 a, p;
@@ -766,6 +889,8 @@ struct Tracer {
     p.bsdfPdf = cosS * (float)(1.0 / M_PI);
     C3 col = traceLight(p.info->hit, p.vi.normal, v);
     col += tracePath(ray, &p);
+    // the MIS partner passed is this vertex's own cosine-sampled pdf (bsdf.cpp:86-88)
+    col += traceEnvmapLight(p.info->hit, p.vi.normal, p.bsdfPdf, v);
     p.throughput = savedT;
     p.bsdfPdf = savedPdf;
     return col * albedo;
@@ -849,6 +974,16 @@ struct Tracer {
         if (evalGlossy(lDir, fCos, pb)) {
           const float w = pl * pl / (pl * pl + pb * pb);
           direct += Le * fCos * (w / pl);
+        }
+      }
+    }
+    {  // envmap NEE with MIS (bsdf.cpp:302-314)
+      V3 eDir; float pe = 0.0f; C3 Li;
+      if (sampleEnvmapForNEE(p.info->hit, normal, v, eDir, pe, Li)) {
+        C3 fCos; float pb = 0.0f;
+        if (evalGlossy(eDir, fCos, pb)) {
+          const float w = pe * pe / (pe * pe + pb * pb);
+          direct += Li * fCos * (w / pe);
         }
       }
     }
@@ -1097,7 +1232,7 @@ struct Tracer {
     HitInfo info;
     intersectClosest(s, ray, info);
     if (info.tri >= 0) return shadeSimple(info, ray, interp(s, info), nullptr, depth);
-    return C3();
+    return sampleEnvironment(ray.d);  // tracePath miss without BSDF parameters
   }
 
   // tracePath: rayrenderer.cpp:1596-1864 (homogeneous media only)
@@ -1108,7 +1243,7 @@ struct Tracer {
     const Medium* med = medId >= 0 ? &s.media[medId] : nullptr;
     if (!med || !med->active()) {
       if (info.tri >= 0) return shade5(info, ray, interp(s, info), sp);
-      return C3();  // no environment map: sampleEnvironment == 0
+      return missRadiance(ray, sp);
     }
     const float maxT = info.tri >= 0 ? info.t : RAY_MAX_DISTANCE;
     const int v = c.vertex;  // the event index this segment ends in
@@ -1131,6 +1266,9 @@ struct Tracer {
       V3 lDir; float pl = 0.0f; C3 Le;
       if (sampleAreaLightForNEE(pos, proxy, v, lDir, pl, Le) && pl > 0.0f)
         direct += Le * med->phasePdf(-ray.d, lDir) * (1.0f / pl);
+      V3 eDir; float pe = 0.0f; C3 Li;
+      if (sampleEnvmapForNEE(pos, proxy, v, eDir, pe, Li) && pe > 0.0f)
+        direct += Li * med->phasePdf(-ray.d, eDir) * (1.0f / pe);
       const V3 nd = med->samplePhase(ray.d, c.prng(v, S_PHASE0), c.prng(v, S_PHASE1));
       Param q;
       q.info = &info; q.inray = ray; q.passes = passes; q.medium = medId;
@@ -1161,7 +1299,7 @@ struct Tracer {
       if (dot(ray.d, vi.normal) > 0.0f && dot(ray.d, geomN) < 0.0f) vi.normal = geomN;
       return medEm + surfW * shade5(info, ray, vi, sp);
     }
-    return medEm;  // no environment map
+    return medEm + surfW * missRadiance(ray, sp);
   }
 
   // traceEyeRay: rayrenderer.cpp:1254-1297 ; returns rgb of the color4
@@ -1169,12 +1307,13 @@ struct Tracer {
     HitInfo info;
     intersectClosest(s, ray, info);
     const C3 back(s.st.backColor[0], s.st.backColor[1], s.st.backColor[2]);
+    const C3 env = info.tri >= 0 ? C3() : sampleEnvironment(ray.d);  // rayrenderer.cpp:1292-1296
     if (s.st.shader != 5) {
       if (info.tri >= 0) {
         const C3 r = shadeSimple(info, ray, interp(s, info), nullptr, 0);
         return C3(fmaxf(r.x, 0.0f), fmaxf(r.y, 0.0f), fmaxf(r.z, 0.0f));
       }
-      return back;
+      return isZero(env) ? back : env;
     }
     const Medium* gm = s.globalMedium >= 0 ? &s.media[s.globalMedium] : nullptr;
     if (gm && gm->active()) {
@@ -1186,7 +1325,7 @@ struct Tracer {
       const C3 r = shade5(info, ray, interp(s, info), nullptr);
       return C3(fmaxf(r.x, 0.0f), fmaxf(r.y, 0.0f), fmaxf(r.z, 0.0f));
     }
-    return back;
+    return isZero(env) ? back : env;
   }
 };
 
@@ -1581,6 +1720,45 @@ static V3 viewDir(const ViewM& M, const float* p) {
   return l > 0.0f ? V3(o[0] / l, o[1] / l, o[2] / l) : V3(o[0], o[1], o[2]);
 }
 
+// Scene::buildEnvmapCDF, equirectangular part (scene.cpp:414-463): per-row
+// running sums of luminance x sin(theta) over raw texels (no sRGB decode),
+// each row normalised to a conditional CDF, a marginal CDF over the row sums,
+// sequential float sums in file order.
+static void buildEnvmapCDF(Scene& s) {
+  const Texture& T = s.textures[s.envTex];
+  const int W = T.w, H = T.h;
+  if (W <= 0 || H <= 0) return;
+  s.envW = W;
+  s.envH = H;
+  std::vector<float> rowWeight(H, 0.0f);
+  s.envCond.assign((size_t)H * (W + 1), 0.0f);
+  for (int y = 0; y < H; y++) {
+    const float v = (y + 0.5f) / (float)H;
+    const float sinTheta = sinf((float)M_PI * v);
+    float rowSum = 0.0f;
+    for (int x = 0; x < W; x++) {
+      const float* c = &T.rgba[((size_t)y * W + x) * 4];
+      const float lum = fmaxf(0.0f, 0.2126f * c[0] + 0.7152f * c[1] + 0.0722f * c[2]);
+      rowSum += lum * sinTheta;
+      s.envCond[(size_t)y * (W + 1) + (x + 1)] = rowSum;
+    }
+    rowWeight[y] = rowSum;
+  }
+  for (int y = 0; y < H; y++) {
+    if (rowWeight[y] > 0.0f) {
+      const float inv = 1.0f / rowWeight[y];
+      for (int x = 1; x <= W; x++) s.envCond[(size_t)y * (W + 1) + x] *= inv;
+    }
+  }
+  s.envMarg.assign(H + 1, 0.0f);
+  for (int y = 0; y < H; y++) s.envMarg[y + 1] = s.envMarg[y] + rowWeight[y];
+  s.envTotal = s.envMarg[H];
+  if (s.envTotal > 0.0f) {
+    const float inv = 1.0f / s.envTotal;
+    for (int y = 0; y <= H; y++) s.envMarg[y] *= inv;
+  }
+}
+
 static Scene* buildScene(const rg_scene_desc* d, int bins) {
   Scene* s = new Scene();
   const int nt = d->num_triangles;
@@ -1665,6 +1843,14 @@ static Scene* buildScene(const rg_scene_desc* d, int bins) {
     T.w = d->textures[i].width; T.h = d->textures[i].height; T.hdr = d->textures[i].is_hdr;
     T.rgba.assign(d->textures[i].rgba, d->textures[i].rgba + (size_t)T.w * T.h * 4);
     s->textures.push_back(std::move(T));
+  }
+  if (d->has_envmap && d->envmap_texture >= 0 && d->envmap_texture < d->num_textures) {
+    s->envTex = d->envmap_texture;
+    s->envIntensity = d->envmap_intensity;
+    const float yaw = d->envmap_rotation * (float)(M_PI / 180.0);
+    s->envCosY = cosf(yaw);
+    s->envSinY = sinf(yaw);
+    buildEnvmapCDF(*s);
   }
   buildBVH(*s, bins);
   return s;
@@ -1791,6 +1977,33 @@ float orc_phase_pdf(float g, float cosTheta) {
 void orc_sample_phase(float g, float u1, float u2, float* out3) {
   Medium m{}; m.g = g; const V3 d = m.samplePhase(V3(0, 0, 1), u1, u2);
   out3[0] = d.x; out3[1] = d.y; out3[2] = d.z;
+}
+
+// Environment-map probes for the tests: n view-space directions (n x 3).
+// radiance: n x 3 (sampleEnvironment); pdf: n (envmapDirectionPdf);
+// sample: u n x 2 -> dir n x 3 + pdf n (sampleEnvmapDirection).
+void orc_env_eval(void* sp, const float* dirs, int32_t n, float* out_rgb, float* out_pdf) {
+  const Scene& s = *static_cast<Scene*>(sp);
+  Ctx c{};
+  Tracer t(s, c);
+  for (int i = 0; i < n; i++) {
+    const V3 d(dirs[i * 3], dirs[i * 3 + 1], dirs[i * 3 + 2]);
+    const C3 L = t.sampleEnvironment(d);
+    out_rgb[i * 3] = L.x; out_rgb[i * 3 + 1] = L.y; out_rgb[i * 3 + 2] = L.z;
+    out_pdf[i] = t.envmapDirectionPdf(d);
+  }
+}
+void orc_env_sample(void* sp, const float* u, int32_t n, float* out_dir, float* out_pdf) {
+  const Scene& s = *static_cast<Scene*>(sp);
+  Ctx c{};
+  Tracer t(s, c);
+  for (int i = 0; i < n; i++) {
+    V3 d;
+    float pdf;
+    t.sampleEnvmapDirection(u[i * 2], u[i * 2 + 1], d, pdf);
+    out_dir[i * 3] = d.x; out_dir[i * 3 + 1] = d.y; out_dir[i * 3 + 2] = d.z;
+    out_pdf[i] = pdf;
+  }
 }
 
 }  // extern "C"

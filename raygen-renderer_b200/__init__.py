@@ -123,6 +123,8 @@ class rg_scene_desc(C.Structure):
         ("num_point_lights", C.c_int32), ("point_lights", C.POINTER(rg_point_light)),
         ("num_textures", C.c_int32), ("textures", C.POINTER(rg_texture)),
         ("camera", rg_camera),
+        ("has_envmap", C.c_int32), ("envmap_texture", C.c_int32),
+        ("envmap_intensity", C.c_float), ("envmap_rotation", C.c_float),
     ]
 
 
@@ -348,7 +350,10 @@ class Scene:
 
     @classmethod
     def from_arrays(cls, positions, normals, tri_mesh, mesh_object, objects, materials, camera,
-                    media=(), global_medium=-1, point_lights=(), uvs=None) -> "Scene":
+                    media=(), global_medium=-1, point_lights=(), uvs=None, textures=(),
+                    envmap=None, envmap_intensity=1.0, envmap_rotation=0.0) -> "Scene":
+        """Scene from arrays.  textures: sequence of (H x W x 4 float32 RGBA, is_hdr);
+        envmap: index of the equirectangular environment texture (None = no environment)."""
         pos = np.ascontiguousarray(positions, dtype=np.float32).reshape(-1, 9)
         nrm = np.ascontiguousarray(normals, dtype=np.float32).reshape(-1, 9)
         tm = np.ascontiguousarray(tri_mesh, dtype=np.int32)
@@ -378,7 +383,26 @@ class Scene:
         d.num_point_lights = len(point_lights)
         d.point_lights = pls
         d.camera = camera
-        keep = (pos, nrm, tm, mo, objs, mats, meds, pls, uv, d)
+        texs = []
+        if textures:
+            tarr = (rg_texture * len(textures))()
+            for i, (img, is_hdr) in enumerate(textures):
+                a = np.ascontiguousarray(img, dtype=np.float32)
+                if a.ndim != 3 or a.shape[2] != 4:
+                    raise ValueError("textures must be H x W x 4 RGBA arrays")
+                texs.append(a)
+                tarr[i].height, tarr[i].width = a.shape[0], a.shape[1]
+                tarr[i].is_hdr = int(bool(is_hdr))
+                tarr[i].rgba = _fptr(a)
+            d.num_textures = len(textures)
+            d.textures = tarr
+            texs.append(tarr)
+        if envmap is not None:
+            d.has_envmap = 1
+            d.envmap_texture = int(envmap)
+            d.envmap_intensity = float(envmap_intensity)
+            d.envmap_rotation = float(envmap_rotation)
+        keep = (pos, nrm, tm, mo, objs, mats, meds, pls, uv, d, texs)
         return cls(C.pointer(d), False, keep)
 
     def arrays(self):

@@ -140,7 +140,7 @@ struct rg_handle {
   int W = 0, H = 0;
   bool haveResult = false;
   // wavefront
-  DevBuf<float4> rayO0, rayO1, rayD0, rayD1, hits, pathT, pathR, pathL, shO0, shO1, shD0, shD1, shC0, shC1;
+  DevBuf<float4> rayO0, rayO1, rayD0, rayD1, hits, pathT, pathR, pathL, shO0, shO1, shO2, shD0, shD1, shD2, shC0, shC1, shC2;
   DevBuf<int2> pathPS;
   DevBuf<DevJob> jobsDev;
   DevBuf<DevSegment> segs;
@@ -174,6 +174,7 @@ rg_status ensureQueues(rg_handle* h, int capacity, int maxIter) {
   bool ok = h->rayO0.alloc(c) && h->rayO1.alloc(c) && h->rayD0.alloc(c) && h->rayD1.alloc(c) && h->hits.alloc(c) &&
             h->pathT.alloc(c) && h->pathR.alloc(c) && h->pathL.alloc(c) && h->shO0.alloc(c) && h->shO1.alloc(c) &&
             h->shD0.alloc(c) && h->shD1.alloc(c) && h->shC0.alloc(c) && h->shC1.alloc(c) && h->pathPS.alloc(c) &&
+            h->shO2.alloc(c) && h->shD2.alloc(c) && h->shC2.alloc(c) &&
             h->counters.alloc((size_t)(mi + 1) * kCountersPerIter) && h->error.alloc(1) && h->stats.alloc(8) &&
             h->curWave.alloc(1);
   if (!ok) {
@@ -197,9 +198,9 @@ DevQueues makeQueues(rg_handle* h, int maxIter) {
   Q.hits = h->hits.p;
   Q.pathT = h->pathT.p; Q.pathR = h->pathR.p; Q.pathL = h->pathL.p;
   Q.pathPS = h->pathPS.p;
-  Q.shO[0] = h->shO0.p; Q.shO[1] = h->shO1.p;
-  Q.shD[0] = h->shD0.p; Q.shD[1] = h->shD1.p;
-  Q.shC[0] = h->shC0.p; Q.shC[1] = h->shC1.p;
+  Q.shO[0] = h->shO0.p; Q.shO[1] = h->shO1.p; Q.shO[2] = h->shO2.p;
+  Q.shD[0] = h->shD0.p; Q.shD[1] = h->shD1.p; Q.shD[2] = h->shD2.p;
+  Q.shC[0] = h->shC0.p; Q.shC[1] = h->shC1.p; Q.shC[2] = h->shC2.p;
   Q.counters = h->counters.p;
   Q.stats = h->stats.p;
   Q.error = h->error.p;
@@ -276,6 +277,7 @@ void enqueueWave(rg_handle* h, const DevRender& R, const DevQueues& Q, const Dev
       if (profile) cudaEventRecord((*ev)[it * 4 + 2], st);
       launchConnect(&h->dscene, jobs, width, Q, it, 0, g.conn, st);
       if (h->dscene.numPointLights > 0) launchConnect(&h->dscene, jobs, width, Q, it, 1, g.conn, st);
+      if (h->dscene.envTex >= 0) launchConnect(&h->dscene, jobs, width, Q, it, 2, g.conn, st);
       if (profile) cudaEventRecord((*ev)[it * 4 + 3], st);
     }
   }
@@ -399,6 +401,45 @@ rg_status rg_cancel(rg_handle* h) {
 
 namespace rg {
 
+// Importance-sampling CDFs of an equirectangular map, Scene::buildEnvmapCDF
+// (scene.cpp:414-463): per row, running sums of luminance x sin(theta) over
+// the raw texels, normalised to a conditional CDF; a marginal CDF over the
+// row sums.  Sequential float sums in texel order, as the reference.  A
+// W x H map is a few hundred microseconds of host work at scene set-up.
+// Returns false (no sampling) for an empty image.
+bool buildEnvmapCdf(const rg_texture& T, std::vector<float>& marg, std::vector<float>& cond, float& total) {
+  const int W = T.width, H = T.height;
+  total = 0.0f;
+  if (W <= 0 || H <= 0) return false;
+  std::vector<float> rowWeight(H, 0.0f);
+  cond.assign((size_t)H * (W + 1), 0.0f);
+  for (int y = 0; y < H; y++) {
+    const float v = (y + 0.5f) / (float)H;
+    const float sinTheta = sinf((float)M_PI * v);
+    float rowSum = 0.0f;
+    for (int x = 0; x < W; x++) {
+      const float* c = T.rgba + ((size_t)y * W + x) * 4;
+      const float lum = fmaxf(0.0f, 0.2126f * c[0] + 0.7152f * c[1] + 0.0722f * c[2]);
+      rowSum += lum * sinTheta;
+      cond[(size_t)y * (W + 1) + (x + 1)] = rowSum;
+    }
+    rowWeight[y] = rowSum;
+  }
+  for (int y = 0; y < H; y++)
+    if (rowWeight[y] > 0.0f) {
+      const float inv = 1.0f / rowWeight[y];
+      for (int x = 1; x <= W; x++) cond[(size_t)y * (W + 1) + x] *= inv;
+    }
+  marg.assign(H + 1, 0.0f);
+  for (int y = 0; y < H; y++) marg[y + 1] = marg[y] + rowWeight[y];
+  total = marg[H];
+  if (total > 0.0f) {
+    const float inv = 1.0f / total;
+    for (int y = 0; y <= H; y++) marg[y] *= inv;
+  }
+  return true;
+}
+
 // Validates a scene description, uploads it, builds its BVH and fills the
 // device-side table of pointers.  Used by rg_set_scene and the job server.
 rg_status prepareScene(const rg_scene_desc* d, int bins, bool wide, cudaStream_t st, int* errWord,
@@ -440,6 +481,16 @@ rg_status prepareScene(const rg_scene_desc* d, int bins, bool wide, cudaStream_t
     }
   if (d->global_medium >= d->num_media || d->num_media > 1000) {
     setLastError("global medium index out of range");
+    return RG_ERR_INVALID_ARGUMENT;
+  }
+  for (int i = 0; i < d->num_textures; i++)
+    if (d->textures[i].width < 0 || d->textures[i].height < 0 ||
+        (d->textures[i].width > 0 && d->textures[i].height > 0 && !d->textures[i].rgba)) {
+      setLastError("texture without texels");
+      return RG_ERR_INVALID_ARGUMENT;
+    }
+  if (d->has_envmap && (d->envmap_texture < 0 || d->envmap_texture >= d->num_textures)) {
+    setLastError("envmap texture index out of range");
     return RG_ERR_INVALID_ARGUMENT;
   }
   out.reset(new DeviceScene());
@@ -524,6 +575,22 @@ rg_status prepareScene(const rg_scene_desc* d, int bins, bool wide, cudaStream_t
     texs[i] = DevTexture{buf->p, t.width, t.height, t.is_hdr, 0};
   }
   if (ok) ok = ds.textures.upload(texs.data(), texs.size(), st);
+  if (ok && d->has_envmap) {
+    const rg_texture& T = d->textures[d->envmap_texture];
+    std::vector<float> marg, cond;
+    ds.envTex = d->envmap_texture;
+    ds.envIntensity = d->envmap_intensity;
+    const float yaw = d->envmap_rotation * (float)(M_PI / 180.0);
+    ds.envCosY = cosf(yaw);
+    ds.envSinY = sinf(yaw);
+    if (buildEnvmapCdf(T, marg, cond, ds.envTotal)) {
+      ds.envW = T.width;
+      ds.envH = T.height;
+      ok = ds.envMarg.upload(marg.data(), marg.size(), st) && ds.envCond.upload(cond.data(), cond.size(), st);
+      // the host vectors go out of scope: finish the copies first
+      if (ok) ok = cudaStreamSynchronize(st) == cudaSuccess;
+    }
+  }
   if (!ok) {
     setLastError("scene upload failed (device memory)");
     out.reset();
@@ -585,6 +652,15 @@ rg_status prepareScene(const rg_scene_desc* d, int bins, bool wide, cudaStream_t
   S.nodes8 = ds.nodes8.p;
   S.numNodes8 = ds.numNodes8;
   S.bvhWidth = ds.bvhWidth;
+  S.envTex = ds.envTex;
+  S.envW = ds.envW;
+  S.envH = ds.envH;
+  S.envIntensity = ds.envIntensity;
+  S.envCosY = ds.envCosY;
+  S.envSinY = ds.envSinY;
+  S.envTotal = ds.envTotal;
+  S.envMarg = ds.envMarg.p;
+  S.envCond = ds.envCond.p;
   return RG_OK;
 }
 

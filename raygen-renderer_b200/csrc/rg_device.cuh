@@ -84,6 +84,12 @@ struct DevScene {
   const float4* nodes8;       // 5 float4 per 8-wide compressed node (when bvhWidth == 8)
   int numNodes8;
   int bvhWidth;               // 2 or 8
+  // equirectangular environment map, looked up by view-space direction
+  int envTex;                 // texture index, -1 none
+  int envW, envH;             // importance-sampling grid (the texture size); 0 when not sampled
+  float envIntensity, envCosY, envSinY, envTotal;
+  const float* envMarg;       // H+1 marginal CDF over rows
+  const float* envCond;       // H x (W+1) conditional CDFs
 };
 
 // device error codes
@@ -158,9 +164,9 @@ struct DevQueues {
   float4* pathR;              // (rrT rgb, flags bits)
   float4* pathL;              // (L rgb, vertex bits)
   int2* pathPS;               // (pixel, sample) of every path
-  float4* shO[2];             // shadow queues A (area) / B (point): (origin, path id bits)
-  float4* shD[2];             // (dir, tmax)
-  float4* shC[2];             // (contribution rgb, job slot bits)
+  float4* shO[3];             // shadow queues A (area) / B (point) / C (environment): (origin, path id bits)
+  float4* shD[3];             // (dir, tmax)
+  float4* shC[3];             // (contribution rgb, job slot bits)
   int* counters;              // per-iteration counters, zeroed by the generate kernel
   unsigned long long* stats;  // [0] nodes closest [1] tris closest [2] nodes shadow [3] tris shadow [4] closest rays [5] shadow rays
   int* error;                 // first device error code
@@ -168,9 +174,17 @@ struct DevQueues {
   int maxIter;
 };
 
-// counters layout: [k*8 + c] for iteration k
-enum CounterSlot { C_RAYS = 0, C_FETCH_EXT = 1, C_SHA = 2, C_SHB = 3, C_FETCH_SHA = 4, C_FETCH_SHB = 5, C_FETCH_SHADE = 6 };
-constexpr int kCountersPerIter = 8;
+// counters layout: [k*kCountersPerIter + c] for iteration k
+enum CounterSlot {
+  C_RAYS = 0, C_FETCH_EXT = 1, C_SHA = 2, C_SHB = 3, C_FETCH_SHA = 4, C_FETCH_SHB = 5, C_FETCH_SHADE = 6,
+  C_SHC = 7, C_FETCH_SHC = 8
+};
+constexpr int kCountersPerIter = 12;
+// shadow queue `which` (0 area, 1 point, 2 environment) -> its counter slots
+__host__ __device__ inline int shadowCountSlot(int which) { return which == 0 ? C_SHA : (which == 1 ? C_SHB : C_SHC); }
+__host__ __device__ inline int shadowFetchSlot(int which) {
+  return which == 0 ? C_FETCH_SHA : (which == 1 ? C_FETCH_SHB : C_FETCH_SHC);
+}
 
 // path flags (pathR.w)
 constexpr uint32_t F_PASSES_MASK = 0xFFu;

@@ -82,12 +82,19 @@ struct SceneStore {
   std::vector<TextureStore> textures;
   std::vector<rg_texture> textureDescs;
   rg_camera camera{};
+  int32_t envmapTexture = -1;  // index into textures, -1 none
+  float envmapIntensity = 1.0f, envmapRotation = 0.0f;
   rg_scene_desc desc{};
   void finalize();
 };
 
 rg_status buildBuiltinScene(int kind, uint32_t seed, const int32_t* ip, int nip, SceneStore** out);
 rg_status loadSceneJson(const char* path, SceneStore** out, std::string& err);
+
+// Image files (rg_image.cpp): RGBA float, row 0 at the top.
+bool readRadianceHdr(const std::string& path, TextureStore& out, std::string& err);
+bool readPfm(const std::string& path, TextureStore& out, std::string& err);
+bool readImageFile(const std::string& path, TextureStore& out, std::string& err);
 
 // Device-resident scene (BVH + triangle and light tables).
 struct DeviceScene {
@@ -111,6 +118,10 @@ struct DeviceScene {
   DevBuf<DevTexture> textures;
   std::vector<DevBuf<float4>*> texels;
   int numTextures = 0;
+  // equirectangular environment map: texture index and importance-sampling CDFs
+  int envTex = -1, envW = 0, envH = 0;
+  float envIntensity = 1.0f, envCosY = 1.0f, envSinY = 0.0f, envTotal = 0.0f;
+  DevBuf<float> envMarg, envCond;
   // BVH + leaf-order triangles
   DevBuf<float4> nodes, nodes8, triVerts, triShade;
   int numNodes8 = 0;

@@ -6,8 +6,8 @@
 //  * JSONC: '//' and '/* */' comments, trailing commas and bare identifier
 //    keys tolerated; containers still open at the end of input are closed
 //    there (one sample scene lacks its final brace).
-//  * Root keys: mainCamera, _materials, envmap (parsed; environment lighting
-//    is not rendered yet), medium (global), and child objects.
+//  * Root keys: mainCamera, _materials, envmap (equirectangular Radiance
+//    .hdr / .pfm), medium (global), and child objects.
 //  * Object keys: location, angle (degrees), scale, mesh (path | [paths] |
 //    {type: plane|cube|sphere|cone, ...}), mat (name | object), visible,
 //    medium (interior), children.  Keys are applied in file order.  Objects
@@ -866,7 +866,7 @@ struct Loader {
           else n.medium = (int)st.media.size() - 1;
         }
       } else if (k == "envmap") {
-        // environment maps are parsed but not yet rendered
+        if (!readEnvmap(v)) return false;
       } else if (v.type == JVal::Obj) {
         std::unique_ptr<Node> c(new Node());
         c->mat = defaultMat();
@@ -881,6 +881,49 @@ struct Loader {
       }
     }
     scopes.pop_back();
+    return true;
+  }
+
+  // "envmap": a path, or {texture, intensity, rotation, cubemap, ext}
+  // (sceneloader.cpp:700-748); the last one read wins.  As in the reference,
+  // an image that cannot be opened leaves the scene without an environment
+  // (Texture::loadFromFile yields an empty image, which samples black).  A
+  // malformed file or a cubemap (six JPEG faces, no decoder here) is an error.
+  bool readEnvmap(const JVal& v) {
+    std::string rel;
+    float intensity = 1.0f, rotation = 0.0f;
+    if (v.type == JVal::Str) {
+      rel = v.s;
+    } else if (v.type == JVal::Obj) {
+      if (const JVal* c = v.get("cubemap"))
+        if (c->type == JVal::Str && !c->s.empty()) {
+          err = "cubemap environment maps are not read (their faces are JPEG images): " + c->s;
+          code = RG_ERR_UNSUPPORTED;
+          return false;
+        }
+      if (const JVal* t = v.get("texture"))
+        if (t->type == JVal::Str) rel = t->s;
+      v.num("intensity", intensity);
+      v.num("rotation", rotation);
+    }
+    st.envmapIntensity = intensity;
+    st.envmapRotation = rotation;
+    if (rel.empty()) return true;
+    const std::string path = rel[0] == '/' ? rel : baseDir + rel;
+    {
+      std::ifstream probe(path, std::ios::binary);
+      if (!probe) {
+        st.envmapTexture = -1;
+        return true;
+      }
+    }
+    TextureStore tex;
+    if (!readImageFile(path, tex, err)) {
+      code = RG_ERR_PARSE;
+      return false;
+    }
+    st.textures.push_back(std::move(tex));
+    st.envmapTexture = (int)st.textures.size() - 1;
     return true;
   }
 

@@ -418,6 +418,10 @@ void SceneStore::finalize() {
   desc.num_textures = (int32_t)textureDescs.size();
   desc.textures = textureDescs.data();
   desc.camera = camera;
+  desc.has_envmap = envmapTexture >= 0 ? 1 : 0;
+  desc.envmap_texture = envmapTexture;
+  desc.envmap_intensity = envmapIntensity;
+  desc.envmap_rotation = envmapRotation;
 }
 
 rg_status buildBuiltinScene(int kind, uint32_t seed, const int32_t* ip, int nip, SceneStore** out) {

@@ -259,6 +259,130 @@ __device__ bool sampleAreaLightForNEE(const DevScene& S, const DevRender& R, con
   return true;
 }
 
+// ---- equirectangular environment map ----------------------------------------
+// Directions are view space, as in the reference (the map turns with the
+// camera).  Lookups go through Texture::sample; the importance-sampling grid
+// and its CDFs (Scene::buildEnvmapCDF) are built at scene set-up.  These are
+// kept out of line (only scenes with an environment map reach them) and read
+// the scene through its copy in the job table (global memory), with scalar
+// arguments and by-value results, so the shade kernel keeps no local frame.
+constexpr float kInv2Pi = (float)(0.5 / 3.14159265358979323846);
+constexpr float kInvPi = (float)(1.0 / 3.14159265358979323846);
+constexpr float kPi2 = (float)(3.14159265358979323846 * 3.14159265358979323846);
+
+__device__ __forceinline__ bool envSampling(const DevScene* S) {
+  return S->envTex >= 0 && S->envW > 0 && S->envTotal > 0.0f;
+}
+
+__device__ __forceinline__ float envTexelLum(const DevScene* S, int x, int y) {
+  const float4 c = __ldg(S->textures[S->envTex].texels + (size_t)y * S->envW + x);
+  return fmaxf(0.0f, 0.2126f * c.x + 0.7152f * c.y + 0.0722f * c.z);
+}
+
+// sampleEnvironment, equirectangular branch (rayrenderer.cpp:1299-1348)
+__device__ __noinline__ V3 envRadiance(const DevScene* S, V3 dir) {
+  if (S->envTex < 0) return v3(0, 0, 0);
+  const V3 d = normalize(dir);
+  const float rx = d.x * S->envCosY - d.z * S->envSinY;
+  const float rz = d.x * S->envSinY + d.z * S->envCosY;
+  const float u = 0.5f + atan2f(rz, rx) * kInv2Pi;
+  const float v = 0.5f - asinf(fminf(fmaxf(d.y, -1.0f), 1.0f)) * kInvPi;
+  return texSample(*S, S->envTex, u, v) * S->envIntensity;
+}
+
+// envmapDirectionPdf, equirectangular branch (rayrenderer.cpp:1521-1573)
+__device__ __noinline__ float envPdf(const DevScene* S, V3 dir) {
+  if (!envSampling(S)) return 0.0f;
+  const V3 d = normalize(dir);
+  const float rx = d.x * S->envCosY - d.z * S->envSinY;
+  const float rz = d.x * S->envSinY + d.z * S->envCosY;
+  const int W = S->envW, H = S->envH;
+  const float u = 0.5f + atan2f(rz, rx) * kInv2Pi;
+  const float v = 0.5f - asinf(fminf(fmaxf(d.y, -1.0f), 1.0f)) * kInvPi;
+  const int x = min(max((int)(u * W), 0), W - 1);
+  const int y = min(max((int)(v * H), 0), H - 1);
+  const float lum = envTexelLum(S, x, y);
+  const float sinTheta = sinf(kPi * v);
+  if (sinTheta <= 0.0f) return 0.0f;
+  const float pdfUV = (lum * sinTheta) / S->envTotal;
+  return pdfUV * (float)(W * H) / (2.0f * kPi2 * sinTheta);
+}
+
+// searchCDF (rayrenderer.cpp:1353-1362): largest i with cdf[i] <= u, in [0, n-1]
+__device__ __forceinline__ int searchCDF(const float* __restrict__ cdf, int n, float u) {
+  int lo = 0, hi = n;
+  while (lo < hi) {
+    const int mid = (lo + hi) >> 1;
+    if (__ldg(cdf + mid + 1) <= u) lo = mid + 1;
+    else hi = mid;
+  }
+  return lo < n ? lo : n - 1;
+}
+
+struct EnvSample {
+  V3 dir;
+  float pdf;  // 0: no sample
+  V3 Li;
+};
+
+// sampleEnvmapDirection, equirectangular branch (rayrenderer.cpp:1426-1482),
+// plus the radiance toward the sample (the NEE part of sampleEnvmapForNEE,
+// rayrenderer.cpp:2038-2065, before its front-facing and shadow tests).
+__device__ __noinline__ EnvSample envSample(const DevScene* S, float u0, float u1) {
+  EnvSample r;
+  r.dir = v3(0, 1, 0);
+  r.pdf = 0.0f;
+  r.Li = v3(0, 0, 0);
+  if (!envSampling(S)) return r;
+  const int W = S->envW, H = S->envH;
+  const int y = searchCDF(S->envMarg, H, u0);
+  const float* row = S->envCond + (size_t)y * (W + 1);
+  const int x = searchCDF(row, W, u1);
+  const float yPrev = __ldg(S->envMarg + y), ySpan = __ldg(S->envMarg + y + 1) - yPrev;
+  const float xPrev = __ldg(row + x), xSpan = __ldg(row + x + 1) - xPrev;
+  const float yFrac = ySpan > 0.0f ? (u0 - yPrev) / ySpan : 0.5f;
+  const float xFrac = xSpan > 0.0f ? (u1 - xPrev) / xSpan : 0.5f;
+  const float u = (x + xFrac) / (float)W;
+  const float v = (y + yFrac) / (float)H;
+  const float phi = (u - 0.5f) * 2.0f * kPi;
+  const float theta = (0.5f - v) * kPi;
+  const float cosT = cosf(theta);
+  const float dx = cosT * cosf(phi), dy = sinf(theta), dz = cosT * sinf(phi);
+  r.dir = normalize(v3(dx * S->envCosY + dz * S->envSinY, dy, -dx * S->envSinY + dz * S->envCosY));
+  const float lum = envTexelLum(S, x, y);
+  const float sinTheta = sinf(kPi * v);
+  if (sinTheta <= 0.0f) return r;
+  const float pdfUV = (lum * sinTheta) / S->envTotal;
+  r.pdf = pdfUV * (float)(W * H) / (2.0f * kPi2 * sinTheta);
+  if (r.pdf > 0.0f) r.Li = envRadiance(S, r.dir);
+  return r;
+}
+
+// sampleEnvmapForNEE (rayrenderer.cpp:2038-2065) up to the shadow test: an
+// unbounded shadow ray (tmax 1e30) with the point/env occluders, queue C.
+__device__ __forceinline__ bool envNEE(const DevScene* S, const Rng& rng, int v, V3 hit, V3 n, EnvSample& e,
+                                       Shadow& sh) {
+  if (!envSampling(S)) return false;
+  e = envSample(S, rng.prng(v, S_ENV0), rng.prng(v, S_ENV1));
+  if (e.pdf <= 0.0f || dot(e.dir, n) <= 0.0f) return false;
+  sh.o = surfaceOrigin(hit, e.dir, n);
+  sh.d = e.dir;
+  sh.tmax = 1e30f;
+  return true;
+}
+
+// Radiance of a ray that left the scene, with the BSDF-side MIS weight against
+// environment NEE when the last bounce advertised a pdf (rayrenderer.cpp:1619-1630).
+__device__ __noinline__ V3 envMiss(const DevScene* S, V3 d, float bsdfPdf) {
+  V3 env = envRadiance(S, d);
+  if (bsdfPdf > 0.0f) {
+    const float e = envPdf(S, d);
+    const float b2 = bsdfPdf * bsdfPdf, e2 = e * e;
+    env = env * ((b2 + e2 > 0.0f) ? b2 / (b2 + e2) : 1.0f);
+  }
+  return env;
+}
+
 // ------------------------------------------------------------ kernels ----
 // Segment of the wave holding path p (segments are few; linear scan after a
 // binary search on the path prefix).
@@ -383,12 +507,12 @@ __global__ void __launch_bounds__(128) k_extend(const DevJob* __restrict__ jobs,
 
 // Shadow-ray visibility; unoccluded contributions are added to the path.
 __global__ void __launch_bounds__(128) k_connect(const DevJob* __restrict__ jobs, DevQueues Q, int iter, int which) {
-  const int count = Q.counters[iter * kCountersPerIter + (which ? C_SHB : C_SHA)];
-  int* fetch = &Q.counters[iter * kCountersPerIter + (which ? C_FETCH_SHB : C_FETCH_SHA)];
+  const int count = Q.counters[iter * kCountersPerIter + shadowCountSlot(which)];
+  int* fetch = &Q.counters[iter * kCountersPerIter + shadowFetchSlot(which)];
   const float4* __restrict__ sO = Q.shO[which];
   const float4* __restrict__ sD = Q.shD[which];
   const float4* __restrict__ sC = Q.shC[which];
-  const uint32_t occ = which ? kOccPoint : kOccArea;
+  const uint32_t occ = which ? kOccPoint : kOccArea;  // point lights and the environment share one class
   const int lane = threadIdx.x & 31;
   uint32_t nodes = 0, tris = 0, rays = 0;
   for (;;) {
@@ -614,9 +738,9 @@ __global__ void __launch_bounds__(128) k_extend8(DevScene S0, const DevJob* __re
 template <bool MULTI>
 __global__ void __launch_bounds__(128) k_connect8(DevScene S0, const DevJob* __restrict__ jobs, DevQueues Q, int iter,
                                                   int which) {
-  const int count = Q.counters[iter * kCountersPerIter + (which ? C_SHB : C_SHA)];
+  const int count = Q.counters[iter * kCountersPerIter + shadowCountSlot(which)];
   uint32_t nodes = 0, tris = 0, rays = 0;
-  traverseWave8<true, MULTI>(S0, jobs, count, &Q.counters[iter * kCountersPerIter + (which ? C_FETCH_SHB : C_FETCH_SHA)],
+  traverseWave8<true, MULTI>(S0, jobs, count, &Q.counters[iter * kCountersPerIter + shadowFetchSlot(which)],
                       Q.shO[which], Q.shD[which], which ? kOccPoint : kOccArea, nullptr, Q.shC[which], Q.pathL, nodes,
                       tris, rays);
   warpAddStat(&Q.stats[2], nodes);
@@ -627,7 +751,9 @@ __global__ void __launch_bounds__(128) k_connect8(DevScene S0, const DevJob* __r
 // One path vertex (RayBSDFShaderProvider::shade + lobes + tracePath's medium branch).
 // MULTI = false: one job whose scene and render constants come in as kernel
 // parameters (constant bank); MULTI = true: per-ray job slot into the table.
-template <bool MULTI>
+// ENV = false drops the environment-map code (misses, environment NEE) for
+// scenes without one, so they keep the smaller kernel.
+template <bool MULTI, bool ENV>
 __global__ void __launch_bounds__(256) k_shade(DevScene S0, DevRender R0, const DevJob* __restrict__ jobs, DevQueues Q,
                                                int iter) {
   const int count = Q.counters[iter * kCountersPerIter + C_RAYS];
@@ -636,9 +762,10 @@ __global__ void __launch_bounds__(256) k_shade(DevScene S0, DevRender R0, const 
   const int rounded = ((count + 31) / 32) * 32;
   for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < rounded; q += stride) {
     const bool valid = q < count;
-    Shadow shA, shB;
+    Shadow shA, shB, shE;  // area light / point light / environment
     shA.on = false;
     shB.on = false;
+    shE.on = false;
     bool cont = false;
     V3 no = v3(0, 0, 0), nd = v3(0, 0, 0);
     int pid = 0, slot = 0;
@@ -695,13 +822,22 @@ __global__ void __launch_bounds__(256) k_shade(DevScene S0, DevRender R0, const 
             const V3 proxy = -d;
             V3 lDir, Le;
             float pl;
-            if (sampleAreaLightForNEE(S, R, rng, v, pos, proxy, lDir, pl, Le, shA) && pl > 0.0f) {
+            auto phaseTo = [&](V3 w) {  // HG phasePdf (medium.cpp:519-525)
               const float g = M.g;
-              const float cosT = dot(-d, lDir);
+              const float cosT = dot(-d, w);
               const float den = 1.0f + g * g - 2.0f * g * cosT;
-              const float phase = (1.0f - g * g) * (1.0f / (4.0f * kPi)) / (den * sqrtf(fmaxf(1e-8f, den)));
+              return (1.0f - g * g) * (1.0f / (4.0f * kPi)) / (den * sqrtf(fmaxf(1e-8f, den)));
+            };
+            if (sampleAreaLightForNEE(S, R, rng, v, pos, proxy, lDir, pl, Le, shA) && pl > 0.0f) {
               shA.on = true;
-              shA.c = beta * sw * Le * (phase / pl);
+              shA.c = beta * sw * Le * (phaseTo(lDir) / pl);
+            }
+            if (ENV && S.envTex >= 0) {  // environment NEE at the scatter point (rayrenderer.cpp:1757-1761)
+              EnvSample e;
+              if (envNEE(&jobs[slot].S, rng, v, pos, proxy, e, shE)) {
+                shE.on = true;
+                shE.c = beta * sw * e.Li * (phaseTo(e.dir) / e.pdf);
+              }
             }
             // samplePhase: medium.cpp:496-517
             const float u1 = rng.prng(v, S_PHASE0), u2 = rng.prng(v, S_PHASE1);
@@ -746,11 +882,16 @@ __global__ void __launch_bounds__(256) k_shade(DevScene S0, DevRender R0, const 
           const float surv = expf(-M.hero * maxT);
           if (surv > 0.0f)
             beta = beta * v3(expf(-M.str * maxT) / surv, expf(-M.stg * maxT) / surv, expf(-M.stb * maxT) / surv);
-          if (prim < 0) done = true;
+          if (prim < 0) {
+            if (ENV && S.envTex >= 0) L = L + beta * envMiss(&jobs[slot].S, d, bsdfPdf);  // rayrenderer.cpp:1852-1863
+            done = true;
+          }
           silhouette = true;
         }
       } else if (prim < 0) {
-        done = true;  // environment miss: no environment map
+        // environment miss (rayrenderer.cpp:1619-1630; the eye ray has no pdf, so no weight)
+        if (ENV && S.envTex >= 0) L = L + beta * envMiss(&jobs[slot].S, d, bsdfPdf);
+        done = true;
       }
       // ---- surface vertex (RayBSDFShaderProvider::shade, rayrenderer.cpp:2776-2896)
       if (!done && !cont) {
@@ -855,6 +996,15 @@ __global__ void __launch_bounds__(256) k_shade(DevScene S0, DevRender R0, const 
             const V3 dir = cosineWeightedDirection(h.n, rng.lds(d0), rng.lds(d0 + 1));
             traceLight(S, R, rng, v, h.p, h.n, beta * albedo, shA, shB);
             bsdfPdf = fmaxf(0.0f, dot(dir, h.n)) * (1.0f / kPi);
+            if (ENV && S.envTex >= 0) {  // traceEnvmapLight (rayrenderer.cpp:1484-1519)
+              EnvSample e;
+              if (envNEE(&jobs[slot].S, rng, v, h.p, h.n, e, shE)) {
+                // the MIS partner is this vertex's own sampled-direction pdf, as passed at bsdf.cpp:86-88
+                const float w = bsdfPdf > 0.0f ? e.pdf * e.pdf / (e.pdf * e.pdf + bsdfPdf * bsdfPdf) : 1.0f;
+                shE.on = true;
+                shE.c = beta * albedo * e.Li * (dot(e.dir, h.n) * w / (kPi * e.pdf));
+              }
+            }
             beta = beta * albedo;
             rrT = rrT * albedo;
             cont = true;
@@ -906,28 +1056,36 @@ __global__ void __launch_bounds__(256) k_shade(DevScene S0, DevRender R0, const 
                   return 1.0f / (1.0f + lambda);
                 };
                 const float G1v = smithG1(Vl);
+                // evalGlossy (bsdf.cpp:260-280): f*cos_L and the VNDF pdf toward dw
+                auto evalGlossy = [&](V3 dw, V3& fCos, float& pb) {
+                  const V3 Ll = v3(dot(dw, t), dot(dw, b), dot(dw, h.n));
+                  if (Ll.z <= 0.0f) return false;
+                  V3 Hl = Vl + Ll;
+                  const float hl2 = dot(Hl, Hl);
+                  if (hl2 <= 0.0f) return false;
+                  Hl = Hl * (1.0f / sqrtf(hl2));
+                  const float VdotH = fmaxf(0.0f, dot(Vl, Hl));
+                  if (Hl.z <= 0.0f || VdotH <= 0.0f) return false;
+                  const float hx = Hl.x / ax, hy = Hl.y / ay;
+                  const float den = hx * hx + hy * hy + Hl.z * Hl.z;
+                  const float D = 1.0f / (kPi * ax * ay * den * den);
+                  fCos = schlick(VdotH) * (D * G1v * smithG1(Ll) / (4.0f * Vl.z));
+                  pb = G1v * D / (4.0f * Vl.z);
+                  return true;
+                };
                 // area-light NEE with MIS (bsdf.cpp:271-284)
-                V3 lDir, Le;
-                float pl;
-                if (sampleAreaLightForNEE(S, R, rng, v, h.p, h.n, lDir, pl, Le, shA)) {
-                  const V3 Ll = v3(dot(lDir, t), dot(lDir, b), dot(lDir, h.n));
-                  if (Ll.z > 0.0f) {
-                    V3 Hl = Vl + Ll;
-                    const float hl2 = dot(Hl, Hl);
-                    if (hl2 > 0.0f) {
-                      Hl = Hl * (1.0f / sqrtf(hl2));
-                      const float VdotH = fmaxf(0.0f, dot(Vl, Hl));
-                      if (Hl.z > 0.0f && VdotH > 0.0f) {
-                        const float hx = Hl.x / ax, hy = Hl.y / ay;
-                        const float den = hx * hx + hy * hy + Hl.z * Hl.z;
-                        const float D = 1.0f / (kPi * ax * ay * den * den);
-                        const V3 fCos = schlick(VdotH) * (D * G1v * smithG1(Ll) / (4.0f * Vl.z));
-                        const float pb = G1v * D / (4.0f * Vl.z);
-                        const float wl = pl * pl / (pl * pl + pb * pb);
-                        shA.on = true;
-                        shA.c = beta * Le * fCos * (wl / pl);
-                      }
-                    }
+                V3 lDir, Le, fCos;
+                float pl, pb;
+                if (sampleAreaLightForNEE(S, R, rng, v, h.p, h.n, lDir, pl, Le, shA) && evalGlossy(lDir, fCos, pb)) {
+                  shA.on = true;
+                  shA.c = beta * Le * fCos * (pl * pl / (pl * pl + pb * pb) / pl);
+                }
+                // environment NEE with MIS (bsdf.cpp:302-314)
+                if (ENV && S.envTex >= 0) {
+                  EnvSample e;
+                  if (envNEE(&jobs[slot].S, rng, v, h.p, h.n, e, shE) && evalGlossy(e.dir, fCos, pb)) {
+                    shE.on = true;
+                    shE.c = beta * e.Li * fCos * (e.pdf * e.pdf / (e.pdf * e.pdf + pb * pb) / e.pdf);
                   }
                 }
                 // VNDF sample (bsdf.cpp:139-161, 319-373)
@@ -1055,6 +1213,14 @@ __global__ void __launch_bounds__(256) k_shade(DevScene S0, DevRender R0, const 
       Q.shD[1][sb] = make_float4(shB.d.x, shB.d.y, shB.d.z, shB.tmax);
       Q.shC[1][sb] = make_float4(shB.c.x, shB.c.y, shB.c.z, __int_as_float(slot));
     }
+    if (ENV) {
+      const int se = warpPush(&Q.counters[iter * kCountersPerIter + C_SHC], shE.on);
+      if (se >= 0) {
+        Q.shO[2][se] = make_float4(shE.o.x, shE.o.y, shE.o.z, __int_as_float(pid));
+        Q.shD[2][se] = make_float4(shE.d.x, shE.d.y, shE.d.z, shE.tmax);
+        Q.shC[2][se] = make_float4(shE.c.x, shE.c.y, shE.c.z, __int_as_float(slot));
+      }
+    }
   }
 }
 
@@ -1111,7 +1277,11 @@ __global__ void __launch_bounds__(128) k_simple(const DevJob* __restrict__ jobs,
     bool eyeHit = false;
     for (int depth = 0, v = 0; depth < R.maxDepth; depth++, v++) {
       const ClosestHit ch = traceClosest(S, o, d, nodes, tris);
-      if (ch.prim < 0) break;
+      if (ch.prim < 0) {
+        // traceEyeRay's miss and tracePath's miss without BSDF parameters (rayrenderer.cpp:1292, 1619)
+        if (S.envTex >= 0) total = total + w * envRadiance(&S, d);
+        break;
+      }
       if (depth == 0) eyeHit = true;
       const Hit h = loadHit(S, ch.prim, o, d, ch.t, ch.u, ch.v);
       const DevMaterial m = S.mats[S.objMat[S.meshObj[h.mesh]]];
@@ -1270,8 +1440,9 @@ void launchExtend(const DevScene* single, const DevJob* jobs, int width, const D
 }
 void launchShade(const DevScene* single, const DevRender* singleR, const DevJob* jobs, const DevQueues& Q, int iter,
                  int grid, cudaStream_t st) {
-  if (single) k_shade<false><<<grid, 256, 0, st>>>(*single, *singleR, jobs, Q, iter);
-  else k_shade<true><<<grid, 256, 0, st>>>(DevScene{}, DevRender{}, jobs, Q, iter);
+  if (single && single->envTex < 0) k_shade<false, false><<<grid, 256, 0, st>>>(*single, *singleR, jobs, Q, iter);
+  else if (single) k_shade<false, true><<<grid, 256, 0, st>>>(*single, *singleR, jobs, Q, iter);
+  else k_shade<true, true><<<grid, 256, 0, st>>>(DevScene{}, DevRender{}, jobs, Q, iter);
 }
 void launchConnect(const DevScene* single, const DevJob* jobs, int width, const DevQueues& Q, int iter, int which,
                    int grid, cudaStream_t st) {

@@ -139,3 +139,85 @@ JSON_ROOM = """
   },
 }
 """
+
+
+# ---------------------------------------------------------------- image files
+def rgbe_encode(img):
+    """H x W x 3 float -> H x W x 4 uint8 RGBE (mantissa scaled by frexp)."""
+    img = np.asarray(img, np.float64)
+    m = img.max(axis=2)
+    mant, e = np.frexp(m)
+    ok = m > 1e-32
+    scale = np.where(ok, mant * 256.0 / np.where(ok, m, 1.0), 0.0)
+    rgb = np.floor(img * scale[..., None]).clip(0, 255)
+    E = np.where(ok, e + 128, 0)
+    return np.concatenate([rgb, E[..., None]], axis=2).astype(np.uint8)
+
+
+def rgbe_decode(q):
+    """Radiance decoding: channel * 2^(E - 136), black when E == 0."""
+    q = np.asarray(q)
+    sc = np.where(q[..., 3] == 0, 0.0, np.ldexp(1.0, q[..., 3].astype(np.int32) - 136))
+    return (q[..., :3] * sc[..., None]).astype(np.float32)
+
+
+def write_hdr(path, img, rle=True):
+    """Radiance .hdr writer: adaptive-RLE scanlines (runs of >= 4 equal bytes, else literals) or flat."""
+    q = rgbe_encode(img)
+    H, W = q.shape[:2]
+    out = bytearray(b"#?RADIANCE\n# test image\nFORMAT=32-bit_rle_rgbe\n\n" + f"-Y {H} +X {W}\n".encode())
+    for y in range(H):
+        if not rle:
+            out += q[y].tobytes()
+            continue
+        out += bytes([2, 2, W >> 8, W & 255])
+        for ch in range(4):
+            row = [int(v) for v in q[y, :, ch]]
+            x = 0
+            while x < W:
+                run = 1
+                while x + run < W and run < 127 and row[x + run] == row[x]:
+                    run += 1
+                if run >= 4:
+                    out += bytes([128 + run, row[x]])
+                    x += run
+                    continue
+                lit = []
+                while x < W and len(lit) < 128:
+                    r = 1
+                    while x + r < W and r < 127 and row[x + r] == row[x]:
+                        r += 1
+                    if r >= 4:
+                        break
+                    lit.append(row[x])
+                    x += 1
+                out += bytes([len(lit)]) + bytes(lit)
+    with open(path, "wb") as f:
+        f.write(bytes(out))
+    return rgbe_decode(q)
+
+
+def write_pfm(path, img):
+    """Little-endian RGB PFM, rows bottom to top."""
+    img = np.asarray(img, np.float32)
+    H, W = img.shape[:2]
+    with open(path, "wb") as f:
+        f.write(f"PF\n{W} {H}\n-1.0\n".encode())
+        f.write(np.ascontiguousarray(img[::-1]).astype("<f4").tobytes())
+
+
+def sky_image(W=64, H=32, sun=(0.62, 0.27), sun_radius=0.03, sun_level=80.0, seed=0):
+    """Synthetic lat-long sky: blue gradient above, brown ground below, a bright sun disc."""
+    rng = np.random.default_rng(seed)
+    v = (np.arange(H) + 0.5) / H
+    u = (np.arange(W) + 0.5) / W
+    U, V = np.meshgrid(u, v)
+    img = np.zeros((H, W, 3), np.float32)
+    up = V < 0.5
+    t = (0.5 - V) * 2
+    img[up] = np.stack([0.35 + 0.2 * t, 0.5 + 0.2 * t, 0.9 + 0.1 * t], axis=-1)[up]
+    img[~up] = [0.25, 0.2, 0.15]
+    d = np.hypot((U - sun[0]) * 2, V - sun[1])
+    img[d < sun_radius] = sun_level
+    img *= (1.0 + 0.05 * rng.standard_normal((H, W, 1))).astype(np.float32)
+    return np.maximum(img, 0).astype(np.float32)
