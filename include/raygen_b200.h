@@ -17,10 +17,13 @@
  *   rg_cancel              <- RayRenderer::cancelRequested  src/raygen/rayrenderer.h:427
  *   rg_get_hdr             <- RayRenderer::getHdrResult   src/raygen/rayrenderer.h:411
  *   rg_get_ldr             <- RayRenderer::getRenderResult src/raygen/rayrenderer.h:404
+ *   rg_reapply_postprocess <- RayRenderer::reapplyPostProcess src/raygen/rayrenderer.cpp:698-711
+ *   rg_save_image          <- saveImage in the CLI's output step src/main.cpp:479-485
  *   rg_trace_closest       <- TriangleBVH::intersectClosest src/raygen/bvh.cpp:233-285
  *   rg_trace_any           <- TriangleBVH::intersectAny   src/raygen/bvh.h:63-101
  *   rg_denoise_atrous      <- RayRenderer::denoiseImage   src/raygen/rayrenderer.cpp:2649-2772
  *   rg_tonemap             <- RayRenderer::applyTonemapGamma src/raygen/rayrenderer.cpp:2610-2647
+ *   rg_bloom               <- RayRenderer::applyPostProcess src/raygen/rayrenderer.cpp:598-696
  *   rg_scene_builtin       <- (procedural stand-ins for the sample scenes; no reference symbol)
  *   rg_load_scene_json     <- RendererSceneLoader::load   src/raygen/sceneloader.cpp:1113-1137
  *   rg_server_*            <- the viewer's render-job worker (src/viewer/main.cpp:775-850),
@@ -198,6 +201,10 @@ rg_status rg_set_progress_cb(rg_handle* h, rg_progress_fn fn, void* user);
 rg_status rg_cancel(rg_handle* h);
 /* Linear HDR result (width*height*4 floats, alpha = 1). */
 rg_status rg_get_hdr(rg_handle* h, float* rgba, size_t count);
+/* Re-run the post-processing (HDR bloom when enable_rendering_postprocess,
+ * then the tonemap) from the last render's denoised, not yet bloomed HDR,
+ * with the current settings (set them with rg_update_settings first). */
+rg_status rg_reapply_postprocess(rg_handle* h);
 /* Tonemapped result in [0,1] (width*height*4 floats). */
 rg_status rg_get_ldr(rg_handle* h, float* rgba, size_t count);
 /* Guide buffers of the last render (normal*0.5+0.5, albedo, depth), 3 floats
@@ -251,6 +258,10 @@ rg_status rg_denoise_atrous_noalloc(int32_t w, int32_t h, const float* color_rgb
                                     int32_t levels, float sigma_color, float sigma_normal,
                                     float sigma_depth, float intensity, float* out_rgba, void* stream);
 rg_status rg_tonemap(int32_t w, int32_t h, const float* hdr_rgba, float* ldr_rgba);
+/* Energy-based HDR bloom on caller buffers (device work, host pointers):
+ * out = hdr + strength * blur(excess luminance above threshold), w*h RGBA. */
+rg_status rg_bloom(int32_t w, int32_t h, const float* hdr_rgba, float threshold, float strength, float radius,
+                   float size_aspect, float curve, float* out_rgba);
 
 /* Procedural scenes (host C++, no device work).
  * kind 1: cube room (10 walls, two boxes, one 2.5x2.5 ceiling light).
@@ -265,6 +276,11 @@ rg_status rg_scene_builtin(int32_t kind, uint32_t seed, const int32_t* iparams, 
 rg_status rg_scene_free(rg_scene_desc* scene);
 /* Reference scene JSON (sceneloader.cpp schema) -> flattened description. */
 rg_status rg_load_scene_json(const char* path, rg_scene_desc** out);
+/* Write width*height RGBA floats (row 0 at the top) to an image file chosen by
+ * extension: .hdr (Radiance RGBE, RLE scanlines) and .pfm keep linear values;
+ * .jpg / .jpeg (baseline JPEG, quality 92, 4:4:4), .png and .ppm store
+ * round(clamp(v, 0, 1) * 255).  Host work only. */
+rg_status rg_save_image(const char* path, int32_t width, int32_t height, const float* rgba);
 
 /* ---- resident multi-job server (batched and served rendering) ----------- */
 #define RG_JOB_QUEUED 0

@@ -69,6 +69,7 @@ def load(fast: bool = False) -> C.CDLL:
     lib.orc_phase_pdf.argtypes = [C.c_float, C.c_float]
     lib.orc_sample_phase.argtypes = [C.c_float, C.c_float, C.c_float, f]
     lib.orc_env_eval.argtypes = [C.c_void_p, f, C.c_int32, f, f]
+    lib.orc_bloom.argtypes = [C.c_int32, C.c_int32, f] + [C.c_float] * 5
     lib.orc_env_sample.argtypes = [C.c_void_p, f, C.c_int32, f, f]
     _libs[name] = lib
     return lib
@@ -192,6 +193,15 @@ def tonemap(hdr):
     h, w = hdr.shape[:2]
     out = np.empty_like(hdr)
     lib.orc_tonemap(w, h, _fp(hdr), _fp(out))
+    return out
+
+
+def bloom(hdr, threshold=1.0, strength=1.0, radius=0.03, size_aspect=0.15, curve=1.0):
+    """HDR bloom (RayRenderer::applyPostProcess) of an H x W x 4 image; returns a new array."""
+    lib = load()
+    out = np.ascontiguousarray(hdr, np.float32).copy()
+    h, w = out.shape[:2]
+    lib.orc_bloom(w, h, _fp(out), threshold, strength, radius, size_aspect, curve)
     return out
 
 

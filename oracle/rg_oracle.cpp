@@ -1640,6 +1640,106 @@ static void denoise(int w, int h, const float* noisy, const float* normal, const
     }
 }
 
+// applyPostProcess (rayrenderer.cpp:598-696): energy-based HDR bloom on an
+// RGBA image in place.  Extract the luminance above the threshold (with the
+// knee curve), area-average it into a glow buffer of size_aspect x the image
+// (downsampleArea, :386-413), blur it twice with a Gaussian of sigma / sqrt 2
+// where sigma = radius x W x size_aspect (separableGaussianBlur, :423-475),
+// upsample bilinearly (texel centres aligned, edges clamped: the reference's
+// Image::resize lives in the graphics-module submodule, not in its tree) and
+// add strength x glow.
+static void bloom(int W, int H, float* hdr, float threshold, float strength, float radius, float sizeAspect,
+                  float curve) {
+  if (W <= 0 || H <= 0) return;
+  threshold = fmaxf(threshold, 0.0f);
+  curve = fmaxf(curve, 1e-3f);
+  const float aspect = fmaxf(0.02f, sizeAspect);
+  const int gw = std::max(1, (int)((float)W * aspect));
+  const int gh = std::max(1, (int)((float)H * aspect));
+  std::vector<float> glow((size_t)gw * gh * 3, 0.0f), tmp(glow.size());
+  for (int y = 0; y < gh; ++y) {
+    const int y0 = (int)((int64_t)y * H / gh);
+    const int y1 = std::max(y0 + 1, (int)((int64_t)(y + 1) * H / gh));
+    for (int x = 0; x < gw; ++x) {
+      const int x0 = (int)((int64_t)x * W / gw);
+      const int x1 = std::max(x0 + 1, (int)((int64_t)(x + 1) * W / gw));
+      float ar = 0.0f, ag = 0.0f, ab = 0.0f;
+      int count = 0;
+      for (int sy = y0; sy < y1 && sy < H; ++sy)
+        for (int sx = x0; sx < x1 && sx < W; ++sx) {
+          const float* c = &hdr[((size_t)sy * W + sx) * 4];
+          const float L = 0.2126f * c[0] + 0.7152f * c[1] + 0.0722f * c[2];
+          float gr = 0.0f, gg = 0.0f, gb = 0.0f;
+          if (L > threshold && L > 1e-6f) {
+            float scale = (L - threshold) / L;
+            if (curve != 1.0f) scale = powf(scale, curve);
+            gr = c[0] * scale; gg = c[1] * scale; gb = c[2] * scale;
+          }
+          ar += gr; ag += gg; ab += gb;
+          count++;
+        }
+      if (count > 0) {
+        const float inv = 1.0f / (float)count;
+        float* o = &glow[((size_t)y * gw + x) * 3];
+        o[0] = ar * inv; o[1] = ag * inv; o[2] = ab * inv;
+      }
+    }
+  }
+  const float sigmaDown = fmaxf(0.0f, radius) * (float)W * aspect;
+  if (sigmaDown >= 0.5f) {
+    const float sigma = sigmaDown * 0.70710678f;
+    if (sigma >= 0.25f) {
+      const int r = std::max(1, (int)ceilf(sigma * 3.0f));
+      std::vector<float> k(2 * r + 1);
+      float sum = 0.0f;
+      const float twoSigmaSq = 2.0f * sigma * sigma;
+      for (int i = 0; i < 2 * r + 1; ++i) {
+        const float x = (float)(i - r);
+        k[i] = expf(-(x * x) / twoSigmaSq);
+        sum += k[i];
+      }
+      const float invSum = 1.0f / sum;
+      for (float& w : k) w *= invSum;
+      auto pass = [&](const std::vector<float>& src, std::vector<float>& dst, bool vertical) {
+        for (int y = 0; y < gh; ++y)
+          for (int x = 0; x < gw; ++x) {
+            float a[3] = {0.0f, 0.0f, 0.0f};
+            for (int t = -r; t <= r; ++t) {
+              int sx = x, sy = y;
+              if (vertical) sy = std::min(std::max(y + t, 0), gh - 1);
+              else sx = std::min(std::max(x + t, 0), gw - 1);
+              const float* c = &src[((size_t)sy * gw + sx) * 3];
+              for (int ch = 0; ch < 3; ch++) a[ch] += c[ch] * k[t + r];
+            }
+            float* o = &dst[((size_t)y * gw + x) * 3];
+            o[0] = a[0]; o[1] = a[1]; o[2] = a[2];
+          }
+      };
+      for (int twice = 0; twice < 2; ++twice) {
+        pass(glow, tmp, false);
+        pass(tmp, glow, true);
+      }
+    }
+  }
+  for (int y = 0; y < H; ++y)
+    for (int x = 0; x < W; ++x) {
+      float sx = ((float)x + 0.5f) * (float)gw / (float)W - 0.5f;
+      float sy = ((float)y + 0.5f) * (float)gh / (float)H - 0.5f;
+      sx = fminf(fmaxf(sx, 0.0f), (float)(gw - 1));
+      sy = fminf(fmaxf(sy, 0.0f), (float)(gh - 1));
+      const int x0 = (int)sx, y0 = (int)sy;
+      const int x1 = std::min(x0 + 1, gw - 1), y1 = std::min(y0 + 1, gh - 1);
+      const float fx = sx - (float)x0, fy = sy - (float)y0;
+      float* a = &hdr[((size_t)y * W + x) * 4];
+      for (int ch = 0; ch < 3; ch++) {
+        auto at = [&](int xx, int yy) { return glow[((size_t)yy * gw + xx) * 3 + ch]; };
+        auto lerp = [](float p, float q, float t) { return p + (q - p) * t; };
+        const float g = lerp(lerp(at(x0, y0), at(x1, y0), fx), lerp(at(x0, y1), at(x1, y1), fx), fy);
+        a[ch] = a[ch] + g * strength;
+      }
+    }
+}
+
 // applyTonemapGamma: rayrenderer.cpp:2610-2647
 static void tonemap(int w, int h, const float* src, float* dst) {
   const float invGamma = 1.0f / 2.2f;
@@ -1962,6 +2062,10 @@ void orc_denoise(int32_t w, int32_t h, const float* color, const float* normal, 
   denoise(w, h, color, normal, depth, albedo, albedo_alpha, levels, sc, sn, sd, intensity, out);
 }
 void orc_tonemap(int32_t w, int32_t h, const float* hdr, float* ldr) { tonemap(w, h, hdr, ldr); }
+void orc_bloom(int32_t w, int32_t h, float* hdr, float threshold, float strength, float radius, float size_aspect,
+               float curve) {
+  bloom(w, h, hdr, threshold, strength, radius, size_aspect, curve);
+}
 
 // RNG probes (shared specification with the device code).
 float orc_lds(uint32_t x, uint32_t y, uint32_t width, uint32_t sample, uint32_t seed, int32_t dim) {

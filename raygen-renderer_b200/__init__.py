@@ -203,6 +203,9 @@ def load_library(path: str = LIB_PATH) -> C.CDLL:
                                         P(C.c_float), P(C.c_float), C.c_int32, C.c_float, C.c_float,
                                         C.c_float, C.c_float, P(C.c_float)]),
         "rg_tonemap": (C.c_int, [C.c_int32, C.c_int32, P(C.c_float), P(C.c_float)]),
+        "rg_bloom": (C.c_int, [C.c_int32, C.c_int32, P(C.c_float)] + [C.c_float] * 5 + [P(C.c_float)]),
+        "rg_save_image": (C.c_int, [C.c_char_p, C.c_int32, C.c_int32, P(C.c_float)]),
+        "rg_reapply_postprocess": (C.c_int, [C.c_void_p]),
         "rg_scene_builtin": (C.c_int, [C.c_int32, C.c_uint32, P(C.c_int32), C.c_int32, P(P(rg_scene_desc))]),
         "rg_scene_free": (C.c_int, [P(rg_scene_desc)]),
         "rg_load_scene_json": (C.c_int, [C.c_char_p, P(P(rg_scene_desc))]),
@@ -327,7 +330,10 @@ class Scene:
 
     @property
     def desc(self) -> rg_scene_desc:
-        return self._ptr.contents
+        """The rg_scene_desc; it keeps this Scene (and so the memory it points into) alive."""
+        c = self._ptr.contents
+        c._owner = self
+        return c
 
     @property
     def ptr(self):
@@ -465,6 +471,12 @@ class RayRenderer:
     def _size(self):
         return self.settings.resolutionHeight, self.settings.resolutionWidth
 
+    def reapply_post_process(self) -> None:
+        """RayRenderer::reapplyPostProcess: bloom + tonemap again from the last pre-bloom HDR
+        with the current settings (e.g. after changing bloomStrength)."""
+        self._sync_settings()
+        _check(self._lib.rg_reapply_postprocess(self._h))
+
     def get_hdr_result(self) -> np.ndarray:
         h, w = self._size()
         out = np.empty((h, w, 4), np.float32)
@@ -546,6 +558,23 @@ def denoise_atrous(color, normal, depth, albedo, albedo_alpha, levels=5, sigma_c
                                  _fptr(args[3]), levels, sigma_color, sigma_normal, sigma_depth,
                                  intensity, _fptr(out)))
     return out
+
+
+def bloom(hdr_rgba: np.ndarray, threshold=1.0, strength=1.0, radius=0.03, size_aspect=0.15, curve=1.0) -> np.ndarray:
+    """Device HDR bloom on a host RGBA image (RayRenderer::applyPostProcess, rayrenderer.cpp:598-696)."""
+    lib = load_library()
+    hdr = np.ascontiguousarray(hdr_rgba, np.float32)
+    h, w = hdr.shape[:2]
+    out = np.empty_like(hdr)
+    _check(lib.rg_bloom(w, h, _fptr(hdr), threshold, strength, radius, size_aspect, curve, _fptr(out)))
+    return out
+
+
+def save_image(path: str, rgba: np.ndarray) -> None:
+    """Write an H x W x 4 float image; the format follows the extension (.hdr .pfm .jpg .png .ppm)."""
+    lib = load_library()
+    a = np.ascontiguousarray(rgba, np.float32)
+    _check(lib.rg_save_image(path.encode(), a.shape[1], a.shape[0], _fptr(a)))
 
 
 def tonemap(hdr_rgba: np.ndarray) -> np.ndarray:

@@ -6,8 +6,10 @@
 // unknown flags print "unknown argument" and return 1.  Tracer knobs added:
 // --seed, --max-depth, --rr-depth, --light-pick-fix, --adaptive-mode pixel|tile,
 // --bvh-bins.  A scene path of the form builtin:<kind>[:<seed>] renders one of
-// the procedural workloads.  Output: .hdr (RGBE, linear), .pfm (float),
-// anything else a binary PPM of the tonemapped image.
+// the procedural workloads.  Output (rg_save_image): .hdr (Radiance RGBE) and
+// .pfm hold the linear HDR result; .jpg (the default, <scene dir>/<base>.jpg
+// as in the reference), .png and .ppm the tonemapped image.
+#include <cctype>
 #include <chrono>
 #include <cmath>
 #include <cstdio>
@@ -31,61 +33,6 @@ std::string ext(const std::string& p) {
   std::string e = p.substr(d + 1);
   for (auto& c : e) c = (char)std::tolower(c);
   return e;
-}
-
-// Radiance RGBE writer (flat, uncompressed scanlines).
-bool writeHdr(const std::string& path, int w, int h, const std::vector<float>& rgba) {
-  FILE* f = std::fopen(path.c_str(), "wb");
-  if (!f) return false;
-  std::fprintf(f, "#?RADIANCE\nFORMAT=32-bit_rle_rgbe\n\n-Y %d +X %d\n", h, w);
-  std::vector<unsigned char> row((size_t)w * 4);
-  for (int y = 0; y < h; y++) {
-    for (int x = 0; x < w; x++) {
-      const float* p = &rgba[((size_t)y * w + x) * 4];
-      const float m = std::fmax(p[0], std::fmax(p[1], p[2]));
-      unsigned char* o = &row[(size_t)x * 4];
-      if (m < 1e-32f) {
-        o[0] = o[1] = o[2] = o[3] = 0;
-      } else {
-        int e;
-        const float s = std::frexp(m, &e) * 256.0f / m;
-        o[0] = (unsigned char)(p[0] * s);
-        o[1] = (unsigned char)(p[1] * s);
-        o[2] = (unsigned char)(p[2] * s);
-        o[3] = (unsigned char)(e + 128);
-      }
-    }
-    std::fwrite(row.data(), 1, row.size(), f);
-  }
-  std::fclose(f);
-  return true;
-}
-
-bool writePfm(const std::string& path, int w, int h, const std::vector<float>& rgba) {
-  FILE* f = std::fopen(path.c_str(), "wb");
-  if (!f) return false;
-  std::fprintf(f, "PF\n%d %d\n-1.0\n", w, h);
-  for (int y = h - 1; y >= 0; y--)
-    for (int x = 0; x < w; x++) std::fwrite(&rgba[((size_t)y * w + x) * 4], sizeof(float), 3, f);
-  std::fclose(f);
-  return true;
-}
-
-bool writePpm(const std::string& path, int w, int h, const std::vector<float>& rgba) {
-  FILE* f = std::fopen(path.c_str(), "wb");
-  if (!f) return false;
-  std::fprintf(f, "P6\n%d %d\n255\n", w, h);
-  std::vector<unsigned char> row((size_t)w * 3);
-  for (int y = 0; y < h; y++) {
-    for (int x = 0; x < w; x++)
-      for (int k = 0; k < 3; k++) {
-        const float v = rgba[((size_t)y * w + x) * 4 + k];
-        row[(size_t)x * 3 + k] = (unsigned char)std::lround(std::fmin(std::fmax(v, 0.0f), 1.0f) * 255.0f);
-      }
-    std::fwrite(row.data(), 1, row.size(), f);
-  }
-  std::fclose(f);
-  return true;
 }
 
 void progress(float p, void*) {
@@ -194,7 +141,7 @@ int main(int argc, const char* argv[]) {
     const size_t d = base.find_last_of('.');
     if (d != std::string::npos && base.find('/', d) == std::string::npos) base = base.substr(0, d);
     for (auto& c : base) if (c == ':') c = '_';
-    out = base + ".ppm";
+    out = base + ".jpg";
   }
   std::printf("%s\n\n  input : %s\n  output: %s\n\n", rg_version(), scene.c_str(), out.c_str());
   std::printf("  resolution     : %d x %d\n  shader system  : %d\n  samples        : %d\n  denoise        : %s\n\n",
@@ -214,11 +161,11 @@ int main(int argc, const char* argv[]) {
   }
   const auto t1 = std::chrono::steady_clock::now();
   std::vector<float> img((size_t)rs.resolution_width * rs.resolution_height * 4);
+  // .hdr / .pfm: the linear HDR buffer, no tonemap (main.cpp:479-485); otherwise the LDR result
   const std::string e = ext(out);
-  bool ok;
-  if (e == "hdr") ok = rg_get_hdr(h, img.data(), img.size()) == RG_OK && writeHdr(out, rs.resolution_width, rs.resolution_height, img);
-  else if (e == "pfm") ok = rg_get_hdr(h, img.data(), img.size()) == RG_OK && writePfm(out, rs.resolution_width, rs.resolution_height, img);
-  else ok = rg_get_ldr(h, img.data(), img.size()) == RG_OK && writePpm(out, rs.resolution_width, rs.resolution_height, img);
+  const bool linear = e == "hdr" || e == "pfm";
+  const bool ok = (linear ? rg_get_hdr(h, img.data(), img.size()) : rg_get_ldr(h, img.data(), img.size())) == RG_OK &&
+                  rg_save_image(out.c_str(), rs.resolution_width, rs.resolution_height, img.data()) == RG_OK;
   rg_stats stats;
   rg_get_stats(h, &stats);
   std::printf("\rdone. (%.3f s; trace %.1f ms, %.1f Msamples/s)\n", std::chrono::duration<double>(t1 - t0).count(),
@@ -226,7 +173,7 @@ int main(int argc, const char* argv[]) {
   rg_destroy(h);
   rg_scene_free(desc);
   if (!ok) {
-    std::printf("raygen: cannot write %s\n", out.c_str());
+    std::printf("raygen: cannot write %s: %s\n", out.c_str(), rg_last_error());
     return 1;
   }
   return 0;

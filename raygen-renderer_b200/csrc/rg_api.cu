@@ -135,6 +135,8 @@ struct rg_handle {
   bool hasScene = false;
   // render buffers
   DevBuf<float4> sum, sumSq, hdr, ldr, bufA, bufB;
+  DevBuf<float4> preBloom, bloomA, bloomB;  // HDR before bloom (reapply), glow buffers
+  DevBuf<float> bloomW;                     // Gaussian taps
   DevBuf<int> cnt, pixelList, listCount;
   DevBuf<__half> aovNormal, aovAlbedo, aovAlbedoA, aovDepth;
   int W = 0, H = 0;
@@ -691,6 +693,38 @@ rg_status rg_set_scene(rg_handle* h, const rg_scene_desc* d) {
   return RG_OK;
 }
 
+// Keeps the denoised, not yet bloomed HDR (RayRenderer::preBloomHdrImage) and
+// applies the bloom when post-processing is on (rayrenderer.cpp:584-592).
+static rg_status postProcess(rg_handle* h, bool restore) {
+  const rg_settings& s = h->st;
+  const int W = h->W, H = h->H;
+  const size_t N = (size_t)W * H;
+  cudaStream_t st = h->stream;
+  if (restore) {
+    RG_CUDA_CHECK(cudaMemcpyAsync(h->hdr.p, h->preBloom.p, sizeof(float4) * N, cudaMemcpyDeviceToDevice, st));
+  } else {
+    if (!h->preBloom.alloc(N)) {
+      setLastError("out of device memory (pre-bloom copy)");
+      return RG_ERR_OUT_OF_MEMORY;
+    }
+    RG_CUDA_CHECK(cudaMemcpyAsync(h->preBloom.p, h->hdr.p, sizeof(float4) * N, cudaMemcpyDeviceToDevice, st));
+  }
+  if (s.enable_rendering_postprocess) {
+    const BloomPlan p = planBloom(W, H, s.bloom_radius, s.bloom_size_aspect);
+    const size_t n = (size_t)p.gw * p.gh;
+    if (!h->bloomA.alloc(n) || !h->bloomB.alloc(n) || !h->bloomW.alloc(std::max<size_t>(1, p.weights.size()))) {
+      setLastError("out of device memory (bloom buffers)");
+      return RG_ERR_OUT_OF_MEMORY;
+    }
+    if (!p.weights.empty())  // pageable source: staged before the call returns
+      RG_CUDA_CHECK(cudaMemcpyAsync(h->bloomW.p, p.weights.data(), sizeof(float) * p.weights.size(),
+                                    cudaMemcpyHostToDevice, st));
+    launchBloom(W, H, h->hdr.p, p, h->bloomW.p, s.bloom_threshold, s.bloom_strength, s.bloom_curve, h->bloomA.p,
+                h->bloomB.p, st);
+  }
+  return RG_OK;
+}
+
 static rg_status runPass(rg_handle* h, const DevRender& R, int numPixels, const int* pixelList, int spp,
                          int& wavesDone, int totalWavesHint, bool profile, double* kernelMs) {
   if (numPixels <= 0 || spp <= 0) return RG_OK;
@@ -911,6 +945,16 @@ rg_status rg_render(rg_handle* h) {
                   h->bufB.p, h->ldr.p, st);
     RG_CUDA_CHECK(cudaMemcpyAsync(h->hdr.p, h->ldr.p, sizeof(float4) * N, cudaMemcpyDeviceToDevice, st));
   }
+  {
+    const rg_status ps = postProcess(h, false);
+    if (ps != RG_OK) {
+      cudaStreamSynchronize(st);
+      cudaEventDestroy(t0);
+      cudaEventDestroy(t1);
+      cudaEventDestroy(t2);
+      return ps;
+    }
+  }
   launchTonemap(N, h->hdr.p, h->ldr.p, st);
   cudaEventRecord(t2, st);
   const cudaError_t se = cudaStreamSynchronize(st);
@@ -956,6 +1000,17 @@ rg_status rg_render(rg_handle* h) {
     return RG_ERR_DEVICE_STATUS;
   }
   h->haveResult = true;
+  return RG_OK;
+}
+
+rg_status rg_reapply_postprocess(rg_handle* h) {
+  if (!h) return RG_ERR_INVALID_ARGUMENT;
+  std::lock_guard<std::mutex> lk(h->mu);
+  if (!h->haveResult) return RG_ERR_NO_SCENE;
+  const rg_status rs = postProcess(h, true);
+  if (rs != RG_OK) return rs;
+  launchTonemap(h->W * h->H, h->hdr.p, h->ldr.p, h->stream);
+  RG_CUDA_CHECK(cudaStreamSynchronize(h->stream));
   return RG_OK;
 }
 
@@ -1112,6 +1167,27 @@ rg_status rg_tonemap(int32_t w, int32_t h, const float* hdr_rgba, float* ldr_rgb
   return RG_OK;
 }
 
+rg_status rg_bloom(int32_t w, int32_t h, const float* hdr_rgba, float threshold, float strength, float radius,
+                   float size_aspect, float curve, float* out_rgba) {
+  if (w <= 0 || h <= 0 || !hdr_rgba || !out_rgba) return RG_ERR_INVALID_ARGUMENT;
+  int dc = 0;
+  if (cudaGetDeviceCount(&dc) != cudaSuccess || dc == 0) {
+    cudaGetLastError();
+    return RG_ERR_NO_DEVICE;
+  }
+  const int N = w * h;
+  const BloomPlan p = planBloom(w, h, radius, size_aspect);
+  const size_t n = (size_t)p.gw * p.gh;
+  DevBuf<float4> a, sa, sb;
+  DevBuf<float> wt;
+  if (!a.upload(reinterpret_cast<const float4*>(hdr_rgba), N, 0) || !sa.alloc(n) || !sb.alloc(n) ||
+      !wt.upload(p.weights.data(), p.weights.size(), 0))
+    return RG_ERR_OUT_OF_MEMORY;
+  launchBloom(w, h, a.p, p, wt.p, threshold, strength, curve, sa.p, sb.p, 0);
+  RG_CUDA_CHECK(cudaMemcpy(out_rgba, a.p, sizeof(float4) * N, cudaMemcpyDeviceToHost));
+  return RG_OK;
+}
+
 static std::mutex g_storeMu;
 static std::unordered_map<const rg_scene_desc*, SceneStore*> g_stores;
 
@@ -1141,6 +1217,16 @@ rg_status rg_scene_free(rg_scene_desc* scene) {
     g_stores.erase(it);
   }
   delete st;
+  return RG_OK;
+}
+
+rg_status rg_save_image(const char* path, int32_t width, int32_t height, const float* rgba) {
+  if (!path || !rgba || width <= 0 || height <= 0) return RG_ERR_INVALID_ARGUMENT;
+  std::string err;
+  if (!writeImageFile(path, width, height, rgba, err)) {
+    setLastError(err);
+    return err.rfind("unsupported", 0) == 0 ? RG_ERR_UNSUPPORTED : RG_ERR_IO;
+  }
   return RG_OK;
 }
 

@@ -95,6 +95,7 @@ rg_status loadSceneJson(const char* path, SceneStore** out, std::string& err);
 bool readRadianceHdr(const std::string& path, TextureStore& out, std::string& err);
 bool readPfm(const std::string& path, TextureStore& out, std::string& err);
 bool readImageFile(const std::string& path, TextureStore& out, std::string& err);
+bool writeImageFile(const std::string& path, int W, int H, const float* rgba, std::string& err);
 
 // Device-resident scene (BVH + triangle and light tables).
 struct DeviceScene {

@@ -1,4 +1,5 @@
-// rg_post.cu - resolve, adaptive-sampling masks, A-Trous denoiser and tonemap.
+// rg_post.cu - resolve, adaptive-sampling masks, A-Trous denoiser, HDR bloom
+// and tonemap.
 //
 // Reference: renderPixel / hdrToPreview (rayrenderer.cpp:959-1009),
 // computeTileNoise / renderAdaptive (:1038-1252), denoiseImage / atrousPass
@@ -8,6 +9,9 @@
 // FP32 colour and FP16 guide buffers; every pass is one kernel, one thread
 // per pixel, reading its taps through the read-only cache.
 #include <cuda_fp16.h>
+
+#include <algorithm>
+#include <vector>
 
 #include "rg_device.cuh"
 #include "rg_trace.cuh"
@@ -235,6 +239,100 @@ __global__ void k_f2h(int n, const float* in, __half* out) {
 
 inline int g256(int n) { return (n + 255) / 256; }
 
+// ---- HDR bloom (RayRenderer::applyPostProcess, rayrenderer.cpp:598-696) ------
+// Every product that feeds a sum is rounded on its own (no contraction), in
+// the reference's loop order, so the oracle's restatement agrees bit for bit
+// (powf for a bloom curve other than 1 aside).
+__device__ __forceinline__ float3 bloomExtract(float4 c, float threshold, float curve) {
+  // excess luminance above the threshold (rayrenderer.cpp:614-633)
+  const float L = __fadd_rn(__fadd_rn(__fmul_rn(0.2126f, c.x), __fmul_rn(0.7152f, c.y)), __fmul_rn(0.0722f, c.z));
+  float3 g = make_float3(0.0f, 0.0f, 0.0f);
+  if (L > threshold && L > 1e-6f) {
+    float scale = __fdiv_rn(__fsub_rn(L, threshold), L);
+    if (curve != 1.0f) scale = powf(scale, curve);
+    g = make_float3(__fmul_rn(c.x, scale), __fmul_rn(c.y, scale), __fmul_rn(c.z, scale));
+  }
+  return g;
+}
+
+// extract + downsampleArea (rayrenderer.cpp:386-413): one thread per glow pixel,
+// the box of full-resolution pixels it covers summed row by row.
+__global__ void k_bloomDown(int W, int H, int gw, int gh, const float4* __restrict__ hdr, float threshold, float curve,
+                            float4* __restrict__ small) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= gw * gh) return;
+  const int x = i % gw, y = i / gw;
+  const int y0 = (int)((long long)y * H / gh);
+  const int y1 = max(y0 + 1, (int)((long long)(y + 1) * H / gh));
+  const int x0 = (int)((long long)x * W / gw);
+  const int x1 = max(x0 + 1, (int)((long long)(x + 1) * W / gw));
+  float ar = 0.0f, ag = 0.0f, ab = 0.0f;
+  int count = 0;
+  for (int sy = y0; sy < y1 && sy < H; ++sy)
+    for (int sx = x0; sx < x1 && sx < W; ++sx) {
+      const float3 g = bloomExtract(__ldg(hdr + (size_t)sy * W + sx), threshold, curve);
+      ar = __fadd_rn(ar, g.x);
+      ag = __fadd_rn(ag, g.y);
+      ab = __fadd_rn(ab, g.z);
+      count++;
+    }
+  float4 o = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+  if (count > 0) {
+    const float inv = __fdiv_rn(1.0f, (float)count);
+    o = make_float4(__fmul_rn(ar, inv), __fmul_rn(ag, inv), __fmul_rn(ab, inv), 0.0f);
+  }
+  small[i] = o;
+}
+
+// separableGaussianBlur, one direction (rayrenderer.cpp:423-475): clamp to edge,
+// taps k = -r..r in order.
+__global__ void k_bloomBlur(int w, int h, int r, const float* __restrict__ wts, int vertical,
+                            const float4* __restrict__ src, float4* __restrict__ dst) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= w * h) return;
+  const int x = i % w, y = i / w;
+  float ar = 0.0f, ag = 0.0f, ab = 0.0f;
+  for (int k = -r; k <= r; ++k) {
+    int sx = x, sy = y;
+    if (vertical) sy = min(max(y + k, 0), h - 1);
+    else sx = min(max(x + k, 0), w - 1);
+    const float4 c = __ldg(src + (size_t)sy * w + sx);
+    const float wk = __ldg(wts + k + r);
+    ar = __fadd_rn(ar, __fmul_rn(c.x, wk));
+    ag = __fadd_rn(ag, __fmul_rn(c.y, wk));
+    ab = __fadd_rn(ab, __fmul_rn(c.z, wk));
+  }
+  dst[i] = make_float4(ar, ag, ab, 0.0f);
+}
+
+// Bilinear upsample of the glow (Image::resize; texel centres aligned, edges
+// clamped) and the unclamped add hdr += glow * strength (rayrenderer.cpp:675-693).
+__device__ __forceinline__ float lerpRn(float a, float b, float t) { return __fadd_rn(a, __fmul_rn(__fsub_rn(b, a), t)); }
+
+__global__ void k_bloomUpAdd(int W, int H, int gw, int gh, const float4* __restrict__ small, float strength,
+                             float4* __restrict__ hdr) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= W * H) return;
+  const int x = i % W, y = i / W;
+  float sx = __fsub_rn(__fdiv_rn(__fmul_rn((float)x + 0.5f, (float)gw), (float)W), 0.5f);
+  float sy = __fsub_rn(__fdiv_rn(__fmul_rn((float)y + 0.5f, (float)gh), (float)H), 0.5f);
+  sx = fminf(fmaxf(sx, 0.0f), (float)(gw - 1));
+  sy = fminf(fmaxf(sy, 0.0f), (float)(gh - 1));
+  const int x0 = (int)sx, y0 = (int)sy;
+  const int x1 = min(x0 + 1, gw - 1), y1 = min(y0 + 1, gh - 1);
+  const float fx = __fsub_rn(sx, (float)x0), fy = __fsub_rn(sy, (float)y0);
+  const float4 p00 = __ldg(small + (size_t)y0 * gw + x0), p10 = __ldg(small + (size_t)y0 * gw + x1);
+  const float4 p01 = __ldg(small + (size_t)y1 * gw + x0), p11 = __ldg(small + (size_t)y1 * gw + x1);
+  const float gr = lerpRn(lerpRn(p00.x, p10.x, fx), lerpRn(p01.x, p11.x, fx), fy);
+  const float gg = lerpRn(lerpRn(p00.y, p10.y, fx), lerpRn(p01.y, p11.y, fx), fy);
+  const float gb = lerpRn(lerpRn(p00.z, p10.z, fx), lerpRn(p01.z, p11.z, fx), fy);
+  float4 a = hdr[i];
+  a.x = __fadd_rn(a.x, __fmul_rn(gr, strength));
+  a.y = __fadd_rn(a.y, __fmul_rn(gg, strength));
+  a.z = __fadd_rn(a.z, __fmul_rn(gb, strength));
+  hdr[i] = a;
+}
+
 }  // namespace
 
 void launchResolve(int n, const float4* sum, const int* cnt, float exposure, float4* hdr, cudaStream_t st) {
@@ -262,6 +360,48 @@ void launchDenoise(int w, int h, const float4* noisy, const __half* normal, cons
 }
 
 void launchTonemap(int n, const float4* hdr, float4* ldr, cudaStream_t st) { k_tonemap<<<g256(n), 256, 0, st>>>(n, hdr, ldr); }
+
+BloomPlan planBloom(int W, int H, float radius, float sizeAspect) {
+  BloomPlan p;
+  const float aspect = fmaxf(0.02f, sizeAspect);
+  p.gw = std::max(1, (int)((float)W * aspect));
+  p.gh = std::max(1, (int)((float)H * aspect));
+  const float sigmaDown = fmaxf(0.0f, radius) * (float)W * aspect;
+  p.r = 0;
+  p.weights.clear();
+  if (sigmaDown >= 0.5f) {
+    // two passes of sigma / sqrt(2) (rayrenderer.cpp:660-666); kernel as separableGaussianBlur
+    const float sigma = sigmaDown * 0.70710678f;
+    if (sigma >= 0.25f) {
+      p.r = std::max(1, (int)ceilf(sigma * 3.0f));
+      const int k = 2 * p.r + 1;
+      p.weights.resize(k);
+      float sum = 0.0f;
+      const float twoSigmaSq = 2.0f * sigma * sigma;
+      for (int i = 0; i < k; ++i) {
+        const float x = (float)(i - p.r);
+        p.weights[i] = expf(-(x * x) / twoSigmaSq);
+        sum += p.weights[i];
+      }
+      const float inv = 1.0f / sum;
+      for (float& w : p.weights) w *= inv;
+    }
+  }
+  return p;
+}
+
+void launchBloom(int W, int H, float4* hdr, const BloomPlan& p, const float* weightsDev, float threshold,
+                 float strength, float curve, float4* smallA, float4* smallB, cudaStream_t st) {
+  const int n = p.gw * p.gh;
+  k_bloomDown<<<g256(n), 256, 0, st>>>(W, H, p.gw, p.gh, hdr, fmaxf(threshold, 0.0f), fmaxf(curve, 1e-3f), smallA);
+  if (p.r > 0) {
+    for (int pass = 0; pass < 2; ++pass) {
+      k_bloomBlur<<<g256(n), 256, 0, st>>>(p.gw, p.gh, p.r, weightsDev, 0, smallA, smallB);
+      k_bloomBlur<<<g256(n), 256, 0, st>>>(p.gw, p.gh, p.r, weightsDev, 1, smallB, smallA);
+    }
+  }
+  k_bloomUpAdd<<<g256(W * H), 256, 0, st>>>(W, H, p.gw, p.gh, smallA, strength, hdr);
+}
 
 void launchAdaptivePixels(int n, const float4* sum, const float4* sumSq, const int* cnt, int target, float threshold,
                           int* list, int* outCount, cudaStream_t st) {

@@ -1,5 +1,7 @@
 // rg_trace.cuh - launchers of the trace and post kernels (host-callable).
 #pragma once
+
+#include <vector>
 #include <cuda_fp16.h>
 #include <cuda_runtime.h>
 
@@ -31,6 +33,15 @@ void launchDenoise(int w, int h, const float4* noisy, const __half* normal, cons
                    const __half* albedoA, int levels, float sigC, float sigN, float sigD, float intensity,
                    float4* bufA, float4* bufB, float4* out, cudaStream_t st);
 void launchTonemap(int n, const float4* hdr, float4* ldr, cudaStream_t st);
+// HDR bloom: glow buffer size and the normalised Gaussian taps (host), then
+// extract + area downsample, 2 x (horizontal, vertical) blur, upsample + add.
+struct BloomPlan {
+  int gw = 1, gh = 1, r = 0;    // glow buffer size, blur radius (0: no blur)
+  std::vector<float> weights;   // 2r+1 taps
+};
+BloomPlan planBloom(int W, int H, float radius, float sizeAspect);
+void launchBloom(int W, int H, float4* hdr, const BloomPlan& p, const float* weightsDev, float threshold,
+                 float strength, float curve, float4* smallA, float4* smallB, cudaStream_t st);
 // adaptive: per-pixel relative SEM -> compacted active pixel list; returns count via *outCount (device)
 void launchAdaptivePixels(int n, const float4* sum, const float4* sumSq, const int* cnt, int target, float threshold,
                           int* list, int* outCount, cudaStream_t st);
