@@ -639,6 +639,7 @@ rg_status prepareScene(const rg_scene_desc* d, int bins, bool wide, cudaStream_t
   S.objMedium = ds.objMedium.p;
   S.mats = ds.mats.p;
   S.media = ds.media.p;
+  S.numMedia = d->num_media;
   S.globalMedium = ds.globalMedium;
   S.numAreaLights = ds.numAreaLights;
   S.areaLightObj = ds.areaLightObj.p;

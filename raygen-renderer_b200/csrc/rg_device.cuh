@@ -69,6 +69,7 @@ struct DevScene {
   const int* objMedium;       // object -> interior medium (-1 none)
   const DevMaterial* mats;
   const DevMedium* media;
+  int numMedia;
   int globalMedium;
   int numAreaLights;
   const int* areaLightObj;    // area light -> object

@@ -752,8 +752,10 @@ __global__ void __launch_bounds__(128) k_connect8(DevScene S0, const DevJob* __r
 // MULTI = false: one job whose scene and render constants come in as kernel
 // parameters (constant bank); MULTI = true: per-ray job slot into the table.
 // ENV = false drops the environment-map code (misses, environment NEE) for
-// scenes without one, so they keep the smaller kernel.
-template <bool MULTI, bool ENV>
+// scenes without one, MED = false the participating-medium branch for scenes
+// without media, so those scenes run a smaller kernel (instruction fetch is
+// this kernel's main stall).
+template <bool MULTI, bool ENV, bool MED>
 __global__ void __launch_bounds__(256) k_shade(DevScene S0, DevRender R0, const DevJob* __restrict__ jobs, DevQueues Q,
                                                int iter) {
   const int count = Q.counters[iter * kCountersPerIter + C_RAYS];
@@ -797,7 +799,7 @@ __global__ void __launch_bounds__(256) k_shade(DevScene S0, DevRender R0, const 
       bool done = false;
       bool silhouette = false;
       // ---- participating medium on the segment (tracePath, rayrenderer.cpp:1665-1831)
-      const bool medActive = med >= 0 && S.media[med].hero > 0.0f;
+      const bool medActive = MED && med >= 0 && S.media[med].hero > 0.0f;
       if (medActive) {
         const DevMedium M = S.media[med];
         const float maxT = prim >= 0 ? hq.x : kRayMaxDistance;
@@ -1440,9 +1442,15 @@ void launchExtend(const DevScene* single, const DevJob* jobs, int width, const D
 }
 void launchShade(const DevScene* single, const DevRender* singleR, const DevJob* jobs, const DevQueues& Q, int iter,
                  int grid, cudaStream_t st) {
-  if (single && single->envTex < 0) k_shade<false, false><<<grid, 256, 0, st>>>(*single, *singleR, jobs, Q, iter);
-  else if (single) k_shade<false, true><<<grid, 256, 0, st>>>(*single, *singleR, jobs, Q, iter);
-  else k_shade<true, true><<<grid, 256, 0, st>>>(DevScene{}, DevRender{}, jobs, Q, iter);
+  if (!single) {
+    k_shade<true, true, true><<<grid, 256, 0, st>>>(DevScene{}, DevRender{}, jobs, Q, iter);
+    return;
+  }
+  const bool env = single->envTex >= 0, med = single->numMedia > 0;
+  if (!env && !med) k_shade<false, false, false><<<grid, 256, 0, st>>>(*single, *singleR, jobs, Q, iter);
+  else if (!env) k_shade<false, false, true><<<grid, 256, 0, st>>>(*single, *singleR, jobs, Q, iter);
+  else if (!med) k_shade<false, true, false><<<grid, 256, 0, st>>>(*single, *singleR, jobs, Q, iter);
+  else k_shade<false, true, true><<<grid, 256, 0, st>>>(*single, *singleR, jobs, Q, iter);
 }
 void launchConnect(const DevScene* single, const DevJob* jobs, int width, const DevQueues& Q, int iter, int which,
                    int grid, cudaStream_t st) {
