@@ -263,6 +263,13 @@ rg_status rg_tonemap(int32_t w, int32_t h, const float* hdr_rgba, float* ldr_rgb
 rg_status rg_bloom(int32_t w, int32_t h, const float* hdr_rgba, float threshold, float strength, float radius,
                    float size_aspect, float curve, float* out_rgba);
 
+/* Tensor-core (tcgen05) BF16 GEMM of the learned denoiser, exposed for tests:
+ * D[M x N] = A[M x K] * B[N x K]^T with FP32 accumulation; A, B row-major
+ * BF16 bit patterns (K contiguous), D row-major FP32, host pointers.
+ * N in 16..128 and K in 16..256, both multiples of 16.  No reference
+ * counterpart (the reference has no learned denoiser). */
+rg_status rg_tc_gemm_bf16(int32_t M, int32_t N, int32_t K, const uint16_t* A, const uint16_t* B, float* D);
+
 /* Procedural scenes (host C++, no device work).
  * kind 1: cube room (10 walls, two boxes, one 2.5x2.5 ceiling light).
  * kind 2: displaced icosphere x4 in a 20x20 room with 16 ceiling lights;

@@ -205,6 +205,7 @@ def load_library(path: str = LIB_PATH) -> C.CDLL:
         "rg_tonemap": (C.c_int, [C.c_int32, C.c_int32, P(C.c_float), P(C.c_float)]),
         "rg_bloom": (C.c_int, [C.c_int32, C.c_int32, P(C.c_float)] + [C.c_float] * 5 + [P(C.c_float)]),
         "rg_save_image": (C.c_int, [C.c_char_p, C.c_int32, C.c_int32, P(C.c_float)]),
+        "rg_tc_gemm_bf16": (C.c_int, [C.c_int32, C.c_int32, C.c_int32, P(C.c_uint16), P(C.c_uint16), P(C.c_float)]),
         "rg_reapply_postprocess": (C.c_int, [C.c_void_p]),
         "rg_scene_builtin": (C.c_int, [C.c_int32, C.c_uint32, P(C.c_int32), C.c_int32, P(P(rg_scene_desc))]),
         "rg_scene_free": (C.c_int, [P(rg_scene_desc)]),
@@ -575,6 +576,30 @@ def save_image(path: str, rgba: np.ndarray) -> None:
     lib = load_library()
     a = np.ascontiguousarray(rgba, np.float32)
     _check(lib.rg_save_image(path.encode(), a.shape[1], a.shape[0], _fptr(a)))
+
+
+def to_bf16_bits(a: np.ndarray) -> np.ndarray:
+    """float32 -> BF16 bit patterns (uint16), round to nearest even."""
+    u = np.ascontiguousarray(a, np.float32).view(np.uint32).astype(np.uint64)
+    r = ((u + 0x7FFF + ((u >> 16) & 1)) >> 16).astype(np.uint16)
+    return r
+
+
+def from_bf16_bits(b: np.ndarray) -> np.ndarray:
+    return (np.asarray(b, np.uint16).astype(np.uint32) << 16).view(np.float32)
+
+
+def tc_gemm_bf16(A: np.ndarray, B: np.ndarray) -> np.ndarray:
+    """Tensor-core BF16 GEMM (tcgen05, FP32 accumulation): A (M x K) @ B (N x K)^T."""
+    lib = load_library()
+    a = np.ascontiguousarray(to_bf16_bits(A))
+    b = np.ascontiguousarray(to_bf16_bits(B))
+    M, K = a.shape
+    N = b.shape[0]
+    d = np.empty((M, N), np.float32)
+    P16 = C.POINTER(C.c_uint16)
+    _check(lib.rg_tc_gemm_bf16(M, N, K, a.ctypes.data_as(P16), b.ctypes.data_as(P16), _fptr(d)))
+    return d
 
 
 def tonemap(hdr_rgba: np.ndarray) -> np.ndarray:
