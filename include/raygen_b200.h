@@ -270,6 +270,38 @@ rg_status rg_bloom(int32_t w, int32_t h, const float* hdr_rgba, float threshold,
  * counterpart (the reference has no learned denoiser). */
 rg_status rg_tc_gemm_bf16(int32_t M, int32_t N, int32_t K, const uint16_t* A, const uint16_t* B, float* D);
 
+/* ---- learned denoiser (kernel-predicting CNN on the tensor cores) --------
+ * No reference counterpart: the reference denoises with A-Trous only, which
+ * stays the renderer's default and its fallback.  Six 3x3 convolutions (10
+ * input features: log radiance, albedo, normal and depth guides; 32 channels)
+ * predict a 5x5 filter per pixel that is applied to the noisy radiance.
+ * Convolutions run forward and backward as BF16 tcgen05 GEMMs with FP32
+ * accumulation; training (relMSE loss against a high-spp render, Adam) runs
+ * on the device.  Images: noisy/ref w*h RGBA floats, normal and albedo w*h*3
+ * floats as returned by rg_get_aovs (normal * 0.5 + 0.5), depth w*h floats. */
+typedef struct rg_denoiser rg_denoiser;
+int32_t rg_denoiser_num_params(void);
+/* He-initialised weights from `seed`. */
+rg_status rg_denoiser_create(uint32_t seed, rg_denoiser** out);
+rg_status rg_denoiser_destroy(rg_denoiser* d);
+rg_status rg_denoiser_get_params(rg_denoiser* d, float* out, size_t n);
+rg_status rg_denoiser_set_params(rg_denoiser* d, const float* in, size_t n);
+/* Training pairs (all of one size) kept on the device. */
+rg_status rg_denoiser_add_example(rg_denoiser* d, int32_t w, int32_t h, const float* noisy_rgba, const float* normal,
+                                  const float* albedo, const float* depth, const float* ref_rgba);
+rg_status rg_denoiser_clear_examples(rg_denoiser* d);
+/* `steps` Adam steps on random batches of `batch` examples; losses[steps] (may be NULL). */
+rg_status rg_denoiser_train(rg_denoiser* d, int32_t steps, int32_t batch, float lr, float* losses);
+/* Loss and gradient (rg_denoiser_num_params floats) on `count` images of w x h. */
+rg_status rg_denoiser_gradients(rg_denoiser* d, int32_t count, int32_t w, int32_t h, const float* noisy_rgba,
+                                const float* normal, const float* albedo, const float* depth, const float* ref_rgba,
+                                float* loss, float* grad);
+rg_status rg_denoiser_apply(rg_denoiser* d, int32_t w, int32_t h, const float* noisy_rgba, const float* normal,
+                            const float* albedo, const float* depth, float* out_rgba);
+/* Use `d` instead of A-Trous when enable_denoise is set (NULL: back to A-Trous).
+ * The handle keeps the pointer; destroy `d` only after detaching it. */
+rg_status rg_set_denoiser(rg_handle* h, rg_denoiser* d);
+
 /* Procedural scenes (host C++, no device work).
  * kind 1: cube room (10 walls, two boxes, one 2.5x2.5 ceiling light).
  * kind 2: displaced icosphere x4 in a 20x20 room with 16 ceiling lights;

@@ -206,6 +206,17 @@ def load_library(path: str = LIB_PATH) -> C.CDLL:
         "rg_bloom": (C.c_int, [C.c_int32, C.c_int32, P(C.c_float)] + [C.c_float] * 5 + [P(C.c_float)]),
         "rg_save_image": (C.c_int, [C.c_char_p, C.c_int32, C.c_int32, P(C.c_float)]),
         "rg_tc_gemm_bf16": (C.c_int, [C.c_int32, C.c_int32, C.c_int32, P(C.c_uint16), P(C.c_uint16), P(C.c_float)]),
+        "rg_denoiser_num_params": (C.c_int32, []),
+        "rg_denoiser_create": (C.c_int, [C.c_uint32, P(C.c_void_p)]),
+        "rg_denoiser_destroy": (C.c_int, [C.c_void_p]),
+        "rg_denoiser_get_params": (C.c_int, [C.c_void_p, P(C.c_float), C.c_size_t]),
+        "rg_denoiser_set_params": (C.c_int, [C.c_void_p, P(C.c_float), C.c_size_t]),
+        "rg_denoiser_add_example": (C.c_int, [C.c_void_p, C.c_int32, C.c_int32] + [P(C.c_float)] * 5),
+        "rg_denoiser_clear_examples": (C.c_int, [C.c_void_p]),
+        "rg_denoiser_train": (C.c_int, [C.c_void_p, C.c_int32, C.c_int32, C.c_float, P(C.c_float)]),
+        "rg_denoiser_gradients": (C.c_int, [C.c_void_p, C.c_int32, C.c_int32, C.c_int32] + [P(C.c_float)] * 7),
+        "rg_denoiser_apply": (C.c_int, [C.c_void_p, C.c_int32, C.c_int32] + [P(C.c_float)] * 5),
+        "rg_set_denoiser": (C.c_int, [C.c_void_p, C.c_void_p]),
         "rg_reapply_postprocess": (C.c_int, [C.c_void_p]),
         "rg_scene_builtin": (C.c_int, [C.c_int32, C.c_uint32, P(C.c_int32), C.c_int32, P(P(rg_scene_desc))]),
         "rg_scene_free": (C.c_int, [P(rg_scene_desc)]),
@@ -472,6 +483,11 @@ class RayRenderer:
     def _size(self):
         return self.settings.resolutionHeight, self.settings.resolutionWidth
 
+    def set_denoiser(self, denoiser) -> None:
+        """Use a trained Denoiser when enableDenoise is set (None: back to A-Trous)."""
+        self._denoiser = denoiser  # keep it alive while attached
+        _check(self._lib.rg_set_denoiser(self._h, denoiser._h if denoiser is not None else None))
+
     def reapply_post_process(self) -> None:
         """RayRenderer::reapplyPostProcess: bloom + tonemap again from the last pre-bloom HDR
         with the current settings (e.g. after changing bloomStrength)."""
@@ -600,6 +616,90 @@ def tc_gemm_bf16(A: np.ndarray, B: np.ndarray) -> np.ndarray:
     P16 = C.POINTER(C.c_uint16)
     _check(lib.rg_tc_gemm_bf16(M, N, K, a.ctypes.data_as(P16), b.ctypes.data_as(P16), _fptr(d)))
     return d
+
+
+class Denoiser:
+    """Learned denoiser: a kernel-predicting CNN trained and run on the tensor cores.
+
+    Images are H x W (x C) float arrays: noisy / ref RGBA, normal and albedo guides
+    (as RayRenderer.get_aovs returns them), depth guide H x W.  Batched calls take
+    N x H x W (x C) arrays."""
+
+    def __init__(self, seed: int = 0, params=None):
+        self._lib = load_library()
+        h = C.c_void_p()
+        _check(self._lib.rg_denoiser_create(int(seed) & 0xFFFFFFFF, C.byref(h)))
+        self._h = h
+        if params is not None:
+            self.params = params
+
+    @staticmethod
+    def num_params() -> int:
+        return int(load_library().rg_denoiser_num_params())
+
+    @property
+    def params(self) -> np.ndarray:
+        out = np.empty(self.num_params(), np.float32)
+        _check(self._lib.rg_denoiser_get_params(self._h, _fptr(out), out.size))
+        return out
+
+    @params.setter
+    def params(self, p) -> None:
+        a = np.ascontiguousarray(p, np.float32).ravel()
+        _check(self._lib.rg_denoiser_set_params(self._h, _fptr(a), a.size))
+
+    def save(self, path: str) -> None:
+        self.params.tofile(path)
+
+    def load(self, path: str) -> None:
+        self.params = np.fromfile(path, np.float32)
+
+    @staticmethod
+    def _f(a, shape_tail):
+        return np.ascontiguousarray(a, np.float32)
+
+    def add_example(self, noisy, normal, albedo, depth, ref) -> None:
+        noisy, normal, albedo, depth, ref = (np.ascontiguousarray(a, np.float32) for a in (noisy, normal, albedo, depth, ref))
+        h, w = depth.shape
+        _check(self._lib.rg_denoiser_add_example(self._h, w, h, _fptr(noisy), _fptr(normal), _fptr(albedo),
+                                                 _fptr(depth), _fptr(ref)))
+
+    def clear_examples(self) -> None:
+        _check(self._lib.rg_denoiser_clear_examples(self._h))
+
+    def train(self, steps: int, batch: int = 8, lr: float = 1e-3) -> np.ndarray:
+        losses = np.zeros(max(1, steps), np.float32)
+        _check(self._lib.rg_denoiser_train(self._h, steps, batch, lr, _fptr(losses)))
+        return losses[:steps]
+
+    def gradients(self, noisy, normal, albedo, depth, ref):
+        """(loss, gradient) for a batch N x H x W (relMSE against ref)."""
+        noisy, normal, albedo, depth, ref = (np.ascontiguousarray(a, np.float32) for a in (noisy, normal, albedo, depth, ref))
+        n, h, w = depth.shape
+        loss = np.zeros(1, np.float32)
+        grad = np.zeros(self.num_params(), np.float32)
+        _check(self._lib.rg_denoiser_gradients(self._h, n, w, h, _fptr(noisy), _fptr(normal), _fptr(albedo),
+                                               _fptr(depth), _fptr(ref), _fptr(loss), _fptr(grad)))
+        return float(loss[0]), grad
+
+    def apply(self, noisy, normal, albedo, depth) -> np.ndarray:
+        noisy, normal, albedo, depth = (np.ascontiguousarray(a, np.float32) for a in (noisy, normal, albedo, depth))
+        h, w = depth.shape
+        out = np.empty((h, w, 4), np.float32)
+        _check(self._lib.rg_denoiser_apply(self._h, w, h, _fptr(noisy), _fptr(normal), _fptr(albedo), _fptr(depth),
+                                           _fptr(out)))
+        return out
+
+    def close(self) -> None:
+        if getattr(self, "_h", None):
+            self._lib.rg_denoiser_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 def tonemap(hdr_rgba: np.ndarray) -> np.ndarray:

@@ -136,6 +136,7 @@ struct rg_handle {
   // render buffers
   DevBuf<float4> sum, sumSq, hdr, ldr, bufA, bufB;
   DevBuf<float4> preBloom, bloomA, bloomB;  // HDR before bloom (reapply), glow buffers
+  rg_denoiser* denoiser = nullptr;           // learned denoiser (NULL: A-Trous)
   DevBuf<float> bloomW;                     // Gaussian taps
   DevBuf<int> cnt, pixelList, listCount;
   DevBuf<__half> aovNormal, aovAlbedo, aovAlbedoA, aovDepth;
@@ -383,6 +384,13 @@ rg_status rg_update_settings(rg_handle* h, const rg_settings* s) {
   if (!h || !s) return RG_ERR_INVALID_ARGUMENT;
   std::lock_guard<std::mutex> lk(h->mu);
   h->st = *s;
+  return RG_OK;
+}
+
+rg_status rg_set_denoiser(rg_handle* h, rg_denoiser* d) {
+  if (!h) return RG_ERR_INVALID_ARGUMENT;
+  std::lock_guard<std::mutex> lk(h->mu);
+  h->denoiser = d;
   return RG_OK;
 }
 
@@ -940,7 +948,18 @@ rg_status rg_render(rg_handle* h) {
     return rs;
   }
   launchResolve(N, h->sum.p, h->cnt.p, h->camera.exposure, h->hdr.p, st);
-  if (s.enable_denoise) {
+  if (s.enable_denoise && h->denoiser) {
+    const rg_status ds = kpcnDenoiseDevice(*kpcnOf(h->denoiser), W, H, h->hdr.p, h->aovNormal.p, h->aovAlbedo.p,
+                                           h->aovDepth.p, s.denoise_intensity, h->ldr.p, st);
+    if (ds != RG_OK) {
+      cudaStreamSynchronize(st);
+      cudaEventDestroy(t0);
+      cudaEventDestroy(t1);
+      cudaEventDestroy(t2);
+      return ds;
+    }
+    RG_CUDA_CHECK(cudaMemcpyAsync(h->hdr.p, h->ldr.p, sizeof(float4) * N, cudaMemcpyDeviceToDevice, st));
+  } else if (s.enable_denoise) {
     launchDenoise(W, H, h->hdr.p, h->aovNormal.p, h->aovDepth.p, h->aovAlbedo.p, h->aovAlbedoA.p, s.denoise_levels,
                   s.denoise_sigma_color, s.denoise_sigma_normal, s.denoise_sigma_depth, s.denoise_intensity, h->bufA.p,
                   h->bufB.p, h->ldr.p, st);

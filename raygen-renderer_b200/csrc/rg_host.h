@@ -1,5 +1,6 @@
 // rg_host.h - host-side internals of the B200 tracer (not part of the C ABI).
 #pragma once
+#include <cuda_fp16.h>
 #include <cuda_runtime.h>
 
 #include <atomic>
@@ -138,6 +139,13 @@ struct DeviceScene {
 };
 
 rg_status buildDeviceBvh(DeviceScene& ds, int nbins, bool wide, cudaStream_t st, std::string& err);
+
+// Learned denoiser (rg_kpcn.cu): inference on device buffers (noisy HDR and the
+// renderer's half guides), blended with the noisy image by `intensity`.
+struct KpcnNet;
+KpcnNet* kpcnOf(rg_denoiser* d);
+rg_status kpcnDenoiseDevice(KpcnNet& n, int W, int H, const float4* noisy, const __half* normal, const __half* albedo,
+                            const __half* depth, float intensity, float4* out, cudaStream_t st);
 rg_status prepareScene(const rg_scene_desc* d, int bins, bool wide, cudaStream_t st, int* errWord,
                        std::unique_ptr<DeviceScene>& out, DevScene& S, Mat4& view, float* buildMs);
 

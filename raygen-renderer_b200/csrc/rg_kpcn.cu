@@ -1,13 +1,34 @@
 // rg_kpcn.cu - learned denoiser: a kernel-predicting CNN on the 5th-generation
 // tensor cores (tcgen05, BF16 operands, FP32 accumulation in tensor memory).
 //
-// This part: the tensor-core GEMM building block and its stand-alone test
-// entry point.  The convolution passes (forward, backward data, backward
-// weights) stage their operands with their own gathers around the same block.
+// Network (after Bako et al. 2017, kernel-predicting convolutional networks
+// for Monte Carlo denoising): features [P x 16] = log1p(radiance), albedo,
+// normal and depth guides (the A-Trous guides, rayrenderer.cpp:819-844) and 6
+// zero channels; five 3x3 convolutions with ReLU (16 -> 32, then 32 -> 32);
+// a 3x3 convolution to 25 logits; softmax -> a 5 x 5 kernel per pixel applied
+// to the noisy radiance (clamp to edge).  Loss: relMSE (o - r)^2 / (r^2 + 0.01).
+//
+// Every convolution pass is an implicit GEMM on the tensor-core block of
+// rg_tc.cuh (M = 128 rows, N = 32, K a multiple of 16):
+//   forward        rows = pixels, K = (tap, input channel), B = weights;
+//   backward data  rows = pixels, K = (tap, output channel) of the gradient
+//                  gathered at p - offset, B = transposed weights, ReLU mask
+//                  of the layer input applied in the epilogue;
+//   backward wt.   rows = (tap, input channel), K = pixels (a chunk of 2048
+//                  per CTA, 128 at a time), B = the output gradient;
+//                  per-chunk partials reduced in chunk order (deterministic).
+// Activations and gradients are stored BF16 (NHWC, channels contiguous),
+// master weights and Adam moments FP32.  Softmax, kernel application, loss,
+// bias gradients and Adam run on the CUDA cores.
 #include <cuda_bf16.h>
+#include <cuda_fp16.h>
 #include <cuda_runtime.h>
 
+#include <algorithm>
+#include <cmath>
 #include <cstring>
+#include <memory>
+#include <random>
 #include <string>
 #include <vector>
 
@@ -78,6 +99,454 @@ __global__ void __launch_bounds__(128) k_tcGemm(int M, int N, int K, const __nv_
   if (warp == 0) tc::tmemFree(tmem, cols);
 }
 
+
+// ---------------------------------------------------------------- network --
+constexpr int kC = 32;          // hidden channels (and padded logits)
+constexpr int kKP = 25;         // predicted kernel taps (5 x 5)
+constexpr int kLayers = 6;
+__host__ __device__ constexpr int cinOf(int l) { return l == 0 ? 16 : 32; }  // 16, 32, 32, 32, 32, 32
+constexpr int kChunk = 2048;    // pixels per backward-weight CTA
+constexpr int kSub = 128;       // pixels per backward-weight staging step
+constexpr float kLossEps = 0.01f;
+
+__host__ __device__ constexpr int layerWeights(int l) { return kC * 9 * cinOf(l); }
+__host__ __device__ constexpr int layerOffset(int l) {
+  int o = 0;
+  for (int i = 0; i < l; ++i) o += layerWeights(i) + kC;
+  return o;
+}
+constexpr int kNumParams = layerOffset(kLayers);
+
+// (b, y, x) of pixel p in a batch of H x W images, neighbour at (dy, dx) or -1
+__device__ __forceinline__ int neighbor(int p, int dy, int dx, int H, int W) {
+  const int x = p % W, t = p / W, y = t % H, b = t / H;
+  const int yy = y + dy, xx = x + dx;
+  if (yy < 0 || yy >= H || xx < 0 || xx >= W) return -1;
+  return (b * H + yy) * W + xx;
+}
+
+__device__ __forceinline__ int clampNeighbor(int p, int dy, int dx, int H, int W) {
+  const int x = p % W, t = p / W, y = t % H, b = t / H;
+  const int yy = min(max(y + dy, 0), H - 1), xx = min(max(x + dx, 0), W - 1);
+  return (b * H + yy) * W + xx;
+}
+
+template <typename T>
+__device__ __forceinline__ float loadf(const T* p, size_t i);
+template <>
+__device__ __forceinline__ float loadf<float>(const float* p, size_t i) { return p[i]; }
+template <>
+__device__ __forceinline__ float loadf<__half>(const __half* p, size_t i) { return __half2float(p[i]); }
+
+// Features: X0[p] = (log1p(max(rgb, 0)), albedo, normal guide, depth guide, 0 x 6), BF16.
+template <typename T>
+__global__ void k_features(int P, const float4* __restrict__ noisy, const T* __restrict__ normal,
+                           const T* __restrict__ albedo, const T* __restrict__ depth, __nv_bfloat16* __restrict__ X0) {
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= P) return;
+  const float4 c = noisy[p];
+  float f[16];
+  f[0] = log1pf(fmaxf(c.x, 0.0f));
+  f[1] = log1pf(fmaxf(c.y, 0.0f));
+  f[2] = log1pf(fmaxf(c.z, 0.0f));
+  for (int k = 0; k < 3; ++k) {
+    f[3 + k] = loadf(albedo, (size_t)p * 3 + k);
+    f[6 + k] = loadf(normal, (size_t)p * 3 + k);
+  }
+  f[9] = loadf(depth, (size_t)p);
+  for (int k = 10; k < 16; ++k) f[k] = 0.0f;
+  __align__(16) __nv_bfloat16 o[16];
+  for (int k = 0; k < 16; ++k) o[k] = __float2bfloat16_rn(f[k]);
+  uint4* dst = reinterpret_cast<uint4*>(X0 + (size_t)p * 16);
+  dst[0] = reinterpret_cast<const uint4*>(o)[0];
+  dst[1] = reinterpret_cast<const uint4*>(o)[1];
+}
+
+// Forward convolution.  LAST = false: Y = bf16(relu(conv + b)); LAST = true:
+// Z = conv + b in FP32 (the logits).  Persistent: each CTA walks 128-pixel tiles.
+template <int CIN, bool LAST>
+__global__ void __launch_bounds__(128) k_convFwd(int B, int H, int W, const __nv_bfloat16* __restrict__ X,
+                                                 const __nv_bfloat16* __restrict__ Wk, const float* __restrict__ bias,
+                                                 __nv_bfloat16* __restrict__ Y, float* __restrict__ Z,
+                                                 int* __restrict__ err) {
+  constexpr int K = 9 * CIN, KC = K / 8, CC = CIN / 8;
+  extern __shared__ __align__(1024) unsigned char sm[];
+  __shared__ uint64_t bar;
+  __shared__ uint32_t tbase;
+  unsigned char* sA = sm;
+  unsigned char* sB = sm + (size_t)128 * K * 2;
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int P = B * H * W, tiles = (P + 127) / 128;
+  if (warp == 0) tc::tmemAlloc(&tbase, 32);
+  if (tid == 0) tc::mbarInit(&bar, 1);
+  for (int c = tid; c < kC * KC; c += 128) {
+    const int r = c / KC, q = c % KC;
+    *reinterpret_cast<uint4*>(sB + tc::chunkOffset(r, q, K)) = *reinterpret_cast<const uint4*>(Wk + (size_t)r * K + q * 8);
+  }
+  float bv[kC];
+#pragma unroll
+  for (int j = 0; j < kC; ++j) bv[j] = bias[j];
+  __syncthreads();
+  const uint32_t tmem = tbase;
+  const uint32_t idesc = tc::instrDescBf16(128, kC);
+  uint32_t phase = 0;
+  bool ok = true;
+  for (int tile = blockIdx.x; tile < tiles; tile += gridDim.x) {
+    const int p0 = tile * 128;
+    for (int c = tid; c < 128 * 9 * CC; c += 128) {
+      const int r = c / (9 * CC), rem = c % (9 * CC), t = rem / CC, q = rem % CC;
+      const int p = p0 + r;
+      uint4 v = make_uint4(0, 0, 0, 0);
+      if (p < P) {
+        const int n = neighbor(p, t / 3 - 1, t % 3 - 1, H, W);
+        if (n >= 0) v = *reinterpret_cast<const uint4*>(X + (size_t)n * CIN + q * 8);
+      }
+      *reinterpret_cast<uint4*>(sA + tc::chunkOffset(r, t * CC + q, K)) = v;
+    }
+    tc::fenceProxyAsync();
+    __syncthreads();
+    tc::fenceAfterSync();
+    if (tid == 0) {
+      const uint32_t aBase = tc::smemAddr(sA), bBase = tc::smemAddr(sB);
+      for (int s = 0; s < K / 16; ++s)
+        tc::mmaBf16(tmem, tc::smemDesc(aBase + s * 256, 128, KC * 128), tc::smemDesc(bBase + s * 256, 128, KC * 128),
+                    idesc, s > 0);
+      tc::commit(&bar);
+    }
+    ok = __syncthreads_and(tc::mbarWait(&bar, phase)) != 0;
+    phase ^= 1u;
+    tc::fenceAfterSync();
+    if (!ok) break;
+    float v[32];
+    tc::tmemLoad32(tmem + ((uint32_t)(warp * 32) << 16), v);
+    const int p = p0 + warp * 32 + lane;
+    if (p < P) {
+      if (LAST) {
+        float4* z = reinterpret_cast<float4*>(Z + (size_t)p * kC);
+#pragma unroll
+        for (int j = 0; j < kC; j += 4) z[j / 4] = make_float4(v[j] + bv[j], v[j + 1] + bv[j + 1], v[j + 2] + bv[j + 2], v[j + 3] + bv[j + 3]);
+      } else {
+        __align__(16) __nv_bfloat16 o[kC];
+#pragma unroll
+        for (int j = 0; j < kC; ++j) o[j] = __float2bfloat16_rn(fmaxf(v[j] + bv[j], 0.0f));
+        uint4* y = reinterpret_cast<uint4*>(Y + (size_t)p * kC);
+#pragma unroll
+        for (int j = 0; j < 4; ++j) y[j] = reinterpret_cast<const uint4*>(o)[j];
+      }
+    }
+    tc::fenceBeforeSync();
+    __syncthreads();
+  }
+  if (!ok) {
+    if (tid == 0) atomicCAS(err, 0, tc::kErrTcTimeout);
+    tc::mbarWait(&bar, phase ^ 1u);
+  }
+  tc::fenceBeforeSync();
+  __syncthreads();
+  if (warp == 0) tc::tmemFree(tmem, 32);
+}
+
+// Backward data of a 32 -> 32 (or 32 -> logits) convolution, fused with the
+// ReLU mask of its input: Gprev[p][ci] = bf16(mask(Xin[p][ci]) * sum_{t,co}
+// G[p - off(t)][co] * W[co][t][ci]).  Wt = W transposed to [ci][(t, co)].
+__global__ void __launch_bounds__(128) k_convBwdData(int B, int H, int W, const __nv_bfloat16* __restrict__ G,
+                                                     const __nv_bfloat16* __restrict__ Wt,
+                                                     const __nv_bfloat16* __restrict__ Xin,
+                                                     __nv_bfloat16* __restrict__ Gprev, int* __restrict__ err) {
+  constexpr int K = 9 * kC, KC = K / 8, CC = kC / 8;
+  extern __shared__ __align__(1024) unsigned char sm[];
+  __shared__ uint64_t bar;
+  __shared__ uint32_t tbase;
+  unsigned char* sA = sm;
+  unsigned char* sB = sm + (size_t)128 * K * 2;
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int P = B * H * W, tiles = (P + 127) / 128;
+  if (warp == 0) tc::tmemAlloc(&tbase, 32);
+  if (tid == 0) tc::mbarInit(&bar, 1);
+  for (int c = tid; c < kC * KC; c += 128) {
+    const int r = c / KC, q = c % KC;
+    *reinterpret_cast<uint4*>(sB + tc::chunkOffset(r, q, K)) = *reinterpret_cast<const uint4*>(Wt + (size_t)r * K + q * 8);
+  }
+  __syncthreads();
+  const uint32_t tmem = tbase;
+  const uint32_t idesc = tc::instrDescBf16(128, kC);
+  uint32_t phase = 0;
+  bool ok = true;
+  for (int tile = blockIdx.x; tile < tiles; tile += gridDim.x) {
+    const int p0 = tile * 128;
+    for (int c = tid; c < 128 * 9 * CC; c += 128) {
+      const int r = c / (9 * CC), rem = c % (9 * CC), t = rem / CC, q = rem % CC;
+      const int p = p0 + r;
+      uint4 v = make_uint4(0, 0, 0, 0);
+      if (p < P) {
+        const int n = neighbor(p, -(t / 3 - 1), -(t % 3 - 1), H, W);
+        if (n >= 0) v = *reinterpret_cast<const uint4*>(G + (size_t)n * kC + q * 8);
+      }
+      *reinterpret_cast<uint4*>(sA + tc::chunkOffset(r, t * CC + q, K)) = v;
+    }
+    tc::fenceProxyAsync();
+    __syncthreads();
+    tc::fenceAfterSync();
+    if (tid == 0) {
+      const uint32_t aBase = tc::smemAddr(sA), bBase = tc::smemAddr(sB);
+      for (int s = 0; s < K / 16; ++s)
+        tc::mmaBf16(tmem, tc::smemDesc(aBase + s * 256, 128, KC * 128), tc::smemDesc(bBase + s * 256, 128, KC * 128),
+                    idesc, s > 0);
+      tc::commit(&bar);
+    }
+    ok = __syncthreads_and(tc::mbarWait(&bar, phase)) != 0;
+    phase ^= 1u;
+    tc::fenceAfterSync();
+    if (!ok) break;
+    float v[32];
+    tc::tmemLoad32(tmem + ((uint32_t)(warp * 32) << 16), v);
+    const int p = p0 + warp * 32 + lane;
+    if (p < P) {
+      __align__(16) __nv_bfloat16 xin[kC];
+      const uint4* xs = reinterpret_cast<const uint4*>(Xin + (size_t)p * kC);
+#pragma unroll
+      for (int j = 0; j < 4; ++j) reinterpret_cast<uint4*>(xin)[j] = xs[j];
+      __align__(16) __nv_bfloat16 o[kC];
+#pragma unroll
+      for (int j = 0; j < kC; ++j) o[j] = __float2bfloat16_rn(__bfloat162float(xin[j]) > 0.0f ? v[j] : 0.0f);
+      uint4* y = reinterpret_cast<uint4*>(Gprev + (size_t)p * kC);
+#pragma unroll
+      for (int j = 0; j < 4; ++j) y[j] = reinterpret_cast<const uint4*>(o)[j];
+    }
+    tc::fenceBeforeSync();
+    __syncthreads();
+  }
+  if (!ok) {
+    if (tid == 0) atomicCAS(err, 0, tc::kErrTcTimeout);
+    tc::mbarWait(&bar, phase ^ 1u);
+  }
+  tc::fenceBeforeSync();
+  __syncthreads();
+  if (warp == 0) tc::tmemFree(tmem, 32);
+}
+
+// Backward weights: partial[chunk][m = (t, ci)][co] = sum over the chunk's
+// pixels q of X[q + off(t)][ci] * G[q][co].  Grid: (M tiles of 128 rows,
+// pixel chunks).  Rows beyond 9 * CIN are zero.
+template <int CIN>
+__global__ void __launch_bounds__(128) k_convBwdWeight(int B, int H, int W, const __nv_bfloat16* __restrict__ X,
+                                                       const __nv_bfloat16* __restrict__ G, float* __restrict__ partial,
+                                                       int* __restrict__ err) {
+  constexpr int M = 9 * CIN;
+  __shared__ __align__(1024) unsigned char sA[128 * kSub * 2];
+  __shared__ __align__(1024) unsigned char sB[kC * kSub * 2];
+  __shared__ uint64_t bar;
+  __shared__ uint32_t tbase;
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int P = B * H * W;
+  const int mt = blockIdx.x, chunk = blockIdx.y;
+  const int m0 = mt * 128;
+  if (warp == 0) tc::tmemAlloc(&tbase, 32);
+  if (tid == 0) tc::mbarInit(&bar, 1);
+  __syncthreads();
+  const uint32_t tmem = tbase;
+  const uint32_t idesc = tc::instrDescBf16(128, kC);
+  uint32_t phase = 0;
+  bool ok = true;
+  for (int sub = 0; sub < kChunk / kSub; ++sub) {
+    const int q0 = chunk * kChunk + sub * kSub;
+    if (q0 >= P) break;
+    // thread tid stages pixel q = q0 + tid: its column in A (all rows of this tile) and in B
+    const int q = q0 + tid;
+    const int kcol = tid;
+    auto put = [&](unsigned char* base, int row, __nv_bfloat16 val) {
+      *reinterpret_cast<__nv_bfloat16*>(base + tc::chunkOffset(row, kcol >> 3, kSub) + (kcol & 7) * 2) = val;
+    };
+    for (int r = 0; r < 128; r += CIN) {  // one tap (CIN rows) at a time
+      const int m = m0 + r, t = m / CIN;
+      __align__(16) __nv_bfloat16 xv[CIN];
+#pragma unroll
+      for (int j = 0; j < CIN; ++j) xv[j] = __float2bfloat16_rn(0.0f);
+      if (m < M && q < P) {
+        const int n = neighbor(q, t / 3 - 1, t % 3 - 1, H, W);
+        if (n >= 0) {
+          const uint4* src = reinterpret_cast<const uint4*>(X + (size_t)n * CIN);
+#pragma unroll
+          for (int j = 0; j < CIN / 8; ++j) reinterpret_cast<uint4*>(xv)[j] = src[j];
+        }
+      }
+#pragma unroll
+      for (int j = 0; j < CIN; ++j) put(sA, r + j, xv[j]);
+    }
+    {
+      __align__(16) __nv_bfloat16 gv[kC];
+#pragma unroll
+      for (int j = 0; j < kC; ++j) gv[j] = __float2bfloat16_rn(0.0f);
+      if (q < P) {
+        const uint4* src = reinterpret_cast<const uint4*>(G + (size_t)q * kC);
+#pragma unroll
+        for (int j = 0; j < 4; ++j) reinterpret_cast<uint4*>(gv)[j] = src[j];
+      }
+#pragma unroll
+      for (int j = 0; j < kC; ++j) put(sB, j, gv[j]);
+    }
+    tc::fenceProxyAsync();
+    __syncthreads();
+    tc::fenceAfterSync();
+    if (tid == 0) {
+      const uint32_t aBase = tc::smemAddr(sA), bBase = tc::smemAddr(sB);
+      for (int s = 0; s < kSub / 16; ++s)
+        tc::mmaBf16(tmem, tc::smemDesc(aBase + s * 256, 128, (kSub / 8) * 128),
+                    tc::smemDesc(bBase + s * 256, 128, (kSub / 8) * 128), idesc, sub > 0 || s > 0);
+      tc::commit(&bar);
+    }
+    ok = __syncthreads_and(tc::mbarWait(&bar, phase)) != 0;
+    phase ^= 1u;
+    tc::fenceAfterSync();
+    if (!ok) break;
+  }
+  if (ok) {
+    float v[32];
+    tc::tmemLoad32(tmem + ((uint32_t)(warp * 32) << 16), v);
+    const int m = m0 + warp * 32 + lane;
+    // a chunk that starts past the end of the batch contributes zeros
+    const bool any = chunk * kChunk < P;
+    if (m < M) {
+      float4* dst = reinterpret_cast<float4*>(partial + ((size_t)chunk * M + m) * kC);
+#pragma unroll
+      for (int j = 0; j < kC; j += 4)
+        dst[j / 4] = any ? make_float4(v[j], v[j + 1], v[j + 2], v[j + 3]) : make_float4(0.f, 0.f, 0.f, 0.f);
+    }
+  } else {
+    if (tid == 0) atomicCAS(err, 0, tc::kErrTcTimeout);
+    tc::mbarWait(&bar, phase ^ 1u);
+  }
+  tc::fenceBeforeSync();
+  __syncthreads();
+  if (warp == 0) tc::tmemFree(tmem, 32);
+}
+
+// grad W[co][t][ci] = sum over chunks (in order) of partial[chunk][(t, ci)][co].
+__global__ void k_reduceWeightGrad(int M, int chunks, const float* __restrict__ partial, float* __restrict__ gradW) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;  // over M * 32
+  if (i >= M * kC) return;
+  const int co = i / M, m = i % M;
+  float s = 0.0f;
+  for (int c = 0; c < chunks; ++c) s += partial[((size_t)c * M + m) * kC + co];
+  gradW[(size_t)co * M + m] = s;
+}
+
+// grad b[co] = sum_q G[q][co]: per-chunk partials, then an in-order reduction.
+__global__ void k_biasPartial(int P, const __nv_bfloat16* __restrict__ G, float* __restrict__ partial) {
+  const int chunk = blockIdx.x, co = threadIdx.x & 31, lane4 = threadIdx.x >> 5;  // 128 threads: 4 pixel lanes
+  __shared__ float acc[4][kC];
+  float s = 0.0f;
+  for (int q = chunk * kChunk + lane4; q < min(P, (chunk + 1) * kChunk); q += 4) s += __bfloat162float(G[(size_t)q * kC + co]);
+  acc[lane4][co] = s;
+  __syncthreads();
+  if (lane4 == 0) partial[(size_t)chunk * kC + co] = ((acc[0][co] + acc[1][co]) + acc[2][co]) + acc[3][co];
+}
+
+__global__ void k_reduceBiasGrad(int chunks, const float* __restrict__ partial, float* __restrict__ gradB) {
+  const int co = threadIdx.x;
+  if (co >= kC) return;
+  float s = 0.0f;
+  for (int c = 0; c < chunks; ++c) s += partial[(size_t)c * kC + co];
+  gradB[co] = s;
+}
+
+// Softmax + 5 x 5 kernel application.  TRAIN: also the relMSE loss and its
+// gradient with respect to the logits, G[p][0..24] (BF16), zero for the pad.
+template <bool TRAIN>
+__global__ void k_head(int B, int H, int W, const float* __restrict__ Z, const float4* __restrict__ noisy,
+                       const float4* __restrict__ ref, float4* __restrict__ out, __nv_bfloat16* __restrict__ G,
+                       float* __restrict__ lossSum) {
+  const int P = B * H * W;
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  float lp = 0.0f;
+  if (p < P) {
+    float w[kKP];
+    float mx = -3.0e38f;
+    const float* z = Z + (size_t)p * kC;
+#pragma unroll
+    for (int j = 0; j < kKP; ++j) {
+      w[j] = z[j];
+      mx = fmaxf(mx, w[j]);
+    }
+    float sum = 0.0f;
+#pragma unroll
+    for (int j = 0; j < kKP; ++j) {
+      w[j] = expf(w[j] - mx);
+      sum += w[j];
+    }
+    const float inv = 1.0f / sum;
+    float o0 = 0.0f, o1 = 0.0f, o2 = 0.0f;
+#pragma unroll
+    for (int j = 0; j < kKP; ++j) {
+      w[j] *= inv;
+      const float4 c = noisy[clampNeighbor(p, j / 5 - 2, j % 5 - 2, H, W)];
+      o0 += w[j] * c.x;
+      o1 += w[j] * c.y;
+      o2 += w[j] * c.z;
+    }
+    if (out) out[p] = make_float4(o0, o1, o2, 1.0f);
+    if (TRAIN) {
+      const float4 r = ref[p];
+      const float d0 = 1.0f / (r.x * r.x + kLossEps), d1 = 1.0f / (r.y * r.y + kLossEps),
+                  d2 = 1.0f / (r.z * r.z + kLossEps);
+      lp = (o0 - r.x) * (o0 - r.x) * d0 + (o1 - r.y) * (o1 - r.y) * d1 + (o2 - r.z) * (o2 - r.z) * d2;
+      const float sc = 2.0f / (3.0f * (float)P);
+      const float g0 = sc * (o0 - r.x) * d0, g1 = sc * (o1 - r.y) * d1, g2 = sc * (o2 - r.z) * d2;
+      float dw[kKP];
+      float dot = 0.0f;
+#pragma unroll
+      for (int j = 0; j < kKP; ++j) {
+        const float4 c = noisy[clampNeighbor(p, j / 5 - 2, j % 5 - 2, H, W)];
+        dw[j] = g0 * c.x + g1 * c.y + g2 * c.z;
+        dot += w[j] * dw[j];
+      }
+      __align__(16) __nv_bfloat16 gz[kC];
+#pragma unroll
+      for (int j = 0; j < kC; ++j) gz[j] = __float2bfloat16_rn(j < kKP ? w[j] * (dw[j] - dot) : 0.0f);
+      uint4* dst = reinterpret_cast<uint4*>(G + (size_t)p * kC);
+#pragma unroll
+      for (int j = 0; j < 4; ++j) dst[j] = reinterpret_cast<const uint4*>(gz)[j];
+    }
+  }
+  if (TRAIN) {
+    __shared__ float red[256];
+    red[threadIdx.x] = lp;
+    __syncthreads();
+    for (int s = blockDim.x / 2; s > 0; s >>= 1) {
+      if (threadIdx.x < s) red[threadIdx.x] += red[threadIdx.x + s];
+      __syncthreads();
+    }
+    if (threadIdx.x == 0) atomicAdd(lossSum, red[0] / (3.0f * (float)P));
+  }
+}
+
+// Adam (Kingma & Ba 2015) on the FP32 master parameters.
+__global__ void k_adam(int n, float* __restrict__ p, const float* __restrict__ g, float* __restrict__ m,
+                       float* __restrict__ v, float lr, float b1, float b2, float c1, float c2, float eps) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const float gi = g[i];
+  const float mi = b1 * m[i] + (1.0f - b1) * gi, vi = b2 * v[i] + (1.0f - b2) * gi * gi;
+  m[i] = mi;
+  v[i] = vi;
+  p[i] -= lr * (mi / c1) / (sqrtf(vi / c2) + eps);
+}
+
+// Master FP32 weights -> BF16 forward layout [co][(t, ci)] and the transposed
+// backward-data layout [ci][(t, co)] (32-channel inputs only).
+__global__ void k_packWeights(const float* __restrict__ params, __nv_bfloat16* __restrict__ wf,
+                              __nv_bfloat16* __restrict__ wt, int layer) {
+  const int cin = layer == 0 ? 16 : 32;
+  const int n = kC * 9 * cin;
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const float* W = params + layerOffset(layer);
+  const int co = i / (9 * cin), rem = i % (9 * cin), t = rem / cin, ci = rem % cin;
+  const __nv_bfloat16 b = __float2bfloat16_rn(W[i]);
+  wf[i] = b;
+  if (wt) wt[(size_t)ci * (9 * kC) + t * kC + co] = b;
+}
+
 }  // namespace
 
 }  // namespace rg
@@ -121,3 +590,398 @@ extern "C" rg_status rg_tc_gemm_bf16(int32_t M, int32_t N, int32_t K, const uint
   cudaMemcpy(D, d.p, sizeof(float) * (size_t)M * N, cudaMemcpyDeviceToHost);
   return RG_OK;
 }
+
+// ------------------------------------------------------------------ host --
+#define RG_CUDA_CHECK(call)                                              \
+  do {                                                                   \
+    cudaError_t e__ = (call);                                            \
+    if (e__ != cudaSuccess) {                                            \
+      setLastError(std::string(#call) + ": " + cudaGetErrorString(e__)); \
+      return RG_ERR_CUDA;                                                \
+    }                                                                    \
+  } while (0)
+
+namespace rg {
+
+namespace {
+// out = noisy * (1 - t) + denoised * t, t = clamp(intensity, 0, 1) (the blend of denoiseImage).
+__global__ void k_blend(int n, const float4* __restrict__ noisy, const float4* __restrict__ den, float intensity,
+                        float4* __restrict__ out) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const float t = fminf(fmaxf(intensity, 0.0f), 1.0f), s = 1.0f - t;
+  const float4 a = noisy[i], b = den[i];
+  out[i] = make_float4(a.x * s + b.x * t, a.y * s + b.y * t, a.z * s + b.z * t, 1.0f);
+}
+}  // namespace
+
+struct KpcnNet {
+  cudaStream_t st = nullptr;
+  int numSMs = 148;
+  DevBuf<float> params, grad, m, v;
+  DevBuf<__nv_bfloat16> wf[kLayers], wt[kLayers];
+  int adamStep = 0;
+  std::mt19937 rng;
+  // training examples (all W x H)
+  int dsW = 0, dsH = 0, dsN = 0;
+  std::vector<__nv_bfloat16*> exX;
+  std::vector<float4*> exNoisy, exRef;
+  // work buffers for P pixels
+  size_t cap = 0;
+  DevBuf<__nv_bfloat16> X0, act[kLayers - 1], gA, gB;
+  DevBuf<float> Z, partial, bpartial, loss;
+  DevBuf<float4> noisy, ref, out;
+  DevBuf<int> err;
+  ~KpcnNet() {
+    for (auto* p : exX) cudaFree(p);
+    for (auto* p : exNoisy) cudaFree(p);
+    for (auto* p : exRef) cudaFree(p);
+    if (st) cudaStreamDestroy(st);
+  }
+};
+
+namespace {
+
+int chunksFor(size_t P) { return (int)((P + kChunk - 1) / kChunk); }
+
+bool ensureWork(KpcnNet& n, size_t P) {
+  if (P <= n.cap) return true;
+  const int ch = chunksFor(P);
+  bool ok = n.X0.alloc(P * 16) && n.gA.alloc(P * kC) && n.gB.alloc(P * kC) && n.Z.alloc(P * kC) &&
+            n.partial.alloc((size_t)ch * 9 * kC * kC) && n.bpartial.alloc((size_t)ch * kC) && n.loss.alloc(1) &&
+            n.noisy.alloc(P) && n.ref.alloc(P) && n.out.alloc(P) && n.err.alloc(1);
+  for (int l = 0; l < kLayers - 1; ++l) ok = ok && n.act[l].alloc(P * kC);
+  if (ok) {
+    n.cap = P;
+    ok = cudaMemsetAsync(n.err.p, 0, sizeof(int), n.st) == cudaSuccess;  // the error word starts clear
+  }
+  return ok;
+}
+
+template <typename K>
+void setSmem(K kernel, size_t bytes) {
+  cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+}
+
+void packWeights(KpcnNet& n) {
+  for (int l = 0; l < kLayers; ++l) {
+    const int cnt = layerWeights(l);
+    k_packWeights<<<(cnt + 255) / 256, 256, 0, n.st>>>(n.params.p, n.wf[l].p, l > 0 ? n.wt[l].p : nullptr, l);
+  }
+}
+
+int persistentGrid(const KpcnNet& n, size_t P) {
+  const int tiles = (int)((P + 127) / 128);
+  return std::max(1, std::min(tiles, n.numSMs * 2));
+}
+
+// X0 must be filled; writes act[0..4] and Z.
+void forward(KpcnNet& n, int B, int H, int W) {
+  const size_t P = (size_t)B * H * W;
+  const int grid = persistentGrid(n, P);
+  const size_t smem16 = (size_t)(128 + kC) * 9 * 16 * 2, smem32 = (size_t)(128 + kC) * 9 * 32 * 2;
+  k_convFwd<16, false><<<grid, 128, smem16, n.st>>>(B, H, W, n.X0.p, n.wf[0].p, n.params.p + layerOffset(0) + layerWeights(0),
+                                                    n.act[0].p, nullptr, n.err.p);
+  for (int l = 1; l < kLayers - 1; ++l)
+    k_convFwd<32, false><<<grid, 128, smem32, n.st>>>(B, H, W, n.act[l - 1].p, n.wf[l].p,
+                                                      n.params.p + layerOffset(l) + layerWeights(l), n.act[l].p, nullptr,
+                                                      n.err.p);
+  k_convFwd<32, true><<<grid, 128, smem32, n.st>>>(B, H, W, n.act[kLayers - 2].p, n.wf[kLayers - 1].p,
+                                                   n.params.p + layerOffset(kLayers - 1) + layerWeights(kLayers - 1),
+                                                   nullptr, n.Z.p, n.err.p);
+}
+
+// Head gradient must be in gA; fills n.grad.
+void backward(KpcnNet& n, int B, int H, int W) {
+  const size_t P = (size_t)B * H * W;
+  const int ch = chunksFor(P);
+  const int grid = persistentGrid(n, P);
+  const size_t smem32 = (size_t)(128 + kC) * 9 * 32 * 2;
+  __nv_bfloat16* G = n.gA.p;
+  __nv_bfloat16* Gn = n.gB.p;
+  for (int l = kLayers - 1; l >= 0; --l) {
+    const __nv_bfloat16* in = l == 0 ? n.X0.p : n.act[l - 1].p;
+    const int M = 9 * cinOf(l);
+    const dim3 g((M + 127) / 128, ch);
+    if (l == 0) k_convBwdWeight<16><<<g, 128, 0, n.st>>>(B, H, W, in, G, n.partial.p, n.err.p);
+    else k_convBwdWeight<32><<<g, 128, 0, n.st>>>(B, H, W, in, G, n.partial.p, n.err.p);
+    k_reduceWeightGrad<<<(M * kC + 255) / 256, 256, 0, n.st>>>(M, ch, n.partial.p, n.grad.p + layerOffset(l));
+    k_biasPartial<<<ch, 128, 0, n.st>>>((int)P, G, n.bpartial.p);
+    k_reduceBiasGrad<<<1, 32, 0, n.st>>>(ch, n.bpartial.p, n.grad.p + layerOffset(l) + layerWeights(l));
+    if (l > 0) {
+      k_convBwdData<<<grid, 128, smem32, n.st>>>(B, H, W, G, n.wt[l].p, in, Gn, n.err.p);
+      std::swap(G, Gn);
+    }
+  }
+}
+
+rg_status checkErr(KpcnNet& n, const char* what) {
+  cudaError_t e = cudaGetLastError();
+  if (e == cudaSuccess) e = cudaStreamSynchronize(n.st);
+  if (e != cudaSuccess) {
+    setLastError(std::string(what) + ": " + cudaGetErrorString(e));
+    return RG_ERR_CUDA;
+  }
+  int flag = 0;
+  cudaMemcpy(&flag, n.err.p, sizeof(int), cudaMemcpyDeviceToHost);
+  if (flag) {
+    cudaMemset(n.err.p, 0, sizeof(int));  // reported once
+    setLastError(std::string(what) + ": tensor-core completion wait timed out");
+    return RG_ERR_DEVICE_STATUS;
+  }
+  return RG_OK;
+}
+
+bool initNet(KpcnNet& n, uint32_t seed) {
+  int dev = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&n.numSMs, cudaDevAttrMultiProcessorCount, dev);
+  if (cudaStreamCreateWithFlags(&n.st, cudaStreamNonBlocking) != cudaSuccess) return false;
+  n.rng.seed(seed);
+  bool ok = n.params.alloc(kNumParams) && n.grad.alloc(kNumParams) && n.m.alloc(kNumParams) && n.v.alloc(kNumParams);
+  for (int l = 0; l < kLayers && ok; ++l) {
+    ok = n.wf[l].alloc(layerWeights(l));
+    if (l > 0) ok = ok && n.wt[l].alloc(layerWeights(l));
+  }
+  if (!ok) return false;
+  // He-normal weights (fan-in 9 x input channels; 10 real inputs for layer 1),
+  // zero biases, the last layer scaled by 0.1 and its 7 padding logits zero.
+  std::vector<float> h(kNumParams, 0.0f);
+  std::normal_distribution<float> nd(0.0f, 1.0f);
+  for (int l = 0; l < kLayers; ++l) {
+    const int cin = cinOf(l), fan = 9 * (l == 0 ? 10 : cin);
+    const float sd = std::sqrt(2.0f / fan) * (l == kLayers - 1 ? 0.1f : 1.0f);
+    float* W = h.data() + layerOffset(l);
+    for (int co = 0; co < kC; ++co)
+      for (int t = 0; t < 9; ++t)
+        for (int ci = 0; ci < cin; ++ci) {
+          const bool pad = (l == 0 && ci >= 10) || (l == kLayers - 1 && co >= kKP);
+          W[(co * 9 + t) * cin + ci] = pad ? 0.0f : nd(n.rng) * sd;
+        }
+  }
+  cudaMemcpyAsync(n.params.p, h.data(), sizeof(float) * kNumParams, cudaMemcpyHostToDevice, n.st);
+  cudaMemsetAsync(n.m.p, 0, sizeof(float) * kNumParams, n.st);
+  cudaMemsetAsync(n.v.p, 0, sizeof(float) * kNumParams, n.st);
+  setSmem(k_convFwd<16, false>, (size_t)(128 + kC) * 9 * 16 * 2);
+  setSmem(k_convFwd<32, false>, (size_t)(128 + kC) * 9 * 32 * 2);
+  setSmem(k_convFwd<32, true>, (size_t)(128 + kC) * 9 * 32 * 2);
+  setSmem(k_convBwdData, (size_t)(128 + kC) * 9 * 32 * 2);
+  packWeights(n);
+  return cudaStreamSynchronize(n.st) == cudaSuccess;
+}
+
+// Upload host images (n images of w x h) into the work buffers and build X0.
+bool uploadInputs(KpcnNet& n, size_t P, const float* noisy, const float* normal, const float* albedo, const float* depth,
+                  const float* ref) {
+  DevBuf<float> nb, ab, db;
+  if (!nb.upload(normal, P * 3, n.st) || !ab.upload(albedo, P * 3, n.st) || !db.upload(depth, P, n.st)) return false;
+  if (cudaMemcpyAsync(n.noisy.p, noisy, sizeof(float4) * P, cudaMemcpyHostToDevice, n.st) != cudaSuccess) return false;
+  if (ref && cudaMemcpyAsync(n.ref.p, ref, sizeof(float4) * P, cudaMemcpyHostToDevice, n.st) != cudaSuccess) return false;
+  k_features<float><<<(unsigned)((P + 255) / 256), 256, 0, n.st>>>((int)P, n.noisy.p, nb.p, ab.p, db.p, n.X0.p);
+  return cudaStreamSynchronize(n.st) == cudaSuccess;  // the temporaries die here
+}
+
+}  // namespace
+
+// Denoise W x H on the device: noisy float4 HDR, half guides (the renderer's
+// AOV buffers), result into out (may alias nothing else); intensity blends
+// with the noisy image as denoiseImage does.
+rg_status kpcnDenoiseDevice(KpcnNet& n, int W, int H, const float4* noisy, const __half* normal, const __half* albedo,
+                            const __half* depth, float intensity, float4* out, cudaStream_t st) {
+  const size_t P = (size_t)W * H;
+  if (!ensureWork(n, P)) {
+    setLastError("learned denoiser: out of device memory");
+    return RG_ERR_OUT_OF_MEMORY;
+  }
+  cudaEvent_t ev;
+  cudaEventCreateWithFlags(&ev, cudaEventDisableTiming);
+  cudaEventRecord(ev, st);
+  cudaStreamWaitEvent(n.st, ev, 0);
+  k_features<__half><<<(unsigned)((P + 255) / 256), 256, 0, n.st>>>((int)P, noisy, normal, albedo, depth, n.X0.p);
+  forward(n, 1, H, W);
+  k_head<false><<<(unsigned)((P + 255) / 256), 256, 0, n.st>>>(1, H, W, n.Z.p, noisy, nullptr, n.out.p, nullptr, nullptr);
+  const rg_status rs = checkErr(n, "learned denoiser");
+  if (rs != RG_OK) {
+    cudaEventDestroy(ev);
+    return rs;
+  }
+  // the renderer's stream waits for the denoiser before blending
+  cudaEventRecord(ev, n.st);
+  cudaStreamWaitEvent(st, ev, 0);
+  k_blend<<<(unsigned)((P + 255) / 256), 256, 0, st>>>((int)P, noisy, n.out.p, intensity, out);
+  cudaEventDestroy(ev);
+  return RG_OK;
+}
+
+}  // namespace rg
+
+struct rg_denoiser {
+  rg::KpcnNet net;
+};
+
+namespace rg {
+KpcnNet* kpcnOf(rg_denoiser* d) { return d ? &d->net : nullptr; }
+}  // namespace rg
+
+extern "C" {
+
+int32_t rg_denoiser_num_params(void) { return rg::kNumParams; }
+
+rg_status rg_denoiser_create(uint32_t seed, rg_denoiser** out) {
+  if (!out) return RG_ERR_INVALID_ARGUMENT;
+  int dc = 0;
+  if (cudaGetDeviceCount(&dc) != cudaSuccess || dc == 0) {
+    cudaGetLastError();
+    return RG_ERR_NO_DEVICE;
+  }
+  std::unique_ptr<rg_denoiser> d(new rg_denoiser());
+  if (!rg::initNet(d->net, seed)) {
+    setLastError("learned denoiser: device set-up failed");
+    return RG_ERR_OUT_OF_MEMORY;
+  }
+  *out = d.release();
+  return RG_OK;
+}
+
+rg_status rg_denoiser_destroy(rg_denoiser* d) {
+  delete d;
+  return RG_OK;
+}
+
+rg_status rg_denoiser_get_params(rg_denoiser* d, float* out, size_t n) {
+  if (!d || !out || n < (size_t)rg::kNumParams) return RG_ERR_INVALID_ARGUMENT;
+  RG_CUDA_CHECK(cudaMemcpyAsync(out, d->net.params.p, sizeof(float) * rg::kNumParams, cudaMemcpyDeviceToHost, d->net.st));
+  RG_CUDA_CHECK(cudaStreamSynchronize(d->net.st));
+  return RG_OK;
+}
+
+rg_status rg_denoiser_set_params(rg_denoiser* d, const float* in, size_t n) {
+  if (!d || !in || n != (size_t)rg::kNumParams) return RG_ERR_INVALID_ARGUMENT;
+  RG_CUDA_CHECK(cudaMemcpyAsync(d->net.params.p, in, sizeof(float) * rg::kNumParams, cudaMemcpyHostToDevice, d->net.st));
+  RG_CUDA_CHECK(cudaMemsetAsync(d->net.m.p, 0, sizeof(float) * rg::kNumParams, d->net.st));
+  RG_CUDA_CHECK(cudaMemsetAsync(d->net.v.p, 0, sizeof(float) * rg::kNumParams, d->net.st));
+  d->net.adamStep = 0;
+  rg::packWeights(d->net);
+  RG_CUDA_CHECK(cudaStreamSynchronize(d->net.st));
+  return RG_OK;
+}
+
+rg_status rg_denoiser_add_example(rg_denoiser* d, int32_t w, int32_t h, const float* noisy_rgba, const float* normal,
+                                  const float* albedo, const float* depth, const float* ref_rgba) {
+  if (!d || w <= 0 || h <= 0 || !noisy_rgba || !normal || !albedo || !depth || !ref_rgba) return RG_ERR_INVALID_ARGUMENT;
+  rg::KpcnNet& n = d->net;
+  if (n.dsN > 0 && (w != n.dsW || h != n.dsH)) {
+    setLastError("learned denoiser: every training example must have the same size");
+    return RG_ERR_INVALID_ARGUMENT;
+  }
+  const size_t P = (size_t)w * h;
+  if (!rg::ensureWork(n, P) || !rg::uploadInputs(n, P, noisy_rgba, normal, albedo, depth, ref_rgba))
+    return RG_ERR_OUT_OF_MEMORY;
+  __nv_bfloat16* x = nullptr;
+  float4 *nz = nullptr, *rf = nullptr;
+  if (cudaMalloc(&x, P * 16 * sizeof(__nv_bfloat16)) != cudaSuccess || cudaMalloc(&nz, P * sizeof(float4)) != cudaSuccess ||
+      cudaMalloc(&rf, P * sizeof(float4)) != cudaSuccess) {
+    cudaFree(x);
+    cudaFree(nz);
+    cudaFree(rf);
+    setLastError("learned denoiser: out of device memory (examples)");
+    return RG_ERR_OUT_OF_MEMORY;
+  }
+  cudaMemcpyAsync(x, n.X0.p, P * 16 * sizeof(__nv_bfloat16), cudaMemcpyDeviceToDevice, n.st);
+  cudaMemcpyAsync(nz, n.noisy.p, P * sizeof(float4), cudaMemcpyDeviceToDevice, n.st);
+  cudaMemcpyAsync(rf, n.ref.p, P * sizeof(float4), cudaMemcpyDeviceToDevice, n.st);
+  RG_CUDA_CHECK(cudaStreamSynchronize(n.st));
+  n.exX.push_back(x);
+  n.exNoisy.push_back(nz);
+  n.exRef.push_back(rf);
+  n.dsW = w;
+  n.dsH = h;
+  n.dsN++;
+  return RG_OK;
+}
+
+rg_status rg_denoiser_clear_examples(rg_denoiser* d) {
+  if (!d) return RG_ERR_INVALID_ARGUMENT;
+  rg::KpcnNet& n = d->net;
+  for (auto* p : n.exX) cudaFree(p);
+  for (auto* p : n.exNoisy) cudaFree(p);
+  for (auto* p : n.exRef) cudaFree(p);
+  n.exX.clear();
+  n.exNoisy.clear();
+  n.exRef.clear();
+  n.dsN = 0;
+  return RG_OK;
+}
+
+rg_status rg_denoiser_train(rg_denoiser* d, int32_t steps, int32_t batch, float lr, float* losses) {
+  if (!d || steps < 0 || batch <= 0) return RG_ERR_INVALID_ARGUMENT;
+  rg::KpcnNet& n = d->net;
+  if (n.dsN == 0) {
+    setLastError("learned denoiser: no training examples");
+    return RG_ERR_INVALID_ARGUMENT;
+  }
+  const int B = batch, H = n.dsH, W = n.dsW;
+  const size_t Pi = (size_t)H * W, P = Pi * B;
+  if (!rg::ensureWork(n, P)) return RG_ERR_OUT_OF_MEMORY;
+  std::uniform_int_distribution<int> pick(0, n.dsN - 1);
+  for (int s = 0; s < steps; ++s) {
+    for (int b = 0; b < B; ++b) {  // random examples into the batch
+      const int e = pick(n.rng);
+      cudaMemcpyAsync(n.X0.p + b * Pi * 16, n.exX[e], Pi * 16 * sizeof(__nv_bfloat16), cudaMemcpyDeviceToDevice, n.st);
+      cudaMemcpyAsync(n.noisy.p + b * Pi, n.exNoisy[e], Pi * sizeof(float4), cudaMemcpyDeviceToDevice, n.st);
+      cudaMemcpyAsync(n.ref.p + b * Pi, n.exRef[e], Pi * sizeof(float4), cudaMemcpyDeviceToDevice, n.st);
+    }
+    cudaMemsetAsync(n.loss.p, 0, sizeof(float), n.st);
+    rg::forward(n, B, H, W);
+    rg::k_head<true><<<(unsigned)((P + 255) / 256), 256, 0, n.st>>>(B, H, W, n.Z.p, n.noisy.p, n.ref.p, nullptr, n.gA.p,
+                                                                     n.loss.p);
+    rg::backward(n, B, H, W);
+    n.adamStep++;
+    const float b1 = 0.9f, b2 = 0.999f;
+    rg::k_adam<<<(rg::kNumParams + 255) / 256, 256, 0, n.st>>>(rg::kNumParams, n.params.p, n.grad.p, n.m.p, n.v.p, lr, b1,
+                                                               b2, 1.0f - std::pow(b1, (float)n.adamStep),
+                                                               1.0f - std::pow(b2, (float)n.adamStep), 1e-8f);
+    rg::packWeights(n);
+    if (losses) cudaMemcpyAsync(losses + s, n.loss.p, sizeof(float), cudaMemcpyDeviceToHost, n.st);
+  }
+  return rg::checkErr(n, "learned denoiser training");
+}
+
+rg_status rg_denoiser_gradients(rg_denoiser* d, int32_t count, int32_t w, int32_t h, const float* noisy_rgba,
+                                const float* normal, const float* albedo, const float* depth, const float* ref_rgba,
+                                float* loss, float* grad) {
+  if (!d || count <= 0 || w <= 0 || h <= 0 || !noisy_rgba || !normal || !albedo || !depth || !ref_rgba || !grad)
+    return RG_ERR_INVALID_ARGUMENT;
+  rg::KpcnNet& n = d->net;
+  const size_t P = (size_t)count * w * h;
+  if (!rg::ensureWork(n, P) || !rg::uploadInputs(n, P, noisy_rgba, normal, albedo, depth, ref_rgba))
+    return RG_ERR_OUT_OF_MEMORY;
+  cudaMemsetAsync(n.loss.p, 0, sizeof(float), n.st);
+  rg::forward(n, count, h, w);
+  rg::k_head<true><<<(unsigned)((P + 255) / 256), 256, 0, n.st>>>(count, h, w, n.Z.p, n.noisy.p, n.ref.p, nullptr, n.gA.p,
+                                                                   n.loss.p);
+  rg::backward(n, count, h, w);
+  const rg_status rs = rg::checkErr(n, "learned denoiser gradients");
+  if (rs != RG_OK) return rs;
+  RG_CUDA_CHECK(cudaMemcpy(grad, n.grad.p, sizeof(float) * rg::kNumParams, cudaMemcpyDeviceToHost));
+  if (loss) RG_CUDA_CHECK(cudaMemcpy(loss, n.loss.p, sizeof(float), cudaMemcpyDeviceToHost));
+  return RG_OK;
+}
+
+rg_status rg_denoiser_apply(rg_denoiser* d, int32_t w, int32_t h, const float* noisy_rgba, const float* normal,
+                            const float* albedo, const float* depth, float* out_rgba) {
+  if (!d || w <= 0 || h <= 0 || !noisy_rgba || !normal || !albedo || !depth || !out_rgba) return RG_ERR_INVALID_ARGUMENT;
+  rg::KpcnNet& n = d->net;
+  const size_t P = (size_t)w * h;
+  if (!rg::ensureWork(n, P) || !rg::uploadInputs(n, P, noisy_rgba, normal, albedo, depth, nullptr))
+    return RG_ERR_OUT_OF_MEMORY;
+  rg::forward(n, 1, h, w);
+  rg::k_head<false><<<(unsigned)((P + 255) / 256), 256, 0, n.st>>>(1, h, w, n.Z.p, n.noisy.p, nullptr, n.out.p, nullptr,
+                                                                    nullptr);
+  const rg_status rs = rg::checkErr(n, "learned denoiser");
+  if (rs != RG_OK) return rs;
+  RG_CUDA_CHECK(cudaMemcpy(out_rgba, n.out.p, sizeof(float4) * P, cudaMemcpyDeviceToHost));
+  return RG_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,103 @@
+"""Training data and training loop of the learned denoiser.
+
+Pairs are rendered by the tracer itself: a low-spp render (the network's input:
+noisy radiance plus the albedo / normal / depth guides) and a high-spp render of
+the same job (the target).  Scenes are the seeded procedural batch jobs
+(heterogeneous triangle counts, emitters and materials) and the cube room.
+
+    python -m raygen_b200.kpcn_train --out weights.bin   (from the package's parent)
+
+or through `train(...)` from Python.
+"""
+import argparse
+import time
+
+import numpy as np
+
+
+def render_pair(rg, scene, width, height, spp_lo, spp_hi, seed, max_depth=6):
+    """-> (noisy RGBA, normal, albedo, depth, reference RGBA) for one job."""
+    st = rg.RendererSettings(resolutionWidth=width, resolutionHeight=height, samples=spp_lo, maxDepth=max_depth,
+                             seed=seed, enableDenoise=True, denoiseIntensity=0.0)
+    r = rg.RayRenderer(st)
+    r.set_scene(scene)
+    r.render()
+    noisy = r.get_hdr_result()  # intensity 0: the denoiser pass leaves the radiance as rendered
+    normal, albedo, depth = r.get_aovs()
+    r.settings.samples = spp_hi
+    r.settings.enableDenoise = False
+    r.settings.seed = seed + 7919
+    r.render()
+    ref = r.get_hdr_result()
+    r.close()
+    return noisy, normal, albedo, depth, ref
+
+
+def scene_for(rg, k):
+    """Seeded procedural job k: batch-job scenes of 2k-40k triangles with 1-8 emitters; every 8th the cube room."""
+    if k % 8 == 7:
+        return rg.Scene.builtin(1, 1 + k)
+    rng = np.random.default_rng(1000 + k)
+    tris = int(np.exp(rng.uniform(np.log(2e3), np.log(4e4))))
+    return rg.Scene.builtin(4, 5000 + k, [tris, int(rng.integers(1, 9))])
+
+
+def make_examples(rg, count, size=64, spp_lo=8, spp_hi=512, first=0):
+    out = []
+    for k in range(first, first + count):
+        sc = scene_for(rg, k)
+        out.append(render_pair(rg, sc, size, size, spp_lo, spp_hi, seed=100 + k))
+        sc.close()
+    return out
+
+
+def relmse(img, ref, eps=0.01):
+    a, r = np.asarray(img)[..., :3].astype(np.float64), np.asarray(ref)[..., :3].astype(np.float64)
+    return float(np.mean((a - r) ** 2 / (r * r + eps)))
+
+
+def train(rg, examples, steps=2000, batch=8, lr=1e-3, seed=0, params=None, log=None):
+    d = rg.Denoiser(seed=seed, params=params)
+    for ex in examples:
+        d.add_example(*ex)
+    losses = []
+    t0 = time.time()
+    done = 0
+    while done < steps:
+        n = min(250, steps - done)
+        # step decay of the learning rate over the run
+        cur = lr * (0.3 if done >= 0.75 * steps else 1.0)
+        losses.append(d.train(n, batch, cur))
+        done += n
+        if log:
+            log(f"step {done}: loss {losses[-1][-n:].mean():.5f} ({time.time() - t0:.1f} s)")
+    return d, np.concatenate(losses) if losses else np.zeros(0)
+
+
+def main():
+    import os
+    import sys
+    here = os.path.dirname(os.path.abspath(__file__))
+    sys.path.insert(0, os.path.dirname(here))
+    from __graft_entry__ import load_package
+    rg = load_package()
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--out", default=os.path.join(here, "kpcn_weights.bin"))
+    ap.add_argument("--examples", type=int, default=256)
+    ap.add_argument("--size", type=int, default=64)
+    ap.add_argument("--spp-lo", type=int, default=8)
+    ap.add_argument("--spp-hi", type=int, default=512)
+    ap.add_argument("--steps", type=int, default=3000)
+    ap.add_argument("--batch", type=int, default=16)
+    ap.add_argument("--lr", type=float, default=1e-3)
+    a = ap.parse_args()
+    t0 = time.time()
+    ex = make_examples(rg, a.examples, a.size, a.spp_lo, a.spp_hi)
+    print(f"{len(ex)} examples in {time.time() - t0:.1f} s", flush=True)
+    d, losses = train(rg, ex, a.steps, a.batch, a.lr, log=lambda m: print(m, flush=True))
+    d.save(a.out)
+    print(f"saved {a.out}; final loss {losses[-100:].mean():.5f}", flush=True)
+
+
+if __name__ == "__main__":
+    main()

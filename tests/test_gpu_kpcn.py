@@ -16,3 +16,72 @@ def test_tc_gemm_matches_fp64(rg, M, N, K):
     b = rg.from_bf16_bits(rg.to_bf16_bits(B)).astype(np.float64)
     ref = a @ b.T
     np.testing.assert_allclose(got, ref, rtol=1e-5, atol=1e-4 * np.sqrt(K))
+
+
+# ---------------------------------------------------------------- the network
+import kpcn_oracle as ko  # noqa: E402
+
+
+def synth(n, h, w, seed):
+    rng = np.random.default_rng(seed)
+    noisy = np.concatenate([rng.gamma(1.5, 0.5, (n, h, w, 3)), np.ones((n, h, w, 1))], -1).astype(np.float32)
+    ref = noisy.copy()
+    ref[..., :3] = noisy[..., :3] * 0.5 + 0.3
+    normal = rng.random((n, h, w, 3)).astype(np.float32)
+    albedo = rng.random((n, h, w, 3)).astype(np.float32)
+    depth = rng.random((n, h, w)).astype(np.float32)
+    return noisy, normal, albedo, depth, ref
+
+
+def perturbed(d, seed, scale=0.05):
+    p = d.params.astype(np.float64)
+    rng = np.random.default_rng(seed)
+    p += rng.standard_normal(p.shape) * scale
+    layers = ko.unpack(p)  # keep the padding entries at zero
+    for l, (W, b) in enumerate(layers):
+        if l == 0:
+            W[:, :, 10:] = 0.0
+        if l == 5:
+            W[ko.KP:] = 0.0
+            b[ko.KP:] = 0.0
+    return np.concatenate([np.concatenate([W.ravel(), b]) for W, b in layers]).astype(np.float32)
+
+
+def test_kpcn_forward_matches_oracle(rg):
+    d = rg.Denoiser(seed=3)
+    p = perturbed(d, 1)
+    d.params = p
+    noisy, normal, albedo, depth, ref = synth(1, 37, 45, 1)  # 1665 pixels: a partial last tile
+    got = d.apply(noisy[0], normal[0], albedo[0], depth[0])
+    f = ko.forward(p, ko.features(noisy, normal, albedo, depth), noisy)
+    np.testing.assert_allclose(got[..., :3], f["out"][0], rtol=2e-3, atol=2e-3)
+    assert np.all(got[..., 3] == 1.0)
+    d.close()
+
+
+def test_kpcn_gradients_match_oracle(rg):
+    d = rg.Denoiser(seed=5)
+    p = perturbed(d, 2)
+    d.params = p
+    noisy, normal, albedo, depth, ref = synth(2, 23, 29, 2)
+    loss, g = d.gradients(noisy, normal, albedo, depth, ref)
+    lo, go = ko.backward(p, ko.features(noisy, normal, albedo, depth), noisy, ref)
+    assert loss == pytest.approx(lo, rel=1e-3)
+    offs = np.cumsum([0] + [w + b for w, b in ko.layer_sizes()])
+    for l, (wl, bl) in enumerate(ko.layer_sizes()):
+        for a, b in ((offs[l], offs[l] + wl), (offs[l] + wl, offs[l + 1])):
+            x, y = g[a:b].astype(np.float64), go[a:b]
+            cos = x @ y / (np.linalg.norm(x) * np.linalg.norm(y) + 1e-30)
+            assert cos > 0.999, (l, a, cos)
+            assert abs(np.linalg.norm(x) / np.linalg.norm(y) - 1.0) < 0.01, (l, a)
+    d.close()
+
+
+def test_kpcn_training_reduces_loss(rg):
+    import importlib
+    kt = importlib.import_module(rg.__name__ + ".kpcn_train")
+    ex = kt.make_examples(rg, 8, size=64, spp_lo=4, spp_hi=128)
+    d, losses = kt.train(rg, ex, steps=300, batch=4, lr=2e-3)
+    assert np.all(np.isfinite(losses))
+    assert losses[-30:].mean() < 0.7 * losses[:10].mean(), (losses[:10].mean(), losses[-30:].mean())
+    d.close()
