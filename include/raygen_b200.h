@@ -344,7 +344,9 @@ typedef struct rg_job_desc {
   int32_t width, height, samples;
   int32_t max_depth, rr_depth;  /* <= 0: the server's base settings */
   uint32_t seed;                /* RNG key: results do not depend on the mix */
-  int32_t denoise;              /* 1: A-Trous on the finished image */
+  int32_t denoise;              /* 1: A-Trous on the finished image; 2: the learned
+                                   denoiser set with rg_server_set_denoiser (A-Trous
+                                   when none is set) */
 } rg_job_desc;
 
 typedef struct rg_job_status {
@@ -377,6 +379,9 @@ rg_status rg_server_get_result(rg_server* s, int64_t job_id, float* hdr_rgba, si
 /* Progressive result of a resident job (current sample mean), taken between waves. */
 rg_status rg_server_snapshot(rg_server* s, int64_t job_id, float* hdr_rgba, size_t count, double timeout_ms);
 rg_status rg_server_get_stats(rg_server* s, rg_server_stats* out);
+/* Learned denoiser for jobs submitted with denoise = 2 (NULL: A-Trous).  Keep
+ * `d` alive while it is set. */
+rg_status rg_server_set_denoiser(rg_server* s, rg_denoiser* d);
 rg_status rg_server_destroy(rg_server* s);
 
 #ifdef __cplusplus

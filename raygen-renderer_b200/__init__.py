@@ -217,6 +217,7 @@ def load_library(path: str = LIB_PATH) -> C.CDLL:
         "rg_denoiser_gradients": (C.c_int, [C.c_void_p, C.c_int32, C.c_int32, C.c_int32] + [P(C.c_float)] * 7),
         "rg_denoiser_apply": (C.c_int, [C.c_void_p, C.c_int32, C.c_int32] + [P(C.c_float)] * 5),
         "rg_set_denoiser": (C.c_int, [C.c_void_p, C.c_void_p]),
+        "rg_server_set_denoiser": (C.c_int, [C.c_void_p, C.c_void_p]),
         "rg_reapply_postprocess": (C.c_int, [C.c_void_p]),
         "rg_scene_builtin": (C.c_int, [C.c_int32, C.c_uint32, P(C.c_int32), C.c_int32, P(P(rg_scene_desc))]),
         "rg_scene_free": (C.c_int, [P(rg_scene_desc)]),
@@ -633,6 +634,15 @@ class Denoiser:
         if params is not None:
             self.params = params
 
+    WEIGHTS = os.path.join(os.path.dirname(os.path.abspath(__file__)), "kpcn_weights.bin")
+
+    @classmethod
+    def pretrained(cls, path: Optional[str] = None) -> "Denoiser":
+        """The network trained by kpcn_train.py on tracer-rendered 8 / 512 spp pairs (shipped weights)."""
+        d = cls(seed=0)
+        d.load(path or cls.WEIGHTS)
+        return d
+
     @staticmethod
     def num_params() -> int:
         return int(load_library().rg_denoiser_num_params())
@@ -734,7 +744,8 @@ class RenderServer:
         self._jobs = {}
 
     def submit(self, scene: Scene, width: int, height: int, samples: int, max_depth: int = 8, rr_depth: int = 3,
-               seed: int = 1, denoise: bool = False) -> int:
+               seed: int = 1, denoise=False) -> int:
+        """denoise: False / 0 none, True / 1 A-Trous, 2 the learned denoiser (see set_denoiser)."""
         d = rg_job_desc()
         d.scene = scene.ptr
         d.width, d.height, d.samples = width, height, samples
@@ -743,6 +754,11 @@ class RenderServer:
         _check(self._lib.rg_server_submit(self._h, C.byref(d), C.byref(jid)))
         self._jobs[jid.value] = (scene, width, height)  # keep the scene alive until done
         return jid.value
+
+    def set_denoiser(self, denoiser) -> None:
+        """Learned denoiser for jobs submitted with denoise=2 (None: A-Trous)."""
+        self._denoiser = denoiser
+        _check(self._lib.rg_server_set_denoiser(self._h, denoiser._h if denoiser is not None else None))
 
     def status(self, job: int) -> dict:
         st = rg_job_status()

@@ -28,6 +28,7 @@
 #include <cmath>
 #include <cstring>
 #include <memory>
+#include <mutex>
 #include <random>
 #include <string>
 #include <vector>
@@ -616,6 +617,7 @@ __global__ void k_blend(int n, const float4* __restrict__ noisy, const float4* _
 }  // namespace
 
 struct KpcnNet {
+  std::mutex mu;  // one user of the work buffers at a time (renderers, servers, API calls)
   cudaStream_t st = nullptr;
   int numSMs = 148;
   DevBuf<float> params, grad, m, v;
@@ -788,6 +790,7 @@ bool uploadInputs(KpcnNet& n, size_t P, const float* noisy, const float* normal,
 // with the noisy image as denoiseImage does.
 rg_status kpcnDenoiseDevice(KpcnNet& n, int W, int H, const float4* noisy, const __half* normal, const __half* albedo,
                             const __half* depth, float intensity, float4* out, cudaStream_t st) {
+  std::lock_guard<std::mutex> lk(n.mu);
   const size_t P = (size_t)W * H;
   if (!ensureWork(n, P)) {
     setLastError("learned denoiser: out of device memory");
@@ -850,6 +853,7 @@ rg_status rg_denoiser_destroy(rg_denoiser* d) {
 
 rg_status rg_denoiser_get_params(rg_denoiser* d, float* out, size_t n) {
   if (!d || !out || n < (size_t)rg::kNumParams) return RG_ERR_INVALID_ARGUMENT;
+  std::lock_guard<std::mutex> lk(d->net.mu);
   RG_CUDA_CHECK(cudaMemcpyAsync(out, d->net.params.p, sizeof(float) * rg::kNumParams, cudaMemcpyDeviceToHost, d->net.st));
   RG_CUDA_CHECK(cudaStreamSynchronize(d->net.st));
   return RG_OK;
@@ -857,6 +861,7 @@ rg_status rg_denoiser_get_params(rg_denoiser* d, float* out, size_t n) {
 
 rg_status rg_denoiser_set_params(rg_denoiser* d, const float* in, size_t n) {
   if (!d || !in || n != (size_t)rg::kNumParams) return RG_ERR_INVALID_ARGUMENT;
+  std::lock_guard<std::mutex> lk(d->net.mu);
   RG_CUDA_CHECK(cudaMemcpyAsync(d->net.params.p, in, sizeof(float) * rg::kNumParams, cudaMemcpyHostToDevice, d->net.st));
   RG_CUDA_CHECK(cudaMemsetAsync(d->net.m.p, 0, sizeof(float) * rg::kNumParams, d->net.st));
   RG_CUDA_CHECK(cudaMemsetAsync(d->net.v.p, 0, sizeof(float) * rg::kNumParams, d->net.st));
@@ -870,6 +875,7 @@ rg_status rg_denoiser_add_example(rg_denoiser* d, int32_t w, int32_t h, const fl
                                   const float* albedo, const float* depth, const float* ref_rgba) {
   if (!d || w <= 0 || h <= 0 || !noisy_rgba || !normal || !albedo || !depth || !ref_rgba) return RG_ERR_INVALID_ARGUMENT;
   rg::KpcnNet& n = d->net;
+  std::lock_guard<std::mutex> lk(n.mu);
   if (n.dsN > 0 && (w != n.dsW || h != n.dsH)) {
     setLastError("learned denoiser: every training example must have the same size");
     return RG_ERR_INVALID_ARGUMENT;
@@ -903,6 +909,7 @@ rg_status rg_denoiser_add_example(rg_denoiser* d, int32_t w, int32_t h, const fl
 rg_status rg_denoiser_clear_examples(rg_denoiser* d) {
   if (!d) return RG_ERR_INVALID_ARGUMENT;
   rg::KpcnNet& n = d->net;
+  std::lock_guard<std::mutex> lk(n.mu);
   for (auto* p : n.exX) cudaFree(p);
   for (auto* p : n.exNoisy) cudaFree(p);
   for (auto* p : n.exRef) cudaFree(p);
@@ -916,6 +923,7 @@ rg_status rg_denoiser_clear_examples(rg_denoiser* d) {
 rg_status rg_denoiser_train(rg_denoiser* d, int32_t steps, int32_t batch, float lr, float* losses) {
   if (!d || steps < 0 || batch <= 0) return RG_ERR_INVALID_ARGUMENT;
   rg::KpcnNet& n = d->net;
+  std::lock_guard<std::mutex> lk(n.mu);
   if (n.dsN == 0) {
     setLastError("learned denoiser: no training examples");
     return RG_ERR_INVALID_ARGUMENT;
@@ -953,6 +961,7 @@ rg_status rg_denoiser_gradients(rg_denoiser* d, int32_t count, int32_t w, int32_
   if (!d || count <= 0 || w <= 0 || h <= 0 || !noisy_rgba || !normal || !albedo || !depth || !ref_rgba || !grad)
     return RG_ERR_INVALID_ARGUMENT;
   rg::KpcnNet& n = d->net;
+  std::lock_guard<std::mutex> lk(n.mu);
   const size_t P = (size_t)count * w * h;
   if (!rg::ensureWork(n, P) || !rg::uploadInputs(n, P, noisy_rgba, normal, albedo, depth, ref_rgba))
     return RG_ERR_OUT_OF_MEMORY;
@@ -972,6 +981,7 @@ rg_status rg_denoiser_apply(rg_denoiser* d, int32_t w, int32_t h, const float* n
                             const float* albedo, const float* depth, float* out_rgba) {
   if (!d || w <= 0 || h <= 0 || !noisy_rgba || !normal || !albedo || !depth || !out_rgba) return RG_ERR_INVALID_ARGUMENT;
   rg::KpcnNet& n = d->net;
+  std::lock_guard<std::mutex> lk(n.mu);
   const size_t P = (size_t)w * h;
   if (!rg::ensureWork(n, P) || !rg::uploadInputs(n, P, noisy_rgba, normal, albedo, depth, nullptr))
     return RG_ERR_OUT_OF_MEMORY;

@@ -82,6 +82,7 @@ using namespace rg;
 struct rg_server {
   rg_settings base{};
   rg_server_config cfg{};
+  std::atomic<rg_denoiser*> denoiser{nullptr};  // jobs with denoise == 2
   std::mutex mu;
   std::condition_variable cv;
   std::deque<ServerJob*> pending;
@@ -242,7 +243,13 @@ void finishJob(rg_server* s, ServerJob* j) {
   cudaStream_t st = s->stream;
   const int N = j->pixels;
   launchResolve(N, j->sum.p, j->cnt.p, j->R.exposure, j->hdr.p, st);
-  if (j->desc.denoise) {
+  rg_status dres = RG_OK;
+  rg_denoiser* learned = j->desc.denoise == 2 ? s->denoiser.load() : nullptr;
+  if (learned) {  // learned denoiser on the job's guides
+    dres = kpcnDenoiseDevice(*kpcnOf(learned), j->desc.width, j->desc.height, j->hdr.p, j->aovN.p, j->aovA.p, j->aovD.p,
+                             s->base.denoise_intensity, j->ldr.p, st);
+    if (dres == RG_OK) cudaMemcpyAsync(j->hdr.p, j->ldr.p, sizeof(float4) * N, cudaMemcpyDeviceToDevice, st);
+  } else if (j->desc.denoise) {  // A-Trous (also the fallback of mode 2)
     launchDenoise(j->desc.width, j->desc.height, j->hdr.p, j->aovN.p, j->aovD.p, j->aovA.p, j->aovAA.p,
                   s->base.denoise_levels, s->base.denoise_sigma_color, s->base.denoise_sigma_normal,
                   s->base.denoise_sigma_depth, s->base.denoise_intensity, j->bufA.p, j->bufB.p, j->ldr.p, st);
@@ -253,7 +260,7 @@ void finishJob(rg_server* s, ServerJob* j) {
   int derr = 0;
   cudaMemcpyAsync(&derr, j->errWord.p, sizeof(int), cudaMemcpyDeviceToHost, st);
   const cudaError_t ce = cudaStreamSynchronize(st);
-  j->error = ce != cudaSuccess ? RG_ERR_CUDA : (derr ? RG_ERR_DEVICE_STATUS : RG_OK);
+  j->error = ce != cudaSuccess ? RG_ERR_CUDA : (derr ? RG_ERR_DEVICE_STATUS : dres);
 }
 
 // Admission thread: reserves a slot and budget for queued jobs and prepares
@@ -586,6 +593,12 @@ rg_status rg_server_snapshot(rg_server* s, int64_t job, float* hdr_rgba, size_t 
   const std::vector<float>& src = j->snapshotReady ? j->snapshot : j->result;
   if (count < src.size() || src.empty()) return RG_ERR_BUSY;
   std::memcpy(hdr_rgba, src.data(), src.size() * sizeof(float));
+  return RG_OK;
+}
+
+rg_status rg_server_set_denoiser(rg_server* s, rg_denoiser* d) {
+  if (!s) return RG_ERR_INVALID_ARGUMENT;
+  s->denoiser.store(d);
   return RG_OK;
 }
 

@@ -74,6 +74,23 @@ def train(rg, examples, steps=2000, batch=8, lr=1e-3, seed=0, params=None, log=N
     return d, np.concatenate(losses) if losses else np.zeros(0)
 
 
+def evaluate(rg, denoiser, count=16, size=128, spp_lo=8, spp_hi=2048, first=100000):
+    """relMSE against a high-spp render on held-out jobs: the noisy input, A-Trous
+    (the reference's denoiser, default settings) and the learned denoiser."""
+    rows = []
+    for k in range(first, first + count):
+        sc = scene_for(rg, k)
+        noisy, normal, albedo, depth, ref = render_pair(rg, sc, size, size, spp_lo, spp_hi, seed=100 + k)
+        sc.close()
+        atrous = rg.denoise_atrous(noisy[..., :3], normal, depth, albedo, np.ones_like(depth))
+        learned = denoiser.apply(noisy, normal, albedo, depth)
+        rows.append((relmse(noisy, ref), relmse(atrous, ref), relmse(learned, ref)))
+    r = np.array(rows)
+    return {"noisy": float(r[:, 0].mean()), "atrous": float(r[:, 1].mean()), "learned": float(r[:, 2].mean()),
+            "learned_wins": int((r[:, 2] < r[:, 1]).sum()), "jobs": count, "size": size, "spp": spp_lo,
+            "reference_spp": spp_hi}
+
+
 def main():
     import os
     import sys
@@ -90,6 +107,7 @@ def main():
     ap.add_argument("--steps", type=int, default=3000)
     ap.add_argument("--batch", type=int, default=16)
     ap.add_argument("--lr", type=float, default=1e-3)
+    ap.add_argument("--eval", type=int, default=16, help="held-out jobs to evaluate (0: none)")
     a = ap.parse_args()
     t0 = time.time()
     ex = make_examples(rg, a.examples, a.size, a.spp_lo, a.spp_hi)
@@ -97,6 +115,8 @@ def main():
     d, losses = train(rg, ex, a.steps, a.batch, a.lr, log=lambda m: print(m, flush=True))
     d.save(a.out)
     print(f"saved {a.out}; final loss {losses[-100:].mean():.5f}", flush=True)
+    if a.eval > 0:
+        print("held-out relMSE:", evaluate(rg, d, a.eval), flush=True)
 
 
 if __name__ == "__main__":
