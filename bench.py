@@ -53,7 +53,7 @@ def parse():
     p.add_argument("--res", default=f"{W}x{H}", help="resolution WxH (profiling runs only)")
     p.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline (profiling runs only)")
     p.add_argument("--bvh-width", type=int, default=8, choices=[2, 8])
-    p.add_argument("--mode", default="headline", choices=["headline", "batch", "serve", "learned"],
+    p.add_argument("--mode", default="headline", choices=["headline", "batch", "serve", "learned", "denoiser"],
                    help="headline: heavy single job; batch: 256 heterogeneous jobs in one server; "
                         "serve: Poisson request stream")
     p.add_argument("--jobs", type=int, default=256)
@@ -353,6 +353,64 @@ def run_learned(args):
     return 0
 
 
+DENOISER_FLOPS_PER_PIXEL = 2 * 9 * (16 * 32 + 4 * 32 * 32 + 32 * 32)  # six 3x3 convolutions, padded widths
+
+
+def measured_peak_bf16():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return float(json.load(f)["bf16_tflops"]), "measured (burst)"
+    except Exception:
+        return 1590.0, "fallback"
+
+
+def run_denoiser(args):
+    """Learned denoiser on the tensor cores: device time of one inference at --res
+    (features, six BF16 tcgen05 convolutions, kernel application) and of one
+    training step (batch of 16 tracer-rendered 64 x 64 pairs: forward, backward,
+    Adam).  FLOPs count the convolutions' multiply-adds at their padded widths."""
+    import importlib
+    import numpy as np
+    sys.path.insert(0, ROOT)
+    from __graft_entry__ import load_package
+    rg = load_package()
+    kt = importlib.import_module(rg.__name__ + ".kpcn_train")
+    d = rg.Denoiser.pretrained()
+    w, h = args.w, args.h
+    rng = np.random.default_rng(0)
+    noisy = np.concatenate([rng.random((h, w, 3)), np.ones((h, w, 1))], -1).astype(np.float32)
+    nrm, alb, dep = (rng.random((h, w, 3)).astype(np.float32), rng.random((h, w, 3)).astype(np.float32),
+                     rng.random((h, w)).astype(np.float32))
+    times = []
+    for k in range(args.warmup + args.steps):
+        d.apply(noisy, nrm, alb, dep)
+        if k >= args.warmup:
+            times.append(d.timing()["apply_ms"])
+    ms = float(np.median(times))
+    tflops = DENOISER_FLOPS_PER_PIXEL * w * h / ms / 1e9
+    peak, src = measured_peak_bf16()
+    for ex in kt.make_examples(rg, 16, size=64, spp_lo=8, spp_hi=64):
+        d.add_example(*ex)
+    d.train(args.warmup, 16, 1e-6)
+    d.train(max(1, args.steps * 10), 16, 1e-6)
+    step_ms = d.timing()["train_step_ms"]
+    step_tflops = 3 * DENOISER_FLOPS_PER_PIXEL * 16 * 64 * 64 / step_ms / 1e9
+    d.close()
+    line = {
+        "metric": "learned denoiser: inference and training-step device time", "value": round(ms, 3), "unit": "ms",
+        "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms, 3),
+        "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "bf16 (fp32 accumulation)",
+        "data": "synthetic inputs (inference); tracer-rendered pairs (training)",
+        "config": {"workload": f"denoiser inference {w}x{h}; training step batch 16 x 64x64", "mode": "denoiser"},
+        "roofline": {"bound": "tensor", "achieved": round(tflops, 1), "peak": peak, "unit": "TFLOP/s",
+                     "frac": round(tflops / peak, 4), "traffic": None, "peak_source": src,
+                     "flops_per_pixel": DENOISER_FLOPS_PER_PIXEL},
+        "training": {"step_ms": round(step_ms, 3), "tflops": round(step_tflops, 1)},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def run_reference(args, rank, world):
     if rank != 0:
         return 0
@@ -399,6 +457,8 @@ def main():
         pg = dist
     if args.mode == "learned":
         return run_learned(args)
+    if args.mode == "denoiser":
+        return run_denoiser(args)
     if args.mode != "headline":
         return run_jobs(args)
     if args.impl == "reference":

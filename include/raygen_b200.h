@@ -298,6 +298,10 @@ rg_status rg_denoiser_gradients(rg_denoiser* d, int32_t count, int32_t w, int32_
                                 float* loss, float* grad);
 rg_status rg_denoiser_apply(rg_denoiser* d, int32_t w, int32_t h, const float* noisy_rgba, const float* normal,
                             const float* albedo, const float* depth, float* out_rgba);
+/* Device time (CUDA events) of the last rg_denoiser_apply (features, six
+ * convolutions, kernel application) and of the mean step of the last
+ * rg_denoiser_train call (batch gather, forward, backward, Adam, repacking). */
+rg_status rg_denoiser_timing(rg_denoiser* d, float* apply_ms, float* train_step_ms);
 /* Use `d` instead of A-Trous when enable_denoise is set (NULL: back to A-Trous).
  * The handle keeps the pointer; destroy `d` only after detaching it. */
 rg_status rg_set_denoiser(rg_handle* h, rg_denoiser* d);

@@ -217,6 +217,7 @@ def load_library(path: str = LIB_PATH) -> C.CDLL:
         "rg_denoiser_gradients": (C.c_int, [C.c_void_p, C.c_int32, C.c_int32, C.c_int32] + [P(C.c_float)] * 7),
         "rg_denoiser_apply": (C.c_int, [C.c_void_p, C.c_int32, C.c_int32] + [P(C.c_float)] * 5),
         "rg_set_denoiser": (C.c_int, [C.c_void_p, C.c_void_p]),
+        "rg_denoiser_timing": (C.c_int, [C.c_void_p, P(C.c_float), P(C.c_float)]),
         "rg_server_set_denoiser": (C.c_int, [C.c_void_p, C.c_void_p]),
         "rg_reapply_postprocess": (C.c_int, [C.c_void_p]),
         "rg_scene_builtin": (C.c_int, [C.c_int32, C.c_uint32, P(C.c_int32), C.c_int32, P(P(rg_scene_desc))]),
@@ -699,6 +700,12 @@ class Denoiser:
         _check(self._lib.rg_denoiser_apply(self._h, w, h, _fptr(noisy), _fptr(normal), _fptr(albedo), _fptr(depth),
                                            _fptr(out)))
         return out
+
+    def timing(self) -> dict:
+        """Device ms of the last apply() and of the mean step of the last train()."""
+        a, t = C.c_float(), C.c_float()
+        _check(self._lib.rg_denoiser_timing(self._h, C.byref(a), C.byref(t)))
+        return {"apply_ms": a.value, "train_step_ms": t.value}
 
     def close(self) -> None:
         if getattr(self, "_h", None):

@@ -10,10 +10,11 @@
 //
 // Every convolution pass is an implicit GEMM on the tensor-core block of
 // rg_tc.cuh (M = 128 rows, N = 32, K a multiple of 16):
-//   forward        rows = pixels, K = (tap, input channel), B = weights;
-//   backward data  rows = pixels, K = (tap, output channel) of the gradient
-//                  gathered at p - offset, B = transposed weights, ReLU mask
-//                  of the layer input applied in the epilogue;
+//   forward        rows = 128 pixels of an image row, K = (tap, input
+//                  channel); A is addressed straight in the staged input rows
+//                  by per-tap descriptors (k_convRow); B = weights;
+//   backward data  the same with the gradient, mirrored taps and transposed
+//                  weights, the ReLU mask of the layer input in the epilogue;
 //   backward wt.   rows = (tap, input channel), K = pixels (a chunk of 2048
 //                  per CTA, 128 at a time), B = the output gradient;
 //                  per-chunk partials reduced in chunk order (deterministic).
@@ -163,21 +164,34 @@ __global__ void k_features(int P, const float4* __restrict__ noisy, const T* __r
   dst[1] = reinterpret_cast<const uint4*>(o)[1];
 }
 
-// Forward convolution.  LAST = false: Y = bf16(relu(conv + b)); LAST = true:
-// Z = conv + b in FP32 (the logits).  Persistent: each CTA walks 128-pixel tiles.
-template <int CIN, bool LAST>
-__global__ void __launch_bounds__(128) k_convFwd(int B, int H, int W, const __nv_bfloat16* __restrict__ X,
+// Row-tiled implicit GEMM for the forward and backward-data convolutions.  A
+// tile is up to 128 consecutive pixels of one image row.  The CTA stages the
+// three input rows the tile touches (x0 - 1 .. x0 + 128, zero outside the
+// image) once, as planes of 16-byte slots (8 channels of one pixel), one plane
+// per (row, channel chunk).  The A operand of tap (dy, dx) is then just a
+// descriptor into those planes: 8 consecutive pixels are a core matrix (SBO =
+// 128 bytes), the second 8-channel chunk of an MMA step is the next plane
+// (LBO = plane stride), and the tap's shift moves the start address by
+// (dy, dx) rows / slots -- no duplicated im2col copy.  Plane stride 2208 bytes
+// staggers the banks of the four chunk planes.
+constexpr int kPix = 136;               // slots per plane (>= 130, multiple of 8)
+constexpr int kPlane = (kPix + 2) * 16;  // bytes per plane
+
+// Forward (TRANSPOSED = false): Y = bf16(relu(conv(X) + b)) or, LAST, Z = conv(X) + b.
+// Backward data (TRANSPOSED = true, CIN = 32): out = bf16(mask(Xin) * convT(X = G, Wk = W^T)).
+template <int CIN, bool LAST, bool TRANSPOSED>
+__global__ void __launch_bounds__(128) k_convRow(int B, int H, int W, const __nv_bfloat16* __restrict__ X,
                                                  const __nv_bfloat16* __restrict__ Wk, const float* __restrict__ bias,
-                                                 __nv_bfloat16* __restrict__ Y, float* __restrict__ Z,
-                                                 int* __restrict__ err) {
-  constexpr int K = 9 * CIN, KC = K / 8, CC = CIN / 8;
+                                                 const __nv_bfloat16* __restrict__ Xin, __nv_bfloat16* __restrict__ Y,
+                                                 float* __restrict__ Z, int* __restrict__ err) {
+  constexpr int CC = CIN / 8, K = 9 * CIN, KC = K / 8;
   extern __shared__ __align__(1024) unsigned char sm[];
   __shared__ uint64_t bar;
   __shared__ uint32_t tbase;
-  unsigned char* sA = sm;
-  unsigned char* sB = sm + (size_t)128 * K * 2;
+  unsigned char* sIn = sm;                                   // 3 * CC planes
+  unsigned char* sB = sm + (size_t)3 * CC * kPlane;          // 32 x K weights, K-major core matrices
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-  const int P = B * H * W, tiles = (P + 127) / 128;
+  const int tilesPerRow = (W + 127) / 128, tiles = B * H * tilesPerRow;
   if (warp == 0) tc::tmemAlloc(&tbase, 32);
   if (tid == 0) tc::mbarInit(&bar, 1);
   for (int c = tid; c < kC * KC; c += 128) {
@@ -186,32 +200,41 @@ __global__ void __launch_bounds__(128) k_convFwd(int B, int H, int W, const __nv
   }
   float bv[kC];
 #pragma unroll
-  for (int j = 0; j < kC; ++j) bv[j] = bias[j];
+  for (int j = 0; j < kC; ++j) bv[j] = TRANSPOSED ? 0.0f : bias[j];
   __syncthreads();
   const uint32_t tmem = tbase;
   const uint32_t idesc = tc::instrDescBf16(128, kC);
+  const uint32_t inBase = tc::smemAddr(sIn), bBase = tc::smemAddr(sB);
   uint32_t phase = 0;
   bool ok = true;
   for (int tile = blockIdx.x; tile < tiles; tile += gridDim.x) {
-    const int p0 = tile * 128;
-    for (int c = tid; c < 128 * 9 * CC; c += 128) {
-      const int r = c / (9 * CC), rem = c % (9 * CC), t = rem / CC, q = rem % CC;
-      const int p = p0 + r;
+    const int xt = tile % tilesPerRow, rowIdx = tile / tilesPerRow;  // rowIdx = b * H + y
+    const int y = rowIdx % H, b = rowIdx / H, x0 = xt * 128;
+    for (int c = tid; c < 3 * 130 * CC; c += 128) {
+      const int r = c / (130 * CC), rem = c % (130 * CC), j = rem / CC, q = rem % CC;
+      const int yy = y + r - 1, xx = x0 - 1 + j;
       uint4 v = make_uint4(0, 0, 0, 0);
-      if (p < P) {
-        const int n = neighbor(p, t / 3 - 1, t % 3 - 1, H, W);
-        if (n >= 0) v = *reinterpret_cast<const uint4*>(X + (size_t)n * CIN + q * 8);
-      }
-      *reinterpret_cast<uint4*>(sA + tc::chunkOffset(r, t * CC + q, K)) = v;
+      if (yy >= 0 && yy < H && xx >= 0 && xx < W)
+        v = *reinterpret_cast<const uint4*>(X + ((size_t)(b * H + yy) * W + xx) * CIN + q * 8);
+      *reinterpret_cast<uint4*>(sIn + (r * CC + q) * kPlane + j * 16) = v;
     }
     tc::fenceProxyAsync();
     __syncthreads();
     tc::fenceAfterSync();
     if (tid == 0) {
-      const uint32_t aBase = tc::smemAddr(sA), bBase = tc::smemAddr(sB);
-      for (int s = 0; s < K / 16; ++s)
-        tc::mmaBf16(tmem, tc::smemDesc(aBase + s * 256, 128, KC * 128), tc::smemDesc(bBase + s * 256, 128, KC * 128),
-                    idesc, s > 0);
+      for (int t = 0; t < 9; ++t) {
+        int dy = t / 3 - 1, dx = t % 3 - 1;
+        if (TRANSPOSED) {  // gradient gathered at p - offset
+          dy = -dy;
+          dx = -dx;
+        }
+        for (int s = 0; s < CC / 2; ++s) {
+          const uint32_t aStart = inBase + (uint32_t)(((dy + 1) * CC + 2 * s) * kPlane + (1 + dx) * 16);
+          const uint32_t bStart = bBase + (uint32_t)((t * CC + 2 * s) * 128);
+          tc::mmaBf16(tmem, tc::smemDesc(aStart, kPlane, 128), tc::smemDesc(bStart, 128, KC * 128), idesc,
+                      t > 0 || s > 0);
+        }
+      }
       tc::commit(&bar);
     }
     ok = __syncthreads_and(tc::mbarWait(&bar, phase)) != 0;
@@ -220,19 +243,29 @@ __global__ void __launch_bounds__(128) k_convFwd(int B, int H, int W, const __nv
     if (!ok) break;
     float v[32];
     tc::tmemLoad32(tmem + ((uint32_t)(warp * 32) << 16), v);
-    const int p = p0 + warp * 32 + lane;
-    if (p < P) {
+    const int x = x0 + warp * 32 + lane;
+    if (x < W) {
+      const size_t p = (size_t)rowIdx * W + x;
       if (LAST) {
-        float4* z = reinterpret_cast<float4*>(Z + (size_t)p * kC);
+        float4* z = reinterpret_cast<float4*>(Z + p * kC);
 #pragma unroll
         for (int j = 0; j < kC; j += 4) z[j / 4] = make_float4(v[j] + bv[j], v[j + 1] + bv[j + 1], v[j + 2] + bv[j + 2], v[j + 3] + bv[j + 3]);
       } else {
         __align__(16) __nv_bfloat16 o[kC];
+        if (TRANSPOSED) {
+          __align__(16) __nv_bfloat16 xin[kC];
+          const uint4* xs = reinterpret_cast<const uint4*>(Xin + p * kC);
 #pragma unroll
-        for (int j = 0; j < kC; ++j) o[j] = __float2bfloat16_rn(fmaxf(v[j] + bv[j], 0.0f));
-        uint4* y = reinterpret_cast<uint4*>(Y + (size_t)p * kC);
+          for (int j = 0; j < 4; ++j) reinterpret_cast<uint4*>(xin)[j] = xs[j];
 #pragma unroll
-        for (int j = 0; j < 4; ++j) y[j] = reinterpret_cast<const uint4*>(o)[j];
+          for (int j = 0; j < kC; ++j) o[j] = __float2bfloat16_rn(__bfloat162float(xin[j]) > 0.0f ? v[j] : 0.0f);
+        } else {
+#pragma unroll
+          for (int j = 0; j < kC; ++j) o[j] = __float2bfloat16_rn(fmaxf(v[j] + bv[j], 0.0f));
+        }
+        uint4* yo = reinterpret_cast<uint4*>(Y + p * kC);
+#pragma unroll
+        for (int j = 0; j < 4; ++j) yo[j] = reinterpret_cast<const uint4*>(o)[j];
       }
     }
     tc::fenceBeforeSync();
@@ -247,84 +280,8 @@ __global__ void __launch_bounds__(128) k_convFwd(int B, int H, int W, const __nv
   if (warp == 0) tc::tmemFree(tmem, 32);
 }
 
-// Backward data of a 32 -> 32 (or 32 -> logits) convolution, fused with the
-// ReLU mask of its input: Gprev[p][ci] = bf16(mask(Xin[p][ci]) * sum_{t,co}
-// G[p - off(t)][co] * W[co][t][ci]).  Wt = W transposed to [ci][(t, co)].
-__global__ void __launch_bounds__(128) k_convBwdData(int B, int H, int W, const __nv_bfloat16* __restrict__ G,
-                                                     const __nv_bfloat16* __restrict__ Wt,
-                                                     const __nv_bfloat16* __restrict__ Xin,
-                                                     __nv_bfloat16* __restrict__ Gprev, int* __restrict__ err) {
-  constexpr int K = 9 * kC, KC = K / 8, CC = kC / 8;
-  extern __shared__ __align__(1024) unsigned char sm[];
-  __shared__ uint64_t bar;
-  __shared__ uint32_t tbase;
-  unsigned char* sA = sm;
-  unsigned char* sB = sm + (size_t)128 * K * 2;
-  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-  const int P = B * H * W, tiles = (P + 127) / 128;
-  if (warp == 0) tc::tmemAlloc(&tbase, 32);
-  if (tid == 0) tc::mbarInit(&bar, 1);
-  for (int c = tid; c < kC * KC; c += 128) {
-    const int r = c / KC, q = c % KC;
-    *reinterpret_cast<uint4*>(sB + tc::chunkOffset(r, q, K)) = *reinterpret_cast<const uint4*>(Wt + (size_t)r * K + q * 8);
-  }
-  __syncthreads();
-  const uint32_t tmem = tbase;
-  const uint32_t idesc = tc::instrDescBf16(128, kC);
-  uint32_t phase = 0;
-  bool ok = true;
-  for (int tile = blockIdx.x; tile < tiles; tile += gridDim.x) {
-    const int p0 = tile * 128;
-    for (int c = tid; c < 128 * 9 * CC; c += 128) {
-      const int r = c / (9 * CC), rem = c % (9 * CC), t = rem / CC, q = rem % CC;
-      const int p = p0 + r;
-      uint4 v = make_uint4(0, 0, 0, 0);
-      if (p < P) {
-        const int n = neighbor(p, -(t / 3 - 1), -(t % 3 - 1), H, W);
-        if (n >= 0) v = *reinterpret_cast<const uint4*>(G + (size_t)n * kC + q * 8);
-      }
-      *reinterpret_cast<uint4*>(sA + tc::chunkOffset(r, t * CC + q, K)) = v;
-    }
-    tc::fenceProxyAsync();
-    __syncthreads();
-    tc::fenceAfterSync();
-    if (tid == 0) {
-      const uint32_t aBase = tc::smemAddr(sA), bBase = tc::smemAddr(sB);
-      for (int s = 0; s < K / 16; ++s)
-        tc::mmaBf16(tmem, tc::smemDesc(aBase + s * 256, 128, KC * 128), tc::smemDesc(bBase + s * 256, 128, KC * 128),
-                    idesc, s > 0);
-      tc::commit(&bar);
-    }
-    ok = __syncthreads_and(tc::mbarWait(&bar, phase)) != 0;
-    phase ^= 1u;
-    tc::fenceAfterSync();
-    if (!ok) break;
-    float v[32];
-    tc::tmemLoad32(tmem + ((uint32_t)(warp * 32) << 16), v);
-    const int p = p0 + warp * 32 + lane;
-    if (p < P) {
-      __align__(16) __nv_bfloat16 xin[kC];
-      const uint4* xs = reinterpret_cast<const uint4*>(Xin + (size_t)p * kC);
-#pragma unroll
-      for (int j = 0; j < 4; ++j) reinterpret_cast<uint4*>(xin)[j] = xs[j];
-      __align__(16) __nv_bfloat16 o[kC];
-#pragma unroll
-      for (int j = 0; j < kC; ++j) o[j] = __float2bfloat16_rn(__bfloat162float(xin[j]) > 0.0f ? v[j] : 0.0f);
-      uint4* y = reinterpret_cast<uint4*>(Gprev + (size_t)p * kC);
-#pragma unroll
-      for (int j = 0; j < 4; ++j) y[j] = reinterpret_cast<const uint4*>(o)[j];
-    }
-    tc::fenceBeforeSync();
-    __syncthreads();
-  }
-  if (!ok) {
-    if (tid == 0) atomicCAS(err, 0, tc::kErrTcTimeout);
-    tc::mbarWait(&bar, phase ^ 1u);
-  }
-  tc::fenceBeforeSync();
-  __syncthreads();
-  if (warp == 0) tc::tmemFree(tmem, 32);
-}
+template <int CIN>
+constexpr size_t rowSmem() { return (size_t)3 * (CIN / 8) * kPlane + (size_t)kC * 9 * CIN * 2; }
 
 // Backward weights: partial[chunk][m = (t, ci)][co] = sum over the chunk's
 // pixels q of X[q + off(t)][ci] * G[q][co].  Grid: (M tiles of 128 rows,
@@ -623,6 +580,7 @@ struct KpcnNet {
   DevBuf<float> params, grad, m, v;
   DevBuf<__nv_bfloat16> wf[kLayers], wt[kLayers];
   int adamStep = 0;
+  float lastApplyMs = 0.0f, lastStepMs = 0.0f;  // device time of the last apply / mean training step
   std::mt19937 rng;
   // training examples (all W x H)
   int dsW = 0, dsH = 0, dsN = 0;
@@ -672,33 +630,30 @@ void packWeights(KpcnNet& n) {
   }
 }
 
-int persistentGrid(const KpcnNet& n, size_t P) {
-  const int tiles = (int)((P + 127) / 128);
-  return std::max(1, std::min(tiles, n.numSMs * 2));
+// X0 must be filled; writes act[0..4] and Z.
+int rowGrid(const KpcnNet& n, int B, int H, int W) {
+  const int tiles = B * H * ((W + 127) / 128);
+  return std::max(1, std::min(tiles, n.numSMs * 4));
 }
 
-// X0 must be filled; writes act[0..4] and Z.
 void forward(KpcnNet& n, int B, int H, int W) {
-  const size_t P = (size_t)B * H * W;
-  const int grid = persistentGrid(n, P);
-  const size_t smem16 = (size_t)(128 + kC) * 9 * 16 * 2, smem32 = (size_t)(128 + kC) * 9 * 32 * 2;
-  k_convFwd<16, false><<<grid, 128, smem16, n.st>>>(B, H, W, n.X0.p, n.wf[0].p, n.params.p + layerOffset(0) + layerWeights(0),
-                                                    n.act[0].p, nullptr, n.err.p);
+  const int grid = rowGrid(n, B, H, W);
+  k_convRow<16, false, false><<<grid, 128, rowSmem<16>(), n.st>>>(
+      B, H, W, n.X0.p, n.wf[0].p, n.params.p + layerOffset(0) + layerWeights(0), nullptr, n.act[0].p, nullptr, n.err.p);
   for (int l = 1; l < kLayers - 1; ++l)
-    k_convFwd<32, false><<<grid, 128, smem32, n.st>>>(B, H, W, n.act[l - 1].p, n.wf[l].p,
-                                                      n.params.p + layerOffset(l) + layerWeights(l), n.act[l].p, nullptr,
-                                                      n.err.p);
-  k_convFwd<32, true><<<grid, 128, smem32, n.st>>>(B, H, W, n.act[kLayers - 2].p, n.wf[kLayers - 1].p,
-                                                   n.params.p + layerOffset(kLayers - 1) + layerWeights(kLayers - 1),
-                                                   nullptr, n.Z.p, n.err.p);
+    k_convRow<32, false, false><<<grid, 128, rowSmem<32>(), n.st>>>(
+        B, H, W, n.act[l - 1].p, n.wf[l].p, n.params.p + layerOffset(l) + layerWeights(l), nullptr, n.act[l].p, nullptr,
+        n.err.p);
+  k_convRow<32, true, false><<<grid, 128, rowSmem<32>(), n.st>>>(
+      B, H, W, n.act[kLayers - 2].p, n.wf[kLayers - 1].p,
+      n.params.p + layerOffset(kLayers - 1) + layerWeights(kLayers - 1), nullptr, nullptr, n.Z.p, n.err.p);
 }
 
 // Head gradient must be in gA; fills n.grad.
 void backward(KpcnNet& n, int B, int H, int W) {
   const size_t P = (size_t)B * H * W;
   const int ch = chunksFor(P);
-  const int grid = persistentGrid(n, P);
-  const size_t smem32 = (size_t)(128 + kC) * 9 * 32 * 2;
+  const int grid = rowGrid(n, B, H, W);
   __nv_bfloat16* G = n.gA.p;
   __nv_bfloat16* Gn = n.gB.p;
   for (int l = kLayers - 1; l >= 0; --l) {
@@ -711,7 +666,8 @@ void backward(KpcnNet& n, int B, int H, int W) {
     k_biasPartial<<<ch, 128, 0, n.st>>>((int)P, G, n.bpartial.p);
     k_reduceBiasGrad<<<1, 32, 0, n.st>>>(ch, n.bpartial.p, n.grad.p + layerOffset(l) + layerWeights(l));
     if (l > 0) {
-      k_convBwdData<<<grid, 128, smem32, n.st>>>(B, H, W, G, n.wt[l].p, in, Gn, n.err.p);
+      k_convRow<32, false, true><<<grid, 128, rowSmem<32>(), n.st>>>(B, H, W, G, n.wt[l].p, nullptr, in, Gn, nullptr,
+                                                                    n.err.p);
       std::swap(G, Gn);
     }
   }
@@ -764,10 +720,10 @@ bool initNet(KpcnNet& n, uint32_t seed) {
   cudaMemcpyAsync(n.params.p, h.data(), sizeof(float) * kNumParams, cudaMemcpyHostToDevice, n.st);
   cudaMemsetAsync(n.m.p, 0, sizeof(float) * kNumParams, n.st);
   cudaMemsetAsync(n.v.p, 0, sizeof(float) * kNumParams, n.st);
-  setSmem(k_convFwd<16, false>, (size_t)(128 + kC) * 9 * 16 * 2);
-  setSmem(k_convFwd<32, false>, (size_t)(128 + kC) * 9 * 32 * 2);
-  setSmem(k_convFwd<32, true>, (size_t)(128 + kC) * 9 * 32 * 2);
-  setSmem(k_convBwdData, (size_t)(128 + kC) * 9 * 32 * 2);
+  setSmem(k_convRow<16, false, false>, rowSmem<16>());
+  setSmem(k_convRow<32, false, false>, rowSmem<32>());
+  setSmem(k_convRow<32, true, false>, rowSmem<32>());
+  setSmem(k_convRow<32, false, true>, rowSmem<32>());
   packWeights(n);
   return cudaStreamSynchronize(n.st) == cudaSuccess;
 }
@@ -932,6 +888,10 @@ rg_status rg_denoiser_train(rg_denoiser* d, int32_t steps, int32_t batch, float 
   const size_t Pi = (size_t)H * W, P = Pi * B;
   if (!rg::ensureWork(n, P)) return RG_ERR_OUT_OF_MEMORY;
   std::uniform_int_distribution<int> pick(0, n.dsN - 1);
+  cudaEvent_t e0, e1;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  cudaEventRecord(e0, n.st);
   for (int s = 0; s < steps; ++s) {
     for (int b = 0; b < B; ++b) {  // random examples into the batch
       const int e = pick(n.rng);
@@ -952,7 +912,20 @@ rg_status rg_denoiser_train(rg_denoiser* d, int32_t steps, int32_t batch, float 
     rg::packWeights(n);
     if (losses) cudaMemcpyAsync(losses + s, n.loss.p, sizeof(float), cudaMemcpyDeviceToHost, n.st);
   }
-  return rg::checkErr(n, "learned denoiser training");
+  cudaEventRecord(e1, n.st);
+  const rg_status rs = rg::checkErr(n, "learned denoiser training");
+  float ms = 0.0f;
+  if (rs == RG_OK && steps > 0 && cudaEventElapsedTime(&ms, e0, e1) == cudaSuccess) n.lastStepMs = ms / steps;
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  return rs;
+}
+
+rg_status rg_denoiser_timing(rg_denoiser* d, float* apply_ms, float* train_step_ms) {
+  if (!d) return RG_ERR_INVALID_ARGUMENT;
+  if (apply_ms) *apply_ms = d->net.lastApplyMs;
+  if (train_step_ms) *train_step_ms = d->net.lastStepMs;
+  return RG_OK;
 }
 
 rg_status rg_denoiser_gradients(rg_denoiser* d, int32_t count, int32_t w, int32_t h, const float* noisy_rgba,
@@ -985,10 +958,18 @@ rg_status rg_denoiser_apply(rg_denoiser* d, int32_t w, int32_t h, const float* n
   const size_t P = (size_t)w * h;
   if (!rg::ensureWork(n, P) || !rg::uploadInputs(n, P, noisy_rgba, normal, albedo, depth, nullptr))
     return RG_ERR_OUT_OF_MEMORY;
+  cudaEvent_t e0, e1;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  cudaEventRecord(e0, n.st);
   rg::forward(n, 1, h, w);
   rg::k_head<false><<<(unsigned)((P + 255) / 256), 256, 0, n.st>>>(1, h, w, n.Z.p, n.noisy.p, nullptr, n.out.p, nullptr,
                                                                     nullptr);
+  cudaEventRecord(e1, n.st);
   const rg_status rs = rg::checkErr(n, "learned denoiser");
+  if (rs == RG_OK) cudaEventElapsedTime(&n.lastApplyMs, e0, e1);
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
   if (rs != RG_OK) return rs;
   RG_CUDA_CHECK(cudaMemcpy(out_rgba, n.out.p, sizeof(float4) * P, cudaMemcpyDeviceToHost));
   return RG_OK;
