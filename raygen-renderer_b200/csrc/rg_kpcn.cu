@@ -15,7 +15,7 @@
 //                  by per-tap descriptors (k_convRow); B = weights;
 //   backward data  the same with the gradient, mirrored taps and transposed
 //                  weights, the ReLU mask of the layer input in the epilogue;
-//   backward wt.   rows = (tap, input channel), K = pixels (a chunk of 2048
+//   backward wt.   rows = (tap, input channel), K = pixels (a chunk of 512
 //                  per CTA, 128 at a time), B = the output gradient;
 //                  per-chunk partials reduced in chunk order (deterministic).
 // Activations and gradients are stored BF16 (NHWC, channels contiguous),
@@ -107,7 +107,7 @@ constexpr int kC = 32;          // hidden channels (and padded logits)
 constexpr int kKP = 25;         // predicted kernel taps (5 x 5)
 constexpr int kLayers = 6;
 __host__ __device__ constexpr int cinOf(int l) { return l == 0 ? 16 : 32; }  // 16, 32, 32, 32, 32, 32
-constexpr int kChunk = 2048;    // pixels per backward-weight CTA
+constexpr int kChunk = 512;     // pixels per backward-weight CTA
 constexpr int kSub = 128;       // pixels per backward-weight staging step
 constexpr float kLossEps = 0.01f;
 
