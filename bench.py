@@ -199,7 +199,15 @@ def run_jobs(args):
     srv.wait(w)
     srv.result(w)
     srv.close()
-    srv = rg.RenderServer(rg.RendererSettings(rrDepth=RR), hbm_budget_gb=120.0, max_resident_jobs=256)
+    # autotuner: wave size and launch widths on a probe sample of the mix (its first 32 jobs)
+    t0 = time.time()
+    probe = [(sc, sp["width"], sp["height"], sp["spp"], sp["depth"], sp["seed"])
+             for sp, sc in list(zip(specs, scenes))[:32]]
+    tuned = rg.RenderServer.autotune(probe, rg.RendererSettings(rrDepth=RR))
+    tune_s = time.time() - t0
+    srv = rg.RenderServer(rg.RendererSettings(rrDepth=RR), hbm_budget_gb=120.0, max_resident_jobs=256,
+                          paths_per_wave=tuned["paths_per_wave"], shade_blocks_per_sm=tuned["shade_blocks_per_sm"],
+                          trace_blocks_per_sm=tuned["trace_blocks_per_sm"])
     rng = np.random.default_rng(7)
     clock = ClockSampler(0)
     clock.start()
@@ -227,7 +235,7 @@ def run_jobs(args):
                                "emitters 1-64, side log-uniform 64-1024, spp log-uniform 1-256, depth 4-10)",
                    "mode": args.mode, "rate_per_s": args.rate if args.mode == "serve" else None,
                    "triangles_total": tris, "samples_total": samples, "scene_generation_s": round(gen_s, 1),
-                   "hbm_budget_gb": 120},
+                   "hbm_budget_gb": 120, "autotuned": dict(tuned, tuning_s=round(tune_s, 1))},
         "serve": {"images_per_s": round(st["images_per_s"], 2), "p50_ms": round(st["p50_ms"], 1),
                   "p99_ms": round(st["p99_ms"], 1), "mean_ms": round(st["mean_ms"], 1),
                   "max_ms": round(st["max_ms"], 1), "waves": st["waves"], "resident_peak": st["resident_peak"],

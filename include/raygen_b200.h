@@ -339,6 +339,8 @@ typedef struct rg_server_config {
   int32_t max_resident_jobs;  /* job slots [256]                               */
   int32_t paths_per_wave;     /* wavefront size shared by all jobs [8 Mi]      */
   int32_t max_depth_cap;      /* largest max_depth a job may use [10]          */
+  int32_t shade_blocks_per_sm;  /* shade / generate / accumulate width [0: 4]  */
+  int32_t trace_blocks_per_sm;  /* traversal width [0: occupancy limit]        */
 } rg_server_config;
 
 /* One render request.  The scene description is borrowed: it must stay valid
@@ -383,6 +385,14 @@ rg_status rg_server_get_result(rg_server* s, int64_t job_id, float* hdr_rgba, si
 /* Progressive result of a resident job (current sample mean), taken between waves. */
 rg_status rg_server_snapshot(rg_server* s, int64_t job_id, float* hdr_rgba, size_t count, double timeout_ms);
 rg_status rg_server_get_stats(rg_server* s, rg_server_stats* out);
+/* Autotuner: renders the probe jobs with candidate wave sizes (paths_per_wave)
+ * and launch widths (shade_blocks_per_sm, trace_blocks_per_sm) on servers
+ * built from `cfg`, by coordinate descent on the wall time of the whole mix
+ * (a candidate replaces the incumbent when it is more than 3% faster), and
+ * writes the fastest into `cfg`.  best_ms (may be NULL): its wall time.  The
+ * probe should be a sample of the real mix (its spp included). */
+rg_status rg_server_autotune(const rg_settings* base, const rg_job_desc* probe, int32_t count, rg_server_config* cfg,
+                             double* best_ms);
 /* Learned denoiser for jobs submitted with denoise = 2 (NULL: A-Trous).  Keep
  * `d` alive while it is set. */
 rg_status rg_server_set_denoiser(rg_server* s, rg_denoiser* d);

@@ -142,7 +142,8 @@ class rg_stats(C.Structure):
 
 class rg_server_config(C.Structure):
     _fields_ = [("hbm_budget_bytes", C.c_uint64), ("max_resident_jobs", C.c_int32),
-                ("paths_per_wave", C.c_int32), ("max_depth_cap", C.c_int32)]
+                ("paths_per_wave", C.c_int32), ("max_depth_cap", C.c_int32),
+                ("shade_blocks_per_sm", C.c_int32), ("trace_blocks_per_sm", C.c_int32)]
 
 
 class rg_job_desc(C.Structure):
@@ -219,6 +220,8 @@ def load_library(path: str = LIB_PATH) -> C.CDLL:
         "rg_set_denoiser": (C.c_int, [C.c_void_p, C.c_void_p]),
         "rg_denoiser_timing": (C.c_int, [C.c_void_p, P(C.c_float), P(C.c_float)]),
         "rg_server_set_denoiser": (C.c_int, [C.c_void_p, C.c_void_p]),
+        "rg_server_autotune": (C.c_int, [P(rg_settings), P(rg_job_desc), C.c_int32, P(rg_server_config),
+                                         P(C.c_double)]),
         "rg_reapply_postprocess": (C.c_int, [C.c_void_p]),
         "rg_scene_builtin": (C.c_int, [C.c_int32, C.c_uint32, P(C.c_int32), C.c_int32, P(P(rg_scene_desc))]),
         "rg_scene_free": (C.c_int, [P(rg_scene_desc)]),
@@ -737,18 +740,48 @@ class RenderServer:
     """
 
     def __init__(self, settings: Optional[RendererSettings] = None, hbm_budget_gb: float = 120.0,
-                 max_resident_jobs: int = 256, paths_per_wave: int = 8 << 20, max_depth_cap: int = 10):
+                 max_resident_jobs: int = 256, paths_per_wave: int = 8 << 20, max_depth_cap: int = 10,
+                 shade_blocks_per_sm: int = 0, trace_blocks_per_sm: int = 0):
         self._lib = load_library()
-        cfg = rg_server_config()
-        self._lib.rg_server_config_default(C.byref(cfg))
-        cfg.hbm_budget_bytes = int(hbm_budget_gb * (1 << 30))
-        cfg.max_resident_jobs = max_resident_jobs
-        cfg.paths_per_wave = paths_per_wave
-        cfg.max_depth_cap = max_depth_cap
+        cfg = self._config(hbm_budget_gb, max_resident_jobs, paths_per_wave, max_depth_cap, shade_blocks_per_sm,
+                           trace_blocks_per_sm)
         base = (settings or RendererSettings()).to_c()
         self._h = C.c_void_p()
         _check(self._lib.rg_server_create(C.byref(base), C.byref(cfg), C.byref(self._h)))
         self._jobs = {}
+
+    @staticmethod
+    def _config(hbm_budget_gb=120.0, max_resident_jobs=256, paths_per_wave=8 << 20, max_depth_cap=10,
+                shade_blocks_per_sm=0, trace_blocks_per_sm=0):
+        cfg = rg_server_config()
+        load_library().rg_server_config_default(C.byref(cfg))
+        cfg.hbm_budget_bytes = int(hbm_budget_gb * (1 << 30))
+        cfg.max_resident_jobs = max_resident_jobs
+        cfg.paths_per_wave = paths_per_wave
+        cfg.max_depth_cap = max_depth_cap
+        cfg.shade_blocks_per_sm = shade_blocks_per_sm
+        cfg.trace_blocks_per_sm = trace_blocks_per_sm
+        return cfg
+
+    @staticmethod
+    def autotune(probe, settings: Optional[RendererSettings] = None, hbm_budget_gb: float = 120.0,
+                 max_resident_jobs: int = 256, max_depth_cap: int = 10) -> dict:
+        """Pick paths_per_wave / shade_blocks_per_sm / trace_blocks_per_sm for a job mix.
+
+        probe: list of (scene, width, height, samples, max_depth, seed).  Returns the
+        constructor keyword arguments of the fastest configuration plus its probe time."""
+        lib = load_library()
+        jobs = (rg_job_desc * len(probe))()
+        for k, (sc, w, h, spp, depth, seed) in enumerate(probe):
+            jobs[k].scene = sc.ptr
+            jobs[k].width, jobs[k].height, jobs[k].samples = w, h, spp
+            jobs[k].max_depth, jobs[k].rr_depth, jobs[k].seed, jobs[k].denoise = depth, 0, seed, 0
+        cfg = RenderServer._config(hbm_budget_gb, max_resident_jobs, 8 << 20, max_depth_cap)
+        base = (settings or RendererSettings()).to_c()
+        best = C.c_double()
+        _check(lib.rg_server_autotune(C.byref(base), jobs, len(probe), C.byref(cfg), C.byref(best)))
+        return {"paths_per_wave": cfg.paths_per_wave, "shade_blocks_per_sm": cfg.shade_blocks_per_sm,
+                "trace_blocks_per_sm": cfg.trace_blocks_per_sm, "probe_ms": best.value}
 
     def submit(self, scene: Scene, width: int, height: int, samples: int, max_depth: int = 8, rr_depth: int = 3,
                seed: int = 1, denoise=False) -> int:

@@ -167,18 +167,22 @@ bool allocServer(rg_server* s) {
 // Capture the multi-job wave (generate, bounce loop, accumulate) once.
 bool captureGraph(rg_server* s) {
   const DevQueues Q = serverQueues(s);
-  const int ext = s->numSMs * residentBlocks(0, 8), conn = s->numSMs * residentBlocks(1, 8);
+  // traversal: persistent warps, blocks per SM up to the occupancy limit
+  const int tb = s->cfg.trace_blocks_per_sm;
+  const int ext = s->numSMs * (tb > 0 ? std::min(tb, residentBlocks(0, 8)) : residentBlocks(0, 8));
+  const int conn = s->numSMs * (tb > 0 ? std::min(tb, residentBlocks(1, 8)) : residentBlocks(1, 8));
+  const int shadeGrid = s->numSMs * (s->cfg.shade_blocks_per_sm > 0 ? s->cfg.shade_blocks_per_sm : 4);
   cudaGraph_t g;
   if (cudaStreamBeginCapture(s->stream, cudaStreamCaptureModeThreadLocal) != cudaSuccess) return false;
-  launchGenerate(s->jobTable.p, s->waveSlot.p, Q, s->numSMs * 8, s->stream);
+  launchGenerate(s->jobTable.p, s->waveSlot.p, Q, shadeGrid * 2, s->stream);
   for (int it = 0; it < Q.maxIter; it++) {
     launchExtend(nullptr, s->jobTable.p, 8, Q, it, ext, s->stream);
-    launchShade(nullptr, nullptr, s->jobTable.p, Q, it, s->numSMs * 4, s->stream);
+    launchShade(nullptr, nullptr, s->jobTable.p, Q, it, shadeGrid, s->stream);
     launchConnect(nullptr, s->jobTable.p, 8, Q, it, 0, conn, s->stream);
     launchConnect(nullptr, s->jobTable.p, 8, Q, it, 1, conn, s->stream);
     launchConnect(nullptr, s->jobTable.p, 8, Q, it, 2, conn, s->stream);
   }
-  launchAccumulate(s->jobTable.p, s->waveSlot.p, Q, s->numSMs * 4, s->stream);
+  launchAccumulate(s->jobTable.p, s->waveSlot.p, Q, shadeGrid, s->stream);
   if (cudaStreamEndCapture(s->stream, &g) != cudaSuccess) return false;
   const bool ok = cudaGraphInstantiate(&s->graph, g, 0) == cudaSuccess;
   cudaGraphDestroy(g);
@@ -593,6 +597,66 @@ rg_status rg_server_snapshot(rg_server* s, int64_t job, float* hdr_rgba, size_t 
   const std::vector<float>& src = j->snapshotReady ? j->snapshot : j->result;
   if (count < src.size() || src.empty()) return RG_ERR_BUSY;
   std::memcpy(hdr_rgba, src.data(), src.size() * sizeof(float));
+  return RG_OK;
+}
+
+// Wall time of one probe mix on a server built from cfg (all jobs at t = 0).
+static rg_status probeMix(const rg_settings* base, const rg_job_desc* probe, int32_t count,
+                          const rg_server_config& cfg, double& ms) {
+  rg_server* s = nullptr;
+  rg_status rs = rg_server_create(base, &cfg, &s);
+  if (rs != RG_OK) return rs;
+  std::vector<int64_t> ids(count);
+  const auto t0 = std::chrono::steady_clock::now();
+  for (int i = 0; i < count && rs == RG_OK; i++) rs = rg_server_submit(s, &probe[i], &ids[i]);
+  for (int i = 0; i < count && rs == RG_OK; i++) {
+    rs = rg_server_wait(s, ids[i], 3.6e6);
+    rg_job_status js;
+    if (rs == RG_OK && rg_server_poll(s, ids[i], &js) == RG_OK && js.state == RG_JOB_FAILED) rs = js.error;
+  }
+  ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+  rg_server_destroy(s);
+  return rs;
+}
+
+rg_status rg_server_autotune(const rg_settings* base, const rg_job_desc* probe, int32_t count, rg_server_config* cfg,
+                             double* best_ms) {
+  if (!probe || count <= 0 || !cfg) return RG_ERR_INVALID_ARGUMENT;
+  rg_server_config best = *cfg;
+  double bestMs = 0.0, ms = 0.0;
+  rg_status rs = probeMix(base, probe, count, best, ms);  // warm-up (modules, allocator)
+  if (rs != RG_OK) return rs;
+  rs = probeMix(base, probe, count, best, bestMs);
+  if (rs != RG_OK) return rs;
+  auto tryCfg = [&](rg_server_config c) -> rg_status {
+    double t = 0.0;
+    const rg_status r = probeMix(base, probe, count, c, t);
+    if (r == RG_ERR_OUT_OF_MEMORY) return RG_OK;  // a candidate that does not fit is skipped
+    if (r != RG_OK) return r;
+    if (t < 0.97 * bestMs) {  // a clear win only: wall-time noise must not move the choice
+      bestMs = t;
+      best = c;
+    }
+    return RG_OK;
+  };
+  // coordinate descent: wave size, then shade width, then traversal width
+  for (int ppw : {1 << 18, 1 << 19, 1 << 20, 1 << 21, 1 << 22, 1 << 23}) {
+    rg_server_config c = best;
+    c.paths_per_wave = ppw;
+    if (c.paths_per_wave != cfg->paths_per_wave && (rs = tryCfg(c)) != RG_OK) return rs;
+  }
+  for (int sb : {2, 4, 8, 16}) {
+    rg_server_config c = best;
+    c.shade_blocks_per_sm = sb;
+    if ((rs = tryCfg(c)) != RG_OK) return rs;
+  }
+  for (int tb : {2, 4, 6}) {
+    rg_server_config c = best;
+    c.trace_blocks_per_sm = tb;
+    if ((rs = tryCfg(c)) != RG_OK) return rs;
+  }
+  *cfg = best;
+  if (best_ms) *best_ms = bestMs;
   return RG_OK;
 }
 

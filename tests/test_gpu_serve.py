@@ -78,3 +78,21 @@ def test_progressive_snapshot(rg):
     final = srv.result(j)
     assert final[..., :3].mean() > 0
     srv.close()
+
+
+def test_autotuner_config_is_valid_and_keeps_results(rg):
+    scenes = _scenes(rg, 4, seed0=300)
+    probe = [(sc, 48, 48, 4, 5, 10 + k) for k, sc in enumerate(scenes)]
+    t = rg.RenderServer.autotune(probe, max_resident_jobs=8)
+    assert t["paths_per_wave"] in {1 << p for p in range(18, 24)}
+    assert t["shade_blocks_per_sm"] in {0, 2, 4, 8, 16} and t["trace_blocks_per_sm"] in {0, 2, 4, 6}
+    assert t["probe_ms"] > 0
+    out = []
+    for kw in ({}, {k: t[k] for k in ("paths_per_wave", "shade_blocks_per_sm", "trace_blocks_per_sm")}):
+        srv = rg.RenderServer(max_resident_jobs=8, **kw)
+        j = srv.submit(scenes[0], 64, 48, 8, max_depth=5, seed=3)
+        srv.wait(j)
+        out.append(srv.result(j))
+        srv.close()
+    # the path RNG is keyed by (seed, pixel, sample): wave size and launch widths do not change the image
+    np.testing.assert_allclose(out[0], out[1], rtol=1e-4, atol=1e-6)
