@@ -102,15 +102,76 @@ typedef struct rg_material {
   float tex_tiling[2];
 } rg_material;
 
-/* Homogeneous participating medium (medium.h:37-334, constant emission). */
+/* One control point of a path-mode emission tube (HomogeneousMedium::PathSample,
+ * medium.h:55-59). */
+typedef struct rg_medium_path_point {
+  float p[3];                 /* world space                                  */
+  float radius;               /* tube radius here (lerped along a segment)    */
+  float t;                    /* axial parameter: inner -> outer colour blend */
+} rg_medium_path_point;
+
+enum { RG_EMISSION_CONSTANT = 0, RG_EMISSION_CONE = 1, RG_EMISSION_PATH = 2 };
+enum { RG_DENSITY_NONE = 0, RG_DENSITY_FBM = 1 };
+
+/* Participating medium (HomogeneousMedium, medium.h:37-334; readMedium,
+ * sceneloader.cpp:202-334).  A zero-initialised medium past `density` is the
+ * homogeneous constant-emission medium; rg_medium_defaults() fills the
+ * reference's defaults for the procedural fields (medium.h:80-199).
+ *  - emission_mode CONE: sigma_e(p) is the afterburner profile around the
+ *    axis cone_origin + s * cone_axis, s in [0, cone_length] (emissionAt,
+ *    medium.cpp:303-404); PATH: a tube along path_points (medium.cpp:310-354).
+ *    Both are integrated along each segment with cone/path_emission_samples
+ *    stratified samples (emissionIntegralAlongRay, medium.cpp:443-473).
+ *  - cone_origin / cone_axis and path_points are world space for the CONE and
+ *    PATH modes respectively (the loader applies the owning object's transform
+ *    when coneFollowObject / pathFollowObject is set).  In every other mode
+ *    the renderer uses cone_origin / cone_axis as given, in camera space, as
+ *    the reference's un-baked values are (only the heat-haze falloff reads
+ *    them then; HomogeneousMedium::bake, medium.cpp:59-101).
+ *  - density_field FBM: every sigma is scaled by a fractal value-noise field
+ *    evaluated in camera space, max(0, noise_amplitude * fbm + noise_bias),
+ *    and free flights use delta tracking (medium.cpp:276-301, 406-441).
+ *  - heat_haze: rays crossing the medium are bent by the gradient of
+ *    n(p) = 1 + ior_amplitude * (2 fbm - 1) over ior_march_steps steps and
+ *    the sigma terms are ignored (bendRay, medium.cpp:191-274).
+ * Octave, sample and march-step counts above 64 are clamped to 64. */
 typedef struct rg_medium {
   float sigma_a[3], sigma_s[3], sigma_e[3];
   float g, density;
+  int32_t emission_mode;      /* RG_EMISSION_*                                */
+  float cone_origin[3], cone_axis[3];
+  float cone_length, cone_radius;
+  float cone_inner[3], cone_outer[3];
+  float cone_intensity, cone_peak_axial, cone_peak_sharpness;
+  int32_t cone_emission_samples;
+  int32_t num_path_points;
+  const rg_medium_path_point* path_points;
+  float path_inner[3], path_outer[3];
+  float path_intensity, path_falloff_power;
+  int32_t path_emission_samples;
+  int32_t density_field;      /* RG_DENSITY_*                                 */
+  float noise_frequency;
+  int32_t noise_octaves;
+  float noise_gain, noise_lacunarity, noise_amplitude, noise_bias;
+  float noise_offset[3];
+  int32_t heat_haze;          /* 0 off                                        */
+  float ior_amplitude, ior_frequency;
+  int32_t ior_octaves;
+  float ior_gain, ior_lacunarity;
+  int32_t ior_march_steps;
+  float ior_offset[3];
+  float ior_falloff;
 } rg_medium;
 
 typedef struct rg_object {
   int32_t material;
   int32_t interior_medium;    /* -1 none */
+  /* SceneObject::location (local to the parent).  An object whose interior
+   * medium emits with constant sigma_e is a volume light anchored at this
+   * point taken as camera-relative world coordinates (sampleVolumeLightForNEE,
+   * rayrenderer.cpp:2091-2100).  An object may have no meshes: such an object
+   * only contributes its medium as a volume light. */
+  float location[3];
 } rg_object;
 
 /* A mesh-less emissive object of the reference (a point or spot light). */
@@ -122,7 +183,7 @@ typedef struct rg_point_light {
 
 typedef struct rg_camera {
   float location[3];
-  float angle[3];             /* degrees; see DESIGN.md for the order       */
+  float angle[3];             /* degrees; R = Ry(y) Rx(x) Rz(z)             */
   float field_of_view;        /* vertical, degrees                           */
   float view_near, view_far;
   float depth_of_field, aperture;
@@ -192,6 +253,9 @@ typedef struct rg_handle rg_handle;
 typedef void (*rg_progress_fn)(float progress, void* user);
 
 void rg_settings_default(rg_settings* s);
+/* Zero-fill `m` and set the reference's defaults of every medium field
+ * (density 1, cone / path / noise / heat-haze defaults of medium.h:80-199). */
+void rg_medium_defaults(rg_medium* m);
 rg_status rg_create(const rg_settings* s, rg_handle** out);
 rg_status rg_destroy(rg_handle* h);
 rg_status rg_update_settings(rg_handle* h, const rg_settings* s);
@@ -220,9 +284,17 @@ const char* rg_version(void);
  * rays: n x 6 floats (origin xyz, dir xyz) in view space.
  * closest: out_tuv n x 3 (t, u, v), out_prim n (DFS triangle id, -1 = miss).
  * any: tmax n floats; predicate 0 = area-light occluder, 1 = point/env
- *      occluder, 2 = AO occluder, 3 = every triangle; out_hit n bytes. */
+ *      occluder, 2 = AO occluder, 3 = every triangle, 4 = volume-light
+ *      occluder (rayrenderer.cpp:2167-2171); out_hit n bytes. */
 rg_status rg_trace_closest(rg_handle* h, const float* rays, int32_t n, float* out_tuv, int32_t* out_prim);
 rg_status rg_trace_any(rg_handle* h, const float* rays, const float* tmax, int32_t n, int32_t predicate, uint8_t* out_hit);
+/* Medium field queries on the scene's camera-space media (device work).
+ * eval: points n x 3 -> out n x 5 (densityAt, emissionAt rgb, iorAt;
+ *       medium.cpp:186-215, 276-404).
+ * bend: rays n x 7 (origin xyz, dir xyz, march length) -> out n x 6 (the
+ *       bent ray's origin and direction; bendRay, medium.cpp:237-274). */
+rg_status rg_medium_eval(rg_handle* h, int32_t medium, const float* points, int32_t n, float* out);
+rg_status rg_medium_bend(rg_handle* h, int32_t medium, const float* rays, int32_t n, float* out);
 /* View-space camera transform the scene was flattened with (4x4 row-major,
  * row-vector convention: p_view = [p 1] * M). */
 rg_status rg_get_view_matrix(rg_handle* h, float* m16);

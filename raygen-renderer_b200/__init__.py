@@ -41,7 +41,11 @@ RG_ADAPTIVE_PIXEL = 0
 RG_ADAPTIVE_TILE = 1
 
 # occluder predicates of rg_trace_any
-PRED_AREA, PRED_POINT, PRED_AO, PRED_ALL = 0, 1, 2, 3
+PRED_AREA, PRED_POINT, PRED_AO, PRED_ALL, PRED_VOLUME = 0, 1, 2, 3, 4
+
+# medium emission modes and density fields (rg_medium)
+RG_EMISSION_CONSTANT, RG_EMISSION_CONE, RG_EMISSION_PATH = 0, 1, 2
+RG_DENSITY_NONE, RG_DENSITY_FBM = 0, 1
 
 
 class RayGenError(RuntimeError):
@@ -84,13 +88,33 @@ class rg_material(C.Structure):
     ]
 
 
+class rg_medium_path_point(C.Structure):
+    _fields_ = [("p", C.c_float * 3), ("radius", C.c_float), ("t", C.c_float)]
+
+
 class rg_medium(C.Structure):
     _fields_ = [("sigma_a", C.c_float * 3), ("sigma_s", C.c_float * 3), ("sigma_e", C.c_float * 3),
-                ("g", C.c_float), ("density", C.c_float)]
+                ("g", C.c_float), ("density", C.c_float),
+                ("emission_mode", C.c_int32),
+                ("cone_origin", C.c_float * 3), ("cone_axis", C.c_float * 3),
+                ("cone_length", C.c_float), ("cone_radius", C.c_float),
+                ("cone_inner", C.c_float * 3), ("cone_outer", C.c_float * 3),
+                ("cone_intensity", C.c_float), ("cone_peak_axial", C.c_float), ("cone_peak_sharpness", C.c_float),
+                ("cone_emission_samples", C.c_int32),
+                ("num_path_points", C.c_int32), ("path_points", C.POINTER(rg_medium_path_point)),
+                ("path_inner", C.c_float * 3), ("path_outer", C.c_float * 3),
+                ("path_intensity", C.c_float), ("path_falloff_power", C.c_float),
+                ("path_emission_samples", C.c_int32),
+                ("density_field", C.c_int32), ("noise_frequency", C.c_float), ("noise_octaves", C.c_int32),
+                ("noise_gain", C.c_float), ("noise_lacunarity", C.c_float), ("noise_amplitude", C.c_float),
+                ("noise_bias", C.c_float), ("noise_offset", C.c_float * 3),
+                ("heat_haze", C.c_int32), ("ior_amplitude", C.c_float), ("ior_frequency", C.c_float),
+                ("ior_octaves", C.c_int32), ("ior_gain", C.c_float), ("ior_lacunarity", C.c_float),
+                ("ior_march_steps", C.c_int32), ("ior_offset", C.c_float * 3), ("ior_falloff", C.c_float)]
 
 
 class rg_object(C.Structure):
-    _fields_ = [("material", C.c_int32), ("interior_medium", C.c_int32)]
+    _fields_ = [("material", C.c_int32), ("interior_medium", C.c_int32), ("location", C.c_float * 3)]
 
 
 class rg_point_light(C.Structure):
@@ -223,6 +247,9 @@ def load_library(path: str = LIB_PATH) -> C.CDLL:
         "rg_server_autotune": (C.c_int, [P(rg_settings), P(rg_job_desc), C.c_int32, P(rg_server_config),
                                          P(C.c_double)]),
         "rg_reapply_postprocess": (C.c_int, [C.c_void_p]),
+        "rg_medium_defaults": (None, [P(rg_medium)]),
+        "rg_medium_eval": (C.c_int, [C.c_void_p, C.c_int32, P(C.c_float), C.c_int32, P(C.c_float)]),
+        "rg_medium_bend": (C.c_int, [C.c_void_p, C.c_int32, P(C.c_float), C.c_int32, P(C.c_float)]),
         "rg_scene_builtin": (C.c_int, [C.c_int32, C.c_uint32, P(C.c_int32), C.c_int32, P(P(rg_scene_desc))]),
         "rg_scene_free": (C.c_int, [P(rg_scene_desc)]),
         "rg_load_scene_json": (C.c_int, [C.c_char_p, P(P(rg_scene_desc))]),
@@ -242,6 +269,33 @@ def load_library(path: str = LIB_PATH) -> C.CDLL:
         fn.argtypes = args
     _lib = lib
     return lib
+
+
+def medium(path_points=(), **fields) -> rg_medium:
+    """An rg_medium with the reference's defaults (rg_medium_defaults) and the
+    given fields (sequences for the vector fields).  path_points: sequence of
+    (xyz, radius, t); the array is kept alive by the returned structure."""
+    m = rg_medium()
+    load_library().rg_medium_defaults(C.byref(m))
+    for k, v in fields.items():
+        if not hasattr(m, k):
+            raise AttributeError(f"rg_medium has no field {k}")
+        cur = getattr(m, k)
+        if isinstance(cur, C.Array):
+            for i, x in enumerate(v):
+                cur[i] = x
+        else:
+            setattr(m, k, v)
+    if path_points:
+        arr = (rg_medium_path_point * len(path_points))()
+        for i, (p, radius, t) in enumerate(path_points):
+            arr[i].p[:] = [float(c) for c in p]
+            arr[i].radius = float(radius)
+            arr[i].t = float(t)
+        m.num_path_points = len(path_points)
+        m.path_points = arr
+        m._keep = arr
+    return m
 
 
 def _check(code: int) -> None:
@@ -425,7 +479,8 @@ class Scene:
             d.envmap_texture = int(envmap)
             d.envmap_intensity = float(envmap_intensity)
             d.envmap_rotation = float(envmap_rotation)
-        keep = (pos, nrm, tm, mo, objs, mats, meds, pls, uv, d, texs)
+        keep = (pos, nrm, tm, mo, objs, mats, meds, pls, uv, d, texs,
+                [getattr(m, "_keep", None) for m in media])
         return cls(C.pointer(d), False, keep)
 
     def arrays(self):
@@ -555,6 +610,20 @@ class RayRenderer:
         _check(self._lib.rg_trace_any(self._h, _fptr(rays), _fptr(tmax), n, predicate,
                                       out.ctypes.data_as(C.POINTER(C.c_uint8))))
         return out.astype(bool)
+
+    def medium_eval(self, medium: int, points: np.ndarray) -> np.ndarray:
+        """Camera-space points n x 3 -> n x 5 (density, emission rgb, ior) of medium `medium`."""
+        pts = np.ascontiguousarray(points, dtype=np.float32).reshape(-1, 3)
+        out = np.empty((pts.shape[0], 5), np.float32)
+        _check(self._lib.rg_medium_eval(self._h, medium, _fptr(pts), pts.shape[0], _fptr(out)))
+        return out
+
+    def medium_bend(self, medium: int, rays: np.ndarray) -> np.ndarray:
+        """Rays n x 7 (origin, direction, march length) -> bent rays n x 6 (heat haze)."""
+        r = np.ascontiguousarray(rays, dtype=np.float32).reshape(-1, 7)
+        out = np.empty((r.shape[0], 6), np.float32)
+        _check(self._lib.rg_medium_bend(self._h, medium, _fptr(r), r.shape[0], _fptr(out)))
+        return out
 
     def close(self):
         if self._h:

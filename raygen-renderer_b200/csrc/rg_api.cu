@@ -103,16 +103,127 @@ DevMaterial toDev(const rg_material& m) {
 }
 
 // HomogeneousMedium::prepare (medium.cpp:18-57), constant mode.
-DevMedium toDev(const rg_medium& m) {
+inline int capCount(int n) { return n > kMaxMediumCount ? kMaxMediumCount : n; }
+
+// One medium after HomogeneousMedium::prepare() and bake() (medium.cpp:18-101),
+// in camera space: cone origin / axis transformed for cone-mode media only,
+// path points for path-mode media only (the reference bakes nothing else),
+// and isActive() (medium.h:226-234).
+DevMedium toDev(const rg_medium& m, const Mat4& view, std::vector<DevPathPoint>& pts) {
   DevMedium d;
+  std::memset(&d, 0, sizeof(d));
   const float dn = std::fmax(0.0f, m.density);
   d.ssr = m.sigma_s[0] * dn; d.ssg = m.sigma_s[1] * dn; d.ssb = m.sigma_s[2] * dn;
   d.ser = m.sigma_e[0] * dn; d.seg = m.sigma_e[1] * dn; d.seb = m.sigma_e[2] * dn;
   d.str = m.sigma_a[0] * dn + d.ssr; d.stg = m.sigma_a[1] * dn + d.ssg; d.stb = m.sigma_a[2] * dn + d.ssb;
   d.hero = (d.str + d.stg + d.stb) * (1.0f / 3.0f);
   d.g = m.g;
-  d.pad = 0;
+  d.densityScale = dn;
+  d.mode = (m.emission_mode == RG_EMISSION_CONE || m.emission_mode == RG_EMISSION_PATH) ? m.emission_mode : 0;
+  d.field = m.density_field == RG_DENSITY_FBM ? 1 : 0;
+  d.tMaxHero = d.field ? d.hero * std::fmax(0.0f, m.noise_amplitude * 1.0f + m.noise_bias) : d.hero;
+  // cone frame
+  const float al2 = m.cone_axis[0] * m.cone_axis[0] + m.cone_axis[1] * m.cone_axis[1] + m.cone_axis[2] * m.cone_axis[2];
+  float axN[3] = {0.0f, 0.0f, -1.0f};
+  if (al2 > 1e-12f) {
+    const float inv = 1.0f / std::sqrt(al2);
+    for (int k = 0; k < 3; k++) axN[k] = m.cone_axis[k] * inv;
+  }
+  float org[3] = {m.cone_origin[0], m.cone_origin[1], m.cone_origin[2]}, ax[3] = {axN[0], axN[1], axN[2]};
+  if (d.mode == RG_EMISSION_CONE) {
+    xformPoint(view, m.cone_origin, org);
+    float av[3];
+    for (int j = 0; j < 3; j++) av[j] = (axN[0] * view.m[j] + axN[1] * view.m[4 + j]) + axN[2] * view.m[8 + j];
+    const float vl2 = av[0] * av[0] + av[1] * av[1] + av[2] * av[2];
+    if (vl2 > 1e-12f) {
+      const float inv = 1.0f / std::sqrt(vl2);
+      for (int k = 0; k < 3; k++) ax[k] = av[k] * inv;
+    }
+  }
+  d.cox = org[0]; d.coy = org[1]; d.coz = org[2];
+  d.cax = ax[0]; d.cay = ax[1]; d.caz = ax[2];
+  d.coneLength = m.cone_length; d.coneRadius = m.cone_radius;
+  d.cir = m.cone_inner[0]; d.cig = m.cone_inner[1]; d.cib = m.cone_inner[2];
+  d.cor = m.cone_outer[0]; d.cog = m.cone_outer[1]; d.cob = m.cone_outer[2];
+  d.coneIntensity = m.cone_intensity; d.conePeakAxial = m.cone_peak_axial; d.conePeakSharpness = m.cone_peak_sharpness;
+  d.coneSamples = capCount(m.cone_emission_samples);
+  // path tube
+  d.pathCount = std::max(0, m.num_path_points);
+  d.pathFirst = (int)pts.size();
+  if (d.mode == RG_EMISSION_PATH)
+    for (int i = 0; i < d.pathCount; i++) {
+      const rg_medium_path_point& q = m.path_points[i];
+      float pv[3];
+      xformPoint(view, q.p, pv);
+      pts.push_back(DevPathPoint{make_float4(pv[0], pv[1], pv[2], q.radius), make_float4(q.t, 0.0f, 0.0f, 0.0f)});
+    }
+  d.pir = m.path_inner[0]; d.pig = m.path_inner[1]; d.pib = m.path_inner[2];
+  d.por = m.path_outer[0]; d.pog = m.path_outer[1]; d.pob = m.path_outer[2];
+  d.pathIntensity = m.path_intensity; d.pathFalloff = m.path_falloff_power;
+  d.pathSamples = capCount(m.path_emission_samples);
+  // fBm density
+  d.nFreq = m.noise_frequency; d.nOct = capCount(m.noise_octaves); d.nGain = m.noise_gain; d.nLac = m.noise_lacunarity;
+  d.nAmp = m.noise_amplitude; d.nBias = m.noise_bias;
+  d.nox = m.noise_offset[0]; d.noy = m.noise_offset[1]; d.noz = m.noise_offset[2];
+  // heat haze
+  d.hazeOn = m.heat_haze != 0;
+  d.iAmp = m.ior_amplitude; d.iFreq = m.ior_frequency; d.iOct = capCount(m.ior_octaves); d.iGain = m.ior_gain;
+  d.iLac = m.ior_lacunarity; d.iSteps = capCount(m.ior_march_steps);
+  d.iox = m.ior_offset[0]; d.ioy = m.ior_offset[1]; d.ioz = m.ior_offset[2];
+  d.iFalloff = m.ior_falloff;
+  d.haze = d.hazeOn && d.iAmp > 0.0f && d.iSteps > 0;
+  const bool glow = d.ser != 0.0f || d.seg != 0.0f || d.seb != 0.0f;
+  d.active = d.hero > 0.0f || (d.mode == RG_EMISSION_CONE && d.coneIntensity > 0.0f) ||
+             (d.mode == RG_EMISSION_PATH && d.pathIntensity > 0.0f && d.pathCount >= 2) || (d.hazeOn && d.iAmp > 0.0f) ||
+             glow;
   return d;
+}
+
+// Camera-space media, the objects' interior media and the global medium with
+// inactive media removed (readMedium drops them, sceneloader.cpp:325-333),
+// the emissive volumes sampled by volume-light NEE in object order
+// (rayrenderer.cpp:180-206), and the shade-kernel variant the scene needs.
+struct MediaTables {
+  std::vector<DevMedium> media;
+  std::vector<DevPathPoint> pts;
+  std::vector<DevVolLight> vols;
+  std::vector<int> objMed;
+  int globalMedium = -1;
+  int level = 0;
+  bool hasHaze = false;
+};
+
+void buildMedia(const rg_scene_desc* d, const Mat4& view, MediaTables& T) {
+  T.media.resize(d->num_media);
+  for (int i = 0; i < d->num_media; i++) T.media[i] = toDev(d->media[i], view, T.pts);
+  auto live = [&](int m) { return m >= 0 && m < d->num_media && T.media[m].active ? m : -1; };
+  T.globalMedium = live(d->global_medium);
+  T.objMed.resize(d->num_objects);
+  std::vector<char> used(d->num_media, 0);
+  if (T.globalMedium >= 0) used[T.globalMedium] = 1;
+  for (int o = 0; o < d->num_objects; o++) {
+    const int m = live(d->objects[o].interior_medium);
+    T.objMed[o] = m;
+    if (m < 0) continue;
+    used[m] = 1;
+    const DevMedium& M = T.media[m];
+    const bool cone = M.mode == RG_EMISSION_CONE && M.coneIntensity > 0.0f;
+    const bool glow = M.mode == 0 && (M.ser != 0.0f || M.seg != 0.0f || M.seb != 0.0f);
+    if (cone || glow) {
+      float a[3];
+      xformPoint(view, d->objects[o].location, a);
+      T.vols.push_back(DevVolLight{m, a[0], a[1], a[2]});
+    }
+  }
+  bool any = false, procedural = !T.vols.empty();
+  for (int i = 0; i < d->num_media; i++) {
+    if (!used[i]) continue;
+    const DevMedium& M = T.media[i];
+    any = true;
+    if (M.mode != 0 || M.field != 0 || M.haze) procedural = true;
+    if (M.haze) T.hasHaze = true;
+  }
+  T.level = procedural ? 2 : (any ? 1 : 0);
 }
 
 
@@ -144,6 +255,7 @@ struct rg_handle {
   bool haveResult = false;
   // wavefront
   DevBuf<float4> rayO0, rayO1, rayD0, rayD1, hits, pathT, pathR, pathL, shO0, shO1, shO2, shD0, shD1, shD2, shC0, shC1, shC2;
+  DevBuf<float4> shO3, shD3, shC3;  // volume-light shadow queue, allocated for scenes with volume lights
   DevBuf<int2> pathPS;
   DevBuf<DevJob> jobsDev;
   DevBuf<DevSegment> segs;
@@ -170,7 +282,14 @@ struct rg_handle {
 namespace rg {
 namespace {
 
-rg_status ensureQueues(rg_handle* h, int capacity, int maxIter) {
+rg_status ensureQueues(rg_handle* h, int capacity, int maxIter, bool volQueue) {
+  if (volQueue) {
+    const size_t c = (size_t)std::max(capacity, h->capacity);
+    if (!h->shO3.alloc(c) || !h->shD3.alloc(c) || !h->shC3.alloc(c)) {
+      setLastError("out of device memory (wavefront queues)");
+      return RG_ERR_OUT_OF_MEMORY;
+    }
+  }
   if (capacity <= h->capacity && maxIter <= h->maxIter) return RG_OK;
   const size_t c = (size_t)std::max(capacity, h->capacity);
   const int mi = std::max(maxIter, h->maxIter);
@@ -204,6 +323,7 @@ DevQueues makeQueues(rg_handle* h, int maxIter) {
   Q.shO[0] = h->shO0.p; Q.shO[1] = h->shO1.p; Q.shO[2] = h->shO2.p;
   Q.shD[0] = h->shD0.p; Q.shD[1] = h->shD1.p; Q.shD[2] = h->shD2.p;
   Q.shC[0] = h->shC0.p; Q.shC[1] = h->shC1.p; Q.shC[2] = h->shC2.p;
+  Q.shO[3] = h->shO3.p; Q.shD[3] = h->shD3.p; Q.shC[3] = h->shC3.p;
   Q.counters = h->counters.p;
   Q.stats = h->stats.p;
   Q.error = h->error.p;
@@ -281,6 +401,7 @@ void enqueueWave(rg_handle* h, const DevRender& R, const DevQueues& Q, const Dev
       launchConnect(&h->dscene, jobs, width, Q, it, 0, g.conn, st);
       if (h->dscene.numPointLights > 0) launchConnect(&h->dscene, jobs, width, Q, it, 1, g.conn, st);
       if (h->dscene.envTex >= 0) launchConnect(&h->dscene, jobs, width, Q, it, 2, g.conn, st);
+      if (h->dscene.numVolLights > 0) launchConnect(&h->dscene, jobs, width, Q, it, 3, g.conn, st);
       if (profile) cudaEventRecord((*ev)[it * 4 + 3], st);
     }
   }
@@ -493,6 +614,12 @@ rg_status prepareScene(const rg_scene_desc* d, int bins, bool wide, cudaStream_t
     setLastError("global medium index out of range");
     return RG_ERR_INVALID_ARGUMENT;
   }
+  for (int i = 0; i < d->num_media; i++)
+    if (d->media[i].num_path_points < 0 || d->media[i].num_path_points > 1024 ||
+        (d->media[i].num_path_points > 0 && !d->media[i].path_points)) {
+      setLastError("medium path points: count outside [0, 1024] or no array");
+      return RG_ERR_INVALID_ARGUMENT;
+    }
   for (int i = 0; i < d->num_textures; i++)
     if (d->textures[i].width < 0 || d->textures[i].height < 0 ||
         (d->textures[i].width > 0 && d->textures[i].height > 0 && !d->textures[i].rgba)) {
@@ -511,13 +638,16 @@ rg_status prepareScene(const rg_scene_desc* d, int bins, bool wide, cudaStream_t
   // tables
   std::vector<int> meshTriCount(d->num_meshes, 0);
   for (int i = 0; i < nt; i++) meshTriCount[d->tri_mesh[i]]++;
-  std::vector<int> objMat(d->num_objects), objMed(d->num_objects);
-  for (int i = 0; i < d->num_objects; i++) { objMat[i] = d->objects[i].material; objMed[i] = d->objects[i].interior_medium; }
+  std::vector<int> objMat(d->num_objects);
+  for (int i = 0; i < d->num_objects; i++) objMat[i] = d->objects[i].material;
   std::vector<DevMaterial> mats(d->num_materials);
   for (int i = 0; i < d->num_materials; i++) mats[i] = toDev(d->materials[i]);
-  std::vector<DevMedium> media(d->num_media);
-  for (int i = 0; i < d->num_media; i++) media[i] = toDev(d->media[i]);
-  ds.globalMedium = d->global_medium;
+  MediaTables MT;
+  buildMedia(d, view, MT);
+  std::vector<int>& objMed = MT.objMed;
+  std::vector<DevMedium>& media = MT.media;
+  ds.globalMedium = MT.globalMedium;
+  ds.hasHaze = MT.hasHaze;
   // area lights (rayrenderer.cpp:333-353): emissive objects with meshes, object order
   std::vector<std::vector<int>> objMeshes(d->num_objects);
   for (int i = 0; i < d->num_meshes; i++) objMeshes[d->mesh_object[i]].push_back(i);
@@ -565,7 +695,8 @@ rg_status prepareScene(const rg_scene_desc* d, int bins, bool wide, cudaStream_t
   bool ok = ds.meshTriCount.upload(meshTriCount.data(), meshTriCount.size(), st) &&
             ds.meshObj.upload(d->mesh_object, d->num_meshes, st) && ds.objMat.upload(objMat.data(), objMat.size(), st) &&
             ds.objMedium.upload(objMed.data(), objMed.size(), st) && ds.mats.upload(mats.data(), mats.size(), st) &&
-            ds.media.upload(media.data(), media.size(), st) &&
+            ds.media.upload(media.data(), media.size(), st) && ds.pathPts.upload(MT.pts.data(), MT.pts.size(), st) &&
+            ds.volLights.upload(MT.vols.data(), MT.vols.size(), st) &&
             ds.areaLightObj.upload(areaLightObj.data(), areaLightObj.size(), st) &&
             ds.lightMeshList.upload(lightMeshList.data(), lightMeshList.size(), st) &&
             ds.lightObjMeshes.upload(lightObjMeshes.data(), lightObjMeshes.size(), st) &&
@@ -649,6 +780,10 @@ rg_status prepareScene(const rg_scene_desc* d, int bins, bool wide, cudaStream_t
   S.media = ds.media.p;
   S.numMedia = d->num_media;
   S.globalMedium = ds.globalMedium;
+  S.pathPts = ds.pathPts.p;
+  S.volLights = ds.volLights.p;
+  S.numVolLights = (int)MT.vols.size();
+  S.mediaLevel = MT.level;
   S.numAreaLights = ds.numAreaLights;
   S.areaLightObj = ds.areaLightObj.p;
   S.lightObjMeshes = ds.lightObjMeshes.p;
@@ -767,8 +902,10 @@ static rg_status runPass(rg_handle* h, const DevRender& R, int numPixels, const 
   }
   RG_CUDA_CHECK(cudaMemcpyAsync(h->segs.p, sg.data(), sg.size() * sizeof(DevSegment), cudaMemcpyHostToDevice, h->stream));
   const int capacity = std::min<long long>(cap, (long long)pixChunk * spw);
-  const int maxIter = R.maxDepth + 2;
-  rg_status rs = ensureQueues(h, capacity, maxIter);
+  // one segment per vertex plus the eye ray; a heat-haze crossing adds a
+  // segment without a vertex, at most one per medium entry
+  const int maxIter = h->scene->hasHaze ? 2 * R.maxDepth + 3 : R.maxDepth + 2;
+  rg_status rs = ensureQueues(h, capacity, maxIter, h->dscene.numVolLights > 0);
   if (rs != RG_OK) return rs;
   if (!h->waves.alloc(ws.size() + 1)) {
     setLastError("out of device memory (waves)");
@@ -802,7 +939,7 @@ static rg_status runPass(rg_handle* h, const DevRender& R, int numPixels, const 
   const std::string key = std::to_string((uintptr_t)h->waves.p) + ":" + std::to_string((uintptr_t)slot) + ":" +
                           std::to_string(maxIter) + ":" + std::to_string(R.shader) + ":" + std::to_string(h->capacity) +
                           ":" + std::to_string((uintptr_t)pixelList) + ":" + std::to_string((uintptr_t)h->jobsDev.p) + ":" +
-                          std::string((const char*)&R, sizeof(R));
+                          std::to_string((uintptr_t)h->shO3.p) + ":" + std::string((const char*)&R, sizeof(R));
   if (!profile && (h->graph == nullptr || h->graphKey != key)) {
     if (h->graph) {
       cudaGraphExecDestroy(h->graph);
@@ -1013,7 +1150,8 @@ rg_status rg_render(rg_handle* h) {
     for (int v : c) tot += (uint64_t)v;
     S.samples = tot;
   }
-  const int perWave = s.shader_provider == 5 ? (3 + (h->maxIter) * (3 + (h->dscene.numPointLights > 0))) : 4;
+  const int perIter = 3 + (h->dscene.numPointLights > 0) + (h->dscene.envTex >= 0) + (h->dscene.numVolLights > 0);
+  const int perWave = s.shader_provider == 5 ? (3 + h->maxIter * perIter) : 4;
   S.kernel_launches = wavesDone * perWave;
   if (derr != 0) {
     setLastError("device error flag raised: " + std::to_string(derr));
@@ -1093,6 +1231,37 @@ rg_status rg_get_stats(rg_handle* h, rg_stats* out) {
   return RG_OK;
 }
 
+namespace {
+rg_status mediumQuery(rg_handle* h, int32_t medium, bool bend, const float* in, int32_t n, float* out) {
+  if (!h || n < 0 || (n > 0 && (!in || !out))) return RG_ERR_INVALID_ARGUMENT;
+  std::lock_guard<std::mutex> lk(h->mu);
+  if (!h->hasScene) return RG_ERR_NO_SCENE;
+  if (medium < 0 || medium >= h->dscene.numMedia) return RG_ERR_INVALID_ARGUMENT;
+  if (n == 0) return RG_OK;
+  const int inW = bend ? 7 : 3, outW = bend ? 6 : 5;
+  DevBuf<float> di, dout;
+  DevBuf<DevJob> job;
+  DevJob J;
+  std::memset(&J, 0, sizeof(J));
+  J.S = h->dscene;
+  if (!di.upload(in, (size_t)n * inW, h->stream) || !dout.alloc((size_t)n * outW) || !job.upload(&J, 1, h->stream))
+    return RG_ERR_OUT_OF_MEMORY;
+  launchMediumQuery(job.p, medium, bend, di.p, n, dout.p, h->stream);
+  RG_CUDA_CHECK(cudaGetLastError());
+  RG_CUDA_CHECK(cudaMemcpyAsync(out, dout.p, sizeof(float) * (size_t)n * outW, cudaMemcpyDeviceToHost, h->stream));
+  RG_CUDA_CHECK(cudaStreamSynchronize(h->stream));
+  return RG_OK;
+}
+}  // namespace
+
+rg_status rg_medium_eval(rg_handle* h, int32_t medium, const float* points, int32_t n, float* out) {
+  return mediumQuery(h, medium, false, points, n, out);
+}
+
+rg_status rg_medium_bend(rg_handle* h, int32_t medium, const float* rays, int32_t n, float* out) {
+  return mediumQuery(h, medium, true, rays, n, out);
+}
+
 rg_status rg_get_view_matrix(rg_handle* h, float* m16) {
   if (!h || !m16) return RG_ERR_INVALID_ARGUMENT;
   std::memcpy(m16, h->view.m, sizeof(float) * 16);
@@ -1121,14 +1290,15 @@ rg_status rg_trace_closest(rg_handle* h, const float* rays, int32_t n, float* ou
 }
 
 rg_status rg_trace_any(rg_handle* h, const float* rays, const float* tmax, int32_t n, int32_t predicate, uint8_t* out) {
-  if (!h || n < 0 || predicate < 0 || predicate > 3 || (n > 0 && (!rays || !tmax || !out))) return RG_ERR_INVALID_ARGUMENT;
+  if (!h || n < 0 || predicate < 0 || predicate > 4 || (n > 0 && (!rays || !tmax || !out))) return RG_ERR_INVALID_ARGUMENT;
   std::lock_guard<std::mutex> lk(h->mu);
   if (!h->hasScene) return RG_ERR_NO_SCENE;
   if (n == 0) return RG_OK;
   DevBuf<float> r, tm;
   DevBuf<uint8_t> o;
   if (!r.upload(rays, (size_t)n * 6, h->stream) || !tm.upload(tmax, n, h->stream) || !o.alloc(n)) return RG_ERR_OUT_OF_MEMORY;
-  const uint32_t occ = predicate == 0 ? kOccArea : (predicate == 1 ? kOccPoint : (predicate == 2 ? kOccAO : kOccAll));
+  const uint32_t occs[5] = {kOccArea, kOccPoint, kOccAO, kOccAll, kOccVol};
+  const uint32_t occ = occs[predicate];
   launchQueryAny(h->dscene, r.p, tm.p, n, occ, o.p, h->stream);
   RG_CUDA_CHECK(cudaMemcpyAsync(out, o.p, n, cudaMemcpyDeviceToHost, h->stream));
   int derr = 0;

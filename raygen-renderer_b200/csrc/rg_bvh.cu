@@ -89,6 +89,7 @@ __global__ void k_prepTriangles(int n, const float* __restrict__ pos, const floa
   if (mt.transparency < 0.01f && mt.emission <= 0.0f) occ |= kOccArea;
   if (mt.emission <= 0.0f && (mt.transparency < 0.01f || mt.refraction > 0.1f)) occ |= kOccPoint;
   if (mt.transparency < 0.01f) occ |= kOccAO;
+  if (mt.emission <= 0.0f && mt.transparency < 0.01f && mt.refraction <= 0.1f) occ |= kOccVol;
   verts[(size_t)i * 3 + 0] = make_float4(v[0].x, v[0].y, v[0].z, __int_as_float(mesh));
   verts[(size_t)i * 3 + 1] = make_float4(e1.x, e1.y, e1.z, __uint_as_float(occ));
   verts[(size_t)i * 3 + 2] = make_float4(e2.x, e2.y, e2.z, 0.0f);

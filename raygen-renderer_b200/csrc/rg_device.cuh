@@ -13,6 +13,7 @@ constexpr float kMaxRayDistance = 1.0e6f;     // MAX_RAY_DISTANCE, raycommon.h:3
 constexpr float kRayMaxDistance = 100.0f;     // RAY_MAX_DISTANCE, rayrenderer.h:48
 constexpr float kRRMin = 0.05f, kRRMax = 0.95f;  // rayrenderer.cpp:44-45
 constexpr int kMaxLeaf = 8;                   // triangles per leaf in the device BVH
+constexpr int kMaxMediumCount = 64;           // cap on a medium's octaves, strata and march steps
 constexpr int kStackSize = 64;
 
 // occluder classes (bit per shadow-ray predicate)
@@ -20,6 +21,7 @@ constexpr uint32_t kOccArea = 1u;   // transparency < 0.01 && emission <= 0   (r
 constexpr uint32_t kOccPoint = 2u;  // emission <= 0 && (transparency < 0.01 || refraction > 0.1) (:2211-2215)
 constexpr uint32_t kOccAO = 4u;     // transparency < 0.01                    (:2388-2390)
 constexpr uint32_t kOccAll = 8u;
+constexpr uint32_t kOccVol = 16u;   // emission <= 0 && transparency < 0.01 && refraction <= 0.1 (:2167-2171)
 
 // -------------------------------------------------------------- structs ----
 struct DevMaterial {
@@ -32,11 +34,56 @@ struct DevMaterial {
   float pad;
 };
 
+// A participating medium in camera space (HomogeneousMedium after prepare()
+// and bake(), medium.cpp:18-101).  The first twelve words are all the
+// homogeneous branch reads.
 struct DevMedium {
   float ssr, ssg, ssb;   // sigma_s * density
   float ser, seg, seb;   // sigma_e * density
   float str, stg, stb;   // sigma_t
-  float hero, g, pad;
+  float hero, g;
+  int active;            // isActive(), medium.h:226-234
+  int mode;              // emission mode: 0 constant, 1 cone, 2 path
+  int field;             // density field: 0 none, 1 fBm
+  int haze;              // isHeatHaze(), medium.h:240-242
+  int hazeOn;            // the heatHaze switch alone (iorAt's test)
+  float tMaxHero;        // sigma_t_max_hero: delta-tracking majorant
+  float densityScale;    // max(0, density)
+  // cone (coneOriginR / coneAxisR: camera space)
+  float cox, coy, coz, cax, cay, caz;
+  float coneLength, coneRadius;
+  float cir, cig, cib, cor, cog, cob;
+  float coneIntensity, conePeakAxial, conePeakSharpness;
+  int coneSamples;
+  // path tube (points in DevScene::pathPts, camera space)
+  int pathFirst, pathCount;
+  float pir, pig, pib, por, pog, pob;
+  float pathIntensity, pathFalloff;
+  int pathSamples;
+  // fBm density
+  float nFreq;
+  int nOct;
+  float nGain, nLac, nAmp, nBias, nox, noy, noz;
+  // heat haze
+  float iAmp, iFreq;
+  int iOct;
+  float iGain, iLac;
+  int iSteps;
+  float iox, ioy, ioz, iFalloff;
+};
+
+// A path-tube control point: (p.xyz, radius) and (t, 0, 0, 0).
+struct DevPathPoint {
+  float4 pr;
+  float4 t;
+};
+
+// An emissive volume sampled by volume-light NEE (EmissiveVolumeSource,
+// rayrenderer.cpp:180-206): its medium and, for constant-mode media, the
+// owning object's location in camera space.
+struct DevVolLight {
+  int medium;
+  float ax, ay, az;
 };
 
 struct DevPointLight {
@@ -91,6 +138,11 @@ struct DevScene {
   float envIntensity, envCosY, envSinY, envTotal;
   const float* envMarg;       // H+1 marginal CDF over rows
   const float* envCond;       // H x (W+1) conditional CDFs
+  // procedural media and volume lights
+  const DevPathPoint* pathPts;
+  const DevVolLight* volLights;
+  int numVolLights;
+  int mediaLevel;             // 0 no active medium, 1 homogeneous only, 2 procedural / volume lights
 };
 
 // device error codes
@@ -165,9 +217,9 @@ struct DevQueues {
   float4* pathR;              // (rrT rgb, flags bits)
   float4* pathL;              // (L rgb, vertex bits)
   int2* pathPS;               // (pixel, sample) of every path
-  float4* shO[3];             // shadow queues A (area) / B (point) / C (environment): (origin, path id bits)
-  float4* shD[3];             // (dir, tmax)
-  float4* shC[3];             // (contribution rgb, job slot bits)
+  float4* shO[4];             // shadow queues A (area) / B (point) / C (environment) / D (volume): (origin, path id bits)
+  float4* shD[4];             // (dir, tmax)
+  float4* shC[4];             // (contribution rgb, job slot bits)
   int* counters;              // per-iteration counters, zeroed by the generate kernel
   unsigned long long* stats;  // [0] nodes closest [1] tris closest [2] nodes shadow [3] tris shadow [4] closest rays [5] shadow rays
   int* error;                 // first device error code
@@ -178,13 +230,19 @@ struct DevQueues {
 // counters layout: [k*kCountersPerIter + c] for iteration k
 enum CounterSlot {
   C_RAYS = 0, C_FETCH_EXT = 1, C_SHA = 2, C_SHB = 3, C_FETCH_SHA = 4, C_FETCH_SHB = 5, C_FETCH_SHADE = 6,
-  C_SHC = 7, C_FETCH_SHC = 8
+  C_SHC = 7, C_FETCH_SHC = 8, C_SHD = 9, C_FETCH_SHD = 10
 };
 constexpr int kCountersPerIter = 12;
-// shadow queue `which` (0 area, 1 point, 2 environment) -> its counter slots
-__host__ __device__ inline int shadowCountSlot(int which) { return which == 0 ? C_SHA : (which == 1 ? C_SHB : C_SHC); }
+// shadow queue `which` (0 area, 1 point, 2 environment, 3 volume) -> its counter slots
+__host__ __device__ inline int shadowCountSlot(int which) {
+  return which == 0 ? C_SHA : (which == 1 ? C_SHB : (which == 2 ? C_SHC : C_SHD));
+}
 __host__ __device__ inline int shadowFetchSlot(int which) {
-  return which == 0 ? C_FETCH_SHA : (which == 1 ? C_FETCH_SHB : C_FETCH_SHC);
+  return which == 0 ? C_FETCH_SHA : (which == 1 ? C_FETCH_SHB : (which == 2 ? C_FETCH_SHC : C_FETCH_SHD));
+}
+// occluder class of shadow queue `which`; point lights and the environment share one
+__host__ __device__ inline uint32_t shadowOccluder(int which) {
+  return which == 0 ? kOccArea : (which == 3 ? kOccVol : kOccPoint);
 }
 
 // path flags (pathR.w)
@@ -303,6 +361,7 @@ enum Slot {
   S_LOBE = 0, S_LIGHT = 1, S_MESH = 2, S_TRI = 3, S_VNDF0 = 4, S_VNDF1 = 5, S_RR = 6,
   S_FRESNEL = 7, S_CHROMA = 8, S_HEMI0 = 9, S_HEMI1 = 10, S_POINT = 11, S_ENV0 = 12,
   S_ENV1 = 13, S_FLIGHT = 14, S_PHASE0 = 15, S_PHASE1 = 16, S_MEDRR = 17, S_EYETR = 18,
+  S_DTSTEP = 19, S_DTACC = 20, S_EMIS = 21, S_VOLPICK = 22, S_VOLU = 23,
   S_LDS = 63
 };
 
@@ -318,6 +377,12 @@ struct Rng {
   }
   __device__ __forceinline__ float prng(int v, int slot) const {
     const uint32_t h = pcg4d_x(pixel, sample, ((uint32_t)v << 6) | (uint32_t)slot, seed);
+    return (float)(h >> 8) * (1.0f / 16777216.0f);
+  }
+  // k-th draw of a repeated use at vertex v (delta-tracking steps, emission
+  // strata); k = 0 is prng(v, slot).
+  __device__ __forceinline__ float prngk(int v, int slot, int k) const {
+    const uint32_t h = pcg4d_x(pixel, sample, ((uint32_t)k << 16) | ((uint32_t)v << 6) | (uint32_t)slot, seed);
     return (float)(h >> 8) * (1.0f / 16777216.0f);
   }
   __device__ __forceinline__ float lds(int dim) const {

@@ -16,6 +16,8 @@ namespace rg {
 
 struct DevMaterial;
 struct DevMedium;
+struct DevPathPoint;
+struct DevVolLight;
 struct DevScene;
 struct DevRender;
 
@@ -78,6 +80,7 @@ struct SceneStore {
   std::vector<rg_object> objects;
   std::vector<rg_material> materials;
   std::vector<rg_medium> media;
+  std::vector<std::vector<rg_medium_path_point>> mediumPaths;  // per medium; finalize() points media at them
   int32_t globalMedium = -1;
   std::vector<rg_point_light> pointLights;
   std::vector<TextureStore> textures;
@@ -110,7 +113,10 @@ struct DeviceScene {
   DevBuf<int> meshObj, meshTriCount, objMat, objMedium;
   DevBuf<DevMaterial> mats;
   DevBuf<DevMedium> media;
+  DevBuf<DevPathPoint> pathPts;
+  DevBuf<DevVolLight> volLights;
   int globalMedium = -1;
+  bool hasHaze = false;       // a heat-haze medium is in use: paths take extra segments
   DevBuf<int> areaLightObj, lightMeshList;
   DevBuf<int2> lightObjMeshes, lightMeshTris;
   DevBuf<float4> lightTris;

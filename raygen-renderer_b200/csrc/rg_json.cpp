@@ -677,16 +677,118 @@ void readMaterial(const JVal& j, rg_material& m) {
   }
 }
 
-// readMedium (sceneloader.cpp:202-245), constant-emission mode.  The JSON key
-// of the emission coefficient is "emission".
-void readMedium(const JVal& j, rg_medium& md) {
-  std::memset(&md, 0, sizeof(md));
-  md.density = 1.0f;
+// A medium as read from JSON; the owning object's transform is applied when
+// the object is flattened (coneFollowObject / pathFollowObject).
+struct MediumSpec {
+  rg_medium m;
+  std::vector<rg_medium_path_point> pts;
+  bool coneFollow = false, pathFollow = false;
+};
+
+bool readBool(const JVal& j, const char* k, bool& out) {
+  const JVal* v = j.get(k);
+  if (!v || v->type != JVal::Bool) return false;
+  out = v->b;
+  return true;
+}
+
+bool readInt(const JVal& j, const char* k, int32_t& out) {
+  const JVal* v = j.get(k);
+  if (!v || v->type != JVal::Num) return false;
+  out = (int32_t)v->n;
+  return true;
+}
+
+bool isString(const JVal& j, const char* k, const char* value) {
+  const JVal* v = j.get(k);
+  return v && v->type == JVal::Str && v->s == value;
+}
+
+// HomogeneousMedium::isActive after prepare() (medium.h:226-234, medium.cpp:18-57).
+bool mediumActive(const rg_medium& m, size_t numPathPoints) {
+  const float d = std::fmax(0.0f, m.density);
+  float st[3], se[3];
+  for (int k = 0; k < 3; k++) {
+    st[k] = m.sigma_a[k] * d + m.sigma_s[k] * d;
+    se[k] = m.sigma_e[k] * d;
+  }
+  const float hero = (st[0] + st[1] + st[2]) * (1.0f / 3.0f);
+  if (hero > 0.0f) return true;
+  if (m.emission_mode == RG_EMISSION_CONE && m.cone_intensity > 0.0f) return true;
+  if (m.emission_mode == RG_EMISSION_PATH && m.path_intensity > 0.0f && numPathPoints >= 2) return true;
+  if (m.heat_haze && m.ior_amplitude > 0.0f) return true;
+  return se[0] != 0.0f || se[1] != 0.0f || se[2] != 0.0f;
+}
+
+// An emissive volume registered for volume-light NEE (rayrenderer.cpp:193-203).
+bool emissiveVolume(const rg_medium& m) {
+  if (m.emission_mode == RG_EMISSION_CONE) return m.cone_intensity > 0.0f;
+  if (m.emission_mode != RG_EMISSION_CONSTANT) return false;
+  const float d = std::fmax(0.0f, m.density);
+  return m.sigma_e[0] * d != 0.0f || m.sigma_e[1] * d != 0.0f || m.sigma_e[2] * d != 0.0f;
+}
+
+// readMedium (sceneloader.cpp:202-334): every key over the member defaults;
+// false when the result is inactive, which the reference drops (the object
+// or scene keeps what it had).  The JSON key of sigma_e is "emission".
+bool readMedium(const JVal& j, MediumSpec& sp) {
+  rg_medium& md = sp.m;
+  rg_medium_defaults(&md);
+  sp.pts.clear();
   readVec3(j.get("sigma_a"), md.sigma_a);
   readVec3(j.get("sigma_s"), md.sigma_s);
   readVec3(j.get("emission"), md.sigma_e);
   j.num("g", md.g);
   j.num("density", md.density);
+  if (isString(j, "emissionMode", "cone")) md.emission_mode = RG_EMISSION_CONE;
+  else if (isString(j, "emissionMode", "path")) md.emission_mode = RG_EMISSION_PATH;
+  readVec3(j.get("coneAxis"), md.cone_axis);
+  readVec3(j.get("coneOrigin"), md.cone_origin);
+  j.num("coneLength", md.cone_length);
+  j.num("coneRadius", md.cone_radius);
+  readVec3(j.get("coneInner"), md.cone_inner);
+  readVec3(j.get("coneOuter"), md.cone_outer);
+  j.num("coneIntensity", md.cone_intensity);
+  j.num("conePeakAxial", md.cone_peak_axial);
+  j.num("conePeakSharpness", md.cone_peak_sharpness);
+  readInt(j, "coneEmissionSamples", md.cone_emission_samples);
+  readBool(j, "coneFollowObject", sp.coneFollow);
+  readVec3(j.get("pathInner"), md.path_inner);
+  readVec3(j.get("pathOuter"), md.path_outer);
+  j.num("pathIntensity", md.path_intensity);
+  j.num("pathFalloffPower", md.path_falloff_power);
+  readInt(j, "pathEmissionSamples", md.path_emission_samples);
+  readBool(j, "pathFollowObject", sp.pathFollow);
+  if (const JVal* arr = j.get("pathPoints")) {
+    if (arr->type == JVal::Arr)
+      for (const JVal& el : arr->arr) {
+        if (el.type != JVal::Obj) continue;
+        rg_medium_path_point q{{0.0f, 0.0f, 0.0f}, 0.1f, 0.0f};
+        readVec3(el.get("p"), q.p);
+        el.num("radius", q.radius);
+        el.num("t", q.t);
+        sp.pts.push_back(q);
+      }
+  }
+  if (isString(j, "densityField", "fbm")) md.density_field = RG_DENSITY_FBM;
+  j.num("noiseFrequency", md.noise_frequency);
+  readInt(j, "noiseOctaves", md.noise_octaves);
+  j.num("noiseGain", md.noise_gain);
+  j.num("noiseLacunarity", md.noise_lacunarity);
+  j.num("noiseAmplitude", md.noise_amplitude);
+  j.num("noiseBias", md.noise_bias);
+  readVec3(j.get("noiseOffset"), md.noise_offset);
+  bool haze = false;
+  if (readBool(j, "heatHaze", haze)) md.heat_haze = haze ? 1 : 0;
+  j.num("iorAmplitude", md.ior_amplitude);
+  j.num("iorFrequency", md.ior_frequency);
+  readInt(j, "iorOctaves", md.ior_octaves);
+  j.num("iorGain", md.ior_gain);
+  j.num("iorLacunarity", md.ior_lacunarity);
+  readInt(j, "iorMarchSteps", md.ior_march_steps);
+  readVec3(j.get("iorOffset"), md.ior_offset);
+  j.num("iorFalloff", md.ior_falloff);
+  return mediumActive(md, sp.pts.size());
 }
 
 struct Loader {
@@ -739,7 +841,8 @@ struct Loader {
   struct Node {
     std::vector<MeshTris> meshes;
     rg_material mat;
-    int medium = -1;
+    bool hasMedium = false;
+    MediumSpec medium;
     bool visible = true;
     bool isCamera = false;
     float loc[3] = {0, 0, 0}, ang[3] = {0, 0, 0}, scl[3] = {1, 1, 1};
@@ -858,12 +961,14 @@ struct Loader {
       } else if (k == "visible" && v.type == JVal::Bool) {
         n.visible = v.b;
       } else if (k == "medium") {
-        if (v.type == JVal::Obj) {
-          rg_medium md;
-          readMedium(v, md);
-          st.media.push_back(md);
-          if (root) st.globalMedium = (int)st.media.size() - 1;
-          else n.medium = (int)st.media.size() - 1;
+        MediumSpec sp;
+        if (v.type == JVal::Obj && readMedium(v, sp)) {
+          if (root) {
+            st.globalMedium = addMedium(sp, M4::ident());
+          } else {
+            n.medium = sp;
+            n.hasMedium = true;
+          }
         }
       } else if (k == "envmap") {
         if (!readEnvmap(v)) return false;
@@ -941,23 +1046,63 @@ struct Loader {
   bool haveCamera = false;
   const Node* cameraNode = nullptr;
 
+  // A medium into the scene, with the owning object's transform W applied to
+  // the cone and the path points when they follow the object
+  // (HomogeneousMedium::bake, medium.cpp:59-101; the camera part is applied
+  // at render set-up).  Returns its index.
+  int addMedium(const MediumSpec& sp, const M4& W) {
+    rg_medium md = sp.m;
+    std::vector<rg_medium_path_point> pts = sp.pts;
+    auto point = [&](float p[3]) {
+      double o[3];
+      for (int a = 0; a < 3; a++) o[a] = W.m[a][0] * p[0] + W.m[a][1] * p[1] + W.m[a][2] * p[2] + W.m[a][3];
+      for (int a = 0; a < 3; a++) p[a] = (float)o[a];
+    };
+    if (sp.coneFollow && md.emission_mode == RG_EMISSION_CONE) {
+      point(md.cone_origin);
+      double ax[3];
+      for (int a = 0; a < 3; a++)
+        ax[a] = W.m[a][0] * md.cone_axis[0] + W.m[a][1] * md.cone_axis[1] + W.m[a][2] * md.cone_axis[2];
+      for (int a = 0; a < 3; a++) md.cone_axis[a] = (float)ax[a];
+    }
+    if (sp.pathFollow && md.emission_mode == RG_EMISSION_PATH)
+      for (auto& q : pts) point(q.p);
+    md.num_path_points = 0;
+    md.path_points = nullptr;  // set by SceneStore::finalize
+    st.media.push_back(md);
+    st.mediumPaths.resize(st.media.size() - 1);
+    st.mediumPaths.push_back(std::move(pts));
+    return (int)st.media.size() - 1;
+  }
+
   // transformObject / transformScene (rayrenderer.cpp:156-363): depth first,
   // an object's own meshes before its children; invisible objects are
-  // skipped together with their children.
-  void flatten(const Node& n, const M4& parent) {
-    if (!n.visible || n.isCamera) return;
+  // skipped together with their children, except that any object whose
+  // interior medium emits (cone or constant sigma_e) is a volume light
+  // whether it is visible or has meshes (rayrenderer.cpp:180-206); such an
+  // object without rendered meshes becomes an object without meshes.
+  void flatten(const Node& n, const M4& parent, bool parentVisible = true) {
+    if (n.isCamera) return;
+    const bool vis = parentVisible && n.visible;
     const M4 W = parent * trs(n.loc, n.ang, n.scl);
-    if (!n.meshes.empty()) {
-      rg_object o;
+    const bool meshObject = vis && !n.meshes.empty();
+    const bool volume = n.hasMedium && emissiveVolume(n.medium.m);
+    int medium = -1;
+    if (n.hasMedium && (meshObject || volume)) medium = addMedium(n.medium, W);
+    if (meshObject || volume) {
+      rg_object o{};
       o.material = addMaterial(n.mat);
-      o.interior_medium = n.medium;
+      o.interior_medium = medium;
+      for (int a = 0; a < 3; a++) o.location[a] = n.loc[a];
       st.objects.push_back(o);
+    }
+    if (meshObject) {
       const int obj = (int)st.objects.size() - 1;
       for (auto& m : n.meshes) {
         st.meshObject.push_back(obj);
         emitMesh(m, W, (int)st.meshObject.size() - 1);
       }
-    } else if (n.mat.emission > 0.0f) {
+    } else if (vis && n.mat.emission > 0.0f) {
       // Mesh-less emissive object -> point light at the object's origin
       // (rayrenderer.cpp:333-353).  The reference builds the object-space
       // normal from sin/cos of RADIAN_TO_DEGREE(angle) although the angle is
@@ -982,7 +1127,7 @@ struct Loader {
       pl.material = addMaterial(n.mat);
       st.pointLights.push_back(pl);
     }
-    for (auto& c : n.children) flatten(*c, W);
+    for (auto& c : n.children) flatten(*c, W, vis);
   }
 };
 

@@ -89,7 +89,7 @@ struct SceneBuilder {
     return (int)st.materials.size() - 1;
   }
   int object(int mat, int medium = -1) {
-    rg_object o;
+    rg_object o{};
     o.material = mat;
     o.interior_medium = medium;
     st.objects.push_back(o);
@@ -404,6 +404,11 @@ void SceneStore::finalize() {
   desc.objects = objects.data();
   desc.num_materials = (int32_t)materials.size();
   desc.materials = materials.data();
+  mediumPaths.resize(media.size());
+  for (size_t i = 0; i < media.size(); i++) {
+    media[i].num_path_points = (int32_t)mediumPaths[i].size();
+    media[i].path_points = mediumPaths[i].empty() ? nullptr : mediumPaths[i].data();
+  }
   desc.num_media = (int32_t)media.size();
   desc.media = media.data();
   desc.global_medium = globalMedium;
@@ -423,6 +428,46 @@ void SceneStore::finalize() {
   desc.envmap_intensity = envmapIntensity;
   desc.envmap_rotation = envmapRotation;
 }
+
+}  // namespace rg
+
+// HomogeneousMedium's member defaults (medium.h:80-199, PathSample medium.h:55-59).
+extern "C" void rg_medium_defaults(rg_medium* m) {
+  if (!m) return;
+  std::memset(m, 0, sizeof(*m));
+  m->density = 1.0f;
+  m->cone_axis[2] = -1.0f;
+  m->cone_length = 1.0f;
+  m->cone_radius = 0.3f;
+  const float inner[3] = {0.6f, 0.7f, 1.0f}, outer[3] = {1.0f, 0.4f, 0.05f};
+  const float pInner[3] = {0.6f, 0.7f, 1.0f}, pOuter[3] = {0.3f, 0.4f, 0.6f};
+  for (int k = 0; k < 3; k++) {
+    m->cone_inner[k] = inner[k];
+    m->cone_outer[k] = outer[k];
+    m->path_inner[k] = pInner[k];
+    m->path_outer[k] = pOuter[k];
+  }
+  m->cone_intensity = 50.0f;
+  m->cone_emission_samples = 4;
+  m->cone_peak_axial = 0.15f;
+  m->cone_peak_sharpness = 5.0f;
+  m->path_intensity = 1.0f;
+  m->path_falloff_power = 2.0f;
+  m->path_emission_samples = 6;
+  m->noise_frequency = 1.0f;
+  m->noise_octaves = 4;
+  m->noise_gain = 0.5f;
+  m->noise_lacunarity = 2.0f;
+  m->noise_amplitude = 1.0f;
+  m->ior_amplitude = 0.005f;
+  m->ior_frequency = 4.0f;
+  m->ior_octaves = 3;
+  m->ior_gain = 0.5f;
+  m->ior_lacunarity = 2.0f;
+  m->ior_march_steps = 16;
+}
+
+namespace rg {
 
 rg_status buildBuiltinScene(int kind, uint32_t seed, const int32_t* ip, int nip, SceneStore** out) {
   SceneStore* st = new (std::nothrow) SceneStore();

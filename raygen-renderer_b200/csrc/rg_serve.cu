@@ -103,6 +103,7 @@ struct rg_server {
   DevBuf<DevSegment> segs;
   DevBuf<DevWave> waveSlot;
   DevBuf<float4> rayO0, rayO1, rayD0, rayD1, hits, pathT, pathR, pathL, shO0, shO1, shO2, shD0, shD1, shD2, shC0, shC1, shC2;
+  DevBuf<float4> shO3, shD3, shC3;  // volume-light shadow queue
   DevBuf<int2> pathPS;
   DevBuf<int> counters;
   DevBuf<unsigned long long> stats;
@@ -139,6 +140,7 @@ DevQueues serverQueues(rg_server* s) {
   Q.shO[0] = s->shO0.p; Q.shO[1] = s->shO1.p; Q.shO[2] = s->shO2.p;
   Q.shD[0] = s->shD0.p; Q.shD[1] = s->shD1.p; Q.shD[2] = s->shD2.p;
   Q.shC[0] = s->shC0.p; Q.shC[1] = s->shC1.p; Q.shC[2] = s->shC2.p;
+  Q.shO[3] = s->shO3.p; Q.shD[3] = s->shD3.p; Q.shC[3] = s->shC3.p;
   Q.counters = s->counters.p;
   Q.stats = s->stats.p;
   Q.error = s->errWord.p;
@@ -153,8 +155,8 @@ bool allocServer(rg_server* s) {
   bool ok = s->rayO0.alloc(c) && s->rayO1.alloc(c) && s->rayD0.alloc(c) && s->rayD1.alloc(c) && s->hits.alloc(c) &&
             s->pathT.alloc(c) && s->pathR.alloc(c) && s->pathL.alloc(c) && s->shO0.alloc(c) && s->shO1.alloc(c) &&
             s->shD0.alloc(c) && s->shD1.alloc(c) && s->shC0.alloc(c) && s->shC1.alloc(c) && s->pathPS.alloc(c) &&
-            s->shO2.alloc(c) && s->shD2.alloc(c) && s->shC2.alloc(c) &&
-            s->counters.alloc((size_t)(s->maxIter + 1) * kCountersPerIter) && s->stats.alloc(8) &&
+            s->shO2.alloc(c) && s->shD2.alloc(c) && s->shC2.alloc(c) && s->shO3.alloc(c) && s->shD3.alloc(c) &&
+            s->shC3.alloc(c) && s->counters.alloc((size_t)(s->maxIter + 1) * kCountersPerIter) && s->stats.alloc(8) &&
             s->errWord.alloc(1) && s->jobTable.alloc(slots) && s->segs.alloc((size_t)slots * 2) && s->waveSlot.alloc(1);
   if (!ok) return false;
   if (cudaMallocHost((void**)&s->hostSegs, sizeof(DevSegment) * (size_t)slots * 2) != cudaSuccess) return false;
@@ -181,6 +183,7 @@ bool captureGraph(rg_server* s) {
     launchConnect(nullptr, s->jobTable.p, 8, Q, it, 0, conn, s->stream);
     launchConnect(nullptr, s->jobTable.p, 8, Q, it, 1, conn, s->stream);
     launchConnect(nullptr, s->jobTable.p, 8, Q, it, 2, conn, s->stream);
+    launchConnect(nullptr, s->jobTable.p, 8, Q, it, 3, conn, s->stream);
   }
   launchAccumulate(s->jobTable.p, s->waveSlot.p, Q, shadeGrid, s->stream);
   if (cudaStreamEndCapture(s->stream, &g) != cudaSuccess) return false;

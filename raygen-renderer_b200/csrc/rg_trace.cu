@@ -16,6 +16,7 @@
 #include <cuda_fp16.h>
 
 #include "rg_device.cuh"
+#include "rg_medium.cuh"
 #include "rg_trace.cuh"
 #include "rg_traverse.cuh"
 
@@ -512,7 +513,7 @@ __global__ void __launch_bounds__(128) k_connect(const DevJob* __restrict__ jobs
   const float4* __restrict__ sO = Q.shO[which];
   const float4* __restrict__ sD = Q.shD[which];
   const float4* __restrict__ sC = Q.shC[which];
-  const uint32_t occ = which ? kOccPoint : kOccArea;  // point lights and the environment share one class
+  const uint32_t occ = shadowOccluder(which);
   const int lane = threadIdx.x & 31;
   uint32_t nodes = 0, tris = 0, rays = 0;
   for (;;) {
@@ -741,7 +742,7 @@ __global__ void __launch_bounds__(128) k_connect8(DevScene S0, const DevJob* __r
   const int count = Q.counters[iter * kCountersPerIter + shadowCountSlot(which)];
   uint32_t nodes = 0, tris = 0, rays = 0;
   traverseWave8<true, MULTI>(S0, jobs, count, &Q.counters[iter * kCountersPerIter + shadowFetchSlot(which)],
-                      Q.shO[which], Q.shD[which], which ? kOccPoint : kOccArea, nullptr, Q.shC[which], Q.pathL, nodes,
+                      Q.shO[which], Q.shD[which], shadowOccluder(which), nullptr, Q.shC[which], Q.pathL, nodes,
                       tris, rays);
   warpAddStat(&Q.stats[2], nodes);
   warpAddStat(&Q.stats[3], tris);
@@ -752,10 +753,12 @@ __global__ void __launch_bounds__(128) k_connect8(DevScene S0, const DevJob* __r
 // MULTI = false: one job whose scene and render constants come in as kernel
 // parameters (constant bank); MULTI = true: per-ray job slot into the table.
 // ENV = false drops the environment-map code (misses, environment NEE) for
-// scenes without one, MED = false the participating-medium branch for scenes
-// without media, so those scenes run a smaller kernel (instruction fetch is
-// this kernel's main stall).
-template <bool MULTI, bool ENV, bool MED>
+// scenes without one; MEDL selects the participating-medium code: 0 none,
+// 1 homogeneous media, 2 procedural media (fBm density with delta tracking,
+// cone / path emission, heat haze) and volume-light NEE.  Scenes without
+// those features run a smaller kernel (instruction fetch is this kernel's
+// main stall).
+template <bool MULTI, bool ENV, int MEDL>
 __global__ void __launch_bounds__(256) k_shade(DevScene S0, DevRender R0, const DevJob* __restrict__ jobs, DevQueues Q,
                                                int iter) {
   const int count = Q.counters[iter * kCountersPerIter + C_RAYS];
@@ -764,10 +767,11 @@ __global__ void __launch_bounds__(256) k_shade(DevScene S0, DevRender R0, const 
   const int rounded = ((count + 31) / 32) * 32;
   for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < rounded; q += stride) {
     const bool valid = q < count;
-    Shadow shA, shB, shE;  // area light / point light / environment
+    Shadow shA, shB, shE, shV;  // area light / point light / environment / volume light
     shA.on = false;
     shB.on = false;
     shE.on = false;
+    shV.on = false;
     bool cont = false;
     V3 no = v3(0, 0, 0), nd = v3(0, 0, 0);
     int pid = 0, slot = 0;
@@ -798,24 +802,54 @@ __global__ void __launch_bounds__(256) k_shade(DevScene S0, DevRender R0, const 
       rng.init(x, y, R.width, (uint32_t)ps.y, R.seed, dimBaseOf(R));
       bool done = false;
       bool silhouette = false;
-      // ---- participating medium on the segment (tracePath, rayrenderer.cpp:1665-1831)
-      const bool medActive = MED && med >= 0 && S.media[med].hero > 0.0f;
-      if (medActive) {
-        const DevMedium M = S.media[med];
+      // ---- participating medium on the segment (tracePath, rayrenderer.cpp:1612-1863)
+      const bool medActive = MEDL > 0 && med >= 0 && S.media[med].active;
+      if (MEDL == 2 && medActive && S.media[med].haze) {
+        // heat haze (rayrenderer.cpp:1645-1660): march to the next surface bending
+        // the ray, then continue from the bent ray in the outer (global) medium.
+        // A heat-haze global medium bends once and the path goes on without a
+        // medium (the reference recurses without end there).
         const float maxT = prim >= 0 ? hq.x : kRayMaxDistance;
-        const float xi = fminf(0.9999999f, fmaxf(0.0f, rng.prng(v, S_FLIGHT)));
-        const float tF = -logf(1.0f - xi) / M.hero;
-        const bool scat = tF < maxT;
+        const med::Ray6 bent = med::bendRay(S.media + med, o, d, fminf(maxT, 1000.0f));
+        const int outer = S.globalMedium;
+        med = (outer >= 0 && S.media[outer].haze) ? -1 : outer;
+        cont = true;
+        no = bent.o;
+        nd = bent.d;
+      } else if (medActive) {
+        const DevMedium* Mg = S.media + med;
+        const DevMedium M = *Mg;
+        const bool het = MEDL == 2 && M.field != 0;
+        const float maxT = prim >= 0 ? hq.x : kRayMaxDistance;
+        float tF, dens = 1.0f;
+        bool scat;
+        if (het) {  // delta tracking (medium.cpp:406-441)
+          const med::Collision col = med::deltaTrack(Mg, o, d, maxT, rng, v);
+          scat = col.hit;
+          tF = col.hit ? col.t : maxT;
+          dens = col.density;
+        } else {
+          const float xi = fminf(0.9999999f, fmaxf(0.0f, rng.prng(v, S_FLIGHT)));
+          tF = -logf(1.0f - xi) / M.hero;
+          scat = tF < maxT;
+        }
         const float el = scat ? tF : maxT;
-        if (el > 0.0f) {
+        if (MEDL == 2) {
+          L = L + beta * med::emissionIntegral(&jobs[slot].S, Mg, o, d, el, rng, v);
+        } else if (el > 0.0f) {
           auto ew = [](float st, float dd) { return st < 1e-6f ? dd : (1.0f - expf(-st * dd)) / st; };
           L = L + beta * v3(M.ser * ew(M.str, el), M.seg * ew(M.stg, el), M.seb * ew(M.stb, el));
         }
         if (scat) {
-          const float pHero = M.hero * expf(-M.hero * tF);
           V3 sw = v3(0, 0, 0);
-          if (pHero > 0.0f)
-            sw = v3(M.ssr * expf(-M.str * tF) / pHero, M.ssg * expf(-M.stg * tF) / pHero, M.ssb * expf(-M.stb * tF) / pHero);
+          if (het) {  // sigma_s(p) / sigma_t_max: the rejection walk carries the decay
+            const float inv = M.tMaxHero > 0.0f ? 1.0f / M.tMaxHero : 0.0f;
+            sw = v3(M.ssr * dens * inv, M.ssg * dens * inv, M.ssb * dens * inv);
+          } else {
+            const float pHero = M.hero * expf(-M.hero * tF);
+            if (pHero > 0.0f)
+              sw = v3(M.ssr * expf(-M.str * tF) / pHero, M.ssg * expf(-M.stg * tF) / pHero, M.ssb * expf(-M.stb * tF) / pHero);
+          }
           const int passesS = eye ? 1 : passes + 1;
           if ((sw.x == 0.0f && sw.y == 0.0f && sw.z == 0.0f) || passesS > R.maxDepth) {
             done = true;
@@ -839,6 +873,16 @@ __global__ void __launch_bounds__(256) k_shade(DevScene S0, DevRender R0, const 
               if (envNEE(&jobs[slot].S, rng, v, pos, proxy, e, shE)) {
                 shE.on = true;
                 shE.c = beta * sw * e.Li * (phaseTo(e.dir) / e.pdf);
+              }
+            }
+            if (MEDL == 2 && S.numVolLights > 0) {  // volume-light NEE (rayrenderer.cpp:1763-1767)
+              const med::VolSample vs = med::sampleVolumeLight(&jobs[slot].S, rng, v, pos, proxy);
+              if (vs.ok && vs.pdf > 0.0f) {
+                shV.on = true;
+                shV.o = vs.so;
+                shV.d = vs.sd;
+                shV.tmax = 0.99999f;
+                shV.c = beta * sw * vs.Le * (phaseTo(vs.dir) / vs.pdf);
               }
             }
             // samplePhase: medium.cpp:496-517
@@ -881,7 +925,7 @@ __global__ void __launch_bounds__(256) k_shade(DevScene S0, DevRender R0, const 
             }
           }
         } else {
-          const float surv = expf(-M.hero * maxT);
+          const float surv = het ? 0.0f : expf(-M.hero * maxT);  // delta tracking: weight 1 (rayrenderer.cpp:1815-1822)
           if (surv > 0.0f)
             beta = beta * v3(expf(-M.str * maxT) / surv, expf(-M.stg * maxT) / surv, expf(-M.stb * maxT) / surv);
           if (prim < 0) {
@@ -1007,6 +1051,17 @@ __global__ void __launch_bounds__(256) k_shade(DevScene S0, DevRender R0, const 
                 shE.c = beta * albedo * e.Li * (dot(e.dir, h.n) * w / (kPi * e.pdf));
               }
             }
+            if (MEDL == 2 && S.numVolLights > 0) {  // volume-light NEE, no MIS (bsdf.cpp:91-101)
+              const med::VolSample vs = med::sampleVolumeLight(&jobs[slot].S, rng, v, h.p, h.n);
+              const float cosL = vs.ok && vs.pdf > 0.0f ? fmaxf(0.0f, dot(vs.dir, h.n)) : 0.0f;
+              if (cosL > 0.0f) {
+                shV.on = true;
+                shV.o = vs.so;
+                shV.d = vs.sd;
+                shV.tmax = 0.99999f;
+                shV.c = beta * albedo * vs.Le * (cosL * (1.0f / kPi) / vs.pdf);
+              }
+            }
             beta = beta * albedo;
             rrT = rrT * albedo;
             cont = true;
@@ -1088,6 +1143,17 @@ __global__ void __launch_bounds__(256) k_shade(DevScene S0, DevRender R0, const 
                   if (envNEE(&jobs[slot].S, rng, v, h.p, h.n, e, shE) && evalGlossy(e.dir, fCos, pb)) {
                     shE.on = true;
                     shE.c = beta * e.Li * fCos * (e.pdf * e.pdf / (e.pdf * e.pdf + pb * pb) / e.pdf);
+                  }
+                }
+                // volume-light NEE, no MIS (bsdf.cpp:316-328)
+                if (MEDL == 2 && S.numVolLights > 0) {
+                  const med::VolSample vs = med::sampleVolumeLight(&jobs[slot].S, rng, v, h.p, h.n);
+                  if (vs.ok && vs.pdf > 0.0f && evalGlossy(vs.dir, fCos, pb)) {
+                    shV.on = true;
+                    shV.o = vs.so;
+                    shV.d = vs.sd;
+                    shV.tmax = 0.99999f;
+                    shV.c = beta * vs.Le * fCos * (1.0f / vs.pdf);
                   }
                 }
                 // VNDF sample (bsdf.cpp:139-161, 319-373)
@@ -1221,6 +1287,14 @@ __global__ void __launch_bounds__(256) k_shade(DevScene S0, DevRender R0, const 
         Q.shO[2][se] = make_float4(shE.o.x, shE.o.y, shE.o.z, __int_as_float(pid));
         Q.shD[2][se] = make_float4(shE.d.x, shE.d.y, shE.d.z, shE.tmax);
         Q.shC[2][se] = make_float4(shE.c.x, shE.c.y, shE.c.z, __int_as_float(slot));
+      }
+    }
+    if (MEDL == 2) {
+      const int sv = warpPush(&Q.counters[iter * kCountersPerIter + C_SHD], shV.on);
+      if (sv >= 0) {
+        Q.shO[3][sv] = make_float4(shV.o.x, shV.o.y, shV.o.z, __int_as_float(pid));
+        Q.shD[3][sv] = make_float4(shV.d.x, shV.d.y, shV.d.z, shV.tmax);
+        Q.shC[3][sv] = make_float4(shV.c.x, shV.c.y, shV.c.z, __int_as_float(slot));
       }
     }
   }
@@ -1419,6 +1493,38 @@ __global__ void k_queryAny(DevScene S, const float* __restrict__ rays, const flo
   out[i] = traceAny(S, o, d, tmax[i], occ, nodes, tris) ? 1 : 0;
 }
 
+// Medium field queries (rg_medium_eval / rg_medium_bend).  The scene copy
+// sits in the job table so the field functions read it from global memory.
+__global__ void k_mediumEval(const DevJob* __restrict__ jobs, int medium, const float* __restrict__ pts, int n,
+                             float* __restrict__ out) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const DevScene* S = &jobs[0].S;
+  const DevMedium* M = S->media + medium;
+  const V3 p = v3(pts[i * 3], pts[i * 3 + 1], pts[i * 3 + 2]);
+  const V3 e = med::emissionAt(S, M, p);
+  out[i * 5 + 0] = med::densityAt(M, p);
+  out[i * 5 + 1] = e.x;
+  out[i * 5 + 2] = e.y;
+  out[i * 5 + 3] = e.z;
+  out[i * 5 + 4] = med::iorAt(M, p.x, p.y, p.z);
+}
+
+__global__ void k_mediumBend(const DevJob* __restrict__ jobs, int medium, const float* __restrict__ rays, int n,
+                             float* __restrict__ out) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const DevMedium* M = jobs[0].S.media + medium;
+  const float* r = rays + (size_t)i * 7;
+  const med::Ray6 b = med::bendRay(M, v3(r[0], r[1], r[2]), v3(r[3], r[4], r[5]), r[6]);
+  out[i * 6 + 0] = b.o.x;
+  out[i * 6 + 1] = b.o.y;
+  out[i * 6 + 2] = b.o.z;
+  out[i * 6 + 3] = b.d.x;
+  out[i * 6 + 4] = b.d.y;
+  out[i * 6 + 5] = b.d.z;
+}
+
 // ------------------------------------------------------------ launchers ----
 // Resident blocks per SM for the persistent traversal kernels.
 int residentBlocks(int kernel, int width) {
@@ -1443,14 +1549,20 @@ void launchExtend(const DevScene* single, const DevJob* jobs, int width, const D
 void launchShade(const DevScene* single, const DevRender* singleR, const DevJob* jobs, const DevQueues& Q, int iter,
                  int grid, cudaStream_t st) {
   if (!single) {
-    k_shade<true, true, true><<<grid, 256, 0, st>>>(DevScene{}, DevRender{}, jobs, Q, iter);
+    k_shade<true, true, 2><<<grid, 256, 0, st>>>(DevScene{}, DevRender{}, jobs, Q, iter);
     return;
   }
-  const bool env = single->envTex >= 0, med = single->numMedia > 0;
-  if (!env && !med) k_shade<false, false, false><<<grid, 256, 0, st>>>(*single, *singleR, jobs, Q, iter);
-  else if (!env) k_shade<false, false, true><<<grid, 256, 0, st>>>(*single, *singleR, jobs, Q, iter);
-  else if (!med) k_shade<false, true, false><<<grid, 256, 0, st>>>(*single, *singleR, jobs, Q, iter);
-  else k_shade<false, true, true><<<grid, 256, 0, st>>>(*single, *singleR, jobs, Q, iter);
+  const bool env = single->envTex >= 0;
+  const int ml = single->mediaLevel;
+  if (!env) {
+    if (ml == 0) k_shade<false, false, 0><<<grid, 256, 0, st>>>(*single, *singleR, jobs, Q, iter);
+    else if (ml == 1) k_shade<false, false, 1><<<grid, 256, 0, st>>>(*single, *singleR, jobs, Q, iter);
+    else k_shade<false, false, 2><<<grid, 256, 0, st>>>(*single, *singleR, jobs, Q, iter);
+  } else {
+    if (ml == 0) k_shade<false, true, 0><<<grid, 256, 0, st>>>(*single, *singleR, jobs, Q, iter);
+    else if (ml == 1) k_shade<false, true, 1><<<grid, 256, 0, st>>>(*single, *singleR, jobs, Q, iter);
+    else k_shade<false, true, 2><<<grid, 256, 0, st>>>(*single, *singleR, jobs, Q, iter);
+  }
 }
 void launchConnect(const DevScene* single, const DevJob* jobs, int width, const DevQueues& Q, int iter, int which,
                    int grid, cudaStream_t st) {
@@ -1478,6 +1590,11 @@ void launchQueryClosest(const DevScene& S, const float* rays, int n, float* tuv,
 void launchQueryAny(const DevScene& S, const float* rays, const float* tmax, int n, uint32_t occ, uint8_t* out,
                     cudaStream_t st) {
   if (n > 0) k_queryAny<<<(n + 127) / 128, 128, 0, st>>>(S, rays, tmax, n, occ, out);
+}
+void launchMediumQuery(const DevJob* jobs, int medium, bool bend, const float* in, int n, float* out, cudaStream_t st) {
+  if (n <= 0) return;
+  if (bend) k_mediumBend<<<(n + 127) / 128, 128, 0, st>>>(jobs, medium, in, n, out);
+  else k_mediumEval<<<(n + 127) / 128, 128, 0, st>>>(jobs, medium, in, n, out);
 }
 
 }  // namespace rg
