@@ -71,6 +71,11 @@ def load(fast: bool = False) -> C.CDLL:
     lib.orc_env_eval.argtypes = [C.c_void_p, f, C.c_int32, f, f]
     lib.orc_bloom.argtypes = [C.c_int32, C.c_int32, f] + [C.c_float] * 5
     lib.orc_env_sample.argtypes = [C.c_void_p, f, C.c_int32, f, f]
+    lib.orc_medium_eval.argtypes = [C.c_void_p, C.c_int32, f, C.c_int32, f]
+    lib.orc_medium_bend.argtypes = [C.c_void_p, C.c_int32, f, C.c_int32, f]
+    lib.orc_volume_nee.argtypes = [C.c_void_p, f, f, C.c_int32, C.c_uint32, f, f, f, P(C.c_uint8)]
+    lib.orc_num_volume_lights.restype = C.c_int32
+    lib.orc_num_volume_lights.argtypes = [C.c_void_p]
     _libs[name] = lib
     return lib
 
@@ -124,6 +129,35 @@ class OracleScene:
         pdf = np.zeros(d.shape[0], np.float32)
         self.lib.orc_env_eval(self.h, _fp(d), d.shape[0], _fp(rgb), _fp(pdf))
         return rgb, pdf
+
+    def medium_eval(self, medium, points):
+        """Camera-space points n x 3 -> n x 5 (density, emission rgb, ior) of medium `medium`."""
+        pts = np.ascontiguousarray(points, np.float32).reshape(-1, 3)
+        out = np.zeros((pts.shape[0], 5), np.float32)
+        self.lib.orc_medium_eval(self.h, medium, _fp(pts), pts.shape[0], _fp(out))
+        return out
+
+    def medium_bend(self, medium, rays):
+        """Rays n x 7 (origin, direction, length) -> bent rays n x 6."""
+        r = np.ascontiguousarray(rays, np.float32).reshape(-1, 7)
+        out = np.zeros((r.shape[0], 6), np.float32)
+        self.lib.orc_medium_bend(self.h, medium, _fp(r), r.shape[0], _fp(out))
+        return out
+
+    def volume_nee(self, hit, normal, n, seed=1):
+        """n volume-light NEE draws at a camera-space point: (dir n x 3, pdf n, Le n x 3, ok n)."""
+        h = np.ascontiguousarray(hit, np.float32).reshape(3)
+        nn = np.ascontiguousarray(normal, np.float32).reshape(3)
+        d = np.zeros((n, 3), np.float32)
+        pdf = np.zeros(n, np.float32)
+        le = np.zeros((n, 3), np.float32)
+        ok = np.zeros(n, np.uint8)
+        self.lib.orc_volume_nee(self.h, _fp(h), _fp(nn), n, seed, _fp(d), _fp(pdf), _fp(le),
+                                ok.ctypes.data_as(C.POINTER(C.c_uint8)))
+        return d, pdf, le, ok.astype(bool)
+
+    def num_volume_lights(self):
+        return self.lib.orc_num_volume_lights(self.h)
 
     def env_sample(self, u):
         """Luminance-importance samples: u n x 2 in [0,1) -> (directions n x 3, pdf n)."""

@@ -35,6 +35,7 @@
 #include <cstdint>
 #include <cstdio>
 #include <cstring>
+#include <limits>
 #include <random>
 #include <thread>
 #include <vector>
@@ -130,6 +131,7 @@ enum Slot {
   S_LOBE = 0, S_LIGHT = 1, S_MESH = 2, S_TRI = 3, S_VNDF0 = 4, S_VNDF1 = 5, S_RR = 6,
   S_FRESNEL = 7, S_CHROMA = 8, S_HEMI0 = 9, S_HEMI1 = 10, S_POINT = 11, S_ENV0 = 12,
   S_ENV1 = 13, S_FLIGHT = 14, S_PHASE0 = 15, S_PHASE1 = 16, S_MEDRR = 17, S_EYETR = 18,
+  S_DTSTEP = 19, S_DTACC = 20, S_EMIS = 21, S_VOLPICK = 22, S_VOLU = 23,
   S_LDS = 63
 };
 
@@ -144,6 +146,11 @@ struct Ctx {
   }
   float prng(int v, int slot) const {
     const uint32_t h = pcg4d_x(pixel, sample, ((uint32_t)v << 6) | (uint32_t)slot, seed);
+    return (float)(h >> 8) * (1.0f / 16777216.0f);
+  }
+  // k-th draw of a repeated use at vertex v (delta-tracking steps, emission strata)
+  float prngk(int v, int slot, int k) const {
+    const uint32_t h = pcg4d_x(pixel, sample, ((uint32_t)k << 16) | ((uint32_t)v << 6) | (uint32_t)slot, seed);
     return (float)(h >> 8) * (1.0f / 16777216.0f);
   }
   // ldsNext1D: raycommon.cpp:71-87 (dimension passed explicitly)
@@ -209,10 +216,86 @@ struct Material {
   float tiling[2];
 };
 
-struct Medium {  // medium.cpp:18-57 prepare()
+// ---- participating media (medium.h / medium.cpp) -------------------------
+// The procedural fields are written in the reference's evaluation order; the
+// device kernels evaluate the same expressions with explicit round-to-nearest
+// operations, so with this file built without contraction the noise,
+// density, emission and bending values agree bit for bit.
+
+// Integer lattice hash -> [0, 1): medium.cpp:127-136
+static inline float hash3(int x, int y, int z) {
+  uint32_t h = (uint32_t)x * 374761393u + (uint32_t)y * 668265263u + (uint32_t)z * 2147483647u;
+  h = (h ^ (h >> 13)) * 1274126177u;
+  h ^= h >> 16;
+  return (float)(h & 0x00FFFFFFu) / (float)0x01000000u;
+}
+static inline float smoothstep01(float x) { return x * x * (3.0f - 2.0f * x); }
+// valueNoise3D: medium.cpp:142-163
+static float valueNoise3D(float x, float y, float z) {
+  const int xi = (int)floorf(x), yi = (int)floorf(y), zi = (int)floorf(z);
+  const float xf = smoothstep01(x - (float)xi), yf = smoothstep01(y - (float)yi), zf = smoothstep01(z - (float)zi);
+  const float c000 = hash3(xi, yi, zi), c100 = hash3(xi + 1, yi, zi);
+  const float c010 = hash3(xi, yi + 1, zi), c110 = hash3(xi + 1, yi + 1, zi);
+  const float c001 = hash3(xi, yi, zi + 1), c101 = hash3(xi + 1, yi, zi + 1);
+  const float c011 = hash3(xi, yi + 1, zi + 1), c111 = hash3(xi + 1, yi + 1, zi + 1);
+  const float x00 = c000 * (1.0f - xf) + c100 * xf;
+  const float x10 = c010 * (1.0f - xf) + c110 * xf;
+  const float x01 = c001 * (1.0f - xf) + c101 * xf;
+  const float x11 = c011 * (1.0f - xf) + c111 * xf;
+  const float y0 = x00 * (1.0f - yf) + x10 * yf;
+  const float y1 = x01 * (1.0f - yf) + x11 * yf;
+  return y0 * (1.0f - zf) + y1 * zf;
+}
+// fbmNormalised: medium.cpp:171-185 (densityAt's loop, :276-301, is the same)
+static float fbmNormalised(float x, float y, float z, float freq, int octaves, float gain, float lac) {
+  float fx = x * freq, fy = y * freq, fz = z * freq;
+  float amp = 1.0f, total = 0.0f, ampSum = 0.0f;
+  const int oct = octaves > 0 ? octaves : 1;
+  for (int i = 0; i < oct; i++) {
+    total += amp * valueNoise3D(fx, fy, fz);
+    ampSum += amp;
+    amp *= gain;
+    fx *= lac; fy *= lac; fz *= lac;
+  }
+  return ampSum > 0.0f ? total / ampSum : 0.0f;
+}
+
+struct PathPt { V3 p; float radius, t; };
+
+// HomogeneousMedium after prepare() and bake() (medium.cpp:18-101), camera space.
+struct Medium {
   C3 sigma_s_eff, sigma_e_eff, sigma_t;
-  float hero, g;
-  bool active() const { return hero > 0.0f; }  // medium.h:226-233 (constant mode)
+  float hero = 0.0f, g = 0.0f, density = 1.0f;
+  int mode = 0, field = 0;  // emission mode (0 constant 1 cone 2 path), density field (0 none 1 fBm)
+  bool hazeOn = false;      // heatHaze
+  float tMaxHero = 0.0f;    // sigma_t_max_hero
+  V3 coneOriginR, coneAxisR;
+  float coneLength = 1, coneRadius = 0.3f, coneIntensity = 50, conePeakAxial = 0.15f, conePeakSharpness = 5;
+  C3 coneInner, coneOuter;
+  int coneSamples = 4;
+  std::vector<PathPt> pathPointsR;
+  int pathCount = 0;
+  C3 pathInner, pathOuter;
+  float pathIntensity = 1, pathFalloffPower = 2;
+  int pathSamples = 6;
+  float noiseFrequency = 1, noiseGain = 0.5f, noiseLacunarity = 2, noiseAmplitude = 1, noiseBias = 0;
+  int noiseOctaves = 4;
+  V3 noiseOffset;
+  float iorAmplitude = 0.005f, iorFrequency = 4, iorGain = 0.5f, iorLacunarity = 2, iorFalloff = 0;
+  int iorOctaves = 3, iorMarchSteps = 16;
+  V3 iorOffset;
+
+  static bool isZero3(const C3& c) { return c.x == 0.0f && c.y == 0.0f && c.z == 0.0f; }
+  // medium.h:226-234
+  bool active() const {
+    if (hero > 0.0f) return true;
+    if (mode == 1 && coneIntensity > 0.0f) return true;
+    if (mode == 2 && pathIntensity > 0.0f && pathCount >= 2) return true;
+    if (hazeOn && iorAmplitude > 0.0f) return true;
+    return !isZero3(sigma_e_eff);
+  }
+  bool heatHaze() const { return hazeOn && iorAmplitude > 0.0f && iorMarchSteps > 0; }  // medium.h:240-242
+  bool heterogeneous() const { return field != 0; }
   C3 transmittance(float d) const {            // medium.cpp:103-108
     if (d <= 0.0f) return C3(1, 1, 1);
     return C3(expf(-sigma_t.x * d), expf(-sigma_t.y * d), expf(-sigma_t.z * d));
@@ -222,6 +305,164 @@ struct Medium {  // medium.cpp:18-57 prepare()
     if (d <= 0.0f) return C3();
     return C3(sigma_e_eff.x * ew(sigma_t.x, d), sigma_e_eff.y * ew(sigma_t.y, d),
               sigma_e_eff.z * ew(sigma_t.z, d));
+  }
+  // densityAt: medium.cpp:276-301
+  float densityAt(V3 p) const {
+    if (field == 0) return 1.0f;
+    const float n = fbmNormalised(p.x - noiseOffset.x, p.y - noiseOffset.y, p.z - noiseOffset.z, noiseFrequency,
+                                  noiseOctaves, noiseGain, noiseLacunarity);
+    return fmaxf(0.0f, noiseAmplitude * n + noiseBias);
+  }
+  // emissionAt: medium.cpp:303-404
+  C3 emissionAt(V3 p) const {
+    if (mode == 0) {
+      if (field == 0) return sigma_e_eff;
+      const float dn = densityAt(p);
+      return C3(sigma_e_eff.x * dn, sigma_e_eff.y * dn, sigma_e_eff.z * dn);
+    }
+    if (mode == 2) {
+      const size_t n = pathPointsR.size();
+      if (n < 2) return C3();
+      float bestD2 = std::numeric_limits<float>::infinity(), bestT = 0.0f, bestRadius = 0.0f;
+      for (size_t i = 0; i + 1 < n; i++) {
+        const PathPt& a = pathPointsR[i];
+        const PathPt& b = pathPointsR[i + 1];
+        const float abx = b.p.x - a.p.x, aby = b.p.y - a.p.y, abz = b.p.z - a.p.z;
+        const float ab2 = abx * abx + aby * aby + abz * abz;
+        if (ab2 < 1e-12f) continue;
+        const float apx = p.x - a.p.x, apy = p.y - a.p.y, apz = p.z - a.p.z;
+        float u = (apx * abx + apy * aby + apz * abz) / ab2;
+        if (u < 0.0f) u = 0.0f;
+        else if (u > 1.0f) u = 1.0f;
+        const float qx = a.p.x + abx * u, qy = a.p.y + aby * u, qz = a.p.z + abz * u;
+        const float dx = p.x - qx, dy = p.y - qy, dz = p.z - qz;
+        const float d2 = dx * dx + dy * dy + dz * dz;
+        if (d2 < bestD2) {
+          bestD2 = d2;
+          bestT = a.t + (b.t - a.t) * u;
+          bestRadius = a.radius + (b.radius - a.radius) * u;
+        }
+      }
+      if (bestRadius <= 0.0f) return C3();
+      if (bestD2 >= bestRadius * bestRadius) return C3();
+      const float r = sqrtf(bestD2) / bestRadius;
+      const float radial = powf(fmaxf(0.0f, 1.0f - r), pathFalloffPower);
+      if (radial <= 0.0f) return C3();
+      const float tb = bestT < 0.0f ? 0.0f : (bestT > 1.0f ? 1.0f : bestT);
+      const C3 col(pathInner.x * (1.0f - tb) + pathOuter.x * tb, pathInner.y * (1.0f - tb) + pathOuter.y * tb,
+                   pathInner.z * (1.0f - tb) + pathOuter.z * tb);
+      float scale = radial * pathIntensity * fmaxf(0.0f, density);
+      if (field != 0) scale *= densityAt(p);
+      return C3(col.x * scale, col.y * scale, col.z * scale);
+    }
+    const float rx = p.x - coneOriginR.x, ry = p.y - coneOriginR.y, rz = p.z - coneOriginR.z;
+    const float axialT = rx * coneAxisR.x + ry * coneAxisR.y + rz * coneAxisR.z;
+    if (coneLength <= 0.0f) return C3();
+    const float u = axialT / coneLength;
+    if (u < 0.0f || u > 1.0f) return C3();
+    const float px = rx - coneAxisR.x * axialT, py = ry - coneAxisR.y * axialT, pz = rz - coneAxisR.z * axialT;
+    const float radial2 = px * px + py * py + pz * pz;
+    if (coneRadius <= 0.0f) return C3();
+    const float v2 = radial2 / (coneRadius * coneRadius);
+    if (v2 > 1.0f) return C3();
+    const float dx = (u - conePeakAxial) * conePeakSharpness;
+    const float axialFalloff = expf(-(dx * dx));
+    const float radialFalloff = (1.0f - v2) * (1.0f - v2);
+    const float t = axialFalloff * radialFalloff;
+    if (t <= 0.0f) return C3();
+    const C3 col(coneInner.x * t + coneOuter.x * (1.0f - t), coneInner.y * t + coneOuter.y * (1.0f - t),
+                 coneInner.z * t + coneOuter.z * (1.0f - t));
+    float scale = t * coneIntensity * fmaxf(0.0f, density);
+    if (field != 0) scale *= densityAt(p);
+    return C3(col.x * scale, col.y * scale, col.z * scale);
+  }
+  // emissionIntegralAlongRay: medium.cpp:443-473 (jitter per stratum from the k-th draw)
+  C3 emissionIntegral(const Ray& ray, float maxT, const Ctx& c, int v) const {
+    if (mode == 0) return emissionAlongRay(maxT);
+    if (maxT <= 0.0f) return C3();
+    const int count = mode == 2 ? pathSamples : coneSamples;
+    const int N = count > 0 ? count : 1;
+    const float dt = maxT / (float)N;
+    C3 acc;
+    for (int i = 0; i < N; i++) {
+      const float t = ((float)i + c.prngk(v, S_EMIS, i)) * dt;
+      const V3 p(ray.o.x + ray.d.x * t, ray.o.y + ray.d.y * t, ray.o.z + ray.d.z * t);
+      const C3 se = emissionAt(p);
+      if (isZero3(se)) continue;
+      const C3 tr = transmittance(t);
+      acc.x += se.x * tr.x * dt;
+      acc.y += se.y * tr.y * dt;
+      acc.z += se.z * tr.z * dt;
+    }
+    return acc;
+  }
+  // sampleDeltaTracking: medium.cpp:406-441
+  bool sampleDeltaTracking(const Ray& ray, float maxT, const Ctx& c, int v, float& outT, float& outDensity) const {
+    if (tMaxHero <= 0.0f || maxT <= 0.0f) return false;
+    const float peak = hero > 0.0f ? tMaxHero / hero : 1.0f;
+    if (peak <= 0.0f) return false;
+    float t = 0.0f;
+    for (int i = 0; i < 64; i++) {
+      const float xi = fminf(0.9999999f, fmaxf(0.0f, c.prngk(v, S_DTSTEP, i)));
+      t += -logf(1.0f - xi) / tMaxHero;
+      if (t >= maxT) return false;
+      const V3 p(ray.o.x + ray.d.x * t, ray.o.y + ray.d.y * t, ray.o.z + ray.d.z * t);
+      const float d = densityAt(p);
+      const float pAccept = peak > 0.0f ? d / peak : 1.0f;
+      if (c.prngk(v, S_DTACC, i) < pAccept) {
+        outT = t;
+        outDensity = d;
+        return true;
+      }
+    }
+    return false;
+  }
+  // iorAt: medium.cpp:186-215
+  float iorAt(V3 p) const {
+    if (!hazeOn) return 1.0f;
+    const float n = fbmNormalised(p.x - iorOffset.x, p.y - iorOffset.y, p.z - iorOffset.z, iorFrequency, iorOctaves,
+                                  iorGain, iorLacunarity);
+    float ampMul = 1.0f;
+    if (iorFalloff != 0.0f && coneLength > 0.0f) {
+      const float axialT = (p.x - coneOriginR.x) * coneAxisR.x + (p.y - coneOriginR.y) * coneAxisR.y +
+                           (p.z - coneOriginR.z) * coneAxisR.z;
+      float u = axialT / coneLength;
+      if (u < 0.0f) u = 0.0f;
+      else if (u > 1.0f) u = 1.0f;
+      const float mag = iorFalloff < 0.0f ? -iorFalloff : iorFalloff;
+      const float t = iorFalloff >= 0.0f ? u : (1.0f - u);
+      ampMul = 1.0f - mag * t;
+      if (ampMul < 0.0f) ampMul = 0.0f;
+    }
+    return 1.0f + iorAmplitude * ampMul * (n - 0.5f) * 2.0f;
+  }
+  // bendRay with iorGradientAt: medium.cpp:217-274
+  Ray bendRay(const Ray& ray, float length) const {
+    if (length <= 0.0f || !heatHaze())
+      return Ray{V3(ray.o.x + ray.d.x * length, ray.o.y + ray.d.y * length, ray.o.z + ray.d.z * length), ray.d};
+    const int N = iorMarchSteps;
+    const float ds = length / (float)N;
+    const float h = iorFrequency > 0.0f ? (0.5f / iorFrequency) : 0.05f;
+    const float inv2h = 0.5f / h;
+    V3 pos = ray.o, dir = ray.d;
+    for (int i = 0; i < N; i++) {
+      const V3 mid(pos.x + dir.x * (ds * 0.5f), pos.y + dir.y * (ds * 0.5f), pos.z + dir.z * (ds * 0.5f));
+      const float n = iorAt(mid);
+      const float gx = (iorAt(V3(mid.x + h, mid.y, mid.z)) - iorAt(V3(mid.x - h, mid.y, mid.z))) * inv2h;
+      const float gy = (iorAt(V3(mid.x, mid.y + h, mid.z)) - iorAt(V3(mid.x, mid.y - h, mid.z))) * inv2h;
+      const float gz = (iorAt(V3(mid.x, mid.y, mid.z + h)) - iorAt(V3(mid.x, mid.y, mid.z - h))) * inv2h;
+      const float gd = gx * dir.x + gy * dir.y + gz * dir.z;
+      const float px = gx - dir.x * gd, py = gy - dir.y * gd, pz = gz - dir.z * gd;
+      const float invN = n > 1e-6f ? (1.0f / n) : 1.0f;
+      const V3 nd(dir.x + px * (ds * invN), dir.y + py * (ds * invN), dir.z + pz * (ds * invN));
+      const float l2 = nd.x * nd.x + nd.y * nd.y + nd.z * nd.z;
+      if (l2 > 1e-12f) {
+        const float invL = 1.0f / sqrtf(l2);
+        dir = V3(nd.x * invL, nd.y * invL, nd.z * invL);
+      }
+      pos = V3(pos.x + dir.x * ds, pos.y + dir.y * ds, pos.z + dir.z * ds);
+    }
+    return Ray{pos, dir};
   }
   float sampleFreeFlight(float u) const {       // medium.cpp:475-480
     if (hero <= 0.0f) return 1e30f;
@@ -257,6 +498,10 @@ struct Medium {  // medium.cpp:18-57 prepare()
   }
 };
 
+// EmissiveVolumeSource (rayrenderer.h:71-75): the medium and, for constant
+// emission, the owning object's location in camera space.
+struct VolLight { int medium; V3 anchor; };
+
 struct BVHNode {  // bvh.h:22-30
   V3 bmin; uint32_t firstOrLeft;
   V3 bmax; uint16_t count, axis;
@@ -286,6 +531,7 @@ struct Scene {
   std::vector<Material> mats;
   std::vector<Medium> media;
   int globalMedium = -1;
+  std::vector<VolLight> vols;    // emissive volumes, object order
   std::vector<int> areaLights;   // object ids
   std::vector<PointLight> points;
   std::vector<Texture> textures;
@@ -516,7 +762,7 @@ static bool intersectClosest(const Scene& s, const Ray& ray, HitInfo& info) {
   return any;
 }
 
-enum Pred { P_AREA = 0, P_POINT = 1, P_AO = 2, P_ALL = 3 };
+enum Pred { P_AREA = 0, P_POINT = 1, P_AO = 2, P_ALL = 3, P_VOL = 4 };
 // occluder predicates: rayrenderer.cpp:1956-1959 (area), :2211-2215 (point/env), :2388-2390 (AO)
 static inline bool occluder(const Scene& s, int tri, int pred) {
   const Material& m = s.mats[s.objMat[s.tris[tri].obj]];
@@ -524,6 +770,7 @@ static inline bool occluder(const Scene& s, int tri, int pred) {
     case P_AREA: return m.transparency < 0.01f && m.emission <= 0.0f;
     case P_POINT: if (m.emission > 0.0f) return false; return m.transparency < 0.01f || m.refraction > 0.1f;
     case P_AO: return m.transparency < 0.01f;
+    case P_VOL: if (m.emission > 0.0f) return false; return m.transparency < 0.01f && m.refraction <= 0.1f;  // rayrenderer.cpp:2167-2171
     default: return true;
   }
 }
@@ -688,6 +935,49 @@ struct Tracer {
     outDir = dir;
     outPdf = r2 / (cosLight * sampledArea(tri)) / lightCountFactor();
     outLe = lm.color * lm.emission;
+    return true;
+  }
+
+  // sampleVolumeLightForNEE: rayrenderer.cpp:2067-2203 (the volume pick and
+  // the equiangular draw come from this vertex's own keys)
+  bool sampleVolumeLightForNEE(V3 hit, V3 n, int v, V3& outDir, float& outPdf, C3& outLe) const {
+    const int N = (int)s.vols.size();
+    if (N <= 0) return false;
+    const VolLight& ev = s.vols[pickIndex(c.prng(v, S_VOLPICK), N)];
+    const Medium& m = s.media[ev.medium];
+    V3 segA, segB;
+    if (m.mode == 1) {
+      segA = m.coneOriginR;
+      segB = m.coneOriginR + m.coneAxisR * m.coneLength;
+    } else {
+      segA = ev.anchor;
+      segB = segA;
+    }
+    const V3 segDir = segB - segA;
+    const float segLen = length(segDir);
+    const V3 axis = segLen > 1e-6f ? segDir * (1.0f / segLen) : V3(0.0f, 0.0f, -1.0f);
+    const V3 toA = segA - hit;
+    const float along = dot(toA, axis);
+    const V3 perp = toA - axis * along;
+    const float D = length(perp);
+    if (!(D > 1e-5f) && segLen <= 1e-6f) return false;
+    const float thA = atanf(along / fmaxf(D, 1e-5f)), thB = atanf((along + segLen) / fmaxf(D, 1e-5f));
+    if (!(fabsf(thB - thA) > 1e-6f) && segLen > 1e-6f) return false;
+    const float theta = thA + c.prng(v, S_VOLU) * (thB - thA);
+    const float tS = D * tanf(theta);
+    const V3 sp = segLen > 1e-6f ? segA + axis * (tS - along) : segA;
+    const V3 toS = sp - hit;
+    const float r2 = dot(toS, toS);
+    const float r = sqrtf(r2);
+    if (!(r > 1e-5f)) return false;
+    if (intersectAny(s, SurfaceRay(hit, toS, n), 0.99999f, P_VOL)) return false;
+    C3 se = m.emissionAt(sp);
+    if (isZero(se)) return false;
+    if (m.hero > 0.0f) se = se * m.transmittance(r);
+    const float pdfT = D / (fmaxf(1e-6f, fabsf(thB - thA)) * (D * D + tS * tS));
+    outDir = toS * (1.0f / r);
+    outPdf = pdfT * r2 * (float)N;
+    outLe = se;
     return true;
   }
 
@@ -891,6 +1181,13 @@ struct Tracer {
     col += tracePath(ray, &p);
     // the MIS partner passed is this vertex's own cosine-sampled pdf (bsdf.cpp:86-88)
     col += traceEnvmapLight(p.info->hit, p.vi.normal, p.bsdfPdf, v);
+    {  // volume-light NEE, no MIS (bsdf.cpp:91-101)
+      V3 vDir; float vPdf = 0.0f; C3 vLe;
+      if (sampleVolumeLightForNEE(p.info->hit, p.vi.normal, v, vDir, vPdf, vLe) && vPdf > 0.0f) {
+        const float cosL = fmaxf(0.0f, dot(vDir, p.vi.normal));
+        col += vLe * (cosL * (float)(1.0 / M_PI) / vPdf);
+      }
+    }
     p.throughput = savedT;
     p.bsdfPdf = savedPdf;
     return col * albedo;
@@ -985,6 +1282,13 @@ struct Tracer {
           const float w = pe * pe / (pe * pe + pb * pb);
           direct += Li * fCos * (w / pe);
         }
+      }
+    }
+    {  // volume-light NEE, no MIS (bsdf.cpp:316-328)
+      V3 vDir; float vPdf = 0.0f; C3 vLe;
+      if (sampleVolumeLightForNEE(p.info->hit, normal, v, vDir, vPdf, vLe) && vPdf > 0.0f) {
+        C3 fCos; float pb = 0.0f;
+        if (evalGlossy(vDir, fCos, pb)) direct += vLe * fCos * (1.0f / vPdf);
       }
     }
     // sampleGGXVNDF: bsdf.cpp:139-161
@@ -1125,12 +1429,12 @@ struct Tracer {
   }
 
   // RayBSDFShaderProvider::shade: rayrenderer.cpp:2776-2896
-  C3 shade5(const HitInfo& info, const Ray& inray, const Vi& vi, const Param* sp) {
+  C3 shade5(const HitInfo& info, const Ray& inray, const Vi& vi, const Param* sp, int medOverride = -2) {
     const Material& m = matOfTri(info.tri);
     Param p;
     p.info = &info; p.inray = inray; p.vi = vi;
     p.vertex = c.vertex++;
-    p.medium = sp ? sp->medium : s.globalMedium;
+    p.medium = medOverride >= -1 ? medOverride : (sp ? sp->medium : s.globalMedium);
     if (m.emission > 0.0f) {
       const C3 e = m.color * m.emission;
       if (sp && sp->bsdfPdf > 0.0f) {
@@ -1235,28 +1539,56 @@ struct Tracer {
     return sampleEnvironment(ray.d);  // tracePath miss without BSDF parameters
   }
 
-  // tracePath: rayrenderer.cpp:1596-1864 (homogeneous media only)
-  C3 tracePath(const Ray& ray, const Param* sp) {
+  // tracePath: rayrenderer.cpp:1596-1864.  `medOverride` >= -1 replaces the
+  // segment's medium (the eye segment after a heat-haze bend).
+  C3 tracePath(const Ray& ray, const Param* sp, int medOverride = -2) {
     HitInfo info;
     intersectClosest(s, ray, info);
-    const int medId = sp ? sp->medium : s.globalMedium;
+    const int medId = medOverride >= -1 ? medOverride : (sp ? sp->medium : s.globalMedium);
     const Medium* med = medId >= 0 ? &s.media[medId] : nullptr;
     if (!med || !med->active()) {
-      if (info.tri >= 0) return shade5(info, ray, interp(s, info), sp);
+      if (info.tri >= 0) return shade5(info, ray, interp(s, info), sp, medOverride);
       return missRadiance(ray, sp);
+    }
+    if (med->heatHaze()) {
+      // rayrenderer.cpp:1645-1660: march to the next surface bending the ray,
+      // then go on in the outer (global) medium with the same parameters.  A
+      // heat-haze global medium bends once and the path goes on without a
+      // medium (the reference recurses without end there).
+      const float maxTh = info.tri >= 0 ? info.t : RAY_MAX_DISTANCE;
+      const Ray bent = med->bendRay(ray, fminf(maxTh, 1000.0f));
+      c.vertex++;  // every segment has its own key index
+      int outer = s.globalMedium;
+      if (outer >= 0 && s.media[outer].heatHaze()) outer = -1;
+      if (!sp) return tracePath(bent, nullptr, outer);
+      Param q = *sp;
+      q.medium = outer;
+      return tracePath(bent, &q);
     }
     const float maxT = info.tri >= 0 ? info.t : RAY_MAX_DISTANCE;
     const int v = c.vertex;  // the event index this segment ends in
-    const float tFlight = med->sampleFreeFlight(c.prng(v, S_FLIGHT));
-    const bool scattered = tFlight < maxT;
-    const C3 medEm = med->emissionAlongRay(scattered ? tFlight : maxT);
+    bool scattered;
+    float tFlight, densAt = 1.0f;
+    if (med->heterogeneous()) {  // delta tracking (rayrenderer.cpp:1672-1680)
+      scattered = med->sampleDeltaTracking(ray, maxT, c, v, tFlight, densAt);
+      if (!scattered) tFlight = maxT;
+    } else {
+      tFlight = med->sampleFreeFlight(c.prng(v, S_FLIGHT));
+      scattered = tFlight < maxT;
+    }
+    const C3 medEm = med->emissionIntegral(ray, scattered ? tFlight : maxT, c, v);
     if (scattered) {
       c.vertex++;
       C3 sw;
-      const float pHero = med->freeFlightPdf(tFlight);
-      const C3 Tr = med->transmittance(tFlight);
-      if (pHero > 0.0f) sw = C3(med->sigma_s_eff.x * Tr.x / pHero, med->sigma_s_eff.y * Tr.y / pHero,
-                               med->sigma_s_eff.z * Tr.z / pHero);
+      if (med->heterogeneous()) {  // sigma_s(p) / sigma_t_max (rayrenderer.cpp:1706-1709)
+        const float inv = med->tMaxHero > 0.0f ? 1.0f / med->tMaxHero : 0.0f;
+        sw = C3(med->sigma_s_eff.x * densAt * inv, med->sigma_s_eff.y * densAt * inv, med->sigma_s_eff.z * densAt * inv);
+      } else {
+        const float pHero = med->freeFlightPdf(tFlight);
+        const C3 Tr = med->transmittance(tFlight);
+        if (pHero > 0.0f) sw = C3(med->sigma_s_eff.x * Tr.x / pHero, med->sigma_s_eff.y * Tr.y / pHero,
+                                 med->sigma_s_eff.z * Tr.z / pHero);
+      }
       if (isZero(sw)) return medEm;
       const V3 pos = ray.o + ray.d * tFlight;
       const int passes = sp ? sp->passes + 1 : 1;
@@ -1269,6 +1601,9 @@ struct Tracer {
       V3 eDir; float pe = 0.0f; C3 Li;
       if (sampleEnvmapForNEE(pos, proxy, v, eDir, pe, Li) && pe > 0.0f)
         direct += Li * med->phasePdf(-ray.d, eDir) * (1.0f / pe);
+      V3 vDir; float vPdf = 0.0f; C3 vLe;
+      if (sampleVolumeLightForNEE(pos, proxy, v, vDir, vPdf, vLe) && vPdf > 0.0f)
+        direct += vLe * med->phasePdf(-ray.d, vDir) * (1.0f / vPdf);
       const V3 nd = med->samplePhase(ray.d, c.prng(v, S_PHASE0), c.prng(v, S_PHASE1));
       Param q;
       q.info = &info; q.inray = ray; q.passes = passes; q.medium = medId;
@@ -1287,10 +1622,12 @@ struct Tracer {
       return medEm + sw * (direct + ind);
     }
     C3 surfW(1, 1, 1);
-    const float surv = med->survival(maxT);
-    if (surv > 0.0f) {
-      const C3 Tr = med->transmittance(maxT);
-      surfW = C3(Tr.x / surv, Tr.y / surv, Tr.z / surv);
+    if (!med->heterogeneous()) {  // delta tracking passes the surface with weight 1
+      const float surv = med->survival(maxT);
+      if (surv > 0.0f) {
+        const C3 Tr = med->transmittance(maxT);
+        surfW = C3(Tr.x / surv, Tr.y / surv, Tr.z / surv);
+      }
     }
     if (info.tri >= 0) {
       Vi vi = interp(s, info);
@@ -1883,6 +2220,9 @@ static Scene* buildScene(const rg_scene_desc* d, int bins) {
     o.emission = m.emission; o.spotRange = m.spot_range; o.texture = m.texture;
     o.tiling[0] = m.tex_tiling[0]; o.tiling[1] = m.tex_tiling[1];
   }
+  // media: prepare() + bake() (medium.cpp:18-101); only the cone (cone mode)
+  // and the path points (path mode) are baked into camera space
+  auto cap = [](int n) { return n > 64 ? 64 : n; };
   s->media.resize(d->num_media);
   for (int i = 0; i < d->num_media; i++) {
     const rg_medium& m = d->media[i];
@@ -1894,13 +2234,67 @@ static Scene* buildScene(const rg_scene_desc* d, int bins) {
     o.sigma_t = sa + o.sigma_s_eff;
     o.hero = (o.sigma_t.x + o.sigma_t.y + o.sigma_t.z) * (1.0f / 3.0f);
     o.g = m.g;
+    o.density = m.density;
+    o.mode = (m.emission_mode == 1 || m.emission_mode == 2) ? m.emission_mode : 0;
+    o.field = m.density_field == 1 ? 1 : 0;
+    o.tMaxHero = o.field ? o.hero * fmaxf(0.0f, m.noise_amplitude * 1.0f + m.noise_bias) : o.hero;
+    const float al2 = m.cone_axis[0] * m.cone_axis[0] + m.cone_axis[1] * m.cone_axis[1] + m.cone_axis[2] * m.cone_axis[2];
+    V3 axN(0.0f, 0.0f, -1.0f);
+    if (al2 > 1e-12f) {
+      const float inv = 1.0f / sqrtf(al2);
+      axN = V3(m.cone_axis[0] * inv, m.cone_axis[1] * inv, m.cone_axis[2] * inv);
+    }
+    o.coneOriginR = V3(m.cone_origin[0], m.cone_origin[1], m.cone_origin[2]);
+    o.coneAxisR = axN;
+    if (o.mode == 1) {
+      o.coneOriginR = viewPoint(view, m.cone_origin);
+      float av[3];
+      for (int j = 0; j < 3; j++) av[j] = (axN.x * view.m[j] + axN.y * view.m[4 + j]) + axN.z * view.m[8 + j];
+      const float vl2 = av[0] * av[0] + av[1] * av[1] + av[2] * av[2];
+      if (vl2 > 1e-12f) {
+        const float inv = 1.0f / sqrtf(vl2);
+        o.coneAxisR = V3(av[0] * inv, av[1] * inv, av[2] * inv);
+      }
+    }
+    o.coneLength = m.cone_length; o.coneRadius = m.cone_radius;
+    o.coneInner = C3(m.cone_inner[0], m.cone_inner[1], m.cone_inner[2]);
+    o.coneOuter = C3(m.cone_outer[0], m.cone_outer[1], m.cone_outer[2]);
+    o.coneIntensity = m.cone_intensity; o.conePeakAxial = m.cone_peak_axial;
+    o.conePeakSharpness = m.cone_peak_sharpness; o.coneSamples = cap(m.cone_emission_samples);
+    o.pathCount = m.num_path_points > 0 ? m.num_path_points : 0;
+    if (o.mode == 2)
+      for (int k = 0; k < o.pathCount; k++) {
+        const rg_medium_path_point& q = m.path_points[k];
+        o.pathPointsR.push_back(PathPt{viewPoint(view, q.p), q.radius, q.t});
+      }
+    o.pathInner = C3(m.path_inner[0], m.path_inner[1], m.path_inner[2]);
+    o.pathOuter = C3(m.path_outer[0], m.path_outer[1], m.path_outer[2]);
+    o.pathIntensity = m.path_intensity; o.pathFalloffPower = m.path_falloff_power;
+    o.pathSamples = cap(m.path_emission_samples);
+    o.noiseFrequency = m.noise_frequency; o.noiseOctaves = cap(m.noise_octaves); o.noiseGain = m.noise_gain;
+    o.noiseLacunarity = m.noise_lacunarity; o.noiseAmplitude = m.noise_amplitude; o.noiseBias = m.noise_bias;
+    o.noiseOffset = V3(m.noise_offset[0], m.noise_offset[1], m.noise_offset[2]);
+    o.hazeOn = m.heat_haze != 0;
+    o.iorAmplitude = m.ior_amplitude; o.iorFrequency = m.ior_frequency; o.iorOctaves = cap(m.ior_octaves);
+    o.iorGain = m.ior_gain; o.iorLacunarity = m.ior_lacunarity; o.iorMarchSteps = cap(m.ior_march_steps);
+    o.iorOffset = V3(m.ior_offset[0], m.ior_offset[1], m.ior_offset[2]);
+    o.iorFalloff = m.ior_falloff;
   }
-  s->globalMedium = d->global_medium;
+  // inactive media are dropped by readMedium (sceneloader.cpp:325-333)
+  auto live = [&](int m) { return m >= 0 && m < d->num_media && s->media[m].active() ? m : -1; };
+  s->globalMedium = live(d->global_medium);
   s->objMat.resize(d->num_objects);
   s->objMedium.resize(d->num_objects);
   for (int i = 0; i < d->num_objects; i++) {
     s->objMat[i] = d->objects[i].material;
-    s->objMedium[i] = d->objects[i].interior_medium;
+    s->objMedium[i] = live(d->objects[i].interior_medium);
+    // emissive-volume registration (rayrenderer.cpp:180-206)
+    const int mi = s->objMedium[i];
+    if (mi >= 0) {
+      const Medium& M = s->media[mi];
+      if ((M.mode == 1 && M.coneIntensity > 0.0f) || (M.mode == 0 && !Medium::isZero3(M.sigma_e_eff)))
+        s->vols.push_back(VolLight{mi, viewPoint(view, d->objects[i].location)});
+    }
   }
   s->meshObj.assign(d->mesh_object, d->mesh_object + d->num_meshes);
   s->meshTris.assign(d->num_meshes, {});
@@ -2109,5 +2503,46 @@ void orc_env_sample(void* sp, const float* u, int32_t n, float* out_dir, float* 
     out_pdf[i] = pdf;
   }
 }
+
+// Medium fields of medium `m` at camera-space points: n x 5 (density, emission rgb, ior).
+void orc_medium_eval(void* sp, int32_t m, const float* pts, int32_t n, float* out) {
+  const Medium& M = static_cast<Scene*>(sp)->media[m];
+  for (int i = 0; i < n; i++) {
+    const V3 p(pts[i * 3], pts[i * 3 + 1], pts[i * 3 + 2]);
+    const C3 e = M.emissionAt(p);
+    out[i * 5] = M.densityAt(p);
+    out[i * 5 + 1] = e.x; out[i * 5 + 2] = e.y; out[i * 5 + 3] = e.z;
+    out[i * 5 + 4] = M.iorAt(p);
+  }
+}
+// Heat-haze bending of rays n x 7 (origin, direction, length) -> n x 6.
+void orc_medium_bend(void* sp, int32_t m, const float* rays, int32_t n, float* out) {
+  const Medium& M = static_cast<Scene*>(sp)->media[m];
+  for (int i = 0; i < n; i++) {
+    const float* r = rays + (size_t)i * 7;
+    const Ray b = M.bendRay(Ray{V3(r[0], r[1], r[2]), V3(r[3], r[4], r[5])}, r[6]);
+    out[i * 6] = b.o.x; out[i * 6 + 1] = b.o.y; out[i * 6 + 2] = b.o.z;
+    out[i * 6 + 3] = b.d.x; out[i * 6 + 4] = b.d.y; out[i * 6 + 5] = b.d.z;
+  }
+}
+// n volume-light NEE draws at one camera-space point (sample index i, vertex 0
+// of pixel (0, 0)): direction, solid-angle pdf, radiance and success flag.
+void orc_volume_nee(void* sp, const float* hit, const float* normal, int32_t n, uint32_t seed, float* out_dir,
+                    float* out_pdf, float* out_le, uint8_t* out_ok) {
+  const Scene& s = *static_cast<Scene*>(sp);
+  for (int i = 0; i < n; i++) {
+    Ctx c{};
+    c.begin(0, 0, 1, (uint32_t)i, seed);
+    Tracer t(s, c);
+    V3 d; float pdf = 0.0f; C3 le;
+    const bool ok = t.sampleVolumeLightForNEE(V3(hit[0], hit[1], hit[2]), V3(normal[0], normal[1], normal[2]), 0, d,
+                                              pdf, le);
+    out_dir[i * 3] = d.x; out_dir[i * 3 + 1] = d.y; out_dir[i * 3 + 2] = d.z;
+    out_pdf[i] = pdf;
+    out_le[i * 3] = le.x; out_le[i * 3 + 1] = le.y; out_le[i * 3 + 2] = le.z;
+    out_ok[i] = ok ? 1 : 0;
+  }
+}
+int32_t orc_num_volume_lights(void* sp) { return (int32_t)static_cast<Scene*>(sp)->vols.size(); }
 
 }  // extern "C"
