@@ -110,7 +110,8 @@ struct rg_server {
   DevBuf<int> errWord;
   DevSegment* hostSegs = nullptr;
   DevWave* hostWave = nullptr;
-  cudaGraphExec_t graph = nullptr;
+  // wave graphs: [0] homogeneous media only, [1] procedural media and volume lights
+  cudaGraphExec_t graph[2] = {nullptr, nullptr};
   int maxIter = 12;
   // statistics
   std::vector<double> latencies;
@@ -119,7 +120,8 @@ struct rg_server {
   int64_t waves = 0;
   double deviceMs = 0;
   ~rg_server() {
-    if (graph) cudaGraphExecDestroy(graph);
+    for (auto g : graph)
+      if (g) cudaGraphExecDestroy(g);
     if (hostSegs) cudaFreeHost(hostSegs);
     if (hostWave) cudaFreeHost(hostWave);
     if (stream) cudaStreamDestroy(stream);
@@ -166,7 +168,9 @@ bool allocServer(rg_server* s) {
   return cudaStreamSynchronize(s->stream) == cudaSuccess;
 }
 
-// Capture the multi-job wave (generate, bounce loop, accumulate) once.
+// Capture the multi-job wave (generate, bounce loop, accumulate) once per
+// kernel set: graph[0] with the homogeneous-media shade kernel, graph[1] with
+// the procedural-media kernel and the volume-light shadow queue.
 bool captureGraph(rg_server* s) {
   const DevQueues Q = serverQueues(s);
   // traversal: persistent warps, blocks per SM up to the occupancy limit
@@ -174,22 +178,26 @@ bool captureGraph(rg_server* s) {
   const int ext = s->numSMs * (tb > 0 ? std::min(tb, residentBlocks(0, 8)) : residentBlocks(0, 8));
   const int conn = s->numSMs * (tb > 0 ? std::min(tb, residentBlocks(1, 8)) : residentBlocks(1, 8));
   const int shadeGrid = s->numSMs * (s->cfg.shade_blocks_per_sm > 0 ? s->cfg.shade_blocks_per_sm : 4);
-  cudaGraph_t g;
-  if (cudaStreamBeginCapture(s->stream, cudaStreamCaptureModeThreadLocal) != cudaSuccess) return false;
-  launchGenerate(s->jobTable.p, s->waveSlot.p, Q, shadeGrid * 2, s->stream);
-  for (int it = 0; it < Q.maxIter; it++) {
-    launchExtend(nullptr, s->jobTable.p, 8, Q, it, ext, s->stream);
-    launchShade(nullptr, nullptr, s->jobTable.p, Q, it, shadeGrid, s->stream);
-    launchConnect(nullptr, s->jobTable.p, 8, Q, it, 0, conn, s->stream);
-    launchConnect(nullptr, s->jobTable.p, 8, Q, it, 1, conn, s->stream);
-    launchConnect(nullptr, s->jobTable.p, 8, Q, it, 2, conn, s->stream);
-    launchConnect(nullptr, s->jobTable.p, 8, Q, it, 3, conn, s->stream);
+  for (int k = 0; k < 2; k++) {
+    const bool procedural = k == 1;
+    cudaGraph_t g;
+    if (cudaStreamBeginCapture(s->stream, cudaStreamCaptureModeThreadLocal) != cudaSuccess) return false;
+    launchGenerate(s->jobTable.p, s->waveSlot.p, Q, shadeGrid * 2, s->stream);
+    for (int it = 0; it < Q.maxIter; it++) {
+      launchExtend(nullptr, s->jobTable.p, 8, Q, it, ext, s->stream);
+      launchShade(nullptr, nullptr, s->jobTable.p, Q, it, shadeGrid, s->stream, procedural ? 2 : 1);
+      launchConnect(nullptr, s->jobTable.p, 8, Q, it, 0, conn, s->stream);
+      launchConnect(nullptr, s->jobTable.p, 8, Q, it, 1, conn, s->stream);
+      launchConnect(nullptr, s->jobTable.p, 8, Q, it, 2, conn, s->stream);
+      if (procedural) launchConnect(nullptr, s->jobTable.p, 8, Q, it, 3, conn, s->stream);
+    }
+    launchAccumulate(s->jobTable.p, s->waveSlot.p, Q, shadeGrid, s->stream);
+    if (cudaStreamEndCapture(s->stream, &g) != cudaSuccess) return false;
+    const bool ok = cudaGraphInstantiate(&s->graph[k], g, 0) == cudaSuccess;
+    cudaGraphDestroy(g);
+    if (!ok) return false;
   }
-  launchAccumulate(s->jobTable.p, s->waveSlot.p, Q, shadeGrid, s->stream);
-  if (cudaStreamEndCapture(s->stream, &g) != cudaSuccess) return false;
-  const bool ok = cudaGraphInstantiate(&s->graph, g, 0) == cudaSuccess;
-  cudaGraphDestroy(g);
-  return ok;
+  return true;
 }
 
 void releaseJob(rg_server* s, ServerJob* j) {
@@ -388,7 +396,10 @@ void serverLoop(rg_server* s) {
       cudaMemcpyAsync(s->segs.p, s->hostSegs, sizeof(DevSegment) * nseg, cudaMemcpyHostToDevice, st);
       cudaMemcpyAsync(s->waveSlot.p, w, sizeof(DevWave), cudaMemcpyHostToDevice, st);
       cudaEventRecord(e0, st);
-      cudaGraphLaunch(s->graph, st);
+      // the procedural-media kernel only for waves that hold such a job
+      bool procedural = false;
+      for (auto& pe : plan) procedural = procedural || pe.first->S.mediaLevel >= 2;
+      cudaGraphLaunch(s->graph[procedural ? 1 : 0], st);
       cudaEventRecord(e1, st);
       const cudaError_t ce = cudaStreamSynchronize(st);
       float ms = 0;

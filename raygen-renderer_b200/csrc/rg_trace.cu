@@ -1547,9 +1547,10 @@ void launchExtend(const DevScene* single, const DevJob* jobs, int width, const D
   }
 }
 void launchShade(const DevScene* single, const DevRender* singleR, const DevJob* jobs, const DevQueues& Q, int iter,
-                 int grid, cudaStream_t st) {
+                 int grid, cudaStream_t st, int multiMediaLevel) {
   if (!single) {
-    k_shade<true, true, 2><<<grid, 256, 0, st>>>(DevScene{}, DevRender{}, jobs, Q, iter);
+    if (multiMediaLevel >= 2) k_shade<true, true, 2><<<grid, 256, 0, st>>>(DevScene{}, DevRender{}, jobs, Q, iter);
+    else k_shade<true, true, 1><<<grid, 256, 0, st>>>(DevScene{}, DevRender{}, jobs, Q, iter);
     return;
   }
   const bool env = single->envTex >= 0;

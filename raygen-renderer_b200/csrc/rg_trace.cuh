@@ -15,8 +15,10 @@ void launchGenerate(const DevJob* jobs, const DevWave* W, const DevQueues& Q, in
 // null: per-ray job slots into `jobs`.
 void launchExtend(const DevScene* single, const DevJob* jobs, int width, const DevQueues& Q, int iter, int grid,
                   cudaStream_t st);
+// single == nullptr: the multi-job kernel; multiMediaLevel 2 includes the
+// procedural-media code, 1 homogeneous media only (no volume-light queue)
 void launchShade(const DevScene* single, const DevRender* singleR, const DevJob* jobs, const DevQueues& Q, int iter,
-                 int grid, cudaStream_t st);
+                 int grid, cudaStream_t st, int multiMediaLevel = 2);
 void launchConnect(const DevScene* single, const DevJob* jobs, int width, const DevQueues& Q, int iter, int which,
                    int grid, cudaStream_t st);
 void launchSimple(const DevJob* jobs, const DevWave* W, const DevQueues& Q, int grid, cudaStream_t st);
