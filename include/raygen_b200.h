@@ -19,6 +19,7 @@
  *   rg_get_ldr             <- RayRenderer::getRenderResult src/raygen/rayrenderer.h:404
  *   rg_reapply_postprocess <- RayRenderer::reapplyPostProcess src/raygen/rayrenderer.cpp:698-711
  *   rg_save_image          <- saveImage in the CLI's output step src/main.cpp:479-485
+ *   rg_load_image          <- Texture::loadFromFile         src/raygen/texture.cpp:170-195
  *   rg_trace_closest       <- TriangleBVH::intersectClosest src/raygen/bvh.cpp:233-285
  *   rg_trace_any           <- TriangleBVH::intersectAny   src/raygen/bvh.h:63-101
  *   rg_denoise_atrous      <- RayRenderer::denoiseImage   src/raygen/rayrenderer.cpp:2649-2772
@@ -396,6 +397,14 @@ rg_status rg_load_scene_json(const char* path, rg_scene_desc** out);
  * .jpg / .jpeg (baseline JPEG, quality 92, 4:4:4), .png and .ppm store
  * round(clamp(v, 0, 1) * 255).  Host work only. */
 rg_status rg_save_image(const char* path, int32_t width, int32_t height, const float* rgba);
+/* Read an image file as a texture is read: Radiance .hdr by name (linear,
+ * is_hdr 1), otherwise JPEG (baseline / extended sequential) or PNG by
+ * content, and .pfm by name.  LDR images give their stored values in [0, 1]
+ * (is_hdr 0; the renderer sRGB-decodes them when it samples).  Call with
+ * rgba NULL to get the size; then with count >= width*height*4 floats.
+ * Row 0 at the top.  Host work only. */
+rg_status rg_load_image(const char* path, int32_t* width, int32_t* height, int32_t* is_hdr, float* rgba,
+                        size_t count);
 
 /* ---- resident multi-job server (batched and served rendering) ----------- */
 #define RG_JOB_QUEUED 0

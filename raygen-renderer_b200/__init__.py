@@ -230,6 +230,7 @@ def load_library(path: str = LIB_PATH) -> C.CDLL:
         "rg_tonemap": (C.c_int, [C.c_int32, C.c_int32, P(C.c_float), P(C.c_float)]),
         "rg_bloom": (C.c_int, [C.c_int32, C.c_int32, P(C.c_float)] + [C.c_float] * 5 + [P(C.c_float)]),
         "rg_save_image": (C.c_int, [C.c_char_p, C.c_int32, C.c_int32, P(C.c_float)]),
+        "rg_load_image": (C.c_int, [C.c_char_p, P(C.c_int32), P(C.c_int32), P(C.c_int32), P(C.c_float), C.c_size_t]),
         "rg_tc_gemm_bf16": (C.c_int, [C.c_int32, C.c_int32, C.c_int32, P(C.c_uint16), P(C.c_uint16), P(C.c_float)]),
         "rg_denoiser_num_params": (C.c_int32, []),
         "rg_denoiser_create": (C.c_int, [C.c_uint32, P(C.c_void_p)]),
@@ -666,6 +667,17 @@ def save_image(path: str, rgba: np.ndarray) -> None:
     lib = load_library()
     a = np.ascontiguousarray(rgba, np.float32)
     _check(lib.rg_save_image(path.encode(), a.shape[1], a.shape[0], _fptr(a)))
+
+
+def load_image(path: str):
+    """Read an image file as a texture: (H x W x 4 float32, is_hdr).  Radiance .hdr and .pfm
+    by name, JPEG and PNG by content; LDR values in [0, 1] as stored (not sRGB-decoded)."""
+    lib = load_library()
+    w, h, hdr = C.c_int32(), C.c_int32(), C.c_int32()
+    _check(lib.rg_load_image(path.encode(), C.byref(w), C.byref(h), C.byref(hdr), None, 0))
+    out = np.empty((h.value, w.value, 4), np.float32)
+    _check(lib.rg_load_image(path.encode(), C.byref(w), C.byref(h), C.byref(hdr), _fptr(out), out.size))
+    return out, bool(hdr.value)
 
 
 def to_bf16_bits(a: np.ndarray) -> np.ndarray:

@@ -1420,6 +1420,24 @@ rg_status rg_save_image(const char* path, int32_t width, int32_t height, const f
   return RG_OK;
 }
 
+rg_status rg_load_image(const char* path, int32_t* width, int32_t* height, int32_t* is_hdr, float* rgba,
+                        size_t count) {
+  if (!path || !width || !height) return RG_ERR_INVALID_ARGUMENT;
+  TextureStore t;
+  std::string err;
+  if (!readImageFile(path, t, err)) {
+    setLastError(err);
+    return err.find("cannot open") != std::string::npos ? RG_ERR_IO : RG_ERR_PARSE;
+  }
+  *width = t.width;
+  *height = t.height;
+  if (is_hdr) *is_hdr = t.isHdr;
+  if (!rgba) return RG_OK;
+  if (count < t.rgba.size()) return RG_ERR_INVALID_ARGUMENT;
+  std::memcpy(rgba, t.rgba.data(), t.rgba.size() * sizeof(float));
+  return RG_OK;
+}
+
 rg_status rg_load_scene_json(const char* path, rg_scene_desc** out) {
   if (!path || !out) return RG_ERR_INVALID_ARGUMENT;
   SceneStore* st = nullptr;

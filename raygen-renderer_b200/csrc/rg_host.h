@@ -99,6 +99,9 @@ rg_status loadSceneJson(const char* path, SceneStore** out, std::string& err);
 bool readRadianceHdr(const std::string& path, TextureStore& out, std::string& err);
 bool readPfm(const std::string& path, TextureStore& out, std::string& err);
 bool readImageFile(const std::string& path, TextureStore& out, std::string& err);
+// JPEG (baseline / extended sequential) and PNG decoders (rg_decode.cpp): LDR RGBA in [0, 1].
+bool decodeJpeg(const std::vector<unsigned char>& bytes, TextureStore& out, std::string& err);
+bool decodePng(const std::vector<unsigned char>& bytes, TextureStore& out, std::string& err);
 bool writeImageFile(const std::string& path, int W, int H, const float* rgba, std::string& err);
 
 // Device-resident scene (BVH + triangle and light tables).

@@ -171,13 +171,24 @@ bool readPfm(const std::string& path, TextureStore& out, std::string& err) {
   return true;
 }
 
+// Texture::loadFromFile (texture.cpp:170-195): '.hdr' by name, everything
+// else by content (the reference's loadImage probes the codecs); PFM by name.
 bool readImageFile(const std::string& path, TextureStore& out, std::string& err) {
   const size_t dot = path.find_last_of('.');
   std::string ext = dot == std::string::npos ? "" : path.substr(dot + 1);
   for (char& c : ext) c = (char)std::tolower((unsigned char)c);
   if (ext == "hdr") return readRadianceHdr(path, out, err);
   if (ext == "pfm") return readPfm(path, out, err);
-  err = "unsupported image format (Radiance .hdr and .pfm are read): " + path;
+  std::vector<unsigned char> b;
+  if (!readAll(path, b, err)) return false;
+  if (b.size() >= 2 && b[0] == 0xFF && b[1] == 0xD8) {
+    if (decodeJpeg(b, out, err)) return true;
+  } else if (b.size() >= 8 && b[0] == 0x89 && b[1] == 'P' && b[2] == 'N' && b[3] == 'G') {
+    if (decodePng(b, out, err)) return true;
+  } else {
+    err = "unsupported image format (Radiance .hdr, PFM, JPEG and PNG are read)";
+  }
+  err += ": " + path;
   return false;
 }
 

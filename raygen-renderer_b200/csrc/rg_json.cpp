@@ -16,8 +16,7 @@
 //  * Materials: color ([r,g,b] | "#rgb" | "#rrggbb[aa]"), emission, diffuse,
 //    glossy, roughness, transparency, refraction, refractionRatio,
 //    chromaDispersion, metallic, anisotropy, anisoRotation, spotRange,
-//    texTiling.  Image textures ('tex') are not decoded (no JPEG/PNG codec in
-//    this build) and are ignored.
+//    texTiling, tex (Radiance .hdr, PFM, JPEG or PNG; one texture per path).
 //  * Transforms: world = parent * T(location) * R(angle) * S(scale) with
 //    R = Ry(y) Rx(x) Rz(z), active right-handed rotations (the single-axis
 //    rotations of the sample scenes, e.g. cubeRoom's walls, face inward).
@@ -28,6 +27,7 @@
 //  * The multi-axis rotation order and the colour packing come from the
 //    graphics-module submodule, which the reference tree does not vendor.
 #include <cctype>
+#include <functional>
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
@@ -648,8 +648,11 @@ bool readVec3(const JVal* v, float out[3]) {
   return false;
 }
 
-// readMaterial (sceneloader.cpp:101-165)
-void readMaterial(const JVal& j, rg_material& m) {
+// readMaterial (sceneloader.cpp:101-165).  `texture` resolves a 'tex' path
+// to a texture index (-1: the material keeps its flat colour).
+void readMaterial(const JVal& j, rg_material& m, const std::function<int(const std::string&)>& texture) {
+  if (const JVal* t = j.get("tex"))
+    if (t->type == JVal::Str && !t->s.empty()) m.texture = texture(t->s);
   if (const JVal* t = j.get("texTiling")) {
     if (t->type == JVal::Arr && t->arr.size() >= 2) {
       m.tex_tiling[0] = (float)t->arr[0].n;
@@ -794,6 +797,27 @@ bool readMedium(const JVal& j, MediumSpec& sp) {
 struct Loader {
   SceneStore& st;
   std::string baseDir;
+  // SceneResourcePool::getTexture (scene.cpp:597-681): one texture per path,
+  // relative paths from the scene's directory (transformPath,
+  // sceneloader.cpp:50-62); a file that cannot be read or decoded gives no
+  // texture, and bundle paths (sob:// / tob://) are not read.
+  std::map<std::string, int> texPool;
+  int texture(const std::string& rel) {
+    if (rel.rfind("sob://", 0) == 0 || rel.rfind("tob://", 0) == 0) return -1;
+    const std::string path = (rel[0] == '/' || rel[0] == '\\') ? rel : baseDir + rel;
+    const auto it = texPool.find(path);
+    if (it != texPool.end()) return it->second;
+    TextureStore t;
+    std::string e;
+    int idx = -1;
+    if (readImageFile(path, t, e) && t.width > 0 && t.height > 0) {
+      st.textures.push_back(std::move(t));
+      idx = (int)st.textures.size() - 1;
+    }
+    texPool[path] = idx;
+    return idx;
+  }
+  std::function<int(const std::string&)> texFn = [this](const std::string& r) { return texture(r); };
   // Named materials, one scope per object being read; lookups search the
   // innermost scope first (SceneJsonLoader::findMaterialByName).
   std::vector<std::map<std::string, rg_material>> scopes;
@@ -913,7 +937,7 @@ struct Loader {
         for (auto& p : mats->obj)
           if (p.second.type == JVal::Obj) {
             rg_material m = defaultMat();
-            readMaterial(p.second, m);
+            readMaterial(p.second, m, texFn);
             scopes.back()[p.first] = m;
           }
     if (n.isCamera) readCamera(jo);
@@ -956,7 +980,7 @@ struct Loader {
         if (v.type == JVal::Str) {
           if (const rg_material* m = findMaterial(v.s)) n.mat = *m;
         } else if (v.type == JVal::Obj) {
-          readMaterial(v, n.mat);
+          readMaterial(v, n.mat, texFn);
         }
       } else if (k == "visible" && v.type == JVal::Bool) {
         n.visible = v.b;
@@ -1159,7 +1183,7 @@ rg_status loadSceneJson(const char* path, SceneStore** out, std::string& err) {
   st->camera.aperture = 1.8f;
   st->camera.aperture_blades = 0;
   st->camera.exposure = 1.0f;
-  Loader L{*st, "", {}, "", RG_ERR_IO};
+  Loader L{*st};
   const std::string p(path);
   L.baseDir = p.find_last_of('/') == std::string::npos ? "" : p.substr(0, p.find_last_of('/') + 1);
   Loader::Node top;
