@@ -233,6 +233,14 @@ typedef struct rg_scene_desc {
   int32_t envmap_texture;     /* index into textures                          */
   float envmap_intensity;
   float envmap_rotation;      /* degrees */
+  /* Cubemap environment (Scene::envCubemapFaces, scene.h:198-222): six square
+   * faces of one size, texture indices in the order +X -X +Y -Y +Z -Z (px nx
+   * py ny pz nz).  When envmap_cube is set it takes precedence over the
+   * equirectangular map for lookups, and is importance-sampled per face by
+   * luminance x texel solid angle (scene.cpp:343-410); intensity and rotation
+   * are shared. */
+  int32_t envmap_cube;        /* 0 none */
+  int32_t envmap_cube_faces[6];
 } rg_scene_desc;
 
 typedef struct rg_stats {

@@ -540,6 +540,12 @@ struct Scene {
   int envW = 0, envH = 0;
   float envIntensity = 1.0f, envCosY = 1.0f, envSinY = 0.0f, envTotal = 0.0f;
   std::vector<float> envMarg, envCond;  // H+1 ; H x (W+1)
+  // cubemap environment (Scene::envCubemapFaces, scene.h:198-222): faces px nx py ny pz nz
+  bool envCube = false;
+  int envFace[6] = {-1, -1, -1, -1, -1, -1};
+  int envCubeW = 0;                     // face size of the sampling CDF (0: none)
+  float envCubeTotal = 0.0f;
+  std::vector<float> cubeMargFace, cubeMargY, cubeCond;  // 7 ; 6 x (W+1) ; 6 x W x (W+1)
   // camera (RenderThreadContext, rayrenderer.cpp:97-132)
   V3 camLoc;
   float fov, viewNear, viewFar, dof, aperture, apertureRot, exposure;
@@ -1019,8 +1025,31 @@ struct Tracer {
     return a + p;
   }
 
-  // ---- equirectangular environment map ----------------------------------
+  // ---- environment map: equirectangular or cubemap ----------------------
   bool envSampling() const { return s.envTex >= 0 && s.envW > 0 && s.envTotal > 0.0f; }
+  bool cubeSampling() const { return s.envCubeW > 0 && s.envCubeTotal > 0.0f; }
+  // face and face-local (s, t) of a rotated direction (OpenGL convention, rayrenderer.cpp:1311-1333)
+  static int cubeFace(float rx, float ry, float rz, float& sc, float& tc, float& ma) {
+    const float ax = fabsf(rx), ay = fabsf(ry), az = fabsf(rz);
+    int face;
+    if (ax >= ay && ax >= az) {
+      ma = ax;
+      if (rx > 0) { face = 0; sc = -rz; tc = ry; }
+      else { face = 1; sc = rz; tc = ry; }
+    } else if (ay >= ax && ay >= az) {
+      ma = ay;
+      if (ry > 0) { face = 2; sc = rx; tc = rz; }
+      else { face = 3; sc = rx; tc = -rz; }
+    } else {
+      ma = az;
+      if (rz > 0) { face = 4; sc = rx; tc = ry; }
+      else { face = 5; sc = -rx; tc = ry; }
+    }
+    return face;
+  }
+  const float* cubeTexel(int face, int x, int y) const {
+    return &s.textures[s.envFace[face]].rgba[((size_t)y * s.envCubeW + x) * 4];
+  }
   const float* envTexel(int x, int y) const {
     return &s.textures[s.envTex].rgba[((size_t)y * s.envW + x) * 4];
   }
@@ -1029,10 +1058,17 @@ struct Tracer {
   // sampleEnvironment, equirectangular branch (rayrenderer.cpp:1299-1348):
   // view-space direction, yaw about +Y, lat-long lookup through Texture::sample.
   C3 sampleEnvironment(V3 dir) const {
-    if (s.envTex < 0) return C3();
+    if (s.envTex < 0 && !s.envCube) return C3();
     const V3 d = normalize(dir);
     const float rx = d.x * s.envCosY - d.z * s.envSinY;
     const float rz = d.x * s.envSinY + d.z * s.envCosY;
+    if (s.envCube) {  // the cubemap takes precedence (rayrenderer.cpp:1310-1340)
+      float sc, tc, ma;
+      const int face = cubeFace(rx, d.y, rz, sc, tc, ma);
+      const float u = 0.5f * (sc / ma + 1.0f);
+      const float v = 0.5f * (1.0f - tc / ma);
+      return texSample(s, s.envFace[face], u, v) * s.envIntensity;
+    }
     const float u = 0.5f + atan2f(rz, rx) * (float)(0.5 / M_PI);
     const float v = 0.5f - asinf(fminf(fmaxf(d.y, -1.0f), 1.0f)) * (float)(1.0 / M_PI);
     return texSample(s, s.envTex, u, v) * s.envIntensity;
@@ -1040,10 +1076,22 @@ struct Tracer {
 
   // envmapDirectionPdf, equirectangular branch (rayrenderer.cpp:1521-1573)
   float envmapDirectionPdf(V3 dir) const {
-    if (!envSampling()) return 0.0f;
     const V3 d = normalize(dir);
     const float rx = d.x * s.envCosY - d.z * s.envSinY;
     const float rz = d.x * s.envSinY + d.z * s.envCosY;
+    if (cubeSampling()) {  // rayrenderer.cpp:1530-1555
+      float sc, tc, ma;
+      const int face = cubeFace(rx, d.y, rz, sc, tc, ma);
+      if (ma <= 0.0f) return 0.0f;
+      const float u = 0.5f * (sc / ma + 1.0f);
+      const float v = 0.5f * (1.0f - tc / ma);
+      const int W = s.envCubeW;
+      int x = (int)(u * W); if (x < 0) x = 0; if (x >= W) x = W - 1;
+      int y = (int)(v * W); if (y < 0) y = 0; if (y >= W) y = W - 1;
+      const float lum = texelLum(cubeTexel(face, x, y));
+      return lum * (float)(W * W) / (4.0f * s.envCubeTotal);
+    }
+    if (!envSampling()) return 0.0f;
     const int W = s.envW, H = s.envH;
     const float u = 0.5f + atan2f(rz, rx) * (float)(0.5 / M_PI);
     const float v = 0.5f - asinf(fminf(fmaxf(d.y, -1.0f), 1.0f)) * (float)(1.0 / M_PI);
@@ -1071,6 +1119,36 @@ struct Tracer {
   void sampleEnvmapDirection(float u0, float u1, V3& outDir, float& outPdf) const {
     outDir = V3(0, 1, 0);
     outPdf = 0.0f;
+    if (cubeSampling()) {  // face, row, texel from the three-level CDF (rayrenderer.cpp:1384-1433)
+      const int W = s.envCubeW, H = W;
+      const int face = searchCDF(s.cubeMargFace.data(), 6, u0);
+      const float faceLo = s.cubeMargFace[face], faceSpan = s.cubeMargFace[face + 1] - faceLo;
+      const float u0r = faceSpan > 0.0f ? (u0 - faceLo) / faceSpan : 0.5f;
+      const float* marY = &s.cubeMargY[(size_t)face * (H + 1)];
+      const int y = searchCDF(marY, H, u0r);
+      const float yLo = marY[y], ySpan = marY[y + 1] - yLo;
+      const float yFrac = ySpan > 0.0f ? (u0r - yLo) / ySpan : 0.5f;
+      const float* condX = &s.cubeCond[((size_t)face * H + y) * (W + 1)];
+      const int x = searchCDF(condX, W, u1);
+      const float xLo = condX[x], xSpan = condX[x + 1] - xLo;
+      const float xFrac = xSpan > 0.0f ? (u1 - xLo) / xSpan : 0.5f;
+      const float u = (x + xFrac) / (float)W;
+      const float v = (y + yFrac) / (float)H;
+      const float sc = 2.0f * u - 1.0f, tc = 1.0f - 2.0f * v;
+      V3 l;  // cubeFaceDir (rayrenderer.cpp:1367-1376)
+      switch (face) {
+        case 0: l = V3(1.0f, tc, -sc); break;
+        case 1: l = V3(-1.0f, tc, sc); break;
+        case 2: l = V3(sc, 1.0f, tc); break;
+        case 3: l = V3(sc, -1.0f, -tc); break;
+        case 4: l = V3(sc, tc, 1.0f); break;
+        default: l = V3(-sc, tc, -1.0f); break;
+      }
+      outDir = normalize(V3(l.x * s.envCosY + l.z * s.envSinY, l.y, -l.x * s.envSinY + l.z * s.envCosY));
+      const float lum = texelLum(cubeTexel(face, x, y));
+      outPdf = lum * (float)(W * H) / (4.0f * s.envCubeTotal);
+      return;
+    }
     if (!envSampling()) return;
     const int W = s.envW, H = s.envH;
     const int y = searchCDF(s.envMarg.data(), H, u0);
@@ -1099,7 +1177,7 @@ struct Tracer {
   // sampleEnvmapForNEE (rayrenderer.cpp:2038-2065): luminance-IS direction,
   // front-facing test, unbounded shadow ray with the point/env occluders.
   bool sampleEnvmapForNEE(V3 hit, V3 n, int v, V3& outDir, float& outPdf, C3& outLi) const {
-    if (!envSampling()) return false;
+    if (!envSampling() && !cubeSampling()) return false;
     V3 dir;
     float pdf = 0.0f;
     sampleEnvmapDirection(c.prng(v, S_ENV0), c.prng(v, S_ENV1), dir, pdf);
@@ -2196,6 +2274,65 @@ static void buildEnvmapCDF(Scene& s) {
   }
 }
 
+// Scene::buildEnvmapCDF, cubemap part (scene.cpp:343-410): per face, running
+// row sums of luminance x the texel's solid-angle Jacobian 1/(s^2+t^2+1)^1.5,
+// rows normalised to conditional CDFs, a per-face marginal over rows and a CDF
+// over the face totals; raw texels, sequential float sums.
+static void buildCubeCDF(Scene& s) {
+  const int W = s.textures[s.envFace[0]].w, H = s.textures[s.envFace[0]].h;
+  if (W <= 0 || H <= 0) return;
+  s.envCubeW = W;
+  s.cubeMargFace.assign(7, 0.0f);
+  s.cubeMargY.assign((size_t)6 * (H + 1), 0.0f);
+  s.cubeCond.assign((size_t)6 * H * (W + 1), 0.0f);
+  float faceWeights[6] = {0, 0, 0, 0, 0, 0};
+  for (int f = 0; f < 6; f++) {
+    const Texture& T = s.textures[s.envFace[f]];
+    std::vector<float> rowWeight(H, 0.0f);
+    for (int y = 0; y < H; y++) {
+      float* cond = &s.cubeCond[((size_t)f * H + y) * (W + 1)];
+      cond[0] = 0.0f;
+      float rowSum = 0.0f;
+      const float t = 1.0f - (y + 0.5f) * (2.0f / (float)H);
+      for (int x = 0; x < W; x++) {
+        const float sx = (x + 0.5f) * (2.0f / (float)W) - 1.0f;
+        const float denom = sx * sx + t * t + 1.0f;
+        const float jac = 1.0f / (denom * sqrtf(denom));
+        const float* c = &T.rgba[((size_t)y * W + x) * 4];
+        const float lum = fmaxf(0.0f, 0.2126f * c[0] + 0.7152f * c[1] + 0.0722f * c[2]);
+        rowSum += lum * jac;
+        cond[x + 1] = rowSum;
+      }
+      if (rowSum > 0.0f) {
+        const float inv = 1.0f / rowSum;
+        for (int x = 1; x <= W; x++) cond[x] *= inv;
+      }
+      rowWeight[y] = rowSum;
+    }
+    float* my = &s.cubeMargY[(size_t)f * (H + 1)];
+    my[0] = 0.0f;
+    for (int y = 0; y < H; y++) my[y + 1] = my[y] + rowWeight[y];
+    const float faceTotal = my[H];
+    faceWeights[f] = faceTotal;
+    if (faceTotal > 0.0f) {
+      const float inv = 1.0f / faceTotal;
+      for (int y = 0; y <= H; y++) my[y] *= inv;
+    }
+  }
+  float total = 0.0f;
+  for (int f = 0; f < 6; f++) total += faceWeights[f];
+  s.envCubeTotal = total;
+  if (total > 0.0f) {
+    const float inv = 1.0f / total;
+    float acc = 0.0f;
+    s.cubeMargFace[0] = 0.0f;
+    for (int f = 0; f < 6; f++) {
+      acc += faceWeights[f];
+      s.cubeMargFace[f + 1] = acc * inv;
+    }
+  }
+}
+
 static Scene* buildScene(const rg_scene_desc* d, int bins) {
   Scene* s = new Scene();
   const int nt = d->num_triangles;
@@ -2338,13 +2475,23 @@ static Scene* buildScene(const rg_scene_desc* d, int bins) {
     T.rgba.assign(d->textures[i].rgba, d->textures[i].rgba + (size_t)T.w * T.h * 4);
     s->textures.push_back(std::move(T));
   }
-  if (d->has_envmap && d->envmap_texture >= 0 && d->envmap_texture < d->num_textures) {
-    s->envTex = d->envmap_texture;
+  const bool eq = d->has_envmap && d->envmap_texture >= 0 && d->envmap_texture < d->num_textures;
+  bool cube = d->envmap_cube != 0;
+  for (int f = 0; cube && f < 6; f++) cube = d->envmap_cube_faces[f] >= 0 && d->envmap_cube_faces[f] < d->num_textures;
+  if (eq || cube) {
     s->envIntensity = d->envmap_intensity;
     const float yaw = d->envmap_rotation * (float)(M_PI / 180.0);
     s->envCosY = cosf(yaw);
     s->envSinY = sinf(yaw);
+  }
+  if (eq) {
+    s->envTex = d->envmap_texture;
     buildEnvmapCDF(*s);
+  }
+  if (cube) {
+    s->envCube = true;
+    for (int f = 0; f < 6; f++) s->envFace[f] = d->envmap_cube_faces[f];
+    buildCubeCDF(*s);
   }
   buildBVH(*s, bins);
   return s;

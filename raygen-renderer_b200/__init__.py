@@ -149,6 +149,7 @@ class rg_scene_desc(C.Structure):
         ("camera", rg_camera),
         ("has_envmap", C.c_int32), ("envmap_texture", C.c_int32),
         ("envmap_intensity", C.c_float), ("envmap_rotation", C.c_float),
+        ("envmap_cube", C.c_int32), ("envmap_cube_faces", C.c_int32 * 6),
     ]
 
 
@@ -429,9 +430,10 @@ class Scene:
     @classmethod
     def from_arrays(cls, positions, normals, tri_mesh, mesh_object, objects, materials, camera,
                     media=(), global_medium=-1, point_lights=(), uvs=None, textures=(),
-                    envmap=None, envmap_intensity=1.0, envmap_rotation=0.0) -> "Scene":
+                    envmap=None, envmap_intensity=1.0, envmap_rotation=0.0, envmap_cube=None) -> "Scene":
         """Scene from arrays.  textures: sequence of (H x W x 4 float32 RGBA, is_hdr);
-        envmap: index of the equirectangular environment texture (None = no environment)."""
+        envmap: index of the equirectangular environment texture (None = no environment);
+        envmap_cube: texture indices of six square cubemap faces (+X -X +Y -Y +Z -Z)."""
         pos = np.ascontiguousarray(positions, dtype=np.float32).reshape(-1, 9)
         nrm = np.ascontiguousarray(normals, dtype=np.float32).reshape(-1, 9)
         tm = np.ascontiguousarray(tri_mesh, dtype=np.int32)
@@ -478,6 +480,10 @@ class Scene:
         if envmap is not None:
             d.has_envmap = 1
             d.envmap_texture = int(envmap)
+        if envmap_cube is not None:  # texture indices of the faces +X -X +Y -Y +Z -Z
+            d.envmap_cube = 1
+            d.envmap_cube_faces[:] = [int(i) for i in envmap_cube]
+        if envmap is not None or envmap_cube is not None:
             d.envmap_intensity = float(envmap_intensity)
             d.envmap_rotation = float(envmap_rotation)
         keep = (pos, nrm, tm, mo, objs, mats, meds, pls, uv, d, texs,

@@ -400,7 +400,7 @@ void enqueueWave(rg_handle* h, const DevRender& R, const DevQueues& Q, const Dev
       if (profile) cudaEventRecord((*ev)[it * 4 + 2], st);
       launchConnect(&h->dscene, jobs, width, Q, it, 0, g.conn, st);
       if (h->dscene.numPointLights > 0) launchConnect(&h->dscene, jobs, width, Q, it, 1, g.conn, st);
-      if (h->dscene.envTex >= 0) launchConnect(&h->dscene, jobs, width, Q, it, 2, g.conn, st);
+      if (h->dscene.envOn) launchConnect(&h->dscene, jobs, width, Q, it, 2, g.conn, st);
       if (h->dscene.numVolLights > 0) launchConnect(&h->dscene, jobs, width, Q, it, 3, g.conn, st);
       if (profile) cudaEventRecord((*ev)[it * 4 + 3], st);
     }
@@ -571,6 +571,58 @@ bool buildEnvmapCdf(const rg_texture& T, std::vector<float>& marg, std::vector<f
   return true;
 }
 
+// Scene::buildEnvmapCDF, cubemap part (scene.cpp:343-410): per face, running
+// row sums of luminance x the texel's solid angle 1/(s^2+t^2+1)^1.5, rows
+// normalised to conditional CDFs, a per-face marginal over rows and a CDF over
+// the face totals; raw texels, sequential float sums.
+void buildCubeCdf(const rg_texture* faces[6], std::vector<float>& margFace, std::vector<float>& margY,
+                  std::vector<float>& cond, float& total) {
+  const int W = faces[0]->width, H = faces[0]->height;
+  margFace.assign(7, 0.0f);
+  margY.assign((size_t)6 * (H + 1), 0.0f);
+  cond.assign((size_t)6 * H * (W + 1), 0.0f);
+  float faceWeights[6] = {0, 0, 0, 0, 0, 0};
+  for (int f = 0; f < 6; f++) {
+    std::vector<float> rowWeight(H, 0.0f);
+    for (int y = 0; y < H; y++) {
+      float* c = &cond[((size_t)f * H + y) * (W + 1)];
+      float rowSum = 0.0f;
+      const float t = 1.0f - (y + 0.5f) * (2.0f / (float)H);
+      for (int x = 0; x < W; x++) {
+        const float sx = (x + 0.5f) * (2.0f / (float)W) - 1.0f;
+        const float denom = sx * sx + t * t + 1.0f;
+        const float jac = 1.0f / (denom * sqrtf(denom));
+        const float* px = faces[f]->rgba + ((size_t)y * W + x) * 4;
+        const float lum = fmaxf(0.0f, 0.2126f * px[0] + 0.7152f * px[1] + 0.0722f * px[2]);
+        rowSum += lum * jac;
+        c[x + 1] = rowSum;
+      }
+      if (rowSum > 0.0f) {
+        const float inv = 1.0f / rowSum;
+        for (int x = 1; x <= W; x++) c[x] *= inv;
+      }
+      rowWeight[y] = rowSum;
+    }
+    float* my = &margY[(size_t)f * (H + 1)];
+    for (int y = 0; y < H; y++) my[y + 1] = my[y] + rowWeight[y];
+    faceWeights[f] = my[H];
+    if (faceWeights[f] > 0.0f) {
+      const float inv = 1.0f / faceWeights[f];
+      for (int y = 0; y <= H; y++) my[y] *= inv;
+    }
+  }
+  total = 0.0f;
+  for (int f = 0; f < 6; f++) total += faceWeights[f];
+  if (total > 0.0f) {
+    const float inv = 1.0f / total;
+    float acc = 0.0f;
+    for (int f = 0; f < 6; f++) {
+      acc += faceWeights[f];
+      margFace[f + 1] = acc * inv;
+    }
+  }
+}
+
 // Validates a scene description, uploads it, builds its BVH and fills the
 // device-side table of pointers.  Used by rg_set_scene and the job server.
 rg_status prepareScene(const rg_scene_desc* d, int bins, bool wide, cudaStream_t st, int* errWord,
@@ -629,6 +681,21 @@ rg_status prepareScene(const rg_scene_desc* d, int bins, bool wide, cudaStream_t
   if (d->has_envmap && (d->envmap_texture < 0 || d->envmap_texture >= d->num_textures)) {
     setLastError("envmap texture index out of range");
     return RG_ERR_INVALID_ARGUMENT;
+  }
+  if (d->envmap_cube) {
+    for (int f = 0; f < 6; f++) {
+      const int t = d->envmap_cube_faces[f];
+      if (t < 0 || t >= d->num_textures) {
+        setLastError("cubemap face texture index out of range");
+        return RG_ERR_INVALID_ARGUMENT;
+      }
+      const rg_texture& T = d->textures[t];
+      const rg_texture& T0 = d->textures[d->envmap_cube_faces[0]];
+      if (T.width <= 0 || T.width != T.height || T.width != T0.width) {
+        setLastError("cubemap faces must be square and of one size");
+        return RG_ERR_INVALID_ARGUMENT;
+      }
+    }
   }
   out.reset(new DeviceScene());
   DeviceScene& ds = *out;
@@ -716,14 +783,30 @@ rg_status prepareScene(const rg_scene_desc* d, int bins, bool wide, cudaStream_t
     texs[i] = DevTexture{buf->p, t.width, t.height, t.is_hdr, 0};
   }
   if (ok) ok = ds.textures.upload(texs.data(), texs.size(), st);
-  if (ok && d->has_envmap) {
-    const rg_texture& T = d->textures[d->envmap_texture];
-    std::vector<float> marg, cond;
-    ds.envTex = d->envmap_texture;
+  if (ok && (d->has_envmap || d->envmap_cube)) {
     ds.envIntensity = d->envmap_intensity;
     const float yaw = d->envmap_rotation * (float)(M_PI / 180.0);
     ds.envCosY = cosf(yaw);
     ds.envSinY = sinf(yaw);
+  }
+  if (ok && d->envmap_cube) {
+    const rg_texture* faces[6];
+    for (int f = 0; f < 6; f++) {
+      faces[f] = &d->textures[d->envmap_cube_faces[f]];
+      ds.envFace[f] = d->envmap_cube_faces[f];
+    }
+    ds.envCube = 1;
+    std::vector<float> mf, my, mc;
+    buildCubeCdf(faces, mf, my, mc, ds.envCubeTotal);
+    ds.envCubeW = faces[0]->width;
+    ok = ds.cubeMargFace.upload(mf.data(), mf.size(), st) && ds.cubeMargY.upload(my.data(), my.size(), st) &&
+         ds.cubeCond.upload(mc.data(), mc.size(), st);
+    if (ok) ok = cudaStreamSynchronize(st) == cudaSuccess;
+  }
+  if (ok && d->has_envmap) {
+    const rg_texture& T = d->textures[d->envmap_texture];
+    std::vector<float> marg, cond;
+    ds.envTex = d->envmap_texture;
     if (buildEnvmapCdf(T, marg, cond, ds.envTotal)) {
       ds.envW = T.width;
       ds.envH = T.height;
@@ -807,6 +890,14 @@ rg_status prepareScene(const rg_scene_desc* d, int bins, bool wide, cudaStream_t
   S.envTotal = ds.envTotal;
   S.envMarg = ds.envMarg.p;
   S.envCond = ds.envCond.p;
+  S.envOn = (ds.envTex >= 0 || ds.envCube) ? 1 : 0;
+  S.envCube = ds.envCube;
+  for (int f = 0; f < 6; f++) S.envFace[f] = ds.envFace[f];
+  S.envCubeW = ds.envCubeW;
+  S.envCubeTotal = ds.envCubeTotal;
+  S.cubeMargFace = ds.cubeMargFace.p;
+  S.cubeMargY = ds.cubeMargY.p;
+  S.cubeCond = ds.cubeCond.p;
   return RG_OK;
 }
 
@@ -1150,7 +1241,7 @@ rg_status rg_render(rg_handle* h) {
     for (int v : c) tot += (uint64_t)v;
     S.samples = tot;
   }
-  const int perIter = 3 + (h->dscene.numPointLights > 0) + (h->dscene.envTex >= 0) + (h->dscene.numVolLights > 0);
+  const int perIter = 3 + (h->dscene.numPointLights > 0) + (h->dscene.envOn != 0) + (h->dscene.numVolLights > 0);
   const int perWave = s.shader_provider == 5 ? (3 + h->maxIter * perIter) : 4;
   S.kernel_launches = wavesDone * perWave;
   if (derr != 0) {

@@ -138,6 +138,14 @@ struct DevScene {
   float envIntensity, envCosY, envSinY, envTotal;
   const float* envMarg;       // H+1 marginal CDF over rows
   const float* envCond;       // H x (W+1) conditional CDFs
+  int envOn;                  // an environment (equirectangular or cubemap) is present
+  int envCube;                // cubemap faces present: lookups use them
+  int envFace[6];             // face textures +X -X +Y -Y +Z -Z
+  int envCubeW;               // face size of the cubemap CDF, 0 when not sampled
+  float envCubeTotal;
+  const float* cubeMargFace;  // 7: CDF over the faces
+  const float* cubeMargY;     // 6 x (W+1) per-face CDFs over rows
+  const float* cubeCond;      // 6 x W x (W+1) per-row CDFs
   // procedural media and volume lights
   const DevPathPoint* pathPts;
   const DevVolLight* volLights;

@@ -87,6 +87,8 @@ struct SceneStore {
   std::vector<rg_texture> textureDescs;
   rg_camera camera{};
   int32_t envmapTexture = -1;  // index into textures, -1 none
+  int32_t envCube = 0;         // cubemap faces present (px nx py ny pz nz)
+  int32_t envCubeFaces[6] = {-1, -1, -1, -1, -1, -1};
   float envmapIntensity = 1.0f, envmapRotation = 0.0f;
   rg_scene_desc desc{};
   void finalize();
@@ -133,6 +135,10 @@ struct DeviceScene {
   int envTex = -1, envW = 0, envH = 0;
   float envIntensity = 1.0f, envCosY = 1.0f, envSinY = 0.0f, envTotal = 0.0f;
   DevBuf<float> envMarg, envCond;
+  // cubemap environment: face textures and the per-face sampling CDFs
+  int envCube = 0, envFace[6] = {-1, -1, -1, -1, -1, -1}, envCubeW = 0;
+  float envCubeTotal = 0.0f;
+  DevBuf<float> cubeMargFace, cubeMargY, cubeCond;
   // BVH + leaf-order triangles
   DevBuf<float4> nodes, nodes8, triVerts, triShade;
   int numNodes8 = 0;

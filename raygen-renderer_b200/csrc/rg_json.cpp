@@ -7,7 +7,8 @@
 //    keys tolerated; containers still open at the end of input are closed
 //    there (one sample scene lacks its final brace).
 //  * Root keys: mainCamera, _materials, envmap (equirectangular Radiance
-//    .hdr / .pfm), medium (global), and child objects.
+//    .hdr / .pfm, or a cubemap directory of six faces), medium (global), and
+//    child objects.
 //  * Object keys: location, angle (degrees), scale, mesh (path | [paths] |
 //    {type: plane|cube|sphere|cone, ...}), mat (name | object), visible,
 //    medium (interior), children.  Keys are applied in file order.  Objects
@@ -1024,11 +1025,25 @@ struct Loader {
     if (v.type == JVal::Str) {
       rel = v.s;
     } else if (v.type == JVal::Obj) {
+      // cubemap: six faces px nx py ny pz nz.<ext> (ext "jpg" by default) in a
+      // directory, read through the texture pool; all six or none
+      // (sceneloader.cpp:725-744, scene.cpp:348)
       if (const JVal* c = v.get("cubemap"))
         if (c->type == JVal::Str && !c->s.empty()) {
-          err = "cubemap environment maps are not read (their faces are JPEG images): " + c->s;
-          code = RG_ERR_UNSUPPORTED;
-          return false;
+          std::string dir = c->s;
+          if (dir.back() != '/' && dir.back() != '\\') dir += "/";
+          std::string ext = "jpg";
+          if (const JVal* e = v.get("ext"))
+            if (e->type == JVal::Str && !e->s.empty()) ext = e->s;
+          static const char* names[6] = {"px", "nx", "py", "ny", "pz", "nz"};
+          int faces[6];
+          bool all = true;
+          for (int f = 0; f < 6; f++) {
+            faces[f] = texture(dir + names[f] + "." + ext);
+            all = all && faces[f] >= 0;
+          }
+          st.envCube = all ? 1 : 0;
+          for (int f = 0; f < 6; f++) st.envCubeFaces[f] = all ? faces[f] : -1;
         }
       if (const JVal* t = v.get("texture"))
         if (t->type == JVal::Str) rel = t->s;

@@ -427,6 +427,8 @@ void SceneStore::finalize() {
   desc.envmap_texture = envmapTexture;
   desc.envmap_intensity = envmapIntensity;
   desc.envmap_rotation = envmapRotation;
+  desc.envmap_cube = envCube;
+  for (int f = 0; f < 6; f++) desc.envmap_cube_faces[f] = envCubeFaces[f];
 }
 
 }  // namespace rg

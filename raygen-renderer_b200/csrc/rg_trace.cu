@@ -274,29 +274,73 @@ constexpr float kPi2 = (float)(3.14159265358979323846 * 3.14159265358979323846);
 __device__ __forceinline__ bool envSampling(const DevScene* S) {
   return S->envTex >= 0 && S->envW > 0 && S->envTotal > 0.0f;
 }
+__device__ __forceinline__ bool cubeSampling(const DevScene* S) { return S->envCubeW > 0 && S->envCubeTotal > 0.0f; }
+
+// Cubemap face and face-local (s, t) of a rotated direction (OpenGL
+// convention, rayrenderer.cpp:1311-1333).
+__device__ __forceinline__ int cubeFace(float rx, float ry, float rz, float& sc, float& tc, float& ma) {
+  const float ax = fabsf(rx), ay = fabsf(ry), az = fabsf(rz);
+  if (ax >= ay && ax >= az) {
+    ma = ax;
+    if (rx > 0) { sc = -rz; tc = ry; return 0; }
+    sc = rz; tc = ry; return 1;
+  }
+  if (ay >= ax && ay >= az) {
+    ma = ay;
+    if (ry > 0) { sc = rx; tc = rz; return 2; }
+    sc = rx; tc = -rz; return 3;
+  }
+  ma = az;
+  if (rz > 0) { sc = rx; tc = ry; return 4; }
+  sc = -rx; tc = ry; return 5;
+}
+
+__device__ __forceinline__ float cubeTexelLum(const DevScene* S, int face, int x, int y) {
+  const float4 c = __ldg(S->textures[S->envFace[face]].texels + (size_t)y * S->envCubeW + x);
+  return fmaxf(0.0f, 0.2126f * c.x + 0.7152f * c.y + 0.0722f * c.z);
+}
 
 __device__ __forceinline__ float envTexelLum(const DevScene* S, int x, int y) {
   const float4 c = __ldg(S->textures[S->envTex].texels + (size_t)y * S->envW + x);
   return fmaxf(0.0f, 0.2126f * c.x + 0.7152f * c.y + 0.0722f * c.z);
 }
 
-// sampleEnvironment, equirectangular branch (rayrenderer.cpp:1299-1348)
+// sampleEnvironment (rayrenderer.cpp:1299-1348): the cubemap when present, else
+// the equirectangular map
 __device__ __noinline__ V3 envRadiance(const DevScene* S, V3 dir) {
-  if (S->envTex < 0) return v3(0, 0, 0);
+  if (!S->envOn) return v3(0, 0, 0);
   const V3 d = normalize(dir);
   const float rx = d.x * S->envCosY - d.z * S->envSinY;
   const float rz = d.x * S->envSinY + d.z * S->envCosY;
+  if (S->envCube) {
+    float sc, tc, ma;
+    const int face = cubeFace(rx, d.y, rz, sc, tc, ma);
+    const float u = 0.5f * (sc / ma + 1.0f);
+    const float v = 0.5f * (1.0f - tc / ma);
+    return texSample(*S, S->envFace[face], u, v) * S->envIntensity;
+  }
   const float u = 0.5f + atan2f(rz, rx) * kInv2Pi;
   const float v = 0.5f - asinf(fminf(fmaxf(d.y, -1.0f), 1.0f)) * kInvPi;
   return texSample(*S, S->envTex, u, v) * S->envIntensity;
 }
 
-// envmapDirectionPdf, equirectangular branch (rayrenderer.cpp:1521-1573)
+// envmapDirectionPdf (rayrenderer.cpp:1521-1573)
 __device__ __noinline__ float envPdf(const DevScene* S, V3 dir) {
-  if (!envSampling(S)) return 0.0f;
   const V3 d = normalize(dir);
   const float rx = d.x * S->envCosY - d.z * S->envSinY;
   const float rz = d.x * S->envSinY + d.z * S->envCosY;
+  if (cubeSampling(S)) {
+    float sc, tc, ma;
+    const int face = cubeFace(rx, d.y, rz, sc, tc, ma);
+    if (ma <= 0.0f) return 0.0f;
+    const float u = 0.5f * (sc / ma + 1.0f);
+    const float v = 0.5f * (1.0f - tc / ma);
+    const int W = S->envCubeW;
+    const int x = min(max((int)(u * W), 0), W - 1);
+    const int y = min(max((int)(v * W), 0), W - 1);
+    return cubeTexelLum(S, face, x, y) * (float)(W * W) / (4.0f * S->envCubeTotal);
+  }
+  if (!envSampling(S)) return 0.0f;
   const int W = S->envW, H = S->envH;
   const float u = 0.5f + atan2f(rz, rx) * kInv2Pi;
   const float v = 0.5f - asinf(fminf(fmaxf(d.y, -1.0f), 1.0f)) * kInvPi;
@@ -334,6 +378,34 @@ __device__ __noinline__ EnvSample envSample(const DevScene* S, float u0, float u
   r.dir = v3(0, 1, 0);
   r.pdf = 0.0f;
   r.Li = v3(0, 0, 0);
+  if (cubeSampling(S)) {  // face, row, texel (rayrenderer.cpp:1384-1433)
+    const int W = S->envCubeW, H = W;
+    const int face = searchCDF(S->cubeMargFace, 6, u0);
+    const float faceLo = __ldg(S->cubeMargFace + face), faceSpan = __ldg(S->cubeMargFace + face + 1) - faceLo;
+    const float u0r = faceSpan > 0.0f ? (u0 - faceLo) / faceSpan : 0.5f;
+    const float* marY = S->cubeMargY + (size_t)face * (H + 1);
+    const int y = searchCDF(marY, H, u0r);
+    const float yLo = __ldg(marY + y), ySpan = __ldg(marY + y + 1) - yLo;
+    const float yFrac = ySpan > 0.0f ? (u0r - yLo) / ySpan : 0.5f;
+    const float* condX = S->cubeCond + ((size_t)face * H + y) * (W + 1);
+    const int x = searchCDF(condX, W, u1);
+    const float xLo = __ldg(condX + x), xSpan = __ldg(condX + x + 1) - xLo;
+    const float xFrac = xSpan > 0.0f ? (u1 - xLo) / xSpan : 0.5f;
+    const float sc = 2.0f * ((x + xFrac) / (float)W) - 1.0f, tc = 1.0f - 2.0f * ((y + yFrac) / (float)H);
+    V3 l;  // cubeFaceDir (rayrenderer.cpp:1367-1376)
+    switch (face) {
+      case 0: l = v3(1.0f, tc, -sc); break;
+      case 1: l = v3(-1.0f, tc, sc); break;
+      case 2: l = v3(sc, 1.0f, tc); break;
+      case 3: l = v3(sc, -1.0f, -tc); break;
+      case 4: l = v3(sc, tc, 1.0f); break;
+      default: l = v3(-sc, tc, -1.0f); break;
+    }
+    r.dir = normalize(v3(l.x * S->envCosY + l.z * S->envSinY, l.y, -l.x * S->envSinY + l.z * S->envCosY));
+    r.pdf = cubeTexelLum(S, face, x, y) * (float)(W * H) / (4.0f * S->envCubeTotal);
+    if (r.pdf > 0.0f) r.Li = envRadiance(S, r.dir);
+    return r;
+  }
   if (!envSampling(S)) return r;
   const int W = S->envW, H = S->envH;
   const int y = searchCDF(S->envMarg, H, u0);
@@ -363,7 +435,7 @@ __device__ __noinline__ EnvSample envSample(const DevScene* S, float u0, float u
 // unbounded shadow ray (tmax 1e30) with the point/env occluders, queue C.
 __device__ __forceinline__ bool envNEE(const DevScene* S, const Rng& rng, int v, V3 hit, V3 n, EnvSample& e,
                                        Shadow& sh) {
-  if (!envSampling(S)) return false;
+  if (!envSampling(S) && !cubeSampling(S)) return false;
   e = envSample(S, rng.prng(v, S_ENV0), rng.prng(v, S_ENV1));
   if (e.pdf <= 0.0f || dot(e.dir, n) <= 0.0f) return false;
   sh.o = surfaceOrigin(hit, e.dir, n);
@@ -868,7 +940,7 @@ __global__ void __launch_bounds__(256) k_shade(DevScene S0, DevRender R0, const 
               shA.on = true;
               shA.c = beta * sw * Le * (phaseTo(lDir) / pl);
             }
-            if (ENV && S.envTex >= 0) {  // environment NEE at the scatter point (rayrenderer.cpp:1757-1761)
+            if (ENV && S.envOn) {  // environment NEE at the scatter point (rayrenderer.cpp:1757-1761)
               EnvSample e;
               if (envNEE(&jobs[slot].S, rng, v, pos, proxy, e, shE)) {
                 shE.on = true;
@@ -929,14 +1001,14 @@ __global__ void __launch_bounds__(256) k_shade(DevScene S0, DevRender R0, const 
           if (surv > 0.0f)
             beta = beta * v3(expf(-M.str * maxT) / surv, expf(-M.stg * maxT) / surv, expf(-M.stb * maxT) / surv);
           if (prim < 0) {
-            if (ENV && S.envTex >= 0) L = L + beta * envMiss(&jobs[slot].S, d, bsdfPdf);  // rayrenderer.cpp:1852-1863
+            if (ENV && S.envOn) L = L + beta * envMiss(&jobs[slot].S, d, bsdfPdf);  // rayrenderer.cpp:1852-1863
             done = true;
           }
           silhouette = true;
         }
       } else if (prim < 0) {
         // environment miss (rayrenderer.cpp:1619-1630; the eye ray has no pdf, so no weight)
-        if (ENV && S.envTex >= 0) L = L + beta * envMiss(&jobs[slot].S, d, bsdfPdf);
+        if (ENV && S.envOn) L = L + beta * envMiss(&jobs[slot].S, d, bsdfPdf);
         done = true;
       }
       // ---- surface vertex (RayBSDFShaderProvider::shade, rayrenderer.cpp:2776-2896)
@@ -1042,7 +1114,7 @@ __global__ void __launch_bounds__(256) k_shade(DevScene S0, DevRender R0, const 
             const V3 dir = cosineWeightedDirection(h.n, rng.lds(d0), rng.lds(d0 + 1));
             traceLight(S, R, rng, v, h.p, h.n, beta * albedo, shA, shB);
             bsdfPdf = fmaxf(0.0f, dot(dir, h.n)) * (1.0f / kPi);
-            if (ENV && S.envTex >= 0) {  // traceEnvmapLight (rayrenderer.cpp:1484-1519)
+            if (ENV && S.envOn) {  // traceEnvmapLight (rayrenderer.cpp:1484-1519)
               EnvSample e;
               if (envNEE(&jobs[slot].S, rng, v, h.p, h.n, e, shE)) {
                 // the MIS partner is this vertex's own sampled-direction pdf, as passed at bsdf.cpp:86-88
@@ -1138,7 +1210,7 @@ __global__ void __launch_bounds__(256) k_shade(DevScene S0, DevRender R0, const 
                   shA.c = beta * Le * fCos * (pl * pl / (pl * pl + pb * pb) / pl);
                 }
                 // environment NEE with MIS (bsdf.cpp:302-314)
-                if (ENV && S.envTex >= 0) {
+                if (ENV && S.envOn) {
                   EnvSample e;
                   if (envNEE(&jobs[slot].S, rng, v, h.p, h.n, e, shE) && evalGlossy(e.dir, fCos, pb)) {
                     shE.on = true;
@@ -1355,7 +1427,7 @@ __global__ void __launch_bounds__(128) k_simple(const DevJob* __restrict__ jobs,
       const ClosestHit ch = traceClosest(S, o, d, nodes, tris);
       if (ch.prim < 0) {
         // traceEyeRay's miss and tracePath's miss without BSDF parameters (rayrenderer.cpp:1292, 1619)
-        if (S.envTex >= 0) total = total + w * envRadiance(&S, d);
+        if (S.envOn) total = total + w * envRadiance(&S, d);
         break;
       }
       if (depth == 0) eyeHit = true;
@@ -1553,7 +1625,7 @@ void launchShade(const DevScene* single, const DevRender* singleR, const DevJob*
     else k_shade<true, true, 1><<<grid, 256, 0, st>>>(DevScene{}, DevRender{}, jobs, Q, iter);
     return;
   }
-  const bool env = single->envTex >= 0;
+  const bool env = single->envOn != 0;
   const int ml = single->mediaLevel;
   if (!env) {
     if (ml == 0) k_shade<false, false, 0><<<grid, 256, 0, st>>>(*single, *singleR, jobs, Q, iter);

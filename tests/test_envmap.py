@@ -76,11 +76,9 @@ def test_envmap_json_keys(rg, tmp_path):
     (tmp_path / "m.json").write_text(json.dumps({"envmap": {"texture": "nothere.hdr"}, "f": {"mesh": {"type": "plane"}}}))
     d = rg.Scene.from_json(str(tmp_path / "m.json")).desc
     assert d.has_envmap == 0 and d.num_triangles == 2
-    # cubemaps (JPEG faces) are refused
+    # a cubemap with missing faces gives no cubemap (all six or none, scene.cpp:348)
     (tmp_path / "c.json").write_text(json.dumps({"envmap": {"cubemap": "../cube", "ext": "jpg"}}))
-    with pytest.raises(rg.RayGenError, match="cubemap") as e:
-        rg.Scene.from_json(str(tmp_path / "c.json"))
-    assert e.value.code == rg.RG_ERR_UNSUPPORTED
+    assert rg.Scene.from_json(str(tmp_path / "c.json")).desc.envmap_cube == 0
 
 
 def random_dirs(n, seed):
@@ -181,3 +179,76 @@ def test_oracle_eye_miss_sees_environment(rg, orc, tmp_path):
     for shader in (5, 2, 0):
         r = orc.OracleScene(sc.ptr).render(16, 16, 4, shader=shader, seed=1)
         np.testing.assert_allclose(r["hdr"][..., :3], np.broadcast_to(ref[0, 0] * 2.0, (16, 16, 3)), rtol=1e-6)
+
+
+# ---------------------------------------------------------------- cubemaps
+FACE_COLOURS = [(230, 40, 40), (40, 230, 40), (40, 40, 230), (230, 230, 40), (40, 230, 230), (230, 40, 230)]
+
+
+def cube_dir(tmp_path, colours=FACE_COLOURS, size=8, ext="png", sun=None):
+    """Six PNG faces px nx py ny pz nz, each one flat colour (optionally a bright texel on one face)."""
+    import image_codecs as ic
+    d = tmp_path / "cube"
+    d.mkdir(exist_ok=True)
+    for k, name in enumerate(("px", "nx", "py", "ny", "pz", "nz")):
+        img = np.tile(np.array(colours[k], np.int64), (size, size, 1))
+        if sun is not None and sun[0] == k:
+            img[sun[1], sun[2]] = (255, 255, 255)
+        ic.write_png(str(d / f"{name}.{ext}"), img, 2, 8)
+    return d
+
+
+def test_cubemap_loads_and_looks_up_faces(rg, orc, tmp_path):
+    cube_dir(tmp_path)
+    doc = {"envmap": {"cubemap": "cube", "ext": "png", "intensity": 2.0}, "f": {"mesh": {"type": "plane"}}}
+    (tmp_path / "cube.json").write_text(json.dumps(doc))
+    sc = rg.Scene.from_json(str(tmp_path / "cube.json"))
+    d = sc.desc
+    assert d.envmap_cube == 1 and d.has_envmap == 0 and d.num_textures == 6
+    assert len(set(d.envmap_cube_faces)) == 6
+    o = orc.OracleScene(sc.ptr)
+    dirs = np.array([[1, 0.1, 0.2], [-1, 0.2, -0.1], [0.1, 1, 0.3], [0.2, -1, 0.1], [0.1, 0.2, 1], [0.3, 0.1, -1]],
+                    np.float32)  # camera at the origin with zero angles: view = world
+    rgb, pdf = o.env_eval(dirs)
+    srgb = lambda c: np.where(c <= 0.04045, c / 12.92, ((c + 0.055) / 1.055) ** 2.4)
+    want = 2.0 * srgb(np.array(FACE_COLOURS) / 255.0)
+    np.testing.assert_allclose(rgb, want, rtol=1e-5)
+    assert np.all(pdf > 0)
+
+
+def test_cubemap_pdf_normalises_and_matches_its_sampler(rg, orc, tmp_path):
+    cube_dir(tmp_path, sun=(2, 3, 5))
+    doc = {"envmap": {"cubemap": "cube", "ext": "png", "rotation": 25}, "f": {"mesh": {"type": "plane"}}}
+    (tmp_path / "cube.json").write_text(json.dumps(doc))
+    sc = rg.Scene.from_json(str(tmp_path / "cube.json"))  # keeps the description alive
+    o = orc.OracleScene(sc.ptr)
+    # integral of the pdf over the sphere (uniform directions)
+    _, pdf = o.env_eval(random_dirs(400000, 3))
+    assert pdf.mean() * 4 * np.pi == pytest.approx(1.0, rel=0.02)
+    # directions drawn by the sampler carry the pdf that the lookup reports
+    u = np.random.default_rng(4).random((20000, 2)).astype(np.float32)
+    dirs, spdf = o.env_sample(u)
+    _, lpdf = o.env_eval(dirs)
+    ok = spdf > 0
+    assert ok.mean() > 0.99
+    assert np.mean(np.isclose(spdf[ok], lpdf[ok], rtol=1e-4)) > 0.99  # texel-boundary ties aside
+    # per region of the sphere, the share of samples equals the pdf's mass there
+    region = lambda v: np.argmax(np.abs(v), axis=1) * 2 + (np.take_along_axis(v, np.argmax(np.abs(v), axis=1)[:, None], 1)[:, 0] < 0)
+    uni = random_dirs(400000, 5)
+    _, updf = o.env_eval(uni)
+    for r in range(6):
+        mass = 4 * np.pi * np.mean(updf * (region(uni) == r))
+        assert np.mean(region(dirs) == r) == pytest.approx(mass, abs=0.01)
+
+
+def test_cubemap_white_furnace_in_the_oracle(rg, orc, tmp_path):
+    cube_dir(tmp_path, colours=[(204, 204, 204)] * 6)
+    doc = {"mainCamera": {"location": [0, 1, 0], "angle": [-90, 0, 0], "fieldOfView": 40},
+           "envmap": {"cubemap": "cube", "ext": "png"},
+           "floor": {"scale": [1000, 1, 1000], "mesh": {"type": "plane"}, "mat": {"color": [0.5, 0.5, 0.5]}}}
+    (tmp_path / "f.json").write_text(json.dumps(doc))
+    sc = rg.Scene.from_json(str(tmp_path / "f.json"))
+    out = orc.OracleScene(sc.ptr).render(8, 8, 64, max_depth=8, seed=2)
+    L = ((204 / 255 + 0.055) / 1.055) ** 2.4
+    mean = out["sum"].sum(axis=(0, 1)) / out["n"].sum()
+    assert np.allclose(mean, 0.5 * L, rtol=0.02), (mean, 0.5 * L)

@@ -81,3 +81,33 @@ def test_env_server_matches_renderer(rg, tmp_path):
     b = r.get_hdr_result()
     r.close()
     np.testing.assert_allclose(a, b, rtol=1e-4, atol=1e-6)
+
+
+def _cube(tmp_path, colours, sun=None, size=16):
+    from test_envmap import cube_dir
+    return cube_dir(tmp_path, colours=colours, size=size, sun=sun)
+
+
+def test_cubemap_white_furnace_on_device(rg, tmp_path):
+    _cube(tmp_path, [(204, 204, 204)] * 6)
+    doc = {"mainCamera": {"location": [0, 1, 0], "angle": [-90, 0, 0], "fieldOfView": 40},
+           "envmap": {"cubemap": "cube", "ext": "png"},
+           "floor": {"scale": [1000, 1, 1000], "mesh": {"type": "plane"}, "mat": {"color": [0.5, 0.5, 0.5]}}}
+    (tmp_path / "f.json").write_text(json.dumps(doc))
+    r = render_gpu(rg, rg.Scene.from_json(str(tmp_path / "f.json")), 64, 64, 64, maxDepth=8, seed=2)
+    m = r.get_hdr_result()[..., :3]
+    r.close()
+    L = ((204 / 255 + 0.055) / 1.055) ** 2.4
+    assert m.mean() == pytest.approx(0.5 * L, rel=0.005)
+
+
+def test_cubemap_image_parity(rg, orc, tmp_path):
+    from test_envmap import FACE_COLOURS
+    _cube(tmp_path, FACE_COLOURS, sun=(2, 5, 9))
+    doc = {"mainCamera": CAMERA, "envmap": {"cubemap": "cube", "ext": "png", "intensity": 1.2, "rotation": 40}}
+    doc.update(SPHERES)
+    (tmp_path / "cube.json").write_text(json.dumps(doc))
+    sc = rg.Scene.from_json(str(tmp_path / "cube.json"))
+    assert sc.desc.envmap_cube == 1
+    z, g, m, stats = image_parity(rg, orc, sc, 64, 40, 128, maxDepth=8, rrDepth=3, seed=6)
+    check_z(z, g, m, "cubemap-lit spheres", tail=0.01)

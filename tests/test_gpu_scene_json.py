@@ -78,3 +78,40 @@ def test_cli_renders_json_scene(rg, tmp_path):
     assert img.shape == ref.shape
     np.testing.assert_allclose(img, ref, rtol=0, atol=0)
     assert img.mean() > 0.01
+
+
+def test_json_textured_materials_image_parity(rg, orc, tmp_path):
+    """'tex' textures from a JPEG (4:2:0, restart intervals) and a PNG, sampled
+    with the sRGB decode (Texture::sample, texture.cpp:210-241)."""
+    import image_codecs as ic
+    y, x = np.mgrid[0:64, 0:96]
+    checker = np.where(((x // 12) + (y // 12)) % 2 == 0, 220, 40)
+    img = np.stack([checker, 0.6 * checker + 40, 255 - checker], axis=-1).astype(np.float64)
+    ic.encode_jpeg(str(tmp_path / "wood.jpg"), img, sampling=((2, 2), (1, 1), (1, 1)), restart=4)
+    stripes = np.stack([np.where((x // 8) % 2 == 0, 250, 20)[:32, :32]] * 3, axis=-1)
+    ic.write_png(str(tmp_path / "stripes.png"), stripes.astype(np.int64), 2, 8)
+    doc = {
+        "mainCamera": {"location": [0, 1.5, 5], "angle": [-15, 0, 0], "fieldOfView": 50},
+        "lamp": {"location": [0, 4, 0], "angle": [180, 0, 0], "scale": [2, 1, 2], "mesh": {"type": "plane"},
+                 "mat": {"color": [1, 1, 1], "emission": 8}},
+        "floor": {"location": [0, -1, 0], "scale": [8, 1, 8], "mesh": {"type": "plane"},
+                  "mat": {"tex": "wood.jpg", "texTiling": [2, 2]}},
+        "box": {"location": [0.8, -0.3, 0], "angle": [0, 30, 0], "scale": [1.2, 1.4, 1.2], "mesh": {"type": "cube"},
+                "mat": {"tex": "stripes.png", "color": [0.9, 0.8, 0.7]}},
+        "ball": {"location": [-1.3, -0.2, 0.5], "mesh": {"type": "sphere", "radius": 0.8, "stacks": 16, "slices": 32},
+                 "mat": {"tex": "wood.jpg", "glossy": 1, "roughness": 0.3}},
+    }
+    (tmp_path / "tex.json").write_text(json.dumps(doc))
+    sc = rg.Scene.from_json(str(tmp_path / "tex.json"))
+    assert sc.desc.num_textures == 2
+    z, g, m, stats = image_parity(rg, orc, sc, 64, 40, 64, maxDepth=6, rrDepth=3, seed=3)
+    check_z(z, g, m, "textured JSON scene", tail=0.01)
+    # the textures really are sampled: the same scene without them renders differently
+    doc2 = json.loads(json.dumps(doc))
+    for k in ("floor", "box", "ball"):
+        doc2[k]["mat"].pop("tex")
+    (tmp_path / "flat.json").write_text(json.dumps(doc2))
+    r = render_gpu(rg, rg.Scene.from_json(str(tmp_path / "flat.json")), 64, 40, 64, maxDepth=6, rrDepth=3, seed=3)
+    flat = r.get_hdr_result()[..., :3]
+    r.close()
+    assert np.abs(flat - g).mean() > 0.02 * max(g.mean(), 1e-3)
