@@ -624,7 +624,7 @@ __global__ void __launch_bounds__(128) k_connect(const DevJob* __restrict__ jobs
 // Stack entries: node group (childBase, hits | imask << 8) or triangle group
 // (triBase | 0x80000000, triangle mask).
 constexpr int kRefillIdle = 8;     // refill once this many lanes are idle
-constexpr int kTriVotes = 10;      // lanes with triangles needed to run a triangle step
+constexpr int kTriVotes = 4;       // lanes with triangles needed to run a triangle step (swept: 2-4 best, 10 -1.6%)
 
 template <bool ANY, bool MULTI>
 __device__ __forceinline__ void traverseWave8(const DevScene& S0, const DevJob* __restrict__ jobs, int count, int* fetch, const float4* __restrict__ rO,
@@ -797,8 +797,10 @@ __device__ __forceinline__ void traverseWave8(const DevScene& S0, const DevJob* 
   }
 }
 
+// 8 resident blocks per SM (64 registers): the traversals are latency-bound, and
+// 32 warps per SM beat 28 (72 registers); more blocks spill and lose.
 template <bool MULTI>
-__global__ void __launch_bounds__(128) k_extend8(DevScene S0, const DevJob* __restrict__ jobs, DevQueues Q, int iter) {
+__global__ void __launch_bounds__(128, 8) k_extend8(DevScene S0, const DevJob* __restrict__ jobs, DevQueues Q, int iter) {
   const int count = Q.counters[iter * kCountersPerIter + C_RAYS];
   uint32_t nodes = 0, tris = 0, rays = 0;
   traverseWave8<false, MULTI>(S0, jobs, count, &Q.counters[iter * kCountersPerIter + C_FETCH_EXT], Q.rayO[iter & 1],
@@ -809,7 +811,7 @@ __global__ void __launch_bounds__(128) k_extend8(DevScene S0, const DevJob* __re
 }
 
 template <bool MULTI>
-__global__ void __launch_bounds__(128) k_connect8(DevScene S0, const DevJob* __restrict__ jobs, DevQueues Q, int iter,
+__global__ void __launch_bounds__(128, 8) k_connect8(DevScene S0, const DevJob* __restrict__ jobs, DevQueues Q, int iter,
                                                   int which) {
   const int count = Q.counters[iter * kCountersPerIter + shadowCountSlot(which)];
   uint32_t nodes = 0, tris = 0, rays = 0;
