@@ -40,6 +40,33 @@ void setLastError(const std::string& msg) { g_lastError = msg; }
 
 __global__ void k_nextWave(int* cur) { *cur += 1; }
 
+void keepPoolMemory() {
+  static std::mutex mu;
+  static std::vector<char> done;
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) return;
+  std::lock_guard<std::mutex> lk(mu);
+  if ((int)done.size() <= dev) done.resize(dev + 1, 0);
+  if (done[dev]) return;
+  cudaMemPool_t pool;
+  if (cudaDeviceGetDefaultMemPool(&pool, dev) == cudaSuccess) {
+    uint64_t keep = ~0ull;
+    cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+  }
+  cudaGetLastError();
+  done[dev] = 1;
+}
+
+void trimPoolMemory() {
+  int dev = 0;
+  cudaMemPool_t pool;
+  if (cudaGetDevice(&dev) == cudaSuccess && cudaDeviceGetDefaultMemPool(&pool, dev) == cudaSuccess) {
+    cudaStreamSynchronize(cudaStreamPerThread);
+    cudaMemPoolTrimTo(pool, 0);
+  }
+  cudaGetLastError();
+}
+
 // Camera view matrix, row-vector convention p_view = [p 1] * M.
 // Camera orientation R = Ry(angle.y) * Rx(angle.x) * Rz(angle.z) (degrees);
 // p_view = R^T (p - location).  With zero angles this is exactly p - location.
@@ -482,6 +509,7 @@ rg_status rg_create(const rg_settings* s, rg_handle** out) {
   else rg_settings_default(&h->st);
   cudaGetDevice(&h->device);
   cudaDeviceGetAttribute(&h->numSMs, cudaDevAttrMultiProcessorCount, h->device);
+  keepPoolMemory();
   if (cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking) != cudaSuccess) {
     setLastError("cudaStreamCreate failed");
     delete h;
@@ -498,6 +526,7 @@ rg_status rg_destroy(rg_handle* h) {
     if (h->stream) cudaStreamSynchronize(h->stream);
   }
   delete h;
+  trimPoolMemory();
   return RG_OK;
 }
 

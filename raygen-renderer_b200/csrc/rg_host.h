@@ -30,6 +30,14 @@ DevRender makeRenderParams(const rg_settings& s, const rg_camera& c);
 struct DevPointLight;
 struct DevTexture;
 
+// Device buffers come from the device's default stream-ordered pool.  With
+// its default release threshold (0) every synchronisation hands freed memory
+// back to the driver, so re-uploading a large scene re-maps hundreds of MB;
+// keepPoolMemory() raises the threshold for the current device (once), and
+// trimPoolMemory() returns unused memory when a handle goes away.
+void keepPoolMemory();
+void trimPoolMemory();
+
 // Owning device allocation from the stream-ordered pool.  Allocation and free
 // are ordered on the calling thread's per-thread stream, so releasing a buffer
 // does not synchronise the device; callers release a buffer only after the

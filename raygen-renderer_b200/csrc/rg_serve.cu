@@ -489,6 +489,7 @@ rg_status rg_server_create(const rg_settings* base, const rg_server_config* cfg,
   }
   rg_server* s = new (std::nothrow) rg_server();
   if (!s) return RG_ERR_OUT_OF_MEMORY;
+  keepPoolMemory();
   if (base) s->base = *base;
   else rg_settings_default(&s->base);
   if (cfg) s->cfg = *cfg;
@@ -729,6 +730,7 @@ rg_status rg_server_destroy(rg_server* s) {
   for (auto* j : s->slotJob)
     if (j) releaseJob(s, j);
   delete s;
+  trimPoolMemory();
   return RG_OK;
 }
 
