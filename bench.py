@@ -133,14 +133,17 @@ def measured_peak_hbm():
 
 
 def profile_traffic():
-    """Per-launch DRAM bytes of the extend kernel from the committed ncu summary, if any."""
-    path = os.path.join(ROOT, "profiles", "extend_dram.json")
+    """DRAM bytes per closest-hit ray of the extend kernel, from the committed ncu
+    summary (a line "DRAM bytes per closest-hit ray: N"), or None."""
+    path = os.path.join(ROOT, "profiles", "extend_dram_heavy_480x270.md")
     try:
         with open(path) as f:
-            d = json.load(f)
-        return d
-    except Exception:
-        return None
+            for line in f:
+                if line.startswith("DRAM bytes per closest-hit ray:"):
+                    return {"bytes_per_ray": float(line.split(":")[1].split()[0])}
+    except OSError:
+        pass
+    return None
 
 
 def cpu_scene(scene_ptr):
@@ -557,7 +560,7 @@ def main():
                 "launches": launches_ext, "avg_launch_ms": round(ext_ms / max(1, launches_ext), 4),
                 "algorithmic_bytes_per_launch": round(alg_bytes / max(1, launches_ext)),
                 "shade_ms": round(s["shade_ms"], 2), "connect_ms": round(s["connect_ms"], 2),
-                "extend_ms": round(ext_ms, 2),
+                "extend_ms": round(ext_ms, 2), "closest_rays_per_render": int(s["closest_rays"]),
                 "rays_per_sample": round((s["closest_rays"] + s["shadow_rays"]) / max(1, s["samples"]), 3),
                 "nodes_per_ray": round(s["nodes_visited"] / max(1, s["closest_rays"]), 2),
                 "tris_per_ray": round(s["tris_tested"] / max(1, s["closest_rays"]), 2),
