@@ -727,9 +727,9 @@ __device__ __forceinline__ void traverseWave8(const DevScene& S0, const DevJob* 
           tMask &= tMask - 1u;
           const int tk = tBase + i;
           const float4* tp = trisP + (size_t)tk * 3;
-          const float4 b = ldg4(tp + 1);
+          const float4 b = ldTri4(tp + 1);
           if (!ANY || (__float_as_uint(b.w) & occ)) {
-            const float4 a = ldg4(tp), c = ldg4(tp + 2);
+            const float4 a = ldTri4(tp), c = ldTri4(tp + 2);
             tris++;
             if (ANY) {
               if (mtAny(o, d, xyz(a), xyz(b), xyz(c), tmax)) result = 2;

@@ -19,6 +19,9 @@
 namespace rg {
 
 __device__ __forceinline__ float4 ldg4(const float4* p) { return __ldg(p); }
+// BVH node and triangle fetches of the 8-wide traversal
+__device__ __forceinline__ float4 ldNode4(const float4* p) { return __ldg(p); }
+__device__ __forceinline__ float4 ldTri4(const float4* p) { return __ldg(p); }
 
 __device__ __forceinline__ V3 safeInv(V3 d) {
   return v3(fabsf(d.x) > 1e-20f ? 1.0f / d.x : 1e30f, fabsf(d.y) > 1e-20f ? 1.0f / d.y : 1e30f,
@@ -227,7 +230,8 @@ __device__ __forceinline__ float biasedByte(uint32_t w, uint32_t k) {
 }
 
 __device__ __forceinline__ Node8Hit intersectNode8(const float4* np, V3 o, V3 inv, float tcap, uint32_t oct) {
-  const float4 n0 = ldg4(np), n1 = ldg4(np + 1), n2 = ldg4(np + 2), n3 = ldg4(np + 3), n4 = ldg4(np + 4);
+  const float4 n0 = ldNode4(np), n1 = ldNode4(np + 1), n2 = ldNode4(np + 2), n3 = ldNode4(np + 3),
+               n4 = ldNode4(np + 4);
   const uint32_t eb = __float_as_uint(n0.w);
   const int ex = (int)(int8_t)(eb & 0xffu), ey = (int)(int8_t)((eb >> 8) & 0xffu), ez = (int)(int8_t)((eb >> 16) & 0xffu);
   const float sx = __int_as_float((ex + 127) << 23), sy = __int_as_float((ey + 127) << 23),
