@@ -561,15 +561,23 @@ class RayRenderer:
         self._sync_settings()
         _check(self._lib.rg_reapply_postprocess(self._h))
 
-    def get_hdr_result(self) -> np.ndarray:
+    def _result_buffer(self, out):
         h, w = self._size()
-        out = np.empty((h, w, 4), np.float32)
+        if out is None:
+            return np.empty((h, w, 4), np.float32)
+        if out.dtype != np.float32 or out.shape != (h, w, 4) or not out.flags.c_contiguous:
+            raise ValueError(f"out must be a C-contiguous float32 array of shape {(h, w, 4)}")
+        return out
+
+    def get_hdr_result(self, out: np.ndarray = None) -> np.ndarray:
+        """Linear HDR result (H x W x 4); `out` may be a preallocated (e.g. page-locked) array."""
+        out = self._result_buffer(out)
         _check(self._lib.rg_get_hdr(self._h, _fptr(out), out.size))
         return out
 
-    def get_render_result(self) -> np.ndarray:
-        h, w = self._size()
-        out = np.empty((h, w, 4), np.float32)
+    def get_render_result(self, out: np.ndarray = None) -> np.ndarray:
+        """Tonemapped result (H x W x 4); `out` may be a preallocated array."""
+        out = self._result_buffer(out)
         _check(self._lib.rg_get_ldr(self._h, _fptr(out), out.size))
         return out
 
