@@ -98,6 +98,11 @@ class ClockSampler:
         for line in self.proc.stdout:
             self.lines.append(line.strip())
 
+    def mark(self):
+        """Start of the timed region: samples taken before it (nvidia-smi's own
+        start-up, which briefly disturbs the GPU, falls in the warm-up) are dropped."""
+        self.first = len(self.lines)
+
     def stop(self):
         if self.proc is None:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
@@ -108,7 +113,7 @@ class ClockSampler:
             self.proc.kill()
         mhz, mx, reasons = [], None, set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for ln in self.lines:
+        for ln in self.lines[getattr(self, "first", 0):]:
             parts = [x.strip() for x in ln.split(",")]
             if len(parts) < 9:
                 continue
@@ -600,13 +605,14 @@ def main():
     r.set_scene(scene)
     build_ms = r.stats()["build_ms"]
 
-    # ---- device-resident timing
+    # ---- device-resident timing (the clock sampler starts before the warm-up)
+    clock = ClockSampler(local if world == 1 else 0)
+    clock.start()
     for _ in range(args.warmup):
         r.render()
     if pg:
         pg.barrier()
-    clock = ClockSampler(local if world == 1 else 0)
-    clock.start()
+    clock.mark()
     dev_ms, samples, launches = 0.0, 0, 0
     for _ in range(args.steps):
         r.render()

@@ -90,7 +90,9 @@ typedef struct rg_settings {
   int32_t max_depth;          /* MAX_TRACE_DEPTH [32]                         */
   int32_t rr_depth;           /* MIN_RR_DEPTH [3]                             */
   int32_t light_pick_fix;     /* 1: weight NEE by the light count [0]         */
-  int32_t paths_per_wave;     /* wavefront size; 0 = automatic                */
+  int32_t paths_per_wave;     /* wavefront size; 0 = automatic: up to 64 Mi
+                               * paths (about 330 B of queues each), at most a
+                               * fifth of the free device memory             */
   int32_t bvh_bins;           /* SAH bins for the device build [32]           */
   int32_t bvh_width;          /* 8: compressed 8-wide BVH (default), 2: binary */
 } rg_settings;

@@ -989,10 +989,26 @@ static rg_status postProcess(rg_handle* h, bool restore) {
   return RG_OK;
 }
 
+// Automatic wave size: large waves amortise the few-ray tail of the last
+// bounces (measured on the 1080p 4M-triangle job: 8 Mi paths 239, 16 Mi 255,
+// 32 Mi 264, 64 Mi 269 Msamples/s); bounded by a fifth of the free memory.
+static long long wavePaths(const rg_settings& s) {
+  if (s.paths_per_wave > 0) return s.paths_per_wave;
+  constexpr long long kBytesPerPath = 330;  // ray / hit / path state and four shadow queues
+  long long cap = 64ll << 20;
+  size_t freeB = 0, totalB = 0;
+  if (cudaMemGetInfo(&freeB, &totalB) == cudaSuccess) {
+    const long long fit = (long long)(freeB / 5) / kBytesPerPath;
+    while (cap > (1ll << 20) && cap > fit) cap >>= 1;
+  }
+  cudaGetLastError();
+  return cap;
+}
+
 static rg_status runPass(rg_handle* h, const DevRender& R, int numPixels, const int* pixelList, int spp,
                          int& wavesDone, int totalWavesHint, bool profile, double* kernelMs) {
   if (numPixels <= 0 || spp <= 0) return RG_OK;
-  const long long cap = h->st.paths_per_wave > 0 ? h->st.paths_per_wave : (8ll << 20);
+  const long long cap = wavePaths(h->st);
   std::vector<DevSegment> sg;
   const int spw = numPixels >= cap ? 1 : (int)std::min<long long>(spp, std::max<long long>(1, cap / numPixels));
   const int pixChunk = (int)std::min<long long>(numPixels, cap);
@@ -1170,7 +1186,7 @@ rg_status rg_render(rg_handle* h) {
   rg_status rs = RG_OK;
   const int target = std::max(0, s.samples);
   if (!s.enable_adaptive_sampling) {
-    const long long cap = s.paths_per_wave > 0 ? s.paths_per_wave : (8ll << 20);
+    const long long cap = wavePaths(s);
     const int spw = N >= cap ? 1 : (int)std::min<long long>(std::max(1, target), std::max<long long>(1, cap / N));
     const int hint = (int)(((target + spw - 1) / std::max(1, spw)) * ((N + cap - 1) / cap));
     rs = runPass(h, R, N, nullptr, target, wavesDone, hint, profile, kms);

@@ -655,7 +655,7 @@ rg_status rg_server_autotune(const rg_settings* base, const rg_job_desc* probe, 
     return RG_OK;
   };
   // coordinate descent: wave size, then shade width, then traversal width
-  for (int ppw : {1 << 18, 1 << 19, 1 << 20, 1 << 21, 1 << 22, 1 << 23}) {
+  for (int ppw : {1 << 20, 1 << 21, 1 << 22, 1 << 23, 1 << 24, 1 << 25, 1 << 26}) {
     rg_server_config c = best;
     c.paths_per_wave = ppw;
     if (c.paths_per_wave != cfg->paths_per_wave && (rs = tryCfg(c)) != RG_OK) return rs;
