@@ -624,6 +624,8 @@ __global__ void __launch_bounds__(128) k_connect(const DevJob* __restrict__ jobs
 // Stack entries: node group (childBase, hits | imask << 8) or triangle group
 // (triBase | 0x80000000, triangle mask).
 constexpr int kRefillIdle = 8;     // refill once this many lanes are idle
+constexpr int kSharedStack = 8;    // traversal stack entries kept in shared memory (the rest in local)
+constexpr int kTraceBlock = 128;   // block size of the persistent traversal kernels
 constexpr int kTriVotes = 4;       // lanes with triangles needed to run a triangle step (swept: 2-4 best, 10 -1.6%)
 
 template <bool ANY, bool MULTI>
@@ -640,7 +642,19 @@ __device__ __forceinline__ void traverseWave8(const DevScene& S0, const DevJob* 
   int prim = -1, pid = 0;
   uint32_t gInner = 0, gImask = 0, tMask = 0;
   int gBase = 0, tBase = 0, sp = 0, steps = 0;
-  uint2 stack[kStack8];
+  // traversal stack: entries [0, kSharedStack) in shared memory, entry-major so a
+  // warp at one depth touches consecutive words; deeper entries in local memory
+  __shared__ uint2 sStack[kSharedStack > 0 ? kSharedStack : 1][kTraceBlock];
+  uint2 lStack[kStack8 - kSharedStack];
+  auto push = [&](uint2 e) {
+    if (sp < kSharedStack) sStack[sp][threadIdx.x] = e;
+    else lStack[sp - kSharedStack] = e;
+    sp++;
+  };
+  auto pop = [&]() -> uint2 {
+    --sp;
+    return sp < kSharedStack ? sStack[sp][threadIdx.x] : lStack[sp - kSharedStack];
+  };
   const float4* nodesP = nullptr;
   const float4* trisP = nullptr;
   int numNodes = 0;
@@ -707,7 +721,7 @@ __device__ __forceinline__ void traverseWave8(const DevScene& S0, const DevJob* 
         if (sp == 0) {
           result = 1;
         } else {
-          const uint2 e = stack[--sp];
+          const uint2 e = pop();
           if (e.x & 0x80000000u) {
             tBase = (int)(e.x & 0x7fffffffu);
             tMask = e.y;
@@ -749,7 +763,7 @@ __device__ __forceinline__ void traverseWave8(const DevScene& S0, const DevJob* 
         } else {
           // node step (pending triangles are postponed onto the stack)
           if (hasTri) {
-            if (sp < kStack8) stack[sp++] = make_uint2((uint32_t)tBase | 0x80000000u, tMask);
+            if (sp < kStack8) push(make_uint2((uint32_t)tBase | 0x80000000u, tMask));
             else atomicCAS(errP, 0, kErrStackOverflow);
             tMask = 0;
           }
@@ -758,7 +772,7 @@ __device__ __forceinline__ void traverseWave8(const DevScene& S0, const DevJob* 
           const int slot = pos ^ (int)oct;
           const int node = gBase + __popc(gImask & ((1u << slot) - 1u));
           if (gInner) {
-            if (sp < kStack8) stack[sp++] = make_uint2((uint32_t)gBase, gInner | (gImask << 8));
+            if (sp < kStack8) push(make_uint2((uint32_t)gBase, gInner | (gImask << 8)));
             else atomicCAS(errP, 0, kErrStackOverflow);
           }
           if (node >= numNodes || ++steps > kMaxTraversalSteps) {
@@ -1614,8 +1628,8 @@ void launchGenerate(const DevJob* jobs, const DevWave* W, const DevQueues& Q, in
 void launchExtend(const DevScene* single, const DevJob* jobs, int width, const DevQueues& Q, int iter, int grid,
                   cudaStream_t st) {
   if (width == 8) {
-    if (single) k_extend8<false><<<grid, 128, 0, st>>>(*single, jobs, Q, iter);
-    else k_extend8<true><<<grid, 128, 0, st>>>(DevScene{}, jobs, Q, iter);
+    if (single) k_extend8<false><<<grid, kTraceBlock, 0, st>>>(*single, jobs, Q, iter);
+    else k_extend8<true><<<grid, kTraceBlock, 0, st>>>(DevScene{}, jobs, Q, iter);
   } else {
     k_extend<<<grid, 128, 0, st>>>(jobs, Q, iter);
   }
@@ -1642,8 +1656,8 @@ void launchShade(const DevScene* single, const DevRender* singleR, const DevJob*
 void launchConnect(const DevScene* single, const DevJob* jobs, int width, const DevQueues& Q, int iter, int which,
                    int grid, cudaStream_t st) {
   if (width == 8) {
-    if (single) k_connect8<false><<<grid, 128, 0, st>>>(*single, jobs, Q, iter, which);
-    else k_connect8<true><<<grid, 128, 0, st>>>(DevScene{}, jobs, Q, iter, which);
+    if (single) k_connect8<false><<<grid, kTraceBlock, 0, st>>>(*single, jobs, Q, iter, which);
+    else k_connect8<true><<<grid, kTraceBlock, 0, st>>>(DevScene{}, jobs, Q, iter, which);
   } else {
     k_connect<<<grid, 128, 0, st>>>(jobs, Q, iter, which);
   }
