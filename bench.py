@@ -65,6 +65,19 @@ def parse():
     return a
 
 
+def aggregate(pg, dev_ms, samples):
+    """Whole-job figures over the replicas (one per GPU, no data exchange): the
+    slowest rank's device time and the samples of all ranks."""
+    if not pg:
+        return dev_ms, float(samples)
+    import torch
+    t = torch.tensor([float(dev_ms)], dtype=torch.float64)
+    pg.all_reduce(t, op=pg.ReduceOp.MAX)
+    c = torch.tensor([float(samples)], dtype=torch.float64)
+    pg.all_reduce(c, op=pg.ReduceOp.SUM)
+    return float(t.item()), float(c.item())
+
+
 def dist_env():
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -621,16 +634,7 @@ def main():
         samples += s["samples"]
         launches += s["kernel_launches"]
     clocks = clock.stop()
-    if pg:
-        import torch
-        t = torch.tensor([dev_ms], dtype=torch.float64)
-        pg.all_reduce(t, op=pg.ReduceOp.MAX)
-        dev_ms_max = float(t.item())
-        c = torch.tensor([float(samples)], dtype=torch.float64)
-        pg.all_reduce(c, op=pg.ReduceOp.SUM)
-        total_samples = float(c.item())
-    else:
-        dev_ms_max, total_samples = dev_ms, float(samples)
+    dev_ms_max, total_samples = aggregate(pg, dev_ms, samples)
     value = total_samples / (dev_ms_max * 1e-3) / 1e6
 
     # ---- end to end through the C ABI with host buffers: every step uploads the
