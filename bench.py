@@ -425,6 +425,10 @@ def run_learned(args):
 
 
 DENOISER_FLOPS_PER_PIXEL = 2 * 9 * (16 * 32 + 4 * 32 * 32 + 32 * 32)  # six 3x3 convolutions, padded widths
+# HBM bytes per pixel of one inference (BF16 NHWC activations, each read and written once):
+# layer 0 reads 16 channels (32 B) and writes 32 (64 B); layers 1-4 read and write 64 B;
+# the last layer reads 64 B, the noisy radiance (16 B) and writes the denoised pixel (16 B).
+DENOISER_BYTES_PER_PIXEL = (32 + 64) + 4 * (64 + 64) + (64 + 16 + 16)
 
 
 def measured_peak_bf16():
@@ -437,9 +441,12 @@ def measured_peak_bf16():
 
 def run_denoiser(args):
     """Learned denoiser on the tensor cores: device time of one inference at --res
-    (features, six BF16 tcgen05 convolutions, kernel application) and of one
-    training step (batch of 16 tracer-rendered 64 x 64 pairs: forward, backward,
-    Adam).  FLOPs count the convolutions' multiply-adds at their padded widths."""
+    (six BF16 tcgen05 convolutions, the last with the softmax and kernel
+    application fused) and of one training step (batch of 16 tracer-rendered
+    64 x 64 pairs: forward, backward, Adam).  The convolutions carry 144 FLOP
+    per HBM byte, under the B200's ridge point, so the roofline is HBM: bytes
+    per pixel (activations read and written once) over the device time; the
+    tensor-core rate is reported beside it."""
     import importlib
     import numpy as np
     sys.path.insert(0, ROOT)
@@ -459,7 +466,9 @@ def run_denoiser(args):
             times.append(d.timing()["apply_ms"])
     ms = float(np.median(times))
     tflops = DENOISER_FLOPS_PER_PIXEL * w * h / ms / 1e9
+    gbs = DENOISER_BYTES_PER_PIXEL * w * h / ms / 1e6
     peak, src = measured_peak_bf16()
+    hbm, hsrc = measured_peak_hbm()
     for ex in kt.make_examples(rg, 16, size=64, spp_lo=8, spp_hi=64):
         d.add_example(*ex)
     d.train(args.warmup, 16, 1e-6)
@@ -473,9 +482,11 @@ def run_denoiser(args):
         "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "bf16 (fp32 accumulation)",
         "data": "synthetic inputs (inference); tracer-rendered pairs (training)",
         "config": {"workload": f"denoiser inference {w}x{h}; training step batch 16 x 64x64", "mode": "denoiser"},
-        "roofline": {"bound": "tensor", "achieved": round(tflops, 1), "peak": peak, "unit": "TFLOP/s",
-                     "frac": round(tflops / peak, 4), "traffic": None, "peak_source": src,
-                     "flops_per_pixel": DENOISER_FLOPS_PER_PIXEL},
+        "roofline": {"bound": "hbm", "achieved": round(gbs, 1), "peak": hbm, "unit": "GB/s",
+                     "frac": round(gbs / hbm, 4), "traffic": None, "peak_source": hsrc,
+                     "bytes_per_pixel": DENOISER_BYTES_PER_PIXEL},
+        "tensor": {"achieved": round(tflops, 1), "peak": peak, "unit": "TFLOP/s", "frac": round(tflops / peak, 4),
+                   "peak_source": src, "flops_per_pixel": DENOISER_FLOPS_PER_PIXEL},
         "training": {"step_ms": round(step_ms, 3), "tflops": round(step_tflops, 1)},
     }
     print(json.dumps(line), flush=True)

@@ -78,6 +78,42 @@ __device__ __forceinline__ bool mbarWait(uint64_t* bar, uint32_t phase) {
   return false;
 }
 
+// 16-byte asynchronous global -> shared copy; with `valid` false nothing is
+// read and the 16 destination bytes are zero-filled.
+__device__ __forceinline__ void cpAsync16(uint32_t dst, const void* src, bool valid) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(dst), "l"(src), "r"(valid ? 16u : 0u)
+               : "memory");
+}
+__device__ __forceinline__ void cpAsyncCommit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+// Wait until at most N of this thread's committed copy groups are still in flight.
+template <int N>
+__device__ __forceinline__ void cpAsyncWait() {
+  asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
+}
+
+// The barrier expects `bytes` more transaction bytes in its current phase; this thread arrives.
+__device__ __forceinline__ void mbarArriveExpectTx(uint64_t* bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smemAddr(bar)), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ void mbarArrive(uint64_t* bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smemAddr(bar)) : "memory");
+}
+// Make initialised barriers visible to the asynchronous proxy (TMA, tensor cores).
+__device__ __forceinline__ void fenceBarrierInit() { asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory"); }
+
+// TMA tile load (no multicast) of a 4-D box at (c0, c1, c2, c3) into this CTA's
+// shared memory; completes `bytes` of transactions on `bar`.  c0 is the
+// innermost coordinate and must address a 16-byte boundary; the others may be
+// negative or past the end (those elements are zero-filled).
+__device__ __forceinline__ void tmaLoad4d(uint32_t dst, const void* tmap, int c0, int c1, int c2, int c3,
+                                          uint64_t* bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.4d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4, %5}], "
+      "[%6];" ::"r"(dst),
+      "l"(tmap), "r"(c0), "r"(c1), "r"(c2), "r"(c3), "r"(smemAddr(bar))
+      : "memory");
+}
+
 __device__ __forceinline__ void fenceProxyAsync() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
 __device__ __forceinline__ void fenceAfterSync() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
 __device__ __forceinline__ void fenceBeforeSync() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }

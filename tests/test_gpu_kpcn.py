@@ -59,6 +59,49 @@ def test_kpcn_forward_matches_oracle(rg):
     d.close()
 
 
+def test_kpcn_forward_matches_oracle_over_many_tiles(rg):
+    """300 rows of 4 column tiles (the last 36 pixels wide): strips of
+    several rows, so the ring of input rows wraps inside a strip while the
+    next row loads during the current row's MMAs and epilogue."""
+    d = rg.Denoiser(seed=4)
+    p = perturbed(d, 3)
+    d.params = p
+    noisy, normal, albedo, depth, ref = synth(1, 300, 420, 6)
+    got = d.apply(noisy[0], normal[0], albedo[0], depth[0])
+    f = ko.forward(p, ko.features(noisy, normal, albedo, depth), noisy)
+    np.testing.assert_allclose(got[..., :3], f["out"][0], rtol=2e-3, atol=2e-3)
+    d.close()
+
+
+def test_kpcn_gradients_match_oracle_over_many_tiles(rg):
+    d = rg.Denoiser(seed=6)
+    p = perturbed(d, 4)
+    d.params = p
+    noisy, normal, albedo, depth, ref = synth(2, 160, 300, 7)  # 960 row tiles per convolution
+    loss, g = d.gradients(noisy, normal, albedo, depth, ref)
+    lo, go = ko.backward(p, ko.features(noisy, normal, albedo, depth), noisy, ref)
+    assert loss == pytest.approx(lo, rel=1e-3)
+    x, y = g.astype(np.float64), go
+    assert x @ y / (np.linalg.norm(x) * np.linalg.norm(y)) > 0.999
+    d.close()
+
+
+def test_kpcn_gradients_match_oracle_with_several_strips_per_cta(rg):
+    """450 images of 8 x 8: more column tiles than resident convolution CTAs,
+    so each CTA convolves two or three strips in turn and its ring of input
+    rows wraps across strip boundaries (forward and backward data)."""
+    d = rg.Denoiser(seed=8)
+    p = perturbed(d, 5)
+    d.params = p
+    noisy, normal, albedo, depth, ref = synth(450, 8, 8, 9)
+    loss, g = d.gradients(noisy, normal, albedo, depth, ref)
+    lo, go = ko.backward(p, ko.features(noisy, normal, albedo, depth), noisy, ref)
+    assert loss == pytest.approx(lo, rel=1e-3)
+    x, y = g.astype(np.float64), go
+    assert x @ y / (np.linalg.norm(x) * np.linalg.norm(y)) > 0.999
+    d.close()
+
+
 def test_kpcn_gradients_match_oracle(rg):
     d = rg.Denoiser(seed=5)
     p = perturbed(d, 2)
