@@ -195,20 +195,21 @@ __global__ void k_features(int P, const float4* __restrict__ noisy, const T* __r
 // Strip-pipelined implicit GEMM for the forward and backward-data
 // convolutions.  A CTA owns strips of S image rows x 128 columns; one output
 // row of a strip (128 pixels) is one M = 128 tile.  Input rows live in a ring
-// of kRing row slots in shared memory, each a set of planes of 16-byte slots
-// (8 channels of one pixel), one plane per 8-channel chunk, covering pixels
-// x0 - 1 .. x0 + 128.  The A operand of tap (dy, dx) is a descriptor into the
-// ring slot of input row y + dy, shifted by 1 + dx pixel slots: 8 consecutive
-// pixels are a core matrix (SBO = 128 bytes) and the second chunk of an MMA
-// step is the next plane (LBO = plane stride) -- no im2col copy, and each
-// input row is loaded once per strip (plus two halo rows).
+// of kRing row slots in shared memory, each holding pixels x0 - 1 .. x0 + 128
+// pixel-major (CIN x 2 bytes per pixel) in the 32- or 64-byte swizzled K-major
+// layout: one TMA box of all channels x 130 pixels per row (rows and columns
+// outside the image are zero-filled by the copy).  The A operand of tap
+// (dy, dx) is a descriptor into the slot of input row y + dy, its start moved
+// by 1 + dx pixels (and by 32 bytes for the second K step of 32 channels) --
+// no im2col copy, and each input row is loaded once per strip (plus two halo
+// rows).  One wide box per row matters: a box of 16-byte rows (one 8-channel
+// chunk) costs the copy engine about as much per row as a box of 64-byte rows.
 //
 // Roles (160 threads):
-//  * warp 4, one thread: the producer.  It loads input rows into the ring with
-//    TMA (a 4-D tensor map over [B][H][W][C]; rows and columns outside the
-//    image are zero-filled by the copy), two rows ahead of the tensor cores,
-//    and issues the 9 taps x C / 16 MMAs of each output row into one of two
-//    32-column TMEM accumulators, committed to tmemFull[row & 1];
+//  * warp 4, one thread: the producer.  It loads input rows two ahead of the
+//    tensor cores and issues the 9 taps x CIN / 16 MMAs of each output row
+//    into one of two 32-column TMEM accumulators, committed to
+//    tmemFull[row & 1];
 //  * warps 0-3: the epilogue.  Each reads its 32 accumulator lanes, frees the
 //    accumulator (tmemEmpty) and writes bias + ReLU in BF16, the FP32 logits
 //    (LAST), the denoised pixel (LAST and APPLY: softmax of the logits and the
@@ -218,13 +219,14 @@ __global__ void k_features(int P, const float4* __restrict__ noisy, const T* __r
 // bounded; a wait that runs out sets the error word and the CTA drains its
 // outstanding copies and MMAs before it frees the tensor memory.
 constexpr int kRing = 6;                // input row slots: 3 in use, 1 landing, 2 loading ahead
-constexpr int kSlots = 130;             // pixels per plane: x0 - 1 .. x0 + 128
-constexpr int kPlane = 17 * 128;        // bytes per plane (>= 130 x 16, 128-byte aligned for TMA)
-constexpr int kRowBox = kSlots * 16;    // bytes one TMA box (8 channels x 130 pixels) writes
+constexpr int kSlots = 130;             // pixels per slot: x0 - 1 .. x0 + 128
 constexpr int kConvThreads = 160;
 
+// Bytes per ring slot (1024-aligned: the swizzle follows the address).
 template <int CIN>
-__host__ __device__ constexpr size_t ringBytes() { return (size_t)kRing * (CIN / 8) * kPlane; }
+__host__ __device__ constexpr int slotBytes() { return (kSlots * CIN * 2 + 1023) / 1024 * 1024; }
+template <int CIN>
+__host__ __device__ constexpr size_t ringBytes() { return (size_t)kRing * slotBytes<CIN>(); }
 template <int CIN>
 __host__ __device__ constexpr size_t rowSmem() { return ringBytes<CIN>() + (size_t)kC * 9 * CIN * 2; }
 
@@ -274,6 +276,8 @@ __global__ void __launch_bounds__(kConvThreads) k_convStrip(const __grid_constan
     if (lane == 0) {
       // ------------------------------------------------------------ producer
       const uint32_t idesc = tc::instrDescBf16(128, kC);
+      const uint64_t aDesc0 = CIN == 32 ? tc::smemDescSw64(0) : tc::smemDescSw32(0);
+      const uint64_t bDesc0 = tc::smemDesc(bBase, 128, KC * 128);
       int r = 0;      // output rows issued
       int uNext = 0;  // next input row (CTA-local index) to load
       int uBase = 0;  // index of the current strip's first input row
@@ -290,27 +294,28 @@ __global__ void __launch_bounds__(kConvThreads) k_convStrip(const __grid_constan
           if (r >= 2 && !(ok = tc::mbarWait(&tmemEmpty[r & 1], ((r - 2) >> 1) & 1))) break;
           for (const int last = min(t + kRing - 2, uBase + n + 1); uNext <= last; ++uNext) {
             const int slot = uNext % kRing, yy = y0 - 1 + (uNext - uBase);
-            tc::mbarArriveExpectTx(&full[slot], (uint32_t)(CC * kRowBox));
-            for (int q = 0; q < CC; ++q)
-              tc::tmaLoad4d(ringBase + (uint32_t)((slot * CC + q) * kPlane), &xmap, q * 8, x0 - 1, yy, b, &full[slot]);
+            tc::mbarArriveExpectTx(&full[slot], (uint32_t)(kSlots * CIN * 2));
+            tc::tmaLoad4d(ringBase + (uint32_t)(slot * slotBytes<CIN>()), &xmap, 0, x0 - 1, yy, b, &full[slot]);
           }
-          for (int i = 0; i < 3 && ok; ++i) ok = tc::mbarWait(&full[(t + i) % kRing], ((t + i) / kRing) & 1);
+          for (int i = j == 0 ? 0 : 2; i < 3 && ok; ++i)  // rows t, t + 1 were waited for by row r - 1
+            ok = tc::mbarWait(&full[(t + i) % kRing], ((t + i) / kRing) & 1);
           if (!ok) break;
           tc::fenceAfterSync();
+          // The issue loop is this thread's whole per-row cost, so the descriptors are a
+          // fixed template plus (address >> 4) in the start field, the tap and chunk
+          // offsets folded at compile time.
           const uint32_t acc = tmem + (uint32_t)((r & 1) * 32);
+          uint32_t rowStart[3];  // start field of input rows t, t + 1, t + 2
+#pragma unroll
+          for (int i = 0; i < 3; ++i) rowStart[i] = (ringBase + (uint32_t)(((t + i) % kRing) * slotBytes<CIN>())) >> 4;
+#pragma unroll
           for (int tap = 0; tap < 9; ++tap) {
-            int dy = tap / 3 - 1, dx = tap % 3 - 1;
-            if (TRANSPOSED) {  // gradient gathered at p - offset
-              dy = -dy;
-              dx = -dx;
-            }
-            const uint32_t slotBase = ringBase + (uint32_t)(((t + 1 + dy) % kRing) * CC * kPlane + (1 + dx) * 16);
-            for (int k = 0; k < CC / 2; ++k) {
-              const uint32_t aStart = slotBase + (uint32_t)(2 * k * kPlane);
-              const uint32_t bStart = bBase + (uint32_t)((tap * CC + 2 * k) * 128);
-              tc::mmaBf16(acc, tc::smemDesc(aStart, kPlane, 128), tc::smemDesc(bStart, 128, KC * 128), idesc,
-                          tap > 0 || k > 0);
-            }
+            // gradient gathered at p - offset for the data gradient
+            const int dy = TRANSPOSED ? 1 - tap / 3 : tap / 3 - 1, dx = TRANSPOSED ? 1 - tap % 3 : tap % 3 - 1;
+#pragma unroll
+            for (int k = 0; k < CC / 2; ++k)
+              tc::mmaBf16(acc, aDesc0 + rowStart[dy + 1] + (uint32_t)(((1 + dx) * CIN * 2 + k * 32) >> 4),
+                          bDesc0 + (uint32_t)(((tap * CC + 2 * k) * 128) >> 4), idesc, tap > 0 || k > 0);
           }
           tc::commit(&tmemFull[r & 1]);
         }
@@ -754,18 +759,21 @@ PFN_cuTensorMapEncodeTiled_v12000 tensorMapEncoder() {
   return fn;
 }
 
-// Tensor map of a BF16 NHWC activation [B][H][W][C]: boxes of 8 channels x 130
-// pixels of one row, zero fill outside the tensor.
+// Tensor map of a BF16 NHWC activation [B][H][W][C], C = 16 or 32: boxes of all
+// channels x 130 pixels of one row (32- / 64-byte swizzle), zero fill outside
+// the tensor.
 bool rowMap(CUtensorMap& m, const __nv_bfloat16* X, int B, int H, int W, int C) {
   const PFN_cuTensorMapEncodeTiled_v12000 enc = tensorMapEncoder();
   if (!enc) return false;
   const cuuint64_t dims[4] = {(cuuint64_t)C, (cuuint64_t)W, (cuuint64_t)H, (cuuint64_t)B};
   const cuuint64_t strides[3] = {(cuuint64_t)C * 2, (cuuint64_t)W * C * 2, (cuuint64_t)H * W * C * 2};
-  const cuuint32_t box[4] = {8, (cuuint32_t)kSlots, 1, 1};
+  // one box of all channels per row, with the swizzle the convolution's descriptors read
+  if (C != 16 && C != 32) return false;
+  const cuuint32_t box[4] = {(cuuint32_t)C, (cuuint32_t)kSlots, 1, 1};
   const cuuint32_t elemStrides[4] = {1, 1, 1, 1};
   return enc(&m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 4, const_cast<__nv_bfloat16*>(X), dims, strides, box, elemStrides,
-             CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
-             CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+             CU_TENSOR_MAP_INTERLEAVE_NONE, C == 32 ? CU_TENSOR_MAP_SWIZZLE_64B : CU_TENSOR_MAP_SWIZZLE_32B,
+             CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
 
 // Strip height S and grid for B images of H rows x ceil(W / 128) column tiles

@@ -37,6 +37,34 @@ __device__ __forceinline__ uint64_t smemDesc(uint32_t addr, uint32_t lbo, uint32
   return d;                 // base offset 0, no swizzle
 }
 
+// K-major operand in the 64-byte swizzled layout TMA writes with a 64-byte
+// swizzle: rows of 64 bytes, 8-row groups 512 bytes apart (SBO), and the
+// 16-byte chunk c of row r stored at chunk c ^ ((r >> 1) & 3).  The swizzle
+// follows the shared-memory address, so a start moved by whole rows or by a
+// 32-byte K step within the row still reads the data TMA placed (the buffer is
+// 1024-byte aligned).
+__device__ __forceinline__ uint64_t smemDescSw64(uint32_t addr) {
+  uint64_t d = 0;
+  d |= (uint64_t)((addr >> 4) & 0x3FFFu);
+  d |= (uint64_t)1u << 16;           // leading byte offset: unused for a swizzled K-major operand
+  d |= (uint64_t)(512u >> 4) << 32;  // 8 rows x 64 bytes
+  d |= (uint64_t)1u << 46;           // descriptor version for this architecture
+  d |= (uint64_t)4u << 61;           // layout type: 64-byte swizzle
+  return d;
+}
+
+// The same for rows of 32 bytes (16 BF16 channels) in the 32-byte swizzled
+// layout: 8-row groups 256 bytes apart, chunk c of row r at c ^ ((r >> 2) & 1).
+__device__ __forceinline__ uint64_t smemDescSw32(uint32_t addr) {
+  uint64_t d = 0;
+  d |= (uint64_t)((addr >> 4) & 0x3FFFu);
+  d |= (uint64_t)1u << 16;           // leading byte offset: unused for a swizzled K-major operand
+  d |= (uint64_t)(256u >> 4) << 32;  // 8 rows x 32 bytes
+  d |= (uint64_t)1u << 46;           // descriptor version for this architecture
+  d |= (uint64_t)6u << 61;           // layout type: 32-byte swizzle
+  return d;
+}
+
 __host__ __device__ constexpr uint32_t instrDescBf16(int M, int N) {
   return (1u << 4)                       // FP32 accumulator
          | (1u << 7)                     // A: BF16
