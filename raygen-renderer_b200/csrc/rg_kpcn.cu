@@ -136,10 +136,8 @@ __device__ __forceinline__ int clampNeighbor(int p, int dy, int dx, int H, int W
   return (b * H + yy) * W + xx;
 }
 
-// Softmax of the 25 logits w (replaced by the kernel weights) and the 5 x 5
-// kernel applied to the noisy radiance around pixel p (clamp to edge).
-__device__ __forceinline__ void softmaxApply(float (&w)[kKP], int p, int H, int W, const float4* __restrict__ noisy,
-                                             float& o0, float& o1, float& o2) {
+// Softmax of the 25 logits w, in place: the 5 x 5 kernel weights.
+__device__ __forceinline__ void softmax25(float (&w)[kKP]) {
   float mx = -3.0e38f;
 #pragma unroll
   for (int j = 0; j < kKP; ++j) mx = fmaxf(mx, w[j]);
@@ -150,10 +148,18 @@ __device__ __forceinline__ void softmaxApply(float (&w)[kKP], int p, int H, int 
     sum += w[j];
   }
   const float inv = 1.0f / sum;
+#pragma unroll
+  for (int j = 0; j < kKP; ++j) w[j] *= inv;
+}
+
+// Softmax of the 25 logits w (replaced by the kernel weights) and the 5 x 5
+// kernel applied to the noisy radiance around pixel p (clamp to edge).
+__device__ __forceinline__ void softmaxApply(float (&w)[kKP], int p, int H, int W, const float4* __restrict__ noisy,
+                                             float& o0, float& o1, float& o2) {
+  softmax25(w);
   o0 = o1 = o2 = 0.0f;
 #pragma unroll
   for (int j = 0; j < kKP; ++j) {
-    w[j] *= inv;
     const float4 c = noisy[clampNeighbor(p, j / 5 - 2, j % 5 - 2, H, W)];
     o0 += w[j] * c.x;
     o1 += w[j] * c.y;
@@ -661,7 +667,6 @@ struct KpcnNet {
   std::mutex mu;  // one user of the work buffers at a time (renderers, servers, API calls)
   cudaStream_t st = nullptr;
   int numSMs = 148;
-  int stripPerSm16 = 1, stripPerSm32 = 1;  // resident strip-convolution CTAs per SM (16- / 32-channel input)
   bool mapFailed = false;                  // a convolution's tensor map could not be encoded
   DevBuf<float> params, grad, m, v;
   DevBuf<__nv_bfloat16> wf[kLayers], wt[kLayers];
@@ -802,8 +807,9 @@ void launchConv(KpcnNet& n, int B, int H, int W, const __nv_bfloat16* X, const _
     n.mapFailed = true;
     return;
   }
+  static const int perSm = stripResidency(k_convStrip<CIN, LAST, TRANSPOSED, APPLY>, rowSmem<CIN>());
   int grid = 1, S = 1;
-  stripPlan(B, H, W, n.numSMs * (CIN == 16 ? n.stripPerSm16 : n.stripPerSm32), grid, S);
+  stripPlan(B, H, W, n.numSMs * perSm, grid, S);
   k_convStrip<CIN, LAST, TRANSPOSED, APPLY><<<grid, kConvThreads, rowSmem<CIN>(), n.st>>>(m, B, H, W, S, Wk, bias, Xin,
                                                                                          Y, Z, noisy, out, n.err.p);
 }
@@ -905,11 +911,6 @@ bool initNet(KpcnNet& n, uint32_t seed) {
   setSmem(k_convStrip<32, true, false, false>, rowSmem<32>());
   setSmem(k_convStrip<32, true, false, true>, rowSmem<32>());
   setSmem(k_convStrip<32, false, true, false>, rowSmem<32>());
-  n.stripPerSm16 = stripResidency(k_convStrip<16, false, false, false>, rowSmem<16>());
-  n.stripPerSm32 = std::min({stripResidency(k_convStrip<32, false, false, false>, rowSmem<32>()),
-                             stripResidency(k_convStrip<32, true, false, false>, rowSmem<32>()),
-                             stripResidency(k_convStrip<32, true, false, true>, rowSmem<32>()),
-                             stripResidency(k_convStrip<32, false, true, false>, rowSmem<32>())});
   packWeights(n);
   return cudaStreamSynchronize(n.st) == cudaSuccess;
 }
