@@ -1005,8 +1005,13 @@ static long long wavePaths(const rg_settings& s) {
   return cap;
 }
 
+// `start` is recorded on the stream right before the render's first wave (once
+// per render, `started`), after this pass's host-side set-up: the render's
+// device time then covers the device work and the waits between passes, not
+// the host's preparation of the first one.
 static rg_status runPass(rg_handle* h, const DevRender& R, int numPixels, const int* pixelList, int spp,
-                         int& wavesDone, int totalWavesHint, bool profile, double* kernelMs) {
+                         int& wavesDone, int totalWavesHint, bool profile, double* kernelMs, cudaEvent_t start,
+                         bool& started) {
   if (numPixels <= 0 || spp <= 0) return RG_OK;
   const long long cap = wavePaths(h->st);
   std::vector<DevSegment> sg;
@@ -1097,6 +1102,10 @@ static rg_status runPass(rg_handle* h, const DevRender& R, int numPixels, const 
   }
   for (size_t k = 0; k < ws.size(); k++) {
     if (h->cancel.load()) return RG_ERR_CANCELLED;
+    if (!started) {
+      cudaEventRecord(start, h->stream);
+      started = true;
+    }
     if (profile) {
       k_selectWave<<<1, 1, 0, h->stream>>>(h->waves.p, h->curWave.p, slot);
       enqueueWave(h, R, Q, h->jobsDev.p, slot, true, &ev);
@@ -1180,7 +1189,7 @@ rg_status rg_render(rg_handle* h) {
   cudaEventCreate(&t0);
   cudaEventCreate(&t1);
   cudaEventCreate(&t2);
-  cudaEventRecord(t0, st);
+  bool started = false;  // t0 is recorded by runPass right before the first wave
   int wavesDone = 0;
   double kms[3] = {0, 0, 0};
   rg_status rs = RG_OK;
@@ -1189,12 +1198,12 @@ rg_status rg_render(rg_handle* h) {
     const long long cap = wavePaths(s);
     const int spw = N >= cap ? 1 : (int)std::min<long long>(std::max(1, target), std::max<long long>(1, cap / N));
     const int hint = (int)(((target + spw - 1) / std::max(1, spw)) * ((N + cap - 1) / cap));
-    rs = runPass(h, R, N, nullptr, target, wavesDone, hint, profile, kms);
+    rs = runPass(h, R, N, nullptr, target, wavesDone, hint, profile, kms, t0, started);
   } else {
     // renderAdaptive (rayrenderer.cpp:1162-1252): base pass, then refinement passes
     const int base = std::max(1, s.adaptive_base_samples);
     int spent = std::min(base, target);
-    rs = runPass(h, R, N, nullptr, spent, wavesDone, 0, profile, kms);
+    rs = runPass(h, R, N, nullptr, spent, wavesDone, 0, profile, kms, t0, started);
     while (rs == RG_OK && spent < target) {
       RG_CUDA_CHECK(cudaMemsetAsync(h->listCount.p, 0, sizeof(int), st));
       if (s.adaptive_mode == RG_ADAPTIVE_TILE)
@@ -1208,10 +1217,11 @@ rg_status rg_render(rg_handle* h) {
       RG_CUDA_CHECK(cudaStreamSynchronize(st));
       if (active == 0) break;
       const int passCount = std::min(base, target - spent);
-      rs = runPass(h, R, active, h->pixelList.p, passCount, wavesDone, 0, profile, kms);
+      rs = runPass(h, R, active, h->pixelList.p, passCount, wavesDone, 0, profile, kms, t0, started);
       spent += passCount;
     }
   }
+  if (!started) cudaEventRecord(t0, st);  // no wave ran (0 samples)
   cudaEventRecord(t1, st);
   if (rs != RG_OK) {
     cudaStreamSynchronize(st);
