@@ -852,8 +852,48 @@ __global__ void __launch_bounds__(256) k_shade(DevScene S0, DevRender R0, const 
   const int count = Q.counters[iter * kCountersPerIter + C_RAYS];
   const int inB = iter & 1, outB = (iter + 1) & 1;
   const int stride = gridDim.x * blockDim.x;
-  const int rounded = ((count + 31) / 32) * 32;
-  for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < rounded; q += stride) {
+  // Each block iteration takes 256 consecutive queue entries and shades them in
+  // the order of the hit's material (a counting sort in shared memory; misses
+  // last), so that a warp mostly runs one lobe: incoherent bounces otherwise
+  // leave a third of the lanes active and the kernel waiting on instruction fetch.
+  constexpr int kBins = 64;
+  __shared__ int sBin[kBins];
+  __shared__ int sOrder[256];
+  for (int base = blockIdx.x * blockDim.x; base < count; base += stride) {
+    int q = base + threadIdx.x;
+    {
+      int key = kBins - 1;
+      if (q < count) {
+        const int prim0 = __float_as_int(Q.hits[q].w);
+        if (prim0 >= 0) {
+          const int slot0 = MULTI ? __float_as_int(Q.rayD[inB][q].w) : 0;
+          const DevScene& Sk = MULTI ? jobs[slot0].S : S0;
+          const int mesh0 = __float_as_int(__ldg(&Sk.triVerts[(size_t)prim0 * 3].w));
+          const unsigned mat0 = (unsigned)Sk.objMat[Sk.meshObj[mesh0]];
+          key = (int)((mat0 + (MULTI ? (unsigned)slot0 * 17u : 0u)) % (unsigned)(kBins - 1));
+        }
+      }
+      __syncthreads();  // the previous iteration has read sBin and sOrder
+      if (threadIdx.x < kBins) sBin[threadIdx.x] = 0;
+      __syncthreads();
+      const int rank = atomicAdd(&sBin[key], 1);
+      __syncthreads();
+      if (threadIdx.x < 32) {  // exclusive scan of the bins, two per lane
+        const int a = sBin[2 * threadIdx.x], b = sBin[2 * threadIdx.x + 1];
+        int incl = a + b;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+          const int t = __shfl_up_sync(0xffffffffu, incl, o);
+          if ((int)threadIdx.x >= o) incl += t;
+        }
+        sBin[2 * threadIdx.x] = incl - a - b;
+        sBin[2 * threadIdx.x + 1] = incl - b;
+      }
+      __syncthreads();
+      sOrder[sBin[key] + rank] = q;
+      __syncthreads();
+      q = sOrder[threadIdx.x];
+    }
     const bool valid = q < count;
     Shadow shA, shB, shE, shV;  // area light / point light / environment / volume light
     shA.on = false;
