@@ -852,47 +852,58 @@ __global__ void __launch_bounds__(256) k_shade(DevScene S0, DevRender R0, const 
   const int count = Q.counters[iter * kCountersPerIter + C_RAYS];
   const int inB = iter & 1, outB = (iter + 1) & 1;
   const int stride = gridDim.x * blockDim.x;
-  // Each block iteration takes 256 consecutive queue entries and shades them in
-  // the order of the hit's material (a counting sort in shared memory; misses
-  // last), so that a warp mostly runs one lobe: incoherent bounces otherwise
-  // leave a third of the lanes active and the kernel waiting on instruction fetch.
-  constexpr int kBins = 64;
-  __shared__ int sBin[kBins];
-  __shared__ int sOrder[256];
-  for (int base = blockIdx.x * blockDim.x; base < count; base += stride) {
+  // Each block iteration takes 256 consecutive queue entries and shades them
+  // grouped by the branch their hit takes (a counting sort in shared memory), so
+  // that a warp mostly runs one lobe: incoherent bounces otherwise leave a third
+  // of the lanes active and the kernel waiting on instruction fetch.  Classes:
+  // 0 emitter, 1 diffuse, 2 rough glossy, 3 mirror, 4 refraction,
+  // 5 transparency, 6 mixed lobes, 7 miss.  The bins and the order are double
+  // buffered by iteration, which leaves three block barriers per iteration.
+  constexpr int kBins = 8;
+  __shared__ int sBin[2][kBins];
+  __shared__ int sOrder[2][256];
+  if (threadIdx.x < 2 * kBins) sBin[threadIdx.x / kBins][threadIdx.x % kBins] = 0;
+  __syncthreads();
+  int buf = 0;
+  for (int base = blockIdx.x * blockDim.x; base < count; base += stride, buf ^= 1) {
     int q = base + threadIdx.x;
     {
       int key = kBins - 1;
       if (q < count) {
         const int prim0 = __float_as_int(Q.hits[q].w);
         if (prim0 >= 0) {
-          const int slot0 = MULTI ? __float_as_int(Q.rayD[inB][q].w) : 0;
-          const DevScene& Sk = MULTI ? jobs[slot0].S : S0;
+          const DevScene& Sk = MULTI ? jobs[__float_as_int(Q.rayD[inB][q].w)].S : S0;
           const int mesh0 = __float_as_int(__ldg(&Sk.triVerts[(size_t)prim0 * 3].w));
-          const unsigned mat0 = (unsigned)Sk.objMat[Sk.meshObj[mesh0]];
-          key = (int)((mat0 + (MULTI ? (unsigned)slot0 * 17u : 0u)) % (unsigned)(kBins - 1));
+          const DevMaterial& mk = Sk.mats[Sk.objMat[Sk.meshObj[mesh0]]];
+          const float gl = mk.glossy, rf = mk.refraction;
+          if (mk.emission > 0.0f) key = 0;
+          else if (mk.transparency > 0.001f) key = 5;
+          else if (gl <= 0.00001f && rf <= 0.00001f) key = 1;
+          else if (rf <= 0.00001f && gl >= 1.0f - 0.00001f) key = mk.roughness < 1e-3f ? 3 : 2;
+          else if (gl <= 0.00001f && rf >= 1.0f - 0.00001f) key = 4;
+          else key = 6;
         }
       }
-      __syncthreads();  // the previous iteration has read sBin and sOrder
-      if (threadIdx.x < kBins) sBin[threadIdx.x] = 0;
+      // sBin[buf] was zeroed, and this buffer's order last read, before the previous
+      // iteration's second barrier
+      const int rank = atomicAdd(&sBin[buf][key], 1);
       __syncthreads();
-      const int rank = atomicAdd(&sBin[key], 1);
-      __syncthreads();
-      if (threadIdx.x < 32) {  // exclusive scan of the bins, two per lane
-        const int a = sBin[2 * threadIdx.x], b = sBin[2 * threadIdx.x + 1];
-        int incl = a + b;
+      if (threadIdx.x < 32) {  // exclusive scan of the bins
+        const int c = threadIdx.x < kBins ? sBin[buf][threadIdx.x] : 0;
+        int incl = c;
 #pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {
+        for (int o = 1; o < kBins; o <<= 1) {
           const int t = __shfl_up_sync(0xffffffffu, incl, o);
           if ((int)threadIdx.x >= o) incl += t;
         }
-        sBin[2 * threadIdx.x] = incl - a - b;
-        sBin[2 * threadIdx.x + 1] = incl - b;
+        if (threadIdx.x < kBins) sBin[buf][threadIdx.x] = incl - c;
+      } else if (threadIdx.x < 32 + kBins) {
+        sBin[buf ^ 1][threadIdx.x - 32] = 0;  // every thread is past the previous iteration's reads
       }
       __syncthreads();
-      sOrder[sBin[key] + rank] = q;
+      sOrder[buf][sBin[buf][key] + rank] = q;
       __syncthreads();
-      q = sOrder[threadIdx.x];
+      q = sOrder[buf][threadIdx.x];
     }
     const bool valid = q < count;
     Shadow shA, shB, shE, shV;  // area light / point light / environment / volume light
