@@ -569,15 +569,49 @@ __global__ void k_head(int B, int H, int W, const float* __restrict__ Z, const f
 }
 
 // Adam (Kingma & Ba 2015) on the FP32 master parameters.
+// Adam; the step number t = state[1] + 1 is read on the device so that a
+// captured training step can be replayed.
 __global__ void k_adam(int n, float* __restrict__ p, const float* __restrict__ g, float* __restrict__ m,
-                       float* __restrict__ v, float lr, float b1, float b2, float c1, float c2, float eps) {
+                       float* __restrict__ v, float lr, float b1, float b2, const int* __restrict__ state, float eps) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
+  const float t = (float)(state[1] + 1);
+  const float c1 = 1.0f - powf(b1, t), c2 = 1.0f - powf(b2, t);
   const float gi = g[i];
   const float mi = b1 * m[i] + (1.0f - b1) * gi, vi = b2 * v[i] + (1.0f - b2) * gi * gi;
   m[i] = mi;
   v[i] = vi;
   p[i] -= lr * (mi / c1) / (sqrtf(vi / c2) + eps);
+}
+
+// One training example on the device: features, noisy radiance, reference.
+struct ExampleRef {
+  const __nv_bfloat16* x;
+  const float4* noisy;
+  const float4* ref;
+};
+
+// The batch of training step state[0]: example picks[step * B + b] into slot b.
+__global__ void k_gatherBatch(int B, int Pi, const int* __restrict__ picks, const int* __restrict__ state,
+                              const ExampleRef* __restrict__ ex, __nv_bfloat16* __restrict__ X0,
+                              float4* __restrict__ noisy, float4* __restrict__ ref) {
+  const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= (size_t)B * Pi) return;
+  const int b = (int)(i / Pi), p = (int)(i % Pi);
+  const ExampleRef e = ex[picks[state[0] * B + b]];
+  const uint4* xs = reinterpret_cast<const uint4*>(e.x + (size_t)p * 16);
+  uint4* xd = reinterpret_cast<uint4*>(X0 + i * 16);
+  xd[0] = xs[0];
+  xd[1] = xs[1];
+  noisy[i] = e.noisy[p];
+  ref[i] = e.ref[p];
+}
+
+// End of a training step: its loss into the history, next step, one more Adam step.
+__global__ void k_stepEnd(int* __restrict__ state, const float* __restrict__ loss, float* __restrict__ hist) {
+  hist[state[0]] = *loss;
+  state[0]++;
+  state[1]++;
 }
 
 // Master FP32 weights -> BF16 forward layout [co][(t, ci)] and the transposed
@@ -670,13 +704,23 @@ struct KpcnNet {
   bool mapFailed = false;                  // a convolution's tensor map could not be encoded
   DevBuf<float> params, grad, m, v;
   DevBuf<__nv_bfloat16> wf[kLayers], wt[kLayers];
-  int adamStep = 0;
   float lastApplyMs = 0.0f, lastStepMs = 0.0f;  // device time of the last apply / mean training step
   std::mt19937 rng;
+  int perSm[5] = {1, 1, 1, 1, 1};  // resident strip-convolution CTAs per SM, by kernel variant (convVariant)
   // training examples (all W x H)
   int dsW = 0, dsH = 0, dsN = 0;
   std::vector<__nv_bfloat16*> exX;
   std::vector<float4*> exNoisy, exRef;
+  // A training step is captured once and replayed as a CUDA graph; what changes
+  // between steps lives on the device: state[0] = step of the current train()
+  // call, state[1] = Adam steps taken; the example picks of every step and the
+  // loss history of the call.
+  DevBuf<int> state, picks;
+  DevBuf<float> lossHist;
+  DevBuf<ExampleRef> exRefs;
+  bool exDirty = true;
+  cudaGraphExec_t trainGraph = nullptr;
+  std::string trainKey;
   // work buffers for P pixels
   size_t cap = 0;
   DevBuf<__nv_bfloat16> X0, act[kLayers - 1], gA, gB;
@@ -684,6 +728,7 @@ struct KpcnNet {
   DevBuf<float4> noisy, ref, out;
   DevBuf<int> err;
   ~KpcnNet() {
+    if (trainGraph) cudaGraphExecDestroy(trainGraph);
     for (auto* p : exX) cudaFree(p);
     for (auto* p : exNoisy) cudaFree(p);
     for (auto* p : exRef) cudaFree(p);
@@ -798,6 +843,11 @@ void stripPlan(int B, int H, int W, int slots, int& grid, int& S) {
   grid = (int)std::min<long>(tiles * ((H + S - 1) / S), slots);
 }
 
+// Index of a strip-convolution variant in KpcnNet::perSm.
+constexpr int convVariant(int cin, bool last, bool transposed, bool apply) {
+  return cin == 16 ? 0 : transposed ? 4 : !last ? 1 : apply ? 3 : 2;
+}
+
 template <int CIN, bool LAST, bool TRANSPOSED, bool APPLY = false>
 void launchConv(KpcnNet& n, int B, int H, int W, const __nv_bfloat16* X, const __nv_bfloat16* Wk, const float* bias,
                 const __nv_bfloat16* Xin, __nv_bfloat16* Y, float* Z, const float4* noisy = nullptr,
@@ -807,9 +857,8 @@ void launchConv(KpcnNet& n, int B, int H, int W, const __nv_bfloat16* X, const _
     n.mapFailed = true;
     return;
   }
-  static const int perSm = stripResidency(k_convStrip<CIN, LAST, TRANSPOSED, APPLY>, rowSmem<CIN>());
   int grid = 1, S = 1;
-  stripPlan(B, H, W, n.numSMs * perSm, grid, S);
+  stripPlan(B, H, W, n.numSMs * n.perSm[convVariant(CIN, LAST, TRANSPOSED, APPLY)], grid, S);
   k_convStrip<CIN, LAST, TRANSPOSED, APPLY><<<grid, kConvThreads, rowSmem<CIN>(), n.st>>>(m, B, H, W, S, Wk, bias, Xin,
                                                                                          Y, Z, noisy, out, n.err.p);
 }
@@ -911,6 +960,12 @@ bool initNet(KpcnNet& n, uint32_t seed) {
   setSmem(k_convStrip<32, true, false, false>, rowSmem<32>());
   setSmem(k_convStrip<32, true, false, true>, rowSmem<32>());
   setSmem(k_convStrip<32, false, true, false>, rowSmem<32>());
+  n.perSm[convVariant(16, false, false, false)] = stripResidency(k_convStrip<16, false, false, false>, rowSmem<16>());
+  n.perSm[convVariant(32, false, false, false)] = stripResidency(k_convStrip<32, false, false, false>, rowSmem<32>());
+  n.perSm[convVariant(32, true, false, false)] = stripResidency(k_convStrip<32, true, false, false>, rowSmem<32>());
+  n.perSm[convVariant(32, true, false, true)] = stripResidency(k_convStrip<32, true, false, true>, rowSmem<32>());
+  n.perSm[convVariant(32, false, true, false)] = stripResidency(k_convStrip<32, false, true, false>, rowSmem<32>());
+  if (!n.state.alloc(2) || cudaMemsetAsync(n.state.p, 0, 2 * sizeof(int), n.st) != cudaSuccess) return false;
   packWeights(n);
   return cudaStreamSynchronize(n.st) == cudaSuccess;
 }
@@ -1007,7 +1062,7 @@ rg_status rg_denoiser_set_params(rg_denoiser* d, const float* in, size_t n) {
   RG_CUDA_CHECK(cudaMemcpyAsync(d->net.params.p, in, sizeof(float) * rg::kNumParams, cudaMemcpyHostToDevice, d->net.st));
   RG_CUDA_CHECK(cudaMemsetAsync(d->net.m.p, 0, sizeof(float) * rg::kNumParams, d->net.st));
   RG_CUDA_CHECK(cudaMemsetAsync(d->net.v.p, 0, sizeof(float) * rg::kNumParams, d->net.st));
-  d->net.adamStep = 0;
+  RG_CUDA_CHECK(cudaMemsetAsync(d->net.state.p, 0, 2 * sizeof(int), d->net.st));  // Adam restarts
   rg::packWeights(d->net);
   RG_CUDA_CHECK(cudaStreamSynchronize(d->net.st));
   return RG_OK;
@@ -1042,6 +1097,7 @@ rg_status rg_denoiser_add_example(rg_denoiser* d, int32_t w, int32_t h, const fl
   n.exX.push_back(x);
   n.exNoisy.push_back(nz);
   n.exRef.push_back(rf);
+  n.exDirty = true;
   n.dsW = w;
   n.dsH = h;
   n.dsN++;
@@ -1058,6 +1114,7 @@ rg_status rg_denoiser_clear_examples(rg_denoiser* d) {
   n.exX.clear();
   n.exNoisy.clear();
   n.exRef.clear();
+  n.exDirty = true;
   n.dsN = 0;
   return RG_OK;
 }
@@ -1073,37 +1130,69 @@ rg_status rg_denoiser_train(rg_denoiser* d, int32_t steps, int32_t batch, float 
   const int B = batch, H = n.dsH, W = n.dsW;
   const size_t Pi = (size_t)H * W, P = Pi * B;
   if (!rg::ensureWork(n, P)) return RG_ERR_OUT_OF_MEMORY;
+  if (steps == 0) return RG_OK;
+  // the picks of every step, drawn in the order of the host generator
   std::uniform_int_distribution<int> pick(0, n.dsN - 1);
-  cudaEvent_t e0, e1;
-  cudaEventCreate(&e0);
-  cudaEventCreate(&e1);
-  cudaEventRecord(e0, n.st);
-  for (int s = 0; s < steps; ++s) {
-    for (int b = 0; b < B; ++b) {  // random examples into the batch
-      const int e = pick(n.rng);
-      cudaMemcpyAsync(n.X0.p + b * Pi * 16, n.exX[e], Pi * 16 * sizeof(__nv_bfloat16), cudaMemcpyDeviceToDevice, n.st);
-      cudaMemcpyAsync(n.noisy.p + b * Pi, n.exNoisy[e], Pi * sizeof(float4), cudaMemcpyDeviceToDevice, n.st);
-      cudaMemcpyAsync(n.ref.p + b * Pi, n.exRef[e], Pi * sizeof(float4), cudaMemcpyDeviceToDevice, n.st);
+  std::vector<int> pk((size_t)steps * B);
+  for (auto& e : pk) e = pick(n.rng);
+  if (!n.picks.upload(pk.data(), pk.size(), n.st) || !n.lossHist.alloc((size_t)steps)) return RG_ERR_OUT_OF_MEMORY;
+  if (n.exDirty) {
+    std::vector<rg::ExampleRef> ex(n.dsN);
+    for (int i = 0; i < n.dsN; ++i) ex[i] = {n.exX[i], n.exNoisy[i], n.exRef[i]};
+    if (!n.exRefs.upload(ex.data(), ex.size(), n.st)) return RG_ERR_OUT_OF_MEMORY;
+    n.exDirty = false;
+  }
+  RG_CUDA_CHECK(cudaMemsetAsync(n.state.p, 0, sizeof(int), n.st));  // step 0 of this call
+  uint32_t lrBits;
+  std::memcpy(&lrBits, &lr, sizeof(lrBits));
+  const std::string key = std::to_string(B) + ":" + std::to_string(H) + ":" + std::to_string(W) + ":" +
+                          std::to_string(lrBits) + ":" + std::to_string(n.cap) + ":" +
+                          std::to_string((uintptr_t)n.X0.p) + ":" + std::to_string((uintptr_t)n.picks.p) + ":" +
+                          std::to_string((uintptr_t)n.lossHist.p) + ":" + std::to_string((uintptr_t)n.exRefs.p);
+  if (!n.trainGraph || n.trainKey != key) {
+    if (n.trainGraph) {
+      cudaGraphExecDestroy(n.trainGraph);
+      n.trainGraph = nullptr;
     }
+    cudaGraph_t g;
+    RG_CUDA_CHECK(cudaStreamBeginCapture(n.st, cudaStreamCaptureModeThreadLocal));
     cudaMemsetAsync(n.loss.p, 0, sizeof(float), n.st);
+    rg::k_gatherBatch<<<(unsigned)((P + 255) / 256), 256, 0, n.st>>>(B, (int)Pi, n.picks.p, n.state.p, n.exRefs.p,
+                                                                     n.X0.p, n.noisy.p, n.ref.p);
     rg::forward(n, B, H, W);
     rg::k_head<true><<<(unsigned)((P + 255) / 256), 256, 0, n.st>>>(B, H, W, n.Z.p, n.noisy.p, n.ref.p, nullptr, n.gA.p,
                                                                      n.loss.p);
     rg::backward(n, B, H, W);
-    n.adamStep++;
-    const float b1 = 0.9f, b2 = 0.999f;
-    rg::k_adam<<<(rg::kNumParams + 255) / 256, 256, 0, n.st>>>(rg::kNumParams, n.params.p, n.grad.p, n.m.p, n.v.p, lr, b1,
-                                                               b2, 1.0f - std::pow(b1, (float)n.adamStep),
-                                                               1.0f - std::pow(b2, (float)n.adamStep), 1e-8f);
+    rg::k_adam<<<(rg::kNumParams + 255) / 256, 256, 0, n.st>>>(rg::kNumParams, n.params.p, n.grad.p, n.m.p, n.v.p, lr,
+                                                               0.9f, 0.999f, n.state.p, 1e-8f);
     rg::packWeights(n);
-    if (losses) cudaMemcpyAsync(losses + s, n.loss.p, sizeof(float), cudaMemcpyDeviceToHost, n.st);
+    rg::k_stepEnd<<<1, 1, 0, n.st>>>(n.state.p, n.loss.p, n.lossHist.p);
+    RG_CUDA_CHECK(cudaStreamEndCapture(n.st, &g));
+    const cudaError_t ie = cudaGraphInstantiate(&n.trainGraph, g, 0);
+    cudaGraphDestroy(g);
+    if (ie != cudaSuccess || n.mapFailed) {
+      if (n.trainGraph) cudaGraphExecDestroy(n.trainGraph);
+      n.trainGraph = nullptr;
+      n.mapFailed = false;
+      setLastError(std::string("learned denoiser: training graph: ") +
+                   (ie != cudaSuccess ? cudaGetErrorString(ie) : "the driver could not encode a TMA tensor map"));
+      return RG_ERR_CUDA;
+    }
+    n.trainKey = key;
   }
+  cudaEvent_t e0, e1;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  cudaEventRecord(e0, n.st);
+  for (int s = 0; s < steps; ++s) RG_CUDA_CHECK(cudaGraphLaunch(n.trainGraph, n.st));
   cudaEventRecord(e1, n.st);
   const rg_status rs = rg::checkErr(n, "learned denoiser training");
   float ms = 0.0f;
-  if (rs == RG_OK && steps > 0 && cudaEventElapsedTime(&ms, e0, e1) == cudaSuccess) n.lastStepMs = ms / steps;
+  if (rs == RG_OK && cudaEventElapsedTime(&ms, e0, e1) == cudaSuccess) n.lastStepMs = ms / steps;
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
+  if (rs == RG_OK && losses)
+    RG_CUDA_CHECK(cudaMemcpy(losses, n.lossHist.p, sizeof(float) * steps, cudaMemcpyDeviceToHost));
   return rs;
 }
 

@@ -120,6 +120,31 @@ def test_kpcn_gradients_match_oracle(rg):
     d.close()
 
 
+def test_kpcn_training_steps_are_adam_on_the_gradient(rg):
+    """Two replayed training steps on one example (batch 1) equal two Adam updates
+    (b1 0.9, b2 0.999, eps 1e-8) with the gradient of that example at the current
+    weights: the captured step's gather, backward and device-side step count."""
+    d = rg.Denoiser(seed=11)
+    d.params = perturbed(d, 6)
+    noisy, normal, albedo, depth, ref = synth(1, 24, 40, 12)
+    d.add_example(noisy[0], normal[0], albedo[0], depth[0], ref[0])
+    lr, b1, b2, eps = 1e-3, 0.9, 0.999, 1e-8
+    p = d.params.astype(np.float64)
+    m = np.zeros_like(p)
+    v = np.zeros_like(p)
+    for t in (1, 2):
+        loss, g = d.gradients(noisy, normal, albedo, depth, ref)
+        g = g.astype(np.float64)
+        m = b1 * m + (1 - b1) * g
+        v = b2 * v + (1 - b2) * g * g
+        want = p - lr * (m / (1 - b1 ** t)) / (np.sqrt(v / (1 - b2 ** t)) + eps)
+        losses = d.train(1, 1, lr)
+        assert losses[0] == pytest.approx(loss, rel=1e-5)
+        p = d.params.astype(np.float64)
+        np.testing.assert_allclose(p, want, rtol=0, atol=lr * 1e-3)
+    d.close()
+
+
 def test_kpcn_training_reduces_loss(rg):
     import importlib
     kt = importlib.import_module(rg.__name__ + ".kpcn_train")
