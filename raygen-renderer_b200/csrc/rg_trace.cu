@@ -851,42 +851,46 @@ __global__ void __launch_bounds__(256) k_shade(DevScene S0, DevRender R0, const 
                                                int iter) {
   const int count = Q.counters[iter * kCountersPerIter + C_RAYS];
   const int inB = iter & 1, outB = (iter + 1) & 1;
-  const int stride = gridDim.x * blockDim.x;
-  // Each block iteration takes 256 consecutive queue entries and shades them
-  // grouped by the branch their hit takes (a counting sort in shared memory), so
-  // that a warp mostly runs one lobe: incoherent bounces otherwise leave a third
-  // of the lanes active and the kernel waiting on instruction fetch.  Classes:
-  // 0 emitter, 1 diffuse, 2 rough glossy, 3 mirror, 4 refraction,
-  // 5 transparency, 6 mixed lobes, 7 miss.  The bins and the order are double
-  // buffered by iteration, which leaves three block barriers per iteration.
-  constexpr int kBins = 8;
+  // Each block iteration takes 512 consecutive queue entries (two per thread)
+  // and shades them grouped by the branch their hit takes (a counting sort in
+  // shared memory), so that a warp mostly runs one lobe: incoherent bounces
+  // otherwise leave a third of the lanes active and the kernel waiting on
+  // instruction fetch.  Classes: 0 emitter, 1 diffuse, 2 rough glossy,
+  // 3 mirror, 4 refraction, 5 transparency, 6 mixed lobes, 7 miss.  The bins and
+  // the order are double buffered by iteration, which leaves three block
+  // barriers per iteration.
+  constexpr int kBins = 8, kPer = 2, kWin = 256 * kPer;
   __shared__ int sBin[2][kBins];
-  __shared__ int sOrder[2][256];
+  __shared__ int sOrder[2][kWin];
   if (threadIdx.x < 2 * kBins) sBin[threadIdx.x / kBins][threadIdx.x % kBins] = 0;
   __syncthreads();
   int buf = 0;
-  for (int base = blockIdx.x * blockDim.x; base < count; base += stride, buf ^= 1) {
-    int q = base + threadIdx.x;
+  for (int base = blockIdx.x * kWin; base < count; base += gridDim.x * kWin, buf ^= 1) {
     {
-      int key = kBins - 1;
-      if (q < count) {
-        const int prim0 = __float_as_int(Q.hits[q].w);
-        if (prim0 >= 0) {
-          const DevScene& Sk = MULTI ? jobs[__float_as_int(Q.rayD[inB][q].w)].S : S0;
-          const int mesh0 = __float_as_int(__ldg(&Sk.triVerts[(size_t)prim0 * 3].w));
-          const DevMaterial& mk = Sk.mats[Sk.objMat[Sk.meshObj[mesh0]]];
-          const float gl = mk.glossy, rf = mk.refraction;
-          if (mk.emission > 0.0f) key = 0;
-          else if (mk.transparency > 0.001f) key = 5;
-          else if (gl <= 0.00001f && rf <= 0.00001f) key = 1;
-          else if (rf <= 0.00001f && gl >= 1.0f - 0.00001f) key = mk.roughness < 1e-3f ? 3 : 2;
-          else if (gl <= 0.00001f && rf >= 1.0f - 0.00001f) key = 4;
-          else key = 6;
+      int key[kPer], rank[kPer];
+#pragma unroll
+      for (int h = 0; h < kPer; ++h) {
+        const int q0 = base + h * 256 + threadIdx.x;
+        key[h] = kBins - 1;
+        if (q0 < count) {
+          const int prim0 = __float_as_int(Q.hits[q0].w);
+          if (prim0 >= 0) {
+            const DevScene& Sk = MULTI ? jobs[__float_as_int(Q.rayD[inB][q0].w)].S : S0;
+            const int mesh0 = __float_as_int(__ldg(&Sk.triVerts[(size_t)prim0 * 3].w));
+            const DevMaterial& mk = Sk.mats[Sk.objMat[Sk.meshObj[mesh0]]];
+            const float gl = mk.glossy, rf = mk.refraction;
+            if (mk.emission > 0.0f) key[h] = 0;
+            else if (mk.transparency > 0.001f) key[h] = 5;
+            else if (gl <= 0.00001f && rf <= 0.00001f) key[h] = 1;
+            else if (rf <= 0.00001f && gl >= 1.0f - 0.00001f) key[h] = mk.roughness < 1e-3f ? 3 : 2;
+            else if (gl <= 0.00001f && rf >= 1.0f - 0.00001f) key[h] = 4;
+            else key[h] = 6;
+          }
         }
+        // sBin[buf] was zeroed, and this buffer's order last read, before the previous
+        // iteration's second barrier
+        rank[h] = atomicAdd(&sBin[buf][key[h]], 1);
       }
-      // sBin[buf] was zeroed, and this buffer's order last read, before the previous
-      // iteration's second barrier
-      const int rank = atomicAdd(&sBin[buf][key], 1);
       __syncthreads();
       if (threadIdx.x < 32) {  // exclusive scan of the bins
         const int c = threadIdx.x < kBins ? sBin[buf][threadIdx.x] : 0;
@@ -901,539 +905,542 @@ __global__ void __launch_bounds__(256) k_shade(DevScene S0, DevRender R0, const 
         sBin[buf ^ 1][threadIdx.x - 32] = 0;  // every thread is past the previous iteration's reads
       }
       __syncthreads();
-      sOrder[buf][sBin[buf][key] + rank] = q;
+#pragma unroll
+      for (int h = 0; h < kPer; ++h) sOrder[buf][sBin[buf][key[h]] + rank[h]] = base + h * 256 + threadIdx.x;
       __syncthreads();
-      q = sOrder[buf][threadIdx.x];
     }
-    const bool valid = q < count;
-    Shadow shA, shB, shE, shV;  // area light / point light / environment / volume light
-    shA.on = false;
-    shB.on = false;
-    shE.on = false;
-    shV.on = false;
-    bool cont = false;
-    V3 no = v3(0, 0, 0), nd = v3(0, 0, 0);
-    int pid = 0, slot = 0;
-    if (valid) {
-      const float4 ro = Q.rayO[inB][q], rd = Q.rayD[inB][q];
-      pid = __float_as_int(ro.w);
-      slot = __float_as_int(rd.w);
-      const DevScene S = MULTI ? jobs[slot].S : S0;
-      const DevRender R = MULTI ? jobs[slot].R : R0;
-      const V3 o = xyz(ro), d = xyz(rd);
-      const float4 hq = Q.hits[q];
-      const int prim = __float_as_int(hq.w);
-      const float4 PT = Q.pathT[pid], PR = Q.pathR[pid], PL = Q.pathL[pid];
-      V3 beta = xyz(PT);
-      float bsdfPdf = PT.w;
-      V3 rrT = xyz(PR);
-      uint32_t flags = __float_as_uint(PR.w);
-      V3 L = xyz(PL);
-      const int v = __float_as_int(PL.w);
-      bool eye = (flags & F_EYE) != 0;
-      int passes = (int)(flags & F_PASSES_MASK);
-      int chroma = (int)((flags & F_CHROMA_MASK) >> F_CHROMA_SHIFT) - 1;
-      int med = (int)((flags & F_MED_MASK) >> F_MED_SHIFT) - 1;
-      if (eye && prim < 0) flags |= F_EYE_NOHIT;
-      const int2 ps = Q.pathPS[pid];
-      const int x = ps.x % R.width, y = ps.x / R.width;
-      Rng rng;
-      rng.init(x, y, R.width, (uint32_t)ps.y, R.seed, dimBaseOf(R));
-      bool done = false;
-      bool silhouette = false;
-      // ---- participating medium on the segment (tracePath, rayrenderer.cpp:1612-1863)
-      const bool medActive = MEDL > 0 && med >= 0 && S.media[med].active;
-      if (MEDL == 2 && medActive && S.media[med].haze) {
-        // heat haze (rayrenderer.cpp:1645-1660): march to the next surface bending
-        // the ray, then continue from the bent ray in the outer (global) medium.
-        // A heat-haze global medium bends once and the path goes on without a
-        // medium (the reference recurses without end there).
-        const float maxT = prim >= 0 ? hq.x : kRayMaxDistance;
-        const med::Ray6 bent = med::bendRay(S.media + med, o, d, fminf(maxT, 1000.0f));
-        const int outer = S.globalMedium;
-        med = (outer >= 0 && S.media[outer].haze) ? -1 : outer;
-        cont = true;
-        no = bent.o;
-        nd = bent.d;
-      } else if (medActive) {
-        const DevMedium* Mg = S.media + med;
-        const DevMedium M = *Mg;
-        const bool het = MEDL == 2 && M.field != 0;
-        const float maxT = prim >= 0 ? hq.x : kRayMaxDistance;
-        float tF, dens = 1.0f;
-        bool scat;
-        if (het) {  // delta tracking (medium.cpp:406-441)
-          const med::Collision col = med::deltaTrack(Mg, o, d, maxT, rng, v);
-          scat = col.hit;
-          tF = col.hit ? col.t : maxT;
-          dens = col.density;
-        } else {
-          const float xi = fminf(0.9999999f, fmaxf(0.0f, rng.prng(v, S_FLIGHT)));
-          tF = -logf(1.0f - xi) / M.hero;
-          scat = tF < maxT;
-        }
-        const float el = scat ? tF : maxT;
-        if (MEDL == 2) {
-          L = L + beta * med::emissionIntegral(&jobs[slot].S, Mg, o, d, el, rng, v);
-        } else if (el > 0.0f) {
-          auto ew = [](float st, float dd) { return st < 1e-6f ? dd : (1.0f - expf(-st * dd)) / st; };
-          L = L + beta * v3(M.ser * ew(M.str, el), M.seg * ew(M.stg, el), M.seb * ew(M.stb, el));
-        }
-        if (scat) {
-          V3 sw = v3(0, 0, 0);
-          if (het) {  // sigma_s(p) / sigma_t_max: the rejection walk carries the decay
-            const float inv = M.tMaxHero > 0.0f ? 1.0f / M.tMaxHero : 0.0f;
-            sw = v3(M.ssr * dens * inv, M.ssg * dens * inv, M.ssb * dens * inv);
+    for (int h = 0; h < kPer; ++h) {
+      const int q = sOrder[buf][threadIdx.x + h * 256];
+      const bool valid = q < count;
+      Shadow shA, shB, shE, shV;  // area light / point light / environment / volume light
+      shA.on = false;
+      shB.on = false;
+      shE.on = false;
+      shV.on = false;
+      bool cont = false;
+      V3 no = v3(0, 0, 0), nd = v3(0, 0, 0);
+      int pid = 0, slot = 0;
+      if (valid) {
+        const float4 ro = Q.rayO[inB][q], rd = Q.rayD[inB][q];
+        pid = __float_as_int(ro.w);
+        slot = __float_as_int(rd.w);
+        const DevScene S = MULTI ? jobs[slot].S : S0;
+        const DevRender R = MULTI ? jobs[slot].R : R0;
+        const V3 o = xyz(ro), d = xyz(rd);
+        const float4 hq = Q.hits[q];
+        const int prim = __float_as_int(hq.w);
+        const float4 PT = Q.pathT[pid], PR = Q.pathR[pid], PL = Q.pathL[pid];
+        V3 beta = xyz(PT);
+        float bsdfPdf = PT.w;
+        V3 rrT = xyz(PR);
+        uint32_t flags = __float_as_uint(PR.w);
+        V3 L = xyz(PL);
+        const int v = __float_as_int(PL.w);
+        bool eye = (flags & F_EYE) != 0;
+        int passes = (int)(flags & F_PASSES_MASK);
+        int chroma = (int)((flags & F_CHROMA_MASK) >> F_CHROMA_SHIFT) - 1;
+        int med = (int)((flags & F_MED_MASK) >> F_MED_SHIFT) - 1;
+        if (eye && prim < 0) flags |= F_EYE_NOHIT;
+        const int2 ps = Q.pathPS[pid];
+        const int x = ps.x % R.width, y = ps.x / R.width;
+        Rng rng;
+        rng.init(x, y, R.width, (uint32_t)ps.y, R.seed, dimBaseOf(R));
+        bool done = false;
+        bool silhouette = false;
+        // ---- participating medium on the segment (tracePath, rayrenderer.cpp:1612-1863)
+        const bool medActive = MEDL > 0 && med >= 0 && S.media[med].active;
+        if (MEDL == 2 && medActive && S.media[med].haze) {
+          // heat haze (rayrenderer.cpp:1645-1660): march to the next surface bending
+          // the ray, then continue from the bent ray in the outer (global) medium.
+          // A heat-haze global medium bends once and the path goes on without a
+          // medium (the reference recurses without end there).
+          const float maxT = prim >= 0 ? hq.x : kRayMaxDistance;
+          const med::Ray6 bent = med::bendRay(S.media + med, o, d, fminf(maxT, 1000.0f));
+          const int outer = S.globalMedium;
+          med = (outer >= 0 && S.media[outer].haze) ? -1 : outer;
+          cont = true;
+          no = bent.o;
+          nd = bent.d;
+        } else if (medActive) {
+          const DevMedium* Mg = S.media + med;
+          const DevMedium M = *Mg;
+          const bool het = MEDL == 2 && M.field != 0;
+          const float maxT = prim >= 0 ? hq.x : kRayMaxDistance;
+          float tF, dens = 1.0f;
+          bool scat;
+          if (het) {  // delta tracking (medium.cpp:406-441)
+            const med::Collision col = med::deltaTrack(Mg, o, d, maxT, rng, v);
+            scat = col.hit;
+            tF = col.hit ? col.t : maxT;
+            dens = col.density;
           } else {
-            const float pHero = M.hero * expf(-M.hero * tF);
-            if (pHero > 0.0f)
-              sw = v3(M.ssr * expf(-M.str * tF) / pHero, M.ssg * expf(-M.stg * tF) / pHero, M.ssb * expf(-M.stb * tF) / pHero);
+            const float xi = fminf(0.9999999f, fmaxf(0.0f, rng.prng(v, S_FLIGHT)));
+            tF = -logf(1.0f - xi) / M.hero;
+            scat = tF < maxT;
           }
-          const int passesS = eye ? 1 : passes + 1;
-          if ((sw.x == 0.0f && sw.y == 0.0f && sw.z == 0.0f) || passesS > R.maxDepth) {
-            done = true;
-          } else {
-            const V3 pos = o + d * tF;
-            const V3 proxy = -d;
-            V3 lDir, Le;
-            float pl;
-            auto phaseTo = [&](V3 w) {  // HG phasePdf (medium.cpp:519-525)
-              const float g = M.g;
-              const float cosT = dot(-d, w);
-              const float den = 1.0f + g * g - 2.0f * g * cosT;
-              return (1.0f - g * g) * (1.0f / (4.0f * kPi)) / (den * sqrtf(fmaxf(1e-8f, den)));
-            };
-            if (sampleAreaLightForNEE(S, R, rng, v, pos, proxy, lDir, pl, Le, shA) && pl > 0.0f) {
-              shA.on = true;
-              shA.c = beta * sw * Le * (phaseTo(lDir) / pl);
+          const float el = scat ? tF : maxT;
+          if (MEDL == 2) {
+            L = L + beta * med::emissionIntegral(&jobs[slot].S, Mg, o, d, el, rng, v);
+          } else if (el > 0.0f) {
+            auto ew = [](float st, float dd) { return st < 1e-6f ? dd : (1.0f - expf(-st * dd)) / st; };
+            L = L + beta * v3(M.ser * ew(M.str, el), M.seg * ew(M.stg, el), M.seb * ew(M.stb, el));
+          }
+          if (scat) {
+            V3 sw = v3(0, 0, 0);
+            if (het) {  // sigma_s(p) / sigma_t_max: the rejection walk carries the decay
+              const float inv = M.tMaxHero > 0.0f ? 1.0f / M.tMaxHero : 0.0f;
+              sw = v3(M.ssr * dens * inv, M.ssg * dens * inv, M.ssb * dens * inv);
+            } else {
+              const float pHero = M.hero * expf(-M.hero * tF);
+              if (pHero > 0.0f)
+                sw = v3(M.ssr * expf(-M.str * tF) / pHero, M.ssg * expf(-M.stg * tF) / pHero, M.ssb * expf(-M.stb * tF) / pHero);
             }
-            if (ENV && S.envOn) {  // environment NEE at the scatter point (rayrenderer.cpp:1757-1761)
-              EnvSample e;
-              if (envNEE(&jobs[slot].S, rng, v, pos, proxy, e, shE)) {
-                shE.on = true;
-                shE.c = beta * sw * e.Li * (phaseTo(e.dir) / e.pdf);
-              }
-            }
-            if (MEDL == 2 && S.numVolLights > 0) {  // volume-light NEE (rayrenderer.cpp:1763-1767)
-              const med::VolSample vs = med::sampleVolumeLight(&jobs[slot].S, rng, v, pos, proxy);
-              if (vs.ok && vs.pdf > 0.0f) {
-                shV.on = true;
-                shV.o = vs.so;
-                shV.d = vs.sd;
-                shV.tmax = 0.99999f;
-                shV.c = beta * sw * vs.Le * (phaseTo(vs.dir) / vs.pdf);
-              }
-            }
-            // samplePhase: medium.cpp:496-517
-            const float u1 = rng.prng(v, S_PHASE0), u2 = rng.prng(v, S_PHASE1);
-            float cosTheta;
-            if (fabsf(M.g) < 1e-3f) cosTheta = 1.0f - 2.0f * u1;
-            else {
-              const float sq = (1.0f - M.g * M.g) / (1.0f - M.g + 2.0f * M.g * u1);
-              cosTheta = (1.0f + M.g * M.g - sq * sq) / (2.0f * M.g);
-            }
-            const float sinTheta = sqrtf(fmaxf(0.0f, 1.0f - cosTheta * cosTheta));
-            float sp, cp;
-            sincosf(2.0f * kPi * u2, &sp, &cp);
-            V3 t1;
-            if (fabsf(d.x) > fabsf(d.y)) { const float inv = 1.0f / sqrtf(d.x * d.x + d.z * d.z); t1 = v3(-d.z * inv, 0.0f, d.x * inv); }
-            else { const float inv = 1.0f / sqrtf(d.y * d.y + d.z * d.z); t1 = v3(0.0f, d.z * inv, -d.y * inv); }
-            const V3 t2 = cross(d, t1);
-            const V3 ndir = normalize(t1 * (sinTheta * cp) + t2 * (sinTheta * sp) + d * cosTheta);
-            const V3 rrBase = eye ? v3(1, 1, 1) : rrT;
-            float rrW = 1.0f;
-            bool killed = false;
-            if (passesS >= R.rrDepth) {
-              float qq = maxc(rrBase * sw);
-              qq = fminf(kRRMax, fmaxf(kRRMin, qq));
-              if (rng.prng(v, S_MEDRR) >= qq) killed = true;
-              else rrW = 1.0f / qq;
-            }
-            if (killed) {
+            const int passesS = eye ? 1 : passes + 1;
+            if ((sw.x == 0.0f && sw.y == 0.0f && sw.z == 0.0f) || passesS > R.maxDepth) {
               done = true;
             } else {
-              beta = beta * sw * rrW;
-              rrT = rrBase;
-              if (eye) chroma = -1;
-              bsdfPdf = 0.0f;
-              passes = passesS;
-              eye = false;
-              cont = true;
-              no = pos + normalize(ndir) * kSurfaceThickness;  // ThicknessRay
-              nd = ndir;
-            }
-          }
-        } else {
-          const float surv = het ? 0.0f : expf(-M.hero * maxT);  // delta tracking: weight 1 (rayrenderer.cpp:1815-1822)
-          if (surv > 0.0f)
-            beta = beta * v3(expf(-M.str * maxT) / surv, expf(-M.stg * maxT) / surv, expf(-M.stb * maxT) / surv);
-          if (prim < 0) {
-            if (ENV && S.envOn) L = L + beta * envMiss(&jobs[slot].S, d, bsdfPdf);  // rayrenderer.cpp:1852-1863
-            done = true;
-          }
-          silhouette = true;
-        }
-      } else if (prim < 0) {
-        // environment miss (rayrenderer.cpp:1619-1630; the eye ray has no pdf, so no weight)
-        if (ENV && S.envOn) L = L + beta * envMiss(&jobs[slot].S, d, bsdfPdf);
-        done = true;
-      }
-      // ---- surface vertex (RayBSDFShaderProvider::shade, rayrenderer.cpp:2776-2896)
-      if (!done && !cont) {
-        Hit h = loadHit(S, prim, o, d, hq.x, hq.y, hq.z);
-        if (silhouette) {  // rayrenderer.cpp:1842-1846
-          const V3 geomN = dot(h.gn, d) <= 0.0f ? h.gn : -h.gn;
-          if (dot(d, h.n) > 0.0f && dot(d, geomN) < 0.0f) h.n = geomN;
-        }
-        const int obj = S.meshObj[h.mesh];
-        const DevMaterial m = S.mats[S.objMat[obj]];
-        const V3 gN = dot(h.gn, h.n) >= 0.0f ? h.gn : -h.gn;  // geomNormal, bsdf.cpp:27-30
-        const float lf = R.lightFix ? (float)S.numAreaLights : 1.0f;
-        int lobe = -1;  // 0 diffuse 1 glossy 2 refraction 3 transparency
-        if (m.emission > 0.0f) {
-          V3 e = matColor(m) * m.emission;
-          if (!eye && bsdfPdf > 0.0f) {
-            const float cosL = -dot(d, h.n);
-            if (cosL <= 0.0f) e = v3(0, 0, 0);
-            else {
-              const V3 dv = h.p - o;
-              const float r2 = dot(dv, dv);
-              const float4 e1 = __ldg(&S.triVerts[(size_t)prim * 3 + 1]), e2 = __ldg(&S.triVerts[(size_t)prim * 3 + 2]);
-              const V3 cr = cross(xyz(e1), xyz(e2));
-              const float area = 0.5f * sqrtf(dot(cr, cr)) * (float)S.meshTriCount[h.mesh];
-              const float pl = r2 / (cosL * area) / lf;
-              e = e * (bsdfPdf * bsdfPdf / (bsdfPdf * bsdfPdf + pl * pl));
-            }
-          }
-          L = L + beta * e;
-          done = true;
-        } else {
-          bool backTransparency = false;
-          if (dot(d, h.n) > 0.0f) {
-            if (m.transparency > 0.001f) {
-              if (!eye && passes + 1 <= R.maxDepth) {
-                backTransparency = true;
-                passes = passes + 1;
-                chroma = -1;
+              const V3 pos = o + d * tF;
+              const V3 proxy = -d;
+              V3 lDir, Le;
+              float pl;
+              auto phaseTo = [&](V3 w) {  // HG phasePdf (medium.cpp:519-525)
+                const float g = M.g;
+                const float cosT = dot(-d, w);
+                const float den = 1.0f + g * g - 2.0f * g * cosT;
+                return (1.0f - g * g) * (1.0f / (4.0f * kPi)) / (den * sqrtf(fmaxf(1e-8f, den)));
+              };
+              if (sampleAreaLightForNEE(S, R, rng, v, pos, proxy, lDir, pl, Le, shA) && pl > 0.0f) {
+                shA.on = true;
+                shA.c = beta * sw * Le * (phaseTo(lDir) / pl);
+              }
+              if (ENV && S.envOn) {  // environment NEE at the scatter point (rayrenderer.cpp:1757-1761)
+                EnvSample e;
+                if (envNEE(&jobs[slot].S, rng, v, pos, proxy, e, shE)) {
+                  shE.on = true;
+                  shE.c = beta * sw * e.Li * (phaseTo(e.dir) / e.pdf);
+                }
+              }
+              if (MEDL == 2 && S.numVolLights > 0) {  // volume-light NEE (rayrenderer.cpp:1763-1767)
+                const med::VolSample vs = med::sampleVolumeLight(&jobs[slot].S, rng, v, pos, proxy);
+                if (vs.ok && vs.pdf > 0.0f) {
+                  shV.on = true;
+                  shV.o = vs.so;
+                  shV.d = vs.sd;
+                  shV.tmax = 0.99999f;
+                  shV.c = beta * sw * vs.Le * (phaseTo(vs.dir) / vs.pdf);
+                }
+              }
+              // samplePhase: medium.cpp:496-517
+              const float u1 = rng.prng(v, S_PHASE0), u2 = rng.prng(v, S_PHASE1);
+              float cosTheta;
+              if (fabsf(M.g) < 1e-3f) cosTheta = 1.0f - 2.0f * u1;
+              else {
+                const float sq = (1.0f - M.g * M.g) / (1.0f - M.g + 2.0f * M.g * u1);
+                cosTheta = (1.0f + M.g * M.g - sq * sq) / (2.0f * M.g);
+              }
+              const float sinTheta = sqrtf(fmaxf(0.0f, 1.0f - cosTheta * cosTheta));
+              float sp, cp;
+              sincosf(2.0f * kPi * u2, &sp, &cp);
+              V3 t1;
+              if (fabsf(d.x) > fabsf(d.y)) { const float inv = 1.0f / sqrtf(d.x * d.x + d.z * d.z); t1 = v3(-d.z * inv, 0.0f, d.x * inv); }
+              else { const float inv = 1.0f / sqrtf(d.y * d.y + d.z * d.z); t1 = v3(0.0f, d.z * inv, -d.y * inv); }
+              const V3 t2 = cross(d, t1);
+              const V3 ndir = normalize(t1 * (sinTheta * cp) + t2 * (sinTheta * sp) + d * cosTheta);
+              const V3 rrBase = eye ? v3(1, 1, 1) : rrT;
+              float rrW = 1.0f;
+              bool killed = false;
+              if (passesS >= R.rrDepth) {
+                float qq = maxc(rrBase * sw);
+                qq = fminf(kRRMax, fmaxf(kRRMin, qq));
+                if (rng.prng(v, S_MEDRR) >= qq) killed = true;
+                else rrW = 1.0f / qq;
+              }
+              if (killed) {
+                done = true;
+              } else {
+                beta = beta * sw * rrW;
+                rrT = rrBase;
+                if (eye) chroma = -1;
                 bsdfPdf = 0.0f;
-                lobe = 3;
-              } else {
-                done = true;
+                passes = passesS;
+                eye = false;
+                cont = true;
+                no = pos + normalize(ndir) * kSurfaceThickness;  // ThicknessRay
+                nd = ndir;
               }
-            } else if (m.refraction < 0.001f && m.glossy > 0.001f) {
+            }
+          } else {
+            const float surv = het ? 0.0f : expf(-M.hero * maxT);  // delta tracking: weight 1 (rayrenderer.cpp:1815-1822)
+            if (surv > 0.0f)
+              beta = beta * v3(expf(-M.str * maxT) / surv, expf(-M.stg * maxT) / surv, expf(-M.stb * maxT) / surv);
+            if (prim < 0) {
+              if (ENV && S.envOn) L = L + beta * envMiss(&jobs[slot].S, d, bsdfPdf);  // rayrenderer.cpp:1852-1863
               done = true;
             }
+            silhouette = true;
           }
-          if (!done && !backTransparency) {
-            if (!eye) {
-              if (passes + 1 >= R.maxDepth) {  // depth cap: direct light only
-                if (1.0f - m.glossy - m.refraction > 0.00001f) {
-                  const V3 col = R.colorSampling ? albedoOf(S, m, h) : v3(0, 0, 0);
-                  traceLight(S, R, rng, v, h.p, h.n, beta * col, shA, shB);
+        } else if (prim < 0) {
+          // environment miss (rayrenderer.cpp:1619-1630; the eye ray has no pdf, so no weight)
+          if (ENV && S.envOn) L = L + beta * envMiss(&jobs[slot].S, d, bsdfPdf);
+          done = true;
+        }
+        // ---- surface vertex (RayBSDFShaderProvider::shade, rayrenderer.cpp:2776-2896)
+        if (!done && !cont) {
+          Hit h = loadHit(S, prim, o, d, hq.x, hq.y, hq.z);
+          if (silhouette) {  // rayrenderer.cpp:1842-1846
+            const V3 geomN = dot(h.gn, d) <= 0.0f ? h.gn : -h.gn;
+            if (dot(d, h.n) > 0.0f && dot(d, geomN) < 0.0f) h.n = geomN;
+          }
+          const int obj = S.meshObj[h.mesh];
+          const DevMaterial m = S.mats[S.objMat[obj]];
+          const V3 gN = dot(h.gn, h.n) >= 0.0f ? h.gn : -h.gn;  // geomNormal, bsdf.cpp:27-30
+          const float lf = R.lightFix ? (float)S.numAreaLights : 1.0f;
+          int lobe = -1;  // 0 diffuse 1 glossy 2 refraction 3 transparency
+          if (m.emission > 0.0f) {
+            V3 e = matColor(m) * m.emission;
+            if (!eye && bsdfPdf > 0.0f) {
+              const float cosL = -dot(d, h.n);
+              if (cosL <= 0.0f) e = v3(0, 0, 0);
+              else {
+                const V3 dv = h.p - o;
+                const float r2 = dot(dv, dv);
+                const float4 e1 = __ldg(&S.triVerts[(size_t)prim * 3 + 1]), e2 = __ldg(&S.triVerts[(size_t)prim * 3 + 2]);
+                const V3 cr = cross(xyz(e1), xyz(e2));
+                const float area = 0.5f * sqrtf(dot(cr, cr)) * (float)S.meshTriCount[h.mesh];
+                const float pl = r2 / (cosL * area) / lf;
+                e = e * (bsdfPdf * bsdfPdf / (bsdfPdf * bsdfPdf + pl * pl));
+              }
+            }
+            L = L + beta * e;
+            done = true;
+          } else {
+            bool backTransparency = false;
+            if (dot(d, h.n) > 0.0f) {
+              if (m.transparency > 0.001f) {
+                if (!eye && passes + 1 <= R.maxDepth) {
+                  backTransparency = true;
+                  passes = passes + 1;
+                  chroma = -1;
+                  bsdfPdf = 0.0f;
+                  lobe = 3;
+                } else {
+                  done = true;
                 }
+              } else if (m.refraction < 0.001f && m.glossy > 0.001f) {
                 done = true;
-              } else {
-                passes = passes + 1;
-                if (passes >= R.rrDepth) {
-                  float qq = maxc(rrT);
-                  qq = fminf(kRRMax, fmaxf(kRRMin, qq));
-                  if (rng.prng(v, S_RR) >= qq) done = true;
-                  else beta = beta * (1.0f / qq);
-                }
-                if (!done) lobe = m.transparency > 0.001f ? 3 : 4;
-              }
-            } else {
-              passes = 0;
-              rrT = v3(1, 1, 1);
-              chroma = -1;
-              bsdfPdf = 0.0f;
-              if (m.transparency > 0.01f) {
-                // mix * (1 - t) + transparency: pick transparency with probability t
-                lobe = rng.prng(v, S_EYETR) < m.transparency ? 3 : 4;
-                if (lobe == 3) beta = beta * (1.0f / m.transparency);
-              } else {
-                lobe = 4;
               }
             }
-          }
-          if (!done && lobe == 4) {  // MixShader (bsdf.cpp:579-610), one lobe selected
-            const float wv[3] = {1.0f - m.glossy - m.refraction, m.glossy, m.refraction};
-            float sum = 0.0f;
-            for (int k = 0; k < 3; k++) if (wv[k] > 0.00001f) sum += wv[k];
-            if (sum > 0.0f) {
-              const float u = rng.prng(v, S_LOBE) * sum;
-              float acc = 0.0f;
-              for (int k = 0; k < 3; k++) {
-                if (!(wv[k] > 0.00001f)) continue;
-                lobe = k;
-                acc += wv[k];
-                if (u < acc) break;
-              }
-              beta = beta * sum;
-              rrT = rrT * wv[lobe];
-            } else {
-              done = true;
-            }
-          }
-          if (!done && lobe == 0) {  // DiffuseShader (bsdf.cpp:54-108)
-            const V3 albedo = R.colorSampling ? albedoOf(S, m, h) : v3(1, 1, 1);
-            const int d0 = rng.dirDim(v);
-            const V3 dir = cosineWeightedDirection(h.n, rng.lds(d0), rng.lds(d0 + 1));
-            traceLight(S, R, rng, v, h.p, h.n, beta * albedo, shA, shB);
-            bsdfPdf = fmaxf(0.0f, dot(dir, h.n)) * (1.0f / kPi);
-            if (ENV && S.envOn) {  // traceEnvmapLight (rayrenderer.cpp:1484-1519)
-              EnvSample e;
-              if (envNEE(&jobs[slot].S, rng, v, h.p, h.n, e, shE)) {
-                // the MIS partner is this vertex's own sampled-direction pdf, as passed at bsdf.cpp:86-88
-                const float w = bsdfPdf > 0.0f ? e.pdf * e.pdf / (e.pdf * e.pdf + bsdfPdf * bsdfPdf) : 1.0f;
-                shE.on = true;
-                shE.c = beta * albedo * e.Li * (dot(e.dir, h.n) * w / (kPi * e.pdf));
-              }
-            }
-            if (MEDL == 2 && S.numVolLights > 0) {  // volume-light NEE, no MIS (bsdf.cpp:91-101)
-              const med::VolSample vs = med::sampleVolumeLight(&jobs[slot].S, rng, v, h.p, h.n);
-              const float cosL = vs.ok && vs.pdf > 0.0f ? fmaxf(0.0f, dot(vs.dir, h.n)) : 0.0f;
-              if (cosL > 0.0f) {
-                shV.on = true;
-                shV.o = vs.so;
-                shV.d = vs.sd;
-                shV.tmax = 0.99999f;
-                shV.c = beta * albedo * vs.Le * (cosL * (1.0f / kPi) / vs.pdf);
-              }
-            }
-            beta = beta * albedo;
-            rrT = rrT * albedo;
-            cont = true;
-            no = surfaceOrigin(h.p, dir, gN);
-            nd = dir;
-          } else if (!done && lobe == 1) {  // GlossyShader (bsdf.cpp:173-374)
-            V3 albedo = matColor(m);
-            if (R.colorSampling && m.texture >= 0) albedo = albedoOf(S, m, h);
-            const V3 F0 = m.metallic >= 1.0f ? albedo : (albedo * m.metallic + v3(0.04f, 0.04f, 0.04f) * (1.0f - m.metallic));
-            auto schlick = [&](float VdotH) {
-              const float a1 = fmaxf(0.0f, 1.0f - VdotH);
-              const float a5 = a1 * a1 * a1 * a1 * a1;
-              return F0 + (v3(1, 1, 1) - F0) * a5;
-            };
-            if (m.roughness < 1e-3f) {
-              V3 r = reflect(d, h.n);
-              if (dot(r, gN) <= 0.0f) r = reflect(d, gN);
-              const V3 F = schlick(fmaxf(0.0f, -dot(d, h.n)));
-              beta = beta * F;
-              rrT = rrT * F;
-              bsdfPdf = 0.0f;
-              cont = true;
-              no = surfaceOrigin(h.p, r, gN);
-              nd = r;
-            } else {
-              const V3 up = fabsf(h.n.y) > 0.99f ? v3(1, 0, 0) : v3(0, 1, 0);
-              V3 t = normalize(cross(up, h.n));
-              V3 b = cross(h.n, t);
-              if (fabsf(m.anisoRot) > 0.0f) {
-                float sa, ca;
-                sincosf(m.anisoRot * (kPi / 180.0f), &sa, &ca);
-                const V3 t2 = t * ca + b * sa, b2 = b * ca - t * sa;
-                t = t2;
-                b = b2;
-              }
-              const float aniso = fmaxf(-0.99f, fminf(0.99f, m.aniso));
-              const float r2 = m.roughness * m.roughness;
-              const float ax = fmaxf(1e-3f, r2 * (1.0f - aniso));
-              const float ay = fmaxf(1e-3f, r2 * (1.0f + aniso));
-              const V3 Vw = -d;
-              const V3 Vl = v3(dot(Vw, t), dot(Vw, b), dot(Vw, h.n));
-              if (Vl.z <= 0.0f) {
-                done = true;
-              } else {
-                auto smithG1 = [&](V3 w) {
-                  if (w.z <= 0.0f) return 0.0f;
-                  const float ax2 = (ax * w.x) * (ax * w.x), ay2 = (ay * w.y) * (ay * w.y);
-                  const float lambda = 0.5f * (sqrtf(1.0f + (ax2 + ay2) / (w.z * w.z)) - 1.0f);
-                  return 1.0f / (1.0f + lambda);
-                };
-                const float G1v = smithG1(Vl);
-                // evalGlossy (bsdf.cpp:260-280): f*cos_L and the VNDF pdf toward dw
-                auto evalGlossy = [&](V3 dw, V3& fCos, float& pb) {
-                  const V3 Ll = v3(dot(dw, t), dot(dw, b), dot(dw, h.n));
-                  if (Ll.z <= 0.0f) return false;
-                  V3 Hl = Vl + Ll;
-                  const float hl2 = dot(Hl, Hl);
-                  if (hl2 <= 0.0f) return false;
-                  Hl = Hl * (1.0f / sqrtf(hl2));
-                  const float VdotH = fmaxf(0.0f, dot(Vl, Hl));
-                  if (Hl.z <= 0.0f || VdotH <= 0.0f) return false;
-                  const float hx = Hl.x / ax, hy = Hl.y / ay;
-                  const float den = hx * hx + hy * hy + Hl.z * Hl.z;
-                  const float D = 1.0f / (kPi * ax * ay * den * den);
-                  fCos = schlick(VdotH) * (D * G1v * smithG1(Ll) / (4.0f * Vl.z));
-                  pb = G1v * D / (4.0f * Vl.z);
-                  return true;
-                };
-                // area-light NEE with MIS (bsdf.cpp:271-284)
-                V3 lDir, Le, fCos;
-                float pl, pb;
-                if (sampleAreaLightForNEE(S, R, rng, v, h.p, h.n, lDir, pl, Le, shA) && evalGlossy(lDir, fCos, pb)) {
-                  shA.on = true;
-                  shA.c = beta * Le * fCos * (pl * pl / (pl * pl + pb * pb) / pl);
-                }
-                // environment NEE with MIS (bsdf.cpp:302-314)
-                if (ENV && S.envOn) {
-                  EnvSample e;
-                  if (envNEE(&jobs[slot].S, rng, v, h.p, h.n, e, shE) && evalGlossy(e.dir, fCos, pb)) {
-                    shE.on = true;
-                    shE.c = beta * e.Li * fCos * (e.pdf * e.pdf / (e.pdf * e.pdf + pb * pb) / e.pdf);
+            if (!done && !backTransparency) {
+              if (!eye) {
+                if (passes + 1 >= R.maxDepth) {  // depth cap: direct light only
+                  if (1.0f - m.glossy - m.refraction > 0.00001f) {
+                    const V3 col = R.colorSampling ? albedoOf(S, m, h) : v3(0, 0, 0);
+                    traceLight(S, R, rng, v, h.p, h.n, beta * col, shA, shB);
                   }
-                }
-                // volume-light NEE, no MIS (bsdf.cpp:316-328)
-                if (MEDL == 2 && S.numVolLights > 0) {
-                  const med::VolSample vs = med::sampleVolumeLight(&jobs[slot].S, rng, v, h.p, h.n);
-                  if (vs.ok && vs.pdf > 0.0f && evalGlossy(vs.dir, fCos, pb)) {
-                    shV.on = true;
-                    shV.o = vs.so;
-                    shV.d = vs.sd;
-                    shV.tmax = 0.99999f;
-                    shV.c = beta * vs.Le * fCos * (1.0f / vs.pdf);
-                  }
-                }
-                // VNDF sample (bsdf.cpp:139-161, 319-373)
-                const float u1 = rng.prng(v, S_VNDF0), u2 = rng.prng(v, S_VNDF1);
-                const V3 Vh = normalize(v3(ax * Vl.x, ay * Vl.y, Vl.z));
-                const float lensq = Vh.x * Vh.x + Vh.y * Vh.y;
-                const V3 T1 = lensq > 0.0f ? v3(-Vh.y, Vh.x, 0.0f) * (1.0f / sqrtf(lensq)) : v3(1, 0, 0);
-                const V3 T2 = cross(Vh, T1);
-                const float rr = sqrtf(u1);
-                float sphi, cphi;
-                sincosf(2.0f * kPi * u2, &sphi, &cphi);
-                const float t1 = rr * cphi;
-                float t2 = rr * sphi;
-                const float sw = 0.5f * (1.0f + Vh.z);
-                t2 = (1.0f - sw) * sqrtf(fmaxf(0.0f, 1.0f - t1 * t1)) + sw * t2;
-                const V3 Nh = T1 * t1 + T2 * t2 + Vh * sqrtf(fmaxf(0.0f, 1.0f - t1 * t1 - t2 * t2));
-                const V3 H = normalize(v3(ax * Nh.x, ay * Nh.y, fmaxf(0.0f, Nh.z)));
-                const V3 Ll = H * (2.0f * dot(Vl, H)) - Vl;
-                if (Ll.z <= 0.0f) {
                   done = true;
                 } else {
-                  const V3 Lw = t * Ll.x + b * Ll.y + h.n * Ll.z;
-                  if (dot(Lw, gN) <= 0.0f) {
-                    done = true;
-                  } else {
-                    const V3 F = schlick(fmaxf(0.0f, dot(Vl, H)));
-                    const V3 wgt = F * smithG1(Ll);
-                    const float hx = H.x / ax, hy = H.y / ay;
-                    const float den = hx * hx + hy * hy + H.z * H.z;
-                    const float D = 1.0f / (kPi * ax * ay * den * den);
-                    bsdfPdf = G1v * D / (4.0f * Vl.z);
-                    beta = beta * wgt;
-                    rrT = rrT * wgt;
-                    cont = true;
-                    no = surfaceOrigin(h.p, Lw, gN);
-                    nd = Lw;
+                  passes = passes + 1;
+                  if (passes >= R.rrDepth) {
+                    float qq = maxc(rrT);
+                    qq = fminf(kRRMax, fmaxf(kRRMin, qq));
+                    if (rng.prng(v, S_RR) >= qq) done = true;
+                    else beta = beta * (1.0f / qq);
                   }
+                  if (!done) lobe = m.transparency > 0.001f ? 3 : 4;
+                }
+              } else {
+                passes = 0;
+                rrT = v3(1, 1, 1);
+                chroma = -1;
+                bsdfPdf = 0.0f;
+                if (m.transparency > 0.01f) {
+                  // mix * (1 - t) + transparency: pick transparency with probability t
+                  lobe = rng.prng(v, S_EYETR) < m.transparency ? 3 : 4;
+                  if (lobe == 3) beta = beta * (1.0f / m.transparency);
+                } else {
+                  lobe = 4;
                 }
               }
             }
-          } else if (!done && lobe == 2) {  // RefractionShader (bsdf.cpp:376-483)
-            const float cosTheta = fabsf(dot(d, h.n));
-            float ior = m.ior;
-            V3 mask = v3(1, 1, 1);
-            if (m.chroma > 0.0f) {
-              bool first = false;
-              if (chroma < 0) {
-                chroma = (int)fminf(2.0f, floorf(rng.prng(v, S_CHROMA) * 3.0f));
-                first = true;
+            if (!done && lobe == 4) {  // MixShader (bsdf.cpp:579-610), one lobe selected
+              const float wv[3] = {1.0f - m.glossy - m.refraction, m.glossy, m.refraction};
+              float sum = 0.0f;
+              for (int k = 0; k < 3; k++) if (wv[k] > 0.00001f) sum += wv[k];
+              if (sum > 0.0f) {
+                const float u = rng.prng(v, S_LOBE) * sum;
+                float acc = 0.0f;
+                for (int k = 0; k < 3; k++) {
+                  if (!(wv[k] > 0.00001f)) continue;
+                  lobe = k;
+                  acc += wv[k];
+                  if (u < acc) break;
+                }
+                beta = beta * sum;
+                rrT = rrT * wv[lobe];
+              } else {
+                done = true;
               }
-              if (chroma == 0) ior = m.ior * (1.0f - m.chroma);
-              else if (chroma == 2) ior = m.ior * (1.0f + m.chroma);
-              if (first) mask = chroma == 0 ? v3(3, 0, 0) : (chroma == 1 ? v3(0, 3, 0) : v3(0, 0, 3));
             }
-            float r0 = (1.0f - ior) / (1.0f + ior);
-            r0 = r0 * r0;
-            const float mm = 1.0f - cosTheta;
-            const float F = r0 + (1.0f - r0) * (mm * mm) * (mm * mm) * mm;
-            const bool pickReflect = rng.prng(v, S_FRESNEL) < F;
-            V3 dir;
-            if (pickReflect) {
-              dir = reflect(d, h.n);
-            } else {  // refract (bsdf.cpp:39-52)
-              const V3 nl = dot(d, h.n) < 0.0f ? h.n : -h.n;
-              const bool into = dot(nl, h.n) > 0.0f;
-              const float rr = into ? 1.0f / ior : ior;
-              const float c = dot(d, nl);
-              const float tt = 1.0f - rr * rr * (1.0f - c * c);
-              if (tt < 0.0f) dir = reflect(d, h.n);
-              else dir = normalize(d * rr - h.n * ((into ? 1.0f : -1.0f) * (c * rr + sqrtf(tt))));
-            }
-            if (m.roughness > 0.0f)
-              dir = normalize(dir + randomRayInHemisphere(h.n, rng.prng(v, S_HEMI0), rng.prng(v, S_HEMI1)) * m.roughness);
-            if (pickReflect && dot(dir, gN) <= 0.0f) dir = reflect(d, gN);
-            const float dIn = dot(d, h.n), dOut = dot(dir, h.n);
-            if (dIn * dOut > 0.0f) {
-              if (dIn < 0.0f) { const int im = S.objMedium[obj]; if (im >= 0) med = im; }
+            if (!done && lobe == 0) {  // DiffuseShader (bsdf.cpp:54-108)
+              const V3 albedo = R.colorSampling ? albedoOf(S, m, h) : v3(1, 1, 1);
+              const int d0 = rng.dirDim(v);
+              const V3 dir = cosineWeightedDirection(h.n, rng.lds(d0), rng.lds(d0 + 1));
+              traceLight(S, R, rng, v, h.p, h.n, beta * albedo, shA, shB);
+              bsdfPdf = fmaxf(0.0f, dot(dir, h.n)) * (1.0f / kPi);
+              if (ENV && S.envOn) {  // traceEnvmapLight (rayrenderer.cpp:1484-1519)
+                EnvSample e;
+                if (envNEE(&jobs[slot].S, rng, v, h.p, h.n, e, shE)) {
+                  // the MIS partner is this vertex's own sampled-direction pdf, as passed at bsdf.cpp:86-88
+                  const float w = bsdfPdf > 0.0f ? e.pdf * e.pdf / (e.pdf * e.pdf + bsdfPdf * bsdfPdf) : 1.0f;
+                  shE.on = true;
+                  shE.c = beta * albedo * e.Li * (dot(e.dir, h.n) * w / (kPi * e.pdf));
+                }
+              }
+              if (MEDL == 2 && S.numVolLights > 0) {  // volume-light NEE, no MIS (bsdf.cpp:91-101)
+                const med::VolSample vs = med::sampleVolumeLight(&jobs[slot].S, rng, v, h.p, h.n);
+                const float cosL = vs.ok && vs.pdf > 0.0f ? fmaxf(0.0f, dot(vs.dir, h.n)) : 0.0f;
+                if (cosL > 0.0f) {
+                  shV.on = true;
+                  shV.o = vs.so;
+                  shV.d = vs.sd;
+                  shV.tmax = 0.99999f;
+                  shV.c = beta * albedo * vs.Le * (cosL * (1.0f / kPi) / vs.pdf);
+                }
+              }
+              beta = beta * albedo;
+              rrT = rrT * albedo;
+              cont = true;
+              no = surfaceOrigin(h.p, dir, gN);
+              nd = dir;
+            } else if (!done && lobe == 1) {  // GlossyShader (bsdf.cpp:173-374)
+              V3 albedo = matColor(m);
+              if (R.colorSampling && m.texture >= 0) albedo = albedoOf(S, m, h);
+              const V3 F0 = m.metallic >= 1.0f ? albedo : (albedo * m.metallic + v3(0.04f, 0.04f, 0.04f) * (1.0f - m.metallic));
+              auto schlick = [&](float VdotH) {
+                const float a1 = fmaxf(0.0f, 1.0f - VdotH);
+                const float a5 = a1 * a1 * a1 * a1 * a1;
+                return F0 + (v3(1, 1, 1) - F0) * a5;
+              };
+              if (m.roughness < 1e-3f) {
+                V3 r = reflect(d, h.n);
+                if (dot(r, gN) <= 0.0f) r = reflect(d, gN);
+                const V3 F = schlick(fmaxf(0.0f, -dot(d, h.n)));
+                beta = beta * F;
+                rrT = rrT * F;
+                bsdfPdf = 0.0f;
+                cont = true;
+                no = surfaceOrigin(h.p, r, gN);
+                nd = r;
+              } else {
+                const V3 up = fabsf(h.n.y) > 0.99f ? v3(1, 0, 0) : v3(0, 1, 0);
+                V3 t = normalize(cross(up, h.n));
+                V3 b = cross(h.n, t);
+                if (fabsf(m.anisoRot) > 0.0f) {
+                  float sa, ca;
+                  sincosf(m.anisoRot * (kPi / 180.0f), &sa, &ca);
+                  const V3 t2 = t * ca + b * sa, b2 = b * ca - t * sa;
+                  t = t2;
+                  b = b2;
+                }
+                const float aniso = fmaxf(-0.99f, fminf(0.99f, m.aniso));
+                const float r2 = m.roughness * m.roughness;
+                const float ax = fmaxf(1e-3f, r2 * (1.0f - aniso));
+                const float ay = fmaxf(1e-3f, r2 * (1.0f + aniso));
+                const V3 Vw = -d;
+                const V3 Vl = v3(dot(Vw, t), dot(Vw, b), dot(Vw, h.n));
+                if (Vl.z <= 0.0f) {
+                  done = true;
+                } else {
+                  auto smithG1 = [&](V3 w) {
+                    if (w.z <= 0.0f) return 0.0f;
+                    const float ax2 = (ax * w.x) * (ax * w.x), ay2 = (ay * w.y) * (ay * w.y);
+                    const float lambda = 0.5f * (sqrtf(1.0f + (ax2 + ay2) / (w.z * w.z)) - 1.0f);
+                    return 1.0f / (1.0f + lambda);
+                  };
+                  const float G1v = smithG1(Vl);
+                  // evalGlossy (bsdf.cpp:260-280): f*cos_L and the VNDF pdf toward dw
+                  auto evalGlossy = [&](V3 dw, V3& fCos, float& pb) {
+                    const V3 Ll = v3(dot(dw, t), dot(dw, b), dot(dw, h.n));
+                    if (Ll.z <= 0.0f) return false;
+                    V3 Hl = Vl + Ll;
+                    const float hl2 = dot(Hl, Hl);
+                    if (hl2 <= 0.0f) return false;
+                    Hl = Hl * (1.0f / sqrtf(hl2));
+                    const float VdotH = fmaxf(0.0f, dot(Vl, Hl));
+                    if (Hl.z <= 0.0f || VdotH <= 0.0f) return false;
+                    const float hx = Hl.x / ax, hy = Hl.y / ay;
+                    const float den = hx * hx + hy * hy + Hl.z * Hl.z;
+                    const float D = 1.0f / (kPi * ax * ay * den * den);
+                    fCos = schlick(VdotH) * (D * G1v * smithG1(Ll) / (4.0f * Vl.z));
+                    pb = G1v * D / (4.0f * Vl.z);
+                    return true;
+                  };
+                  // area-light NEE with MIS (bsdf.cpp:271-284)
+                  V3 lDir, Le, fCos;
+                  float pl, pb;
+                  if (sampleAreaLightForNEE(S, R, rng, v, h.p, h.n, lDir, pl, Le, shA) && evalGlossy(lDir, fCos, pb)) {
+                    shA.on = true;
+                    shA.c = beta * Le * fCos * (pl * pl / (pl * pl + pb * pb) / pl);
+                  }
+                  // environment NEE with MIS (bsdf.cpp:302-314)
+                  if (ENV && S.envOn) {
+                    EnvSample e;
+                    if (envNEE(&jobs[slot].S, rng, v, h.p, h.n, e, shE) && evalGlossy(e.dir, fCos, pb)) {
+                      shE.on = true;
+                      shE.c = beta * e.Li * fCos * (e.pdf * e.pdf / (e.pdf * e.pdf + pb * pb) / e.pdf);
+                    }
+                  }
+                  // volume-light NEE, no MIS (bsdf.cpp:316-328)
+                  if (MEDL == 2 && S.numVolLights > 0) {
+                    const med::VolSample vs = med::sampleVolumeLight(&jobs[slot].S, rng, v, h.p, h.n);
+                    if (vs.ok && vs.pdf > 0.0f && evalGlossy(vs.dir, fCos, pb)) {
+                      shV.on = true;
+                      shV.o = vs.so;
+                      shV.d = vs.sd;
+                      shV.tmax = 0.99999f;
+                      shV.c = beta * vs.Le * fCos * (1.0f / vs.pdf);
+                    }
+                  }
+                  // VNDF sample (bsdf.cpp:139-161, 319-373)
+                  const float u1 = rng.prng(v, S_VNDF0), u2 = rng.prng(v, S_VNDF1);
+                  const V3 Vh = normalize(v3(ax * Vl.x, ay * Vl.y, Vl.z));
+                  const float lensq = Vh.x * Vh.x + Vh.y * Vh.y;
+                  const V3 T1 = lensq > 0.0f ? v3(-Vh.y, Vh.x, 0.0f) * (1.0f / sqrtf(lensq)) : v3(1, 0, 0);
+                  const V3 T2 = cross(Vh, T1);
+                  const float rr = sqrtf(u1);
+                  float sphi, cphi;
+                  sincosf(2.0f * kPi * u2, &sphi, &cphi);
+                  const float t1 = rr * cphi;
+                  float t2 = rr * sphi;
+                  const float sw = 0.5f * (1.0f + Vh.z);
+                  t2 = (1.0f - sw) * sqrtf(fmaxf(0.0f, 1.0f - t1 * t1)) + sw * t2;
+                  const V3 Nh = T1 * t1 + T2 * t2 + Vh * sqrtf(fmaxf(0.0f, 1.0f - t1 * t1 - t2 * t2));
+                  const V3 H = normalize(v3(ax * Nh.x, ay * Nh.y, fmaxf(0.0f, Nh.z)));
+                  const V3 Ll = H * (2.0f * dot(Vl, H)) - Vl;
+                  if (Ll.z <= 0.0f) {
+                    done = true;
+                  } else {
+                    const V3 Lw = t * Ll.x + b * Ll.y + h.n * Ll.z;
+                    if (dot(Lw, gN) <= 0.0f) {
+                      done = true;
+                    } else {
+                      const V3 F = schlick(fmaxf(0.0f, dot(Vl, H)));
+                      const V3 wgt = F * smithG1(Ll);
+                      const float hx = H.x / ax, hy = H.y / ay;
+                      const float den = hx * hx + hy * hy + H.z * H.z;
+                      const float D = 1.0f / (kPi * ax * ay * den * den);
+                      bsdfPdf = G1v * D / (4.0f * Vl.z);
+                      beta = beta * wgt;
+                      rrT = rrT * wgt;
+                      cont = true;
+                      no = surfaceOrigin(h.p, Lw, gN);
+                      nd = Lw;
+                    }
+                  }
+                }
+              }
+            } else if (!done && lobe == 2) {  // RefractionShader (bsdf.cpp:376-483)
+              const float cosTheta = fabsf(dot(d, h.n));
+              float ior = m.ior;
+              V3 mask = v3(1, 1, 1);
+              if (m.chroma > 0.0f) {
+                bool first = false;
+                if (chroma < 0) {
+                  chroma = (int)fminf(2.0f, floorf(rng.prng(v, S_CHROMA) * 3.0f));
+                  first = true;
+                }
+                if (chroma == 0) ior = m.ior * (1.0f - m.chroma);
+                else if (chroma == 2) ior = m.ior * (1.0f + m.chroma);
+                if (first) mask = chroma == 0 ? v3(3, 0, 0) : (chroma == 1 ? v3(0, 3, 0) : v3(0, 0, 3));
+              }
+              float r0 = (1.0f - ior) / (1.0f + ior);
+              r0 = r0 * r0;
+              const float mm = 1.0f - cosTheta;
+              const float F = r0 + (1.0f - r0) * (mm * mm) * (mm * mm) * mm;
+              const bool pickReflect = rng.prng(v, S_FRESNEL) < F;
+              V3 dir;
+              if (pickReflect) {
+                dir = reflect(d, h.n);
+              } else {  // refract (bsdf.cpp:39-52)
+                const V3 nl = dot(d, h.n) < 0.0f ? h.n : -h.n;
+                const bool into = dot(nl, h.n) > 0.0f;
+                const float rr = into ? 1.0f / ior : ior;
+                const float c = dot(d, nl);
+                const float tt = 1.0f - rr * rr * (1.0f - c * c);
+                if (tt < 0.0f) dir = reflect(d, h.n);
+                else dir = normalize(d * rr - h.n * ((into ? 1.0f : -1.0f) * (c * rr + sqrtf(tt))));
+              }
+              if (m.roughness > 0.0f)
+                dir = normalize(dir + randomRayInHemisphere(h.n, rng.prng(v, S_HEMI0), rng.prng(v, S_HEMI1)) * m.roughness);
+              if (pickReflect && dot(dir, gN) <= 0.0f) dir = reflect(d, gN);
+              const float dIn = dot(d, h.n), dOut = dot(dir, h.n);
+              if (dIn * dOut > 0.0f) {
+                if (dIn < 0.0f) { const int im = S.objMedium[obj]; if (im >= 0) med = im; }
+                else med = S.globalMedium;
+              }
+              const V3 col = matColor(m);
+              beta = beta * col * mask;
+              rrT = rrT * col;
+              bsdfPdf = 0.0f;
+              cont = true;
+              no = surfaceOrigin(h.p, dir, gN);
+              nd = dir;
+            } else if (!done && lobe == 3) {  // TransparencyShader (bsdf.cpp:513-546)
+              const float tr = m.transparency;
+              beta = beta * tr;
+              rrT = rrT * tr;
+              if (dot(d, h.n) < 0.0f) { const int im = S.objMedium[obj]; if (im >= 0) med = im; }
               else med = S.globalMedium;
+              cont = true;
+              no = surfaceOrigin(h.p, d, gN);
+              nd = d;
             }
-            const V3 col = matColor(m);
-            beta = beta * col * mask;
-            rrT = rrT * col;
-            bsdfPdf = 0.0f;
-            cont = true;
-            no = surfaceOrigin(h.p, dir, gN);
-            nd = dir;
-          } else if (!done && lobe == 3) {  // TransparencyShader (bsdf.cpp:513-546)
-            const float tr = m.transparency;
-            beta = beta * tr;
-            rrT = rrT * tr;
-            if (dot(d, h.n) < 0.0f) { const int im = S.objMedium[obj]; if (im >= 0) med = im; }
-            else med = S.globalMedium;
-            cont = true;
-            no = surfaceOrigin(h.p, d, gN);
-            nd = d;
+            if (!done && cont) eye = false;
           }
-          if (!done && cont) eye = false;
+        }
+        // write back the path state
+        flags = (flags & ~(F_PASSES_MASK | F_CHROMA_MASK | F_MED_MASK | F_EYE)) | ((uint32_t)passes & F_PASSES_MASK) |
+                ((uint32_t)(chroma + 1) << F_CHROMA_SHIFT) | ((uint32_t)(med + 1) << F_MED_SHIFT) | (eye ? F_EYE : 0u);
+        Q.pathT[pid] = make_float4(beta.x, beta.y, beta.z, bsdfPdf);
+        Q.pathR[pid] = make_float4(rrT.x, rrT.y, rrT.z, __uint_as_float(flags));
+        Q.pathL[pid] = make_float4(L.x, L.y, L.z, __int_as_float(v + 1));
+        if (!cont) {
+          no = v3(0, 0, 0);
         }
       }
-      // write back the path state
-      flags = (flags & ~(F_PASSES_MASK | F_CHROMA_MASK | F_MED_MASK | F_EYE)) | ((uint32_t)passes & F_PASSES_MASK) |
-              ((uint32_t)(chroma + 1) << F_CHROMA_SHIFT) | ((uint32_t)(med + 1) << F_MED_SHIFT) | (eye ? F_EYE : 0u);
-      Q.pathT[pid] = make_float4(beta.x, beta.y, beta.z, bsdfPdf);
-      Q.pathR[pid] = make_float4(rrT.x, rrT.y, rrT.z, __uint_as_float(flags));
-      Q.pathL[pid] = make_float4(L.x, L.y, L.z, __int_as_float(v + 1));
-      if (!cont) {
-        no = v3(0, 0, 0);
+      // queue pushes (warp-aggregated)
+      const int qslot = warpPush(&Q.counters[(iter + 1) * kCountersPerIter + C_RAYS], cont && (iter + 1) < Q.maxIter);
+      if (qslot >= 0) {
+        Q.rayO[outB][qslot] = make_float4(no.x, no.y, no.z, __int_as_float(pid));
+        Q.rayD[outB][qslot] = make_float4(nd.x, nd.y, nd.z, __int_as_float(slot));
       }
-    }
-    // queue pushes (warp-aggregated)
-    const int qslot = warpPush(&Q.counters[(iter + 1) * kCountersPerIter + C_RAYS], cont && (iter + 1) < Q.maxIter);
-    if (qslot >= 0) {
-      Q.rayO[outB][qslot] = make_float4(no.x, no.y, no.z, __int_as_float(pid));
-      Q.rayD[outB][qslot] = make_float4(nd.x, nd.y, nd.z, __int_as_float(slot));
-    }
-    const int sa = warpPush(&Q.counters[iter * kCountersPerIter + C_SHA], shA.on);
-    if (sa >= 0) {
-      Q.shO[0][sa] = make_float4(shA.o.x, shA.o.y, shA.o.z, __int_as_float(pid));
-      Q.shD[0][sa] = make_float4(shA.d.x, shA.d.y, shA.d.z, shA.tmax);
-      Q.shC[0][sa] = make_float4(shA.c.x, shA.c.y, shA.c.z, __int_as_float(slot));
-    }
-    const int sb = warpPush(&Q.counters[iter * kCountersPerIter + C_SHB], shB.on);
-    if (sb >= 0) {
-      Q.shO[1][sb] = make_float4(shB.o.x, shB.o.y, shB.o.z, __int_as_float(pid));
-      Q.shD[1][sb] = make_float4(shB.d.x, shB.d.y, shB.d.z, shB.tmax);
-      Q.shC[1][sb] = make_float4(shB.c.x, shB.c.y, shB.c.z, __int_as_float(slot));
-    }
-    if (ENV) {
-      const int se = warpPush(&Q.counters[iter * kCountersPerIter + C_SHC], shE.on);
-      if (se >= 0) {
-        Q.shO[2][se] = make_float4(shE.o.x, shE.o.y, shE.o.z, __int_as_float(pid));
-        Q.shD[2][se] = make_float4(shE.d.x, shE.d.y, shE.d.z, shE.tmax);
-        Q.shC[2][se] = make_float4(shE.c.x, shE.c.y, shE.c.z, __int_as_float(slot));
+      const int sa = warpPush(&Q.counters[iter * kCountersPerIter + C_SHA], shA.on);
+      if (sa >= 0) {
+        Q.shO[0][sa] = make_float4(shA.o.x, shA.o.y, shA.o.z, __int_as_float(pid));
+        Q.shD[0][sa] = make_float4(shA.d.x, shA.d.y, shA.d.z, shA.tmax);
+        Q.shC[0][sa] = make_float4(shA.c.x, shA.c.y, shA.c.z, __int_as_float(slot));
       }
-    }
-    if (MEDL == 2) {
-      const int sv = warpPush(&Q.counters[iter * kCountersPerIter + C_SHD], shV.on);
-      if (sv >= 0) {
-        Q.shO[3][sv] = make_float4(shV.o.x, shV.o.y, shV.o.z, __int_as_float(pid));
-        Q.shD[3][sv] = make_float4(shV.d.x, shV.d.y, shV.d.z, shV.tmax);
-        Q.shC[3][sv] = make_float4(shV.c.x, shV.c.y, shV.c.z, __int_as_float(slot));
+      const int sb = warpPush(&Q.counters[iter * kCountersPerIter + C_SHB], shB.on);
+      if (sb >= 0) {
+        Q.shO[1][sb] = make_float4(shB.o.x, shB.o.y, shB.o.z, __int_as_float(pid));
+        Q.shD[1][sb] = make_float4(shB.d.x, shB.d.y, shB.d.z, shB.tmax);
+        Q.shC[1][sb] = make_float4(shB.c.x, shB.c.y, shB.c.z, __int_as_float(slot));
+      }
+      if (ENV) {
+        const int se = warpPush(&Q.counters[iter * kCountersPerIter + C_SHC], shE.on);
+        if (se >= 0) {
+          Q.shO[2][se] = make_float4(shE.o.x, shE.o.y, shE.o.z, __int_as_float(pid));
+          Q.shD[2][se] = make_float4(shE.d.x, shE.d.y, shE.d.z, shE.tmax);
+          Q.shC[2][se] = make_float4(shE.c.x, shE.c.y, shE.c.z, __int_as_float(slot));
+        }
+      }
+      if (MEDL == 2) {
+        const int sv = warpPush(&Q.counters[iter * kCountersPerIter + C_SHD], shV.on);
+        if (sv >= 0) {
+          Q.shO[3][sv] = make_float4(shV.o.x, shV.o.y, shV.o.z, __int_as_float(pid));
+          Q.shD[3][sv] = make_float4(shV.d.x, shV.d.y, shV.d.z, shV.tmax);
+          Q.shC[3][sv] = make_float4(shV.c.x, shV.c.y, shV.c.z, __int_as_float(slot));
+        }
       }
     }
   }

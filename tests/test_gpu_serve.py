@@ -84,7 +84,7 @@ def test_autotuner_config_is_valid_and_keeps_results(rg):
     scenes = _scenes(rg, 4, seed0=300)
     probe = [(sc, 48, 48, 4, 5, 10 + k) for k, sc in enumerate(scenes)]
     t = rg.RenderServer.autotune(probe, max_resident_jobs=8)
-    assert t["paths_per_wave"] in {1 << p for p in range(18, 24)}
+    assert t["paths_per_wave"] in {1 << p for p in range(20, 27)}  # the autotuner's candidates, 1 Mi .. 64 Mi
     assert t["shade_blocks_per_sm"] in {0, 2, 4, 8, 16} and t["trace_blocks_per_sm"] in {0, 2, 4, 6}
     assert t["probe_ms"] > 0
     out = []
