@@ -10,9 +10,10 @@
 //  * continuous batching: every wave takes a share of paths from every
 //    resident job (one segment per job in the wave table), so jobs that
 //    arrive while others are in flight join the next wave;
-//  * completion: a job whose samples are all traced is resolved (optionally
-//    A-Trous denoised) and tonemapped on the device, read back, and its
-//    memory and slot are released.
+//  * completion: a job whose samples are all traced is handed to a finisher
+//    thread with a stream of its own, which resolves it (optionally denoises
+//    it) on the device, reads it back and releases its memory and slot while
+//    the next waves render.
 // The per-path RNG is keyed by (job seed, pixel, sample), never by slot or
 // wave, so a job's image does not depend on the mix it was rendered in.
 #include <cuda_fp16.h>
@@ -95,6 +96,9 @@ struct rg_server {
   bool stop = false;
   std::thread worker;
   std::vector<std::thread> admitters;
+  std::thread finisher;                // resolves, denoises and reads back finished jobs
+  std::deque<ServerJob*> finishing;    // jobs whose last wave has run, for the finisher
+  cudaStream_t finishStream = nullptr;
   cudaStream_t stream = nullptr;
   std::vector<cudaStream_t> admitStreams;
   int numSMs = 148;
@@ -125,6 +129,7 @@ struct rg_server {
     if (hostSegs) cudaFreeHost(hostSegs);
     if (hostWave) cudaFreeHost(hostWave);
     if (stream) cudaStreamDestroy(stream);
+    if (finishStream) cudaStreamDestroy(finishStream);
     for (auto a : admitStreams) cudaStreamDestroy(a);
   }
 };
@@ -254,8 +259,7 @@ rg_status admit(rg_server* s, ServerJob* j, cudaStream_t st) {
   return RG_OK;
 }
 
-void finishJob(rg_server* s, ServerJob* j) {
-  cudaStream_t st = s->stream;
+void finishJob(rg_server* s, ServerJob* j, cudaStream_t st) {
   const int N = j->pixels;
   launchResolve(N, j->sum.p, j->cnt.p, j->R.exposure, j->hdr.p, st);
   rg_status dres = RG_OK;
@@ -326,6 +330,32 @@ void admitLoop(rg_server* s, int idx) {
   }
 }
 
+// Finisher thread: the job's last wave has completed (the wave thread synchronised
+// its stream), so the resolve, denoiser and read-back run on a stream of their
+// own while the next waves render; the job then completes and frees its slot.
+void finishLoop(rg_server* s) {
+  for (;;) {
+    ServerJob* j = nullptr;
+    {
+      std::unique_lock<std::mutex> lk(s->mu);
+      while (s->finishing.empty()) {
+        if (s->stop) return;
+        s->cv.wait_for(lk, std::chrono::milliseconds(20));
+      }
+      j = s->finishing.front();
+      s->finishing.pop_front();
+    }
+    if (j->error == RG_OK) finishJob(s, j, s->finishStream);
+    std::lock_guard<std::mutex> lk(s->mu);
+    j->state = j->error == RG_OK ? RG_JOB_DONE : RG_JOB_FAILED;
+    j->tDone = nowMs();
+    s->latencies.push_back(j->tDone - j->tSubmit);
+    s->lastDone = j->tDone;
+    releaseJob(s, j);
+    s->cv.notify_all();
+  }
+}
+
 void serverLoop(rg_server* s) {
   cudaStream_t st = s->stream;
   int rr = 0;
@@ -333,9 +363,9 @@ void serverLoop(rg_server* s) {
     {
       std::unique_lock<std::mutex> lk(s->mu);
       if (s->stop) return;
-      bool work = false;
+      bool work = false;  // resident jobs with samples left (finished ones wait for the finisher)
       for (auto* j : s->slotJob)
-        if (j && j->state == RG_JOB_RESIDENT) work = true;
+        if (j && j->state == RG_JOB_RESIDENT && j->issuedSamples < j->desc.samples) work = true;
       if (!work) {
         s->cv.wait_for(lk, std::chrono::milliseconds(20));
         continue;
@@ -432,14 +462,9 @@ void serverLoop(rg_server* s) {
           if (j->issuedSamples >= j->desc.samples) finished.push_back(j);
         }
       }
-      for (auto* j : finished) {
-        if (j->error == RG_OK) finishJob(s, j);
+      if (!finished.empty()) {  // to the finisher; the next wave does not wait for the read-back
         std::lock_guard<std::mutex> lk(s->mu);
-        j->state = j->error == RG_OK ? RG_JOB_DONE : RG_JOB_FAILED;
-        j->tDone = nowMs();
-        s->latencies.push_back(j->tDone - j->tSubmit);
-        s->lastDone = j->tDone;
-        releaseJob(s, j);
+        for (auto* j : finished) s->finishing.push_back(j);
         s->cv.notify_all();
       }
     }
@@ -448,7 +473,8 @@ void serverLoop(rg_server* s) {
     {
       std::lock_guard<std::mutex> lk(s->mu);
       for (auto* j : s->slotJob)
-        if (j && j->snapshotRequested && j->state == RG_JOB_RESIDENT) snaps.push_back(j);
+        if (j && j->snapshotRequested && j->state == RG_JOB_RESIDENT && j->issuedSamples < j->desc.samples)
+          snaps.push_back(j);  // a finished job's waiter gets its result from the finisher
     }
     for (auto* j : snaps) {
       launchResolve(j->pixels, j->sum.p, j->cnt.p, j->R.exposure, j->hdr.p, st);
@@ -502,7 +528,8 @@ rg_status rg_server_create(const rg_settings* base, const rg_server_config* cfg,
   int dev = 0;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&s->numSMs, cudaDevAttrMultiProcessorCount, dev);
-  bool streamsOk = cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking) == cudaSuccess;
+  bool streamsOk = cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking) == cudaSuccess &&
+                   cudaStreamCreateWithFlags(&s->finishStream, cudaStreamNonBlocking) == cudaSuccess;
   for (int i = 0; i < kAdmitThreads && streamsOk; i++) {
     cudaStream_t a = nullptr;
     streamsOk = cudaStreamCreateWithFlags(&a, cudaStreamNonBlocking) == cudaSuccess;
@@ -517,6 +544,7 @@ rg_status rg_server_create(const rg_settings* base, const rg_server_config* cfg,
   s->slotJob.assign(s->cfg.max_resident_jobs, nullptr);
   for (int i = s->cfg.max_resident_jobs - 1; i >= 0; i--) s->freeSlots.push_back(i);
   s->worker = std::thread(serverLoop, s);
+  s->finisher = std::thread(finishLoop, s);
   for (int i = 0; i < (int)s->admitStreams.size(); i++) s->admitters.emplace_back(admitLoop, s, i);
   *out = s;
   return RG_OK;
@@ -724,6 +752,7 @@ rg_status rg_server_destroy(rg_server* s) {
     s->cv.notify_all();
   }
   if (s->worker.joinable()) s->worker.join();
+  if (s->finisher.joinable()) s->finisher.join();
   for (auto& t : s->admitters)
     if (t.joinable()) t.join();
   cudaDeviceSynchronize();
