@@ -306,13 +306,32 @@ rg_status rg_trace_any(rg_handle* h, const float* rays, const float* tmax, int32
  *       bent ray's origin and direction; bendRay, medium.cpp:237-274). */
 rg_status rg_medium_eval(rg_handle* h, int32_t medium, const float* points, int32_t n, float* out);
 rg_status rg_medium_bend(rg_handle* h, int32_t medium, const float* rays, int32_t n, float* out);
+/* Sampling-helper probes (device work, host pointers), one row per input;
+ * each row runs the device function the shade kernel uses:
+ *   0 sampleGGXVNDF      <- bsdf.cpp:139-161  in (Ve xyz, ax, ay, u1, u2) -> H xyz
+ *   1 smithG1            <- bsdf.cpp:164-170  in (w xyz, ax, ay)          -> G1
+ *   2 fresnelSchlick     <- bsdf.cpp:32-37    in (cosTheta, ior)          -> F
+ *   3 refract            <- bsdf.cpp:39-52    in (d xyz, n xyz, ior)      -> dir xyz
+ *   4 buildTangentFrame  <- bsdf.cpp:129-135  in (n xyz)                  -> t xyz, b xyz
+ *   5 cosineWeightedDirection <- raycommon.cpp:94-115, on LDS dims dim, dim+1
+ *                              in (x, y, sample, dim, n xyz)           -> dir xyz
+ *   6 ldsPointInTriangle <- raycommon.cpp:117-122, on LDS dims dim, dim+1
+ *                              in (x, y, sample, dim, v1 v2 v3 xyz)    -> p xyz
+ *   7 ldsNext1D          <- raycommon.cpp:71-87 in (x, y, sample, dim) -> u
+ *   8 samplePhase (HG)   <- medium.cpp:496-517  in (wo xyz, g, u1, u2)   -> wi xyz
+ *   9 phasePdf (HG)      <- medium.cpp:519-525  in (wo xyz, wi xyz, g)   -> pdf
+ *  10 sampleFreeFlight   <- medium.cpp:475-480  in (sigma_t hero, u)     -> t
+ * LDS rows use seed 1 (the reference's unsalted scramble). */
+rg_status rg_probe_sampling(int32_t which, const float* in, int32_t n, float* out);
 /* View-space camera transform the scene was flattened with (4x4 row-major,
  * row-vector convention: p_view = [p 1] * M). */
 rg_status rg_get_view_matrix(rg_handle* h, float* m16);
 
 /* Stand-alone post passes on caller buffers (device work, host pointers).
  * color/out: w*h*3 floats; normal/albedo: w*h*3 (encoded as the AOVs);
- * albedo_alpha: w*h floats (1 = geometry hit); depth: w*h floats. */
+ * albedo_alpha: w*h floats (1 = geometry hit); depth: w*h floats.
+ * levels in [1, 16] (the settings' denoise_levels obeys the same bound), and
+ * w*h*3 at most INT_MAX; otherwise RG_ERR_INVALID_ARGUMENT. */
 rg_status rg_denoise_atrous(int32_t w, int32_t h, const float* color, const float* normal,
                             const float* depth, const float* albedo, const float* albedo_alpha,
                             int32_t levels, float sigma_color, float sigma_normal,
@@ -329,17 +348,24 @@ rg_status rg_denoise_atrous(int32_t w, int32_t h, const float* color, const floa
  *   normal, albedo: w*h*3 floats; depth, albedo_alpha: w*h floats (device).
  *   stream: a cudaStream_t, NULL for the default stream.  The work is
  *   enqueued on it and the call returns; out_rgba is ready when it completes.
- * Limit: w*h <= 1,048,576 pixels, else RG_ERR_INVALID_ARGUMENT.  Host or
- * foreign-device pointers give RG_ERR_INVALID_ARGUMENT.  Buffer sizes cannot
+ * Limit: w*h <= 1,048,576 pixels and levels in [1, 16], else
+ * RG_ERR_INVALID_ARGUMENT.  Host or foreign-device pointers, and an out_rgba
+ * that overlaps any input, give RG_ERR_INVALID_ARGUMENT.  Buffer sizes cannot
  * be checked: each must hold w*h elements of the layout above.
  * Calls whose device work overlaps (other streams, unsynchronised threads)
- * share the working buffers and race; serialise them.  The first call on a
- * device resolves the working array's address; make it before any stream
- * capture begins.  Results equal rg_denoise_atrous on the same inputs. */
+ * share the working buffers and race; serialise them.  The first call in a
+ * CUDA context (once per device, and again after a device reset) resolves the
+ * working array's address; make it before any stream capture begins.
+ * Results equal rg_denoise_atrous on the same inputs bit for bit. */
 rg_status rg_denoise_atrous_noalloc(int32_t w, int32_t h, const float* color_rgba, const float* normal,
                                     const float* depth, const float* albedo, const float* albedo_alpha,
                                     int32_t levels, float sigma_color, float sigma_normal,
                                     float sigma_depth, float intensity, float* out_rgba, void* stream);
+/* Test hook of the no-allocation entry point's address cache, which is keyed
+ * by CUDA context id: runs ids[0..n) through a fresh cache (no CUDA call) and
+ * writes whether each lookup had to resolve (1) or hit (0), and the ordinal
+ * of the address returned.  No reference counterpart. */
+rg_status rg_noalloc_cache_probe(const uint64_t* ids, int32_t n, int32_t* out_resolved, int32_t* out_slot);
 rg_status rg_tonemap(int32_t w, int32_t h, const float* hdr_rgba, float* ldr_rgba);
 /* Energy-based HDR bloom on caller buffers (device work, host pointers):
  * out = hdr + strength * blur(excess luminance above threshold), w*h RGBA. */

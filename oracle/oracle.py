@@ -76,12 +76,101 @@ def load(fast: bool = False) -> C.CDLL:
     lib.orc_volume_nee.argtypes = [C.c_void_p, f, f, C.c_int32, C.c_uint32, f, f, f, P(C.c_uint8)]
     lib.orc_num_volume_lights.restype = C.c_int32
     lib.orc_num_volume_lights.argtypes = [C.c_void_p]
+    vp = C.c_void_p
+    lib.orc_bsdf_probe.argtypes = [C.c_int32, vp, C.c_int32, vp]
+    lib.orc_cosine_direction.argtypes = [C.c_int32] * 4 + [vp, vp]
+    lib.orc_point_in_triangle.argtypes = [C.c_int32] * 4 + [vp, vp]
+    lib.orc_view_triangles.argtypes = [vp, vp, vp]
+    lib.orc_num_triangles.restype = C.c_int32
+    lib.orc_num_triangles.argtypes = [vp]
+    lib.orc_medium_probe.argtypes = [vp, C.c_int32, C.c_int32, vp, C.c_int32, vp]
     _libs[name] = lib
     return lib
 
 
+# Output widths of the probes (the reference harness uses the same layouts).
+BSDF_OUT_WIDTH = (3, 1, 1, 3, 6)
+MEDIUM_OUT_WIDTH = (3, 1, 3, 1, 5, 6)
+
+
+def bsdf_probe(which: int, x) -> np.ndarray:
+    """sampleGGXVNDF / smithG1 / fresnelSchlick / refract / buildTangentFrame rows."""
+    lib = load()
+    x = np.ascontiguousarray(x, np.float32)
+    y = np.zeros((len(x), BSDF_OUT_WIDTH[which]), np.float32)
+    lib.orc_bsdf_probe(which, x.ctypes.data, len(x), y.ctypes.data)
+    return y
+
+
+def lds_probe(rows) -> np.ndarray:
+    """LDS value of rows (x, y, sample, dim) with seed 1."""
+    lib = load()
+    return np.array([lib.orc_lds(int(r[0]), int(r[1]), 1 << 16, int(r[2]), 1, int(r[3])) for r in rows], np.float32)
+
+
+def cosine_probe(rows) -> np.ndarray:
+    """cosineWeightedDirection on LDS dims dim, dim+1 of rows (x, y, sample, dim, n xyz)."""
+    lib = load()
+    out = np.zeros((len(rows), 3), np.float32)
+    for i, r in enumerate(rows):
+        nrm = np.ascontiguousarray(r[4:7], np.float32)
+        lib.orc_cosine_direction(int(r[0]), int(r[1]), int(r[2]), int(r[3]), nrm.ctypes.data, out[i].ctypes.data)
+    return out
+
+
+def triangle_point_probe(rows) -> np.ndarray:
+    """ldsPointInTriangle on LDS dims dim, dim+1 of rows (x, y, sample, dim, triangle 9)."""
+    lib = load()
+    out = np.zeros((len(rows), 3), np.float32)
+    for i, r in enumerate(rows):
+        t9 = np.ascontiguousarray(r[4:13], np.float32)
+        lib.orc_point_in_triangle(int(r[0]), int(r[1]), int(r[2]), int(r[3]), t9.ctypes.data, out[i].ctypes.data)
+    return out
+
+
+def view_triangles(desc_ptr):
+    """The flattened view-space triangles (positions, vertex normals; n x 9 each)
+    in the reference's DFS order, as the oracle flattens the scene."""
+    o = OracleScene(desc_ptr)
+    try:
+        return o.view_triangles()
+    finally:
+        o.close()
+
+
 def _fp(a):
     return a.ctypes.data_as(C.POINTER(C.c_float))
+
+
+class CpuScene:
+    """A seeded procedural scene (rg_scene_builtin's kinds) built on the CPU by
+    libscenegen.so, for the CPU-only timing arm; `ptr` is an rg_scene_desc*."""
+
+    def __init__(self, kind: int, seed: int = 1, iparams=None):
+        path = os.path.join(HERE, "libscenegen.so")
+        if not os.path.exists(path):
+            build()
+        self.lib = C.CDLL(path)
+        self.lib.og_scene_builtin.restype = C.c_int32
+        self.lib.og_scene_builtin.argtypes = [C.c_int32, C.c_uint32, C.POINTER(C.c_int32), C.c_int32,
+                                              C.POINTER(C.c_void_p)]
+        self.lib.og_scene_free.restype = C.c_int32
+        self.lib.og_scene_free.argtypes = [C.c_void_p]
+        ip = (C.c_int32 * max(1, len(iparams or [])))(*(iparams or [0]))
+        out = C.c_void_p()
+        rc = self.lib.og_scene_builtin(kind, seed, ip, len(iparams or []), C.byref(out))
+        if rc != 0:
+            raise RuntimeError(f"og_scene_builtin({kind}) failed: {rc}")
+        self.ptr = out.value
+
+    def num_triangles(self) -> int:
+        # rg_scene_desc starts with int32 num_triangles
+        return C.cast(self.ptr, C.POINTER(C.c_int32))[0]
+
+    def close(self):
+        if self.ptr:
+            self.lib.og_scene_free(self.ptr)
+            self.ptr = None
 
 
 class OracleScene:
@@ -101,6 +190,19 @@ class OracleScene:
             self.close()
         except Exception:
             pass
+
+    def view_triangles(self):
+        n = self.lib.orc_num_triangles(self.h)
+        pos = np.zeros((n, 9), np.float32)
+        nrm = np.zeros((n, 9), np.float32)
+        self.lib.orc_view_triangles(self.h, pos.ctypes.data, nrm.ctypes.data)
+        return pos, nrm
+
+    def medium_probe(self, m: int, which: int, x) -> np.ndarray:
+        x = np.ascontiguousarray(x, np.float32)
+        y = np.zeros((len(x), MEDIUM_OUT_WIDTH[which]), np.float32)
+        self.lib.orc_medium_probe(self.h, m, which, x.ctypes.data, len(x), y.ctypes.data)
+        return y
 
     def bvh_nodes(self) -> int:
         return self.lib.orc_bvh_nodes(self.h)

@@ -251,6 +251,7 @@ def load_library(path: str = LIB_PATH) -> C.CDLL:
         "rg_reapply_postprocess": (C.c_int, [C.c_void_p]),
         "rg_medium_defaults": (None, [P(rg_medium)]),
         "rg_medium_eval": (C.c_int, [C.c_void_p, C.c_int32, P(C.c_float), C.c_int32, P(C.c_float)]),
+        "rg_probe_sampling": (C.c_int, [C.c_int32, P(C.c_float), C.c_int32, P(C.c_float)]),
         "rg_medium_bend": (C.c_int, [C.c_void_p, C.c_int32, P(C.c_float), C.c_int32, P(C.c_float)]),
         "rg_scene_builtin": (C.c_int, [C.c_int32, C.c_uint32, P(C.c_int32), C.c_int32, P(P(rg_scene_desc))]),
         "rg_scene_free": (C.c_int, [P(rg_scene_desc)]),
@@ -663,6 +664,21 @@ def denoise_atrous(color, normal, depth, albedo, albedo_alpha, levels=5, sigma_c
     _check(lib.rg_denoise_atrous(w, h, _fptr(color), _fptr(args[0]), _fptr(args[1]), _fptr(args[2]),
                                  _fptr(args[3]), levels, sigma_color, sigma_normal, sigma_depth,
                                  intensity, _fptr(out)))
+    return out
+
+
+# Output widths of rg_probe_sampling's rows (see the C header for the layouts).
+PROBE_OUT_WIDTH = (3, 1, 1, 3, 6, 3, 3, 1, 3, 1, 1)
+PROBE_VNDF, PROBE_SMITH, PROBE_SCHLICK, PROBE_REFRACT, PROBE_FRAME, PROBE_COSINE, PROBE_TRIANGLE_POINT, \
+    PROBE_LDS, PROBE_PHASE_SAMPLE, PROBE_PHASE_PDF, PROBE_FREE_FLIGHT = range(11)
+
+
+def probe_sampling(which: int, rows: np.ndarray) -> np.ndarray:
+    """Run one of the shade kernel's sampling helpers on the device, one row per input."""
+    lib = load_library()
+    x = np.ascontiguousarray(rows, np.float32)
+    out = np.empty((x.shape[0], PROBE_OUT_WIDTH[which]), np.float32)
+    _check(lib.rg_probe_sampling(which, _fptr(x), x.shape[0], _fptr(out)))
     return out
 
 

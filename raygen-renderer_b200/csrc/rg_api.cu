@@ -11,6 +11,7 @@
 
 #include <algorithm>
 #include <chrono>
+#include <climits>
 #include <cstdlib>
 #include <unordered_map>
 #include <cmath>
@@ -503,6 +504,10 @@ rg_status rg_create(const rg_settings* s, rg_handle** out) {
     setLastError("no CUDA device");
     return RG_ERR_NO_DEVICE;
   }
+  if (s && (s->denoise_levels < 1 || s->denoise_levels > kMaxDenoiseLevels)) {
+    setLastError("rg_create: denoise_levels must be in [1, " + std::to_string(kMaxDenoiseLevels) + "]");
+    return RG_ERR_INVALID_ARGUMENT;
+  }
   rg_handle* h = new (std::nothrow) rg_handle();
   if (!h) return RG_ERR_OUT_OF_MEMORY;
   if (s) h->st = *s;
@@ -532,6 +537,10 @@ rg_status rg_destroy(rg_handle* h) {
 
 rg_status rg_update_settings(rg_handle* h, const rg_settings* s) {
   if (!h || !s) return RG_ERR_INVALID_ARGUMENT;
+  if (s->denoise_levels < 1 || s->denoise_levels > kMaxDenoiseLevels) {
+    setLastError("rg_update_settings: denoise_levels must be in [1, " + std::to_string(kMaxDenoiseLevels) + "]");
+    return RG_ERR_INVALID_ARGUMENT;
+  }
   std::lock_guard<std::mutex> lk(h->mu);
   h->st = *s;
   return RG_OK;
@@ -1408,6 +1417,24 @@ rg_status rg_medium_bend(rg_handle* h, int32_t medium, const float* rays, int32_
   return mediumQuery(h, medium, true, rays, n, out);
 }
 
+rg_status rg_probe_sampling(int32_t which, const float* in, int32_t n, float* out) {
+  static const int kInW[11] = {7, 5, 2, 7, 3, 7, 13, 4, 6, 7, 2};
+  static const int kOutW[11] = {3, 1, 1, 3, 6, 3, 3, 1, 3, 1, 1};
+  if (which < 0 || which > 10 || n < 0 || (n > 0 && (!in || !out))) return RG_ERR_INVALID_ARGUMENT;
+  if (n == 0) return RG_OK;
+  int dc = 0;
+  if (cudaGetDeviceCount(&dc) != cudaSuccess || dc == 0) {
+    cudaGetLastError();
+    return RG_ERR_NO_DEVICE;
+  }
+  DevBuf<float> din, dout;
+  if (!din.upload(in, (size_t)n * kInW[which], 0) || !dout.alloc((size_t)n * kOutW[which])) return RG_ERR_OUT_OF_MEMORY;
+  launchProbeSampling(which, din.p, n, dout.p, 0);
+  RG_CUDA_CHECK(cudaGetLastError());
+  RG_CUDA_CHECK(cudaMemcpy(out, dout.p, sizeof(float) * (size_t)n * kOutW[which], cudaMemcpyDeviceToHost));
+  return RG_OK;
+}
+
 rg_status rg_get_view_matrix(rg_handle* h, float* m16) {
   if (!h || !m16) return RG_ERR_INVALID_ARGUMENT;
   std::memcpy(m16, h->view.m, sizeof(float) * 16);
@@ -1461,12 +1488,21 @@ rg_status rg_denoise_atrous(int32_t w, int32_t h, const float* color, const floa
                             const float* albedo, const float* albedo_alpha, int32_t levels, float sigma_color,
                             float sigma_normal, float sigma_depth, float intensity, float* out) {
   if (w <= 0 || h <= 0 || !color || !normal || !depth || !albedo || !albedo_alpha || !out) return RG_ERR_INVALID_ARGUMENT;
+  if (levels < 1 || levels > kMaxDenoiseLevels) {
+    setLastError("rg_denoise_atrous: levels must be in [1, " + std::to_string(kMaxDenoiseLevels) + "]");
+    return RG_ERR_INVALID_ARGUMENT;
+  }
+  const size_t nPix = (size_t)w * (size_t)h;
+  if (nPix * 3 > (size_t)INT_MAX) {
+    setLastError("rg_denoise_atrous: image of " + std::to_string(nPix) + " pixels is too large");
+    return RG_ERR_INVALID_ARGUMENT;
+  }
   int dc = 0;
   if (cudaGetDeviceCount(&dc) != cudaSuccess || dc == 0) {
     cudaGetLastError();
     return RG_ERR_NO_DEVICE;
   }
-  const int N = w * h;
+  const int N = (int)nPix;
   std::vector<float4> c4(N);
   for (int i = 0; i < N; i++) c4[i] = make_float4(color[i * 3], color[i * 3 + 1], color[i * 3 + 2], 1.0f);
   DevBuf<float4> c, a, b, o;

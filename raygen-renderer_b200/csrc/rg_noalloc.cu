@@ -27,12 +27,16 @@
 //  * Nothing in the working buffers has to start at zero: every pass writes
 //    each pixel of its destination before any later pass reads it, so no
 //    clearing is done between calls.
-//  * The first call on a device resolves the array's device address
-//    (cudaGetSymbolAddress, which may load this module); make that first
-//    call before any stream capture begins.
+//  * The first call in a CUDA context (per device, and again after a device
+//    reset) resolves the array's device address (cudaGetSymbolAddress, which
+//    may load this module); make that first call before any stream capture
+//    begins.
+//  * levels in [1, 16]; out_rgba may not overlap any input.
+#include <cuda.h>
 #include <cuda_fp16.h>
 #include <cuda_runtime.h>
 
+#include <climits>
 #include <mutex>
 #include <string>
 
@@ -61,13 +65,89 @@ static_assert(kOffB % 256 == 0 && kOffNormal % 256 == 0 && kOffAlbedo % 256 == 0
 
 static __device__ __align__(256) unsigned char g_atrousScratch[kScratchBytes];
 
-constexpr int kMaxDevices = 64;
-std::mutex g_setupMu;
-unsigned char* g_scratchOnDevice[kMaxDevices] = {};
+// Working-array addresses by CUDA context id.  Bounded: when full, the oldest
+// entry (most likely a context that no longer exists) is dropped.
+class ScratchCache {
+ public:
+  static constexpr int kEntries = 64;
+  unsigned char* find(unsigned long long id) const {
+    for (int i = 0; i < n_; ++i)
+      if (ids_[i] == id) return ptrs_[i];
+    return nullptr;
+  }
+  void insert(unsigned long long id, unsigned char* p) {
+    int slot;
+    if (n_ < kEntries) {
+      slot = n_++;
+    } else {
+      slot = next_;
+      next_ = (next_ + 1) % kEntries;
+    }
+    ids_[slot] = id;
+    ptrs_[slot] = p;
+  }
 
-// Device address of the working array on the current device, resolved once
-// per device (with that device current).
-rg_status scratchForCurrentDevice(unsigned char** out) {
+ private:
+  unsigned long long ids_[kEntries] = {};
+  unsigned char* ptrs_[kEntries] = {};
+  int n_ = 0;
+  int next_ = 0;
+};
+
+// The array's device address belongs to the CUDA context the module was
+// loaded into: a device reset, or a second (non-primary) context on the same
+// device, loads the module again at another address.  So the cache is keyed
+// by the context's process-unique id (cuCtxGetId), not by device ordinal; an
+// id is never reused, so an entry of a destroyed context can never match.
+// The driver functions come through cudaGetDriverEntryPoint, so the library
+// needs no link against libcuda.
+using CtxGetCurrentFn = CUresult (*)(CUcontext*);
+using CtxGetIdFn = CUresult (*)(CUcontext, unsigned long long*);
+
+std::mutex g_setupMu;
+ScratchCache g_cache;
+
+rg_status currentContextId(unsigned long long* id) {
+  static CtxGetCurrentFn getCurrent = nullptr;
+  static CtxGetIdFn getId = nullptr;
+  if (!getCurrent || !getId) {
+    void* a = nullptr;
+    void* b = nullptr;
+    cudaDriverEntryPointQueryResult qa, qb;
+    if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &a, cudaEnableDefault, &qa) != cudaSuccess ||
+        cudaGetDriverEntryPoint("cuCtxGetId", &b, cudaEnableDefault, &qb) != cudaSuccess ||
+        qa != cudaDriverEntryPointSuccess || qb != cudaDriverEntryPointSuccess || !a || !b) {
+      cudaGetLastError();
+      setLastError("rg_denoise_atrous_noalloc: the driver does not provide cuCtxGetCurrent / cuCtxGetId");
+      return RG_ERR_CUDA;
+    }
+    getCurrent = reinterpret_cast<CtxGetCurrentFn>(a);
+    getId = reinterpret_cast<CtxGetIdFn>(b);
+  }
+  CUcontext ctx = nullptr;
+  if (getCurrent(&ctx) != CUDA_SUCCESS || !ctx) return RG_ERR_NO_DEVICE;
+  if (getId(ctx, id) != CUDA_SUCCESS) {
+    setLastError("rg_denoise_atrous_noalloc: cuCtxGetId failed");
+    return RG_ERR_CUDA;
+  }
+  return RG_OK;
+}
+
+rg_status resolveScratch(unsigned char** out) {
+  void* p = nullptr;
+  const cudaError_t e = cudaGetSymbolAddress(&p, g_atrousScratch);
+  if (e != cudaSuccess || !p) {
+    cudaGetLastError();
+    setLastError(std::string("rg_denoise_atrous_noalloc: cudaGetSymbolAddress failed: ") + cudaGetErrorString(e));
+    return RG_ERR_CUDA;
+  }
+  *out = static_cast<unsigned char*>(p);
+  return RG_OK;
+}
+
+// Device address of the working array in the current context, resolved once
+// per context (with that context current).
+rg_status scratchForCurrentContext(unsigned char** out) {
   int dev = -1;
   cudaError_t e = cudaGetDevice(&dev);
   if (e != cudaSuccess) {
@@ -75,23 +155,35 @@ rg_status scratchForCurrentDevice(unsigned char** out) {
     setLastError(std::string("rg_denoise_atrous_noalloc: no current CUDA device: ") + cudaGetErrorString(e));
     return RG_ERR_NO_DEVICE;
   }
-  if (dev < 0 || dev >= kMaxDevices) {
-    setLastError("rg_denoise_atrous_noalloc: device ordinal out of range");
-    return RG_ERR_NO_DEVICE;
-  }
   std::lock_guard<std::mutex> lk(g_setupMu);
-  if (!g_scratchOnDevice[dev]) {
-    void* p = nullptr;
-    e = cudaGetSymbolAddress(&p, g_atrousScratch);
-    if (e != cudaSuccess || !p) {
-      cudaGetLastError();
-      setLastError(std::string("rg_denoise_atrous_noalloc: cudaGetSymbolAddress failed: ") + cudaGetErrorString(e));
-      return RG_ERR_CUDA;
-    }
-    g_scratchOnDevice[dev] = static_cast<unsigned char*>(p);
+  unsigned long long id = 0;
+  rg_status rs = currentContextId(&id);
+  if (rs == RG_ERR_NO_DEVICE) {
+    // No context is current yet on this thread: the runtime makes the
+    // device's primary context current on its first call that needs one, and
+    // resolving the symbol is such a call.
+    unsigned char* p = nullptr;
+    rs = resolveScratch(&p);
+    if (rs != RG_OK) return rs;
+    rs = currentContextId(&id);
+    if (rs == RG_ERR_NO_DEVICE) setLastError("rg_denoise_atrous_noalloc: no CUDA context is current");
   }
-  *out = g_scratchOnDevice[dev];
+  if (rs != RG_OK) return rs;
+  if (unsigned char* hit = g_cache.find(id)) {
+    *out = hit;
+    return RG_OK;
+  }
+  unsigned char* p = nullptr;
+  rs = resolveScratch(&p);
+  if (rs != RG_OK) return rs;
+  g_cache.insert(id, p);
+  *out = p;
   return RG_OK;
+}
+
+bool overlaps(const void* a, size_t an, const void* b, size_t bn) {
+  const uintptr_t x = reinterpret_cast<uintptr_t>(a), y = reinterpret_cast<uintptr_t>(b);
+  return x < y + bn && y < x + an;
 }
 
 // A caller pointer must be device (or managed) memory visible on the current
@@ -134,8 +226,12 @@ extern "C" rg_status rg_denoise_atrous_noalloc(int32_t w, int32_t h, const float
                  " pixels; use rg_denoise_atrous");
     return RG_ERR_INVALID_ARGUMENT;
   }
+  if (levels < 1 || levels > kMaxDenoiseLevels) {
+    setLastError("rg_denoise_atrous_noalloc: levels must be in [1, " + std::to_string(kMaxDenoiseLevels) + "]");
+    return RG_ERR_INVALID_ARGUMENT;
+  }
   unsigned char* s = nullptr;
-  const rg_status rs = scratchForCurrentDevice(&s);
+  const rg_status rs = scratchForCurrentContext(&s);
   if (rs != RG_OK) return rs;
   int dev = 0;
   cudaGetDevice(&dev);
@@ -143,6 +239,18 @@ extern "C" rg_status rg_denoise_atrous_noalloc(int32_t w, int32_t h, const float
       !deviceBuffer(normal, 4, dev, "normal") || !deviceBuffer(depth, 4, dev, "depth") ||
       !deviceBuffer(albedo, 4, dev, "albedo") || !deviceBuffer(albedo_alpha, 4, dev, "albedo_alpha"))
     return RG_ERR_INVALID_ARGUMENT;
+  // The output is written while the colour input is still read (the last pass
+  // reads the noisy colour beside the filtered one), so it may not share
+  // memory with any input.
+  const size_t outBytes = n * sizeof(float4);
+  if (overlaps(out_rgba, outBytes, color_rgba, n * sizeof(float4)) ||
+      overlaps(out_rgba, outBytes, normal, n * 3 * sizeof(float)) ||
+      overlaps(out_rgba, outBytes, albedo, n * 3 * sizeof(float)) ||
+      overlaps(out_rgba, outBytes, depth, n * sizeof(float)) ||
+      overlaps(out_rgba, outBytes, albedo_alpha, n * sizeof(float))) {
+    setLastError("rg_denoise_atrous_noalloc: out_rgba overlaps an input buffer");
+    return RG_ERR_INVALID_ARGUMENT;
+  }
   cudaStream_t st = static_cast<cudaStream_t>(stream);
   float4* bufA = reinterpret_cast<float4*>(s + kOffA);
   float4* bufB = reinterpret_cast<float4*>(s + kOffB);
@@ -161,6 +269,29 @@ extern "C" rg_status rg_denoise_atrous_noalloc(int32_t w, int32_t h, const float
   if (e != cudaSuccess) {
     setLastError(std::string("rg_denoise_atrous_noalloc: launch failed: ") + cudaGetErrorString(e));
     return RG_ERR_CUDA;
+  }
+  return RG_OK;
+}
+
+// Test hook for the context-keyed address cache (no CUDA call): feeds a
+// sequence of context ids through a fresh cache whose resolver hands out a new
+// address per resolve, and reports for each lookup whether it resolved
+// (out_resolved[i] = 1) and which address it returned (out_slot[i], the
+// resolve's ordinal).  No reference counterpart.
+extern "C" rg_status rg_noalloc_cache_probe(const uint64_t* ids, int32_t n, int32_t* out_resolved, int32_t* out_slot) {
+  using namespace rg;
+  if (n < 0 || (n > 0 && (!ids || !out_resolved || !out_slot))) return RG_ERR_INVALID_ARGUMENT;
+  ScratchCache cache;
+  int32_t resolves = 0;
+  for (int32_t i = 0; i < n; ++i) {
+    unsigned char* hit = cache.find(ids[i]);
+    out_resolved[i] = hit ? 0 : 1;
+    if (!hit) {
+      // stand-in addresses 1, 2, 3, ...: the ordinal of the resolve
+      hit = reinterpret_cast<unsigned char*>(static_cast<uintptr_t>(++resolves));
+      cache.insert(ids[i], hit);
+    }
+    out_slot[i] = (int32_t)reinterpret_cast<uintptr_t>(hit);
   }
   return RG_OK;
 }

@@ -513,6 +513,10 @@ rg_status rg_server_create(const rg_settings* base, const rg_server_config* cfg,
     setLastError("no CUDA device");
     return RG_ERR_NO_DEVICE;
   }
+  if (base && (base->denoise_levels < 1 || base->denoise_levels > kMaxDenoiseLevels)) {
+    setLastError("rg_server_create: denoise_levels must be in [1, " + std::to_string(kMaxDenoiseLevels) + "]");
+    return RG_ERR_INVALID_ARGUMENT;
+  }
   rg_server* s = new (std::nothrow) rg_server();
   if (!s) return RG_ERR_OUT_OF_MEMORY;
   keepPoolMemory();

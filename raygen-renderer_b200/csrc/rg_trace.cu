@@ -74,6 +74,105 @@ __device__ __forceinline__ V3 randomRayInHemisphere(V3 n, float u1, float u2) {
   return d;
 }
 
+// buildTangentFrame: bsdf.cpp:129-135
+__device__ __forceinline__ void buildTangentFrame(V3 n, V3& t, V3& b) {
+  const V3 up = fabsf(n.y) > 0.99f ? v3(1, 0, 0) : v3(0, 1, 0);
+  t = normalize(cross(up, n));
+  b = cross(n, t);
+}
+
+// smithG1 for anisotropic GGX in the local frame: bsdf.cpp:164-170
+__device__ __forceinline__ float smithG1(V3 w, float ax, float ay) {
+  if (w.z <= 0.0f) return 0.0f;
+  const float ax2 = (ax * w.x) * (ax * w.x), ay2 = (ay * w.y) * (ay * w.y);
+  const float lambda = 0.5f * (sqrtf(1.0f + (ax2 + ay2) / (w.z * w.z)) - 1.0f);
+  return 1.0f / (1.0f + lambda);
+}
+
+// sampleGGXVNDF (Heitz 2018): bsdf.cpp:139-161; Ve is the local view direction
+__device__ __forceinline__ V3 sampleGGXVNDF(V3 Ve, float ax, float ay, float u1, float u2) {
+  const V3 Vh = normalize(v3(ax * Ve.x, ay * Ve.y, Ve.z));
+  const float lensq = Vh.x * Vh.x + Vh.y * Vh.y;
+  const V3 T1 = lensq > 0.0f ? v3(-Vh.y, Vh.x, 0.0f) * (1.0f / sqrtf(lensq)) : v3(1, 0, 0);
+  const V3 T2 = cross(Vh, T1);
+  const float rr = sqrtf(u1);
+  float sphi, cphi;
+  sincosf(2.0f * kPi * u2, &sphi, &cphi);
+  const float t1 = rr * cphi;
+  float t2 = rr * sphi;
+  const float sw = 0.5f * (1.0f + Vh.z);
+  t2 = (1.0f - sw) * sqrtf(fmaxf(0.0f, 1.0f - t1 * t1)) + sw * t2;
+  const V3 Nh = T1 * t1 + T2 * t2 + Vh * sqrtf(fmaxf(0.0f, 1.0f - t1 * t1 - t2 * t2));
+  return normalize(v3(ax * Nh.x, ay * Nh.y, fmaxf(0.0f, Nh.z)));
+}
+
+// fresnelSchlick: bsdf.cpp:32-37
+__device__ __forceinline__ float fresnelSchlick(float cosTheta, float ior) {
+  float r0 = (1.0f - ior) / (1.0f + ior);
+  r0 = r0 * r0;
+  const float mm = 1.0f - cosTheta;
+  return r0 + (1.0f - r0) * (mm * mm) * (mm * mm) * mm;
+}
+
+// refract: bsdf.cpp:39-52 (total internal reflection -> reflect)
+__device__ __forceinline__ V3 refractDir(V3 d, V3 n, float ior) {
+  const V3 nl = dot(d, n) < 0.0f ? n : -n;
+  const bool into = dot(nl, n) > 0.0f;
+  const float rr = into ? 1.0f / ior : ior;
+  const float c = dot(d, nl);
+  const float tt = 1.0f - rr * rr * (1.0f - c * c);
+  if (tt < 0.0f) return reflect(d, n);
+  return normalize(d * rr - n * ((into ? 1.0f : -1.0f) * (c * rr + sqrtf(tt))));
+}
+
+// ldsPointInTriangle: raycommon.cpp:117-122 (u, w: two LDS draws)
+__device__ __forceinline__ V3 ldsPointInTriangle(V3 v1, V3 v2, V3 v3, float u, float w) {
+  if (u + w > 1.0f) {
+    u = 1.0f - u;
+    w = 1.0f - w;
+  }
+  return v1 + (v2 - v1) * u + (v3 - v1) * w;
+}
+
+// sampleFreeFlight: medium.cpp:475-480 (hero: the mean of sigma_t)
+__device__ __forceinline__ float sampleFreeFlight(float hero, float u) {
+  if (hero <= 0.0f) return 1e30f;
+  const float xi = fminf(0.9999999f, fmaxf(0.0f, u));
+  return -logf(1.0f - xi) / hero;
+}
+
+// Henyey-Greenstein samplePhase around the travel direction wo: medium.cpp:496-517,
+// with coordSystem (:482-494)
+__device__ __forceinline__ V3 samplePhaseHG(V3 wo, float g, float u1, float u2) {
+  float cosTheta;
+  if (fabsf(g) < 1e-3f) {
+    cosTheta = 1.0f - 2.0f * u1;
+  } else {
+    const float sq = (1.0f - g * g) / (1.0f - g + 2.0f * g * u1);
+    cosTheta = (1.0f + g * g - sq * sq) / (2.0f * g);
+  }
+  const float sinTheta = sqrtf(fmaxf(0.0f, 1.0f - cosTheta * cosTheta));
+  float sp, cp;
+  sincosf(2.0f * kPi * u2, &sp, &cp);
+  V3 t1;
+  if (fabsf(wo.x) > fabsf(wo.y)) {
+    const float inv = 1.0f / sqrtf(wo.x * wo.x + wo.z * wo.z);
+    t1 = v3(-wo.z * inv, 0.0f, wo.x * inv);
+  } else {
+    const float inv = 1.0f / sqrtf(wo.y * wo.y + wo.z * wo.z);
+    t1 = v3(0.0f, wo.z * inv, -wo.y * inv);
+  }
+  const V3 t2 = cross(wo, t1);
+  return normalize(t1 * (sinTheta * cp) + t2 * (sinTheta * sp) + wo * cosTheta);
+}
+
+// Henyey-Greenstein phasePdf: medium.cpp:519-525
+__device__ __forceinline__ float phasePdfHG(V3 wo, V3 wi, float g) {
+  const float cosT = dot(wo, wi);
+  const float den = 1.0f + g * g - 2.0f * g * cosT;
+  return (1.0f - g * g) * (1.0f / (4.0f * kPi)) / (den * sqrtf(fmaxf(1e-8f, den)));
+}
+
 __device__ __forceinline__ float srgbToLinear(float c) {  // texture.cpp:204-207
   if (c <= 0.04045f) return c * (1.0f / 12.92f);
   return powf((c + 0.055f) * (1.0f / 1.055f), 2.4f);
@@ -151,9 +250,7 @@ __device__ bool pickAreaLight(const DevScene& S, const Rng& rng, int v, int ligh
   const float4 a = __ldg(lt), b = __ldg(lt + 1), c = __ldg(lt + 2);
   const float4 na = __ldg(lt + 3), nb = __ldg(lt + 4), nc = __ldg(lt + 5);
   const V3 v1 = xyz(a), v2 = xyz(b), v3_ = xyz(c);
-  float u = rng.lds(rng.neeDim(v)), w = rng.lds(rng.neeDim(v) + 1);  // ldsPointInTriangle
-  if (u + w > 1.0f) { u = 1.0f - u; w = 1.0f - w; }
-  ls.p = v1 + (v2 - v1) * u + (v3_ - v1) * w;
+  ls.p = ldsPointInTriangle(v1, v2, v3_, rng.lds(rng.neeDim(v)), rng.lds(rng.neeDim(v) + 1));
   // calcVertexInterpolation(tri, p): rayrenderer.cpp:2337-2352
   const V3 f1 = v1 - ls.p, f2 = v2 - ls.p, f3 = v3_ - ls.p;
   const V3 c1 = cross(f2, f3), c2 = cross(f3, f1), c3 = cross(f1, f2);
@@ -974,8 +1071,7 @@ __global__ void __launch_bounds__(256) k_shade(DevScene S0, DevRender R0, const 
             tF = col.hit ? col.t : maxT;
             dens = col.density;
           } else {
-            const float xi = fminf(0.9999999f, fmaxf(0.0f, rng.prng(v, S_FLIGHT)));
-            tF = -logf(1.0f - xi) / M.hero;
+            tF = sampleFreeFlight(M.hero, rng.prng(v, S_FLIGHT));
             scat = tF < maxT;
           }
           const float el = scat ? tF : maxT;
@@ -1003,12 +1099,7 @@ __global__ void __launch_bounds__(256) k_shade(DevScene S0, DevRender R0, const 
               const V3 proxy = -d;
               V3 lDir, Le;
               float pl;
-              auto phaseTo = [&](V3 w) {  // HG phasePdf (medium.cpp:519-525)
-                const float g = M.g;
-                const float cosT = dot(-d, w);
-                const float den = 1.0f + g * g - 2.0f * g * cosT;
-                return (1.0f - g * g) * (1.0f / (4.0f * kPi)) / (den * sqrtf(fmaxf(1e-8f, den)));
-              };
+              auto phaseTo = [&](V3 w) { return phasePdfHG(-d, w, M.g); };
               if (sampleAreaLightForNEE(S, R, rng, v, pos, proxy, lDir, pl, Le, shA) && pl > 0.0f) {
                 shA.on = true;
                 shA.c = beta * sw * Le * (phaseTo(lDir) / pl);
@@ -1030,22 +1121,7 @@ __global__ void __launch_bounds__(256) k_shade(DevScene S0, DevRender R0, const 
                   shV.c = beta * sw * vs.Le * (phaseTo(vs.dir) / vs.pdf);
                 }
               }
-              // samplePhase: medium.cpp:496-517
-              const float u1 = rng.prng(v, S_PHASE0), u2 = rng.prng(v, S_PHASE1);
-              float cosTheta;
-              if (fabsf(M.g) < 1e-3f) cosTheta = 1.0f - 2.0f * u1;
-              else {
-                const float sq = (1.0f - M.g * M.g) / (1.0f - M.g + 2.0f * M.g * u1);
-                cosTheta = (1.0f + M.g * M.g - sq * sq) / (2.0f * M.g);
-              }
-              const float sinTheta = sqrtf(fmaxf(0.0f, 1.0f - cosTheta * cosTheta));
-              float sp, cp;
-              sincosf(2.0f * kPi * u2, &sp, &cp);
-              V3 t1;
-              if (fabsf(d.x) > fabsf(d.y)) { const float inv = 1.0f / sqrtf(d.x * d.x + d.z * d.z); t1 = v3(-d.z * inv, 0.0f, d.x * inv); }
-              else { const float inv = 1.0f / sqrtf(d.y * d.y + d.z * d.z); t1 = v3(0.0f, d.z * inv, -d.y * inv); }
-              const V3 t2 = cross(d, t1);
-              const V3 ndir = normalize(t1 * (sinTheta * cp) + t2 * (sinTheta * sp) + d * cosTheta);
+              const V3 ndir = samplePhaseHG(d, M.g, rng.prng(v, S_PHASE0), rng.prng(v, S_PHASE1));
               const V3 rrBase = eye ? v3(1, 1, 1) : rrT;
               float rrW = 1.0f;
               bool killed = false;
@@ -1232,9 +1308,8 @@ __global__ void __launch_bounds__(256) k_shade(DevScene S0, DevRender R0, const 
                 no = surfaceOrigin(h.p, r, gN);
                 nd = r;
               } else {
-                const V3 up = fabsf(h.n.y) > 0.99f ? v3(1, 0, 0) : v3(0, 1, 0);
-                V3 t = normalize(cross(up, h.n));
-                V3 b = cross(h.n, t);
+                V3 t, b;
+                buildTangentFrame(h.n, t, b);
                 if (fabsf(m.anisoRot) > 0.0f) {
                   float sa, ca;
                   sincosf(m.anisoRot * (kPi / 180.0f), &sa, &ca);
@@ -1251,13 +1326,7 @@ __global__ void __launch_bounds__(256) k_shade(DevScene S0, DevRender R0, const 
                 if (Vl.z <= 0.0f) {
                   done = true;
                 } else {
-                  auto smithG1 = [&](V3 w) {
-                    if (w.z <= 0.0f) return 0.0f;
-                    const float ax2 = (ax * w.x) * (ax * w.x), ay2 = (ay * w.y) * (ay * w.y);
-                    const float lambda = 0.5f * (sqrtf(1.0f + (ax2 + ay2) / (w.z * w.z)) - 1.0f);
-                    return 1.0f / (1.0f + lambda);
-                  };
-                  const float G1v = smithG1(Vl);
+                  const float G1v = smithG1(Vl, ax, ay);
                   // evalGlossy (bsdf.cpp:260-280): f*cos_L and the VNDF pdf toward dw
                   auto evalGlossy = [&](V3 dw, V3& fCos, float& pb) {
                     const V3 Ll = v3(dot(dw, t), dot(dw, b), dot(dw, h.n));
@@ -1271,7 +1340,7 @@ __global__ void __launch_bounds__(256) k_shade(DevScene S0, DevRender R0, const 
                     const float hx = Hl.x / ax, hy = Hl.y / ay;
                     const float den = hx * hx + hy * hy + Hl.z * Hl.z;
                     const float D = 1.0f / (kPi * ax * ay * den * den);
-                    fCos = schlick(VdotH) * (D * G1v * smithG1(Ll) / (4.0f * Vl.z));
+                    fCos = schlick(VdotH) * (D * G1v * smithG1(Ll, ax, ay) / (4.0f * Vl.z));
                     pb = G1v * D / (4.0f * Vl.z);
                     return true;
                   };
@@ -1303,19 +1372,7 @@ __global__ void __launch_bounds__(256) k_shade(DevScene S0, DevRender R0, const 
                   }
                   // VNDF sample (bsdf.cpp:139-161, 319-373)
                   const float u1 = rng.prng(v, S_VNDF0), u2 = rng.prng(v, S_VNDF1);
-                  const V3 Vh = normalize(v3(ax * Vl.x, ay * Vl.y, Vl.z));
-                  const float lensq = Vh.x * Vh.x + Vh.y * Vh.y;
-                  const V3 T1 = lensq > 0.0f ? v3(-Vh.y, Vh.x, 0.0f) * (1.0f / sqrtf(lensq)) : v3(1, 0, 0);
-                  const V3 T2 = cross(Vh, T1);
-                  const float rr = sqrtf(u1);
-                  float sphi, cphi;
-                  sincosf(2.0f * kPi * u2, &sphi, &cphi);
-                  const float t1 = rr * cphi;
-                  float t2 = rr * sphi;
-                  const float sw = 0.5f * (1.0f + Vh.z);
-                  t2 = (1.0f - sw) * sqrtf(fmaxf(0.0f, 1.0f - t1 * t1)) + sw * t2;
-                  const V3 Nh = T1 * t1 + T2 * t2 + Vh * sqrtf(fmaxf(0.0f, 1.0f - t1 * t1 - t2 * t2));
-                  const V3 H = normalize(v3(ax * Nh.x, ay * Nh.y, fmaxf(0.0f, Nh.z)));
+                  const V3 H = sampleGGXVNDF(Vl, ax, ay, u1, u2);
                   const V3 Ll = H * (2.0f * dot(Vl, H)) - Vl;
                   if (Ll.z <= 0.0f) {
                     done = true;
@@ -1325,7 +1382,7 @@ __global__ void __launch_bounds__(256) k_shade(DevScene S0, DevRender R0, const 
                       done = true;
                     } else {
                       const V3 F = schlick(fmaxf(0.0f, dot(Vl, H)));
-                      const V3 wgt = F * smithG1(Ll);
+                      const V3 wgt = F * smithG1(Ll, ax, ay);
                       const float hx = H.x / ax, hy = H.y / ay;
                       const float den = hx * hx + hy * hy + H.z * H.z;
                       const float D = 1.0f / (kPi * ax * ay * den * den);
@@ -1353,23 +1410,9 @@ __global__ void __launch_bounds__(256) k_shade(DevScene S0, DevRender R0, const 
                 else if (chroma == 2) ior = m.ior * (1.0f + m.chroma);
                 if (first) mask = chroma == 0 ? v3(3, 0, 0) : (chroma == 1 ? v3(0, 3, 0) : v3(0, 0, 3));
               }
-              float r0 = (1.0f - ior) / (1.0f + ior);
-              r0 = r0 * r0;
-              const float mm = 1.0f - cosTheta;
-              const float F = r0 + (1.0f - r0) * (mm * mm) * (mm * mm) * mm;
+              const float F = fresnelSchlick(cosTheta, ior);
               const bool pickReflect = rng.prng(v, S_FRESNEL) < F;
-              V3 dir;
-              if (pickReflect) {
-                dir = reflect(d, h.n);
-              } else {  // refract (bsdf.cpp:39-52)
-                const V3 nl = dot(d, h.n) < 0.0f ? h.n : -h.n;
-                const bool into = dot(nl, h.n) > 0.0f;
-                const float rr = into ? 1.0f / ior : ior;
-                const float c = dot(d, nl);
-                const float tt = 1.0f - rr * rr * (1.0f - c * c);
-                if (tt < 0.0f) dir = reflect(d, h.n);
-                else dir = normalize(d * rr - h.n * ((into ? 1.0f : -1.0f) * (c * rr + sqrtf(tt))));
-              }
+              V3 dir = pickReflect ? reflect(d, h.n) : refractDir(d, h.n, ior);
               if (m.roughness > 0.0f)
                 dir = normalize(dir + randomRayInHemisphere(h.n, rng.prng(v, S_HEMI0), rng.prng(v, S_HEMI1)) * m.roughness);
               if (pickReflect && dot(dir, gN) <= 0.0f) dir = reflect(d, gN);
@@ -1731,6 +1774,90 @@ void launchAov(const DevScene& S, const DevRender& R, __half* normal, __half* al
   const int n = R.width * R.height;
   k_aov<<<(n + 127) / 128, 128, 0, st>>>(S, R, normal, albedo, albedoA, depth);
 }
+// Sampling-helper probes: each row runs one of the device functions the shade
+// kernel uses, on the row's inputs (layouts in rg_probe_sampling's header).
+__global__ void k_probeSampling(int which, const float* __restrict__ in, int n, float* __restrict__ out) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  auto put3 = [&](float* o, V3 v) {
+    o[0] = v.x;
+    o[1] = v.y;
+    o[2] = v.z;
+  };
+  auto rngOf = [&](const float* a) {
+    Rng r;
+    r.init((uint32_t)a[0], (uint32_t)a[1], 1u << 16, (uint32_t)a[2], 1u, 0);
+    return r;
+  };
+  switch (which) {
+    case 0: {
+      const float* a = in + (size_t)i * 7;
+      put3(out + (size_t)i * 3, sampleGGXVNDF(v3(a[0], a[1], a[2]), a[3], a[4], a[5], a[6]));
+      break;
+    }
+    case 1: {
+      const float* a = in + (size_t)i * 5;
+      out[i] = smithG1(v3(a[0], a[1], a[2]), a[3], a[4]);
+      break;
+    }
+    case 2:
+      out[i] = fresnelSchlick(in[i * 2], in[i * 2 + 1]);
+      break;
+    case 3: {
+      const float* a = in + (size_t)i * 7;
+      put3(out + (size_t)i * 3, refractDir(v3(a[0], a[1], a[2]), v3(a[3], a[4], a[5]), a[6]));
+      break;
+    }
+    case 4: {
+      const float* a = in + (size_t)i * 3;
+      V3 t, b;
+      buildTangentFrame(v3(a[0], a[1], a[2]), t, b);
+      put3(out + (size_t)i * 6, t);
+      put3(out + (size_t)i * 6 + 3, b);
+      break;
+    }
+    case 5: {
+      const float* a = in + (size_t)i * 7;
+      const Rng r = rngOf(a);
+      const int dim = (int)a[3];
+      put3(out + (size_t)i * 3, cosineWeightedDirection(v3(a[4], a[5], a[6]), r.lds(dim), r.lds(dim + 1)));
+      break;
+    }
+    case 6: {
+      const float* a = in + (size_t)i * 13;
+      const Rng r = rngOf(a);
+      const int dim = (int)a[3];
+      put3(out + (size_t)i * 3, ldsPointInTriangle(v3(a[4], a[5], a[6]), v3(a[7], a[8], a[9]), v3(a[10], a[11], a[12]),
+                                                  r.lds(dim), r.lds(dim + 1)));
+      break;
+    }
+    case 7: {
+      const float* a = in + (size_t)i * 4;
+      out[i] = rngOf(a).lds((int)a[3]);
+      break;
+    }
+    case 8: {
+      const float* a = in + (size_t)i * 6;
+      put3(out + (size_t)i * 3, samplePhaseHG(v3(a[0], a[1], a[2]), a[3], a[4], a[5]));
+      break;
+    }
+    case 9: {
+      const float* a = in + (size_t)i * 7;
+      out[i] = phasePdfHG(v3(a[0], a[1], a[2]), v3(a[3], a[4], a[5]), a[6]);
+      break;
+    }
+    case 10:
+      out[i] = sampleFreeFlight(in[i * 2], in[i * 2 + 1]);
+      break;
+    default:
+      break;
+  }
+}
+
+void launchProbeSampling(int which, const float* in, int n, float* out, cudaStream_t st) {
+  k_probeSampling<<<(n + 127) / 128, 128, 0, st>>>(which, in, n, out);
+}
+
 void launchQueryClosest(const DevScene& S, const float* rays, int n, float* tuv, int* prim, cudaStream_t st) {
   if (n > 0) k_queryClosest<<<(n + 127) / 128, 128, 0, st>>>(S, rays, n, tuv, prim);
 }

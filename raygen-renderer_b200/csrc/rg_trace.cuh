@@ -28,10 +28,14 @@ void launchAov(const DevScene& S, const DevRender& R, __half* normal, __half* al
 void launchQueryClosest(const DevScene& S, const float* rays, int n, float* tuv, int* prim, cudaStream_t st);
 void launchQueryAny(const DevScene& S, const float* rays, const float* tmax, int n, uint32_t occ, uint8_t* out,
                     cudaStream_t st);
+// sampling-helper probes (rg_probe_sampling)
+void launchProbeSampling(int which, const float* in, int n, float* out, cudaStream_t st);
 // jobs[0].S is the scene; eval: n x 3 points -> n x 5, bend: n x 7 rays -> n x 6
 void launchMediumQuery(const DevJob* jobs, int medium, bool bend, const float* in, int n, float* out, cudaStream_t st);
 
 // post (rg_post.cu)
+// A-Trous levels accepted by the entry points (step 2^l stays far inside int)
+constexpr int kMaxDenoiseLevels = 16;
 void launchResolve(int n, const float4* sum, const int* cnt, float exposure, float4* hdr, cudaStream_t st);
 void launchDenoise(int w, int h, const float4* noisy, const __half* normal, const __half* depth, const __half* albedo,
                    const __half* albedoA, int levels, float sigC, float sigN, float sigD, float intensity,

@@ -102,3 +102,52 @@ def test_null_arguments_are_rejected(rg):
 
 def test_version_string(rg):
     assert "raygen" in rg.version()
+
+
+def test_noalloc_address_cache_is_keyed_by_context(rg):
+    """The no-allocation A-Trous entry point caches its working array's device
+    address per CUDA context id (a reset or a second context on the same
+    device loads the module at another address).  The cache logic runs here
+    on fake ids, with no CUDA call."""
+    lib = rg.load_library()
+    f = lib.rg_noalloc_cache_probe
+    f.restype = C.c_int32
+    f.argtypes = [C.c_void_p, C.c_int32, C.c_void_p, C.c_void_p]
+    # ctx 7 (device 0), a reset gives ctx 9 on the same device, back to 7 is a hit;
+    # then 70 distinct contexts overflow the 64-entry table, which drops the oldest
+    ids = [7, 7, 9, 9, 7] + list(range(100, 170)) + [7, 169]
+    ids = np.array(ids, np.uint64)
+    n = len(ids)
+    resolved = np.zeros(n, np.int32)
+    slot = np.zeros(n, np.int32)
+    assert f(ids.ctypes.data, n, resolved.ctypes.data, slot.ctypes.data) == 0
+    assert list(resolved[:5]) == [1, 0, 1, 0, 0]
+    assert list(slot[:5]) == [1, 1, 2, 2, 1]
+    assert resolved[5:75].all()  # every new context resolves once
+    assert resolved[75] == 1 and slot[75] == 73  # ctx 7 was evicted; resolves afresh
+    assert resolved[76] == 0 and slot[76] == slot[74]  # the newest entry is still cached
+    assert f(None, -1, None, None) == rg.RG_ERR_INVALID_ARGUMENT
+
+
+@pytest.mark.parametrize("kind,iparams", [(1, None), (2, [2000]), (4, [3000, 5])])
+def test_cpu_scene_generator_matches_the_library(rg, orc, kind, iparams):
+    """The CPU timing arm builds its scenes with oracle/libscenegen.so (the
+    same generator source, host-compiled); the arrays must equal the library's."""
+    import oracle
+    a = rg.Scene.builtin(kind, 3, iparams)
+    b = oracle.CpuScene(kind, 3, iparams)
+    db = C.cast(C.c_void_p(b.ptr), C.POINTER(rg.rg_scene_desc)).contents
+    da = a.desc
+    n = da.num_triangles
+    assert db.num_triangles == n == b.num_triangles()
+    for f, w in (("positions", 9), ("normals", 9)):
+        x = np.ctypeslib.as_array(getattr(da, f), shape=(n, w))
+        y = np.ctypeslib.as_array(getattr(db, f), shape=(n, w))
+        assert np.array_equal(x.view(np.uint32), y.view(np.uint32)), f
+    assert np.array_equal(np.ctypeslib.as_array(da.tri_mesh, shape=(n,)), np.ctypeslib.as_array(db.tri_mesh, shape=(n,)))
+    assert da.num_materials == db.num_materials and da.num_objects == db.num_objects
+    for i in range(da.num_materials):
+        assert bytes(da.materials[i]) == bytes(db.materials[i])
+    assert bytes(da.camera) == bytes(db.camera)
+    a.close()
+    b.close()

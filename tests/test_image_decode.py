@@ -16,7 +16,10 @@ import pytest
 
 import image_codecs as ic
 
-REF_TEXTURES = "/root/reference/resources/textures"
+# The reference project's texture folder (resources/textures of its checkout),
+# when one is available: RAYGEN_REFERENCE_ROOT names the checkout's root.
+REF_TEXTURES = os.path.join(os.environ.get("RAYGEN_REFERENCE_ROOT", ""), "resources", "textures") \
+    if os.environ.get("RAYGEN_REFERENCE_ROOT") else ""
 
 
 def _png_case(rng, ctype, depth, H=13, W=17):
@@ -147,7 +150,8 @@ def test_jpeg_refuses_progressive_and_garbage(rg, tmp_path):
         rg.load_image(str(q))
 
 
-@pytest.mark.skipif(not os.path.isdir(REF_TEXTURES), reason="the reference's texture files are not on this machine")
+@pytest.mark.skipif(not REF_TEXTURES or not os.path.isdir(REF_TEXTURES),
+                    reason="RAYGEN_REFERENCE_ROOT does not name a reference checkout with its textures")
 def test_reference_textures_decode(rg):
     """The reference's own JPEG textures: a grey checkerboard, and 4:2:0 images
     with restart intervals (only where the reference tree is present)."""

@@ -4,7 +4,9 @@ entry point rg_denoise_atrous on the same inputs.
 
 The file sorts last so that, in a full run, the no-alloc path also runs after
 every other GPU test of the process; it passes alone in a fresh process too.
-Tolerance as for the other deterministic passes: 1e-4 relative + 1e-6 absolute.
+Both entry points run the same kernels on the same inputs, so their outputs
+must be equal bit for bit (the allocating entry point is itself checked
+against the CPU oracle within 1e-4 relative in test_gpu_post.py).
 """
 import ctypes as C
 
@@ -59,7 +61,7 @@ def test_noalloc_matches_allocating_entry_point(rg):
         rc, got = run_noalloc(f, torch, inputs, stream.cuda_stream)
         assert rc == 0, lib.rg_last_error()
         ref = rg.denoise_atrous(*inputs)
-        np.testing.assert_allclose(got[..., :3], ref, rtol=1e-4, atol=1e-6)
+        np.testing.assert_array_equal(got[..., :3], ref)
         assert np.all(got[..., 3] == 1.0)
 
 
@@ -71,7 +73,7 @@ def test_noalloc_default_stream_and_parameters(rg):
     rc, got = run_noalloc(f, torch, inputs, None, levels=3, params=(0.8, 64.0, 0.2, 0.6))
     assert rc == 0, lib.rg_last_error()
     ref = rg.denoise_atrous(*inputs, levels=3, sigma_color=0.8, sigma_normal=64.0, sigma_depth=0.2, intensity=0.6)
-    np.testing.assert_allclose(got[..., :3], ref, rtol=1e-4, atol=1e-6)
+    np.testing.assert_array_equal(got[..., :3], ref)
 
 
 def test_noalloc_rejects_oversize_and_host_buffers(rg):
@@ -92,3 +94,28 @@ def test_noalloc_rejects_oversize_and_host_buffers(rg):
     rc = f(4, 4, hp, p, p, p, p, 5, 0.4, 128.0, 0.1, 1.0, p, None)
     assert rc == rg.RG_ERR_INVALID_ARGUMENT
     assert b"not device memory" in lib.rg_last_error()
+
+
+def test_noalloc_rejects_bad_levels_and_aliased_output(rg):
+    torch = pytest.importorskip("torch")
+    lib = rg.load_library()
+    f = bind(lib)
+    dev = torch.device("cuda:0")
+    h, w = 8, 8
+    color = torch.zeros((h, w, 4), dtype=torch.float32, device=dev)
+    guides = torch.zeros((h, w, 3), dtype=torch.float32, device=dev)
+    depth = torch.zeros((h, w), dtype=torch.float32, device=dev)
+    out = torch.zeros((h, w, 4), dtype=torch.float32, device=dev)
+    args = [color.data_ptr(), guides.data_ptr(), depth.data_ptr(), guides.data_ptr(), depth.data_ptr()]
+    for levels in (0, -1, 17, 1 << 20):
+        rc = f(w, h, *args, levels, 0.4, 128.0, 0.1, 1.0, out.data_ptr(), None)
+        assert rc == rg.RG_ERR_INVALID_ARGUMENT
+        assert b"levels" in lib.rg_last_error()
+    # the output may not share memory with an input (here: the colour itself)
+    rc = f(w, h, *args, 5, 0.4, 128.0, 0.1, 1.0, color.data_ptr(), None)
+    assert rc == rg.RG_ERR_INVALID_ARGUMENT
+    assert b"overlaps" in lib.rg_last_error()
+    # a valid call still succeeds afterwards
+    rc = f(w, h, *args, 5, 0.4, 128.0, 0.1, 1.0, out.data_ptr(), None)
+    torch.cuda.synchronize()
+    assert rc == 0, lib.rg_last_error()
