@@ -221,3 +221,60 @@ def sky_image(W=64, H=32, sun=(0.62, 0.27), sun_radius=0.03, sun_level=80.0, see
     img[d < sun_radius] = sun_level
     img *= (1.0 + 0.05 * rng.standard_normal((H, W, 1))).astype(np.float32)
     return np.maximum(img, 0).astype(np.float32)
+
+
+# ---------------------------------------------------------------- GGX furnace
+def ggx_directional_albedo(mu_o, ax, ay, n=1536):
+    """White-furnace known answer: the directional albedo of the GGX lobe with
+    Fresnel 1, E(v) = integral over the hemisphere of D(h) G1(v) G1(l) / (4 v.z)
+    dw_l (Smith separable, bsdf.cpp:260-280), by midpoint quadrature in
+    (cos theta_l, phi_l).  v lies in the x-z plane at cos theta = mu_o."""
+    v = np.array([np.sqrt(max(0.0, 1.0 - mu_o * mu_o)), 0.0, mu_o])
+    mu = (np.arange(n) + 0.5) / n
+    phi = (np.arange(2 * n) + 0.5) / (2 * n) * 2 * np.pi
+    M, P = np.meshgrid(mu, phi, indexing="ij")
+    s = np.sqrt(1.0 - M * M)
+    lx, ly, lz = s * np.cos(P), s * np.sin(P), M
+    hx, hy, hz = lx + v[0], ly + v[1], lz + v[2]
+    hn = np.sqrt(hx * hx + hy * hy + hz * hz)
+    hx, hy, hz = hx / hn, hy / hn, hz / hn
+    den = (hx / ax) ** 2 + (hy / ay) ** 2 + hz * hz
+    D = 1.0 / (np.pi * ax * ay * den * den)
+
+    def g1(wx, wy, wz):
+        lam = 0.5 * (np.sqrt(1.0 + ((ax * wx) ** 2 + (ay * wy) ** 2) / (wz * wz)) - 1.0)
+        return 1.0 / (1.0 + lam)
+
+    f = D * g1(v[0], v[1], v[2]) * g1(lx, ly, lz) / (4.0 * v[2])
+    f[hz <= 0] = 0.0
+    return float(f.sum() * (1.0 / n) * (2 * np.pi / (2 * n)))
+
+
+def furnace_scene(rg, roughness, anisotropy=0.0, tilt_deg=0.0):
+    """A white GGX metal quad (F0 = 1) filling a narrow camera's view inside a
+    constant environment of radiance 1: the image mean is the lobe's
+    directional albedo at cos(tilt)."""
+    p, nrm = quad_z(-5.0, 1.5, +1)
+    if tilt_deg:
+        c, s_ = math.cos(math.radians(tilt_deg)), math.sin(math.radians(tilt_deg))
+        R = np.array([[1, 0, 0], [0, c, -s_], [0, s_, c]], np.float32)
+        centre = np.array([0, 0, -5.0], np.float32)
+        p = ((p.reshape(-1, 3) - centre) @ R.T + centre).reshape(-1, 9).astype(np.float32)
+        nrm = (nrm.reshape(-1, 3) @ R.T).reshape(-1, 9).astype(np.float32)
+    m = material(rg, (1, 1, 1), glossy=1.0, roughness=roughness, metallic=1.0)
+    m.anisotropy = anisotropy
+    env = np.ones((8, 16, 4), np.float32)
+    o = rg.rg_object()
+    o.material = 0
+    o.interior_medium = -1
+    return rg.Scene.from_arrays(p, nrm, [0, 0], [0], [o], [m], camera(rg, fov=6.0), textures=[(env, True)], envmap=0)
+
+
+FURNACE_CASES = [(0.5, 0.0, 0.0), (0.8, 0.0, 0.0), (0.7, 0.6, 0.0), (0.6, 0.0, 60.0)]
+
+
+def furnace_expected(roughness, anisotropy, tilt_deg):
+    r2 = roughness * roughness
+    a = max(-0.99, min(0.99, anisotropy))
+    ax, ay = max(1e-3, r2 * (1 - a)), max(1e-3, r2 * (1 + a))
+    return ggx_directional_albedo(math.cos(math.radians(tilt_deg)), ax, ay)

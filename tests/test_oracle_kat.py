@@ -147,3 +147,17 @@ def test_atrous_identities(orc):
     noisy = rng.random((h, w, 3)).astype(np.float32)
     passthrough = orc.denoise(noisy, normal, depth, albedo, alpha, intensity=0.0)
     assert np.allclose(passthrough, noisy)
+
+
+@pytest.mark.parametrize("roughness,anisotropy,tilt", scenes.FURNACE_CASES)
+def test_ggx_white_furnace(rg, orc, roughness, anisotropy, tilt):
+    """GGX white furnace (energy check): a white metal (F0 = 1) quad in a
+    constant environment of radiance 1 reflects the lobe's directional albedo,
+    computed independently by quadrature (isotropic and anisotropic, normal and
+    60-degree incidence)."""
+    sc = scenes.furnace_scene(rg, roughness, anisotropy, tilt)
+    img = orc.OracleScene(sc.ptr).render(24, 24, 64, max_depth=8, rr_depth=3, seed=3, firefly_clamp=0.0)
+    mean = float(img["hdr"][..., :3].mean())
+    expected = scenes.furnace_expected(roughness, anisotropy, tilt)
+    assert abs(mean - expected) < 0.012 * expected, (mean, expected)
+    sc.close()

@@ -272,3 +272,27 @@ def test_errors(rg, tmp_path):
     # an unterminated root object is closed at the end of the input
     sc = load(rg, tmp_path, '{ "a": { "mesh": { "type": "plane" } }\n// }\n', "open.json")
     assert sc.desc.num_triangles == 2
+
+
+def test_branch_scenes_take_their_branches(rg, tmp_path):
+    """The scenes of the device branch-parity tests (test_gpu_parity_configs.py)
+    load with the materials, lights and camera those tests rely on (no GPU)."""
+    from test_gpu_parity_configs import BRANCH_SCENES
+    for name, doc in BRANCH_SCENES.items():
+        p = tmp_path / f"{name}.json"
+        p.write_text(json.dumps(doc))
+        d = rg.Scene.from_json(str(p)).desc
+        mats = [d.materials[i] for i in range(d.num_materials)]
+        cam = d.camera
+        if name == "anisotropic_ggx":
+            assert sum(abs(mm.anisotropy) > 0.4 for mm in mats) == 3 and any(mm.aniso_rotation != 0 for mm in mats)
+        if name == "rough_dielectric":
+            assert sum(mm.refraction > 0.5 and mm.roughness > 0.1 for mm in mats) == 3
+        if name == "dispersion":
+            assert sum(mm.chroma_dispersion > 0 for mm in mats) == 2
+        if name.startswith("thin_lens"):
+            assert cam.depth_of_field > 0 and cam.aperture > 0
+            assert cam.aperture_blades == (6 if "blades" in name else 0)
+        if name == "thin_lens_blades_spot":
+            assert d.num_point_lights == 2
+            assert sum(mm.spot_range > 0 for mm in mats) == 1
