@@ -15,6 +15,9 @@
  *   rg_render              <- RayRenderer::render         src/raygen/rayrenderer.cpp:478-596
  *   rg_set_progress_cb     <- RayRenderer::progressCallback src/raygen/rayrenderer.h:317
  *   rg_cancel              <- RayRenderer::cancelRequested  src/raygen/rayrenderer.h:427
+ *   rg_render_async, rg_poll, rg_wait, rg_job_free
+ *                          <- the threaded RayRenderer::render + progressCallback
+ *                             src/raygen/rayrenderer.cpp:748-809
  *   rg_get_hdr             <- RayRenderer::getHdrResult   src/raygen/rayrenderer.h:411
  *   rg_get_ldr             <- RayRenderer::getRenderResult src/raygen/rayrenderer.h:404
  *   rg_reapply_postprocess <- RayRenderer::reapplyPostProcess src/raygen/rayrenderer.cpp:698-711
@@ -271,8 +274,31 @@ rg_status rg_create(const rg_settings* s, rg_handle** out);
 rg_status rg_destroy(rg_handle* h);
 rg_status rg_update_settings(rg_handle* h, const rg_settings* s);
 rg_status rg_set_scene(rg_handle* h, const rg_scene_desc* scene);
+/* Blocking render (RayRenderer::render, rayrenderer.cpp:478-596).  Waves are
+ * paced one behind the device, so progress is reported for completed waves and
+ * rg_cancel ends the render within about one wave (RG_ERR_CANCELLED; the
+ * handle stays usable).  RG_ERR_BUSY while an rg_render_async job of the same
+ * handle is in flight. */
 rg_status rg_render(rg_handle* h);
+/* Asynchronous render: the reference's render() runs its tiles on worker
+ * threads and reports through progressCallback (rayrenderer.cpp:748-809,
+ * :804-806); here one host thread per job runs the render of `h` and the
+ * caller polls or waits.  One in-flight render per handle (RG_ERR_BUSY
+ * otherwise); rg_set_scene / rg_update_settings on the handle block until the
+ * job ends.  rg_poll: done (0/1) and progress in [0, 1]; rg_wait: the render's
+ * status, or RG_ERR_BUSY when timeout_ms (< 0: no limit) passes first;
+ * rg_job_free waits for the render to end, then frees the job. */
+typedef struct rg_job rg_job;
+rg_status rg_render_async(rg_handle* h, rg_job** job);
+rg_status rg_poll(rg_job* job, int32_t* done, float* progress);
+rg_status rg_wait(rg_job* job, double timeout_ms);
+rg_status rg_job_free(rg_job* job);
+/* Progress callback (RayRenderer::progressCallback, rayrenderer.h:317): called
+ * from the rendering host thread (the caller's, or the async job's), never
+ * from the device, with non-decreasing values; 1.0 when a render completes. */
 rg_status rg_set_progress_cb(rg_handle* h, rg_progress_fn fn, void* user);
+/* Request cancellation of the handle's render in flight (cancelRequested,
+ * rayrenderer.h:427, polled per tile at rayrenderer.cpp:766). */
 rg_status rg_cancel(rg_handle* h);
 /* Linear HDR result (width*height*4 floats, alpha = 1). */
 rg_status rg_get_hdr(rg_handle* h, float* rgba, size_t count);
@@ -493,10 +519,22 @@ typedef struct rg_server_stats {
 
 void rg_server_config_default(rg_server_config* c);
 rg_status rg_server_create(const rg_settings* base, const rg_server_config* cfg, rg_server** out);
+/* Queue a job.  RG_ERR_OUT_OF_MEMORY when the job's admission estimate alone
+ * exceeds the whole HBM budget (it could never be admitted).  The admission
+ * estimate reserves budget before the upload; once the job is resident its
+ * measured device footprint replaces the reservation (bytes_peak is measured). */
 rg_status rg_server_submit(rg_server* s, const rg_job_desc* job, int64_t* job_id);
 rg_status rg_server_poll(rg_server* s, int64_t job_id, rg_job_status* out);
 /* RG_ERR_BUSY on timeout. */
 rg_status rg_server_wait(rg_server* s, int64_t job_id, double timeout_ms);
+/* Cancel a job (the viewer's cancel button sets cancelRequested on the running
+ * render, src/viewer/MainPanel.cpp:44-47): a
+ * queued job leaves the queue; an admitting or resident job is dropped between
+ * waves and its slot and memory are freed.  The job then polls as
+ * RG_JOB_FAILED with error RG_ERR_CANCELLED, and a waiter returns
+ * RG_ERR_CANCELLED.  RG_ERR_BUSY when the job has finished rendering already
+ * (its result stays available). */
+rg_status rg_server_cancel(rg_server* s, int64_t job_id);
 /* Linear HDR result (width*height*4 floats); release != 0 forgets the job. */
 rg_status rg_server_get_result(rg_server* s, int64_t job_id, float* hdr_rgba, size_t count, int32_t release);
 /* Progressive result of a resident job (current sample mean), taken between waves. */

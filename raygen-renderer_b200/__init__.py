@@ -215,6 +215,10 @@ def load_library(path: str = LIB_PATH) -> C.CDLL:
         "rg_render": (C.c_int, [C.c_void_p]),
         "rg_set_progress_cb": (C.c_int, [C.c_void_p, PROGRESS_FN, C.c_void_p]),
         "rg_cancel": (C.c_int, [C.c_void_p]),
+        "rg_render_async": (C.c_int, [C.c_void_p, P(C.c_void_p)]),
+        "rg_poll": (C.c_int, [C.c_void_p, P(C.c_int32), P(C.c_float)]),
+        "rg_wait": (C.c_int, [C.c_void_p, C.c_double]),
+        "rg_job_free": (C.c_int, [C.c_void_p]),
         "rg_get_hdr": (C.c_int, [C.c_void_p, P(C.c_float), C.c_size_t]),
         "rg_get_ldr": (C.c_int, [C.c_void_p, P(C.c_float), C.c_size_t]),
         "rg_get_aovs": (C.c_int, [C.c_void_p, P(C.c_float), P(C.c_float), P(C.c_float), C.c_size_t]),
@@ -261,6 +265,7 @@ def load_library(path: str = LIB_PATH) -> C.CDLL:
         "rg_server_submit": (C.c_int, [C.c_void_p, P(rg_job_desc), P(C.c_int64)]),
         "rg_server_poll": (C.c_int, [C.c_void_p, C.c_int64, P(rg_job_status)]),
         "rg_server_wait": (C.c_int, [C.c_void_p, C.c_int64, C.c_double]),
+        "rg_server_cancel": (C.c_int, [C.c_void_p, C.c_int64]),
         "rg_server_get_result": (C.c_int, [C.c_void_p, C.c_int64, P(C.c_float), C.c_size_t, C.c_int32]),
         "rg_server_snapshot": (C.c_int, [C.c_void_p, C.c_int64, P(C.c_float), C.c_size_t, C.c_double]),
         "rg_server_get_stats": (C.c_int, [C.c_void_p, P(rg_server_stats)]),
@@ -513,6 +518,44 @@ class Scene:
 
 
 # ---------------------------------------------------------------- renderer
+class RenderJob:
+    """An asynchronous render (rg_render_async): poll(), wait(), then the
+    renderer's result getters.  The job is freed when it is waited for and
+    garbage collected, or by close()."""
+
+    def __init__(self, renderer: "RayRenderer", job: C.c_void_p):
+        self._r = renderer
+        self._lib = renderer._lib
+        self._job = job
+
+    def poll(self):
+        """(done, progress in [0, 1])."""
+        done = C.c_int32()
+        pr = C.c_float()
+        _check(self._lib.rg_poll(self._job, C.byref(done), C.byref(pr)))
+        return bool(done.value), float(pr.value)
+
+    def wait(self, timeout_ms: float = -1.0) -> bool:
+        """Wait for the render; False on timeout; raises RayGenError if the render failed
+        (RG_ERR_CANCELLED after cancel())."""
+        rc = self._lib.rg_wait(self._job, float(timeout_ms))
+        if rc == RG_ERR_BUSY:
+            return False
+        _check(rc)
+        return True
+
+    def close(self) -> None:
+        if self._job:
+            self._lib.rg_job_free(self._job)
+            self._job = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
 class RayRenderer:
     """Mirror of the reference RayRenderer (rayrenderer.h:199-434) over the device tracer."""
 
@@ -537,13 +580,28 @@ class RayRenderer:
 
     setScene = set_scene
 
-    def render(self) -> None:
-        self._sync_settings()
+    def _install_progress(self):
         if self.progressCallback is not None:
             user = self.progressCallback
             self._cb = PROGRESS_FN(lambda p, _u: user(float(p)))
             _check(self._lib.rg_set_progress_cb(self._h, self._cb, None))
+        elif self._cb is not None:
+            self._cb = None
+            _check(self._lib.rg_set_progress_cb(self._h, PROGRESS_FN(0), None))
+
+    def render(self) -> None:
+        self._sync_settings()
+        self._install_progress()
         _check(self._lib.rg_render(self._h))
+
+    def render_async(self) -> "RenderJob":
+        """Start the render on a host thread (the reference's threaded render();
+        progressCallback is called from that thread).  Returns a RenderJob."""
+        self._sync_settings()
+        self._install_progress()
+        job = C.c_void_p()
+        _check(self._lib.rg_render_async(self._h, C.byref(job)))
+        return RenderJob(self, job)
 
     def cancel(self) -> None:
         _check(self._lib.rg_cancel(self._h))
@@ -918,6 +976,14 @@ class RenderServer:
 
     def wait(self, job: int, timeout_ms: float = 600000.0) -> None:
         _check(self._lib.rg_server_wait(self._h, job, timeout_ms))
+
+    def cancel(self, job: int) -> int:
+        """Cancel a queued, admitting or resident job (its slot and memory are freed
+        between waves).  Returns RG_OK, or RG_ERR_BUSY when it finished rendering already."""
+        rc = self._lib.rg_server_cancel(self._h, job)
+        if rc not in (RG_OK, RG_ERR_BUSY):
+            _check(rc)
+        return rc
 
     def result(self, job: int, release: bool = True) -> np.ndarray:
         _, w, h = self._jobs[job]

@@ -11,6 +11,7 @@
 
 #include <algorithm>
 #include <chrono>
+#include <condition_variable>
 #include <climits>
 #include <cstdlib>
 #include <unordered_map>
@@ -19,6 +20,7 @@
 #include <memory>
 #include <mutex>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "rg_device.cuh"
@@ -299,8 +301,13 @@ struct rg_handle {
   rg_progress_fn progress = nullptr;
   void* progressUser = nullptr;
   std::atomic<bool> cancel{false};
+  std::atomic<float> progressValue{0.0f};  // completed waves / waves planned, for rg_poll
+  std::atomic<bool> asyncBusy{false};      // an rg_render_async job is in flight
+  cudaEvent_t waveDone[2] = {nullptr, nullptr};
   rg_stats lastStats{};
   ~rg_handle() {
+    for (auto e : waveDone)
+      if (e) cudaEventDestroy(e);
     if (graph) cudaGraphExecDestroy(graph);
     scene.reset();
     if (stream) cudaStreamDestroy(stream);
@@ -308,6 +315,18 @@ struct rg_handle {
 };
 
 namespace rg {
+
+size_t DeviceScene::deviceBytes() const {
+  size_t b = inPos.bytes() + inNrm.bytes() + inUV.bytes() + inTriMesh.bytes() + view.bytes();
+  b += meshObj.bytes() + meshTriCount.bytes() + objMat.bytes() + objMedium.bytes() + mats.bytes() + media.bytes();
+  b += pathPts.bytes() + volLights.bytes() + areaLightObj.bytes() + lightMeshList.bytes() + lightObjMeshes.bytes();
+  b += lightMeshTris.bytes() + lightTris.bytes() + points.bytes() + textures.bytes() + envMarg.bytes();
+  b += envCond.bytes() + cubeMargFace.bytes() + cubeMargY.bytes() + cubeCond.bytes() + nodes.bytes();
+  b += nodes8.bytes() + triVerts.bytes() + triShade.bytes() + triUV.bytes() + triOrig.bytes();
+  for (const auto* t : texels) b += t ? t->bytes() : 0;
+  return b;
+}
+
 namespace {
 
 rg_status ensureQueues(rg_handle* h, int capacity, int maxIter, bool volQueue) {
@@ -1109,6 +1128,17 @@ static rg_status runPass(rg_handle* h, const DevRender& R, int numPixels, const 
     }
     h->graphKey = key;
   }
+  // Waves are paced: wave k is launched, then the host waits for wave k-1.  One
+  // wave stays queued behind the running one (the device never idles), while
+  // progress is reported for completed waves and a cancel stops the render
+  // within one wave.
+  for (int e = 0; e < 2; e++)
+    if (!h->waveDone[e]) RG_CUDA_CHECK(cudaEventCreateWithFlags(&h->waveDone[e], cudaEventDisableTiming));
+  auto reportProgress = [&](int completed) {
+    const float pr = totalWavesHint > 0 ? std::min(1.0f, (float)completed / (float)totalWavesHint) : 0.0f;
+    if (pr > h->progressValue.load()) h->progressValue.store(pr);
+    if (h->progress) h->progress(h->progressValue.load(), h->progressUser);
+  };
   for (size_t k = 0; k < ws.size(); k++) {
     if (h->cancel.load()) return RG_ERR_CANCELLED;
     if (!started) {
@@ -1133,20 +1163,21 @@ static rg_status runPass(rg_handle* h, const DevRender& R, int numPixels, const 
     } else {
       RG_CUDA_CHECK(cudaGraphLaunch(h->graph, h->stream));
     }
+    RG_CUDA_CHECK(cudaEventRecord(h->waveDone[wavesDone & 1], h->stream));
     wavesDone++;
-    if (h->progress) {
-      // progress is reported from the calling thread once the wave is queued
-      const float pr = totalWavesHint > 0 ? std::min(1.0f, (float)wavesDone / (float)totalWavesHint) : 0.0f;
-      h->progress(pr, h->progressUser);
+    if (wavesDone >= 2) {
+      RG_CUDA_CHECK(cudaEventSynchronize(h->waveDone[wavesDone & 1]));  // wave wavesDone-2 of the render
+      reportProgress(wavesDone - 1);
     }
   }
   for (auto& e : ev) cudaEventDestroy(e);
   return RG_OK;
 }
 
-rg_status rg_render(rg_handle* h) {
-  if (!h) return RG_ERR_INVALID_ARGUMENT;
-  std::lock_guard<std::mutex> lk(h->mu);
+namespace {
+
+// The render itself; the caller holds h->mu.
+rg_status renderLocked(rg_handle* h) {
   const rg_settings& s = h->st;
   if (s.shader_provider == 4) {
     setLastError("shader 4 is reserved (no provider in the reference)");
@@ -1168,6 +1199,7 @@ rg_status rg_render(rg_handle* h) {
   }
   h->cancel.store(false);
   h->haveResult = false;
+  h->progressValue.store(0.0f);
   const int W = s.resolution_width, H = s.resolution_height, N = W * H;
   const bool profile = std::getenv("RG_PROFILE_KERNELS") != nullptr;
   if (!h->sum.alloc(N) || !h->sumSq.alloc(N) || !h->cnt.alloc(N) || !h->hdr.alloc(N) || !h->ldr.alloc(N) ||
@@ -1313,6 +1345,94 @@ rg_status rg_render(rg_handle* h) {
     return RG_ERR_DEVICE_STATUS;
   }
   h->haveResult = true;
+  h->progressValue.store(1.0f);
+  if (h->progress) h->progress(1.0f, h->progressUser);
+  return RG_OK;
+}
+
+}  // namespace
+
+rg_status rg_render(rg_handle* h) {
+  if (!h) return RG_ERR_INVALID_ARGUMENT;
+  if (h->asyncBusy.load()) {
+    setLastError("rg_render: an rg_render_async job of this handle is in flight");
+    return RG_ERR_BUSY;
+  }
+  std::lock_guard<std::mutex> lk(h->mu);
+  return renderLocked(h);
+}
+
+// One asynchronous render: a host thread runs the render of its handle.
+struct rg_job {
+  rg_handle* h = nullptr;
+  std::thread worker;
+  std::mutex mu;
+  std::condition_variable cv;
+  bool done = false;
+  rg_status status = RG_OK;
+};
+
+rg_status rg_render_async(rg_handle* h, rg_job** out) {
+  if (!h || !out) return RG_ERR_INVALID_ARGUMENT;
+  *out = nullptr;
+  bool expected = false;
+  if (!h->asyncBusy.compare_exchange_strong(expected, true)) {
+    setLastError("rg_render_async: a render of this handle is already in flight");
+    return RG_ERR_BUSY;
+  }
+  rg_job* j = new (std::nothrow) rg_job();
+  if (!j) {
+    h->asyncBusy.store(false);
+    return RG_ERR_OUT_OF_MEMORY;
+  }
+  j->h = h;
+  h->progressValue.store(0.0f);
+  try {
+    j->worker = std::thread([j]() {
+      rg_status rs;
+      {
+        std::lock_guard<std::mutex> lk(j->h->mu);
+        rs = renderLocked(j->h);
+      }
+      j->h->asyncBusy.store(false);
+      std::lock_guard<std::mutex> lk(j->mu);
+      j->status = rs;
+      j->done = true;
+      j->cv.notify_all();
+    });
+  } catch (...) {
+    h->asyncBusy.store(false);
+    delete j;
+    setLastError("rg_render_async: could not start the render thread");
+    return RG_ERR_OUT_OF_MEMORY;
+  }
+  *out = j;
+  return RG_OK;
+}
+
+rg_status rg_poll(rg_job* j, int32_t* done, float* progress) {
+  if (!j) return RG_ERR_INVALID_ARGUMENT;
+  std::lock_guard<std::mutex> lk(j->mu);
+  if (done) *done = j->done ? 1 : 0;
+  if (progress) *progress = j->done && j->status == RG_OK ? 1.0f : j->h->progressValue.load();
+  return RG_OK;
+}
+
+rg_status rg_wait(rg_job* j, double timeout_ms) {
+  if (!j) return RG_ERR_INVALID_ARGUMENT;
+  std::unique_lock<std::mutex> lk(j->mu);
+  if (timeout_ms < 0) {
+    j->cv.wait(lk, [j]() { return j->done; });
+  } else if (!j->cv.wait_for(lk, std::chrono::duration<double, std::milli>(timeout_ms), [j]() { return j->done; })) {
+    return RG_ERR_BUSY;
+  }
+  return j->status;
+}
+
+rg_status rg_job_free(rg_job* j) {
+  if (!j) return RG_ERR_INVALID_ARGUMENT;
+  if (j->worker.joinable()) j->worker.join();
+  delete j;
   return RG_OK;
 }
 

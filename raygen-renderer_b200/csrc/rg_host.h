@@ -64,6 +64,7 @@ struct DevBuf {
     n = count;
     return true;
   }
+  size_t bytes() const { return p ? n * sizeof(T) : 0; }
   void release() {
     if (p) cudaFreeAsync(p, cudaStreamPerThread);
     p = nullptr;
@@ -156,6 +157,8 @@ struct DeviceScene {
   int numNodes = 0;
   int rootIsLeaf = 0, rootLeafRef = 0;
   int buildLevels = 0;
+  // device bytes held by the scene after its build (inputs already freed)
+  size_t deviceBytes() const;
   ~DeviceScene() {
     for (auto* t : texels) delete t;
   }

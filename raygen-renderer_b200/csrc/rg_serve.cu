@@ -65,6 +65,7 @@ struct ServerJob {
   std::vector<float> snapshot;
   bool snapshotRequested = false;
   bool snapshotReady = false;
+  bool cancelRequested = false;  // rg_server_cancel on an admitting or resident job
 };
 
 constexpr int kAdmitThreads = 4;
@@ -73,6 +74,15 @@ size_t estimateBytes(const rg_job_desc& d) {
   const size_t tris = d.scene ? (size_t)std::max(0, d.scene->num_triangles) : 0;
   const size_t px = (size_t)std::max(0, d.width) * (size_t)std::max(0, d.height);
   return tris * 520 + px * 176 + ((size_t)64 << 20);
+}
+
+// Device bytes a resident job holds: its scene (BVH, triangles, tables,
+// textures) and its image, accumulation and guide buffers.
+size_t jobDeviceBytes(const ServerJob& j) {
+  size_t b = j.ds ? j.ds->deviceBytes() : 0;
+  b += j.sum.bytes() + j.sumSq.bytes() + j.hdr.bytes() + j.ldr.bytes() + j.bufA.bytes() + j.bufB.bytes();
+  b += j.cnt.bytes() + j.aovN.bytes() + j.aovA.bytes() + j.aovAA.bytes() + j.aovD.bytes() + j.errWord.bytes();
+  return b;
 }
 
 }  // namespace
@@ -316,13 +326,18 @@ void admitLoop(rg_server* s, int idx) {
     }
     const rg_status rs = admit(s, j, st);
     std::lock_guard<std::mutex> lk(s->mu);
-    if (rs != RG_OK) {
-      j->error = rs;
+    if (rs != RG_OK || j->cancelRequested) {
+      j->error = rs != RG_OK ? rs : RG_ERR_CANCELLED;
       j->state = RG_JOB_FAILED;
       j->tDone = nowMs();
       cudaStreamSynchronize(st);
       releaseJob(s, j);
     } else {
+      // the measured device footprint replaces the admission reservation
+      const size_t measured = jobDeviceBytes(*j);
+      s->bytesUsed = s->bytesUsed - std::min(s->bytesUsed, j->bytes) + measured;
+      j->bytes = measured;
+      s->bytesPeak = std::max(s->bytesPeak, s->bytesUsed);
       j->state = RG_JOB_RESIDENT;
       j->tStart = nowMs();
     }
@@ -363,6 +378,18 @@ void serverLoop(rg_server* s) {
     {
       std::unique_lock<std::mutex> lk(s->mu);
       if (s->stop) return;
+      // cancelled resident jobs: no wave of this thread is in flight here, so
+      // their buffers and slots are free to go
+      bool released = false;
+      for (auto* j : s->slotJob)
+        if (j && j->cancelRequested && j->state == RG_JOB_RESIDENT && j->issuedSamples < j->desc.samples) {
+          j->state = RG_JOB_FAILED;
+          j->error = RG_ERR_CANCELLED;
+          j->tDone = nowMs();
+          releaseJob(s, j);
+          released = true;
+        }
+      if (released) s->cv.notify_all();
       bool work = false;  // resident jobs with samples left (finished ones wait for the finisher)
       for (auto* j : s->slotJob)
         if (j && j->state == RG_JOB_RESIDENT && j->issuedSamples < j->desc.samples) work = true;
@@ -378,7 +405,8 @@ void serverLoop(rg_server* s) {
       const int n = (int)s->slotJob.size();
       for (int k = 0; k < n; k++) {
         ServerJob* j = s->slotJob[(rr + k) % n];
-        if (j && j->state == RG_JOB_RESIDENT && j->issuedSamples < j->desc.samples) active.push_back(j);
+        if (j && j->state == RG_JOB_RESIDENT && !j->cancelRequested && j->issuedSamples < j->desc.samples)
+          active.push_back(j);
       }
       int residents = 0;
       for (auto* j : s->slotJob)
@@ -558,6 +586,11 @@ rg_status rg_server_submit(rg_server* s, const rg_job_desc* d, int64_t* job) {
   if (!s || !d || !d->scene || d->width <= 0 || d->height <= 0 || d->samples <= 0 ||
       (long long)d->width * d->height > (1ll << 26))
     return RG_ERR_INVALID_ARGUMENT;
+  if (estimateBytes(*d) > s->cfg.hbm_budget_bytes) {
+    setLastError("rg_server_submit: the job needs about " + std::to_string(estimateBytes(*d) >> 20) +
+                 " MiB, more than the whole HBM budget of " + std::to_string(s->cfg.hbm_budget_bytes >> 20) + " MiB");
+    return RG_ERR_OUT_OF_MEMORY;
+  }
   auto j = std::make_unique<ServerJob>();
   j->desc = *d;
   j->tSubmit = nowMs();
@@ -603,6 +636,35 @@ rg_status rg_server_wait(rg_server* s, int64_t job, double timeout_ms) {
   return j->state == RG_JOB_DONE ? RG_OK : j->error;
 }
 
+rg_status rg_server_cancel(rg_server* s, int64_t job) {
+  if (!s) return RG_ERR_INVALID_ARGUMENT;
+  std::lock_guard<std::mutex> lk(s->mu);
+  auto it = s->jobs.find(job);
+  if (it == s->jobs.end()) return RG_ERR_INVALID_ARGUMENT;
+  ServerJob* j = it->second.get();
+  switch (j->state) {
+    case RG_JOB_QUEUED: {
+      auto q = std::find(s->pending.begin(), s->pending.end(), j);
+      if (q != s->pending.end()) s->pending.erase(q);
+      j->state = RG_JOB_FAILED;
+      j->error = RG_ERR_CANCELLED;
+      j->tDone = nowMs();
+      s->cv.notify_all();
+      return RG_OK;
+    }
+    case RG_JOB_ADMITTING:  // the admission thread drops it when its upload ends
+      j->cancelRequested = true;
+      return RG_OK;
+    case RG_JOB_RESIDENT:
+      if (j->issuedSamples >= j->desc.samples) return RG_ERR_BUSY;  // rendered; the result is being read back
+      j->cancelRequested = true;  // released by the wave thread between waves
+      s->cv.notify_all();
+      return RG_OK;
+    default:
+      return RG_ERR_BUSY;  // done or failed already
+  }
+}
+
 rg_status rg_server_get_result(rg_server* s, int64_t job, float* hdr_rgba, size_t count, int32_t release) {
   if (!s) return RG_ERR_INVALID_ARGUMENT;
   std::lock_guard<std::mutex> lk(s->mu);
@@ -641,6 +703,7 @@ rg_status rg_server_snapshot(rg_server* s, int64_t job, float* hdr_rgba, size_t 
   while (!j->snapshotReady && j->state == RG_JOB_RESIDENT) {
     if (s->cv.wait_until(lk, deadline) == std::cv_status::timeout) return RG_ERR_BUSY;
   }
+  if (!j->snapshotReady && j->state == RG_JOB_FAILED) return j->error;
   const std::vector<float>& src = j->snapshotReady ? j->snapshot : j->result;
   if (count < src.size() || src.empty()) return RG_ERR_BUSY;
   std::memcpy(hdr_rgba, src.data(), src.size() * sizeof(float));

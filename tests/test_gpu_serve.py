@@ -55,13 +55,19 @@ def test_result_is_independent_of_the_mix(rg):
 
 
 def test_admission_respects_the_budget(rg):
+    """Each job reserves its admission estimate (about 66-70 MB here, most of it
+    for the BVH build) until it is resident, then holds its measured footprint
+    (a few MB): with a 75 MB budget no two jobs are admitted at once, at most
+    two are resident together, and the budget is never exceeded."""
     scenes = _scenes(rg, 4, seed0=200)
-    srv = rg.RenderServer(hbm_budget_gb=0.05, max_resident_jobs=8)
+    budget_gb = 0.07
+    srv = rg.RenderServer(hbm_budget_gb=budget_gb, max_resident_jobs=8)
     ids = [srv.submit(sc, 48, 48, 8, max_depth=4, seed=k) for k, sc in enumerate(scenes)]
     for jid in ids:
         srv.wait(jid)
     st = srv.stats()
-    assert st["jobs_done"] == 4 and st["resident_peak"] == 1
+    assert st["jobs_done"] == 4 and 1 <= st["resident_peak"] <= 2
+    assert 0 < st["bytes_peak"] <= budget_gb * (1 << 30)
     assert st["p99_ms"] >= st["p50_ms"] > 0
     for jid in ids:
         assert np.isfinite(srv.result(jid)).all()
@@ -96,3 +102,49 @@ def test_autotuner_config_is_valid_and_keeps_results(rg):
         srv.close()
     # the path RNG is keyed by (seed, pixel, sample): wave size and launch widths do not change the image
     np.testing.assert_allclose(out[0], out[1], rtol=1e-4, atol=1e-6)
+
+
+def test_job_larger_than_the_budget_is_refused(rg):
+    small = rg.Scene.builtin(1, 1)
+    big = rg.Scene.builtin(4, 5, [1000000, 4])  # about 0.5 GB to admit
+    srv = rg.RenderServer(hbm_budget_gb=0.2, max_resident_jobs=4)
+    with pytest.raises(rg.RayGenError) as e:
+        srv.submit(big, 64, 64, 4, max_depth=4, seed=1)
+    assert e.value.code == rg.RG_ERR_OUT_OF_MEMORY
+    j = srv.submit(small, 32, 32, 4, max_depth=4, seed=1)  # the server goes on serving
+    srv.wait(j)
+    assert np.isfinite(srv.result(j)).all()
+    srv.close()
+
+
+def test_cancel_queued_and_resident_jobs_frees_their_slots(rg):
+    """rg_server_cancel: a resident job is dropped between waves (its slot and
+    memory are freed, waiters see RG_ERR_CANCELLED), a queued job leaves the
+    queue, and the other jobs complete with the images they have alone."""
+    sc = rg.Scene.builtin(2, 3, [20000])
+    small = rg.Scene.builtin(1, 1)
+    srv = rg.RenderServer(max_resident_jobs=1, paths_per_wave=1 << 14)
+    long_job = srv.submit(sc, 256, 256, 256, max_depth=8, seed=1)   # many waves of 16 Ki paths
+    queued = srv.submit(small, 32, 32, 8, max_depth=5, seed=2)      # waits for the only slot
+    after = srv.submit(small, 40, 30, 8, max_depth=5, seed=3)
+    srv.snapshot(long_job)                                         # resident and rendering
+    assert srv.status(long_job)["state"] == rg.RG_JOB_RESIDENT
+    assert srv.status(queued)["state"] == rg.RG_JOB_QUEUED
+    assert srv.cancel(queued) == rg.RG_OK
+    assert srv.cancel(long_job) == rg.RG_OK
+    for jid in (long_job, queued):
+        with pytest.raises(rg.RayGenError) as e:
+            srv.wait(jid, 60000.0)
+        assert e.value.code == rg.RG_ERR_CANCELLED
+        st = srv.status(jid)
+        assert st["state"] == rg.RG_JOB_FAILED and st["error"] == rg.RG_ERR_CANCELLED
+    assert srv.status(long_job)["samples_issued"] < 256 * 256 * 256
+    srv.wait(after)  # the freed slot admits the next job
+    assert srv.cancel(after) == rg.RG_ERR_BUSY  # finished: nothing left to cancel
+    got = srv.result(after)
+    r = rg.RayRenderer(rg.RendererSettings(resolutionWidth=40, resolutionHeight=30, samples=8, maxDepth=5, seed=3))
+    r.set_scene(small)
+    r.render()
+    np.testing.assert_allclose(got, r.get_hdr_result(), rtol=1e-4, atol=1e-6)
+    r.close()
+    srv.close()
