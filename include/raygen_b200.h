@@ -332,6 +332,18 @@ rg_status rg_trace_any(rg_handle* h, const float* rays, const float* tmax, int32
  *       bent ray's origin and direction; bendRay, medium.cpp:237-274). */
 rg_status rg_medium_eval(rg_handle* h, int32_t medium, const float* points, int32_t n, float* out);
 rg_status rg_medium_bend(rg_handle* h, int32_t medium, const float* rays, int32_t n, float* out);
+/* Failure-detection test hooks (no reference counterpart).  Both change a
+ * process-wide bound of this library on the current device; pass 0 to restore
+ * the built-in bound, and make no other render of the process overlap the call.
+ *   rg_debug_set_traversal_step_cap: node steps a traversal may take per ray
+ *     before it stops, raises its error flag and the render returns
+ *     RG_ERR_DEVICE_STATUS (built-in: 4,194,304);
+ *   rg_debug_set_tc_wait_limit: polls the learned denoiser's strip pipeline
+ *     makes on a barrier before it gives up, raises its error word (the call
+ *     returns RG_ERR_DEVICE_STATUS) and drains its copies and MMAs under the
+ *     built-in bound before freeing tensor memory (built-in: 67,108,864). */
+rg_status rg_debug_set_traversal_step_cap(int32_t cap);
+rg_status rg_debug_set_tc_wait_limit(uint32_t polls);
 /* Sampling-helper probes (device work, host pointers), one row per input;
  * each row runs the device function the shade kernel uses:
  *   0 sampleGGXVNDF      <- bsdf.cpp:139-161  in (Ve xyz, ax, ay, u1, u2) -> H xyz

@@ -256,6 +256,8 @@ def load_library(path: str = LIB_PATH) -> C.CDLL:
         "rg_medium_defaults": (None, [P(rg_medium)]),
         "rg_medium_eval": (C.c_int, [C.c_void_p, C.c_int32, P(C.c_float), C.c_int32, P(C.c_float)]),
         "rg_probe_sampling": (C.c_int, [C.c_int32, P(C.c_float), C.c_int32, P(C.c_float)]),
+        "rg_debug_set_traversal_step_cap": (C.c_int, [C.c_int32]),
+        "rg_debug_set_tc_wait_limit": (C.c_int, [C.c_uint32]),
         "rg_medium_bend": (C.c_int, [C.c_void_p, C.c_int32, P(C.c_float), C.c_int32, P(C.c_float)]),
         "rg_scene_builtin": (C.c_int, [C.c_int32, C.c_uint32, P(C.c_int32), C.c_int32, P(P(rg_scene_desc))]),
         "rg_scene_free": (C.c_int, [P(rg_scene_desc)]),

@@ -1537,6 +1537,20 @@ rg_status rg_medium_bend(rg_handle* h, int32_t medium, const float* rays, int32_
   return mediumQuery(h, medium, true, rays, n, out);
 }
 
+rg_status rg_debug_set_traversal_step_cap(int32_t cap) {
+  int dc = 0;
+  if (cudaGetDeviceCount(&dc) != cudaSuccess || dc == 0) {
+    cudaGetLastError();
+    return RG_ERR_NO_DEVICE;
+  }
+  if (!setTraversalStepCap(cap)) {
+    cudaGetLastError();
+    setLastError("rg_debug_set_traversal_step_cap: cudaMemcpyToSymbol failed");
+    return RG_ERR_CUDA;
+  }
+  return RG_OK;
+}
+
 rg_status rg_probe_sampling(int32_t which, const float* in, int32_t n, float* out) {
   static const int kInW[11] = {7, 5, 2, 7, 3, 7, 13, 4, 6, 7, 2};
   static const int kOutW[11] = {3, 1, 1, 3, 6, 3, 3, 1, 3, 1, 1};
@@ -1569,6 +1583,7 @@ rg_status rg_trace_closest(rg_handle* h, const float* rays, int32_t n, float* ou
   DevBuf<float> r, t;
   DevBuf<int> p;
   if (!r.upload(rays, (size_t)n * 6, h->stream) || !t.alloc((size_t)n * 3) || !p.alloc(n)) return RG_ERR_OUT_OF_MEMORY;
+  RG_CUDA_CHECK(cudaMemsetAsync(h->error.p, 0, sizeof(int), h->stream));  // this query's flag only
   launchQueryClosest(h->dscene, r.p, n, t.p, p.p, h->stream);
   RG_CUDA_CHECK(cudaMemcpyAsync(out_tuv, t.p, sizeof(float) * n * 3, cudaMemcpyDeviceToHost, h->stream));
   RG_CUDA_CHECK(cudaMemcpyAsync(out_prim, p.p, sizeof(int) * n, cudaMemcpyDeviceToHost, h->stream));
@@ -1592,6 +1607,7 @@ rg_status rg_trace_any(rg_handle* h, const float* rays, const float* tmax, int32
   if (!r.upload(rays, (size_t)n * 6, h->stream) || !tm.upload(tmax, n, h->stream) || !o.alloc(n)) return RG_ERR_OUT_OF_MEMORY;
   const uint32_t occs[5] = {kOccArea, kOccPoint, kOccAO, kOccAll, kOccVol};
   const uint32_t occ = occs[predicate];
+  RG_CUDA_CHECK(cudaMemsetAsync(h->error.p, 0, sizeof(int), h->stream));  // this query's flag only
   launchQueryAny(h->dscene, r.p, tm.p, n, occ, o.p, h->stream);
   RG_CUDA_CHECK(cudaMemcpyAsync(out, o.p, n, cudaMemcpyDeviceToHost, h->stream));
   int derr = 0;

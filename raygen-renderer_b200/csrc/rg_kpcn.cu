@@ -224,6 +224,13 @@ __global__ void k_features(int P, const float4* __restrict__ noisy, const T* __r
 // So row r + 1's loads and MMAs overlap row r's epilogue.  Every wait is
 // bounded; a wait that runs out sets the error word and the CTA drains its
 // outstanding copies and MMAs before it frees the tensor memory.
+// Poll limit of the strip pipeline's waits (loads landed, accumulator full /
+// empty).  The drain before the CTA exits always uses the full tc::kWaitLimit,
+// so a pipeline wait that gives up still lets every issued copy and MMA
+// complete before the tensor memory is freed.  A test lowers this limit
+// (rg_debug_set_tc_wait_limit) to make the pipeline's waits run out.
+__constant__ uint32_t c_pipeWaitLimit = tc::kWaitLimit;
+
 constexpr int kRing = 6;                // input row slots: 3 in use, 1 landing, 2 loading ahead
 constexpr int kSlots = 130;             // pixels per slot: x0 - 1 .. x0 + 128
 constexpr int kConvThreads = 160;
@@ -291,20 +298,20 @@ __global__ void __launch_bounds__(kConvThreads) k_convStrip(const __grid_constan
         const int xt = strip % tilesPerRow, sy = (strip / tilesPerRow) % stripsY, b = strip / (tilesPerRow * stripsY);
         const int y0 = sy * S, n = min(S, H - y0), x0 = xt * 128;
         // Ring slots of earlier strips are reused below: their rows' MMAs must be done.
-        if (r > 0) ok = tc::mbarWait(&tmemFull[(r - 1) & 1], ((r - 1) >> 1) & 1);
+        if (r > 0) ok = tc::mbarWait(&tmemFull[(r - 1) & 1], ((r - 1) >> 1) & 1, c_pipeWaitLimit);
         for (int j = 0; j < n && ok; ++j, ++r) {
           const int t = uBase + j;  // input rows t, t + 1, t + 2 = image rows y0 + j - 1 .. y0 + j + 1
           // The accumulator r & 1 is free once row r - 2's epilogue has read it; that also
           // retires the MMAs of rows up to r - 2, whose ring slots the loads below reuse
           // (input row u goes where row u - kRing <= t - 2 was).
-          if (r >= 2 && !(ok = tc::mbarWait(&tmemEmpty[r & 1], ((r - 2) >> 1) & 1))) break;
+          if (r >= 2 && !(ok = tc::mbarWait(&tmemEmpty[r & 1], ((r - 2) >> 1) & 1, c_pipeWaitLimit))) break;
           for (const int last = min(t + kRing - 2, uBase + n + 1); uNext <= last; ++uNext) {
             const int slot = uNext % kRing, yy = y0 - 1 + (uNext - uBase);
             tc::mbarArriveExpectTx(&full[slot], (uint32_t)(kSlots * CIN * 2));
             tc::tmaLoad4d(ringBase + (uint32_t)(slot * slotBytes<CIN>()), &xmap, 0, x0 - 1, yy, b, &full[slot]);
           }
           for (int i = j == 0 ? 0 : 2; i < 3 && ok; ++i)  // rows t, t + 1 were waited for by row r - 1
-            ok = tc::mbarWait(&full[(t + i) % kRing], ((t + i) / kRing) & 1);
+            ok = tc::mbarWait(&full[(t + i) % kRing], ((t + i) / kRing) & 1, c_pipeWaitLimit);
           if (!ok) break;
           tc::fenceAfterSync();
           // The issue loop is this thread's whole per-row cost, so the descriptors are a
@@ -343,7 +350,7 @@ __global__ void __launch_bounds__(kConvThreads) k_convStrip(const __grid_constan
       const int xt = strip % tilesPerRow, sy = (strip / tilesPerRow) % stripsY, b = strip / (tilesPerRow * stripsY);
       const int y0 = sy * S, n = min(S, H - y0), x = xt * 128 + warp * 32 + lane;
       for (int j = 0; j < n; ++j, ++r) {
-        if (!(ok = tc::mbarWait(&tmemFull[r & 1], (r >> 1) & 1))) break;
+        if (!(ok = tc::mbarWait(&tmemFull[r & 1], (r >> 1) & 1, c_pipeWaitLimit))) break;
         tc::fenceAfterSync();
         float v[32];
         tc::tmemLoad32(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)((r & 1) * 32), v);
@@ -902,6 +909,17 @@ void backward(KpcnNet& n, int B, int H, int W) {
   }
 }
 
+rg_status setPipeWaitLimit(uint32_t polls) {
+  const uint32_t v = polls ? polls : tc::kWaitLimit;
+  const cudaError_t e = cudaMemcpyToSymbol(c_pipeWaitLimit, &v, sizeof(v));
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    setLastError(std::string("rg_debug_set_tc_wait_limit: ") + cudaGetErrorString(e));
+    return RG_ERR_CUDA;
+  }
+  return RG_OK;
+}
+
 rg_status checkErr(KpcnNet& n, const char* what) {
   if (n.mapFailed) {
     n.mapFailed = false;
@@ -1024,6 +1042,8 @@ KpcnNet* kpcnOf(rg_denoiser* d) { return d ? &d->net : nullptr; }
 }  // namespace rg
 
 extern "C" {
+
+rg_status rg_debug_set_tc_wait_limit(uint32_t polls) { return rg::setPipeWaitLimit(polls); }
 
 int32_t rg_denoiser_num_params(void) { return rg::kNumParams; }
 

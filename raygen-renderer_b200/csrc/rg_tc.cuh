@@ -99,9 +99,9 @@ __device__ __forceinline__ bool mbarTryWait(uint64_t* bar, uint32_t phase) {
   return done != 0;
 }
 
-// Bounded wait: false when the limit ran out.
-__device__ __forceinline__ bool mbarWait(uint64_t* bar, uint32_t phase) {
-  for (uint32_t i = 0; i < kWaitLimit; ++i)
+// Bounded wait: false when `limit` polls ran out.
+__device__ __forceinline__ bool mbarWait(uint64_t* bar, uint32_t phase, uint32_t limit = kWaitLimit) {
+  for (uint32_t i = 0; i < limit; ++i)
     if (mbarTryWait(bar, phase)) return true;
   return false;
 }

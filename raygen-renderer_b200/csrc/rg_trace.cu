@@ -872,7 +872,7 @@ __device__ __forceinline__ void traverseWave8(const DevScene& S0, const DevJob* 
             if (sp < kStack8) push(make_uint2((uint32_t)gBase, gInner | (gImask << 8)));
             else atomicCAS(errP, 0, kErrStackOverflow);
           }
-          if (node >= numNodes || ++steps > kMaxTraversalSteps) {
+          if (node >= numNodes || ++steps > c_traversalStepCap) {
             atomicCAS(errP, 0, kErrTraversalSteps);
             result = ANY ? 2 : 1;
           } else {
@@ -1852,6 +1852,11 @@ __global__ void k_probeSampling(int which, const float* __restrict__ in, int n, 
     default:
       break;
   }
+}
+
+bool setTraversalStepCap(int cap) {
+  const int v = cap > 0 ? cap : kMaxTraversalSteps;
+  return cudaMemcpyToSymbol(c_traversalStepCap, &v, sizeof(v)) == cudaSuccess;
 }
 
 void launchProbeSampling(int which, const float* in, int n, float* out, cudaStream_t st) {

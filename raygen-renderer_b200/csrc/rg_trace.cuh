@@ -28,6 +28,8 @@ void launchAov(const DevScene& S, const DevRender& R, __half* normal, __half* al
 void launchQueryClosest(const DevScene& S, const float* rays, int n, float* tuv, int* prim, cudaStream_t st);
 void launchQueryAny(const DevScene& S, const float* rays, const float* tmax, int n, uint32_t occ, uint8_t* out,
                     cudaStream_t st);
+// node-step bound of every traversal loop (cap <= 0: the built-in bound); a test hook
+bool setTraversalStepCap(int cap);
 // sampling-helper probes (rg_probe_sampling)
 void launchProbeSampling(int which, const float* in, int n, float* out, cudaStream_t st);
 // jobs[0].S is the scene; eval: n x 3 points -> n x 5, bend: n x 7 rays -> n x 6

@@ -18,6 +18,11 @@
 
 namespace rg {
 
+// Traversal step bound read by every traversal loop (node steps per ray);
+// kMaxTraversalSteps unless a test lowers it through
+// rg_debug_set_traversal_step_cap to make the bound fire on a small scene.
+__constant__ int c_traversalStepCap = kMaxTraversalSteps;
+
 __device__ __forceinline__ float4 ldg4(const float4* p) { return __ldg(p); }
 // BVH node and triangle fetches of the 8-wide traversal
 __device__ __forceinline__ float4 ldNode4(const float4* p) { return __ldg(p); }
@@ -108,7 +113,7 @@ __device__ __forceinline__ ClosestHit traceClosest2(const DevScene& S, V3 o, V3 
   int steps = 0;
   for (;;) {
     while (ref >= 0) {
-      if (++steps > kMaxTraversalSteps || ref >= S.numNodes) {
+      if (++steps > c_traversalStepCap || ref >= S.numNodes) {
         atomicCAS(S.error, 0, kErrTraversalSteps);
         return h;
       }
@@ -162,7 +167,7 @@ __device__ __forceinline__ bool traceAny2(const DevScene& S, V3 o, V3 d, float m
   int steps = 0;
   for (;;) {
     while (ref >= 0) {
-      if (++steps > kMaxTraversalSteps || ref >= S.numNodes) {
+      if (++steps > c_traversalStepCap || ref >= S.numNodes) {
         atomicCAS(S.error, 0, kErrTraversalSteps);
         return false;
       }
@@ -315,7 +320,7 @@ __device__ __forceinline__ ClosestHit traceClosest8(const DevScene& S, V3 o, V3 
       gImask = e.y >> 8;
       continue;
     }
-    if (++steps > kMaxTraversalSteps) {
+    if (++steps > c_traversalStepCap) {
       atomicCAS(S.error, 0, kErrTraversalSteps);
       break;
     }
@@ -374,7 +379,7 @@ __device__ __forceinline__ bool traceAny8(const DevScene& S, V3 o, V3 d, float m
       gImask = e.y >> 8;
       continue;
     }
-    if (++steps > kMaxTraversalSteps) {
+    if (++steps > c_traversalStepCap) {
       atomicCAS(S.error, 0, kErrTraversalSteps);
       break;
     }
