@@ -641,12 +641,15 @@ def main():
         pg.barrier()
     clock.mark()
     dev_ms, samples, launches = 0.0, 0, 0
+    host_setup, host_total = [], []
     for _ in range(args.steps):
         r.render()
         s = r.stats()
         dev_ms += s["trace_ms"] + s["post_ms"]
         samples += s["samples"]
         launches += s["kernel_launches"]
+        host_setup.append(s["host_setup_ms"])
+        host_total.append(s["host_total_ms"])
     clocks = clock.stop()
     dev_ms_max, total_samples = aggregate(pg, dev_ms, samples)
     value = total_samples / (dev_ms_max * 1e-3) / 1e6
@@ -736,6 +739,10 @@ def main():
                     "ms_per_step": round(1e3 * e2e_s / e2e_steps, 1),
                     "ms_per_step_min_max": [round(1e3 * min(e2e_times), 1), round(1e3 * max(e2e_times), 1)]},
             "gpu_launches": int(launches),
+            "host_ms": {"setup_median": round(statistics.median(host_setup), 2),
+                        "setup_max": round(max(host_setup), 2),
+                        "render_call_median": round(statistics.median(host_total), 2),
+                        "render_call_max": round(max(host_total), 2)},
             "roofline": roofline,
             "cpu_baseline": cpu,
             "clocks": clocks,

@@ -261,6 +261,9 @@ typedef struct rg_stats {
   int32_t waves;
   int32_t kernel_launches;
   int32_t device_error;       /* first device error code, 0 = none           */
+  /* host wall time of the last rg_render: entry -> first wave launched, and
+   * entry -> return (set-up, waves, post, stats read-back) */
+  double host_setup_ms, host_total_ms;
 } rg_stats;
 
 typedef struct rg_handle rg_handle;

@@ -161,7 +161,7 @@ class rg_stats(C.Structure):
         ("shadow_nodes_visited", C.c_uint64), ("shadow_tris_tested", C.c_uint64),
         ("extend_ms", C.c_double), ("shade_ms", C.c_double), ("connect_ms", C.c_double),
         ("bvh_nodes", C.c_int32), ("waves", C.c_int32), ("kernel_launches", C.c_int32),
-        ("device_error", C.c_int32),
+        ("device_error", C.c_int32), ("host_setup_ms", C.c_double), ("host_total_ms", C.c_double),
     ]
 
 

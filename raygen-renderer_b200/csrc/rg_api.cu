@@ -303,6 +303,7 @@ struct rg_handle {
   std::atomic<bool> cancel{false};
   std::atomic<float> progressValue{0.0f};  // completed waves / waves planned, for rg_poll
   std::atomic<bool> asyncBusy{false};      // an rg_render_async job is in flight
+  double firstWaveHostMs = 0.0;            // host clock when the render's first wave was launched
   cudaEvent_t waveDone[2] = {nullptr, nullptr};
   rg_stats lastStats{};
   ~rg_handle() {
@@ -315,6 +316,14 @@ struct rg_handle {
 };
 
 namespace rg {
+
+namespace {
+double hostMs() {
+  using namespace std::chrono;
+  return duration<double, std::milli>(steady_clock::now().time_since_epoch()).count();
+}
+
+}  // namespace
 
 size_t DeviceScene::deviceBytes() const {
   size_t b = inPos.bytes() + inNrm.bytes() + inUV.bytes() + inTriMesh.bytes() + view.bytes();
@@ -1144,6 +1153,7 @@ static rg_status runPass(rg_handle* h, const DevRender& R, int numPixels, const 
     if (!started) {
       cudaEventRecord(start, h->stream);
       started = true;
+      h->firstWaveHostMs = hostMs();
     }
     if (profile) {
       k_selectWave<<<1, 1, 0, h->stream>>>(h->waves.p, h->curWave.p, slot);
@@ -1176,8 +1186,24 @@ static rg_status runPass(rg_handle* h, const DevRender& R, int numPixels, const 
 
 namespace {
 
+// Host-side phase marks of a render, printed to stderr when RG_TRACE_HOST is
+// set (for finding host stalls between the call and the first wave).
+struct HostTrace {
+  bool on = std::getenv("RG_TRACE_HOST") != nullptr;
+  double t0 = hostMs(), last = t0;
+  void mark(const char* what) {
+    if (!on) return;
+    const double t = hostMs();
+    std::fprintf(stderr, "[rg_render] %-28s +%8.3f ms (%8.3f ms)\n", what, t - last, t - t0);
+    last = t;
+  }
+};
+
 // The render itself; the caller holds h->mu.
 rg_status renderLocked(rg_handle* h) {
+  const double tEntry = hostMs();
+  h->firstWaveHostMs = 0.0;
+  HostTrace trace;
   const rg_settings& s = h->st;
   if (s.shader_provider == 4) {
     setLastError("shader 4 is reserved (no provider in the reference)");
@@ -1213,6 +1239,7 @@ rg_status renderLocked(rg_handle* h) {
   RG_CUDA_CHECK(cudaMemsetAsync(h->sum.p, 0, sizeof(float4) * N, st));
   RG_CUDA_CHECK(cudaMemsetAsync(h->sumSq.p, 0, sizeof(float4) * N, st));
   RG_CUDA_CHECK(cudaMemsetAsync(h->cnt.p, 0, sizeof(int) * N, st));
+  trace.mark("image buffers");
   DevRender R = makeRender(h);
   // stats reset
   if (!h->stats.alloc(8) || !h->error.alloc(1)) return RG_ERR_OUT_OF_MEMORY;
@@ -1262,6 +1289,7 @@ rg_status renderLocked(rg_handle* h) {
       spent += passCount;
     }
   }
+  trace.mark("waves launched");
   if (!started) cudaEventRecord(t0, st);  // no wave ran (0 samples)
   cudaEventRecord(t1, st);
   if (rs != RG_OK) {
@@ -1301,7 +1329,9 @@ rg_status renderLocked(rg_handle* h) {
   }
   launchTonemap(N, h->hdr.p, h->ldr.p, st);
   cudaEventRecord(t2, st);
+  trace.mark("post launched");
   const cudaError_t se = cudaStreamSynchronize(st);
+  trace.mark("stream synchronised");
   float traceMs = 0, postMs = 0;
   cudaEventElapsedTime(&traceMs, t0, t1);
   cudaEventElapsedTime(&postMs, t1, t2);
@@ -1345,6 +1375,9 @@ rg_status renderLocked(rg_handle* h) {
     return RG_ERR_DEVICE_STATUS;
   }
   h->haveResult = true;
+  S.host_setup_ms = h->firstWaveHostMs > 0.0 ? h->firstWaveHostMs - tEntry : 0.0;
+  S.host_total_ms = hostMs() - tEntry;
+  trace.mark("stats read back");
   h->progressValue.store(1.0f);
   if (h->progress) h->progress(1.0f, h->progressUser);
   return RG_OK;
