@@ -54,7 +54,7 @@ def parse():
     p.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline (profiling runs only)")
     p.add_argument("--bvh-width", type=int, default=8, choices=[2, 8])
     p.add_argument("--mode", default="headline",
-                   choices=["headline", "batch", "serve", "learned", "denoiser", "configs"],
+                   choices=["headline", "batch", "serve", "learned", "denoiser", "configs", "post"],
                    help="headline: heavy single job; batch: 256 heterogeneous jobs in one server; "
                         "serve: Poisson request stream")
     p.add_argument("--jobs", type=int, default=256)
@@ -493,6 +493,84 @@ def run_denoiser(args):
     return 0
 
 
+# HBM bytes per pixel of one rg_denoise_atrous_noalloc call (float4 colour buffers, FP16 guides):
+#   guide conversion: read normal 12 + albedo 12 + depth 4 + alpha 4, write 6 + 6 + 2 + 2;
+#   pre-pass: read colour 16 + albedo 6 + alpha 2, write 16;
+#   5 levels x (colour 16 in + normal 6 + depth 2 + colour 16 out) -- taps served from L1;
+#   remodulation: read filtered 16 + noisy 16 + albedo 6 + alpha 2, write 16.
+ATROUS_BYTES_PER_PIXEL = (32 + 16) + (24 + 16) + 5 * (16 + 8 + 16) + (40 + 16)
+
+
+def run_post(args):
+    """The post passes on the device: the 5-level A-Trous (rg_denoise_atrous_noalloc on
+    device buffers, 1024 x 1024, its size limit), HDR bloom and the tonemap
+    (rg_bloom, rg_tonemap on host buffers) at 1920 x 1080.  A-Trous device time comes
+    from CUDA events on the stream the call enqueues on; its roofline is HBM at
+    ATROUS_BYTES_PER_PIXEL (guide conversion, pre-pass, 5 levels, remodulation)."""
+    import ctypes as C
+    import numpy as np
+    import torch
+    sys.path.insert(0, ROOT)
+    from __graft_entry__ import load_package
+    rg = load_package()
+    lib = rg.load_library()
+    f = lib.rg_denoise_atrous_noalloc
+    f.restype = C.c_int32
+    f.argtypes = [C.c_int32, C.c_int32] + [C.c_void_p] * 5 + [C.c_int32] + [C.c_float] * 4 + [C.c_void_p, C.c_void_p]
+    n = 1024
+    dev = torch.device("cuda:0")
+    g = torch.Generator(device=dev).manual_seed(1)
+    color = torch.rand((n, n, 4), device=dev, generator=g)
+    normal = torch.rand((n, n, 3), device=dev, generator=g)
+    depth = torch.rand((n, n), device=dev, generator=g)
+    albedo = torch.rand((n, n, 3), device=dev, generator=g)
+    alpha = torch.ones((n, n), device=dev)
+    out = torch.empty((n, n, 4), device=dev)
+    stream = torch.cuda.Stream()
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)  # larger than L2, written between steps
+    ms = []
+    for k in range(args.warmup + args.steps):
+        with torch.cuda.stream(stream):
+            flush.fill_(k & 0xff)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            rc = f(n, n, color.data_ptr(), normal.data_ptr(), depth.data_ptr(), albedo.data_ptr(), alpha.data_ptr(),
+                   5, 0.4, 128.0, 0.1, 1.0, out.data_ptr(), stream.cuda_stream)
+            e1.record(stream)
+        stream.synchronize()
+        if rc != 0:
+            raise RuntimeError(lib.rg_last_error())
+        if k >= args.warmup:
+            ms.append(e0.elapsed_time(e1))
+    atrous_ms = float(np.median(ms))
+    hbm, hsrc = measured_peak_hbm()
+    gbs = ATROUS_BYTES_PER_PIXEL * n * n / atrous_ms / 1e6
+    rng = np.random.default_rng(2)
+    hdr = np.concatenate([rng.random((H, W, 3)) * 4, np.ones((H, W, 1))], -1).astype(np.float32)
+    wall = {}
+    for name, fn in (("bloom", lambda: rg.bloom(hdr)), ("tonemap", lambda: rg.tonemap(hdr))):
+        fn()
+        t0 = time.time()
+        for _ in range(args.steps):
+            fn()
+        wall[name] = round(1e3 * (time.time() - t0) / args.steps, 2)
+    line = {
+        "metric": "post passes: A-Trous device time (1024x1024, 5 levels)", "value": round(atrous_ms, 4), "unit": "ms",
+        "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(atrous_ms, 4),
+        "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f32 colour, f16 guides",
+        "data": "synthetic (seeded uniform colour and guides)",
+        "config": {"workload": "A-Trous 1024x1024 x 5 levels on device buffers; bloom and tonemap at 1920x1080 "
+                               "through the host API (wall time, copies included)", "mode": "post",
+                   "l2": "a 256 MiB buffer is written before every A-Trous call"},
+        "roofline": {"bound": "hbm", "achieved": round(gbs, 1), "peak": hbm, "unit": "GB/s",
+                     "frac": round(gbs / hbm, 4), "traffic": None, "peak_source": hsrc,
+                     "bytes_per_pixel": ATROUS_BYTES_PER_PIXEL},
+        "host_api_wall_ms": wall,
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def run_configs(args):
     """The three single-job configurations, on the device and in the CPU restatement
     with all host threads:
@@ -606,6 +684,8 @@ def main():
         pg = dist
     if args.mode == "learned":
         return run_learned(args)
+    if args.mode == "post":
+        return run_post(args)
     if args.mode == "denoiser":
         return run_denoiser(args)
     if args.mode == "configs":
