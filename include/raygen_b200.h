@@ -542,6 +542,18 @@ rg_status rg_server_submit(rg_server* s, const rg_job_desc* job, int64_t* job_id
 rg_status rg_server_poll(rg_server* s, int64_t job_id, rg_job_status* out);
 /* RG_ERR_BUSY on timeout. */
 rg_status rg_server_wait(rg_server* s, int64_t job_id, double timeout_ms);
+/* Resident scenes: a scene uploaded and built once (BVH, triangles, textures,
+ * light and medium tables stay on the device), then rendered by any number of
+ * jobs without a second upload or build.  rg_server_add_scene copies the
+ * description, builds on the caller's thread and counts the scene's measured
+ * bytes against the HBM budget (RG_ERR_OUT_OF_MEMORY when it does not fit);
+ * the camera is the description's.  rg_server_submit_scene queues a job on it
+ * (job->scene is ignored and may be NULL).  rg_server_remove_scene forgets the
+ * id; the memory is freed when the last job rendering it ends.  No reference
+ * counterpart (the reference renders one scene per process). */
+rg_status rg_server_add_scene(rg_server* s, const rg_scene_desc* scene, int64_t* scene_id);
+rg_status rg_server_submit_scene(rg_server* s, int64_t scene_id, const rg_job_desc* job, int64_t* job_id);
+rg_status rg_server_remove_scene(rg_server* s, int64_t scene_id);
 /* Cancel a job (the viewer's cancel button sets cancelRequested on the running
  * render, src/viewer/MainPanel.cpp:44-47): a
  * queued job leaves the queue; an admitting or resident job is dropped between

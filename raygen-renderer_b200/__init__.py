@@ -268,6 +268,9 @@ def load_library(path: str = LIB_PATH) -> C.CDLL:
         "rg_server_poll": (C.c_int, [C.c_void_p, C.c_int64, P(rg_job_status)]),
         "rg_server_wait": (C.c_int, [C.c_void_p, C.c_int64, C.c_double]),
         "rg_server_cancel": (C.c_int, [C.c_void_p, C.c_int64]),
+        "rg_server_add_scene": (C.c_int, [C.c_void_p, P(rg_scene_desc), P(C.c_int64)]),
+        "rg_server_submit_scene": (C.c_int, [C.c_void_p, C.c_int64, P(rg_job_desc), P(C.c_int64)]),
+        "rg_server_remove_scene": (C.c_int, [C.c_void_p, C.c_int64]),
         "rg_server_get_result": (C.c_int, [C.c_void_p, C.c_int64, P(C.c_float), C.c_size_t, C.c_int32]),
         "rg_server_snapshot": (C.c_int, [C.c_void_p, C.c_int64, P(C.c_float), C.c_size_t, C.c_double]),
         "rg_server_get_stats": (C.c_int, [C.c_void_p, P(rg_server_stats)]),
@@ -954,15 +957,28 @@ class RenderServer:
         return {"paths_per_wave": cfg.paths_per_wave, "shade_blocks_per_sm": cfg.shade_blocks_per_sm,
                 "trace_blocks_per_sm": cfg.trace_blocks_per_sm, "probe_ms": best.value}
 
-    def submit(self, scene: Scene, width: int, height: int, samples: int, max_depth: int = 8, rr_depth: int = 3,
+    def add_scene(self, scene: Scene) -> int:
+        """Upload and build a scene once; jobs submitted with its id reuse it."""
+        sid = C.c_int64()
+        _check(self._lib.rg_server_add_scene(self._h, scene.ptr, C.byref(sid)))
+        return sid.value
+
+    def remove_scene(self, scene_id: int) -> None:
+        _check(self._lib.rg_server_remove_scene(self._h, scene_id))
+
+    def submit(self, scene, width: int, height: int, samples: int, max_depth: int = 8, rr_depth: int = 3,
                seed: int = 1, denoise=False) -> int:
-        """denoise: False / 0 none, True / 1 A-Trous, 2 the learned denoiser (see set_denoiser)."""
+        """scene: a Scene (uploaded for this job) or the id of a resident scene (add_scene).
+        denoise: False / 0 none, True / 1 A-Trous, 2 the learned denoiser (see set_denoiser)."""
         d = rg_job_desc()
-        d.scene = scene.ptr
         d.width, d.height, d.samples = width, height, samples
         d.max_depth, d.rr_depth, d.seed, d.denoise = max_depth, rr_depth, seed, int(denoise)
         jid = C.c_int64()
-        _check(self._lib.rg_server_submit(self._h, C.byref(d), C.byref(jid)))
+        if isinstance(scene, int):
+            _check(self._lib.rg_server_submit_scene(self._h, scene, C.byref(d), C.byref(jid)))
+        else:
+            d.scene = scene.ptr
+            _check(self._lib.rg_server_submit(self._h, C.byref(d), C.byref(jid)))
         self._jobs[jid.value] = (scene, width, height)  # keep the scene alive until done
         return jid.value
 

@@ -42,8 +42,22 @@ double nowMs() {
   return duration<double, std::milli>(steady_clock::now().time_since_epoch()).count();
 }
 
+// A scene uploaded once (rg_server_add_scene) and rendered by many jobs.  Jobs
+// hold a reference; the scene's memory goes when it was removed and its last
+// job has released it.
+struct ServerScene {
+  int64_t id = 0;
+  std::unique_ptr<DeviceScene> ds;
+  DevScene S{};
+  Mat4 view{};
+  rg_camera camera{};
+  size_t bytes = 0;
+  DevBuf<int> buildErr;
+};
+
 struct ServerJob {
   int64_t id = 0;
+  std::shared_ptr<ServerScene> resident;  // the job renders this resident scene (no upload, no build)
   rg_job_desc desc{};
   int state = RG_JOB_QUEUED;
   rg_status error = RG_OK;
@@ -70,10 +84,13 @@ struct ServerJob {
 
 constexpr int kAdmitThreads = 4;
 
-size_t estimateBytes(const rg_job_desc& d) {
-  const size_t tris = d.scene ? (size_t)std::max(0, d.scene->num_triangles) : 0;
+// Admission reservation of a job: scene upload and BVH-build scratch (per
+// triangle) plus its image, accumulation and guide buffers (per pixel) and a
+// fixed build allowance.  A job on a resident scene reserves its buffers only.
+size_t estimateBytes(const rg_job_desc& d, bool residentScene = false) {
+  const size_t tris = (d.scene && !residentScene) ? (size_t)std::max(0, d.scene->num_triangles) : 0;
   const size_t px = (size_t)std::max(0, d.width) * (size_t)std::max(0, d.height);
-  return tris * 520 + px * 176 + ((size_t)64 << 20);
+  return tris * 520 + px * 176 + (residentScene ? ((size_t)1 << 20) : ((size_t)64 << 20));
 }
 
 // Device bytes a resident job holds: its scene (BVH, triangles, tables,
@@ -98,6 +115,8 @@ struct rg_server {
   std::condition_variable cv;
   std::deque<ServerJob*> pending;
   std::map<int64_t, std::unique_ptr<ServerJob>> jobs;
+  std::map<int64_t, std::shared_ptr<ServerScene>> scenes;  // resident scenes by id
+  cudaStream_t sceneStream = nullptr;
   std::vector<ServerJob*> slotJob;
   std::vector<int> freeSlots;
   int64_t nextId = 1;
@@ -140,6 +159,7 @@ struct rg_server {
     if (hostWave) cudaFreeHost(hostWave);
     if (stream) cudaStreamDestroy(stream);
     if (finishStream) cudaStreamDestroy(finishStream);
+    if (sceneStream) cudaStreamDestroy(sceneStream);
     for (auto a : admitStreams) cudaStreamDestroy(a);
   }
 };
@@ -215,8 +235,17 @@ bool captureGraph(rg_server* s) {
   return true;
 }
 
+// Drop a job's reference to its resident scene; the last reference of a
+// removed scene frees it and returns its bytes to the budget.  Caller holds s->mu.
+void dropSceneRef(rg_server* s, std::shared_ptr<ServerScene>& ref) {
+  if (!ref) return;
+  if (ref.use_count() == 1) s->bytesUsed -= std::min(s->bytesUsed, ref->bytes);
+  ref.reset();
+}
+
 void releaseJob(rg_server* s, ServerJob* j) {
   j->ds.reset();
+  dropSceneRef(s, j->resident);
   j->sum.release(); j->sumSq.release(); j->hdr.release(); j->ldr.release(); j->bufA.release(); j->bufB.release();
   j->cnt.release(); j->aovN.release(); j->aovA.release(); j->aovAA.release(); j->aovD.release(); j->errWord.release();
   if (j->slot >= 0) {
@@ -232,8 +261,17 @@ rg_status admit(rg_server* s, ServerJob* j, cudaStream_t st) {
   const rg_job_desc& d = j->desc;
   if (!j->errWord.alloc(1)) return RG_ERR_OUT_OF_MEMORY;
   cudaMemsetAsync(j->errWord.p, 0, sizeof(int), st);
-  rg_status rs = prepareScene(d.scene, s->base.bvh_bins, true, st, j->errWord.p, j->ds, j->S, j->view, nullptr);
-  if (rs != RG_OK) return rs;
+  const rg_camera* camera = d.scene ? &d.scene->camera : nullptr;
+  if (j->resident) {  // the scene is on the device already: this job's own error word only
+    j->S = j->resident->S;
+    j->S.error = j->errWord.p;
+    j->view = j->resident->view;
+    camera = &j->resident->camera;
+  } else {
+    const rg_status rs = prepareScene(d.scene, s->base.bvh_bins, true, st, j->errWord.p, j->ds, j->S, j->view,
+                                      nullptr);
+    if (rs != RG_OK) return rs;
+  }
   rg_settings js = s->base;
   js.resolution_width = d.width;
   js.resolution_height = d.height;
@@ -242,7 +280,7 @@ rg_status admit(rg_server* s, ServerJob* j, cudaStream_t st) {
   js.rr_depth = d.rr_depth > 0 ? d.rr_depth : s->base.rr_depth;
   js.seed = d.seed;
   js.shader_provider = 5;
-  j->R = makeRenderParams(js, d.scene->camera);
+  j->R = makeRenderParams(js, *camera);
   j->pixels = d.width * d.height;
   const int N = j->pixels;
   if (!j->sum.alloc(N) || !j->sumSq.alloc(N) || !j->cnt.alloc(N) || !j->hdr.alloc(N) || !j->ldr.alloc(N))
@@ -582,12 +620,17 @@ rg_status rg_server_create(const rg_settings* base, const rg_server_config* cfg,
   return RG_OK;
 }
 
-rg_status rg_server_submit(rg_server* s, const rg_job_desc* d, int64_t* job) {
-  if (!s || !d || !d->scene || d->width <= 0 || d->height <= 0 || d->samples <= 0 ||
+namespace rg {
+namespace {
+
+rg_status submitJob(rg_server* s, const rg_job_desc* d, int64_t sceneId, int64_t* job) {
+  const bool resident = sceneId > 0;
+  if (!s || !d || (!resident && !d->scene) || d->width <= 0 || d->height <= 0 || d->samples <= 0 ||
       (long long)d->width * d->height > (1ll << 26))
     return RG_ERR_INVALID_ARGUMENT;
-  if (estimateBytes(*d) > s->cfg.hbm_budget_bytes) {
-    setLastError("rg_server_submit: the job needs about " + std::to_string(estimateBytes(*d) >> 20) +
+  const size_t need = estimateBytes(*d, resident);
+  if (need > s->cfg.hbm_budget_bytes) {
+    setLastError("rg_server_submit: the job needs about " + std::to_string(need >> 20) +
                  " MiB, more than the whole HBM budget of " + std::to_string(s->cfg.hbm_budget_bytes >> 20) + " MiB");
     return RG_ERR_OUT_OF_MEMORY;
   }
@@ -596,12 +639,73 @@ rg_status rg_server_submit(rg_server* s, const rg_job_desc* d, int64_t* job) {
   j->tSubmit = nowMs();
   std::lock_guard<std::mutex> lk(s->mu);
   if (s->stop) return RG_ERR_BUSY;
+  if (resident) {
+    auto it = s->scenes.find(sceneId);
+    if (it == s->scenes.end()) {
+      setLastError("rg_server_submit_scene: no resident scene " + std::to_string(sceneId));
+      return RG_ERR_INVALID_ARGUMENT;
+    }
+    j->resident = it->second;
+    j->desc.scene = nullptr;
+  }
   j->id = s->nextId++;
   if (s->firstSubmit < 0) s->firstSubmit = j->tSubmit;
   if (job) *job = j->id;
   s->pending.push_back(j.get());
   s->jobs[j->id] = std::move(j);
   s->cv.notify_all();
+  return RG_OK;
+}
+
+}  // namespace
+}  // namespace rg
+
+rg_status rg_server_submit(rg_server* s, const rg_job_desc* d, int64_t* job) { return submitJob(s, d, 0, job); }
+
+rg_status rg_server_add_scene(rg_server* s, const rg_scene_desc* scene, int64_t* scene_id) {
+  if (!s || !scene || !scene_id) return RG_ERR_INVALID_ARGUMENT;
+  {
+    std::lock_guard<std::mutex> lk(s->mu);
+    const size_t need = (size_t)std::max(0, scene->num_triangles) * 520 + ((size_t)64 << 20);
+    if (s->bytesUsed + need > s->cfg.hbm_budget_bytes) {
+      setLastError("rg_server_add_scene: the scene needs about " + std::to_string(need >> 20) +
+                   " MiB, over what the HBM budget has left");
+      return RG_ERR_OUT_OF_MEMORY;
+    }
+    if (!s->sceneStream && cudaStreamCreateWithFlags(&s->sceneStream, cudaStreamNonBlocking) != cudaSuccess)
+      return RG_ERR_CUDA;
+  }
+  auto sc = std::make_shared<ServerScene>();
+  if (!sc->buildErr.alloc(1)) return RG_ERR_OUT_OF_MEMORY;
+  cudaMemsetAsync(sc->buildErr.p, 0, sizeof(int), s->sceneStream);
+  rg_status rs = prepareScene(scene, s->base.bvh_bins, true, s->sceneStream, sc->buildErr.p, sc->ds, sc->S, sc->view,
+                              nullptr);
+  if (rs == RG_OK && cudaStreamSynchronize(s->sceneStream) != cudaSuccess) rs = RG_ERR_CUDA;
+  if (rs != RG_OK) return rs;
+  sc->camera = scene->camera;
+  sc->bytes = sc->ds->deviceBytes();
+  std::lock_guard<std::mutex> lk(s->mu);
+  sc->id = s->nextId++;
+  s->bytesUsed += sc->bytes;
+  s->bytesPeak = std::max(s->bytesPeak, s->bytesUsed);
+  s->scenes[sc->id] = sc;
+  *scene_id = sc->id;
+  return RG_OK;
+}
+
+rg_status rg_server_submit_scene(rg_server* s, int64_t scene_id, const rg_job_desc* d, int64_t* job) {
+  if (scene_id <= 0) return RG_ERR_INVALID_ARGUMENT;
+  return submitJob(s, d, scene_id, job);
+}
+
+rg_status rg_server_remove_scene(rg_server* s, int64_t scene_id) {
+  if (!s) return RG_ERR_INVALID_ARGUMENT;
+  std::lock_guard<std::mutex> lk(s->mu);
+  auto it = s->scenes.find(scene_id);
+  if (it == s->scenes.end()) return RG_ERR_INVALID_ARGUMENT;
+  std::shared_ptr<ServerScene> ref = std::move(it->second);
+  s->scenes.erase(it);
+  dropSceneRef(s, ref);  // freed now unless jobs still render it
   return RG_OK;
 }
 
@@ -646,6 +750,7 @@ rg_status rg_server_cancel(rg_server* s, int64_t job) {
     case RG_JOB_QUEUED: {
       auto q = std::find(s->pending.begin(), s->pending.end(), j);
       if (q != s->pending.end()) s->pending.erase(q);
+      dropSceneRef(s, j->resident);
       j->state = RG_JOB_FAILED;
       j->error = RG_ERR_CANCELLED;
       j->tDone = nowMs();

@@ -148,3 +148,30 @@ def test_cancel_queued_and_resident_jobs_frees_their_slots(rg):
     np.testing.assert_allclose(got, r.get_hdr_result(), rtol=1e-4, atol=1e-6)
     r.close()
     srv.close()
+
+
+def test_resident_scene_is_built_once_and_renders_like_an_uploaded_one(rg):
+    """rg_server_add_scene keeps the BVH and tables on the device: jobs on it
+    skip the upload and build, render the image an uploaded scene gives, count
+    the scene once against the budget, and the scene outlives its removal until
+    its last job ends."""
+    sc = rg.Scene.builtin(2, 6, [20000])
+    srv = rg.RenderServer(max_resident_jobs=8)
+    j0 = srv.submit(sc, 96, 64, 16, max_depth=6, seed=4)  # uploaded with the job
+    srv.wait(j0)
+    want = srv.result(j0)
+    sid = srv.add_scene(sc)
+    bytes_scene = srv.stats()["bytes_peak"]
+    assert bytes_scene > 0
+    ids = [srv.submit(sid, 96, 64, 16, max_depth=6, seed=4) for _ in range(3)]
+    ids.append(srv.submit(sid, 64, 48, 8, max_depth=5, seed=9))
+    srv.remove_scene(sid)  # jobs still queued on it keep it alive
+    for j in ids:
+        srv.wait(j)
+    for j in ids[:3]:
+        np.testing.assert_allclose(srv.result(j), want, rtol=1e-4, atol=1e-6)
+    assert np.isfinite(srv.result(ids[3])).all()
+    with pytest.raises(rg.RayGenError) as e:  # the id is gone
+        srv.submit(sid, 32, 32, 4)
+    assert e.value.code == rg.RG_ERR_INVALID_ARGUMENT
+    srv.close()
