@@ -52,6 +52,8 @@ def parse():
     p.add_argument("--spp", type=int, default=SPP)
     p.add_argument("--res", default=f"{W}x{H}", help="resolution WxH (profiling runs only)")
     p.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline (profiling runs only)")
+    p.add_argument("--no-learned", action="store_true",
+                   help="skip the learned-denoiser sub-record of the headline line (profiling runs only)")
     p.add_argument("--bvh-width", type=int, default=8, choices=[2, 8])
     p.add_argument("--mode", default="headline",
                    choices=["headline", "batch", "serve", "learned", "denoiser", "configs", "post"],
@@ -315,112 +317,163 @@ LEARNED_METRIC = "images/s at relMSE<=0.01: served+batched tracer with the learn
 LADDER = [4, 8, 16, 32, 64, 128, 256, 512]
 
 
-def run_learned(args):
-    """The learned-denoiser experiment: images/s at equal relMSE <= 0.01.
+def learned_specs(n, seed=11, max_side=384, max_tris=300000):
+    """The learned experiment's jobs: the heterogeneous job mix (triangles log-uniform
+    1e3-2e6, emitters 1-64, side log-uniform 64-1024, depth 4-10), sides capped at
+    max_side and triangles at max_tris to bound the run; every fourth job is the
+    benchmark's heavy-sphere scene (metal / dielectric spheres in a room, 4 x 25k
+    triangles).  in_distribution marks jobs inside the denoiser's training generator
+    (batch-job scenes of 2k-40k triangles with 1-8 emitters, or the cube room)."""
+    out = []
+    for k, sp in enumerate(job_specs(n, seed=seed)):
+        sp = dict(sp)
+        side = min(sp["width"], max_side)
+        sp["width"] = sp["height"] = side
+        sp["tris"] = min(sp["tris"], max_tris)
+        if k % 4 == 3:
+            sp["kind"], sp["params"] = 2, [25000]
+        else:
+            sp["kind"], sp["params"] = 4, [sp["tris"], sp["emitters"]]
+        sp["in_distribution"] = sp["kind"] == 4 and 2000 <= sp["tris"] <= 40000 and sp["emitters"] <= 8
+        out.append(sp)
+    return out
 
-    Jobs: held-out seeds of the denoiser's training generator (procedural batch
-    jobs, 2k-40k triangles, 1-8 emitters; every 8th the cube room), 256 x 256.
-    Reference per job: the FP64 mean of 8 independent 256-spp renders (2048 spp).
-    For each arm the spp ladder is walked up until the job-mean relMSE is <= 0.01:
-    * baseline: the plain single-job tracer, jobs one after another (scene
-      upload + BVH build + render + A-Trous + readback each); at every rung it
-      keeps the better of A-Trous and no denoising;
-    * served + batched + learned: all jobs submitted at once to the job server,
+
+def learned_experiment(rg, specs, budget_s=None, rate=200.0):
+    """Images/s at equal relMSE <= 0.01 (job mean) against FP64-accumulated references:
+    * baseline: the plain single-job tracer, one job after another (scene upload + BVH
+      build + render + A-Trous + read-back each); at each rung the better of A-Trous
+      and no denoising;
+    * served + batched + learned: all jobs submitted at once to the job server, the
       learned denoiser on every finished job (denoise mode 2).
-    images/s = jobs / wall time of that arm at its chosen rung."""
+    Each arm walks up the spp ladder until its job-mean relMSE is <= 0.01; images/s =
+    jobs / wall time of that arm at its rung.  References: the FP64 mean of 4
+    independent 512-spp renders per job (path arithmetic FP32).  Latency: the served
+    arm at its rung under Poisson arrivals at half its measured capacity and at
+    `rate` requests/s (p50 / p99)."""
     import importlib
     import numpy as np
-    sys.path.insert(0, ROOT)
-    from __graft_entry__ import load_package
-    rg = load_package()
     kt = importlib.import_module(rg.__name__ + ".kpcn_train")
-    J, S = args.jobs if args.jobs != 256 else 32, 256
-    scenes = [kt.scene_for(rg, 400000 + k) for k in range(J)]
-    seeds = [900 + k for k in range(J)]
-    # references: FP64 mean of 8 x 256 spp
+    t_start = time.time()
+    scenes = [rg.Scene.builtin(sp["kind"], sp["seed"], sp["params"]) for sp in specs]
+    depth = [sp["depth"] for sp in specs]
     refs = []
-    r = rg.RayRenderer(rg.RendererSettings(resolutionWidth=S, resolutionHeight=S, samples=256, maxDepth=6, rrDepth=RR))
-    for sc in scenes:
+    for sc, sp in zip(scenes, specs):
+        r = rg.RayRenderer(rg.RendererSettings(resolutionWidth=sp["width"], resolutionHeight=sp["height"], samples=512,
+                                               maxDepth=sp["depth"], rrDepth=RR))
         r.set_scene(sc)
-        acc = np.zeros((S, S, 3))
-        for p in range(8):
+        acc = np.zeros((sp["height"], sp["width"], 3))
+        for p in range(4):
             r.settings.seed = 50000 + p
             r.render()
             acc += r.get_hdr_result()[..., :3].astype(np.float64)
-        refs.append(acc / 8.0)
-    r.close()
+        refs.append(acc / 4.0)
+        r.close()
+    ref_s = time.time() - t_start
+    ind = np.array([sp["in_distribution"] for sp in specs])
 
-    def plain(spp, timed):
-        st = rg.RendererSettings(resolutionWidth=S, resolutionHeight=S, samples=spp, maxDepth=6, rrDepth=RR,
-                                 enableDenoise=True)
-        rr = rg.RayRenderer(st)
-        errs_a, errs_n = [], []
+    def plain(spp, denoise):
+        errs = []
         t0 = time.time()
-        for sc, seed, ref in zip(scenes, seeds, refs):
-            rr.settings.seed = seed
+        rr = rg.RayRenderer(rg.RendererSettings(resolutionWidth=64, resolutionHeight=64, samples=spp, rrDepth=RR,
+                                                enableDenoise=denoise))
+        for sc, sp, ref in zip(scenes, specs, refs):
+            rr.settings.resolutionWidth, rr.settings.resolutionHeight = sp["width"], sp["height"]
+            rr.settings.maxDepth, rr.settings.seed = sp["depth"], sp["seed"]
             rr.set_scene(sc)
             rr.render()
-            img = rr.get_hdr_result()
-            errs_a.append(kt.relmse(img, ref))
+            errs.append(kt.relmse(rr.get_hdr_result(), ref))
         wall = time.time() - t0
-        if not timed:  # the same samples without the denoiser
-            rr.settings.enableDenoise = False
-            for sc, seed, ref in zip(scenes, seeds, refs):
-                rr.settings.seed = seed
-                rr.set_scene(sc)
-                rr.render()
-                errs_n.append(kt.relmse(rr.get_hdr_result(), ref))
         rr.close()
-        return wall, float(np.mean(errs_a)), float(np.mean(errs_n)) if errs_n else None
+        return wall, np.array(errs)
 
-    def served(spp, den):
+    def served(spp, den, arrivals=None):
         srv = rg.RenderServer(rg.RendererSettings(rrDepth=RR), hbm_budget_gb=120.0, max_resident_jobs=256)
         srv.set_denoiser(den)
         t0 = time.time()
-        ids = [srv.submit(sc, S, S, spp, max_depth=6, seed=seed, denoise=2) for sc, seed in zip(scenes, seeds)]
+        ids = []
+        for k, (sc, sp) in enumerate(zip(scenes, specs)):
+            if arrivals is not None and k > 0:
+                time.sleep(float(arrivals[k - 1]))
+            ids.append(srv.submit(sc, sp["width"], sp["height"], spp, max_depth=sp["depth"], seed=sp["seed"], denoise=2))
         for j in ids:
             srv.wait(j, 3.6e6)
         wall = time.time() - t0
         st = srv.stats()
-        errs = [kt.relmse(srv.result(j), ref) for j, ref in zip(ids, refs)]
+        errs = np.array([kt.relmse(srv.result(j), ref) for j, ref in zip(ids, refs)])
         srv.close()
-        return wall, float(np.mean(errs)), st
+        return wall, errs, st
+
+    def over_budget():
+        return budget_s is not None and time.time() - t_start > budget_s
 
     den = rg.Denoiser.pretrained()
     served(4, den)  # warm-up (graphs, allocator, modules)
     plain(4, True)
+    n = len(specs)
     base = None
     for spp in LADDER:
-        wall, ea, en = plain(spp, False)
-        best = min(ea, en)
-        if best <= 0.01:
-            wall, _, _ = plain(spp, True)  # timed pass in the chosen mode (A-Trous on)
-            base = dict(spp=spp, relmse=round(best, 5), relmse_atrous=round(ea, 5), relmse_raw=round(en, 5),
-                        wall_s=round(wall, 3), images_per_s=round(J / wall, 2))
+        if over_budget():
+            break
+        wa, ea = plain(spp, True)
+        wn, en = plain(spp, False)
+        best_e, wall, mode = (ea, wa, "A-Trous") if ea.mean() <= en.mean() else (en, wn, "none")
+        if best_e.mean() <= 0.01:
+            base = dict(spp=spp, denoiser=mode, relmse=round(float(best_e.mean()), 5),
+                        relmse_in_distribution=round(float(best_e[ind].mean()), 5) if ind.any() else None,
+                        relmse_out_of_distribution=round(float(best_e[~ind].mean()), 5) if (~ind).any() else None,
+                        wall_s=round(wall, 3), images_per_s=round(n / wall, 2))
             break
     cand = None
     for spp in LADDER:
+        if over_budget():
+            break
         wall, e, st = served(spp, den)
-        if e <= 0.01:
-            cand = dict(spp=spp, relmse=round(e, 5), wall_s=round(wall, 3), images_per_s=round(J / wall, 2),
-                        p50_ms=round(st["p50_ms"], 1), p99_ms=round(st["p99_ms"], 1),
+        if e.mean() <= 0.01:
+            cand = dict(spp=spp, relmse=round(float(e.mean()), 5),
+                        relmse_in_distribution=round(float(e[ind].mean()), 5) if ind.any() else None,
+                        relmse_out_of_distribution=round(float(e[~ind].mean()), 5) if (~ind).any() else None,
+                        wall_s=round(wall, 3), images_per_s=round(n / wall, 2),
+                        batch_p50_ms=round(st["p50_ms"], 1), batch_p99_ms=round(st["p99_ms"], 1),
                         resident_peak=st["resident_peak"])
             break
+    if cand is not None and not over_budget():
+        rng = np.random.default_rng(5)
+        for key, r in (("below_capacity", 0.5 * cand["images_per_s"]), ("at_rate", rate)):
+            wall, e, st = served(cand["spp"], den, arrivals=rng.exponential(1.0 / r, n))
+            cand[f"poisson_{key}"] = dict(rate_per_s=round(r, 2), p50_ms=round(st["p50_ms"], 1),
+                                          p99_ms=round(st["p99_ms"], 1), images_per_s=round(st["images_per_s"], 2))
     den.close()
-    ratio = round(cand["images_per_s"] / base["images_per_s"], 2) if base and cand else None
+    for sc in scenes:
+        sc.close()
+    return dict(jobs=n, in_distribution_jobs=int(ind.sum()),
+                sides=[sp["width"] for sp in specs], triangles=[sp["tris"] if sp["kind"] == 4 else 98044 for sp in specs],
+                depths=depth, reference="FP64 mean of 4 x 512 spp per job", reference_s=round(ref_s, 1),
+                baseline_plain_atrous=base, served_batched_learned=cand,
+                speedup=round(cand["images_per_s"] / base["images_per_s"], 2) if base and cand else None,
+                elapsed_s=round(time.time() - t_start, 1), complete=bool(base and cand))
+
+
+def run_learned(args):
+    """The learned-denoiser experiment alone: images/s at equal relMSE <= 0.01 on
+    --jobs config-4-style jobs (default 32); see learned_experiment."""
+    sys.path.insert(0, ROOT)
+    from __graft_entry__ import load_package
+    rg = load_package()
+    J = args.jobs if args.jobs != 256 else 32
+    rec = learned_experiment(rg, learned_specs(J), rate=args.rate)
+    cand = rec["served_batched_learned"]
     line = {
         "metric": LEARNED_METRIC, "value": cand["images_per_s"] if cand else None, "unit": "images/s", "n_gpus": 1,
         "steps": 1, "warmup": 1, "ms_per_step": round(cand["wall_s"] * 1e3, 1) if cand else None,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32 (BF16 denoiser)",
-        "data": "synthetic (seeded procedural scenes, held out from the denoiser's training)",
-        "config": {"workload": f"learned: {J} jobs of {S}x{S}, procedural batch-job scenes (2k-40k triangles, "
-                               "1-8 emitters) and cube rooms; reference = FP64 mean of 8 x 256 spp",
-                   "mode": "learned", "ladder_spp": LADDER, "max_depth": 6},
-        "baseline_plain_atrous": base, "served_batched_learned": cand, "speedup": ratio,
+        "data": "synthetic (seeded procedural scenes)",
+        "config": {"workload": f"learned: {J} config-4-style jobs (sides <= 384, triangles <= 300k, emitters 1-64, "
+                               "depth 4-10; every 4th the heavy-sphere scene)", "mode": "learned",
+                   "ladder_spp": LADDER},
+        "learned": rec,
     }
     print(json.dumps(line), flush=True)
-    for sc in scenes:
-        sc.close()
     return 0
 
 
@@ -801,6 +854,14 @@ def main():
         cpu = {"value": round(v, 4), "unit": "Msamples/s", "cores": threads, "kind": "port",
                "sample": f"{W}x{H} at 1 spp ({n} samples, {dt:.1f} s; CPU BVH build {build_s:.1f} s not timed)"}
 
+    # ---- learned-denoiser sub-record (rank 0, N = 1): images/s at relMSE <= 0.01 on 12
+    # config-4-style jobs, served + batched + learned against the plain tracer + A-Trous
+    learned = None
+    if rank == 0 and world == 1 and not args.no_learned:
+        r.close()
+        r = None
+        learned = learned_experiment(rg, learned_specs(12), budget_s=150.0)
+
     if rank == 0:
         line = {
             "metric": METRIC, "value": round(value, 3), "unit": "Msamples/s", "n_gpus": world,
@@ -826,9 +887,11 @@ def main():
             "roofline": roofline,
             "cpu_baseline": cpu,
             "clocks": clocks,
+            "learned": learned,
         }
         print(json.dumps(line), flush=True)
-    r.close()
+    if r is not None:
+        r.close()
     scene.close()
     if pg:
         pg.barrier()
