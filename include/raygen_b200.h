@@ -290,7 +290,9 @@ rg_status rg_render(rg_handle* h);
  * otherwise); rg_set_scene / rg_update_settings on the handle block until the
  * job ends.  rg_poll: done (0/1) and progress in [0, 1]; rg_wait: the render's
  * status, or RG_ERR_BUSY when timeout_ms (< 0: no limit) passes first;
- * rg_job_free waits for the render to end, then frees the job. */
+ * rg_job_free waits for the render to end, then frees the job.  rg_destroy on
+ * the handle waits for the job's render; a job that is done stays pollable
+ * after its handle is destroyed. */
 typedef struct rg_job rg_job;
 rg_status rg_render_async(rg_handle* h, rg_job** job);
 rg_status rg_poll(rg_job* job, int32_t* done, float* progress);

@@ -1403,6 +1403,7 @@ struct rg_job {
   std::condition_variable cv;
   bool done = false;
   rg_status status = RG_OK;
+  float finalProgress = 0.0f;  // the handle's progress when the render ended
 };
 
 rg_status rg_render_async(rg_handle* h, rg_job** out) {
@@ -1423,13 +1424,18 @@ rg_status rg_render_async(rg_handle* h, rg_job** out) {
   try {
     j->worker = std::thread([j]() {
       rg_status rs;
+      float pr;
       {
+        // the handle is released (and may be destroyed) once this lock is
+        // dropped: nothing below touches it
         std::lock_guard<std::mutex> lk(j->h->mu);
         rs = renderLocked(j->h);
+        pr = j->h->progressValue.load();
+        j->h->asyncBusy.store(false);
       }
-      j->h->asyncBusy.store(false);
       std::lock_guard<std::mutex> lk(j->mu);
       j->status = rs;
+      j->finalProgress = pr;
       j->done = true;
       j->cv.notify_all();
     });
@@ -1447,7 +1453,7 @@ rg_status rg_poll(rg_job* j, int32_t* done, float* progress) {
   if (!j) return RG_ERR_INVALID_ARGUMENT;
   std::lock_guard<std::mutex> lk(j->mu);
   if (done) *done = j->done ? 1 : 0;
-  if (progress) *progress = j->done && j->status == RG_OK ? 1.0f : j->h->progressValue.load();
+  if (progress) *progress = j->done ? j->finalProgress : j->h->progressValue.load();
   return RG_OK;
 }
 
