@@ -33,20 +33,29 @@ def render_pair(rg, scene, width, height, spp_lo, spp_hi, seed, max_depth=6):
     return noisy, normal, albedo, depth, ref
 
 
-def scene_for(rg, k):
-    """Seeded procedural job k: batch-job scenes of 2k-40k triangles with 1-8 emitters; every 8th the cube room."""
+def scene_for(rg, k, generator="narrow"):
+    """Seeded procedural job k.
+    narrow: batch-job scenes of 2k-40k triangles with 1-8 emitters; every 8th the cube room.
+    config4: the heterogeneous job mix's scenes -- triangles log-uniform 1e3-3e5 (2e6 in the
+      mix; capped for rendering time), emitters 1-64; every 8th the cube room and every 8th the
+      heavy-sphere scene (metal / dielectric spheres, 4 x 25k triangles)."""
     if k % 8 == 7:
         return rg.Scene.builtin(1, 1 + k)
     rng = np.random.default_rng(1000 + k)
+    if generator == "config4":
+        if k % 8 == 3:
+            return rg.Scene.builtin(2, 7000 + k, [25000])
+        tris = int(np.exp(rng.uniform(np.log(1e3), np.log(3e5))))
+        return rg.Scene.builtin(4, 5000 + k, [tris, int(rng.integers(1, 65))])
     tris = int(np.exp(rng.uniform(np.log(2e3), np.log(4e4))))
     return rg.Scene.builtin(4, 5000 + k, [tris, int(rng.integers(1, 9))])
 
 
-def make_examples(rg, count, size=64, spp_lo=8, spp_hi=512, first=0):
+def make_examples(rg, count, size=64, spp_lo=8, spp_hi=512, first=0, generator="narrow", max_depth=6):
     out = []
     for k in range(first, first + count):
-        sc = scene_for(rg, k)
-        out.append(render_pair(rg, sc, size, size, spp_lo, spp_hi, seed=100 + k))
+        sc = scene_for(rg, k, generator)
+        out.append(render_pair(rg, sc, size, size, spp_lo, spp_hi, seed=100 + k, max_depth=max_depth))
         sc.close()
     return out
 
@@ -56,8 +65,10 @@ def relmse(img, ref, eps=0.01):
     return float(np.mean((a - r) ** 2 / (r * r + eps)))
 
 
-def train(rg, examples, steps=2000, batch=8, lr=1e-3, seed=0, params=None, log=None):
-    d = rg.Denoiser(seed=seed, params=params)
+def train(rg, examples, steps=2000, batch=8, lr=1e-3, seed=0, params=None, log=None, denoiser=None):
+    """Adam on the examples (a list of render_pair tuples), or on the examples
+    already added to `denoiser` when one is given."""
+    d = denoiser if denoiser is not None else rg.Denoiser(seed=seed, params=params)
     for ex in examples:
         d.add_example(*ex)
     losses = []
@@ -74,12 +85,12 @@ def train(rg, examples, steps=2000, batch=8, lr=1e-3, seed=0, params=None, log=N
     return d, np.concatenate(losses) if losses else np.zeros(0)
 
 
-def evaluate(rg, denoiser, count=16, size=128, spp_lo=8, spp_hi=2048, first=100000):
+def evaluate(rg, denoiser, count=16, size=128, spp_lo=8, spp_hi=2048, first=100000, generator="narrow"):
     """relMSE against a high-spp render on held-out jobs: the noisy input, A-Trous
     (the reference's denoiser, default settings) and the learned denoiser."""
     rows = []
     for k in range(first, first + count):
-        sc = scene_for(rg, k)
+        sc = scene_for(rg, k, generator)
         noisy, normal, albedo, depth, ref = render_pair(rg, sc, size, size, spp_lo, spp_hi, seed=100 + k)
         sc.close()
         atrous = rg.denoise_atrous(noisy[..., :3], normal, depth, albedo, np.ones_like(depth))
@@ -108,15 +119,27 @@ def main():
     ap.add_argument("--batch", type=int, default=16)
     ap.add_argument("--lr", type=float, default=1e-3)
     ap.add_argument("--eval", type=int, default=16, help="held-out jobs to evaluate (0: none)")
+    ap.add_argument("--generator", default="narrow", choices=["narrow", "config4"],
+                    help="training scenes: the narrow batch-job range, or the heterogeneous job mix's")
+    ap.add_argument("--init", default=None, help="start from these weights (fine-tuning)")
     a = ap.parse_args()
     t0 = time.time()
-    ex = make_examples(rg, a.examples, a.size, a.spp_lo, a.spp_hi)
-    print(f"{len(ex)} examples in {time.time() - t0:.1f} s", flush=True)
-    d, losses = train(rg, ex, a.steps, a.batch, a.lr, log=lambda m: print(m, flush=True))
+    params = np.fromfile(a.init, np.float32) if a.init else None
+    d = rg.Denoiser(seed=0, params=params)
+    for k in range(a.examples):  # rendered pairs go to the device one at a time
+        sc = scene_for(rg, k, a.generator)
+        d.add_example(*render_pair(rg, sc, a.size, a.size, a.spp_lo, a.spp_hi, seed=100 + k))
+        sc.close()
+        if (k + 1) % 128 == 0:
+            print(f"{k + 1} examples ({time.time() - t0:.1f} s)", flush=True)
+    print(f"{a.examples} examples of {a.size}x{a.size} at {a.spp_lo}/{a.spp_hi} spp in {time.time() - t0:.1f} s",
+          flush=True)
+    d, losses = train(rg, [], a.steps, a.batch, a.lr, log=lambda m: print(m, flush=True), denoiser=d)
     d.save(a.out)
     print(f"saved {a.out}; final loss {losses[-100:].mean():.5f}", flush=True)
     if a.eval > 0:
-        print("held-out relMSE:", evaluate(rg, d, a.eval), flush=True)
+        for gen in ("narrow", "config4"):
+            print(f"held-out relMSE ({gen} scenes):", evaluate(rg, d, a.eval, generator=gen), flush=True)
 
 
 if __name__ == "__main__":
