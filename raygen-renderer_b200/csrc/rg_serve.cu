@@ -685,6 +685,11 @@ rg_status rg_server_add_scene(rg_server* s, const rg_scene_desc* scene, int64_t*
   sc->camera = scene->camera;
   sc->bytes = sc->ds->deviceBytes();
   std::lock_guard<std::mutex> lk(s->mu);
+  if (s->bytesUsed + sc->bytes > s->cfg.hbm_budget_bytes) {  // admissions meanwhile took the room
+    setLastError("rg_server_add_scene: the built scene (" + std::to_string(sc->bytes >> 20) +
+                 " MiB) no longer fits the HBM budget");
+    return RG_ERR_OUT_OF_MEMORY;
+  }
   sc->id = s->nextId++;
   s->bytesUsed += sc->bytes;
   s->bytesPeak = std::max(s->bytesPeak, s->bytesUsed);
