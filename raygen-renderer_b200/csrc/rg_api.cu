@@ -284,9 +284,9 @@ struct rg_handle {
   int W = 0, H = 0;
   bool haveResult = false;
   // wavefront
-  DevBuf<float4> rayO0, rayO1, rayD0, rayD1, hits, pathT, pathR, pathL, shO0, shO1, shO2, shD0, shD1, shD2, shC0, shC1, shC2;
+  DevBuf<float4> rayO0, rayO1, rayD0, rayD1, hits, pathT0, pathT1, pathR0, pathR1, pathL, shO0, shO1, shO2, shD0, shD1, shD2, shC0, shC1, shC2;
   DevBuf<float4> shO3, shD3, shC3;  // volume-light shadow queue, allocated for scenes with volume lights
-  DevBuf<int2> pathPS;
+  DevBuf<int2> pathPS0, pathPS1;
   DevBuf<DevJob> jobsDev;
   DevBuf<DevSegment> segs;
   DevBuf<int> counters, error, curWave;
@@ -350,8 +350,9 @@ rg_status ensureQueues(rg_handle* h, int capacity, int maxIter, bool volQueue) {
   const size_t c = (size_t)std::max(capacity, h->capacity);
   const int mi = std::max(maxIter, h->maxIter);
   bool ok = h->rayO0.alloc(c) && h->rayO1.alloc(c) && h->rayD0.alloc(c) && h->rayD1.alloc(c) && h->hits.alloc(c) &&
-            h->pathT.alloc(c) && h->pathR.alloc(c) && h->pathL.alloc(c) && h->shO0.alloc(c) && h->shO1.alloc(c) &&
-            h->shD0.alloc(c) && h->shD1.alloc(c) && h->shC0.alloc(c) && h->shC1.alloc(c) && h->pathPS.alloc(c) &&
+            h->pathT0.alloc(c) && h->pathT1.alloc(c) && h->pathR0.alloc(c) && h->pathR1.alloc(c) &&
+            h->pathL.alloc(c) && h->shO0.alloc(c) && h->shO1.alloc(c) &&
+            h->shD0.alloc(c) && h->shD1.alloc(c) && h->shC0.alloc(c) && h->shC1.alloc(c) && h->pathPS0.alloc(c) && h->pathPS1.alloc(c) &&
             h->shO2.alloc(c) && h->shD2.alloc(c) && h->shC2.alloc(c) &&
             h->counters.alloc((size_t)(mi + 1) * kCountersPerIter) && h->error.alloc(1) && h->stats.alloc(8) &&
             h->curWave.alloc(1);
@@ -374,8 +375,10 @@ DevQueues makeQueues(rg_handle* h, int maxIter) {
   Q.rayO[0] = h->rayO0.p; Q.rayO[1] = h->rayO1.p;
   Q.rayD[0] = h->rayD0.p; Q.rayD[1] = h->rayD1.p;
   Q.hits = h->hits.p;
-  Q.pathT = h->pathT.p; Q.pathR = h->pathR.p; Q.pathL = h->pathL.p;
-  Q.pathPS = h->pathPS.p;
+  Q.pathT[0] = h->pathT0.p; Q.pathT[1] = h->pathT1.p;
+  Q.pathR[0] = h->pathR0.p; Q.pathR[1] = h->pathR1.p;
+  Q.pathL = h->pathL.p;
+  Q.pathPS[0] = h->pathPS0.p; Q.pathPS[1] = h->pathPS1.p;
   Q.shO[0] = h->shO0.p; Q.shO[1] = h->shO1.p; Q.shO[2] = h->shO2.p;
   Q.shD[0] = h->shD0.p; Q.shD[1] = h->shD1.p; Q.shD[2] = h->shD2.p;
   Q.shC[0] = h->shC0.p; Q.shC[1] = h->shC1.p; Q.shC[2] = h->shC2.p;
@@ -1031,7 +1034,7 @@ static rg_status postProcess(rg_handle* h, bool restore) {
 // 32 Mi 264, 64 Mi 269 Msamples/s); bounded by a fifth of the free memory.
 static long long wavePaths(const rg_settings& s) {
   if (s.paths_per_wave > 0) return s.paths_per_wave;
-  constexpr long long kBytesPerPath = 330;  // ray / hit / path state and four shadow queues
+  constexpr long long kBytesPerPath = 370;  // rays / hits / path state (double-buffered) and four shadow queues
   long long cap = 64ll << 20;
   size_t freeB = 0, totalB = 0;
   if (cudaMemGetInfo(&freeB, &totalB) == cudaSuccess) {

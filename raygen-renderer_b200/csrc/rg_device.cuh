@@ -221,10 +221,15 @@ struct DevQueues {
   float4* rayO[2];            // (origin, path id bits)
   float4* rayD[2];            // (dir, job slot bits)
   float4* hits;               // (t, u, v, prim bits) per queue slot
-  float4* pathT;              // (beta rgb, bsdfPdf)
-  float4* pathR;              // (rrT rgb, flags bits)
-  float4* pathL;              // (L rgb, vertex bits)
-  int2* pathPS;               // (pixel, sample) of every path
+  // Path state that travels with its ray, in queue order (entry q of buffer b
+  // belongs to ray q of rayO[b] / rayD[b]): the shade kernel reads it where it
+  // reads the ray and writes it where it pushes the next ray, so no gather by
+  // path id is needed for it.
+  float4* pathT[2];           // (beta rgb, bsdfPdf)
+  float4* pathR[2];           // (rrT rgb, flags bits)
+  int2* pathPS[2];            // (pixel, sample)
+  // By path id: the radiance that shadow rays add to and the accumulation reads.
+  float4* pathL;              // (L rgb, vertex count | kVtxEyeNoHit bits)
   float4* shO[4];             // shadow queues A (area) / B (point) / C (environment) / D (volume): (origin, path id bits)
   float4* shD[4];             // (dir, tmax)
   float4* shC[4];             // (contribution rgb, job slot bits)
@@ -261,6 +266,10 @@ constexpr uint32_t F_MED_SHIFT = 12;         // medium + 1 (0 = none), 10 bits
 constexpr uint32_t F_MED_MASK = 0x3FF000u;
 constexpr uint32_t F_EYE = 1u << 24;         // next event is the eye vertex
 constexpr uint32_t F_EYE_NOHIT = 1u << 25;   // eye ray hit no triangle
+// pathL.w: the path's vertex count in the low bits, and this flag when the eye
+// ray hit no triangle (the accumulation then shows the background colour)
+constexpr int kVtxMask = (1 << 24) - 1;
+constexpr int kVtxEyeNoHit = 1 << 30;
 
 // ------------------------------------------------------------------ math ----
 struct V3 {

@@ -135,9 +135,9 @@ struct rg_server {
   DevBuf<DevJob> jobTable;
   DevBuf<DevSegment> segs;
   DevBuf<DevWave> waveSlot;
-  DevBuf<float4> rayO0, rayO1, rayD0, rayD1, hits, pathT, pathR, pathL, shO0, shO1, shO2, shD0, shD1, shD2, shC0, shC1, shC2;
+  DevBuf<float4> rayO0, rayO1, rayD0, rayD1, hits, pathT0, pathT1, pathR0, pathR1, pathL, shO0, shO1, shO2, shD0, shD1, shD2, shC0, shC1, shC2;
   DevBuf<float4> shO3, shD3, shC3;  // volume-light shadow queue
-  DevBuf<int2> pathPS;
+  DevBuf<int2> pathPS0, pathPS1;
   DevBuf<int> counters;
   DevBuf<unsigned long long> stats;
   DevBuf<int> errWord;
@@ -172,8 +172,10 @@ DevQueues serverQueues(rg_server* s) {
   Q.rayO[0] = s->rayO0.p; Q.rayO[1] = s->rayO1.p;
   Q.rayD[0] = s->rayD0.p; Q.rayD[1] = s->rayD1.p;
   Q.hits = s->hits.p;
-  Q.pathT = s->pathT.p; Q.pathR = s->pathR.p; Q.pathL = s->pathL.p;
-  Q.pathPS = s->pathPS.p;
+  Q.pathT[0] = s->pathT0.p; Q.pathT[1] = s->pathT1.p;
+  Q.pathR[0] = s->pathR0.p; Q.pathR[1] = s->pathR1.p;
+  Q.pathL = s->pathL.p;
+  Q.pathPS[0] = s->pathPS0.p; Q.pathPS[1] = s->pathPS1.p;
   Q.shO[0] = s->shO0.p; Q.shO[1] = s->shO1.p; Q.shO[2] = s->shO2.p;
   Q.shD[0] = s->shD0.p; Q.shD[1] = s->shD1.p; Q.shD[2] = s->shD2.p;
   Q.shC[0] = s->shC0.p; Q.shC[1] = s->shC1.p; Q.shC[2] = s->shC2.p;
@@ -190,8 +192,9 @@ bool allocServer(rg_server* s) {
   const size_t c = (size_t)s->cfg.paths_per_wave;
   const int slots = s->cfg.max_resident_jobs;
   bool ok = s->rayO0.alloc(c) && s->rayO1.alloc(c) && s->rayD0.alloc(c) && s->rayD1.alloc(c) && s->hits.alloc(c) &&
-            s->pathT.alloc(c) && s->pathR.alloc(c) && s->pathL.alloc(c) && s->shO0.alloc(c) && s->shO1.alloc(c) &&
-            s->shD0.alloc(c) && s->shD1.alloc(c) && s->shC0.alloc(c) && s->shC1.alloc(c) && s->pathPS.alloc(c) &&
+            s->pathT0.alloc(c) && s->pathT1.alloc(c) && s->pathR0.alloc(c) && s->pathR1.alloc(c) &&
+            s->pathL.alloc(c) && s->shO0.alloc(c) && s->shO1.alloc(c) &&
+            s->shD0.alloc(c) && s->shD1.alloc(c) && s->shC0.alloc(c) && s->shC1.alloc(c) && s->pathPS0.alloc(c) && s->pathPS1.alloc(c) &&
             s->shO2.alloc(c) && s->shD2.alloc(c) && s->shC2.alloc(c) && s->shO3.alloc(c) && s->shD3.alloc(c) &&
             s->shC3.alloc(c) && s->counters.alloc((size_t)(s->maxIter + 1) * kCountersPerIter) && s->stats.alloc(8) &&
             s->errWord.alloc(1) && s->jobTable.alloc(slots) && s->segs.alloc((size_t)slots * 2) && s->waveSlot.alloc(1);

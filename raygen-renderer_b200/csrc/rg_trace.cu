@@ -641,10 +641,10 @@ __global__ void __launch_bounds__(256) k_generate(const DevJob* __restrict__ job
     const uint32_t medFlag = (uint32_t)(J.S.globalMedium + 1) << F_MED_SHIFT;
     Q.rayO[0][p] = make_float4(o.x, o.y, o.z, __int_as_float(p));
     Q.rayD[0][p] = make_float4(d.x, d.y, d.z, __int_as_float(seg.slot));
-    Q.pathT[p] = make_float4(1.0f, 1.0f, 1.0f, 0.0f);
-    Q.pathR[p] = make_float4(1.0f, 1.0f, 1.0f, __uint_as_float(F_EYE | medFlag));
+    Q.pathT[0][p] = make_float4(1.0f, 1.0f, 1.0f, 0.0f);
+    Q.pathR[0][p] = make_float4(1.0f, 1.0f, 1.0f, __uint_as_float(F_EYE | medFlag));
+    Q.pathPS[0][p] = make_int2(pixel, (int)sample);
     Q.pathL[p] = make_float4(0.0f, 0.0f, 0.0f, __int_as_float(0));
-    Q.pathPS[p] = make_int2(pixel, (int)sample);
   }
 }
 
@@ -1017,6 +1017,8 @@ __global__ void __launch_bounds__(256) k_shade(DevScene S0, DevRender R0, const 
       bool cont = false;
       V3 no = v3(0, 0, 0), nd = v3(0, 0, 0);
       int pid = 0, slot = 0;
+      float4 outT = make_float4(0, 0, 0, 0), outR = make_float4(0, 0, 0, 0);  // state of the continuing path
+      int2 outPS = make_int2(0, 0);
       if (valid) {
         const float4 ro = Q.rayO[inB][q], rd = Q.rayD[inB][q];
         pid = __float_as_int(ro.w);
@@ -1026,19 +1028,21 @@ __global__ void __launch_bounds__(256) k_shade(DevScene S0, DevRender R0, const 
         const V3 o = xyz(ro), d = xyz(rd);
         const float4 hq = Q.hits[q];
         const int prim = __float_as_int(hq.w);
-        const float4 PT = Q.pathT[pid], PR = Q.pathR[pid], PL = Q.pathL[pid];
+        const float4 PT = Q.pathT[inB][q], PR = Q.pathR[inB][q], PL = Q.pathL[pid];
         V3 beta = xyz(PT);
         float bsdfPdf = PT.w;
         V3 rrT = xyz(PR);
         uint32_t flags = __float_as_uint(PR.w);
         V3 L = xyz(PL);
-        const int v = __float_as_int(PL.w);
+        const int vraw = __float_as_int(PL.w);
+        const int v = vraw & kVtxMask;
+        int vflags = vraw & ~kVtxMask;
         bool eye = (flags & F_EYE) != 0;
         int passes = (int)(flags & F_PASSES_MASK);
         int chroma = (int)((flags & F_CHROMA_MASK) >> F_CHROMA_SHIFT) - 1;
         int med = (int)((flags & F_MED_MASK) >> F_MED_SHIFT) - 1;
-        if (eye && prim < 0) flags |= F_EYE_NOHIT;
-        const int2 ps = Q.pathPS[pid];
+        if (eye && prim < 0) vflags |= kVtxEyeNoHit;
+        const int2 ps = Q.pathPS[inB][q];
         const int x = ps.x % R.width, y = ps.x / R.width;
         Rng rng;
         rng.init(x, y, R.width, (uint32_t)ps.y, R.seed, dimBaseOf(R));
@@ -1444,18 +1448,22 @@ __global__ void __launch_bounds__(256) k_shade(DevScene S0, DevRender R0, const 
         // write back the path state
         flags = (flags & ~(F_PASSES_MASK | F_CHROMA_MASK | F_MED_MASK | F_EYE)) | ((uint32_t)passes & F_PASSES_MASK) |
                 ((uint32_t)(chroma + 1) << F_CHROMA_SHIFT) | ((uint32_t)(med + 1) << F_MED_SHIFT) | (eye ? F_EYE : 0u);
-        Q.pathT[pid] = make_float4(beta.x, beta.y, beta.z, bsdfPdf);
-        Q.pathR[pid] = make_float4(rrT.x, rrT.y, rrT.z, __uint_as_float(flags));
-        Q.pathL[pid] = make_float4(L.x, L.y, L.z, __int_as_float(v + 1));
+        outT = make_float4(beta.x, beta.y, beta.z, bsdfPdf);
+        outR = make_float4(rrT.x, rrT.y, rrT.z, __uint_as_float(flags));
+        outPS = ps;
+        Q.pathL[pid] = make_float4(L.x, L.y, L.z, __int_as_float(((v + 1) & kVtxMask) | vflags));
         if (!cont) {
           no = v3(0, 0, 0);
         }
       }
-      // queue pushes (warp-aggregated)
+      // queue pushes (warp-aggregated); the path state goes with the next ray
       const int qslot = warpPush(&Q.counters[(iter + 1) * kCountersPerIter + C_RAYS], cont && (iter + 1) < Q.maxIter);
       if (qslot >= 0) {
         Q.rayO[outB][qslot] = make_float4(no.x, no.y, no.z, __int_as_float(pid));
         Q.rayD[outB][qslot] = make_float4(nd.x, nd.y, nd.z, __int_as_float(slot));
+        Q.pathT[outB][qslot] = outT;
+        Q.pathR[outB][qslot] = outR;
+        Q.pathPS[outB][qslot] = outPS;
       }
       const int sa = warpPush(&Q.counters[iter * kCountersPerIter + C_SHA], shA.on);
       if (sa >= 0) {
@@ -1585,9 +1593,7 @@ __global__ void __launch_bounds__(128) k_simple(const DevJob* __restrict__ jobs,
       w = w * through;
       o = h.p + normalize(d) * kSurfaceThickness;  // ThicknessRay(hit, inray.dir)
     }
-    const uint32_t flags = eyeHit ? 0u : F_EYE_NOHIT;
-    Q.pathR[p] = make_float4(1, 1, 1, __uint_as_float(flags));
-    Q.pathL[p] = make_float4(total.x, total.y, total.z, 0.0f);
+    Q.pathL[p] = make_float4(total.x, total.y, total.z, __int_as_float(eyeHit ? 0 : kVtxEyeNoHit));
   }
   warpAddStat(&Q.stats[0], nodes);
   warpAddStat(&Q.stats[1], tris);
@@ -1607,9 +1613,9 @@ __global__ void __launch_bounds__(256) k_accumulate(const DevJob* __restrict__ j
     for (int s = 0; s < seg.samples; s++) {
       const int p = seg.pathBase + s * seg.numPixels + i;
       const float4 l = Q.pathL[p];
-      const uint32_t flags = __float_as_uint(Q.pathR[p].w);
+      const bool noHit = (__float_as_int(l.w) & kVtxEyeNoHit) != 0;
       float r = l.x, g = l.y, b = l.z;
-      if ((flags & F_EYE_NOHIT) && r == 0.0f && g == 0.0f && b == 0.0f) { r = R.backR; g = R.backG; b = R.backB; }
+      if (noHit && r == 0.0f && g == 0.0f && b == 0.0f) { r = R.backR; g = R.backG; b = R.backB; }
       r = fmaxf(r, 0.0f); g = fmaxf(g, 0.0f); b = fmaxf(b, 0.0f);
       if (R.clampMax > 0.0f) { r = fminf(r, R.clampMax); g = fminf(g, R.clampMax); b = fminf(b, R.clampMax); }
       sr += r; sg += g; sb += b;
