@@ -720,10 +720,24 @@ __global__ void __launch_bounds__(128) k_connect(const DevJob* __restrict__ jobs
 //   warp runs mostly one kind of step at a time.
 // Stack entries: node group (childBase, hits | imask << 8) or triangle group
 // (triBase | 0x80000000, triangle mask).
-constexpr int kRefillIdle = 8;     // refill once this many lanes are idle
+// Refill and triangle-vote thresholds, per traversal kind (closest hit /
+// shadow rays); build-time overridable (-D) for sweeps.
+#ifndef RG_REFILL_IDLE_CLOSEST
+#define RG_REFILL_IDLE_CLOSEST 8
+#endif
+#ifndef RG_REFILL_IDLE_ANY
+#define RG_REFILL_IDLE_ANY 8
+#endif
+#ifndef RG_TRI_VOTES_CLOSEST
+#define RG_TRI_VOTES_CLOSEST 4
+#endif
+#ifndef RG_TRI_VOTES_ANY
+#define RG_TRI_VOTES_ANY 4
+#endif
+constexpr int kRefillIdle = RG_REFILL_IDLE_CLOSEST;  // refill once this many lanes are idle
 constexpr int kSharedStack = 8;    // traversal stack entries kept in shared memory (the rest in local)
 constexpr int kTraceBlock = 128;   // block size of the persistent traversal kernels
-constexpr int kTriVotes = 4;       // lanes with triangles needed to run a triangle step (swept: 2-4 best, 10 -1.6%)
+constexpr int kTriVotes = RG_TRI_VOTES_CLOSEST;  // lanes with triangles needed to run a triangle step (swept: 2-4 best, 10 -1.6%)
 
 template <bool ANY, bool MULTI>
 __device__ __forceinline__ void traverseWave8(const DevScene& S0, const DevJob* __restrict__ jobs, int count, int* fetch, const float4* __restrict__ rO,
@@ -832,7 +846,7 @@ __device__ __forceinline__ void traverseWave8(const DevScene& S0, const DevJob* 
       const bool hasTri = alive && result == 0 && tMask != 0;
       const int triVotes = __popc(__ballot_sync(0xffffffffu, hasTri));
       if (alive && result == 0) {
-        const bool doTri = hasTri && (gInner == 0 || triVotes >= kTriVotes);
+        const bool doTri = hasTri && (gInner == 0 || triVotes >= (ANY ? RG_TRI_VOTES_ANY : kTriVotes));
         if (doTri) {
           const int i = __ffs(tMask) - 1;
           tMask &= tMask - 1u;
@@ -903,7 +917,7 @@ __device__ __forceinline__ void traverseWave8(const DevScene& S0, const DevJob* 
       }
       const unsigned idle = __ballot_sync(0xffffffffu, q == -1);
       const unsigned live = __ballot_sync(0xffffffffu, q >= 0);
-      if (live == 0 || __popc(idle) >= kRefillIdle) break;
+      if (live == 0 || __popc(idle) >= (ANY ? RG_REFILL_IDLE_ANY : kRefillIdle)) break;
     }
   }
 }
