@@ -64,7 +64,7 @@ __device__ __forceinline__ bool mtClosest(V3 o, V3 d, V3 p1, V3 e1, V3 e2, Close
   const V3 pvec = cross_f(d, e2);
   const float det = dot_f(e1, pvec);
   if (fabsf(det) < 1e-8f) return false;
-  const float invDet = __fdiv_rn(1.0f, det);
+  const float invDet = __frcp_rn(det);  // the correctly rounded 1 / det, as 1.0f / det
   const V3 tvec = sub_rn(o, p1);
   const float u = __fmul_rn(dot_f(tvec, pvec), invDet);
   if (u < 0.0f || u > 1.0f) return false;
@@ -85,7 +85,7 @@ __device__ __forceinline__ bool mtAny(V3 o, V3 d, V3 p1, V3 e1, V3 e2, float max
   const V3 h = cross_f(d, e2);
   const float a = dot_f(e1, h);
   if (fabsf(a) < 1e-6f) return false;
-  const float f = __fdiv_rn(1.0f, a);
+  const float f = __frcp_rn(a);  // the correctly rounded 1 / a, as 1.0f / a
   const V3 s = sub_rn(o, p1);
   const float u = __fmul_rn(f, dot_f(s, h));
   if (u < 0.0f || u > 1.0f) return false;
