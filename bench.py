@@ -336,7 +336,8 @@ def run_jobs(args):
 
 
 LEARNED_METRIC = "images/s at relMSE<=0.01: served+batched tracer with the learned denoiser vs plain tracer + A-Trous"
-LADDER = [4, 8, 16, 32, 64, 128, 256, 512]
+LADDER = [4, 8, 16, 32, 64, 128, 256, 512, 1024, 2048]
+REF_PASSES, REF_SPP = 8, 1024  # learned experiment references: FP64 mean of 8 x 1024 spp
 
 
 def learned_specs(n, seed=11, max_side=384, max_tris=300000):
@@ -369,8 +370,9 @@ def learned_experiment(rg, specs, budget_s=None, rate=200.0):
     * served + batched + learned: all jobs submitted at once to the job server, the
       learned denoiser on every finished job (denoise mode 2).
     Each arm walks up the spp ladder until its job-mean relMSE is <= 0.01; images/s =
-    jobs / wall time of that arm at its rung.  References: the FP64 mean of 4
-    independent 512-spp renders per job (path arithmetic FP32).  Latency: the served
+    jobs / wall time of that arm at its rung; every rung's relMSE is recorded.
+    References: the FP64 mean of REF_PASSES independent REF_SPP renders per job
+    (path arithmetic FP32).  Latency: the served
     arm at its rung under Poisson arrivals at half its measured capacity and at
     `rate` requests/s (p50 / p99)."""
     import importlib
@@ -381,15 +383,15 @@ def learned_experiment(rg, specs, budget_s=None, rate=200.0):
     depth = [sp["depth"] for sp in specs]
     refs = []
     for sc, sp in zip(scenes, specs):
-        r = rg.RayRenderer(rg.RendererSettings(resolutionWidth=sp["width"], resolutionHeight=sp["height"], samples=512,
-                                               maxDepth=sp["depth"], rrDepth=RR))
+        r = rg.RayRenderer(rg.RendererSettings(resolutionWidth=sp["width"], resolutionHeight=sp["height"],
+                                               samples=REF_SPP, maxDepth=sp["depth"], rrDepth=RR))
         r.set_scene(sc)
         acc = np.zeros((sp["height"], sp["width"], 3))
-        for p in range(4):
+        for p in range(REF_PASSES):
             r.settings.seed = 50000 + p
             r.render()
             acc += r.get_hdr_result()[..., :3].astype(np.float64)
-        refs.append(acc / 4.0)
+        refs.append(acc / REF_PASSES)
         r.close()
     ref_s = time.time() - t_start
     ind = np.array([sp["in_distribution"] for sp in specs])
@@ -434,11 +436,13 @@ def learned_experiment(rg, specs, budget_s=None, rate=200.0):
     plain(4, True)
     n = len(specs)
     base = None
+    ladder_plain, ladder_served = [], []
     for spp in LADDER:
         if over_budget():
             break
         wa, ea = plain(spp, True)
         wn, en = plain(spp, False)
+        ladder_plain.append([spp, round(float(ea.mean()), 5), round(float(en.mean()), 5)])
         best_e, wall, mode = (ea, wa, "A-Trous") if ea.mean() <= en.mean() else (en, wn, "none")
         if best_e.mean() <= 0.01:
             base = dict(spp=spp, denoiser=mode, relmse=round(float(best_e.mean()), 5),
@@ -451,6 +455,7 @@ def learned_experiment(rg, specs, budget_s=None, rate=200.0):
         if over_budget():
             break
         wall, e, st = served(spp, den)
+        ladder_served.append([spp, round(float(e.mean()), 5)])
         if e.mean() <= 0.01:
             cand = dict(spp=spp, relmse=round(float(e.mean()), 5),
                         relmse_in_distribution=round(float(e[ind].mean()), 5) if ind.any() else None,
@@ -470,7 +475,9 @@ def learned_experiment(rg, specs, budget_s=None, rate=200.0):
         sc.close()
     return dict(jobs=n, in_distribution_jobs=int(ind.sum()),
                 sides=[sp["width"] for sp in specs], triangles=[sp["tris"] if sp["kind"] == 4 else 98044 for sp in specs],
-                depths=depth, reference="FP64 mean of 4 x 512 spp per job", reference_s=round(ref_s, 1),
+                depths=depth, reference=f"FP64 mean of {REF_PASSES} x {REF_SPP} spp per job",
+                reference_s=round(ref_s, 1),
+                ladder_plain_relmse=ladder_plain, ladder_served_learned_relmse=ladder_served,
                 baseline_plain_atrous=base, served_batched_learned=cand,
                 speedup=round(cand["images_per_s"] / base["images_per_s"], 2) if base and cand else None,
                 elapsed_s=round(time.time() - t_start, 1), complete=bool(base and cand))
@@ -882,7 +889,7 @@ def main():
     if rank == 0 and world == 1 and not args.no_learned:
         r.close()
         r = None
-        learned = learned_experiment(rg, learned_specs(12), budget_s=150.0)
+        learned = learned_experiment(rg, learned_specs(12), budget_s=240.0)
 
     if rank == 0:
         line = {

@@ -286,9 +286,9 @@ rg_status rg_render(rg_handle* h);
 /* Asynchronous render: the reference's render() runs its tiles on worker
  * threads and reports through progressCallback (rayrenderer.cpp:748-809,
  * :804-806); here one host thread per job runs the render of `h` and the
- * caller polls or waits.  One in-flight render per handle (RG_ERR_BUSY
- * otherwise); rg_set_scene / rg_update_settings on the handle block until the
- * job ends.  rg_poll: done (0/1) and progress in [0, 1]; rg_wait: the render's
+ * caller polls or waits.  One in-flight render per handle: while a job runs,
+ * rg_render_async, rg_render, rg_set_scene and rg_update_settings on the
+ * handle return RG_ERR_BUSY.  rg_poll: done (0/1) and progress in [0, 1]; rg_wait: the render's
  * status, or RG_ERR_BUSY when timeout_ms (< 0: no limit) passes first;
  * rg_job_free waits for the render to end, then frees the job.  rg_destroy on
  * the handle waits for the job's render; a job that is done stays pollable

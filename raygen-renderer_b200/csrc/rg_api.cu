@@ -568,6 +568,10 @@ rg_status rg_destroy(rg_handle* h) {
 
 rg_status rg_update_settings(rg_handle* h, const rg_settings* s) {
   if (!h || !s) return RG_ERR_INVALID_ARGUMENT;
+  if (h->asyncBusy.load()) {
+    setLastError("rg_update_settings: an rg_render_async job of this handle is in flight");
+    return RG_ERR_BUSY;
+  }
   if (s->denoise_levels < 1 || s->denoise_levels > kMaxDenoiseLevels) {
     setLastError("rg_update_settings: denoise_levels must be in [1, " + std::to_string(kMaxDenoiseLevels) + "]");
     return RG_ERR_INVALID_ARGUMENT;
@@ -976,6 +980,10 @@ extern "C" {
 
 rg_status rg_set_scene(rg_handle* h, const rg_scene_desc* d) {
   if (!h || !d) return RG_ERR_INVALID_ARGUMENT;
+  if (h->asyncBusy.load()) {
+    setLastError("rg_set_scene: an rg_render_async job of this handle is in flight");
+    return RG_ERR_BUSY;
+  }
   std::lock_guard<std::mutex> lk(h->mu);
   h->hasScene = false;
   h->haveResult = false;

@@ -7,10 +7,10 @@ oracle (and, in test_gpu_golden_ref.py, the device) to them.
 
 Tolerances:
 * ray batches: hit triangle ids identical except exact ties (coplanar
-  triangles at the same distance: t agrees within 1e-5 relative) and edge
-  grazes (the nearer of the two hits lies within 1e-5 of its triangle's edge
-  in barycentrics, where rounding decides inside or outside) -- together at
-  most 0.1% of rays; t within 1e-5 relative + 2e-6 absolute
+  triangles at the same distance: t agrees within 1e-5 relative; any number)
+  and edge grazes (the nearer of the two hits lies within 1e-5 of its
+  triangle's edge in barycentrics, where rounding decides inside or outside;
+  at most 0.1% of rays); t within 1e-5 relative + 2e-6 absolute
   (view-space coordinates reach 20, where floats are 2e-6 apart, so a hit a
   hundredth of a unit from the ray origin carries that absolute error); barycentrics as a
   hit point: |sum(dw_i v_i)| <= 1e-5 x the distance from the ray origin to the
@@ -42,25 +42,33 @@ def load(name):
     return np.load(os.path.join(GOLD, name))
 
 
-def edge_graze_or_tie(tuv, prim, rtuv, rprim, eps=1e-5):
-    """Two different closest hits of one ray are acceptable when they are at
-    the same distance (a tie) or when the nearer one sits on an edge of its
-    triangle (a graze that the other side's rounding rejected)."""
-    if prim >= 0 and rprim >= 0 and abs(tuv[0] - rtuv[0]) <= 1e-5 * abs(rtuv[0]) + 2e-6:
-        return True
+def tie(tuv, prim, rtuv, rprim):
+    """Two different closest hits at the same distance (coplanar triangles)."""
+    return prim >= 0 and rprim >= 0 and abs(tuv[0] - rtuv[0]) <= 1e-5 * abs(rtuv[0]) + 2e-6
+
+
+def edge_graze(tuv, prim, rtuv, rprim, eps=1e-5):
+    """The nearer of two different closest hits sits on an edge of its triangle
+    (a graze that the other side's rounding rejected)."""
     near = tuv if (rprim < 0 or (prim >= 0 and tuv[0] < rtuv[0])) else rtuv
     u, v = float(near[1]), float(near[2])
     return min(u, v, 1.0 - u - v) <= eps
 
 
 def check_rays(key, R, tuv, prim, anyhit=None):
-    """Compare one ray batch with the reference's results (ties excepted)."""
+    """Compare one ray batch with the reference's results: every different hit id
+    is an exact tie (any number: the cube room's boxes stand on its floor) or an
+    edge graze (at most 0.1% of the rays)."""
     rays, rprim, rtuv = R[f"{key}_rays"], R[f"{key}_prim"], R[f"{key}_tuv"]
     same = prim == rprim
-    assert same.mean() >= 0.999, f"{key}: {same.mean():.5f} of hit ids equal"
+    grazes = 0
     for i in np.nonzero(~same)[0]:
-        assert edge_graze_or_tie(tuv[i], prim[i], rtuv[i], rprim[i]), \
+        if tie(tuv[i], prim[i], rtuv[i], rprim[i]):
+            continue
+        assert edge_graze(tuv[i], prim[i], rtuv[i], rprim[i]), \
             f"{key} ray {i}: id {prim[i]} t {tuv[i, 0]} against the reference's {rprim[i]} t {rtuv[i, 0]}"
+        grazes += 1
+    assert grazes <= 0.001 * len(prim), f"{key}: {grazes} edge grazes"
     hit = same & (rprim >= 0)
     np.testing.assert_allclose(tuv[hit, 0], rtuv[hit, 0], rtol=1e-5, atol=2e-6)
     if anyhit is not None:

@@ -66,9 +66,9 @@ def test_one_render_in_flight_per_handle(rg):
     with pytest.raises(rg.RayGenError) as e:
         r.render_async()
     assert e.value.code == rg.RG_ERR_BUSY
-    # the blocking entry point refuses too (called directly: the Python wrapper
-    # would first update the settings, which waits for the job)
+    # the blocking entry point and the scene / settings updates refuse too
     assert r._lib.rg_render(r._h) == rg.RG_ERR_BUSY
+    assert r._lib.rg_set_scene(r._h, sc.ptr) == rg.RG_ERR_BUSY
     r.cancel()
     with pytest.raises(rg.RayGenError):
         job.wait()
