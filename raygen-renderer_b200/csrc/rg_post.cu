@@ -95,12 +95,13 @@ __global__ void __launch_bounds__(256) k_atrous(int w, int h, const float4* __re
                   snz = __half2float(normal[si * 3 + 2]) * 2.0f - 1.0f;
       const float sl = lum3(sc.x, sc.y, sc.z);
       const float ld = sl - cl;
-      const float wc = expf(-(ld * ld) * invC2);
       float nd = snx * cnx + sny * cny + snz * cnz;
       if (nd < 0.0f) nd = 0.0f;
-      const float wn = powf(nd, sigN);
-      const float wd = expf(-fabsf(__half2float(depth[si]) - cd) * dScale);
-      const float wgt = kw[kx] * kw[ky] * wc * wn * wd;
+      // exp(-ld^2 / 2sc^2) * max(n.n', 0)^sigN * exp(-|dd| / (sd step)) as one
+      // base-2 exponential of the summed logarithms (powf(0, 0) = 1 kept)
+      const float lnC = -(ld * ld) * invC2 - fabsf(__half2float(depth[si]) - cd) * dScale;
+      const float lg2N = sigN == 0.0f ? 0.0f : (nd > 0.0f ? sigN * __log2f(nd) : -INFINITY);
+      const float wgt = kw[kx] * kw[ky] * exp2f(fmaf(lnC, 1.44269504088896341f, lg2N));
       sx += sc.x * wgt; sy += sc.y * wgt; sz += sc.z * wgt;
       ws += wgt;
     }
