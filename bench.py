@@ -274,7 +274,7 @@ def run_jobs(args):
     tune_s = time.time() - t0
     srv = rg.RenderServer(rg.RendererSettings(rrDepth=RR), hbm_budget_gb=120.0, max_resident_jobs=256,
                           paths_per_wave=tuned["paths_per_wave"], shade_blocks_per_sm=tuned["shade_blocks_per_sm"],
-                          trace_blocks_per_sm=tuned["trace_blocks_per_sm"])
+                          trace_blocks_per_sm=tuned["trace_blocks_per_sm"], wave_fill=tuned["wave_fill"])
     rng = np.random.default_rng(7)
     clock = ClockSampler(0)
     clock.start()
@@ -829,13 +829,20 @@ def main():
     r.set_scene(e2e_scene)
     r.render()
     r.get_hdr_result(out=hdr)
-    e2e_times = []
+    e2e_times, e2e_phases = [], {"set_scene": [], "bvh_build_device": [], "render": [], "readback": []}
     for _ in range(e2e_steps):
         t0 = time.time()
         r.set_scene(e2e_scene)
+        t1 = time.time()
         r.render()
+        t2 = time.time()
         out = r.get_hdr_result(out=hdr)
-        e2e_times.append(time.time() - t0)
+        t3 = time.time()
+        e2e_times.append(t3 - t0)
+        e2e_phases["set_scene"].append(1e3 * (t1 - t0))
+        e2e_phases["bvh_build_device"].append(r.stats()["build_ms"])
+        e2e_phases["render"].append(1e3 * (t2 - t1))
+        e2e_phases["readback"].append(1e3 * (t3 - t2))
     e2e_s = sum(e2e_times)
     r.set_scene(scene)
     e2e_value = (Wr * Hr * args.spp * e2e_steps) / e2e_s / 1e6
@@ -907,7 +914,9 @@ def main():
             "e2e": {"value": round(e2e_value, 3), "unit": "Msamples/s", "h2d_bytes_per_step": int(h2d),
                     "d2h_bytes_per_step": int(d2h), "host_buffers": h2d_source,
                     "ms_per_step": round(1e3 * e2e_s / e2e_steps, 1),
-                    "ms_per_step_min_max": [round(1e3 * min(e2e_times), 1), round(1e3 * max(e2e_times), 1)]},
+                    "ms_per_step_min_max": [round(1e3 * min(e2e_times), 1), round(1e3 * max(e2e_times), 1)],
+                    "phases_ms_median_max": {k: [round(statistics.median(v), 2), round(max(v), 2)]
+                                             for k, v in e2e_phases.items()}},
             "gpu_launches": int(launches),
             "host_ms": {"setup_median": round(statistics.median(host_setup), 2),
                         "setup_max": round(max(host_setup), 2),

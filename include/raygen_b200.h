@@ -424,9 +424,12 @@ rg_status rg_tc_gemm_bf16(int32_t M, int32_t N, int32_t K, const uint16_t* A, co
 
 /* ---- learned denoiser (kernel-predicting CNN on the tensor cores) --------
  * No reference counterpart: the reference denoises with A-Trous only, which
- * stays the renderer's default and its fallback.  Six 3x3 convolutions (10
- * input features: log radiance, albedo, normal and depth guides; 32 channels)
- * predict a 5x5 filter per pixel that is applied to the noisy radiance.
+ * stays the renderer's default and its fallback.  Six 3x3 convolutions (11
+ * input features: log radiance, albedo, normal and depth guides and the noise
+ * level log2(1 + spp) / 12; 32 channels) predict a 5x5 filter per pixel that
+ * is applied to the noisy radiance.  `spp` below is the samples per pixel of
+ * the noisy image (>= 0); the renderer and the job server pass their
+ * per-pixel sample counts instead (adaptive sampling included).
  * Convolutions run forward and backward as BF16 tcgen05 GEMMs with FP32
  * accumulation; training (relMSE loss against a high-spp render, Adam) runs
  * on the device.  Images: noisy/ref w*h RGBA floats, normal and albedo w*h*3
@@ -440,16 +443,16 @@ rg_status rg_denoiser_get_params(rg_denoiser* d, float* out, size_t n);
 rg_status rg_denoiser_set_params(rg_denoiser* d, const float* in, size_t n);
 /* Training pairs (all of one size) kept on the device. */
 rg_status rg_denoiser_add_example(rg_denoiser* d, int32_t w, int32_t h, const float* noisy_rgba, const float* normal,
-                                  const float* albedo, const float* depth, const float* ref_rgba);
+                                  const float* albedo, const float* depth, float spp, const float* ref_rgba);
 rg_status rg_denoiser_clear_examples(rg_denoiser* d);
 /* `steps` Adam steps on random batches of `batch` examples; losses[steps] (may be NULL). */
 rg_status rg_denoiser_train(rg_denoiser* d, int32_t steps, int32_t batch, float lr, float* losses);
 /* Loss and gradient (rg_denoiser_num_params floats) on `count` images of w x h. */
 rg_status rg_denoiser_gradients(rg_denoiser* d, int32_t count, int32_t w, int32_t h, const float* noisy_rgba,
-                                const float* normal, const float* albedo, const float* depth, const float* ref_rgba,
-                                float* loss, float* grad);
+                                const float* normal, const float* albedo, const float* depth, float spp,
+                                const float* ref_rgba, float* loss, float* grad);
 rg_status rg_denoiser_apply(rg_denoiser* d, int32_t w, int32_t h, const float* noisy_rgba, const float* normal,
-                            const float* albedo, const float* depth, float* out_rgba);
+                            const float* albedo, const float* depth, float spp, float* out_rgba);
 /* Device time (CUDA events) of the last rg_denoiser_apply (features, six
  * convolutions, kernel application) and of the mean step of the last
  * rg_denoiser_train call (batch gather, forward, backward, Adam, repacking). */
@@ -501,6 +504,10 @@ typedef struct rg_server_config {
   int32_t max_depth_cap;      /* largest max_depth a job may use [10]          */
   int32_t shade_blocks_per_sm;  /* shade / generate / accumulate width [0: 4]  */
   int32_t trace_blocks_per_sm;  /* traversal width [0: occupancy limit]        */
+  int32_t wave_fill;          /* 0: each wave shared evenly by the resident jobs;
+                                 1: each wave filled from as few jobs as possible,
+                                 in rotating order (fewer scenes per wave, more
+                                 cache reuse; a large job delays the others) [0] */
 } rg_server_config;
 
 /* One render request.  The scene description is borrowed: it must stay valid

@@ -4,7 +4,8 @@ The kernel-predicting CNN (KPCN, after Bako et al. 2017, "Kernel-predicting
 convolutional networks for denoising Monte Carlo renderings") in numpy, forward
 and backward, with the device's rounding points:
 * features X0 [N, H, W, 16]: log1p(max(radiance, 0)) (3), albedo (3), the
-  normal guide n * 0.5 + 0.5 (3), the depth guide (1), zeros (6) -- BF16;
+  normal guide n * 0.5 + 0.5 (3), the depth guide (1), the noise level
+  log2(1 + spp) / 12 (1), zeros (5) -- BF16;
 * five 3x3 convolutions with ReLU (16 -> 32, then 32 -> 32), zero padding,
   weights BF16, accumulation wide, outputs rounded to BF16;
 * a 3x3 convolution 32 -> 25 logits (padded to 32 channels), FP32;
@@ -53,14 +54,16 @@ def bf16(a):
     return r.astype(np.uint32).view(np.float32).astype(np.float64)
 
 
-def features(noisy, normal, albedo, depth, exact=False):
-    """noisy [N,H,W,>=3], normal/albedo [N,H,W,3] guides, depth [N,H,W] -> X0 [N,H,W,16]."""
+def features(noisy, normal, albedo, depth, spp=8.0, exact=False):
+    """noisy [N,H,W,>=3], normal/albedo [N,H,W,3] guides, depth [N,H,W], samples per
+    pixel (a number or an [N,H,W] array) -> X0 [N,H,W,16]."""
     N, H, W = depth.shape
     X = np.zeros((N, H, W, 16))
     X[..., 0:3] = np.log1p(np.maximum(noisy[..., :3], 0.0))
     X[..., 3:6] = albedo
     X[..., 6:9] = normal
     X[..., 9] = depth
+    X[..., 10] = np.log2(1.0 + np.maximum(np.asarray(spp, np.float64), 0.0)) / 12.0
     return X if exact else bf16(X)
 
 
@@ -163,15 +166,15 @@ def backward(params, X0, noisy, ref, exact=False):
 
 
 def init_params(seed):
-    """He-normal weights (fan-in 9 * Cin; the 10 real input channels for layer 1), zero biases;
+    """He-normal weights (fan-in 9 * Cin; the 11 real input channels for layer 1), zero biases;
     the 7 padding logits of the last layer stay zero."""
     rng = np.random.default_rng(seed)
     ps = []
     for l, cin in enumerate(CIN):
-        fan = 9 * (10 if l == 0 else cin)
+        fan = 9 * (11 if l == 0 else cin)
         W = rng.standard_normal((C, 9, cin)) * np.sqrt(2.0 / fan)
         if l == 0:
-            W[:, :, 10:] = 0.0
+            W[:, :, 11:] = 0.0
         if l == 5:
             W *= 0.1
             W[KP:] = 0.0

@@ -168,7 +168,7 @@ class rg_stats(C.Structure):
 class rg_server_config(C.Structure):
     _fields_ = [("hbm_budget_bytes", C.c_uint64), ("max_resident_jobs", C.c_int32),
                 ("paths_per_wave", C.c_int32), ("max_depth_cap", C.c_int32),
-                ("shade_blocks_per_sm", C.c_int32), ("trace_blocks_per_sm", C.c_int32)]
+                ("shade_blocks_per_sm", C.c_int32), ("trace_blocks_per_sm", C.c_int32), ("wave_fill", C.c_int32)]
 
 
 class rg_job_desc(C.Structure):
@@ -242,11 +242,14 @@ def load_library(path: str = LIB_PATH) -> C.CDLL:
         "rg_denoiser_destroy": (C.c_int, [C.c_void_p]),
         "rg_denoiser_get_params": (C.c_int, [C.c_void_p, P(C.c_float), C.c_size_t]),
         "rg_denoiser_set_params": (C.c_int, [C.c_void_p, P(C.c_float), C.c_size_t]),
-        "rg_denoiser_add_example": (C.c_int, [C.c_void_p, C.c_int32, C.c_int32] + [P(C.c_float)] * 5),
+        "rg_denoiser_add_example": (C.c_int, [C.c_void_p, C.c_int32, C.c_int32] + [P(C.c_float)] * 4
+                                    + [C.c_float, P(C.c_float)]),
         "rg_denoiser_clear_examples": (C.c_int, [C.c_void_p]),
         "rg_denoiser_train": (C.c_int, [C.c_void_p, C.c_int32, C.c_int32, C.c_float, P(C.c_float)]),
-        "rg_denoiser_gradients": (C.c_int, [C.c_void_p, C.c_int32, C.c_int32, C.c_int32] + [P(C.c_float)] * 7),
-        "rg_denoiser_apply": (C.c_int, [C.c_void_p, C.c_int32, C.c_int32] + [P(C.c_float)] * 5),
+        "rg_denoiser_gradients": (C.c_int, [C.c_void_p, C.c_int32, C.c_int32, C.c_int32] + [P(C.c_float)] * 4
+                                  + [C.c_float] + [P(C.c_float)] * 3),
+        "rg_denoiser_apply": (C.c_int, [C.c_void_p, C.c_int32, C.c_int32] + [P(C.c_float)] * 4
+                              + [C.c_float, P(C.c_float)]),
         "rg_set_denoiser": (C.c_int, [C.c_void_p, C.c_void_p]),
         "rg_denoiser_timing": (C.c_int, [C.c_void_p, P(C.c_float), P(C.c_float)]),
         "rg_server_set_denoiser": (C.c_int, [C.c_void_p, C.c_void_p]),
@@ -802,7 +805,9 @@ class Denoiser:
 
     Images are H x W (x C) float arrays: noisy / ref RGBA, normal and albedo guides
     (as RayRenderer.get_aovs returns them), depth guide H x W.  Batched calls take
-    N x H x W (x C) arrays."""
+    N x H x W (x C) arrays.  `spp` is the noisy image's samples per pixel, an input
+    of the network (its noise level); the renderer and the job server pass their
+    per-pixel sample counts themselves."""
 
     def __init__(self, seed: int = 0, params=None):
         self._lib = load_library()
@@ -816,7 +821,7 @@ class Denoiser:
 
     @classmethod
     def pretrained(cls, path: Optional[str] = None) -> "Denoiser":
-        """The network trained by kpcn_train.py on tracer-rendered 8 / 512 spp pairs (shipped weights)."""
+        """The network trained by kpcn_train.py on tracer-rendered pairs (shipped weights)."""
         d = cls(seed=0)
         d.load(path or cls.WEIGHTS)
         return d
@@ -843,14 +848,25 @@ class Denoiser:
         self.params = np.fromfile(path, np.float32)
 
     @staticmethod
-    def _f(a, shape_tail):
-        return np.ascontiguousarray(a, np.float32)
+    def _inputs(depth, noisy, normal, albedo, *rgba):
+        """Contiguous float32 arrays of the shapes the C ABI reads: RGB images get an
+        alpha channel of 1; every image must match depth's N x H x W."""
+        depth = np.ascontiguousarray(depth, np.float32)
+        out = [depth]
+        for a, ch in [(noisy, 4), (normal, 3), (albedo, 3)] + [(r, 4) for r in rgba]:
+            a = np.asarray(a, np.float32)
+            if ch == 4 and a.shape[-1] == 3:
+                a = np.concatenate([a, np.ones(a.shape[:-1] + (1,), np.float32)], -1)
+            if a.shape != depth.shape + (ch,):
+                raise ValueError(f"image of shape {a.shape}: expected {depth.shape + (ch,)}")
+            out.append(np.ascontiguousarray(a))
+        return out
 
-    def add_example(self, noisy, normal, albedo, depth, ref) -> None:
-        noisy, normal, albedo, depth, ref = (np.ascontiguousarray(a, np.float32) for a in (noisy, normal, albedo, depth, ref))
+    def add_example(self, noisy, normal, albedo, depth, ref, spp: float = 8.0) -> None:
+        depth, noisy, normal, albedo, ref = self._inputs(depth, noisy, normal, albedo, ref)
         h, w = depth.shape
         _check(self._lib.rg_denoiser_add_example(self._h, w, h, _fptr(noisy), _fptr(normal), _fptr(albedo),
-                                                 _fptr(depth), _fptr(ref)))
+                                                 _fptr(depth), float(spp), _fptr(ref)))
 
     def clear_examples(self) -> None:
         _check(self._lib.rg_denoiser_clear_examples(self._h))
@@ -860,22 +876,22 @@ class Denoiser:
         _check(self._lib.rg_denoiser_train(self._h, steps, batch, lr, _fptr(losses)))
         return losses[:steps]
 
-    def gradients(self, noisy, normal, albedo, depth, ref):
+    def gradients(self, noisy, normal, albedo, depth, ref, spp: float = 8.0):
         """(loss, gradient) for a batch N x H x W (relMSE against ref)."""
-        noisy, normal, albedo, depth, ref = (np.ascontiguousarray(a, np.float32) for a in (noisy, normal, albedo, depth, ref))
+        depth, noisy, normal, albedo, ref = self._inputs(depth, noisy, normal, albedo, ref)
         n, h, w = depth.shape
         loss = np.zeros(1, np.float32)
         grad = np.zeros(self.num_params(), np.float32)
         _check(self._lib.rg_denoiser_gradients(self._h, n, w, h, _fptr(noisy), _fptr(normal), _fptr(albedo),
-                                               _fptr(depth), _fptr(ref), _fptr(loss), _fptr(grad)))
+                                               _fptr(depth), float(spp), _fptr(ref), _fptr(loss), _fptr(grad)))
         return float(loss[0]), grad
 
-    def apply(self, noisy, normal, albedo, depth) -> np.ndarray:
-        noisy, normal, albedo, depth = (np.ascontiguousarray(a, np.float32) for a in (noisy, normal, albedo, depth))
+    def apply(self, noisy, normal, albedo, depth, spp: float = 8.0) -> np.ndarray:
+        depth, noisy, normal, albedo = self._inputs(depth, noisy, normal, albedo)
         h, w = depth.shape
         out = np.empty((h, w, 4), np.float32)
         _check(self._lib.rg_denoiser_apply(self._h, w, h, _fptr(noisy), _fptr(normal), _fptr(albedo), _fptr(depth),
-                                           _fptr(out)))
+                                           float(spp), _fptr(out)))
         return out
 
     def timing(self) -> dict:
@@ -909,16 +925,17 @@ def tonemap(hdr_rgba: np.ndarray) -> np.ndarray:
 class RenderServer:
     """Resident multi-job server: continuous batching of many render jobs on one GPU.
 
-    Jobs are admitted under an HBM budget; every wave mixes paths of all resident
-    jobs; finished jobs are resolved (optionally A-Trous denoised) on the device.
+    Jobs are admitted under an HBM budget; waves mix paths of the resident jobs
+    (shared evenly, or with wave_fill=1 filled from as few jobs as possible);
+    finished jobs are resolved (optionally denoised) on the device.
     """
 
     def __init__(self, settings: Optional[RendererSettings] = None, hbm_budget_gb: float = 120.0,
                  max_resident_jobs: int = 256, paths_per_wave: int = 8 << 20, max_depth_cap: int = 10,
-                 shade_blocks_per_sm: int = 0, trace_blocks_per_sm: int = 0):
+                 shade_blocks_per_sm: int = 0, trace_blocks_per_sm: int = 0, wave_fill: int = 0):
         self._lib = load_library()
         cfg = self._config(hbm_budget_gb, max_resident_jobs, paths_per_wave, max_depth_cap, shade_blocks_per_sm,
-                           trace_blocks_per_sm)
+                           trace_blocks_per_sm, wave_fill)
         base = (settings or RendererSettings()).to_c()
         self._h = C.c_void_p()
         _check(self._lib.rg_server_create(C.byref(base), C.byref(cfg), C.byref(self._h)))
@@ -926,7 +943,7 @@ class RenderServer:
 
     @staticmethod
     def _config(hbm_budget_gb=120.0, max_resident_jobs=256, paths_per_wave=8 << 20, max_depth_cap=10,
-                shade_blocks_per_sm=0, trace_blocks_per_sm=0):
+                shade_blocks_per_sm=0, trace_blocks_per_sm=0, wave_fill=0):
         cfg = rg_server_config()
         load_library().rg_server_config_default(C.byref(cfg))
         cfg.hbm_budget_bytes = int(hbm_budget_gb * (1 << 30))
@@ -935,12 +952,13 @@ class RenderServer:
         cfg.max_depth_cap = max_depth_cap
         cfg.shade_blocks_per_sm = shade_blocks_per_sm
         cfg.trace_blocks_per_sm = trace_blocks_per_sm
+        cfg.wave_fill = wave_fill
         return cfg
 
     @staticmethod
     def autotune(probe, settings: Optional[RendererSettings] = None, hbm_budget_gb: float = 120.0,
                  max_resident_jobs: int = 256, max_depth_cap: int = 10) -> dict:
-        """Pick paths_per_wave / shade_blocks_per_sm / trace_blocks_per_sm for a job mix.
+        """Pick paths_per_wave / shade_blocks_per_sm / trace_blocks_per_sm / wave_fill for a job mix.
 
         probe: list of (scene, width, height, samples, max_depth, seed).  Returns the
         constructor keyword arguments of the fastest configuration plus its probe time."""
@@ -955,7 +973,7 @@ class RenderServer:
         best = C.c_double()
         _check(lib.rg_server_autotune(C.byref(base), jobs, len(probe), C.byref(cfg), C.byref(best)))
         return {"paths_per_wave": cfg.paths_per_wave, "shade_blocks_per_sm": cfg.shade_blocks_per_sm,
-                "trace_blocks_per_sm": cfg.trace_blocks_per_sm, "probe_ms": best.value}
+                "trace_blocks_per_sm": cfg.trace_blocks_per_sm, "wave_fill": cfg.wave_fill, "probe_ms": best.value}
 
     def add_scene(self, scene: Scene) -> int:
         """Upload and build a scene once; jobs submitted with its id reuse it."""

@@ -725,11 +725,6 @@ rg_status prepareScene(const rg_scene_desc* d, int bins, bool wide, cudaStream_t
       setLastError("object material / medium index out of range");
       return RG_ERR_INVALID_ARGUMENT;
     }
-  for (int i = 0; i < nt; i++)
-    if (d->tri_mesh[i] < 0 || d->tri_mesh[i] >= d->num_meshes) {
-      setLastError("tri_mesh index out of range");
-      return RG_ERR_INVALID_ARGUMENT;
-    }
   for (int i = 0; i < d->num_materials; i++)
     if (d->materials[i].texture >= d->num_textures) {
       setLastError("material texture index out of range");
@@ -770,16 +765,33 @@ rg_status prepareScene(const rg_scene_desc* d, int bins, bool wide, cudaStream_t
       }
     }
   }
+  // one pass over the triangles: mesh index check, triangles per mesh, and the
+  // triangles of emissive meshes (area lights, rayrenderer.cpp:333-353: emissive
+  // objects with meshes, object order)
+  std::vector<int> objMat(d->num_objects);
+  for (int i = 0; i < d->num_objects; i++) objMat[i] = d->objects[i].material;
+  std::vector<std::vector<int>> objMeshes(d->num_objects);
+  for (int i = 0; i < d->num_meshes; i++) objMeshes[d->mesh_object[i]].push_back(i);
+  std::vector<char> isLightMesh(d->num_meshes, 0);
+  for (int o = 0; o < d->num_objects; o++)
+    if (d->materials[objMat[o]].emission > 0.0f)
+      for (int m : objMeshes[o]) isLightMesh[m] = 1;
+  std::vector<int> meshTriCount(d->num_meshes, 0);
+  std::vector<std::vector<int>> meshTris(d->num_meshes);
+  for (int i = 0; i < nt; i++) {
+    const int m = d->tri_mesh[i];
+    if (m < 0 || m >= d->num_meshes) {
+      setLastError("tri_mesh index out of range");
+      return RG_ERR_INVALID_ARGUMENT;
+    }
+    meshTriCount[m]++;
+    if (isLightMesh[m]) meshTris[m].push_back(i);
+  }
   out.reset(new DeviceScene());
   DeviceScene& ds = *out;
   ds.numTris = nt;
   view = viewMatrix(d->camera);
   ds.hasUV = d->uvs != nullptr && d->num_textures > 0;
-  // tables
-  std::vector<int> meshTriCount(d->num_meshes, 0);
-  for (int i = 0; i < nt; i++) meshTriCount[d->tri_mesh[i]]++;
-  std::vector<int> objMat(d->num_objects);
-  for (int i = 0; i < d->num_objects; i++) objMat[i] = d->objects[i].material;
   std::vector<DevMaterial> mats(d->num_materials);
   for (int i = 0; i < d->num_materials; i++) mats[i] = toDev(d->materials[i]);
   MediaTables MT;
@@ -789,23 +801,17 @@ rg_status prepareScene(const rg_scene_desc* d, int bins, bool wide, cudaStream_t
   ds.globalMedium = MT.globalMedium;
   ds.hasHaze = MT.hasHaze;
   // area lights (rayrenderer.cpp:333-353): emissive objects with meshes, object order
-  std::vector<std::vector<int>> objMeshes(d->num_objects);
-  for (int i = 0; i < d->num_meshes; i++) objMeshes[d->mesh_object[i]].push_back(i);
-  std::vector<std::vector<int>> meshTris(d->num_meshes);
   std::vector<int> areaLightObj, lightMeshList;
   std::vector<int2> lightObjMeshes(std::max(1, d->num_objects), make_int2(0, 0));
   std::vector<int2> lightMeshTris(std::max(1, d->num_meshes), make_int2(0, 0));
   std::vector<float4> lightTris;
   {
-    std::vector<char> isLightMesh(d->num_meshes, 0);
     for (int o = 0; o < d->num_objects; o++) {
       if (!(d->materials[objMat[o]].emission > 0.0f) || objMeshes[o].empty()) continue;
       areaLightObj.push_back(o);
       lightObjMeshes[o] = make_int2((int)lightMeshList.size(), (int)objMeshes[o].size());
-      for (int m : objMeshes[o]) { lightMeshList.push_back(m); isLightMesh[m] = 1; }
+      for (int m : objMeshes[o]) lightMeshList.push_back(m);
     }
-    for (int i = 0; i < nt; i++)
-      if (isLightMesh[d->tri_mesh[i]]) meshTris[d->tri_mesh[i]].push_back(i);
     for (int m = 0; m < d->num_meshes; m++) {
       if (!isLightMesh[m]) continue;
       lightMeshTris[m] = make_int2((int)(lightTris.size() / 6), (int)meshTris[m].size());
@@ -1313,7 +1319,7 @@ rg_status renderLocked(rg_handle* h) {
   launchResolve(N, h->sum.p, h->cnt.p, h->camera.exposure, h->hdr.p, st);
   if (s.enable_denoise && h->denoiser) {
     const rg_status ds = kpcnDenoiseDevice(*kpcnOf(h->denoiser), W, H, h->hdr.p, h->aovNormal.p, h->aovAlbedo.p,
-                                           h->aovDepth.p, s.denoise_intensity, h->ldr.p, st);
+                                           h->aovDepth.p, h->cnt.p, s.denoise_intensity, h->ldr.p, st);
     if (ds != RG_OK) {
       cudaStreamSynchronize(st);
       cudaEventDestroy(t0);

@@ -171,7 +171,7 @@ rg_status buildDeviceBvh(DeviceScene& ds, int nbins, bool wide, cudaStream_t st,
 struct KpcnNet;
 KpcnNet* kpcnOf(rg_denoiser* d);
 rg_status kpcnDenoiseDevice(KpcnNet& n, int W, int H, const float4* noisy, const __half* normal, const __half* albedo,
-                            const __half* depth, float intensity, float4* out, cudaStream_t st);
+                            const __half* depth, const int* cnt, float intensity, float4* out, cudaStream_t st);
 rg_status prepareScene(const rg_scene_desc* d, int bins, bool wide, cudaStream_t st, int* errWord,
                        std::unique_ptr<DeviceScene>& out, DevScene& S, Mat4& view, float* buildMs);
 

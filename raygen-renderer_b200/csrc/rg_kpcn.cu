@@ -3,8 +3,8 @@
 //
 // Network (after Bako et al. 2017, kernel-predicting convolutional networks
 // for Monte Carlo denoising): features [P x 16] = log1p(radiance), albedo,
-// normal and depth guides (the A-Trous guides, rayrenderer.cpp:819-844) and 6
-// zero channels; five 3x3 convolutions with ReLU (16 -> 32, then 32 -> 32);
+// normal and depth guides (the A-Trous guides, rayrenderer.cpp:819-844), the
+// noise level log2(1 + samples per pixel) / 12 and 5 zero channels; five 3x3 convolutions with ReLU (16 -> 32, then 32 -> 32);
 // a 3x3 convolution to 25 logits; softmax -> a 5 x 5 kernel per pixel applied
 // to the noisy radiance (clamp to edge).  Loss: relMSE (o - r)^2 / (r^2 + 0.01).
 //
@@ -108,6 +108,7 @@ __global__ void __launch_bounds__(128) k_tcGemm(int M, int N, int K, const __nv_
 // ---------------------------------------------------------------- network --
 constexpr int kC = 32;          // hidden channels (and padded logits)
 constexpr int kKP = 25;         // predicted kernel taps (5 x 5)
+constexpr int kRealInputs = 11; // feature channels that carry data (of 16)
 constexpr int kLayers = 6;
 __host__ __device__ constexpr int cinOf(int l) { return l == 0 ? 16 : 32; }  // 16, 32, 32, 32, 32, 32
 constexpr int kChunk = 512;     // pixels per backward-weight CTA
@@ -174,10 +175,16 @@ __device__ __forceinline__ float loadf<float>(const float* p, size_t i) { return
 template <>
 __device__ __forceinline__ float loadf<__half>(const __half* p, size_t i) { return __half2float(p[i]); }
 
-// Features: X0[p] = (log1p(max(rgb, 0)), albedo, normal guide, depth guide, 0 x 6), BF16.
+// Features: X0[p] = (log1p(max(rgb, 0)), albedo, normal guide, depth guide,
+// log2(1 + spp) / 12, 0 x 5), BF16.  spp: the pixel's sample count from `cnt`
+// (the renderer's per-pixel counts, adaptive sampling included) or, without
+// it, the image's uniform `spp`.
+constexpr float kSppFeatureScale = 1.0f / 12.0f;
+
 template <typename T>
 __global__ void k_features(int P, const float4* __restrict__ noisy, const T* __restrict__ normal,
-                           const T* __restrict__ albedo, const T* __restrict__ depth, __nv_bfloat16* __restrict__ X0) {
+                           const T* __restrict__ albedo, const T* __restrict__ depth, const int* __restrict__ cnt,
+                           float spp, __nv_bfloat16* __restrict__ X0) {
   const int p = blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= P) return;
   const float4 c = noisy[p];
@@ -190,7 +197,8 @@ __global__ void k_features(int P, const float4* __restrict__ noisy, const T* __r
     f[6 + k] = loadf(normal, (size_t)p * 3 + k);
   }
   f[9] = loadf(depth, (size_t)p);
-  for (int k = 10; k < 16; ++k) f[k] = 0.0f;
+  f[10] = log2f(1.0f + fmaxf(cnt ? (float)cnt[p] : spp, 0.0f)) * kSppFeatureScale;
+  for (int k = 11; k < 16; ++k) f[k] = 0.0f;
   __align__(16) __nv_bfloat16 o[16];
   for (int k = 0; k < 16; ++k) o[k] = __float2bfloat16_rn(f[k]);
   uint4* dst = reinterpret_cast<uint4*>(X0 + (size_t)p * 16);
@@ -955,18 +963,18 @@ bool initNet(KpcnNet& n, uint32_t seed) {
     if (l > 0) ok = ok && n.wt[l].alloc(layerWeights(l));
   }
   if (!ok) return false;
-  // He-normal weights (fan-in 9 x input channels; 10 real inputs for layer 1),
+  // He-normal weights (fan-in 9 x input channels; 11 real inputs for layer 1),
   // zero biases, the last layer scaled by 0.1 and its 7 padding logits zero.
   std::vector<float> h(kNumParams, 0.0f);
   std::normal_distribution<float> nd(0.0f, 1.0f);
   for (int l = 0; l < kLayers; ++l) {
-    const int cin = cinOf(l), fan = 9 * (l == 0 ? 10 : cin);
+    const int cin = cinOf(l), fan = 9 * (l == 0 ? kRealInputs : cin);
     const float sd = std::sqrt(2.0f / fan) * (l == kLayers - 1 ? 0.1f : 1.0f);
     float* W = h.data() + layerOffset(l);
     for (int co = 0; co < kC; ++co)
       for (int t = 0; t < 9; ++t)
         for (int ci = 0; ci < cin; ++ci) {
-          const bool pad = (l == 0 && ci >= 10) || (l == kLayers - 1 && co >= kKP);
+          const bool pad = (l == 0 && ci >= kRealInputs) || (l == kLayers - 1 && co >= kKP);
           W[(co * 9 + t) * cin + ci] = pad ? 0.0f : nd(n.rng) * sd;
         }
   }
@@ -990,12 +998,13 @@ bool initNet(KpcnNet& n, uint32_t seed) {
 
 // Upload host images (n images of w x h) into the work buffers and build X0.
 bool uploadInputs(KpcnNet& n, size_t P, const float* noisy, const float* normal, const float* albedo, const float* depth,
-                  const float* ref) {
+                  float spp, const float* ref) {
   DevBuf<float> nb, ab, db;
   if (!nb.upload(normal, P * 3, n.st) || !ab.upload(albedo, P * 3, n.st) || !db.upload(depth, P, n.st)) return false;
   if (cudaMemcpyAsync(n.noisy.p, noisy, sizeof(float4) * P, cudaMemcpyHostToDevice, n.st) != cudaSuccess) return false;
   if (ref && cudaMemcpyAsync(n.ref.p, ref, sizeof(float4) * P, cudaMemcpyHostToDevice, n.st) != cudaSuccess) return false;
-  k_features<float><<<(unsigned)((P + 255) / 256), 256, 0, n.st>>>((int)P, n.noisy.p, nb.p, ab.p, db.p, n.X0.p);
+  k_features<float><<<(unsigned)((P + 255) / 256), 256, 0, n.st>>>((int)P, n.noisy.p, nb.p, ab.p, db.p, nullptr, spp,
+                                                                   n.X0.p);
   return cudaStreamSynchronize(n.st) == cudaSuccess;  // the temporaries die here
 }
 
@@ -1005,7 +1014,7 @@ bool uploadInputs(KpcnNet& n, size_t P, const float* noisy, const float* normal,
 // AOV buffers), result into out (may alias nothing else); intensity blends
 // with the noisy image as denoiseImage does.
 rg_status kpcnDenoiseDevice(KpcnNet& n, int W, int H, const float4* noisy, const __half* normal, const __half* albedo,
-                            const __half* depth, float intensity, float4* out, cudaStream_t st) {
+                            const __half* depth, const int* cnt, float intensity, float4* out, cudaStream_t st) {
   std::lock_guard<std::mutex> lk(n.mu);
   const size_t P = (size_t)W * H;
   if (!ensureWork(n, P)) {
@@ -1016,7 +1025,8 @@ rg_status kpcnDenoiseDevice(KpcnNet& n, int W, int H, const float4* noisy, const
   cudaEventCreateWithFlags(&ev, cudaEventDisableTiming);
   cudaEventRecord(ev, st);
   cudaStreamWaitEvent(n.st, ev, 0);
-  k_features<__half><<<(unsigned)((P + 255) / 256), 256, 0, n.st>>>((int)P, noisy, normal, albedo, depth, n.X0.p);
+  k_features<__half><<<(unsigned)((P + 255) / 256), 256, 0, n.st>>>((int)P, noisy, normal, albedo, depth, cnt, 0.0f,
+                                                                    n.X0.p);
   forward(n, 1, H, W, noisy, n.out.p);
   const rg_status rs = checkErr(n, "learned denoiser");
   if (rs != RG_OK) {
@@ -1089,8 +1099,9 @@ rg_status rg_denoiser_set_params(rg_denoiser* d, const float* in, size_t n) {
 }
 
 rg_status rg_denoiser_add_example(rg_denoiser* d, int32_t w, int32_t h, const float* noisy_rgba, const float* normal,
-                                  const float* albedo, const float* depth, const float* ref_rgba) {
-  if (!d || w <= 0 || h <= 0 || !noisy_rgba || !normal || !albedo || !depth || !ref_rgba) return RG_ERR_INVALID_ARGUMENT;
+                                  const float* albedo, const float* depth, float spp, const float* ref_rgba) {
+  if (!d || w <= 0 || h <= 0 || !noisy_rgba || !normal || !albedo || !depth || !ref_rgba || !(spp >= 0.0f))
+    return RG_ERR_INVALID_ARGUMENT;
   rg::KpcnNet& n = d->net;
   std::lock_guard<std::mutex> lk(n.mu);
   if (n.dsN > 0 && (w != n.dsW || h != n.dsH)) {
@@ -1098,7 +1109,7 @@ rg_status rg_denoiser_add_example(rg_denoiser* d, int32_t w, int32_t h, const fl
     return RG_ERR_INVALID_ARGUMENT;
   }
   const size_t P = (size_t)w * h;
-  if (!rg::ensureWork(n, P) || !rg::uploadInputs(n, P, noisy_rgba, normal, albedo, depth, ref_rgba))
+  if (!rg::ensureWork(n, P) || !rg::uploadInputs(n, P, noisy_rgba, normal, albedo, depth, spp, ref_rgba))
     return RG_ERR_OUT_OF_MEMORY;
   __nv_bfloat16* x = nullptr;
   float4 *nz = nullptr, *rf = nullptr;
@@ -1224,14 +1235,15 @@ rg_status rg_denoiser_timing(rg_denoiser* d, float* apply_ms, float* train_step_
 }
 
 rg_status rg_denoiser_gradients(rg_denoiser* d, int32_t count, int32_t w, int32_t h, const float* noisy_rgba,
-                                const float* normal, const float* albedo, const float* depth, const float* ref_rgba,
-                                float* loss, float* grad) {
-  if (!d || count <= 0 || w <= 0 || h <= 0 || !noisy_rgba || !normal || !albedo || !depth || !ref_rgba || !grad)
+                                const float* normal, const float* albedo, const float* depth, float spp,
+                                const float* ref_rgba, float* loss, float* grad) {
+  if (!d || count <= 0 || w <= 0 || h <= 0 || !noisy_rgba || !normal || !albedo || !depth || !ref_rgba || !grad ||
+      !(spp >= 0.0f))
     return RG_ERR_INVALID_ARGUMENT;
   rg::KpcnNet& n = d->net;
   std::lock_guard<std::mutex> lk(n.mu);
   const size_t P = (size_t)count * w * h;
-  if (!rg::ensureWork(n, P) || !rg::uploadInputs(n, P, noisy_rgba, normal, albedo, depth, ref_rgba))
+  if (!rg::ensureWork(n, P) || !rg::uploadInputs(n, P, noisy_rgba, normal, albedo, depth, spp, ref_rgba))
     return RG_ERR_OUT_OF_MEMORY;
   cudaMemsetAsync(n.loss.p, 0, sizeof(float), n.st);
   rg::forward(n, count, h, w);
@@ -1246,12 +1258,13 @@ rg_status rg_denoiser_gradients(rg_denoiser* d, int32_t count, int32_t w, int32_
 }
 
 rg_status rg_denoiser_apply(rg_denoiser* d, int32_t w, int32_t h, const float* noisy_rgba, const float* normal,
-                            const float* albedo, const float* depth, float* out_rgba) {
-  if (!d || w <= 0 || h <= 0 || !noisy_rgba || !normal || !albedo || !depth || !out_rgba) return RG_ERR_INVALID_ARGUMENT;
+                            const float* albedo, const float* depth, float spp, float* out_rgba) {
+  if (!d || w <= 0 || h <= 0 || !noisy_rgba || !normal || !albedo || !depth || !out_rgba || !(spp >= 0.0f))
+    return RG_ERR_INVALID_ARGUMENT;
   rg::KpcnNet& n = d->net;
   std::lock_guard<std::mutex> lk(n.mu);
   const size_t P = (size_t)w * h;
-  if (!rg::ensureWork(n, P) || !rg::uploadInputs(n, P, noisy_rgba, normal, albedo, depth, nullptr))
+  if (!rg::ensureWork(n, P) || !rg::uploadInputs(n, P, noisy_rgba, normal, albedo, depth, spp, nullptr))
     return RG_ERR_OUT_OF_MEMORY;
   cudaEvent_t e0, e1;
   cudaEventCreate(&e0);

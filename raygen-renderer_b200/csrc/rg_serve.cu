@@ -317,7 +317,7 @@ void finishJob(rg_server* s, ServerJob* j, cudaStream_t st) {
   rg_denoiser* learned = j->desc.denoise == 2 ? s->denoiser.load() : nullptr;
   if (learned) {  // learned denoiser on the job's guides
     dres = kpcnDenoiseDevice(*kpcnOf(learned), j->desc.width, j->desc.height, j->hdr.p, j->aovN.p, j->aovA.p, j->aovD.p,
-                             s->base.denoise_intensity, j->ldr.p, st);
+                             j->cnt.p, s->base.denoise_intensity, j->ldr.p, st);
     if (dres == RG_OK) cudaMemcpyAsync(j->hdr.p, j->ldr.p, sizeof(float4) * N, cudaMemcpyDeviceToDevice, st);
   } else if (j->desc.denoise) {  // A-Trous (also the fallback of mode 2)
     launchDenoise(j->desc.width, j->desc.height, j->hdr.p, j->aovN.p, j->aovD.p, j->aovA.p, j->aovAA.p,
@@ -457,7 +457,7 @@ void serverLoop(rg_server* s) {
     }
     if (!active.empty()) {
       const long long cap = s->cfg.paths_per_wave;
-      const long long quota = std::max<long long>(1, cap / (long long)active.size());
+      const long long quota = s->cfg.wave_fill ? cap : std::max<long long>(1, cap / (long long)active.size());
       long long paths = 0, pixTotal = 0;
       int nseg = 0;
       std::vector<std::pair<ServerJob*, DevSegment>> plan;
@@ -593,7 +593,8 @@ rg_status rg_server_create(const rg_settings* base, const rg_server_config* cfg,
   else rg_settings_default(&s->base);
   if (cfg) s->cfg = *cfg;
   else rg_server_config_default(&s->cfg);
-  if (s->cfg.max_resident_jobs <= 0 || s->cfg.max_resident_jobs > 4096 || s->cfg.paths_per_wave <= 0) {
+  if (s->cfg.max_resident_jobs <= 0 || s->cfg.max_resident_jobs > 4096 || s->cfg.paths_per_wave <= 0 ||
+      s->cfg.wave_fill < 0 || s->cfg.wave_fill > 1) {
     delete s;
     return RG_ERR_INVALID_ARGUMENT;
   }
@@ -862,7 +863,7 @@ rg_status rg_server_autotune(const rg_settings* base, const rg_job_desc* probe, 
     }
     return RG_OK;
   };
-  // coordinate descent: wave size, then shade width, then traversal width
+  // coordinate descent: wave size, then shade width, then traversal width, then wave fill
   for (int ppw : {1 << 20, 1 << 21, 1 << 22, 1 << 23, 1 << 24, 1 << 25, 1 << 26}) {
     rg_server_config c = best;
     c.paths_per_wave = ppw;
@@ -876,6 +877,11 @@ rg_status rg_server_autotune(const rg_settings* base, const rg_job_desc* probe, 
   for (int tb : {2, 4, 6}) {
     rg_server_config c = best;
     c.trace_blocks_per_sm = tb;
+    if ((rs = tryCfg(c)) != RG_OK) return rs;
+  }
+  {
+    rg_server_config c = best;
+    c.wave_fill = best.wave_fill ? 0 : 1;
     if ((rs = tryCfg(c)) != RG_OK) return rs;
   }
   *cfg = best;

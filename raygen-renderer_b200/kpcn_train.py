@@ -15,22 +15,40 @@ import time
 import numpy as np
 
 
-def render_pair(rg, scene, width, height, spp_lo, spp_hi, seed, max_depth=6):
-    """-> (noisy RGBA, normal, albedo, depth, reference RGBA) for one job."""
-    st = rg.RendererSettings(resolutionWidth=width, resolutionHeight=height, samples=spp_lo, maxDepth=max_depth,
-                             seed=seed, enableDenoise=True, denoiseIntensity=0.0)
+def render_set(rg, scene, width, height, spp_list, spp_hi, seed, max_depth=6):
+    """-> [(noisy RGBA, normal, albedo, depth, reference RGBA, spp) for spp in spp_list]:
+    one job rendered at each input spp, all against one spp_hi reference."""
+    st = rg.RendererSettings(resolutionWidth=width, resolutionHeight=height, samples=spp_hi, maxDepth=max_depth,
+                             seed=seed + 7919)
     r = rg.RayRenderer(st)
     r.set_scene(scene)
     r.render()
-    noisy = r.get_hdr_result()  # intensity 0: the denoiser pass leaves the radiance as rendered
-    normal, albedo, depth = r.get_aovs()
-    r.settings.samples = spp_hi
-    r.settings.enableDenoise = False
-    r.settings.seed = seed + 7919
-    r.render()
     ref = r.get_hdr_result()
+    r.settings.enableDenoise = True
+    r.settings.denoiseIntensity = 0.0  # the denoiser pass leaves the radiance as rendered
+    out = []
+    for i, spp in enumerate(spp_list):
+        r.settings.samples = int(spp)
+        r.settings.seed = seed + 104729 * i
+        r.render()
+        noisy = r.get_hdr_result()
+        normal, albedo, depth = r.get_aovs()
+        out.append((noisy, normal, albedo, depth, ref, float(spp)))
     r.close()
-    return noisy, normal, albedo, depth, ref
+    return out
+
+
+def render_pair(rg, scene, width, height, spp_lo, spp_hi, seed, max_depth=6):
+    """-> (noisy RGBA, normal, albedo, depth, reference RGBA, spp_lo) for one job."""
+    return render_set(rg, scene, width, height, [spp_lo], spp_hi, seed, max_depth)[0]
+
+
+def input_spp(k, spp_lo, spp_lo_max, per_scene=1):
+    """The input spp of training scene k: `per_scene` distinct powers of two in
+    [spp_lo, spp_lo_max], drawn uniformly over the exponents from a generator seeded by k."""
+    levels = [spp_lo << i for i in range(64) if spp_lo << i <= max(spp_lo, spp_lo_max)]
+    rng = np.random.default_rng(7000 + k)
+    return sorted(int(x) for x in rng.choice(levels, size=min(per_scene, len(levels)), replace=False))
 
 
 def scene_for(rg, k, generator="narrow"):
@@ -91,10 +109,10 @@ def evaluate(rg, denoiser, count=16, size=128, spp_lo=8, spp_hi=2048, first=1000
     rows = []
     for k in range(first, first + count):
         sc = scene_for(rg, k, generator)
-        noisy, normal, albedo, depth, ref = render_pair(rg, sc, size, size, spp_lo, spp_hi, seed=100 + k)
+        noisy, normal, albedo, depth, ref, spp = render_pair(rg, sc, size, size, spp_lo, spp_hi, seed=100 + k)
         sc.close()
         atrous = rg.denoise_atrous(noisy[..., :3], normal, depth, albedo, np.ones_like(depth))
-        learned = denoiser.apply(noisy, normal, albedo, depth)
+        learned = denoiser.apply(noisy, normal, albedo, depth, spp=spp)
         rows.append((relmse(noisy, ref), relmse(atrous, ref), relmse(learned, ref)))
     r = np.array(rows)
     return {"noisy": float(r[:, 0].mean()), "atrous": float(r[:, 1].mean()), "learned": float(r[:, 2].mean()),
@@ -113,8 +131,11 @@ def main():
     ap.add_argument("--out", default=os.path.join(here, "kpcn_weights.bin"))
     ap.add_argument("--examples", type=int, default=256)
     ap.add_argument("--size", type=int, default=64)
-    ap.add_argument("--spp-lo", type=int, default=8)
+    ap.add_argument("--spp-lo", type=int, default=8, help="input spp (the lowest, with --spp-lo-max)")
+    ap.add_argument("--spp-lo-max", type=int, default=0, help="input spp up to this power-of-two multiple of --spp-lo")
+    ap.add_argument("--per-scene", type=int, default=1, help="input spp levels rendered per scene (one reference)")
     ap.add_argument("--spp-hi", type=int, default=512)
+    ap.add_argument("--eval-spp", default="8", help="comma-separated input spp of the held-out evaluation")
     ap.add_argument("--steps", type=int, default=3000)
     ap.add_argument("--batch", type=int, default=16)
     ap.add_argument("--lr", type=float, default=1e-3)
@@ -126,20 +147,27 @@ def main():
     t0 = time.time()
     params = np.fromfile(a.init, np.float32) if a.init else None
     d = rg.Denoiser(seed=0, params=params)
-    for k in range(a.examples):  # rendered pairs go to the device one at a time
+    hist = {}
+    for k in range(a.examples):  # rendered pairs go to the device one scene at a time
         sc = scene_for(rg, k, a.generator)
-        d.add_example(*render_pair(rg, sc, a.size, a.size, a.spp_lo, a.spp_hi, seed=100 + k))
+        spps = input_spp(k, a.spp_lo, a.spp_lo_max, a.per_scene)
+        for ex in render_set(rg, sc, a.size, a.size, spps, a.spp_hi, seed=100 + k):
+            d.add_example(*ex)
+        for spp in spps:
+            hist[spp] = hist.get(spp, 0) + 1
         sc.close()
         if (k + 1) % 128 == 0:
-            print(f"{k + 1} examples ({time.time() - t0:.1f} s)", flush=True)
-    print(f"{a.examples} examples of {a.size}x{a.size} at {a.spp_lo}/{a.spp_hi} spp in {time.time() - t0:.1f} s",
-          flush=True)
+            print(f"{k + 1} scenes ({time.time() - t0:.1f} s)", flush=True)
+    print(f"{a.examples} scenes of {a.size}x{a.size}, input spp {dict(sorted(hist.items()))}, reference {a.spp_hi} spp, "
+          f"in {time.time() - t0:.1f} s", flush=True)
     d, losses = train(rg, [], a.steps, a.batch, a.lr, log=lambda m: print(m, flush=True), denoiser=d)
     d.save(a.out)
     print(f"saved {a.out}; final loss {losses[-100:].mean():.5f}", flush=True)
     if a.eval > 0:
-        for gen in ("narrow", "config4"):
-            print(f"held-out relMSE ({gen} scenes):", evaluate(rg, d, a.eval, generator=gen), flush=True)
+        for spp in (int(x) for x in a.eval_spp.split(",")):
+            for gen in ("narrow", "config4"):
+                print(f"held-out relMSE ({gen} scenes, {spp} spp):", evaluate(rg, d, a.eval, spp_lo=spp, generator=gen),
+                      flush=True)
 
 
 if __name__ == "__main__":

@@ -40,7 +40,7 @@ def perturbed(d, seed, scale=0.05):
     layers = ko.unpack(p)  # keep the padding entries at zero
     for l, (W, b) in enumerate(layers):
         if l == 0:
-            W[:, :, 10:] = 0.0
+            W[:, :, 11:] = 0.0
         if l == 5:
             W[ko.KP:] = 0.0
             b[ko.KP:] = 0.0
@@ -52,8 +52,8 @@ def test_kpcn_forward_matches_oracle(rg):
     p = perturbed(d, 1)
     d.params = p
     noisy, normal, albedo, depth, ref = synth(1, 37, 45, 1)  # 1665 pixels: a partial last tile
-    got = d.apply(noisy[0], normal[0], albedo[0], depth[0])
-    f = ko.forward(p, ko.features(noisy, normal, albedo, depth), noisy)
+    got = d.apply(noisy[0], normal[0], albedo[0], depth[0], spp=37)
+    f = ko.forward(p, ko.features(noisy, normal, albedo, depth, spp=37), noisy)
     np.testing.assert_allclose(got[..., :3], f["out"][0], rtol=2e-3, atol=2e-3)
     assert np.all(got[..., 3] == 1.0)
     d.close()
@@ -107,8 +107,8 @@ def test_kpcn_gradients_match_oracle(rg):
     p = perturbed(d, 2)
     d.params = p
     noisy, normal, albedo, depth, ref = synth(2, 23, 29, 2)
-    loss, g = d.gradients(noisy, normal, albedo, depth, ref)
-    lo, go = ko.backward(p, ko.features(noisy, normal, albedo, depth), noisy, ref)
+    loss, g = d.gradients(noisy, normal, albedo, depth, ref, spp=512)
+    lo, go = ko.backward(p, ko.features(noisy, normal, albedo, depth, spp=512), noisy, ref)
     assert loss == pytest.approx(lo, rel=1e-3)
     offs = np.cumsum([0] + [w + b for w, b in ko.layer_sizes()])
     for l, (wl, bl) in enumerate(ko.layer_sizes()):
@@ -178,7 +178,7 @@ def test_renderer_and_server_use_the_learned_denoiser(rg):
     r.render()
     noisy = r.get_hdr_result()
     normal, albedo, depth = r.get_aovs()
-    expected = d.apply(noisy, normal, albedo, depth)
+    expected = d.apply(noisy, normal, albedo, depth, spp=8)  # the renderer passes its per-pixel counts (8)
     r.settings.denoiseIntensity = 1.0
     r.set_denoiser(d)
     r.render()

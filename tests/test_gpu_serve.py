@@ -54,6 +54,23 @@ def test_result_is_independent_of_the_mix(rg):
     mix.close()
 
 
+def test_wave_fill_gives_the_same_images(rg):
+    """Filling each wave from as few jobs as possible changes which jobs share a
+    wave, not the images."""
+    scenes = _scenes(rg, 5, seed0=300)
+    out = {}
+    for fill in (0, 1):
+        srv = rg.RenderServer(max_resident_jobs=8, paths_per_wave=1 << 15, wave_fill=fill)
+        ids = [srv.submit(sc, 72 + 8 * k, 40 + 8 * k, 6 + 3 * k, max_depth=5, seed=90 + k) for k, sc in enumerate(scenes)]
+        for jid in ids:
+            srv.wait(jid)
+        out[fill] = [srv.result(jid) for jid in ids]
+        assert srv.stats()["waves"] > len(scenes)
+        srv.close()
+    for a, b in zip(out[0], out[1]):
+        np.testing.assert_allclose(a, b, rtol=1e-4, atol=1e-6)
+
+
 def test_admission_respects_the_budget(rg):
     """Each job reserves its admission estimate (about 66-70 MB here, most of it
     for the BVH build) until it is resident, then holds its measured footprint

@@ -20,7 +20,7 @@ def test_param_count_and_layout():
     assert ko.num_params() == 32 * 9 * 16 + 32 + 5 * (32 * 9 * 32 + 32)
     p = ko.init_params(0)
     layers = ko.unpack(p.astype(np.float64))
-    assert np.all(layers[0][0][:, :, 10:] == 0) and np.all(layers[5][0][ko.KP:] == 0)
+    assert np.all(layers[0][0][:, :, 11:] == 0) and np.all(layers[5][0][ko.KP:] == 0)
 
 
 def test_backward_matches_finite_differences():
@@ -36,7 +36,7 @@ def test_backward_matches_finite_differences():
         wlen = ko.layer_sizes()[l][0]
         idx = list(rng.integers(offs[l], offs[l] + wlen, 4)) + [offs[l] + wlen + 3]  # weights + one bias
         for i in idx:
-            if l == 0 and (i - offs[0]) < wlen and (i - offs[0]) % 16 >= 10:
+            if l == 0 and (i - offs[0]) < wlen and (i - offs[0]) % 16 >= 11:
                 continue  # padding input channels carry no signal
             if l == 5 and (i - offs[5]) < wlen and (i - offs[5]) // (9 * 32) >= ko.KP:
                 continue  # padding logits
