@@ -829,7 +829,8 @@ def main():
     r.set_scene(e2e_scene)
     r.render()
     r.get_hdr_result(out=hdr)
-    e2e_times, e2e_phases = [], {"set_scene": [], "bvh_build_device": [], "render": [], "readback": []}
+    e2e_times, e2e_phases = [], {"set_scene": [], "bvh_build_device": [], "render": [], "render_device": [],
+                                 "readback": []}
     for _ in range(e2e_steps):
         t0 = time.time()
         r.set_scene(e2e_scene)
@@ -842,6 +843,7 @@ def main():
         e2e_phases["set_scene"].append(1e3 * (t1 - t0))
         e2e_phases["bvh_build_device"].append(r.stats()["build_ms"])
         e2e_phases["render"].append(1e3 * (t2 - t1))
+        e2e_phases["render_device"].append(r.stats()["trace_ms"] + r.stats()["post_ms"])
         e2e_phases["readback"].append(1e3 * (t3 - t2))
     e2e_s = sum(e2e_times)
     r.set_scene(scene)

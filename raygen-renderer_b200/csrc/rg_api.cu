@@ -1003,11 +1003,7 @@ rg_status rg_set_scene(rg_handle* h, const rg_scene_desc* d) {
   h->lastStats.build_ms = ms;
   h->lastStats.bvh_nodes = h->scene->bvhWidth == 8 ? h->scene->numNodes8 : h->scene->numNodes;
   h->hasScene = true;
-  if (h->graph) {
-    cudaGraphExecDestroy(h->graph);
-    h->graph = nullptr;
-    h->graphKey.clear();
-  }
+  h->graphKey.clear();  // the wave graph carries the scene in its kernel parameters: recapture, then update
   return RG_OK;
 }
 
@@ -1136,16 +1132,24 @@ static rg_status runPass(rg_handle* h, const DevRender& R, int numPixels, const 
                           ":" + std::to_string((uintptr_t)pixelList) + ":" + std::to_string((uintptr_t)h->jobsDev.p) + ":" +
                           std::to_string((uintptr_t)h->shO3.p) + ":" + std::string((const char*)&R, sizeof(R));
   if (!profile && (h->graph == nullptr || h->graphKey != key)) {
-    if (h->graph) {
-      cudaGraphExecDestroy(h->graph);
-      h->graph = nullptr;
-    }
     cudaGraph_t g;
     RG_CUDA_CHECK(cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
     k_selectWave<<<1, 1, 0, h->stream>>>(h->waves.p, h->curWave.p, slot);
     enqueueWave(h, R, Q, h->jobsDev.p, slot, false, nullptr);
     RG_CUDA_CHECK(cudaStreamEndCapture(h->stream, &g));
-    const cudaError_t ie = cudaGraphInstantiate(&h->graph, g, 0);
+    // same kernel sequence with new parameters (a new scene, new settings):
+    // update the instantiated graph in place; otherwise instantiate anew
+    bool updated = false;
+    if (h->graph) {
+      cudaGraphExecUpdateResultInfo info;
+      updated = cudaGraphExecUpdate(h->graph, g, &info) == cudaSuccess;
+      if (!updated) {
+        cudaGetLastError();
+        cudaGraphExecDestroy(h->graph);
+        h->graph = nullptr;
+      }
+    }
+    const cudaError_t ie = updated ? cudaSuccess : cudaGraphInstantiate(&h->graph, g, 0);
     cudaGraphDestroy(g);
     if (ie != cudaSuccess) {
       setLastError(std::string("cudaGraphInstantiate: ") + cudaGetErrorString(ie));

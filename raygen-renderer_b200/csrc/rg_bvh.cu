@@ -557,7 +557,8 @@ __global__ void k_collapse(int numTasks, const int2* __restrict__ tasks, const B
     inv[k] = ldexpf(1.0f, -ex);
     org[k] = __fsub_rd(lo[k], ldexpf(1.0f, ex));
   }
-  uint32_t qlo[3][2] = {{0, 0}, {0, 0}, {0, 0}}, qhi[3][2] = {{0, 0}, {0, 0}, {0, 0}};
+  // empty slots keep an inverted box (lo 255, hi 0) that no ray enters
+  uint32_t qlo[3][2] = {{~0u, ~0u}, {~0u, ~0u}, {~0u, ~0u}}, qhi[3][2] = {{0, 0}, {0, 0}, {0, 0}};
   uint32_t meta[2] = {0, 0};
   uint32_t imask = 0;
   int ni = 0, ntri = 0;
@@ -571,7 +572,7 @@ __global__ void k_collapse(int numTasks, const int2* __restrict__ tasks, const B
       int b = (int)ceilf(__fsub_ru(inflateHi(cn.bmax[k]), org[k]) * inv[k]) + 1;
       a = max(0, min(255, a));
       b = max(0, min(255, b));
-      qlo[k][sl >> 2] |= (uint32_t)a << (8 * (sl & 3));
+      qlo[k][sl >> 2] = (qlo[k][sl >> 2] & ~(0xffu << (8 * (sl & 3)))) | ((uint32_t)a << (8 * (sl & 3)));
       qhi[k][sl >> 2] |= (uint32_t)b << (8 * (sl & 3));
     }
     if (cn.left >= 0) {

@@ -234,6 +234,18 @@ __device__ __forceinline__ float biasedByte(uint32_t w, uint32_t k) {
   return __uint_as_float(__byte_perm(w, 0x4B000000u, 0x7540u | k));
 }
 
+// Three-input minimum / maximum: one instruction each on sm_100 (PTX ISA 8.8).
+__device__ __forceinline__ float fmax3f(float a, float b, float c) {
+  float d;
+  asm("max.f32 %0, %1, %2, %3;" : "=f"(d) : "f"(a), "f"(b), "f"(c));
+  return d;
+}
+__device__ __forceinline__ float fmin3f(float a, float b, float c) {
+  float d;
+  asm("min.f32 %0, %1, %2, %3;" : "=f"(d) : "f"(a), "f"(b), "f"(c));
+  return d;
+}
+
 __device__ __forceinline__ Node8Hit intersectNode8(const float4* np, V3 o, V3 inv, float tcap, uint32_t oct) {
   const float4 n0 = ldNode4(np), n1 = ldNode4(np + 1), n2 = ldNode4(np + 2), n3 = ldNode4(np + 3),
                n4 = ldNode4(np + 4);
@@ -259,21 +271,31 @@ __device__ __forceinline__ Node8Hit intersectNode8(const float4* np, V3 o, V3 in
   const uint32_t fxw[2] = {__float_as_uint(fx ? n2.x : n3.z), __float_as_uint(fx ? n2.y : n3.w)};
   const uint32_t fyw[2] = {__float_as_uint(fy ? n2.z : n4.x), __float_as_uint(fy ? n2.w : n4.y)};
   const uint32_t fzw[2] = {__float_as_uint(fz ? n3.x : n4.z), __float_as_uint(fz ? n3.y : n4.w)};
+  uint32_t hits = 0;
 #pragma unroll
   for (int i = 0; i < 8; i++) {
     const int w = i >> 2;
     const uint32_t k = (uint32_t)(i & 3);
-    const uint32_t m = (meta[w] >> (8 * k)) & 0xffu;
     const float tnx = fmaf(biasedByte(nx[w], k), adj.x, org.x), tfx = fmaf(biasedByte(fxw[w], k), adj.x, org.x);
     const float tny = fmaf(biasedByte(ny[w], k), adj.y, org.y), tfy = fmaf(biasedByte(fyw[w], k), adj.y, org.y);
     const float tnz = fmaf(biasedByte(nz[w], k), adj.z, org.z), tfz = fmaf(biasedByte(fzw[w], k), adj.z, org.z);
-    const float tmin = fmaxf(fmaxf(tnx, tny), tnz);
-    const float tmax = fminf(fminf(tfx, tfy), tfz);
-    const bool hit = m != 0u && !(tmax < 0.0f || tmin > tmax || tmin > tcap);
-    if (hit) {
-      if ((r.imask >> i) & 1u) r.inner |= 1u << (i ^ oct);
-      else r.tris |= ((1u << (m >> 5)) - 1u) << (m & 31u);
-    }
+    // slab test: the interval [max(tnear, 0), min(tfar, tcap)] is not empty
+    // (hits in slot order; an empty slot is an inverted box and never hits)
+    const float tmin = fmax3f(tnx, tny, tnz);
+    const float tmax = fmin3f(tfx, tfy, tfz);
+    if (fmaxf(tmin, 0.0f) <= fminf(tmax, tcap)) hits |= 1u << i;
+  }
+  // inner children: bit (slot ^ octant)
+  uint32_t x = hits & r.imask;
+  if (oct & 1u) x = ((x & 0x55u) << 1) | ((x >> 1) & 0x55u);
+  if (oct & 2u) x = ((x & 0x33u) << 2) | ((x >> 2) & 0x33u);
+  if (oct & 4u) x = ((x & 0x0fu) << 4) | ((x >> 4) & 0x0fu);
+  r.inner = x;
+  // leaf children: their triangle ranges
+  const unsigned long long meta64 = ((unsigned long long)meta[1] << 32) | meta[0];
+  for (uint32_t leaf = hits & ~r.imask; leaf; leaf &= leaf - 1u) {
+    const uint32_t m = (uint32_t)(meta64 >> (8 * (__ffs(leaf) - 1))) & 0xffu;
+    r.tris |= ((1u << (m >> 5)) - 1u) << (m & 31u);
   }
   return r;
 }
