@@ -858,7 +858,7 @@ def main():
     s = r.stats()
     os.environ.pop("RG_PROFILE_KERNELS", None)
     ext_ms = s["extend_ms"]
-    node_bytes = 80 if st.bvhWidth == 8 else 64
+    node_bytes = 208 if st.bvhWidth == 8 else 64  # 8-wide: header + float planes of 8 child boxes
     alg_bytes = s["closest_rays"] * 48 + s["nodes_visited"] * node_bytes + s["tris_tested"] * 48
     launches_ext = s["waves"] * (DEPTH + 2)
     achieved = alg_bytes / (ext_ms * 1e-3) / 1e9 if ext_ms > 0 else None
@@ -867,8 +867,13 @@ def main():
     traffic = None
     if prof and prof.get("bytes_per_ray"):
         traffic = prof["bytes_per_ray"] * s["closest_rays"] / max(1, launches_ext)
+    # the same launches counted with 80-B compressed (CWBVH-size) nodes, the unit an 8-bit
+    # quantised node format would read: comparable across node formats
+    alg80 = s["closest_rays"] * 48 + s["nodes_visited"] * 80 + s["tris_tested"] * 48
+    frac80 = alg80 / (ext_ms * 1e-3) / 1e9 / peak if ext_ms > 0 else None
     roofline = {"bound": "hbm", "achieved": round(achieved, 1) if achieved else None, "peak": peak,
                 "unit": "GB/s", "frac": round(achieved / peak, 4) if achieved else None,
+                "node_bytes": node_bytes, "frac_at_80B_nodes": round(frac80, 4) if frac80 else None,
                 "traffic": round(traffic) if traffic else None,
                 "kernel": "k_extend (closest hit)", "peak_source": f"{peak_kind} hbm_gbs",
                 "launches": launches_ext, "avg_launch_ms": round(ext_ms / max(1, launches_ext), 4),

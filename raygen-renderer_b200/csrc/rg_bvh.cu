@@ -461,12 +461,12 @@ __global__ void k_gather(int n, const int* __restrict__ primIdx, const float4* _
 }
 
 
-// ---- 8-wide compressed BVH (collapse of the binary build) ---------------------
-// Node (80 B = 5 float4): (lo.xyz, e.x | e.y << 8 | e.z << 16 | imask << 24)
-// (childBase, triBase, meta[0..3], meta[4..7]) (qlo.x[8], qlo.y[8]) (qlo.z[8], qhi.x[8])
-// (qhi.y[8], qhi.z[8]).  Child box = lo + 2^e * q.  imask bit s: slot s is an inner
-// child, stored at childBase + popc(imask below s).  meta[s] = (count << 5) | offset
-// for a leaf of `count` (1..4) triangles at triBase + offset; 0 = empty slot.
+// ---- 8-wide BVH (collapse of the binary build) ---------------------------------
+// Node (208 B = kNode8Vec float4): (childBase, triBase, meta[0..3], meta[4..7]), then
+// per axis x, y, z the 8 children's lo planes and their 8 hi planes (2 float4 each).
+// meta[s] = 0x80: slot s is an inner child, stored at childBase + (inner slots
+// below s); ((count - 1) << 5) | offset: a leaf of `count` (1..4) triangles at
+// triBase + offset; an empty slot has an inverted box and is never entered.
 // Slots are assigned per octant: a child whose centre lies on the negative side
 // of the node centre along axis k prefers slots with bit k set, so visiting hit
 // slots in descending order of (slot XOR ray octant) is roughly front to back.
@@ -536,51 +536,29 @@ __global__ void k_collapse(int numTasks, const int2* __restrict__ tasks, const B
   int childAt[8];
   for (int sl = 0; sl < 8; sl++) childAt[sl] = -1;
   for (int j = 0; j < nc; j++) childAt[slotOf[j]] = ch[j];
-  // quantisation frame
-  // The quantum 2^e covers the extent in at most 250 steps and is at least four
-  // ulps of the node's coordinates; the origin sits one quantum below the
-  // box so every child keeps a full quantum of margin after rounding.
-  int e[3];
-  float inv[3], org[3];
-  for (int k = 0; k < 3; k++) {
-    const float ext = __fsub_ru(hi[k], lo[k]);
-    int em;
-    frexpf(fmaxf(fmaxf(fabsf(lo[k]), fabsf(hi[k])), 1e-30f), &em);
-    int ex = em - 22;
-    if (ext > 0.0f) {
-      int e2;
-      frexpf(ext / 250.0f, &e2);
-      ex = max(ex, e2);
+  // float planes of the child boxes (each widened by the inflate margin); an empty
+  // slot keeps an inverted box (+inf / -inf) that no ray enters
+  float pl[3][2][8];
+  for (int k = 0; k < 3; k++)
+    for (int sl = 0; sl < 8; sl++) {
+      pl[k][0][sl] = INFINITY;
+      pl[k][1][sl] = -INFINITY;
     }
-    ex = max(-100, min(100, ex));
-    e[k] = ex;
-    inv[k] = ldexpf(1.0f, -ex);
-    org[k] = __fsub_rd(lo[k], ldexpf(1.0f, ex));
-  }
-  // empty slots keep an inverted box (lo 255, hi 0) that no ray enters
-  uint32_t qlo[3][2] = {{~0u, ~0u}, {~0u, ~0u}, {~0u, ~0u}}, qhi[3][2] = {{0, 0}, {0, 0}, {0, 0}};
   uint32_t meta[2] = {0, 0};
-  uint32_t imask = 0;
   int ni = 0, ntri = 0;
   for (int sl = 0; sl < 8; sl++) {
     const int c = childAt[sl];
     if (c < 0) continue;
     const BNode& cn = nodes[c];
     for (int k = 0; k < 3; k++) {
-      // one quantum of margin on each side (covers the traversal's folded 2^23 offset)
-      int a = (int)floorf(__fsub_rd(inflateLo(cn.bmin[k]), org[k]) * inv[k]) - 1;
-      int b = (int)ceilf(__fsub_ru(inflateHi(cn.bmax[k]), org[k]) * inv[k]) + 1;
-      a = max(0, min(255, a));
-      b = max(0, min(255, b));
-      qlo[k][sl >> 2] = (qlo[k][sl >> 2] & ~(0xffu << (8 * (sl & 3)))) | ((uint32_t)a << (8 * (sl & 3)));
-      qhi[k][sl >> 2] |= (uint32_t)b << (8 * (sl & 3));
+      pl[k][0][sl] = inflateLo(cn.bmin[k]);
+      pl[k][1][sl] = inflateHi(cn.bmax[k]);
     }
     if (cn.left >= 0) {
-      imask |= 1u << sl;
-      meta[sl >> 2] |= 0x20u << (8 * (sl & 3));
+      meta[sl >> 2] |= 0x80u << (8 * (sl & 3));
       ni++;
     } else {
-      meta[sl >> 2] |= (uint32_t)((cn.count << 5) | ntri) << (8 * (sl & 3));
+      meta[sl >> 2] |= (uint32_t)(((cn.count - 1) << 5) | ntri) << (8 * (sl & 3));
       ntri += cn.count;
     }
   }
@@ -590,13 +568,14 @@ __global__ void k_collapse(int numTasks, const int2* __restrict__ tasks, const B
     atomicCAS(&counters[3], 0, kErrPartition);
     return;
   }
-  float4* o = nodes8 + (size_t)task.y * 5;
-  const uint32_t eb = ((uint32_t)(e[0] & 0xff)) | ((uint32_t)(e[1] & 0xff) << 8) | ((uint32_t)(e[2] & 0xff) << 16) | (imask << 24);
-  o[0] = make_float4(org[0], org[1], org[2], __uint_as_float(eb));
-  o[1] = make_float4(__int_as_float(childBase), __int_as_float(triBase), __uint_as_float(meta[0]), __uint_as_float(meta[1]));
-  o[2] = make_float4(__uint_as_float(qlo[0][0]), __uint_as_float(qlo[0][1]), __uint_as_float(qlo[1][0]), __uint_as_float(qlo[1][1]));
-  o[3] = make_float4(__uint_as_float(qlo[2][0]), __uint_as_float(qlo[2][1]), __uint_as_float(qhi[0][0]), __uint_as_float(qhi[0][1]));
-  o[4] = make_float4(__uint_as_float(qhi[1][0]), __uint_as_float(qhi[1][1]), __uint_as_float(qhi[2][0]), __uint_as_float(qhi[2][1]));
+  float4* o = nodes8 + (size_t)task.y * kNode8Vec;
+  o[0] = make_float4(__int_as_float(childBase), __int_as_float(triBase), __uint_as_float(meta[0]), __uint_as_float(meta[1]));
+  for (int k = 0; k < 3; k++)
+    for (int h = 0; h < 2; h++) {
+      const float* q = pl[k][h];
+      o[1 + 4 * k + 2 * h] = make_float4(q[0], q[1], q[2], q[3]);
+      o[2 + 4 * k + 2 * h] = make_float4(q[4], q[5], q[6], q[7]);
+    }
   int k = 0, off = 0;
   for (int sl = 0; sl < 8; sl++) {
     const int c = childAt[sl];
@@ -719,7 +698,7 @@ rg_status buildDeviceBvh(DeviceScene& ds, int nbins, bool wide, cudaStream_t st,
     const int maxNodes8 = numNodes + 1;
     DevBuf<int2> ta, tb;
     DevBuf<int> order, c8;
-    if (!ds.nodes8.alloc((size_t)maxNodes8 * 5) || !ta.alloc(maxNodes8) || !tb.alloc(maxNodes8) || !order.alloc(n) ||
+    if (!ds.nodes8.alloc((size_t)maxNodes8 * kNode8Vec) || !ta.alloc(maxNodes8) || !tb.alloc(maxNodes8) || !order.alloc(n) ||
         !c8.alloc(4)) {
       err = "out of device memory (wide BVH)";
       return RG_ERR_OUT_OF_MEMORY;

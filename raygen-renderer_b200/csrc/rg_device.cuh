@@ -15,6 +15,14 @@ constexpr float kRRMin = 0.05f, kRRMax = 0.95f;  // rayrenderer.cpp:44-45
 constexpr int kMaxLeaf = 8;                   // triangles per leaf in the device BVH
 constexpr int kMaxMediumCount = 64;           // cap on a medium's octaves, strata and march steps
 constexpr int kStackSize = 64;
+// 8-wide BVH node: a header float4 (child base, triangle base, 8 meta bytes) and the
+// float planes of the 8 child boxes, per axis 8 lo then 8 hi values (12 float4);
+// the node stride in float4 is build-time overridable (-D) for sweeps (>= 13)
+#ifndef RG_NODE8_VEC
+#define RG_NODE8_VEC 13
+#endif
+constexpr int kNode8Vec = RG_NODE8_VEC;
+static_assert(kNode8Vec >= 13, "an 8-wide node holds 13 float4");
 
 // occluder classes (bit per shadow-ray predicate)
 constexpr uint32_t kOccArea = 1u;   // transparency < 0.01 && emission <= 0   (rayrenderer.cpp:1956-1959)

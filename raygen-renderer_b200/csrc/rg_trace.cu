@@ -890,7 +890,7 @@ __device__ __forceinline__ void traverseWave8(const DevScene& S0, const DevJob* 
             atomicCAS(errP, 0, kErrTraversalSteps);
             result = ANY ? 2 : 1;
           } else {
-            const Node8Hit g = intersectNode8(nodesP + (size_t)node * 5, o, inv, tmax, oct);
+            const Node8Hit g = intersectNode8(nodesP + (size_t)node * kNode8Vec, o, inv, tmax, oct);
             nodes++;
             gInner = g.inner;
             gImask = g.imask;
@@ -922,10 +922,13 @@ __device__ __forceinline__ void traverseWave8(const DevScene& S0, const DevJob* 
   }
 }
 
-// 8 resident blocks per SM (64 registers): the traversals are latency-bound, and
-// 32 warps per SM beat 28 (72 registers); more blocks spill and lose.
+// Resident blocks per SM of the traversal kernels (8: 64 registers), build-time
+// overridable (-D) for sweeps.
+#ifndef RG_TRACE_MIN_BLOCKS
+#define RG_TRACE_MIN_BLOCKS 8
+#endif
 template <bool MULTI>
-__global__ void __launch_bounds__(128, 8) k_extend8(DevScene S0, const DevJob* __restrict__ jobs, DevQueues Q, int iter) {
+__global__ void __launch_bounds__(128, RG_TRACE_MIN_BLOCKS) k_extend8(DevScene S0, const DevJob* __restrict__ jobs, DevQueues Q, int iter) {
   const int count = Q.counters[iter * kCountersPerIter + C_RAYS];
   uint32_t nodes = 0, tris = 0, rays = 0;
   traverseWave8<false, MULTI>(S0, jobs, count, &Q.counters[iter * kCountersPerIter + C_FETCH_EXT], Q.rayO[iter & 1],
@@ -936,7 +939,7 @@ __global__ void __launch_bounds__(128, 8) k_extend8(DevScene S0, const DevJob* _
 }
 
 template <bool MULTI>
-__global__ void __launch_bounds__(128, 8) k_connect8(DevScene S0, const DevJob* __restrict__ jobs, DevQueues Q, int iter,
+__global__ void __launch_bounds__(128, RG_TRACE_MIN_BLOCKS) k_connect8(DevScene S0, const DevJob* __restrict__ jobs, DevQueues Q, int iter,
                                                   int which) {
   const int count = Q.counters[iter * kCountersPerIter + shadowCountSlot(which)];
   uint32_t nodes = 0, tris = 0, rays = 0;

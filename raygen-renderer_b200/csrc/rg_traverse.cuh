@@ -209,15 +209,11 @@ __device__ __forceinline__ bool traceAny2(const DevScene& S, V3 o, V3 d, float m
   return false;
 }
 
-// ---- 8-wide compressed BVH ----------------------------------------------------
+// ---- 8-wide BVH ---------------------------------------------------------------
 // Node layout: see k_collapse (rg_bvh.cu).  Traversal keeps a "node group"
 // (child base, hit bits, inner-slot mask) and a "triangle group" (triangle base,
 // 32-bit mask); hit inner children are visited in descending order of
 // (slot XOR ray octant), an approximate front-to-back order.
-
-__device__ __forceinline__ float byteAsFloat(uint32_t w, int sh) {
-  return __uint_as_float(0x4B000000u | ((w >> sh) & 0xffu)) - 8388608.0f;
-}
 
 struct Node8Hit {
   uint32_t inner;    // hit inner children, bit (slot ^ octant)
@@ -225,14 +221,6 @@ struct Node8Hit {
   uint32_t imask;
   int childBase, triBase;
 };
-
-// Quantised plane -> float: one PRMT puts byte k of w under the exponent of
-// 2^23, giving 2^23 + q exactly; the 2^23 offset is folded into the per-node
-// origin term.  The folded offset costs at most half a quantum of precision,
-// covered by the one-quantum margin the build adds on every side.
-__device__ __forceinline__ float biasedByte(uint32_t w, uint32_t k) {
-  return __uint_as_float(__byte_perm(w, 0x4B000000u, 0x7540u | k));
-}
 
 // Three-input minimum / maximum: one instruction each on sm_100 (PTX ISA 8.8).
 __device__ __forceinline__ float fmax3f(float a, float b, float c) {
@@ -246,44 +234,40 @@ __device__ __forceinline__ float fmin3f(float a, float b, float c) {
   return d;
 }
 
+// Bit 7 of each byte of w -> 4 bits (byte k -> bit k).
+__device__ __forceinline__ uint32_t byteTopBits(uint32_t w) {
+  return (((w >> 7) & 0x01010101u) * 0x01020408u) >> 24;
+}
+
 __device__ __forceinline__ Node8Hit intersectNode8(const float4* np, V3 o, V3 inv, float tcap, uint32_t oct) {
-  const float4 n0 = ldNode4(np), n1 = ldNode4(np + 1), n2 = ldNode4(np + 2), n3 = ldNode4(np + 3),
-               n4 = ldNode4(np + 4);
-  const uint32_t eb = __float_as_uint(n0.w);
-  const int ex = (int)(int8_t)(eb & 0xffu), ey = (int)(int8_t)((eb >> 8) & 0xffu), ez = (int)(int8_t)((eb >> 16) & 0xffu);
-  const float sx = __int_as_float((ex + 127) << 23), sy = __int_as_float((ey + 127) << 23),
-              sz = __int_as_float((ez + 127) << 23);
-  const V3 adj = v3(sx * inv.x, sy * inv.y, sz * inv.z);
-  const V3 org = v3(fmaf(-8388608.0f, adj.x, (n0.x - o.x) * inv.x), fmaf(-8388608.0f, adj.y, (n0.y - o.y) * inv.y),
-                    fmaf(-8388608.0f, adj.z, (n0.z - o.z) * inv.z));
+  const float4 h = ldNode4(np);
   Node8Hit r;
-  r.imask = eb >> 24;
-  r.childBase = __float_as_int(n1.x);
-  r.triBase = __float_as_int(n1.y);
+  r.childBase = __float_as_int(h.x);
+  r.triBase = __float_as_int(h.y);
+  const uint32_t m0 = __float_as_uint(h.z), m1 = __float_as_uint(h.w);
+  r.imask = byteTopBits(m0) | (byteTopBits(m1) << 4);  // meta 0x80: inner child
   r.inner = 0;
   r.tris = 0;
-  const uint32_t meta[2] = {__float_as_uint(n1.z), __float_as_uint(n1.w)};
-  // near / far planes per axis from the ray direction signs (inv < 0 swaps lo and hi)
-  const bool fx = (oct & 1u) != 0, fy = (oct & 2u) != 0, fz = (oct & 4u) != 0;
-  const uint32_t nx[2] = {__float_as_uint(fx ? n3.z : n2.x), __float_as_uint(fx ? n3.w : n2.y)};
-  const uint32_t ny[2] = {__float_as_uint(fy ? n4.x : n2.z), __float_as_uint(fy ? n4.y : n2.w)};
-  const uint32_t nz[2] = {__float_as_uint(fz ? n4.z : n3.x), __float_as_uint(fz ? n4.w : n3.y)};
-  const uint32_t fxw[2] = {__float_as_uint(fx ? n2.x : n3.z), __float_as_uint(fx ? n2.y : n3.w)};
-  const uint32_t fyw[2] = {__float_as_uint(fy ? n2.z : n4.x), __float_as_uint(fy ? n2.w : n4.y)};
-  const uint32_t fzw[2] = {__float_as_uint(fz ? n3.x : n4.z), __float_as_uint(fz ? n3.y : n4.w)};
+  const V3 oi = v3(o.x * inv.x, o.y * inv.y, o.z * inv.z);
+  // near / far plane arrays per axis from the ray direction signs (inv < 0: the hi planes are near)
+  const int fx = (int)(oct & 1u), fy = (int)((oct >> 1) & 1u), fz = (int)((oct >> 2) & 1u);
+  const float4 *nx = np + 1 + 2 * fx, *fxp = np + 3 - 2 * fx;
+  const float4 *ny = np + 5 + 2 * fy, *fyp = np + 7 - 2 * fy;
+  const float4 *nz = np + 9 + 2 * fz, *fzp = np + 11 - 2 * fz;
   uint32_t hits = 0;
 #pragma unroll
-  for (int i = 0; i < 8; i++) {
-    const int w = i >> 2;
-    const uint32_t k = (uint32_t)(i & 3);
-    const float tnx = fmaf(biasedByte(nx[w], k), adj.x, org.x), tfx = fmaf(biasedByte(fxw[w], k), adj.x, org.x);
-    const float tny = fmaf(biasedByte(ny[w], k), adj.y, org.y), tfy = fmaf(biasedByte(fyw[w], k), adj.y, org.y);
-    const float tnz = fmaf(biasedByte(nz[w], k), adj.z, org.z), tfz = fmaf(biasedByte(fzw[w], k), adj.z, org.z);
-    // slab test: the interval [max(tnear, 0), min(tfar, tcap)] is not empty
-    // (hits in slot order; an empty slot is an inverted box and never hits)
-    const float tmin = fmax3f(tnx, tny, tnz);
-    const float tmax = fmin3f(tfx, tfy, tfz);
-    if (fmaxf(tmin, 0.0f) <= fminf(tmax, tcap)) hits |= 1u << i;
+  for (int half = 0; half < 2; half++) {
+    const float4 a = ldNode4(nx + half), b = ldNode4(fxp + half), c = ldNode4(ny + half), d = ldNode4(fyp + half),
+                 e = ldNode4(nz + half), f = ldNode4(fzp + half);
+    const float pa[4] = {a.x, a.y, a.z, a.w}, pb[4] = {b.x, b.y, b.z, b.w}, pc[4] = {c.x, c.y, c.z, c.w},
+                pd[4] = {d.x, d.y, d.z, d.w}, pe[4] = {e.x, e.y, e.z, e.w}, pf[4] = {f.x, f.y, f.z, f.w};
+#pragma unroll
+    for (int j = 0; j < 4; j++) {
+      // slab test (bvh.cpp:250-265): the interval [max(tnear, 0), min(tfar, tcap)] is not empty
+      const float tmin = fmax3f(fmaf(pa[j], inv.x, -oi.x), fmaf(pc[j], inv.y, -oi.y), fmaf(pe[j], inv.z, -oi.z));
+      const float tmax = fmin3f(fmaf(pb[j], inv.x, -oi.x), fmaf(pd[j], inv.y, -oi.y), fmaf(pf[j], inv.z, -oi.z));
+      if (fmaxf(tmin, 0.0f) <= fminf(tmax, tcap)) hits |= 1u << (4 * half + j);
+    }
   }
   // inner children: bit (slot ^ octant)
   uint32_t x = hits & r.imask;
@@ -292,10 +276,10 @@ __device__ __forceinline__ Node8Hit intersectNode8(const float4* np, V3 o, V3 in
   if (oct & 4u) x = ((x & 0x0fu) << 4) | ((x >> 4) & 0x0fu);
   r.inner = x;
   // leaf children: their triangle ranges
-  const unsigned long long meta64 = ((unsigned long long)meta[1] << 32) | meta[0];
+  const unsigned long long meta64 = ((unsigned long long)m1 << 32) | m0;
   for (uint32_t leaf = hits & ~r.imask; leaf; leaf &= leaf - 1u) {
     const uint32_t m = (uint32_t)(meta64 >> (8 * (__ffs(leaf) - 1))) & 0xffu;
-    r.tris |= ((1u << (m >> 5)) - 1u) << (m & 31u);
+    r.tris |= ((2u << (m >> 5)) - 1u) << (m & 31u);
   }
   return r;
 }
@@ -358,7 +342,7 @@ __device__ __forceinline__ ClosestHit traceClosest8(const DevScene& S, V3 o, V3 
       atomicCAS(S.error, 0, kErrTraversalSteps);
       break;
     }
-    g = intersectNode8(S.nodes8 + (size_t)node * 5, o, inv, h.t, oct);
+    g = intersectNode8(S.nodes8 + (size_t)node * kNode8Vec, o, inv, h.t, oct);
     nodeCount++;
     gInner = g.inner;
     gImask = g.imask;
@@ -417,7 +401,7 @@ __device__ __forceinline__ bool traceAny8(const DevScene& S, V3 o, V3 d, float m
       atomicCAS(S.error, 0, kErrTraversalSteps);
       break;
     }
-    g = intersectNode8(S.nodes8 + (size_t)node * 5, o, inv, maxT, oct);
+    g = intersectNode8(S.nodes8 + (size_t)node * kNode8Vec, o, inv, maxT, oct);
     nodeCount++;
     gInner = g.inner;
     gImask = g.imask;
