@@ -331,7 +331,7 @@ size_t DeviceScene::deviceBytes() const {
   b += pathPts.bytes() + volLights.bytes() + areaLightObj.bytes() + lightMeshList.bytes() + lightObjMeshes.bytes();
   b += lightMeshTris.bytes() + lightTris.bytes() + points.bytes() + textures.bytes() + envMarg.bytes();
   b += envCond.bytes() + cubeMargFace.bytes() + cubeMargY.bytes() + cubeCond.bytes() + nodes.bytes();
-  b += nodes8.bytes() + triVerts.bytes() + triShade.bytes() + triUV.bytes() + triOrig.bytes();
+  b += nodes8.bytes() + triVerts.bytes() + triShade.bytes() + triUV.bytes() + triOrig.bytes() + triMat.bytes();
   for (const auto* t : texels) b += t ? t->bytes() : 0;
   return b;
 }
@@ -977,6 +977,14 @@ rg_status prepareScene(const rg_scene_desc* d, int bins, bool wide, cudaStream_t
   S.cubeMargFace = ds.cubeMargFace.p;
   S.cubeMargY = ds.cubeMargY.p;
   S.cubeCond = ds.cubeCond.p;
+  // per-triangle shading class and material (the shade kernel's sort key)
+  if (!ds.triMat.alloc((size_t)std::max(1, nt))) {
+    setLastError("scene upload failed (device memory)");
+    out.reset();
+    return RG_ERR_OUT_OF_MEMORY;
+  }
+  S.triMat = ds.triMat.p;
+  if (nt > 0) launchTriMaterial(S, nt, ds.triMat.p, st);
   return RG_OK;
 }
 

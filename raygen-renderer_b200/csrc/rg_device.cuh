@@ -117,6 +117,7 @@ struct DevScene {
   const float4* triShade;     // 3 float4: (n1.xyz, n2.x) (n2.yz, n3.xy) (n3.z, gn.xyz)
   const float2* triUV;        // 3 float2 per triangle (NULL when the scene has no textures)
   const int* triOrig;
+  const int* triMat;          // per triangle (leaf order): shading class << 28 | material index
   int numTris;
   const int* meshObj;         // mesh -> object
   const int* meshTriCount;    // mesh -> triangle count (areaLightSampledArea)

@@ -153,7 +153,7 @@ struct DeviceScene {
   int numNodes8 = 0;
   int bvhWidth = 2;
   DevBuf<float2> triUV;
-  DevBuf<int> triOrig;
+  DevBuf<int> triOrig, triMat;
   int numNodes = 0;
   int rootIsLeaf = 0, rootLeafRef = 0;
   int buildLevels = 0;

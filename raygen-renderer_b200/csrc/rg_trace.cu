@@ -951,6 +951,32 @@ __global__ void __launch_bounds__(128, RG_TRACE_MIN_BLOCKS) k_connect8(DevScene 
   warpAddStat(&Q.stats[5], rays);
 }
 
+// Shading class of a material: the branch its surface vertices take in the
+// shade kernel (emitter, diffuse, rough glossy, mirror, refraction,
+// transparency, mixed lobes; 7 = miss), the key of the kernel's sort.
+constexpr int kTriMatIndex = (1 << 28) - 1;
+__device__ __forceinline__ int materialClass(const DevMaterial& m) {
+  const float gl = m.glossy, rf = m.refraction;
+  if (m.emission > 0.0f) return 0;
+  if (m.transparency > 0.001f) return 5;
+  if (gl <= 0.00001f && rf <= 0.00001f) return 1;
+  if (rf <= 0.00001f && gl >= 1.0f - 0.00001f) return m.roughness < 1e-3f ? 3 : 2;
+  if (gl <= 0.00001f && rf >= 1.0f - 0.00001f) return 4;
+  return 6;
+}
+
+__global__ void k_triMaterial(DevScene S, int n, int* __restrict__ triMat) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const int mesh = __float_as_int(S.triVerts[(size_t)i * 3].w);
+  const int mat = S.objMat[S.meshObj[mesh]];
+  triMat[i] = (materialClass(S.mats[mat]) << 28) | (mat & kTriMatIndex);
+}
+
+void launchTriMaterial(const DevScene& S, int n, int* triMat, cudaStream_t st) {
+  k_triMaterial<<<(n + 255) / 256, 256, 0, st>>>(S, n, triMat);
+}
+
 // One path vertex (RayBSDFShaderProvider::shade + lobes + tracePath's medium branch).
 // MULTI = false: one job whose scene and render constants come in as kernel
 // parameters (constant bank); MULTI = true: per-ray job slot into the table.
@@ -990,15 +1016,7 @@ __global__ void __launch_bounds__(256) k_shade(DevScene S0, DevRender R0, const 
           const int prim0 = __float_as_int(Q.hits[q0].w);
           if (prim0 >= 0) {
             const DevScene& Sk = MULTI ? jobs[__float_as_int(Q.rayD[inB][q0].w)].S : S0;
-            const int mesh0 = __float_as_int(__ldg(&Sk.triVerts[(size_t)prim0 * 3].w));
-            const DevMaterial& mk = Sk.mats[Sk.objMat[Sk.meshObj[mesh0]]];
-            const float gl = mk.glossy, rf = mk.refraction;
-            if (mk.emission > 0.0f) key[h] = 0;
-            else if (mk.transparency > 0.001f) key[h] = 5;
-            else if (gl <= 0.00001f && rf <= 0.00001f) key[h] = 1;
-            else if (rf <= 0.00001f && gl >= 1.0f - 0.00001f) key[h] = mk.roughness < 1e-3f ? 3 : 2;
-            else if (gl <= 0.00001f && rf >= 1.0f - 0.00001f) key[h] = 4;
-            else key[h] = 6;
+            key[h] = __ldg(&Sk.triMat[prim0]) >> 28;
           }
         }
         // sBin[buf] was zeroed, and this buffer's order last read, before the previous
@@ -1189,7 +1207,7 @@ __global__ void __launch_bounds__(256) k_shade(DevScene S0, DevRender R0, const 
             if (dot(d, h.n) > 0.0f && dot(d, geomN) < 0.0f) h.n = geomN;
           }
           const int obj = S.meshObj[h.mesh];
-          const DevMaterial m = S.mats[S.objMat[obj]];
+          const DevMaterial m = S.mats[__ldg(&S.triMat[prim]) & kTriMatIndex];
           const V3 gN = dot(h.gn, h.n) >= 0.0f ? h.gn : -h.gn;  // geomNormal, bsdf.cpp:27-30
           const float lf = R.lightFix ? (float)S.numAreaLights : 1.0f;
           int lobe = -1;  // 0 diffuse 1 glossy 2 refraction 3 transparency

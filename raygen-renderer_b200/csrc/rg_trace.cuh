@@ -32,6 +32,8 @@ void launchQueryAny(const DevScene& S, const float* rays, const float* tmax, int
 bool setTraversalStepCap(int cap);
 // sampling-helper probes (rg_probe_sampling)
 void launchProbeSampling(int which, const float* in, int n, float* out, cudaStream_t st);
+// triMat[i] = shading class << 28 | material index of leaf-order triangle i
+void launchTriMaterial(const DevScene& S, int n, int* triMat, cudaStream_t st);
 // jobs[0].S is the scene; eval: n x 3 points -> n x 5, bend: n x 7 rays -> n x 6
 void launchMediumQuery(const DevJob* jobs, int medium, bool bend, const float* in, int n, float* out, cudaStream_t st);
 
