@@ -696,10 +696,23 @@ void buildCubeCdf(const rg_texture* faces[6], std::vector<float>& margFace, std:
   }
 }
 
+// Host-side phase timing printed to stderr when RG_TRACE_HOST is set.
+struct HostTrace {
+  bool on = std::getenv("RG_TRACE_HOST") != nullptr;
+  double t0 = hostMs(), last = t0;
+  void mark(const char* what) {
+    if (!on) return;
+    const double t = hostMs();
+    std::fprintf(stderr, "[rg] %-32s +%8.3f ms (%8.3f ms)\n", what, t - last, t - t0);
+    last = t;
+  }
+};
+
 // Validates a scene description, uploads it, builds its BVH and fills the
 // device-side table of pointers.  Used by rg_set_scene and the job server.
 rg_status prepareScene(const rg_scene_desc* d, int bins, bool wide, cudaStream_t st, int* errWord,
                        std::unique_ptr<DeviceScene>& out, DevScene& S, Mat4& view, float* buildMs) {
+  HostTrace trace;
   const int nt = d->num_triangles;
   if (nt < 0 || d->num_meshes < 0 || d->num_objects < 0 || d->num_materials < 0 || d->num_media < 0 ||
       d->num_point_lights < 0 || d->num_textures < 0) {
@@ -776,22 +789,50 @@ rg_status prepareScene(const rg_scene_desc* d, int bins, bool wide, cudaStream_t
   for (int o = 0; o < d->num_objects; o++)
     if (d->materials[objMat[o]].emission > 0.0f)
       for (int m : objMeshes[o]) isLightMesh[m] = 1;
-  std::vector<int> meshTriCount(d->num_meshes, 0);
-  std::vector<std::vector<int>> meshTris(d->num_meshes);
-  for (int i = 0; i < nt; i++) {
-    const int m = d->tri_mesh[i];
-    if (m < 0 || m >= d->num_meshes) {
-      setLastError("tri_mesh index out of range");
-      return RG_ERR_INVALID_ARGUMENT;
-    }
-    meshTriCount[m]++;
-    if (isLightMesh[m]) meshTris[m].push_back(i);
-  }
+  trace.mark("scene: checks");
+  // the previous scene's memory goes back to the pool; the triangle arrays start
+  // copying now and the host pass below runs while they are in flight
   out.reset(new DeviceScene());
+  trace.mark("scene: previous scene freed");
   DeviceScene& ds = *out;
   ds.numTris = nt;
-  view = viewMatrix(d->camera);
   ds.hasUV = d->uvs != nullptr && d->num_textures > 0;
+  bool ok = ds.inPos.upload(d->positions, (size_t)nt * 9, st) && ds.inNrm.upload(d->normals, (size_t)nt * 9, st) &&
+            ds.inTriMesh.upload(d->tri_mesh, nt, st);
+  if (ok && ds.hasUV) ok = ds.inUV.upload(d->uvs, (size_t)nt * 6, st);
+  if (!ok) {
+    cudaStreamSynchronize(st);
+    setLastError("scene upload failed (device memory)");
+    out.reset();
+    return RG_ERR_OUT_OF_MEMORY;
+  }
+  trace.mark("scene: triangle copies issued");
+  std::vector<int> meshTriCount(d->num_meshes, 0);
+  std::vector<std::vector<int>> meshTris(d->num_meshes);
+  // runs of equal mesh ids (a mesh's triangles are usually consecutive) are counted
+  // in a register and checked once
+  int runMesh = -1, run = 0;
+  bool runLight = false;
+  for (int i = 0; i < nt; i++) {
+    const int m = d->tri_mesh[i];
+    if (m != runMesh) {
+      if (m < 0 || m >= d->num_meshes) {
+        cudaStreamSynchronize(st);  // no copy into the buffers freed below is in flight
+        setLastError("tri_mesh index out of range");
+        out.reset();
+        return RG_ERR_INVALID_ARGUMENT;
+      }
+      if (runMesh >= 0) meshTriCount[runMesh] += run;
+      runMesh = m;
+      run = 0;
+      runLight = isLightMesh[m] != 0;
+    }
+    run++;
+    if (runLight) meshTris[m].push_back(i);
+  }
+  if (runMesh >= 0) meshTriCount[runMesh] += run;
+  trace.mark("scene: triangle pass");
+  view = viewMatrix(d->camera);
   std::vector<DevMaterial> mats(d->num_materials);
   for (int i = 0; i < d->num_materials; i++) mats[i] = toDev(d->materials[i]);
   MediaTables MT;
@@ -838,7 +879,8 @@ rg_status prepareScene(const rg_scene_desc* d, int bins, bool wide, cudaStream_t
     xformDir(view, d->point_lights[i].normal, n);
     pts[i] = DevPointLight{p[0], p[1], p[2], n[0], n[1], n[2], d->point_lights[i].material, 0};
   }
-  bool ok = ds.meshTriCount.upload(meshTriCount.data(), meshTriCount.size(), st) &&
+  trace.mark("scene: tables");
+  ok = ds.meshTriCount.upload(meshTriCount.data(), meshTriCount.size(), st) &&
             ds.meshObj.upload(d->mesh_object, d->num_meshes, st) && ds.objMat.upload(objMat.data(), objMat.size(), st) &&
             ds.objMedium.upload(objMed.data(), objMed.size(), st) && ds.mats.upload(mats.data(), mats.size(), st) &&
             ds.media.upload(media.data(), media.size(), st) && ds.pathPts.upload(MT.pts.data(), MT.pts.size(), st) &&
@@ -848,9 +890,7 @@ rg_status prepareScene(const rg_scene_desc* d, int bins, bool wide, cudaStream_t
             ds.lightObjMeshes.upload(lightObjMeshes.data(), lightObjMeshes.size(), st) &&
             ds.lightMeshTris.upload(lightMeshTris.data(), lightMeshTris.size(), st) &&
             ds.lightTris.upload(lightTris.data(), lightTris.size(), st) && ds.points.upload(pts.data(), pts.size(), st) &&
-            ds.view.upload(view.m, 16, st) && ds.inPos.upload(d->positions, (size_t)nt * 9, st) &&
-            ds.inNrm.upload(d->normals, (size_t)nt * 9, st) && ds.inTriMesh.upload(d->tri_mesh, nt, st);
-  if (ok && ds.hasUV) ok = ds.inUV.upload(d->uvs, (size_t)nt * 6, st);
+            ds.view.upload(view.m, 16, st);
   // textures
   std::vector<DevTexture> texs(d->num_textures);
   for (int i = 0; ok && i < d->num_textures; i++) {
@@ -895,10 +935,12 @@ rg_status prepareScene(const rg_scene_desc* d, int bins, bool wide, cudaStream_t
     }
   }
   if (!ok) {
+    cudaStreamSynchronize(st);  // no copy into the buffers freed below is in flight
     setLastError("scene upload failed (device memory)");
     out.reset();
     return RG_ERR_OUT_OF_MEMORY;
   }
+  trace.mark("scene: uploads issued");
   ds.numAreaLights = (int)areaLightObj.size();
   ds.numPointLights = (int)pts.size();
   ds.numTextures = d->num_textures;
@@ -908,8 +950,10 @@ rg_status prepareScene(const rg_scene_desc* d, int bins, bool wide, cudaStream_t
   cudaEventRecord(e0, st);
   std::string err;
   const rg_status rs = buildDeviceBvh(ds, bins > 1 ? bins : 32, wide, st, err);
+  trace.mark("scene: build launched");
   cudaEventRecord(e1, st);
   cudaStreamSynchronize(st);
+  trace.mark("scene: build done");
   float ms = 0.0f;
   cudaEventElapsedTime(&ms, e0, e1);
   cudaEventDestroy(e0);
@@ -1217,16 +1261,6 @@ namespace {
 
 // Host-side phase marks of a render, printed to stderr when RG_TRACE_HOST is
 // set (for finding host stalls between the call and the first wave).
-struct HostTrace {
-  bool on = std::getenv("RG_TRACE_HOST") != nullptr;
-  double t0 = hostMs(), last = t0;
-  void mark(const char* what) {
-    if (!on) return;
-    const double t = hostMs();
-    std::fprintf(stderr, "[rg_render] %-28s +%8.3f ms (%8.3f ms)\n", what, t - last, t - t0);
-    last = t;
-  }
-};
 
 // The render itself; the caller holds h->mu.
 rg_status renderLocked(rg_handle* h) {

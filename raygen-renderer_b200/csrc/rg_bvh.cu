@@ -13,6 +13,9 @@
 // warp-aggregated atomics.  Leaves hold at most kMaxLeaf (8) triangles:
 // where the reference would keep a larger leaf, the best SAH bin (or, for
 // coincident centroids, an index median) splits it further.
+#include <chrono>
+#include <cstdio>
+#include <cstdlib>
 #include <cub/device/device_scan.cuh>
 
 #include <cfloat>
@@ -194,6 +197,13 @@ __device__ __forceinline__ int binOf(const BNode& nd, float c, int nbins) {
 __device__ __forceinline__ float axisOf(const float4& v, int a) { return a == 0 ? v.x : (a == 1 ? v.y : v.z); }
 
 constexpr int kBinChunk = 4096;
+// Largest leaf of the 8-wide BVH (<= 4: a node's leaves address at most 32 triangles
+// through its 32-bit triangle mask); build-time overridable (-D) for sweeps.
+#ifndef RG_WIDE_MAX_LEAF
+#define RG_WIDE_MAX_LEAF 4
+#endif
+constexpr int kWideMaxLeaf = RG_WIDE_MAX_LEAF;
+static_assert(kWideMaxLeaf >= 1 && kWideMaxLeaf <= 4, "8 leaves of at most 4 triangles fill the 32-bit mask");
 constexpr int kMaxBins = 64;
 
 __global__ void __launch_bounds__(256) k_bin(int n, const int* __restrict__ primIdx, const int* __restrict__ primNode,
@@ -598,7 +608,21 @@ inline int gridFor(long long n, int block) { return (int)((n + block - 1) / bloc
 
 // Builds the view-space triangle arrays and the BVH for `n` triangles whose
 // world-space inputs are already on the device (DeviceSceneBuild fields).
+// Per-level host timing of the build, printed to stderr when RG_TRACE_HOST is set.
+struct BuildTrace {
+  bool on = std::getenv("RG_TRACE_HOST") != nullptr;
+  std::chrono::steady_clock::time_point last = std::chrono::steady_clock::now();
+  void mark(const char* what, int level, int tasks) {
+    if (!on) return;
+    const auto t = std::chrono::steady_clock::now();
+    std::fprintf(stderr, "[rg] bvh %-10s %3d: %8d tasks %8.3f ms\n", what, level, tasks,
+                 std::chrono::duration<double, std::milli>(t - last).count());
+    last = t;
+  }
+};
+
 rg_status buildDeviceBvh(DeviceScene& ds, int nbins, bool wide, cudaStream_t st, std::string& err) {
+  BuildTrace trace;
   const int n = ds.numTris;
   nbins = nbins < 2 ? 2 : (nbins > kMaxBins ? kMaxBins : nbins);
   ds.rootIsLeaf = 0;
@@ -652,8 +676,10 @@ rg_status buildDeviceBvh(DeviceScene& ds, int nbins, bool wide, cudaStream_t st,
   int* curTasks = tasksA.p;
   int* nxtTasks = tasksB.p;
   int levels = 0;
+  trace.mark("prep", 0, numTasks);
   while (numTasks > 0) {
     levels++;
+    const int tasksThisLevel = numTasks;
     cudaMemsetAsync(counters.p + 1, 0, sizeof(int), st);
     for (int c0 = 0; c0 < numTasks; c0 += chunkTasks) {
       const int nt = std::min(chunkTasks, numTasks - c0);
@@ -661,7 +687,7 @@ rg_status buildDeviceBvh(DeviceScene& ds, int nbins, bool wide, cudaStream_t st,
       k_prepareLevel<<<gridFor(prepN, 256), 256, 0, st>>>(nt, curTasks + c0, nodes.p, bins.p, nbins);
       k_bin<<<gridFor(n, kBinChunk), 256, 0, st>>>(n, curIdx, curNode, nodes.p, lo.p, hi.p, bins.p, nbins);
       k_split<<<gridFor(nt, 128), 128, 0, st>>>(nt, curTasks + c0, nodes.p, bins.p, nbins, counters.p, nxtTasks,
-                                                 counters.p + 1, wide ? 4 : kMaxLeaf);
+                                                 counters.p + 1, wide ? kWideMaxLeaf : kMaxLeaf);
     }
     k_partition<<<gridFor(n, 256), 256, 0, st>>>(n, curIdx, curNode, nodes.p, lo.p, hi.p, altIdx, altNode, nbins,
                                                  counters.p + 2);
@@ -673,6 +699,7 @@ rg_status buildDeviceBvh(DeviceScene& ds, int nbins, bool wide, cudaStream_t st,
       err = "BVH build level failed";
       return RG_ERR_CUDA;
     }
+    trace.mark("level", levels, tasksThisLevel);
     if (levels > 200) {
       err = "BVH build did not converge";
       return RG_ERR_DEVICE_STATUS;
@@ -719,6 +746,7 @@ rg_status buildDeviceBvh(DeviceScene& ds, int nbins, bool wide, cudaStream_t st,
         err = "wide BVH collapse failed";
         return RG_ERR_CUDA;
       }
+      trace.mark("collapse", lv + 1, nt);
       std::swap(cur, nxt);
       if (++lv > 200) {
         err = "wide BVH collapse did not converge";
@@ -739,6 +767,7 @@ rg_status buildDeviceBvh(DeviceScene& ds, int nbins, bool wide, cudaStream_t st,
       err = std::string("BVH gather failed: ") + cudaGetErrorString(cudaGetLastError());
       return RG_ERR_CUDA;
     }
+    trace.mark("gather", 0, n);
     return RG_OK;
   }
   // binary traversal layout
