@@ -848,6 +848,11 @@ __device__ __forceinline__ void traverseWave8(const DevScene& S0, const DevJob* 
       if (alive && result == 0) {
         const bool doTri = hasTri && (gInner == 0 || triVotes >= (ANY ? RG_TRI_VOTES_ANY : kTriVotes));
         if (doTri) {
+          // up to two triangles per step: a triangle step costs about half a node
+          // step, so two keep the triangle and node branches of a divergent warp
+          // closer in length (swept: 1 / 2 / 3 / 4 per step)
+#pragma unroll 1
+         for (int rep = 0; rep < 2 && tMask && result == 0; rep++) {
           const int i = __ffs(tMask) - 1;
           tMask &= tMask - 1u;
           const int tk = tBase + i;
@@ -871,6 +876,7 @@ __device__ __forceinline__ void traverseWave8(const DevScene& S0, const DevJob* 
               }
             }
           }
+         }
         } else {
           // node step (pending triangles are postponed onto the stack)
           if (hasTri) {
@@ -897,6 +903,16 @@ __device__ __forceinline__ void traverseWave8(const DevScene& S0, const DevJob* 
             gBase = g.childBase;
             tMask = g.tris;
             tBase = g.triBase;
+            const int nslot = (31 - __clz(gInner)) ^ (int)oct;
+            const int nnode = gBase + __popc(gImask & ((1u << nslot) - 1u));
+            // closest hit: the node this group visits next into L1 while the warp's other
+            // lanes finish their step (for shadow rays it measured slower)
+            if (!ANY && gInner && nnode < numNodes) {
+              const char* np = reinterpret_cast<const char*>(nodesP + (size_t)nnode * kNode8Vec);
+              asm volatile("prefetch.global.L1 [%0];" ::"l"(np));
+              asm volatile("prefetch.global.L1 [%0];" ::"l"(np + 128));
+              asm volatile("prefetch.global.L1 [%0];" ::"l"(np + 207));
+            }
           }
         }
       }
