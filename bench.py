@@ -14,7 +14,7 @@ depth 3, seed 1.  A step is one full render of that job.
                uploads the scene (rg_set_scene, BVH build included), renders and
                reads the HDR image back (rg_get_hdr); host wall clock.
 * roofline   : closest-hit (extend) kernel: algorithmic bytes = rays x 48 B
-               (32 B ray in + 16 B hit out) + nodes visited x 80 B (8-wide) + triangles
+               (32 B ray in + 16 B hit out) + nodes visited x 208 B (8-wide) + triangles
                tested x 48 B, over its CUDA-event time, against the measured HBM
                copy bandwidth.
 * cpu_baseline: the CPU restatement (oracle, reference compiler flags) on the
@@ -867,8 +867,8 @@ def main():
     traffic = None
     if prof and prof.get("bytes_per_ray"):
         traffic = prof["bytes_per_ray"] * s["closest_rays"] / max(1, launches_ext)
-    # the same launches counted with 80-B compressed (CWBVH-size) nodes, the unit an 8-bit
-    # quantised node format would read: comparable across node formats
+    # the same launches counted with 80-B nodes, the size of an 8-bit quantised 8-wide node:
+    # comparable across node formats
     alg80 = s["closest_rays"] * 48 + s["nodes_visited"] * 80 + s["tris_tested"] * 48
     frac80 = alg80 / (ext_ms * 1e-3) / 1e9 / peak if ext_ms > 0 else None
     roofline = {"bound": "hbm", "achieved": round(achieved, 1) if achieved else None, "peak": peak,
@@ -914,7 +914,7 @@ def main():
             "config": {"workload": "heavy geometry single job: 4 x 1,003,520-triangle displaced icospheres "
                                    "in a 20x20 room, 16 emissive quads, metal/dielectric",
                        "triangles": ntris, "resolution": f"{Wr}x{Hr}", "spp": args.spp, "max_depth": DEPTH,
-                       "bvh": f"device binned SAH (32 bins), {st.bvhWidth}-wide" + (" compressed" if st.bvhWidth == 8 else ""),
+                       "bvh": f"device binned SAH (32 bins), {st.bvhWidth}-wide" + (" (float planes)" if st.bvhWidth == 8 else ""),
                        "bvh_build_ms": round(build_ms, 2),
                        "l2": "inputs larger than L2 (BVH + triangles ~400 MB)",
                        "parallelism": f"replicas x{world}" if world > 1 else "single GPU"},

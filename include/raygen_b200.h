@@ -97,7 +97,7 @@ typedef struct rg_settings {
                                * paths (about 330 B of queues each), at most a
                                * fifth of the free device memory             */
   int32_t bvh_bins;           /* SAH bins for the device build [32]           */
-  int32_t bvh_width;          /* 8: compressed 8-wide BVH (default), 2: binary */
+  int32_t bvh_width;          /* 8: 8-wide BVH (default), 2: binary */
 } rg_settings;
 
 typedef struct rg_material {

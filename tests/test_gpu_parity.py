@@ -83,6 +83,48 @@ def test_closest_hit_parity(rg, orc, kind, params, width):
     r.close()
 
 
+def axis_rays(bounds, n, seed):
+    """Rays along the six axis directions and along directions with exactly one zero
+    component: the slab test then divides by zero (the guarded reciprocal) and meets
+    the +-inf planes of empty node slots."""
+    rng = np.random.default_rng(seed)
+    lo, hi = np.array(bounds[0], np.float64), np.array(bounds[1], np.float64)
+    o = lo + (hi - lo) * rng.random((n, 3))
+    d = np.zeros((n, 3))
+    k = rng.integers(0, 3, n)
+    axis_only = rng.random(n) < 0.5
+    d[np.arange(n), k] = np.where(rng.random(n) < 0.5, -1.0, 1.0)
+    other = (k + 1 + rng.integers(0, 2, n)) % 3
+    d[np.arange(n), other] = np.where(axis_only, 0.0, rng.normal(size=n))
+    d /= np.linalg.norm(d, axis=1, keepdims=True)
+    return np.concatenate([o, d], 1).astype(np.float32)
+
+
+@pytest.mark.parametrize("width", [8, 2])
+@pytest.mark.parametrize("kind,params", [(1, None), (2, [20000])])
+def test_axis_aligned_rays_parity(rg, orc, kind, params, width):
+    sc = rg.Scene.builtin(kind, 3, params)
+    r = rg.RayRenderer(rg.RendererSettings(resolutionWidth=8, resolutionHeight=8, samples=1, bvhWidth=width))
+    r.set_scene(sc)
+    o = orc.OracleScene(sc.ptr)
+    bounds = ((-5, -5, -20), (5, 5, -1)) if kind == 1 else ((-9, -4.9, -19), (9, 4.9, -1))
+    rays = axis_rays(bounds, 20000, 31 + kind)
+    assert np.any(rays[:, 3:] == 0.0)
+    tg, pg = r.trace_closest(rays)
+    to, po = o.closest(rays)
+    same = pg == po
+    # exact ties: a vertical ray from inside a box meets the box's bottom and the floor
+    # under it at the same distance; either id is the closest hit
+    tie = ~same & (pg >= 0) & (po >= 0) & np.isclose(tg[:, 0], to[:, 0], rtol=1e-5, atol=2e-6)
+    assert (same | tie).mean() > 0.999, (same.mean(), tie.mean())
+    hit = same & (po >= 0)
+    assert hit.mean() > 0.2
+    np.testing.assert_allclose(tg[hit], to[hit], rtol=1e-5, atol=1e-7)
+    tmax = np.random.default_rng(5).uniform(0.1, 20.0, len(rays)).astype(np.float32)
+    assert (r.trace_any(rays, tmax, 3) == o.any(rays, tmax, 3)).mean() > 0.999
+    r.close()
+
+
 @pytest.mark.parametrize("width", [8, 2])
 def test_any_hit_parity(rg, orc, width):
     sc = rg.Scene.builtin(2, 4, [20000])
