@@ -44,7 +44,6 @@ struct BNode {
   int axis;
   int binSlot;   // slot in the level's bin array while open
   int splitBin;  // bins <= splitBin go left; -2 = index median split
-  int fill[2];   // scatter cursors for the children
 };
 
 struct BinData {  // ordered-uint encoded bounds, 16 words
@@ -151,7 +150,6 @@ __global__ void k_initRoot(int n, const uint32_t* rb, BNode* nodes, int* primIdx
       r.cmin[k] = fdec(rb[6 + k]); r.cmax[k] = fdec(rb[9 + k]);
     }
     r.start = 0; r.count = n; r.left = -1; r.axis = 0; r.binSlot = 0; r.splitBin = -1;
-    r.fill[0] = r.fill[1] = 0;
     nodes[0] = r;
   }
   if (i < n) {
@@ -161,7 +159,7 @@ __global__ void k_initRoot(int n, const uint32_t* rb, BNode* nodes, int* primIdx
 }
 
 // Prepare open nodes of a level: pick the widest centroid axis (bvh.cpp:125-131).
-__global__ void k_prepareLevel(int numTasks, const int* tasks, BNode* nodes, BinData* bins, int nbins) {
+__global__ void k_prepareLevel(int numTasks, const int* tasks, BNode* nodes, BinData* bins, int nbins, bool resetBins) {
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t < numTasks) {
     BNode& nd = nodes[tasks[t]];
@@ -172,9 +170,9 @@ __global__ void k_prepareLevel(int numTasks, const int* tasks, BNode* nodes, Bin
     nd.axis = axis;
     nd.binSlot = t;
   }
-  // reset bins (one thread per bin)
+  // reset bins (one thread per bin) unless the split kernel leaves them reset
   const int b = blockIdx.x * blockDim.x + threadIdx.x;
-  if (b < numTasks * nbins) {
+  if (resetBins && b < numTasks * nbins) {
     BinData z;
     for (int k = 0; k < 3; k++) {
       z.bmin[k] = 0xFFFFFFFFu; z.bmax[k] = 0u; z.cmin[k] = 0xFFFFFFFFu; z.cmax[k] = 0u;
@@ -196,7 +194,11 @@ __device__ __forceinline__ int binOf(const BNode& nd, float c, int nbins) {
 
 __device__ __forceinline__ float axisOf(const float4& v, int a) { return a == 0 ? v.x : (a == 1 ? v.y : v.z); }
 
-constexpr int kBinChunk = 4096;
+// Primitives binned per block (build-time overridable (-D) for sweeps).
+#ifndef RG_BIN_CHUNK
+#define RG_BIN_CHUNK 1024  // swept: 1024 / 2048 / 4096 / 16384 -> 12.5 / 13.0 / 13.9 / 19.4 ms (4M triangles)
+#endif
+constexpr int kBinChunk = RG_BIN_CHUNK;
 // Largest leaf of the 8-wide BVH (<= 4: a node's leaves address at most 32 triangles
 // through its 32-bit triangle mask); build-time overridable (-D) for sweeps.
 #ifndef RG_WIDE_MAX_LEAF
@@ -206,9 +208,11 @@ constexpr int kWideMaxLeaf = RG_WIDE_MAX_LEAF;
 static_assert(kWideMaxLeaf >= 1 && kWideMaxLeaf <= 4, "8 leaves of at most 4 triangles fill the 32-bit mask");
 constexpr int kMaxBins = 64;
 
-__global__ void __launch_bounds__(256) k_bin(int n, const int* __restrict__ primIdx, const int* __restrict__ primNode,
-                                             const BNode* __restrict__ nodes, const float4* __restrict__ bmin,
-                                             const float4* __restrict__ bmax, BinData* bins, int nbins) {
+// bmin / bmax are in the current primitive order (they move with primIdx in
+// k_partition), so the passes over the primitives read them coalesced.
+__global__ void __launch_bounds__(256) k_bin(int n, const int* __restrict__ primNode, const BNode* __restrict__ nodes,
+                                             const float4* __restrict__ bmin, const float4* __restrict__ bmax,
+                                             BinData* bins, int nbins) {
   __shared__ uint32_t sb[kMaxBins][13];
   const int first = blockIdx.x * kBinChunk;
   if (first >= n) return;
@@ -228,8 +232,7 @@ __global__ void __launch_bounds__(256) k_bin(int n, const int* __restrict__ prim
     const float ext = nd.cmax[nd.axis] - nd.cmin[nd.axis];
     if (ext >= 1e-12f) {
       for (int i = first + threadIdx.x; i <= last; i += blockDim.x) {
-        const int p = primIdx[i];
-        const float4 lo = bmin[p], hi = bmax[p];
+        const float4 lo = bmin[i], hi = bmax[i];
         const float4 c = make_float4((lo.x + hi.x) * 0.5f, (lo.y + hi.y) * 0.5f, (lo.z + hi.z) * 0.5f, 0.0f);
         const int b = binOf(nd, axisOf(c, nd.axis), nbins);
         atomicMin(&sb[b][0], fenc(lo.x)); atomicMin(&sb[b][1], fenc(lo.y)); atomicMin(&sb[b][2], fenc(lo.z));
@@ -260,8 +263,7 @@ __global__ void __launch_bounds__(256) k_bin(int n, const int* __restrict__ prim
     if (nd.binSlot < 0) continue;
     const float ext = nd.cmax[nd.axis] - nd.cmin[nd.axis];
     if (ext < 1e-12f) continue;
-    const int p = primIdx[i];
-    const float4 lo = bmin[p], hi = bmax[p];
+    const float4 lo = bmin[i], hi = bmax[i];
     const float4 c = make_float4((lo.x + hi.x) * 0.5f, (lo.y + hi.y) * 0.5f, (lo.z + hi.z) * 0.5f, 0.0f);
     const int b = binOf(nd, axisOf(c, nd.axis), nbins);
     BinData& bd = bins[(size_t)nd.binSlot * nbins + b];
@@ -367,7 +369,6 @@ __global__ void k_split(int numTasks, const int* __restrict__ tasks, BNode* node
     ch[s].axis = 0;
     ch[s].binSlot = -1;
     ch[s].splitBin = -1;
-    ch[s].fill[0] = ch[s].fill[1] = 0;
     nodes[left + s] = ch[s];
     if (cnt[s] > 4) {  // BVH_LEAF_SIZE (bvh.cpp:23): larger children stay open
       const int slot = atomicAdd(nextCount, 1);
@@ -376,55 +377,229 @@ __global__ void k_split(int numTasks, const int* __restrict__ tasks, BNode* node
   }
   nd.left = left;
   nd.splitBin = split;
-  nd.fill[0] = nd.fill[1] = 0;
   nodes[id] = nd;
 }
 
-// Scatter the primitives of split nodes to their children (warp-aggregated).
-__global__ void k_partition(int n, const int* __restrict__ primIdx, const int* __restrict__ primNode,
-                            BNode* nodes, const float4* __restrict__ bmin, const float4* __restrict__ bmax,
-                            int* __restrict__ outIdx, int* __restrict__ outNode, int nbins, int* err) {
+// The same split decision with one warp per open node (nbins <= 32: lane b holds
+// bin b).  Left and right bounds come from inclusive warp scans of min / max (exact,
+// so the same values as the sequential sweeps), the cost of each split from the
+// same formula, and the choice is the lowest bin index of the lowest cost, as the
+// sweeps choose.  The warp then resets its bins for the next use, so levels need
+// no separate clear.
+__device__ __forceinline__ void resetBin(BinData* b) {
+  uint4* w = reinterpret_cast<uint4*>(b);
+  w[0] = make_uint4(0xFFFFFFFFu, 0xFFFFFFFFu, 0xFFFFFFFFu, 0u);  // bmin x y z, bmax x
+  w[1] = make_uint4(0u, 0u, 0xFFFFFFFFu, 0xFFFFFFFFu);           // bmax y z, cmin x y
+  w[2] = make_uint4(0xFFFFFFFFu, 0u, 0u, 0u);                    // cmin z, cmax x y z
+  w[3] = make_uint4(0u, 0u, 0u, 0u);                             // count, pad
+}
+
+__global__ void k_resetBins(size_t count, BinData* bins) {
+  const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < count) resetBin(bins + i);
+}
+
+template <bool MIN>
+__device__ __forceinline__ float warpScanF(float v, int lane, bool reverse) {
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const float u = reverse ? __shfl_down_sync(0xffffffffu, v, o) : __shfl_up_sync(0xffffffffu, v, o);
+    const bool in = reverse ? lane + o < 32 : lane >= o;
+    if (in) v = MIN ? fminf(v, u) : fmaxf(v, u);
+  }
+  return v;
+}
+
+__device__ __forceinline__ int warpScanI(int v, int lane, bool reverse) {
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const int u = reverse ? __shfl_down_sync(0xffffffffu, v, o) : __shfl_up_sync(0xffffffffu, v, o);
+    if (reverse ? lane + o < 32 : lane >= o) v += u;
+  }
+  return v;
+}
+
+__global__ void __launch_bounds__(128) k_splitWarp(int numTasks, const int* __restrict__ tasks, BNode* nodes,
+                                                  BinData* bins, int nbins, int* nodeCounter, int* nextTasks,
+                                                  int* nextCount, int maxLeaf) {
+  const int t = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
+  const int lane = threadIdx.x & 31;
+  if (t >= numTasks) return;
+  const int id = tasks[t];
+  BNode nd = nodes[id];
+  BinData* nb = bins + (size_t)nd.binSlot * nbins;
+  // this lane's bin (identity when empty or past nbins)
+  int cnt = 0;
+  float blo[3] = {FLT_MAX, FLT_MAX, FLT_MAX}, bhi[3] = {-FLT_MAX, -FLT_MAX, -FLT_MAX};
+  float clo[3] = {FLT_MAX, FLT_MAX, FLT_MAX}, chi[3] = {-FLT_MAX, -FLT_MAX, -FLT_MAX};
+  if (lane < nbins) {
+    const BinData b = nb[lane];
+    cnt = (int)b.count;
+    if (cnt > 0)
+      for (int k = 0; k < 3; k++) {
+        blo[k] = fdec(b.bmin[k]); bhi[k] = fdec(b.bmax[k]); clo[k] = fdec(b.cmin[k]); chi[k] = fdec(b.cmax[k]);
+      }
+    resetBin(nb + lane);
+  }
+  // left: bins 0..lane, right: bins lane..nbins-1
+  float llo[3], lhi[3], rlo[3], rhi[3];
+  for (int k = 0; k < 3; k++) {
+    llo[k] = warpScanF<true>(blo[k], lane, false);
+    lhi[k] = warpScanF<false>(bhi[k], lane, false);
+    rlo[k] = warpScanF<true>(blo[k], lane, true);
+    rhi[k] = warpScanF<false>(bhi[k], lane, true);
+  }
+  const int lc = warpScanI(cnt, lane, false), rcAll = warpScanI(cnt, lane, true);
+  // split s = lane: left = bins 0..s, right = bins s+1..nbins-1 (the right sums of lane s + 1)
+  const int rc = __shfl_down_sync(0xffffffffu, rcAll, 1);
+  float rl[3], rh[3];
+  for (int k = 0; k < 3; k++) {
+    rl[k] = __shfl_down_sync(0xffffffffu, rlo[k], 1);
+    rh[k] = __shfl_down_sync(0xffffffffu, rhi[k], 1);
+  }
+  const float pa = areaOf(nd.bmin, nd.bmax);
+  const float invPa = pa > 0.0f ? 1.0f / pa : 0.0f;
+  float cost = FLT_MAX;
+  const bool valid = lane < nbins - 1 && lc > 0 && rc > 0;
+  if (valid) {
+    const float la = areaOf(llo, lhi), ra = areaOf(rl, rh);
+    cost = 1.0f + 1.5f * invPa * (la * (float)lc + ra * (float)rc);
+  }
+  // lowest cost, then lowest split index
+  float bc = cost;
+  int bs = valid ? lane : 0x7fffffff;
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    const float oc = __shfl_xor_sync(0xffffffffu, bc, o);
+    const int os = __shfl_xor_sync(0xffffffffu, bs, o);
+    if (oc < bc || (oc == bc && os < bs)) { bc = oc; bs = os; }
+  }
+  const int forced = bs == 0x7fffffff ? -1 : bs;
+  const int best = (forced >= 0 && bc < (float)nd.count * 1.5f) ? forced : -1;
+  int split = best;
+  if (split < 0 && nd.count > maxLeaf) split = forced >= 0 ? forced : -2;  // -2: index median
+  // child bounds: reductions over the bins of each side
+  float cb[2][12];
+  int cc[2];
+  for (int sd = 0; sd < 2; sd++) {
+    const bool mine = split >= 0 && (sd == 0 ? lane <= split : lane > split);
+    for (int k = 0; k < 3; k++) {
+      float v0 = mine ? blo[k] : FLT_MAX, v1 = mine ? bhi[k] : -FLT_MAX, v2 = mine ? clo[k] : FLT_MAX,
+            v3 = mine ? chi[k] : -FLT_MAX;
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) {
+        v0 = fminf(v0, __shfl_xor_sync(0xffffffffu, v0, o));
+        v1 = fmaxf(v1, __shfl_xor_sync(0xffffffffu, v1, o));
+        v2 = fminf(v2, __shfl_xor_sync(0xffffffffu, v2, o));
+        v3 = fmaxf(v3, __shfl_xor_sync(0xffffffffu, v3, o));
+      }
+      cb[sd][k] = v0; cb[sd][3 + k] = v1; cb[sd][6 + k] = v2; cb[sd][9 + k] = v3;
+    }
+    int c = mine ? cnt : 0;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) c += __shfl_xor_sync(0xffffffffu, c, o);
+    cc[sd] = c;
+  }
+  if (lane != 0) return;
+  nd.binSlot = -1;
+  if (split == -1) {
+    nd.left = -1;
+    nodes[id] = nd;
+    return;
+  }
+  const int left = atomicAdd(nodeCounter, 2);
+  BNode ch[2];
+  int cnts[2];
+  for (int sd = 0; sd < 2; sd++) {
+    if (split == -2) {
+      cnts[0] = nd.count / 2;
+      cnts[1] = nd.count - cnts[0];
+      for (int k = 0; k < 3; k++) {
+        ch[sd].bmin[k] = nd.bmin[k]; ch[sd].bmax[k] = nd.bmax[k];
+        ch[sd].cmin[k] = nd.cmin[k]; ch[sd].cmax[k] = nd.cmax[k];
+      }
+    } else {
+      cnts[sd] = cc[sd];
+      for (int k = 0; k < 3; k++) {
+        ch[sd].bmin[k] = cb[sd][k]; ch[sd].bmax[k] = cb[sd][3 + k];
+        ch[sd].cmin[k] = cb[sd][6 + k]; ch[sd].cmax[k] = cb[sd][9 + k];
+      }
+    }
+  }
+  for (int sd = 0; sd < 2; sd++) {
+    ch[sd].start = nd.start + (sd == 0 ? 0 : cnts[0]);
+    ch[sd].count = cnts[sd];
+    ch[sd].left = -1;
+    ch[sd].axis = 0;
+    ch[sd].binSlot = -1;
+    ch[sd].splitBin = -1;
+    nodes[left + sd] = ch[sd];
+    if (cnts[sd] > 4) {  // BVH_LEAF_SIZE (bvh.cpp:23): larger children stay open
+      const int slot = atomicAdd(nextCount, 1);
+      nextTasks[slot] = left + sd;
+    }
+  }
+  nd.left = left;
+  nd.splitBin = split;
+  nodes[id] = nd;
+}
+
+// Partition, pass 1: flag 1 for a primitive that goes to the left child of its
+// node (the split bin, or the first half of the node's range for a median split).
+__global__ void k_partitionFlags(int n, const int* __restrict__ primNode, const BNode* __restrict__ nodes,
+                                 const float4* __restrict__ bmin, const float4* __restrict__ bmax, int nbins,
+                                 int* __restrict__ flags) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  const bool inRange = i < n;
-  const int node = inRange ? primNode[i] : -1;
-  const int p = inRange ? primIdx[i] : 0;
-  int side = -1, child = -1;
+  if (i >= n) return;
+  const int node = primNode[i];
+  int flag = 0;
   if (node >= 0) {
     const BNode& nd = nodes[node];
     if (nd.left >= 0) {
       if (nd.splitBin == -2) {
-        side = (i - nd.start) < nd.count / 2 ? 0 : 1;
+        flag = (i - nd.start) < nd.count / 2 ? 1 : 0;
       } else {
-        const float4 lo = bmin[p], hi = bmax[p];
+        const float4 lo = bmin[i], hi = bmax[i];
         const float c = nd.axis == 0 ? (lo.x + hi.x) * 0.5f : (nd.axis == 1 ? (lo.y + hi.y) * 0.5f : (lo.z + hi.z) * 0.5f);
-        side = binOf(nd, c, nbins) <= nd.splitBin ? 0 : 1;
+        flag = binOf(nd, c, nbins) <= nd.splitBin ? 1 : 0;
       }
-      child = nd.left + side;
     }
   }
-  // warp-aggregated cursor bump per (child) group
-  const unsigned active = __activemask();
-  const int key = child;
-  const unsigned grp = __match_any_sync(active, key);
-  int pos = -1;
-  if (child >= 0) {
-    const int leader = __ffs(grp) - 1;
-    const int rank = __popc(grp & ((1u << (threadIdx.x & 31)) - 1));
-    int base = 0;
-    if ((int)(threadIdx.x & 31) == leader) base = atomicAdd(&nodes[node].fill[side], __popc(grp));
-    base = __shfl_sync(grp, base, leader);
-    if (base + rank < nodes[child].count) pos = nodes[child].start + base + rank;
-    else atomicCAS(err, 0, kErrPartition);
+  flags[i] = flag;
+}
+
+// Partition, pass 2 (after an exclusive scan of the flags into `before`): a stable
+// scatter of each split node's primitives into its children's ranges, with their
+// bounds; primitives of closed nodes and new leaves stay where they are.  No
+// atomics, so the order (and the BVH) is the same on every run.
+__global__ void k_partitionScatter(int n, const int* __restrict__ primIdx, const int* __restrict__ primNode,
+                                   const BNode* __restrict__ nodes, const float4* __restrict__ bmin,
+                                   const float4* __restrict__ bmax, const int* __restrict__ flags,
+                                   const int* __restrict__ before, int* __restrict__ outIdx, int* __restrict__ outNode,
+                                   float4* __restrict__ outMin, float4* __restrict__ outMax, int* err) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const int node = primNode[i];
+  int pos = i, outN = -1;
+  if (node >= 0) {
+    const BNode& nd = nodes[node];
+    if (nd.left >= 0) {
+      const int leftBefore = before[i] - before[nd.start];
+      const int side = flags[i] ? 0 : 1;
+      const int rank = side == 0 ? leftBefore : (i - nd.start) - leftBefore;
+      const BNode& cn = nodes[nd.left + side];
+      if (rank >= cn.count) {
+        atomicCAS(err, 0, kErrPartition);
+        return;
+      }
+      pos = cn.start + rank;
+      outN = cn.count > 4 ? nd.left + side : -1;
+    }
   }
-  if (!inRange) return;
-  if (child >= 0) {
-    if (pos < 0) return;
-    outIdx[pos] = p;
-    outNode[pos] = nodes[child].count > 4 ? child : -1;
-  } else {
-    outIdx[i] = p;
-    outNode[i] = -1;
-  }
+  outIdx[pos] = primIdx[i];
+  outNode[pos] = outN;
+  outMin[pos] = bmin[i];
+  outMax[pos] = bmax[i];
 }
 
 __global__ void k_innerFlags(int numNodes, const BNode* __restrict__ nodes, int* flags) {
@@ -629,7 +804,7 @@ rg_status buildDeviceBvh(DeviceScene& ds, int nbins, bool wide, cudaStream_t st,
   ds.rootLeafRef = 0;
   ds.numNodes = 0;
   if (n == 0) return RG_OK;
-  DevBuf<float4> vTmp, sTmp, lo, hi;
+  DevBuf<float4> vTmp, sTmp, lo, hi, lo2, hi2;
   DevBuf<float2> uvTmp;
   if (!vTmp.alloc((size_t)n * 3) || !sTmp.alloc((size_t)n * 3) || !lo.alloc(n) || !hi.alloc(n)) {
     err = "out of device memory (triangle staging)";
@@ -652,9 +827,10 @@ rg_status buildDeviceBvh(DeviceScene& ds, int nbins, bool wide, cudaStream_t st,
   // bins for at most chunkTasks open nodes at a time (<= 256 MB)
   const int chunkTasks = (int)std::min<size_t>((size_t)n / 4 + 2, ((size_t)256 << 20) / (sizeof(BinData) * nbins));
   DevBuf<BNode> nodes;
-  DevBuf<int> idxA, idxB, nodeA, nodeB, tasksA, tasksB, counters;
+  DevBuf<int> idxA, idxB, nodeA, nodeB, tasksA, tasksB, counters, pflags, pbefore;
   DevBuf<BinData> bins;
   if (!nodes.alloc(maxNodes) || !idxA.alloc(n) || !idxB.alloc(n) || !nodeA.alloc(n) || !nodeB.alloc(n) ||
+      !lo2.alloc(n) || !hi2.alloc(n) || !pflags.alloc(n) || !pbefore.alloc(n) ||
       !tasksA.alloc((size_t)n / 4 + 2) || !tasksB.alloc((size_t)n / 4 + 2) || !counters.alloc(4) ||
       !bins.alloc((size_t)chunkTasks * nbins)) {
     err = "out of device memory (BVH build)";
@@ -675,6 +851,25 @@ rg_status buildDeviceBvh(DeviceScene& ds, int nbins, bool wide, cudaStream_t st,
   int* altNode = nodeB.p;
   int* curTasks = tasksA.p;
   int* nxtTasks = tasksB.p;
+  // up to 32 bins: one warp per node decides the split and resets its bins, which
+  // therefore start reset once here
+  const bool warpSplit = nbins <= 32;
+  if (warpSplit) {
+    const size_t nb = (size_t)chunkTasks * nbins;
+    k_resetBins<<<(unsigned)((nb + 255) / 256), 256, 0, st>>>(nb, bins.p);
+  }
+  // scratch of the partition's prefix sum
+  size_t scanBytes = 0;
+  cub::DeviceScan::ExclusiveSum(nullptr, scanBytes, pflags.p, pbefore.p, n, st);
+  DevBuf<unsigned char> scanTmp;
+  if (!scanTmp.alloc(scanBytes + 16)) {
+    err = "out of device memory (BVH build)";
+    return RG_ERR_OUT_OF_MEMORY;
+  }
+  float4* curLo = lo.p;
+  float4* curHi = hi.p;
+  float4* altLo = lo2.p;
+  float4* altHi = hi2.p;
   int levels = 0;
   trace.mark("prep", 0, numTasks);
   while (numTasks > 0) {
@@ -683,16 +878,25 @@ rg_status buildDeviceBvh(DeviceScene& ds, int nbins, bool wide, cudaStream_t st,
     cudaMemsetAsync(counters.p + 1, 0, sizeof(int), st);
     for (int c0 = 0; c0 < numTasks; c0 += chunkTasks) {
       const int nt = std::min(chunkTasks, numTasks - c0);
-      const int prepN = std::max(nt, nt * nbins);
-      k_prepareLevel<<<gridFor(prepN, 256), 256, 0, st>>>(nt, curTasks + c0, nodes.p, bins.p, nbins);
-      k_bin<<<gridFor(n, kBinChunk), 256, 0, st>>>(n, curIdx, curNode, nodes.p, lo.p, hi.p, bins.p, nbins);
-      k_split<<<gridFor(nt, 128), 128, 0, st>>>(nt, curTasks + c0, nodes.p, bins.p, nbins, counters.p, nxtTasks,
-                                                 counters.p + 1, wide ? kWideMaxLeaf : kMaxLeaf);
+      const int prepN = warpSplit ? nt : std::max(nt, nt * nbins);
+      k_prepareLevel<<<gridFor(prepN, 256), 256, 0, st>>>(nt, curTasks + c0, nodes.p, bins.p, nbins, !warpSplit);
+      k_bin<<<gridFor(n, kBinChunk), 256, 0, st>>>(n, curNode, nodes.p, curLo, curHi, bins.p, nbins);
+      if (warpSplit)
+        k_splitWarp<<<gridFor((long long)nt * 32, 128), 128, 0, st>>>(nt, curTasks + c0, nodes.p, bins.p, nbins,
+                                                                      counters.p, nxtTasks, counters.p + 1,
+                                                                      wide ? kWideMaxLeaf : kMaxLeaf);
+      else
+        k_split<<<gridFor(nt, 128), 128, 0, st>>>(nt, curTasks + c0, nodes.p, bins.p, nbins, counters.p, nxtTasks,
+                                                   counters.p + 1, wide ? kWideMaxLeaf : kMaxLeaf);
     }
-    k_partition<<<gridFor(n, 256), 256, 0, st>>>(n, curIdx, curNode, nodes.p, lo.p, hi.p, altIdx, altNode, nbins,
-                                                 counters.p + 2);
+    k_partitionFlags<<<gridFor(n, 256), 256, 0, st>>>(n, curNode, nodes.p, curLo, curHi, nbins, pflags.p);
+    cub::DeviceScan::ExclusiveSum(scanTmp.p, scanBytes, pflags.p, pbefore.p, n, st);
+    k_partitionScatter<<<gridFor(n, 256), 256, 0, st>>>(n, curIdx, curNode, nodes.p, curLo, curHi, pflags.p, pbefore.p,
+                                                        altIdx, altNode, altLo, altHi, counters.p + 2);
     std::swap(curIdx, altIdx);
     std::swap(curNode, altNode);
+    std::swap(curLo, altLo);
+    std::swap(curHi, altHi);
     std::swap(curTasks, nxtTasks);
     cudaMemcpyAsync(&numTasks, counters.p + 1, sizeof(int), cudaMemcpyDeviceToHost, st);
     if (cudaStreamSynchronize(st) != cudaSuccess) {
