@@ -305,12 +305,18 @@ struct rg_handle {
   std::atomic<bool> asyncBusy{false};      // an rg_render_async job is in flight
   double firstWaveHostMs = 0.0;            // host clock when the render's first wave was launched
   cudaEvent_t waveDone[2] = {nullptr, nullptr};
+  // second stream of the wave graph: a bounce's shadow rays beside the next bounce's closest hits
+  cudaStream_t side = nullptr;
+  cudaEvent_t fork = nullptr, join = nullptr;
   rg_stats lastStats{};
   ~rg_handle() {
     for (auto e : waveDone)
       if (e) cudaEventDestroy(e);
+    if (fork) cudaEventDestroy(fork);
+    if (join) cudaEventDestroy(join);
     if (graph) cudaGraphExecDestroy(graph);
     scene.reset();
+    if (side) cudaStreamDestroy(side);
     if (stream) cudaStreamDestroy(stream);
   }
 };
@@ -450,19 +456,38 @@ void enqueueWave(rg_handle* h, const DevRender& R, const DevQueues& Q, const Dev
   if (shader != 5) {
     launchSimple(jobs, W, Q, g.simple, st);
   } else {
+    auto connects = [&](int it, cudaStream_t cs) {
+      launchConnect(&h->dscene, jobs, width, Q, it, 0, g.conn, cs);
+      if (h->dscene.numPointLights > 0) launchConnect(&h->dscene, jobs, width, Q, it, 1, g.conn, cs);
+      if (h->dscene.envOn) launchConnect(&h->dscene, jobs, width, Q, it, 2, g.conn, cs);
+      if (h->dscene.numVolLights > 0) launchConnect(&h->dscene, jobs, width, Q, it, 3, g.conn, cs);
+    };
     launchGenerate(jobs, W, Q, g.gen, st);
     for (int it = 0; it < Q.maxIter; it++) {
-      if (profile) cudaEventRecord((*ev)[it * 4 + 0], st);
+      if (profile) {  // serial, one event between kernels
+        cudaEventRecord((*ev)[it * 4 + 0], st);
+        launchExtend(&h->dscene, jobs, width, Q, it, g.ext, st);
+        cudaEventRecord((*ev)[it * 4 + 1], st);
+        launchShade(&h->dscene, &R, jobs, Q, it, g.shade, st);
+        cudaEventRecord((*ev)[it * 4 + 2], st);
+        connects(it, st);
+        cudaEventRecord((*ev)[it * 4 + 3], st);
+        continue;
+      }
+      // the previous bounce's shadow rays (they only add into the path radiance)
+      // run beside this bounce's closest hits; the shade kernel, which rewrites the
+      // shadow queues and the radiance, waits for both
+      if (it > 0) {
+        cudaEventRecord(h->fork, st);
+        cudaStreamWaitEvent(h->side, h->fork, 0);
+        connects(it - 1, h->side);
+        cudaEventRecord(h->join, h->side);
+      }
       launchExtend(&h->dscene, jobs, width, Q, it, g.ext, st);
-      if (profile) cudaEventRecord((*ev)[it * 4 + 1], st);
+      if (it > 0) cudaStreamWaitEvent(st, h->join, 0);
       launchShade(&h->dscene, &R, jobs, Q, it, g.shade, st);
-      if (profile) cudaEventRecord((*ev)[it * 4 + 2], st);
-      launchConnect(&h->dscene, jobs, width, Q, it, 0, g.conn, st);
-      if (h->dscene.numPointLights > 0) launchConnect(&h->dscene, jobs, width, Q, it, 1, g.conn, st);
-      if (h->dscene.envOn) launchConnect(&h->dscene, jobs, width, Q, it, 2, g.conn, st);
-      if (h->dscene.numVolLights > 0) launchConnect(&h->dscene, jobs, width, Q, it, 3, g.conn, st);
-      if (profile) cudaEventRecord((*ev)[it * 4 + 3], st);
     }
+    if (!profile && Q.maxIter > 0) connects(Q.maxIter - 1, st);
   }
   launchAccumulate(jobs, W, Q, g.acc, st);
   k_nextWave<<<1, 1, 0, st>>>(h->curWave.p);
@@ -546,7 +571,10 @@ rg_status rg_create(const rg_settings* s, rg_handle** out) {
   cudaGetDevice(&h->device);
   cudaDeviceGetAttribute(&h->numSMs, cudaDevAttrMultiProcessorCount, h->device);
   keepPoolMemory();
-  if (cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking) != cudaSuccess) {
+  if (cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaStreamCreateWithFlags(&h->side, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaEventCreateWithFlags(&h->fork, cudaEventDisableTiming) != cudaSuccess ||
+      cudaEventCreateWithFlags(&h->join, cudaEventDisableTiming) != cudaSuccess) {
     setLastError("cudaStreamCreate failed");
     delete h;
     return RG_ERR_CUDA;

@@ -129,6 +129,8 @@ struct rg_server {
   std::deque<ServerJob*> finishing;    // jobs whose last wave has run, for the finisher
   cudaStream_t finishStream = nullptr;
   cudaStream_t stream = nullptr;
+  cudaStream_t side = nullptr;  // second stream of the wave graphs
+  cudaEvent_t fork = nullptr, join = nullptr;
   std::vector<cudaStream_t> admitStreams;
   int numSMs = 148;
   // device tables and wavefront buffers
@@ -157,6 +159,9 @@ struct rg_server {
       if (g) cudaGraphExecDestroy(g);
     if (hostSegs) cudaFreeHost(hostSegs);
     if (hostWave) cudaFreeHost(hostWave);
+    if (fork) cudaEventDestroy(fork);
+    if (join) cudaEventDestroy(join);
+    if (side) cudaStreamDestroy(side);
     if (stream) cudaStreamDestroy(stream);
     if (finishStream) cudaStreamDestroy(finishStream);
     if (sceneStream) cudaStreamDestroy(sceneStream);
@@ -220,15 +225,27 @@ bool captureGraph(rg_server* s) {
     const bool procedural = k == 1;
     cudaGraph_t g;
     if (cudaStreamBeginCapture(s->stream, cudaStreamCaptureModeThreadLocal) != cudaSuccess) return false;
+    auto connects = [&](int it, cudaStream_t cs) {
+      launchConnect(nullptr, s->jobTable.p, 8, Q, it, 0, conn, cs);
+      launchConnect(nullptr, s->jobTable.p, 8, Q, it, 1, conn, cs);
+      launchConnect(nullptr, s->jobTable.p, 8, Q, it, 2, conn, cs);
+      if (procedural) launchConnect(nullptr, s->jobTable.p, 8, Q, it, 3, conn, cs);
+    };
     launchGenerate(s->jobTable.p, s->waveSlot.p, Q, shadeGrid * 2, s->stream);
     for (int it = 0; it < Q.maxIter; it++) {
+      // the previous bounce's shadow rays beside this bounce's closest hits; the
+      // shade kernel (it rewrites the shadow queues and the radiance) waits for both
+      if (it > 0) {
+        cudaEventRecord(s->fork, s->stream);
+        cudaStreamWaitEvent(s->side, s->fork, 0);
+        connects(it - 1, s->side);
+        cudaEventRecord(s->join, s->side);
+      }
       launchExtend(nullptr, s->jobTable.p, 8, Q, it, ext, s->stream);
+      if (it > 0) cudaStreamWaitEvent(s->stream, s->join, 0);
       launchShade(nullptr, nullptr, s->jobTable.p, Q, it, shadeGrid, s->stream, procedural ? 2 : 1);
-      launchConnect(nullptr, s->jobTable.p, 8, Q, it, 0, conn, s->stream);
-      launchConnect(nullptr, s->jobTable.p, 8, Q, it, 1, conn, s->stream);
-      launchConnect(nullptr, s->jobTable.p, 8, Q, it, 2, conn, s->stream);
-      if (procedural) launchConnect(nullptr, s->jobTable.p, 8, Q, it, 3, conn, s->stream);
     }
+    if (Q.maxIter > 0) connects(Q.maxIter - 1, s->stream);
     launchAccumulate(s->jobTable.p, s->waveSlot.p, Q, shadeGrid, s->stream);
     if (cudaStreamEndCapture(s->stream, &g) != cudaSuccess) return false;
     const bool ok = cudaGraphInstantiate(&s->graph[k], g, 0) == cudaSuccess;
@@ -603,7 +620,10 @@ rg_status rg_server_create(const rg_settings* base, const rg_server_config* cfg,
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&s->numSMs, cudaDevAttrMultiProcessorCount, dev);
   bool streamsOk = cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking) == cudaSuccess &&
-                   cudaStreamCreateWithFlags(&s->finishStream, cudaStreamNonBlocking) == cudaSuccess;
+                   cudaStreamCreateWithFlags(&s->finishStream, cudaStreamNonBlocking) == cudaSuccess &&
+                   cudaStreamCreateWithFlags(&s->side, cudaStreamNonBlocking) == cudaSuccess &&
+                   cudaEventCreateWithFlags(&s->fork, cudaEventDisableTiming) == cudaSuccess &&
+                   cudaEventCreateWithFlags(&s->join, cudaEventDisableTiming) == cudaSuccess;
   for (int i = 0; i < kAdmitThreads && streamsOk; i++) {
     cudaStream_t a = nullptr;
     streamsOk = cudaStreamCreateWithFlags(&a, cudaStreamNonBlocking) == cudaSuccess;
