@@ -431,6 +431,11 @@ namespace {
 
 DevRender makeRender(const rg_handle* h) { return makeRenderParams(h->st, h->camera); }
 
+// Shade / accumulate blocks per SM of grid (two of 256 threads are resident at 119
+// registers; the rest follow in grid-stride windows); build-time overridable (-D).
+#ifndef RG_SHADE_BLOCKS_PER_SM
+#define RG_SHADE_BLOCKS_PER_SM 4
+#endif
 struct Grids {
   int gen, ext, shade, conn, acc, simple;
 };
@@ -439,7 +444,7 @@ Grids grids(rg_handle* h) {
   Grids g;
   g.gen = h->numSMs * 8;
   g.ext = h->numSMs * residentBlocks(0, h->dscene.bvhWidth);
-  g.shade = h->numSMs * 4;
+  g.shade = h->numSMs * RG_SHADE_BLOCKS_PER_SM;
   g.conn = h->numSMs * residentBlocks(1, h->dscene.bvhWidth);
   g.acc = h->numSMs * 4;
   g.simple = h->numSMs * 8;
