@@ -943,6 +943,9 @@ __device__ __forceinline__ void traverseWave8(const DevScene& S0, const DevJob* 
 #ifndef RG_TRACE_MIN_BLOCKS
 #define RG_TRACE_MIN_BLOCKS 8
 #endif
+#ifndef RG_CONNECT_MIN_BLOCKS
+#define RG_CONNECT_MIN_BLOCKS RG_TRACE_MIN_BLOCKS
+#endif
 template <bool MULTI>
 __global__ void __launch_bounds__(128, RG_TRACE_MIN_BLOCKS) k_extend8(DevScene S0, const DevJob* __restrict__ jobs, DevQueues Q, int iter) {
   const int count = Q.counters[iter * kCountersPerIter + C_RAYS];
@@ -955,7 +958,7 @@ __global__ void __launch_bounds__(128, RG_TRACE_MIN_BLOCKS) k_extend8(DevScene S
 }
 
 template <bool MULTI>
-__global__ void __launch_bounds__(128, RG_TRACE_MIN_BLOCKS) k_connect8(DevScene S0, const DevJob* __restrict__ jobs, DevQueues Q, int iter,
+__global__ void __launch_bounds__(128, RG_CONNECT_MIN_BLOCKS) k_connect8(DevScene S0, const DevJob* __restrict__ jobs, DevQueues Q, int iter,
                                                   int which) {
   const int count = Q.counters[iter * kCountersPerIter + shadowCountSlot(which)];
   uint32_t nodes = 0, tris = 0, rays = 0;
