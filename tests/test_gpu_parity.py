@@ -126,6 +126,24 @@ def test_axis_aligned_rays_parity(rg, orc, kind, params, width):
 
 
 @pytest.mark.parametrize("width", [8, 2])
+def test_bvh_build_is_deterministic(rg, width):
+    """The build partitions with a prefix sum, not atomics: two builds of one scene on two
+    handles give the same BVH, so every hit (exact ties included) and the node counts agree."""
+    sc = rg.Scene.builtin(2, 6, [30000])
+    rays = scenes.random_rays(((-9, -4.9, -19), (9, 4.9, -1)), 30000, 17)
+    out = []
+    for _ in range(2):
+        r = rg.RayRenderer(rg.RendererSettings(resolutionWidth=8, resolutionHeight=8, samples=1, bvhWidth=width))
+        r.set_scene(sc)
+        t, p = r.trace_closest(rays)
+        out.append((t, p, r.stats()["bvh_nodes"]))
+        r.close()
+    np.testing.assert_array_equal(out[0][1], out[1][1])
+    np.testing.assert_array_equal(out[0][0], out[1][0])
+    assert out[0][2] == out[1][2]
+
+
+@pytest.mark.parametrize("width", [8, 2])
 def test_any_hit_parity(rg, orc, width):
     sc = rg.Scene.builtin(2, 4, [20000])
     r = rg.RayRenderer(rg.RendererSettings(resolutionWidth=8, resolutionHeight=8, samples=1, bvhWidth=width))
