@@ -58,3 +58,29 @@ def test_head_is_a_normalised_filter():
     const = np.full_like(noisy, 0.7)
     g = ko.forward(ko.init_params(5), X0, const)
     assert np.allclose(g["out"], 0.7)
+
+
+def test_training_input_spp_levels():
+    """kpcn_train.input_spp: distinct powers of two in [lo, lo_max], the same for a scene
+    index every time, and a single level when no range is given."""
+    import importlib.util
+    import os
+    path = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "raygen-renderer_b200",
+                        "kpcn_train.py")
+    spec = importlib.util.spec_from_file_location("kpcn_train_cpu", path)
+    kt = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(kt)
+    seen = set()
+    for k in range(200):
+        lv = kt.input_spp(k, 4, 256, 2)
+        assert lv == kt.input_spp(k, 4, 256, 2)
+        assert len(lv) == 2 and len(set(lv)) == 2 and lv == sorted(lv)
+        for v in lv:
+            assert 4 <= v <= 256 and (v & (v - 1)) == 0
+            seen.add(v)
+        assert kt.input_spp(k, 8, 0, 1) == [8]
+    assert seen == {4, 8, 16, 32, 64, 128, 256}
+    # the features' noise-level channel: log2(1 + spp) / 12
+    f = ko.features(np.zeros((1, 2, 2, 3)), np.zeros((1, 2, 2, 3)), np.zeros((1, 2, 2, 3)), np.zeros((1, 2, 2)),
+                    spp=255.0, exact=True)
+    assert np.allclose(f[..., 10], 8.0 / 12.0) and np.all(f[..., 11:] == 0)
