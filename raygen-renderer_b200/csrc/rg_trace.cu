@@ -735,7 +735,10 @@ __global__ void __launch_bounds__(128) k_connect(const DevJob* __restrict__ jobs
 #define RG_TRI_VOTES_ANY 4
 #endif
 constexpr int kRefillIdle = RG_REFILL_IDLE_CLOSEST;  // refill once this many lanes are idle
-constexpr int kSharedStack = 8;    // traversal stack entries kept in shared memory (the rest in local)
+#ifndef RG_SHARED_STACK
+#define RG_SHARED_STACK 8
+#endif
+constexpr int kSharedStack = RG_SHARED_STACK;  // traversal stack entries kept in shared memory (the rest in local)
 constexpr int kTraceBlock = 128;   // block size of the persistent traversal kernels
 constexpr int kTriVotes = RG_TRI_VOTES_CLOSEST;  // lanes with triangles needed to run a triangle step (swept: 2-4 best, 10 -1.6%)
 
