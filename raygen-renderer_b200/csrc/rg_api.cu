@@ -331,15 +331,28 @@ double hostMs() {
 
 }  // namespace
 
+// every device buffer of a DeviceScene but the texture texels
+#define RG_SCENE_BUFFERS(X)                                                                                    \
+  X(inPos) X(inNrm) X(inUV) X(inTriMesh) X(view) X(meshObj) X(meshTriCount) X(objMat) X(objMedium) X(mats)      \
+  X(media) X(pathPts) X(volLights) X(areaLightObj) X(lightMeshList) X(lightObjMeshes) X(lightMeshTris)           \
+  X(lightTris) X(points) X(textures) X(envMarg) X(envCond) X(cubeMargFace) X(cubeMargY) X(cubeCond) X(nodes)     \
+  X(nodes8) X(triVerts) X(triShade) X(triUV) X(triOrig) X(triMat)
+
 size_t DeviceScene::deviceBytes() const {
-  size_t b = inPos.bytes() + inNrm.bytes() + inUV.bytes() + inTriMesh.bytes() + view.bytes();
-  b += meshObj.bytes() + meshTriCount.bytes() + objMat.bytes() + objMedium.bytes() + mats.bytes() + media.bytes();
-  b += pathPts.bytes() + volLights.bytes() + areaLightObj.bytes() + lightMeshList.bytes() + lightObjMeshes.bytes();
-  b += lightMeshTris.bytes() + lightTris.bytes() + points.bytes() + textures.bytes() + envMarg.bytes();
-  b += envCond.bytes() + cubeMargFace.bytes() + cubeMargY.bytes() + cubeCond.bytes() + nodes.bytes();
-  b += nodes8.bytes() + triVerts.bytes() + triShade.bytes() + triUV.bytes() + triOrig.bytes() + triMat.bytes();
+  size_t b = 0;
+#define RG_ADD_BYTES(m) b += m.bytes();
+  RG_SCENE_BUFFERS(RG_ADD_BYTES)
+#undef RG_ADD_BYTES
   for (const auto* t : texels) b += t ? t->bytes() : 0;
   return b;
+}
+
+void DeviceScene::adoptBuffers(DeviceScene& old) {
+#define RG_TAKE(m) m.swap(old.m);
+  RG_SCENE_BUFFERS(RG_TAKE)
+#undef RG_TAKE
+  texels.swap(old.texels);
+  std::swap(scratch, old.scratch);
 }
 
 namespace {
@@ -744,7 +757,7 @@ struct HostTrace {
 // Validates a scene description, uploads it, builds its BVH and fills the
 // device-side table of pointers.  Used by rg_set_scene and the job server.
 rg_status prepareScene(const rg_scene_desc* d, int bins, bool wide, cudaStream_t st, int* errWord,
-                       std::unique_ptr<DeviceScene>& out, DevScene& S, Mat4& view, float* buildMs) {
+                       std::unique_ptr<DeviceScene>& out, DevScene& S, Mat4& view, float* buildMs, bool keep) {
   HostTrace trace;
   const int nt = d->num_triangles;
   if (nt < 0 || d->num_meshes < 0 || d->num_objects < 0 || d->num_materials < 0 || d->num_media < 0 ||
@@ -823,10 +836,16 @@ rg_status prepareScene(const rg_scene_desc* d, int bins, bool wide, cudaStream_t
     if (d->materials[objMat[o]].emission > 0.0f)
       for (int m : objMeshes[o]) isLightMesh[m] = 1;
   trace.mark("scene: checks");
-  // the previous scene's memory goes back to the pool; the triangle arrays start
-  // copying now and the host pass below runs while they are in flight
-  out.reset(new DeviceScene());
-  trace.mark("scene: previous scene freed");
+  // the previous scene's memory is reused (keep) or goes back to the pool; the
+  // triangle arrays start copying now and the host pass below runs while they
+  // are in flight
+  {
+    std::unique_ptr<DeviceScene> next(new DeviceScene());
+    if (keep && out) next->adoptBuffers(*out);
+    next->keepBuffers = keep;
+    out = std::move(next);
+  }
+  trace.mark("scene: previous scene replaced");
   DeviceScene& ds = *out;
   ds.numTris = nt;
   ds.hasUV = d->uvs != nullptr && d->num_textures > 0;
@@ -928,11 +947,16 @@ rg_status prepareScene(const rg_scene_desc* d, int bins, bool wide, cudaStream_t
   std::vector<DevTexture> texs(d->num_textures);
   for (int i = 0; ok && i < d->num_textures; i++) {
     const rg_texture& t = d->textures[i];
-    auto* buf = new DevBuf<float4>();
-    ds.texels.push_back(buf);
+    if ((size_t)i >= ds.texels.size()) ds.texels.push_back(new DevBuf<float4>());
+    DevBuf<float4>* buf = ds.texels[i];
     const size_t cnt = (size_t)std::max(0, t.width) * std::max(0, t.height);
     ok = buf->upload(reinterpret_cast<const float4*>(t.rgba), cnt, st);
     texs[i] = DevTexture{buf->p, t.width, t.height, t.is_hdr, 0};
+  }
+  // texels adopted from a scene with more textures
+  while (ok && ds.texels.size() > (size_t)d->num_textures) {
+    delete ds.texels.back();
+    ds.texels.pop_back();
   }
   if (ok) ok = ds.textures.upload(texs.data(), texs.size(), st);
   if (ok && (d->has_envmap || d->envmap_cube)) {
@@ -997,10 +1021,14 @@ rg_status prepareScene(const rg_scene_desc* d, int bins, bool wide, cudaStream_t
     return rs;
   }
   if (buildMs) *buildMs = ms;
-  ds.inPos.release();
-  ds.inNrm.release();
-  ds.inUV.release();
-  ds.inTriMesh.release();
+  if (!keep) {
+    ds.inPos.release();
+    ds.inNrm.release();
+    ds.inUV.release();
+    ds.inTriMesh.release();
+    freeBvhScratch(ds.scratch);
+    ds.scratch = nullptr;
+  }
   std::memset(&S, 0, sizeof(S));
   S.nodes = ds.nodes.p;
   S.numNodes = ds.numNodes;
@@ -1082,7 +1110,7 @@ rg_status rg_set_scene(rg_handle* h, const rg_scene_desc* d) {
   cudaMemsetAsync(h->error.p, 0, sizeof(int), h->stream);
   float ms = 0.0f;
   const rg_status rs = prepareScene(d, h->st.bvh_bins, h->st.bvh_width != 2, h->stream, h->error.p, h->scene,
-                                    h->dscene, h->view, &ms);
+                                    h->dscene, h->view, &ms, /*keep=*/true);
   if (rs != RG_OK) return rs;
   h->camera = d->camera;
   h->lastStats.build_ms = ms;

@@ -655,9 +655,11 @@ __global__ void k_gather(int n, const int* __restrict__ primIdx, const float4* _
 // Slots are assigned per octant: a child whose centre lies on the negative side
 // of the node centre along axis k prefers slots with bit k set, so visiting hit
 // slots in descending order of (slot XOR ray octant) is roughly front to back.
+// countOnly: the same child choices, nothing written but the node count and the
+// next level's tasks (the host sizes the node array with it).
 __global__ void k_collapse(int numTasks, const int2* __restrict__ tasks, const BNode* __restrict__ nodes,
                            const int* __restrict__ primIdx, float4* __restrict__ nodes8, int* counters,
-                           int2* __restrict__ nextTasks, int* __restrict__ triOrder, int maxNodes8) {
+                           int2* __restrict__ nextTasks, int* __restrict__ triOrder, int maxNodes8, bool countOnly) {
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= numTasks) return;
   const int2 task = tasks[t];
@@ -685,6 +687,14 @@ __global__ void k_collapse(int numTasks, const int2* __restrict__ tasks, const B
       ch[best] = l;
       ch[nc++] = l + 1;
     }
+  }
+  if (countOnly) {
+    for (int i = 0; i < nc; i++)
+      if (nodes[ch[i]].left >= 0) {
+        atomicAdd(&counters[0], 1);
+        nextTasks[atomicAdd(&counters[2], 1)] = make_int2(ch[i], 0);
+      }
+    return;
   }
   float lo[3] = {FLT_MAX, FLT_MAX, FLT_MAX}, hi[3] = {-FLT_MAX, -FLT_MAX, -FLT_MAX};
   float cc[8][3];
@@ -796,6 +806,22 @@ struct BuildTrace {
   }
 };
 
+// The build's working arrays; a scene rebuilt in place keeps them, so a build no
+// larger than the last allocates nothing (DevBuf::alloc only grows).
+struct BvhScratch {
+  DevBuf<float4> vTmp, sTmp, lo, hi, lo2, hi2;
+  DevBuf<float2> uvTmp;
+  DevBuf<uint32_t> rb;
+  DevBuf<BNode> nodes;
+  DevBuf<int> idxA, idxB, nodeA, nodeB, tasksA, tasksB, counters, pflags, pbefore;
+  DevBuf<BinData> bins;
+  DevBuf<unsigned char> scanTmp, tmp;
+  DevBuf<int2> ta, tb;
+  DevBuf<int> order, c8, flags, trav;
+};
+
+void freeBvhScratch(BvhScratch* s) { delete s; }
+
 rg_status buildDeviceBvh(DeviceScene& ds, int nbins, bool wide, cudaStream_t st, std::string& err) {
   BuildTrace trace;
   const int n = ds.numTris;
@@ -804,19 +830,25 @@ rg_status buildDeviceBvh(DeviceScene& ds, int nbins, bool wide, cudaStream_t st,
   ds.rootLeafRef = 0;
   ds.numNodes = 0;
   if (n == 0) return RG_OK;
-  DevBuf<float4> vTmp, sTmp, lo, hi, lo2, hi2;
-  DevBuf<float2> uvTmp;
+  if (!ds.scratch) ds.scratch = new BvhScratch();
+  BvhScratch& X = *ds.scratch;
+  DevBuf<float4> &vTmp = X.vTmp, &sTmp = X.sTmp, &lo = X.lo, &hi = X.hi, &lo2 = X.lo2, &hi2 = X.hi2;
+  DevBuf<float2>& uvTmp = X.uvTmp;
   if (!vTmp.alloc((size_t)n * 3) || !sTmp.alloc((size_t)n * 3) || !lo.alloc(n) || !hi.alloc(n)) {
     err = "out of device memory (triangle staging)";
     return RG_ERR_OUT_OF_MEMORY;
   }
   if (ds.hasUV && !uvTmp.alloc((size_t)n * 3)) return RG_ERR_OUT_OF_MEMORY;
+  trace.mark("alloc stage", 0, n);
   k_prepTriangles<<<gridFor(n, 256), 256, 0, st>>>(n, ds.inPos.p, ds.inNrm.p, ds.hasUV ? ds.inUV.p : nullptr,
                                                    ds.inTriMesh.p, ds.meshObj.p, ds.objMat.p, ds.mats.p, ds.view.p,
                                                    vTmp.p, sTmp.p, ds.hasUV ? uvTmp.p : nullptr, lo.p, hi.p);
   // root bounds
-  DevBuf<uint32_t> rb;
-  rb.alloc(12);
+  DevBuf<uint32_t>& rb = X.rb;
+  if (!rb.alloc(12)) {
+    err = "out of device memory (BVH build)";
+    return RG_ERR_OUT_OF_MEMORY;
+  }
   {
     std::vector<uint32_t> init(12);
     for (int k = 0; k < 3; k++) { init[k] = 0xFFFFFFFFu; init[3 + k] = 0u; init[6 + k] = 0xFFFFFFFFu; init[9 + k] = 0u; }
@@ -826,9 +858,11 @@ rg_status buildDeviceBvh(DeviceScene& ds, int nbins, bool wide, cudaStream_t st,
   const size_t maxNodes = 2 * (size_t)n + 1;
   // bins for at most chunkTasks open nodes at a time (<= 256 MB)
   const int chunkTasks = (int)std::min<size_t>((size_t)n / 4 + 2, ((size_t)256 << 20) / (sizeof(BinData) * nbins));
-  DevBuf<BNode> nodes;
-  DevBuf<int> idxA, idxB, nodeA, nodeB, tasksA, tasksB, counters, pflags, pbefore;
-  DevBuf<BinData> bins;
+  DevBuf<BNode>& nodes = X.nodes;
+  DevBuf<int> &idxA = X.idxA, &idxB = X.idxB, &nodeA = X.nodeA, &nodeB = X.nodeB, &tasksA = X.tasksA,
+  &tasksB = X.tasksB, &counters = X.counters, &pflags = X.pflags, &pbefore = X.pbefore;
+  DevBuf<BinData>& bins = X.bins;
+  trace.mark("prep kern", 0, n);
   if (!nodes.alloc(maxNodes) || !idxA.alloc(n) || !idxB.alloc(n) || !nodeA.alloc(n) || !nodeB.alloc(n) ||
       !lo2.alloc(n) || !hi2.alloc(n) || !pflags.alloc(n) || !pbefore.alloc(n) ||
       !tasksA.alloc((size_t)n / 4 + 2) || !tasksB.alloc((size_t)n / 4 + 2) || !counters.alloc(4) ||
@@ -861,7 +895,7 @@ rg_status buildDeviceBvh(DeviceScene& ds, int nbins, bool wide, cudaStream_t st,
   // scratch of the partition's prefix sum
   size_t scanBytes = 0;
   cub::DeviceScan::ExclusiveSum(nullptr, scanBytes, pflags.p, pbefore.p, n, st);
-  DevBuf<unsigned char> scanTmp;
+  DevBuf<unsigned char>& scanTmp = X.scanTmp;
   if (!scanTmp.alloc(scanBytes + 16)) {
     err = "out of device memory (BVH build)";
     return RG_ERR_OUT_OF_MEMORY;
@@ -871,6 +905,7 @@ rg_status buildDeviceBvh(DeviceScene& ds, int nbins, bool wide, cudaStream_t st,
   float4* altLo = lo2.p;
   float4* altHi = hi2.p;
   int levels = 0;
+  trace.mark("alloc tree", 0, n);
   trace.mark("prep", 0, numTasks);
   while (numTasks > 0) {
     levels++;
@@ -918,48 +953,68 @@ rg_status buildDeviceBvh(DeviceScene& ds, int nbins, bool wide, cudaStream_t st,
     return RG_ERR_DEVICE_STATUS;
   }
   ds.buildLevels = levels;
+  trace.mark("levels end", 0, n);
   if (!ds.triVerts.alloc((size_t)n * 3) || !ds.triShade.alloc((size_t)n * 3) || !ds.triOrig.alloc(n)) {
     err = "out of device memory (triangles)";
     return RG_ERR_OUT_OF_MEMORY;
   }
   if (ds.hasUV) ds.triUV.alloc((size_t)n * 3);
+  trace.mark("alloc tris", 0, n);
   if (wide) {
     // collapse to the 8-wide compressed layout, level by level
     ds.bvhWidth = 8;
-    const int maxNodes8 = numNodes + 1;
-    DevBuf<int2> ta, tb;
-    DevBuf<int> order, c8;
-    if (!ds.nodes8.alloc((size_t)maxNodes8 * kNode8Vec) || !ta.alloc(maxNodes8) || !tb.alloc(maxNodes8) || !order.alloc(n) ||
-        !c8.alloc(4)) {
+    const int maxTasks8 = numNodes + 1;
+    DevBuf<int2> &ta = X.ta, &tb = X.tb;
+    DevBuf<int> &order = X.order, &c8 = X.c8;
+    if (!ta.alloc(maxTasks8) || !tb.alloc(maxTasks8) || !order.alloc(n) || !c8.alloc(4)) {
       err = "out of device memory (wide BVH)";
       return RG_ERR_OUT_OF_MEMORY;
     }
-    const int init[4] = {1, 0, 0, 0};  // [0] nodes (root preallocated) [1] triangles [2] next tasks [3] error
-    cudaMemcpyAsync(c8.p, init, sizeof(init), cudaMemcpyHostToDevice, st);
-    const int2 root = make_int2(0, 0);
-    cudaMemcpyAsync(ta.p, &root, sizeof(int2), cudaMemcpyHostToDevice, st);
-    int nt = 1;
-    int2* cur = ta.p;
-    int2* nxt = tb.p;
-    int lv = 0;
-    while (nt > 0) {
-      cudaMemsetAsync(c8.p + 2, 0, sizeof(int), st);
-      k_collapse<<<gridFor(nt, 64), 64, 0, st>>>(nt, cur, nodes.p, curIdx, ds.nodes8.p, c8.p, nxt, order.p, maxNodes8);
-      cudaMemcpyAsync(&nt, c8.p + 2, sizeof(int), cudaMemcpyDeviceToHost, st);
-      if (cudaStreamSynchronize(st) != cudaSuccess) {
-        err = "wide BVH collapse failed";
-        return RG_ERR_CUDA;
+    // two passes over the levels: the first counts the 8-wide nodes, so the node
+    // array is allocated at its size (about a seventh of the binary node count)
+    int numNodes8 = 0;
+    for (int pass = 0; pass < 2; pass++) {
+      const bool countOnly = pass == 0;
+      if (!countOnly && !ds.nodes8.alloc((size_t)numNodes8 * kNode8Vec)) {
+        err = "out of device memory (wide BVH)";
+        return RG_ERR_OUT_OF_MEMORY;
       }
-      trace.mark("collapse", lv + 1, nt);
-      std::swap(cur, nxt);
-      if (++lv > 200) {
-        err = "wide BVH collapse did not converge";
-        return RG_ERR_DEVICE_STATUS;
+      trace.mark(countOnly ? "count wide" : "alloc wide", 0, numNodes8);
+      const int init[4] = {1, 0, 0, 0};  // [0] nodes (root preallocated) [1] triangles [2] next tasks [3] error
+      cudaMemcpyAsync(c8.p, init, sizeof(init), cudaMemcpyHostToDevice, st);
+      const int2 root = make_int2(0, 0);
+      cudaMemcpyAsync(ta.p, &root, sizeof(int2), cudaMemcpyHostToDevice, st);
+      int nt = 1;
+      int2* cur = ta.p;
+      int2* nxt = tb.p;
+      int lv = 0;
+      while (nt > 0) {
+        cudaMemsetAsync(c8.p + 2, 0, sizeof(int), st);
+        k_collapse<<<gridFor(nt, 64), 64, 0, st>>>(nt, cur, nodes.p, curIdx, ds.nodes8.p, c8.p, nxt, order.p,
+                                                   numNodes8, countOnly);
+        cudaMemcpyAsync(&nt, c8.p + 2, sizeof(int), cudaMemcpyDeviceToHost, st);
+        if (cudaStreamSynchronize(st) != cudaSuccess) {
+          err = "wide BVH collapse failed";
+          return RG_ERR_CUDA;
+        }
+        if (!countOnly) trace.mark("collapse", lv + 1, nt);
+        std::swap(cur, nxt);
+        if (++lv > 200) {
+          err = "wide BVH collapse did not converge";
+          return RG_ERR_DEVICE_STATUS;
+        }
+      }
+      if (countOnly) {
+        if (cudaMemcpy(&numNodes8, c8.p, sizeof(int), cudaMemcpyDeviceToHost) != cudaSuccess || numNodes8 < 1 ||
+            numNodes8 > maxTasks8) {
+          err = "wide BVH node count failed";
+          return RG_ERR_DEVICE_STATUS;
+        }
       }
     }
     int h8[4];
     cudaMemcpy(h8, c8.p, sizeof(h8), cudaMemcpyDeviceToHost);
-    if (h8[3] != 0 || h8[1] != n) {
+    if (h8[3] != 0 || h8[1] != n || h8[0] != numNodes8) {
       err = "wide BVH collapse error (nodes " + std::to_string(h8[0]) + ", triangles " + std::to_string(h8[1]) + ")";
       return RG_ERR_DEVICE_STATUS;
     }
@@ -976,14 +1031,19 @@ rg_status buildDeviceBvh(DeviceScene& ds, int nbins, bool wide, cudaStream_t st,
   }
   // binary traversal layout
   ds.bvhWidth = 2;
-  DevBuf<int> flags, trav;
-  flags.alloc(numNodes);
-  trav.alloc(numNodes);
+  DevBuf<int> &flags = X.flags, &trav = X.trav;
+  if (!flags.alloc(numNodes) || !trav.alloc(numNodes)) {
+    err = "out of device memory (BVH layout)";
+    return RG_ERR_OUT_OF_MEMORY;
+  }
   k_innerFlags<<<gridFor(numNodes, 256), 256, 0, st>>>(numNodes, nodes.p, flags.p);
   size_t tmpBytes = 0;
   cub::DeviceScan::ExclusiveSum(nullptr, tmpBytes, flags.p, trav.p, numNodes, st);
-  DevBuf<unsigned char> tmp;
-  tmp.alloc(tmpBytes + 16);
+  DevBuf<unsigned char>& tmp = X.tmp;
+  if (!tmp.alloc(tmpBytes + 16)) {
+    err = "out of device memory (BVH layout)";
+    return RG_ERR_OUT_OF_MEMORY;
+  }
   cub::DeviceScan::ExclusiveSum(tmp.p, tmpBytes, flags.p, trav.p, numNodes, st);
   int lastFlag = 0, lastTrav = 0;
   cudaMemcpyAsync(&lastFlag, flags.p + numNodes - 1, sizeof(int), cudaMemcpyDeviceToHost, st);

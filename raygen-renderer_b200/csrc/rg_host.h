@@ -8,6 +8,7 @@
 #include <cstdint>
 #include <mutex>
 #include <string>
+#include <utility>
 #include <vector>
 
 #include "../../include/raygen_b200.h"
@@ -50,6 +51,10 @@ struct DevBuf {
   DevBuf(const DevBuf&) = delete;
   DevBuf& operator=(const DevBuf&) = delete;
   ~DevBuf() { release(); }
+  void swap(DevBuf& o) {
+    std::swap(p, o.p);
+    std::swap(n, o.n);
+  }
   bool alloc(size_t count) {
     if (count <= n && p) return true;
     release();
@@ -115,11 +120,20 @@ bool decodeJpeg(const std::vector<unsigned char>& bytes, TextureStore& out, std:
 bool decodePng(const std::vector<unsigned char>& bytes, TextureStore& out, std::string& err);
 bool writeImageFile(const std::string& path, int W, int H, const float* rgba, std::string& err);
 
+// Working memory of the BVH build (rg_bvh.cu).
+struct BvhScratch;
+void freeBvhScratch(BvhScratch* s);
+
 // Device-resident scene (BVH + triangle and light tables).
 struct DeviceScene {
   int numTris = 0;
   bool hasUV = false;
-  // world-space inputs (freed after the build)
+  // keepBuffers: the scene is rebuilt in place (a render handle): the inputs and
+  // the build's working memory stay allocated for the next scene, otherwise
+  // they are freed after the build
+  bool keepBuffers = false;
+  BvhScratch* scratch = nullptr;
+  // world-space inputs
   DevBuf<float> inPos, inNrm, inUV;
   DevBuf<int> inTriMesh;
   DevBuf<float> view;
@@ -157,10 +171,14 @@ struct DeviceScene {
   int numNodes = 0;
   int rootIsLeaf = 0, rootLeafRef = 0;
   int buildLevels = 0;
-  // device bytes held by the scene after its build (inputs already freed)
+  // device bytes held by the scene after its build
   size_t deviceBytes() const;
+  // takes over the device buffers of the scene it replaces: DevBuf::alloc only
+  // grows, so a scene no larger than the last one allocates no device memory
+  void adoptBuffers(DeviceScene& old);
   ~DeviceScene() {
     for (auto* t : texels) delete t;
+    freeBvhScratch(scratch);
   }
 };
 
@@ -172,8 +190,10 @@ struct KpcnNet;
 KpcnNet* kpcnOf(rg_denoiser* d);
 rg_status kpcnDenoiseDevice(KpcnNet& n, int W, int H, const float4* noisy, const __half* normal, const __half* albedo,
                             const __half* depth, const int* cnt, float intensity, float4* out, cudaStream_t st);
+// keep: reuse `out`'s buffers for the new scene and keep them afterwards
+// (DeviceScene::keepBuffers); otherwise `out` is replaced by a fresh scene.
 rg_status prepareScene(const rg_scene_desc* d, int bins, bool wide, cudaStream_t st, int* errWord,
-                       std::unique_ptr<DeviceScene>& out, DevScene& S, Mat4& view, float* buildMs);
+                       std::unique_ptr<DeviceScene>& out, DevScene& S, Mat4& view, float* buildMs, bool keep = false);
 
 void setLastError(const std::string& msg);
 
