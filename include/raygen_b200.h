@@ -276,6 +276,11 @@ void rg_medium_defaults(rg_medium* m);
 rg_status rg_create(const rg_settings* s, rg_handle** out);
 rg_status rg_destroy(rg_handle* h);
 rg_status rg_update_settings(rg_handle* h, const rg_settings* s);
+/* Copies the scene to the device and builds its BVH.  The handle rebuilds in
+ * place: the previous scene's device buffers and the build's working arrays are
+ * reused (they only grow), so a scene no larger than the last one allocates no
+ * device memory.  A scene with less than half the previous one's triangles
+ * starts from fresh buffers. */
 rg_status rg_set_scene(rg_handle* h, const rg_scene_desc* scene);
 /* Blocking render (RayRenderer::render, rayrenderer.cpp:478-596).  Waves are
  * paced one behind the device, so progress is reported for completed waves and

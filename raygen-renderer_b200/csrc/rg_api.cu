@@ -43,6 +43,21 @@ void setLastError(const std::string& msg) { g_lastError = msg; }
 
 __global__ void k_nextWave(int* cur) { *cur += 1; }
 
+// The render's sample total: the sum of the per-pixel sample counts, added to *out.
+__global__ void k_sumCounts(int n, const int* __restrict__ cnt, unsigned long long* out) {
+  __shared__ unsigned long long part[8];
+  unsigned long long v = 0;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) v += (unsigned)cnt[i];
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+  if ((threadIdx.x & 31) == 0) part[threadIdx.x >> 5] = v;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    unsigned long long t = 0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); w++) t += part[w];
+    atomicAdd(out, t);
+  }
+}
+
 void keepPoolMemory() {
   static std::mutex mu;
   static std::vector<char> done;
@@ -836,12 +851,12 @@ rg_status prepareScene(const rg_scene_desc* d, int bins, bool wide, cudaStream_t
     if (d->materials[objMat[o]].emission > 0.0f)
       for (int m : objMeshes[o]) isLightMesh[m] = 1;
   trace.mark("scene: checks");
-  // the previous scene's memory is reused (keep) or goes back to the pool; the
-  // triangle arrays start copying now and the host pass below runs while they
-  // are in flight
+  // the previous scene's memory is reused (keep, unless the new scene has less
+  // than half its triangles) or goes back to the pool; the triangle arrays start
+  // copying now and the host pass below runs while they are in flight
   {
     std::unique_ptr<DeviceScene> next(new DeviceScene());
-    if (keep && out) next->adoptBuffers(*out);
+    if (keep && out && 2 * (int64_t)nt >= (int64_t)out->numTris) next->adoptBuffers(*out);
     next->keepBuffers = keep;
     out = std::move(next);
   }
@@ -1176,7 +1191,9 @@ static rg_status runPass(rg_handle* h, const DevRender& R, int numPixels, const 
                          int& wavesDone, int totalWavesHint, bool profile, double* kernelMs, cudaEvent_t start,
                          bool& started) {
   if (numPixels <= 0 || spp <= 0) return RG_OK;
+  HostTrace trace;
   const long long cap = wavePaths(h->st);
+  trace.mark("pass: wave size");
   std::vector<DevSegment> sg;
   const int spw = numPixels >= cap ? 1 : (int)std::min<long long>(spp, std::max<long long>(1, cap / numPixels));
   const int pixChunk = (int)std::min<long long>(numPixels, cap);
@@ -1211,6 +1228,7 @@ static rg_status runPass(rg_handle* h, const DevRender& R, int numPixels, const 
   const int maxIter = h->scene->hasHaze ? 2 * R.maxDepth + 3 : R.maxDepth + 2;
   rg_status rs = ensureQueues(h, capacity, maxIter, h->dscene.numVolLights > 0);
   if (rs != RG_OK) return rs;
+  trace.mark("pass: queues");
   if (!h->waves.alloc(ws.size() + 1)) {
     setLastError("out of device memory (waves)");
     return RG_ERR_OUT_OF_MEMORY;
@@ -1231,6 +1249,7 @@ static rg_status runPass(rg_handle* h, const DevRender& R, int numPixels, const 
     RG_CUDA_CHECK(cudaMemcpyAsync(h->jobsDev.p, &J, sizeof(J), cudaMemcpyHostToDevice, h->stream));
     RG_CUDA_CHECK(cudaStreamSynchronize(h->stream));
   }
+  trace.mark("pass: job copied");
   // the kernels read the current wave from a fixed one-element slot
   if (!h->waveSlot.alloc(1)) return RG_ERR_OUT_OF_MEMORY;
   DevWave* slot = h->waveSlot.p;
@@ -1270,6 +1289,7 @@ static rg_status runPass(rg_handle* h, const DevRender& R, int numPixels, const 
       return RG_ERR_CUDA;
     }
     h->graphKey = key;
+    trace.mark("pass: wave graph captured");
   }
   // Waves are paced: wave k is launched, then the host waits for wave k-1.  One
   // wave stays queued behind the running one (the device never idles), while
@@ -1453,6 +1473,7 @@ rg_status renderLocked(rg_handle* h) {
   }
   launchTonemap(N, h->hdr.p, h->ldr.p, st);
   cudaEventRecord(t2, st);
+  k_sumCounts<<<std::min((N + 255) / 256, 4 * 148), 256, 0, st>>>(N, h->cnt.p, h->stats.p + 6);
   trace.mark("post launched");
   const cudaError_t se = cudaStreamSynchronize(st);
   trace.mark("stream synchronised");
@@ -1484,16 +1505,10 @@ rg_status renderLocked(rg_handle* h) {
   S.connect_ms = kms[2];
   S.waves = wavesDone;
   S.device_error = derr;
-  {
-    std::vector<int> c(N);
-    cudaMemcpy(c.data(), h->cnt.p, sizeof(int) * N, cudaMemcpyDeviceToHost);
-    uint64_t tot = 0;
-    for (int v : c) tot += (uint64_t)v;
-    S.samples = tot;
-  }
+  S.samples = stv[6];
   const int perIter = 3 + (h->dscene.numPointLights > 0) + (h->dscene.envOn != 0) + (h->dscene.numVolLights > 0);
   const int perWave = s.shader_provider == 5 ? (3 + h->maxIter * perIter) : 4;
-  S.kernel_launches = wavesDone * perWave;
+  S.kernel_launches = wavesDone * perWave + 1;  // + the sample total
   if (derr != 0) {
     setLastError("device error flag raised: " + std::to_string(derr));
     return RG_ERR_DEVICE_STATUS;
