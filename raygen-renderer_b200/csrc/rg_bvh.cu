@@ -838,7 +838,10 @@ rg_status buildDeviceBvh(DeviceScene& ds, int nbins, bool wide, cudaStream_t st,
     err = "out of device memory (triangle staging)";
     return RG_ERR_OUT_OF_MEMORY;
   }
-  if (ds.hasUV && !uvTmp.alloc((size_t)n * 3)) return RG_ERR_OUT_OF_MEMORY;
+  if (ds.hasUV && !uvTmp.alloc((size_t)n * 3)) {
+    err = "out of device memory (triangle staging)";
+    return RG_ERR_OUT_OF_MEMORY;
+  }
   trace.mark("alloc stage", 0, n);
   k_prepTriangles<<<gridFor(n, 256), 256, 0, st>>>(n, ds.inPos.p, ds.inNrm.p, ds.hasUV ? ds.inUV.p : nullptr,
                                                    ds.inTriMesh.p, ds.meshObj.p, ds.objMat.p, ds.mats.p, ds.view.p,
@@ -958,7 +961,10 @@ rg_status buildDeviceBvh(DeviceScene& ds, int nbins, bool wide, cudaStream_t st,
     err = "out of device memory (triangles)";
     return RG_ERR_OUT_OF_MEMORY;
   }
-  if (ds.hasUV) ds.triUV.alloc((size_t)n * 3);
+  if (ds.hasUV && !ds.triUV.alloc((size_t)n * 3)) {
+    err = "out of device memory (triangles)";
+    return RG_ERR_OUT_OF_MEMORY;
+  }
   trace.mark("alloc tris", 0, n);
   if (wide) {
     // collapse to the 8-wide compressed layout, level by level
@@ -1054,7 +1060,10 @@ rg_status buildDeviceBvh(DeviceScene& ds, int nbins, bool wide, cudaStream_t st,
   if (numInner == 0) {
     ds.rootIsLeaf = 1;
     ds.rootLeafRef = ~((0 << 3) | (n - 1));
-    ds.nodes.alloc(4);
+    if (!ds.nodes.alloc(4)) {
+      err = "out of device memory (BVH nodes)";
+      return RG_ERR_OUT_OF_MEMORY;
+    }
   } else {
     if (!ds.nodes.alloc((size_t)numInner * 4)) {
       err = "out of device memory (BVH nodes)";
